@@ -1,0 +1,474 @@
+// fs_capi.cu -- the extern "C" entry points of include/fsb200.h.
+#include "fs_internal.cuh"
+#include <cmath>
+#include <cstring>
+#include <new>
+
+namespace {
+
+__global__ void k_initial_mdot(int N, int F, int B, double rho, const int32_t *fown, const int32_t *fnbr,
+                               const double *gf, const double *sf, const double *u, const double *v,
+                               const double *w, double *mdot, const int32_t *btype, const double *bsf,
+                               const double *bu, const double *bv, const double *bw, double *bmdot) {
+  // CalculateInitialmdot (ContinuityEquation/InitializaMdot.for:20-60), Densityf = rho
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < F) {
+    int k = (int)t, i = fown[k], j = fnbr[k];
+    double g = gf[k];
+    double uf = g * u[i] + (1. - g) * u[j];
+    double vf = g * v[i] + (1. - g) * v[j];
+    double wf = g * w[i] + (1. - g) * w[j];
+    mdot[k] = rho * (uf * sf[k] + vf * sf[F + k] + wf * sf[2L * F + k]);
+  } else if (t < (long)F + B) {
+    int b = (int)(t - F), ty = btype[b];
+    if (ty == FS_BC_WALL_NOSLIP || ty == FS_BC_WALL_SLIP) bmdot[b] = 0.;
+    else bmdot[b] = rho * (bsf[b] * bu[b] + bsf[B + b] * bv[b] + bsf[2L * B + b] * bw[b]);
+  }
+}
+
+__global__ void k_divide(int N, double *ac, double urf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) ac[i] = ac[i] / urf;
+}
+
+__device__ double blk_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.;
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;
+}
+__device__ double blk_max(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = -1e300;
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : -1e300;
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+  }
+  return r;
+}
+
+// CalculateResiduals at dphi=0 on the current system (CalculateResidualsRoutine.for:30-67)
+__global__ void k_residual_partials(int N, const double *ac, const double *bc, const double *fi, double *red, int nblk) {
+  __shared__ double sh[32];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double r = 0., acphi = -1.;
+  if (i < N) { r = fabs(bc[i]); acphi = fabs(ac[i] * fi[i]); }
+  double s0 = blk_sum(r, sh), s1 = blk_sum(r * r, sh), m0 = blk_max(r, sh), m1 = blk_max(acphi, sh);
+  if (threadIdx.x == 0) {
+    red[RED_SUM0 * nblk + blockIdx.x] = s0; red[RED_SUM1 * nblk + blockIdx.x] = s1;
+    red[RED_MAX0 * nblk + blockIdx.x] = m0; red[RED_MAX1 * nblk + blockIdx.x] = m1;
+  }
+}
+__global__ void k_residual_final2(const double *red, int nblk, int N, int q, double *rb) {
+  __shared__ double sh[32];
+  double s0 = 0., s1 = 0., m0 = -1., m1 = -1.;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    s0 += red[RED_SUM0 * nblk + b]; s1 += red[RED_SUM1 * nblk + b];
+    m0 = fmax(m0, red[RED_MAX0 * nblk + b]); m1 = fmax(m1, red[RED_MAX1 * nblk + b]);
+  }
+  s0 = blk_sum(s0, sh); s1 = blk_sum(s1, sh); m0 = blk_max(m0, sh); m1 = blk_max(m1, sh);
+  if (threadIdx.x == 0) {
+    rb[RB_ABS + q] = s0; rb[RB_MAX + q] = m0; rb[RB_RMS + q] = sqrt(s1 / N);
+    rb[RB_SCL + q] = (q == 3) ? 0. : m0 / (m1 + 1.0e-15);
+  }
+}
+
+}  // namespace
+
+static double *field_ptr(fs_ctx *c, int f, size_t *n) {
+  const size_t N = c->N, F = c->F, B = c->B, W = c->W;
+  switch (f) {
+  case FS_F_U: *n = N; return c->u;
+  case FS_F_V: *n = N; return c->v;
+  case FS_F_W: *n = N; return c->w;
+  case FS_F_P: *n = N; return c->p;
+  case FS_F_PC: *n = N; return c->pc;
+  case FS_F_MDOT: *n = F; return c->mdot;
+  case FS_F_BU: *n = B; return c->bu;
+  case FS_F_BV: *n = B; return c->bv;
+  case FS_F_BW: *n = B; return c->bw;
+  case FS_F_BP: *n = B; return c->bp;
+  case FS_F_BPC: *n = B; return c->bpc;
+  case FS_F_BMDOT: *n = B; return c->bmdot;
+  case FS_F_AC: *n = N; return c->ac;
+  case FS_F_BC: *n = N; return c->bc;
+  case FS_F_ANB: *n = W * N; return c->anb;
+  case FS_F_DU1: *n = N; return c->du1;
+  case FS_F_DV1: *n = N; return c->dv1;
+  case FS_F_DW1: *n = N; return c->dw1;
+  case FS_F_DU2: *n = N; return c->du2;
+  case FS_F_DV2: *n = N; return c->dv2;
+  case FS_F_DW2: *n = N; return c->dw2;
+  case FS_F_UGRAD: *n = 3 * N; return c->ug;
+  case FS_F_VGRAD: *n = 3 * N; return c->vg;
+  case FS_F_WGRAD: *n = 3 * N; return c->wg;
+  case FS_F_PGRAD: *n = 3 * N; return c->pg;
+  case FS_F_PCGRAD: *n = 3 * N; return c->pcg;
+  case FS_F_VOLUME: *n = N; return c->vol;
+  case FS_F_XC: *n = 3 * N; return c->xc;
+  case FS_F_GFACTOR: *n = F; return c->gf;
+  case FS_F_SF: *n = 3 * F; return c->sf;
+  case FS_F_GDIFF: *n = F; return c->gdiff;
+  case FS_F_FT: *n = 3 * F; return c->tf;
+  case FS_F_BSF: *n = 3 * B; return c->bsf;
+  case FS_F_DPHI: *n = N; return c->dphi;
+  }
+  *n = 0;
+  return nullptr;
+}
+
+static int alloc0(fs_ctx *ctx, double **p, size_t n) {
+  FS_CK(cudaMalloc((void **)p, sizeof(double) * (n ? n : 1)));
+  FS_CK(cudaMemsetAsync(*p, 0, sizeof(double) * (n ? n : 1), ctx->st));
+  return FS_OK;
+}
+
+static void free_all(fs_ctx *c) {
+  void *ptrs[] = {c->slot, c->cn, c->ncf, c->fown, c->fnbr, c->bown, c->btype, c->color_rows,
+                  c->vol, c->xc, c->gf, c->sf, c->dcfv, c->dcf, c->gdiff, c->tf, c->dfp, c->fa,
+                  c->bsf, c->bfa, c->bnf, c->bdv, c->bgdiff, c->btf, c->bnzii,
+                  c->u, c->v, c->w, c->p, c->pc, c->mdot, c->bu, c->bv, c->bw, c->bp, c->bpc, c->bmdot,
+                  c->ug, c->vg, c->wg, c->pg, c->pcg, c->bug, c->bvg, c->bwg, c->bpg, c->bpcg, c->gtmp,
+                  c->du1, c->dv1, c->dw1, c->du2, c->dv2, c->dw2, c->us, c->vs, c->ws,
+                  c->ac, c->anb, c->bc, c->dphi, c->ac_int, c->bc_int, c->effdiv, c->pcoef,
+                  c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky,
+                  c->red, c->redi, c->resblk, c->d_iters, c->d_status};
+  for (void *p : ptrs) if (p) cudaFree(p);
+}
+
+extern "C" {
+
+int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **out) {
+  if (!mesh || !cfg || !out) return FS_E_ARG;
+  *out = nullptr;
+  if (mesh->n_patches != cfg->n_patches || cfg->n_patches > FS_MAX_PATCHES) return FS_E_ARG;
+  if (cfg->method_decompose_s < 1 || cfg->method_decompose_s > 3) return FS_E_ARG;
+  fs_ctx *ctx = new (std::nothrow) fs_ctx();
+  if (!ctx) return FS_E_NOMEM;
+  ctx->cfg = *cfg;
+  ctx->dev = device;
+  int rc = FS_OK;
+  auto fail = [&](int r) { free_all(ctx); if (ctx->st) cudaStreamDestroy(ctx->st); delete ctx; return r; };
+  if (cudaSetDevice(device) != cudaSuccess) return fail(FS_E_CUDA);
+  if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(FS_E_CUDA);
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  for (auto &e : ctx->ev) cudaEventCreate(&e);
+  if (ctx->cfg.set_reference_pressure < 0) ctx->cfg.set_reference_pressure = 0;  // no pressure-specified patch types
+  if ((rc = fs_geometry_build(ctx, mesh))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
+  const size_t N = ctx->N, F = ctx->F, B = ctx->B, W = ctx->W;
+  if (ctx->cfg.ref_pressure_cell >= (int)N) return fail(FS_E_ARG);
+  double **cellv[] = {&ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->pc, &ctx->du1, &ctx->dv1, &ctx->dw1, &ctx->du2,
+                      &ctx->dv2, &ctx->dw2, &ctx->us, &ctx->vs, &ctx->ws, &ctx->ac, &ctx->bc, &ctx->dphi,
+                      &ctx->ac_int, &ctx->effdiv, &ctx->kx, &ctx->kr, &ctx->kr0, &ctx->kp, &ctx->kv, &ctx->ks,
+                      &ctx->kt, &ctx->kz, &ctx->ky};
+  for (auto p : cellv) if ((rc = alloc0(ctx, p, N))) return fail(rc);
+  double **cell3[] = {&ctx->ug, &ctx->vg, &ctx->wg, &ctx->pg, &ctx->pcg, &ctx->bc_int};
+  for (auto p : cell3) if ((rc = alloc0(ctx, p, 3 * N))) return fail(rc);
+  if ((rc = alloc0(ctx, &ctx->gtmp, 12 * N))) return fail(rc);
+  if ((rc = alloc0(ctx, &ctx->anb, W * N))) return fail(rc);
+  if ((rc = alloc0(ctx, &ctx->mdot, F)) || (rc = alloc0(ctx, &ctx->pcoef, F))) return fail(rc);
+  double **bnd[] = {&ctx->bu, &ctx->bv, &ctx->bw, &ctx->bp, &ctx->bpc, &ctx->bmdot};
+  for (auto p : bnd) if ((rc = alloc0(ctx, p, B))) return fail(rc);
+  double **bnd3[] = {&ctx->bug, &ctx->bvg, &ctx->bwg, &ctx->bpg, &ctx->bpcg};
+  for (auto p : bnd3) if ((rc = alloc0(ctx, p, 3 * B))) return fail(rc);
+  size_t nblk = (size_t)fs_grid((long)N);
+  size_t nred = 8 * (nblk > FS_RED_BLOCKS ? nblk : FS_RED_BLOCKS);
+  if ((rc = alloc0(ctx, &ctx->red, nred))) return fail(rc);
+  if (cudaMalloc(&ctx->redi, sizeof(int64_t) * (nblk > FS_RED_BLOCKS ? nblk : FS_RED_BLOCKS)) != cudaSuccess) return fail(FS_E_NOMEM);
+  if ((rc = alloc0(ctx, &ctx->resblk, RB_SIZE))) return fail(rc);
+  if (cudaMalloc(&ctx->d_iters, sizeof(int32_t) * 8) != cudaSuccess) return fail(FS_E_NOMEM);
+  cudaMemsetAsync(ctx->d_iters, 0, sizeof(int32_t) * 8, ctx->st);
+  if (cudaMalloc(&ctx->d_status, sizeof(int32_t) * 8) != cudaSuccess) return fail(FS_E_NOMEM);
+  cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * 8, ctx->st);
+  // boundary values from the patches (setBoundaryConditions): wall / inlet velocities
+  std::vector<double> hb(3 * B, 0.);
+  for (size_t b = 0; b < B; b++) {
+    int s = ctx->h_bset[b], t = ctx->cfg.patch_type[s];
+    if (t == FS_BC_WALL_NOSLIP || t == FS_BC_INLET_VEL) {
+      hb[b] = ctx->cfg.patch_vel[s][0]; hb[B + b] = ctx->cfg.patch_vel[s][1]; hb[2 * B + b] = ctx->cfg.patch_vel[s][2];
+    }
+  }
+  if (B) {
+    cudaMemcpyAsync(ctx->bu, hb.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
+    cudaMemcpyAsync(ctx->bv, hb.data() + B, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
+    cudaMemcpyAsync(ctx->bw, hb.data() + 2 * B, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
+  }
+  k_initial_mdot<<<fs_grid((long)F + B), FS_BLOCK, 0, ctx->st>>>((int)N, (int)F, (int)B, ctx->cfg.rho, ctx->fown, ctx->fnbr,
+      ctx->gf, ctx->sf, ctx->u, ctx->v, ctx->w, ctx->mdot, ctx->btype, ctx->bsf, ctx->bu, ctx->bv, ctx->bw, ctx->bmdot);
+  ctx->launches++;
+  if (cudaStreamSynchronize(ctx->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return fail(FS_E_CUDA);
+  *out = ctx;
+  return FS_OK;
+}
+
+int fs_destroy(fs_ctx *ctx) {
+  if (!ctx) return FS_OK;
+  cudaSetDevice(ctx->dev);
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  fs_mg_free(ctx);
+  free_all(ctx);
+  for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  delete ctx;
+  return FS_OK;
+}
+
+int fs_sizes(const fs_ctx *ctx, int32_t *n, int32_t *f, int32_t *b, int32_t *w) {
+  if (!ctx) return FS_E_ARG;
+  if (n) *n = ctx->N;
+  if (f) *f = ctx->F;
+  if (b) *b = ctx->B;
+  if (w) *w = ctx->W;
+  return FS_OK;
+}
+
+const char *fs_last_error(const fs_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int fs_solve_momentum(fs_ctx *ctx, int comp) {
+  if (!ctx || comp < 0 || comp > 2) return FS_E_ARG;
+  int rc = fs_momentum_assemble(ctx, comp);
+  if (rc) return rc;
+  double *fi = comp == 0 ? ctx->u : comp == 1 ? ctx->v : ctx->w;
+  return fs_linear_solve(ctx, comp + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom);
+}
+
+int fs_solve_continuity(fs_ctx *ctx) {
+  if (!ctx) return FS_E_ARG;
+  int rc = fs_continuity_assemble(ctx);
+  if (rc) return rc;
+  rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
+  if (rc) return rc;
+  return fs_continuity_correct(ctx);
+}
+
+int fs_assemble_momentum(fs_ctx *ctx, int comp) {
+  if (!ctx || comp < 0 || comp > 2) return FS_E_ARG;
+  return fs_momentum_assemble(ctx, comp);
+}
+int fs_assemble_continuity(fs_ctx *ctx) { return ctx ? fs_continuity_assemble(ctx) : FS_E_ARG; }
+int fs_correct_continuity(fs_ctx *ctx) { return ctx ? fs_continuity_correct(ctx) : FS_E_ARG; }
+int fs_set_iteration(fs_ctx *ctx, int n_iter) {
+  if (!ctx) return FS_E_ARG;
+  ctx->nIter = n_iter;
+  return FS_OK;
+}
+
+static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
+  double rb[RB_SIZE];
+  int32_t it[8];
+  FS_CK(cudaMemcpyAsync(rb, ctx->resblk, sizeof(rb), cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaMemcpyAsync(it, ctx->d_iters, sizeof(it), cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  fs_residuals r{};
+  for (int q = 0; q < 5; q++) {
+    r.abs_[q] = rb[RB_ABS + q]; r.max_[q] = rb[RB_MAX + q]; r.rms[q] = rb[RB_RMS + q]; r.scaled[q] = rb[RB_SCL + q];
+    r.lin_iters[q] = it[q];
+  }
+  r.overall_imbalance = rb[RB_OVERALL];
+  r.imax_imbalance = (int)rb[RB_IMAX];
+  // PrintConvergenceHistory stop metric (PrintConvergenceToFileAndScreen.for:613-700)
+  const double *v = ctx->cfg.nstop_type == 1 ? r.abs_ : ctx->cfg.nstop_type == 2 ? r.max_ :
+                    ctx->cfg.nstop_type == 3 ? r.rms : r.scaled;
+  double s = 0.;
+  s = fmax(s, fmax(fabs(v[0]), fmax(fabs(v[1]), fabs(v[2]))));
+  s = fmax(s, fabs(v[4]));
+  r.source = s;
+  if (res) *res = r;
+  for (int q = 0; q < 5; q++)
+    if (!std::isfinite(r.abs_[q])) { ctx->err = "NaN/Inf residual"; return FS_E_NAN; }
+  return FS_OK;
+}
+
+int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res) {
+  if (!ctx) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  ctx->nIter++;
+  int rc;
+  cudaEventRecord(ctx->ev[0], ctx->st);
+  for (int c = 0; c < 3; c++) {
+    if ((rc = fs_momentum_assemble(ctx, c))) return rc;
+    double *fi = c == 0 ? ctx->u : c == 1 ? ctx->v : ctx->w;
+    if ((rc = fs_linear_solve(ctx, c + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom))) return rc;
+  }
+  cudaEventRecord(ctx->ev[1], ctx->st);
+  if ((rc = fs_continuity_assemble(ctx))) return rc;
+  cudaEventRecord(ctx->ev[2], ctx->st);
+  if ((rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont))) return rc;
+  cudaEventRecord(ctx->ev[3], ctx->st);
+  if ((rc = fs_continuity_correct(ctx))) return rc;
+  cudaEventRecord(ctx->ev[4], ctx->st);
+  rc = read_residuals(ctx, res);
+  cudaEventElapsedTime(&ctx->phase_ms[0], ctx->ev[0], ctx->ev[1]);
+  cudaEventElapsedTime(&ctx->phase_ms[2], ctx->ev[1], ctx->ev[2]);
+  cudaEventElapsedTime(&ctx->phase_ms[3], ctx->ev[2], ctx->ev[3]);
+  cudaEventElapsedTime(&ctx->phase_ms[4], ctx->ev[3], ctx->ev[4]);
+  ctx->phase_ms[1] = 0.f;
+  return rc;
+}
+
+int fs_simple_iteration_host(fs_ctx *ctx, double *u, double *v, double *w, double *p, double *mdot,
+                             double *bu, double *bv, double *bw, double *bp, double *bmdot, fs_residuals *res) {
+  if (!ctx || !u || !v || !w || !p || !mdot || !bu || !bv || !bw || !bp || !bmdot) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  const size_t N = ctx->N, F = ctx->F, B = ctx->B;
+  struct { double *h; double *d; size_t n; } t[] = {{u, ctx->u, N}, {v, ctx->v, N}, {w, ctx->w, N}, {p, ctx->p, N},
+      {mdot, ctx->mdot, F}, {bu, ctx->bu, B}, {bv, ctx->bv, B}, {bw, ctx->bw, B}, {bp, ctx->bp, B}, {bmdot, ctx->bmdot, B}};
+  for (auto &e : t) if (e.n) FS_CK(cudaMemcpyAsync(e.d, e.h, sizeof(double) * e.n, cudaMemcpyHostToDevice, ctx->st));
+  int rc = fs_simple_iteration(ctx, res);
+  if (rc) return rc;
+  for (auto &e : t) if (e.n) FS_CK(cudaMemcpyAsync(e.h, e.d, sizeof(double) * e.n, cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  return FS_OK;
+}
+
+int fs_gradient(fs_ctx *ctx, int var, int method, int n_iter) {
+  if (!ctx) return FS_E_ARG;
+  const double *phi, *bphi;
+  double *g, *bg;
+  switch (var) {
+  case FS_VAR_U: phi = ctx->u; bphi = ctx->bu; g = ctx->ug; bg = ctx->bug; break;
+  case FS_VAR_V: phi = ctx->v; bphi = ctx->bv; g = ctx->vg; bg = ctx->bvg; break;
+  case FS_VAR_W: phi = ctx->w; bphi = ctx->bw; g = ctx->wg; bg = ctx->bwg; break;
+  case FS_VAR_P: phi = ctx->p; bphi = ctx->bp; g = ctx->pg; bg = ctx->bpg; break;
+  case FS_VAR_PC: phi = ctx->pc; bphi = ctx->bpc; g = ctx->pcg; bg = ctx->bpcg; break;
+  default: return FS_E_ARG;
+  }
+  return fs_gradient_dev(ctx, 1, &var, &phi, &bphi, &g, &bg, &method, &n_iter);
+}
+
+int fs_gradient_host(fs_ctx *ctx, int var, int method, int n_iter, const double *phi, const double *bphi,
+                     double *grad, double *bgrad) {
+  if (!ctx || !phi || !bphi || !grad || !bgrad) return FS_E_ARG;
+  if (var < FS_VAR_U || var > FS_VAR_P || var == FS_VAR_MASS) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  const size_t N = ctx->N, B = ctx->B;
+  // stage through the (otherwise unused during this call) Krylov vectors
+  double *dphi_ = ctx->kz, *dbphi = nullptr, *dg = ctx->gtmp + 9 * N, *dbg = nullptr;
+  FS_CK(cudaMalloc(&dbphi, sizeof(double) * (B ? B : 1)));
+  FS_CK(cudaMalloc(&dbg, sizeof(double) * 3 * (B ? B : 1)));
+  FS_CK(cudaMemcpyAsync(dphi_, phi, sizeof(double) * N, cudaMemcpyHostToDevice, ctx->st));
+  if (B) FS_CK(cudaMemcpyAsync(dbphi, bphi, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st));
+  // the scratch of field slot 0 of the gradient passes is gtmp[0:3N]; dg sits in slot 3
+  double *gout = nullptr;
+  FS_CK(cudaMalloc(&gout, sizeof(double) * 3 * N));
+  const double *pp = dphi_, *bp = dbphi;
+  int rc = fs_gradient_dev(ctx, 1, &var, &pp, &bp, &gout, &dbg, &method, &n_iter);
+  (void)dg;
+  if (!rc) {
+    FS_CK(cudaMemcpyAsync(grad, gout, sizeof(double) * 3 * N, cudaMemcpyDeviceToHost, ctx->st));
+    if (B) FS_CK(cudaMemcpyAsync(bgrad, dbg, sizeof(double) * 3 * B, cudaMemcpyDeviceToHost, ctx->st));
+    FS_CK(cudaStreamSynchronize(ctx->st));
+  }
+  cudaFree(gout); cudaFree(dbphi); cudaFree(dbg);
+  return rc;
+}
+
+int fs_under_relax(fs_ctx *ctx, double urf) {
+  if (!ctx || urf == 0.) return FS_E_ARG;
+  k_divide<<<fs_grid(ctx->N), FS_BLOCK, 0, ctx->st>>>(ctx->N, ctx->ac, urf);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+static int residual_of_system(fs_ctx *ctx, int nf, const double *fi) {
+  int nblk = fs_grid(ctx->N);
+  k_residual_partials<<<nblk, FS_BLOCK, 0, ctx->st>>>(ctx->N, ctx->ac, ctx->bc, fi, ctx->red, nblk);
+  FS_LAUNCH_CHECK();
+  k_residual_final2<<<1, 1024, 0, ctx->st>>>(ctx->red, nblk, ctx->N, nf - 1, ctx->resblk);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+int fs_solve_equation(fs_ctx *ctx, int var, double rrf, int itmax, int solver) {
+  if (!ctx || var < FS_VAR_U || var > FS_VAR_PC) return FS_E_ARG;
+  double *fi = var == FS_VAR_U ? ctx->u : var == FS_VAR_V ? ctx->v : var == FS_VAR_W ? ctx->w : ctx->pc;
+  int rc = residual_of_system(ctx, var, fi);
+  if (rc) return rc;
+  return fs_linear_solve(ctx, var, fi, rrf, itmax, solver);
+}
+
+int fs_solve_system_host(fs_ctx *ctx, const double *ac, const double *anb, const double *bc, double *dphi,
+                         double rrf, int itmax, int solver, int *iters) {
+  if (!ctx || !ac || !anb || !bc || !dphi) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  const size_t N = ctx->N, W = ctx->W;
+  FS_CK(cudaMemcpyAsync(ctx->ac, ac, sizeof(double) * N, cudaMemcpyHostToDevice, ctx->st));
+  FS_CK(cudaMemcpyAsync(ctx->anb, anb, sizeof(double) * N * W, cudaMemcpyHostToDevice, ctx->st));
+  FS_CK(cudaMemcpyAsync(ctx->bc, bc, sizeof(double) * N, cudaMemcpyHostToDevice, ctx->st));
+  // solve into a zero field so the update equals dphi
+  double *fz = ctx->ky;
+  FS_CK(cudaMemsetAsync(fz, 0, sizeof(double) * N, ctx->st));
+  int rc = residual_of_system(ctx, FS_VAR_PC, fz);
+  if (rc) return rc;
+  rc = fs_linear_solve(ctx, FS_VAR_PC, fz, rrf, itmax, solver);
+  if (rc) return rc;
+  int32_t it = 0;
+  FS_CK(cudaMemcpyAsync(dphi, fz, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaMemcpyAsync(&it, ctx->d_iters + 3, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  if (iters) *iters = it;
+  return FS_OK;
+}
+
+int fs_residuals_get(fs_ctx *ctx, fs_residuals *res) {
+  if (!ctx || !res) return FS_E_ARG;
+  return read_residuals(ctx, res);
+}
+
+int fs_get_field(fs_ctx *ctx, int field, double *host, size_t n) {
+  if (!ctx || !host) return FS_E_ARG;
+  size_t m = 0;
+  double *d = field_ptr(ctx, field, &m);
+  if (!d || n != m) { ctx->err = "field id or size mismatch"; return FS_E_ARG; }
+  FS_CK(cudaMemcpyAsync(host, d, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  return FS_OK;
+}
+
+int fs_set_field(fs_ctx *ctx, int field, const double *host, size_t n) {
+  if (!ctx || !host) return FS_E_ARG;
+  size_t m = 0;
+  double *d = field_ptr(ctx, field, &m);
+  if (!d || n != m) { ctx->err = "field id or size mismatch"; return FS_E_ARG; }
+  FS_CK(cudaMemcpyAsync(d, host, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->st));
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  return FS_OK;
+}
+
+int fs_get_connectivity(fs_ctx *ctx, int32_t *ncf, int32_t *cf, int32_t *cn, int32_t *own_slot, int32_t *nbr_slot) {
+  if (!ctx) return FS_E_ARG;
+  const size_t N = ctx->N, W = ctx->W, F = ctx->F;
+  if (ncf) memcpy(ncf, ctx->h_ncf.data(), sizeof(int32_t) * N);
+  if (cf) memcpy(cf, ctx->h_cf.data(), sizeof(int32_t) * N * W);
+  if (cn) memcpy(cn, ctx->h_cn.data(), sizeof(int32_t) * N * W);
+  if (own_slot) memcpy(own_slot, ctx->h_own_slot.data(), sizeof(int32_t) * F);
+  if (nbr_slot) memcpy(nbr_slot, ctx->h_nbr_slot.data(), sizeof(int32_t) * F);
+  return FS_OK;
+}
+
+int fs_phase_times(fs_ctx *ctx, float *ms5) {
+  if (!ctx || !ms5) return FS_E_ARG;
+  for (int i = 0; i < 5; i++) ms5[i] = ctx->phase_ms[i];
+  return FS_OK;
+}
+
+int64_t fs_launch_count(const fs_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int fs_sync(fs_ctx *ctx) {
+  if (!ctx) return FS_E_ARG;
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  return FS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// fs_internal.cuh -- device context of the B200 SIMPLE inner loop.
+//
+// Data layout in HBM (all FP64 unless noted, SoA so every kernel streams
+// contiguous arrays):
+//   cells  (N):  vol, xc/yc/zc, u/v/w/p/pc, gradients as 3 blocks of N
+//   slots (W*N, slot-major like the reference's anb(N,NElementFaces)):
+//          slot[j*N+i] = (face<<1)|side  (face < F interior, F+b boundary;
+//          side 1 = this cell is the face's neighbour), -1 unused;
+//          cn[j*N+i]   = neighbour cell or -1 (ElementNeighbor)
+//   interior faces (F): own/nbr (int32), gf, S, dCF vector and length,
+//          gDiff, T vector, dfp = r_f - r_f' (Green-Gauss correction vector)
+//   boundary faces (B, linear patch-major index = reference i4-NIFaces):
+//          own, type (int32), S, |S|, n, dCF (BDistanceCF), gDiff, T, nz(i,i)
+//   matrix: ac (N), anb (W*N slot-major), bc (N)
+#pragma once
+#include "../../include/fsb200.h"
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include <cstdint>
+
+#define FS_BLOCK 256
+#define FS_RED_BLOCKS 1184           // 148 SMs x 8: partial-sum slots of the grid reductions
+
+// reduction slots in ctx->red (double); each quantity has FS_RED_BLOCKS partials
+enum { RED_SUM0 = 0, RED_SUM1, RED_SUM2, RED_MAX0, RED_MAX1, RED_NQ };
+
+struct fs_mg_dev;  // multigrid hierarchy (fs_mg.cu)
+
+struct fs_ctx {
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  fs_case cfg{};
+  int N = 0, F = 0, B = 0, W = 0, NS = 0;
+  int nIter = 0;
+  int64_t launches = 0;
+  std::string err;
+  int num_sms = 148;
+
+  // host copies (connectivity restated from Readit, 0-based)
+  std::vector<int32_t> h_ncf, h_cf, h_cn, h_own_slot, h_nbr_slot, h_fown, h_fnbr, h_bown, h_bset;
+  std::vector<int32_t> h_bset_start, h_bset_n, h_btype;
+  std::vector<int32_t> h_color_ptr, h_color_rows;  // multicolour ordering for GS
+  int ncolors = 0;
+
+  // connectivity (device)
+  int32_t *slot = nullptr, *cn = nullptr, *ncf = nullptr;
+  int32_t *fown = nullptr, *fnbr = nullptr, *bown = nullptr, *btype = nullptr;
+  int32_t *color_rows = nullptr;
+
+  // geometry (device)
+  double *vol = nullptr, *xc = nullptr;                     // xc: 3N
+  double *gf = nullptr, *sf = nullptr, *dcfv = nullptr, *dcf = nullptr, *gdiff = nullptr;  // sf,dcfv: 3F
+  double *tf = nullptr, *dfp = nullptr, *fa = nullptr;      // 3F, 3F, F
+  double *bsf = nullptr, *bfa = nullptr, *bnf = nullptr, *bdv = nullptr, *bgdiff = nullptr, *btf = nullptr, *bnzii = nullptr;
+
+  // state (device)
+  double *u = nullptr, *v = nullptr, *w = nullptr, *p = nullptr, *pc = nullptr, *mdot = nullptr;
+  double *bu = nullptr, *bv = nullptr, *bw = nullptr, *bp = nullptr, *bpc = nullptr, *bmdot = nullptr;
+  double *ug = nullptr, *vg = nullptr, *wg = nullptr, *pg = nullptr, *pcg = nullptr;      // 3N
+  double *bug = nullptr, *bvg = nullptr, *bwg = nullptr, *bpg = nullptr, *bpcg = nullptr; // 3B
+  double *gtmp = nullptr;                                  // 12N double buffer for GG passes
+  double *du1 = nullptr, *dv1 = nullptr, *dw1 = nullptr, *du2 = nullptr, *dv2 = nullptr, *dw2 = nullptr;
+  double *us = nullptr, *vs = nullptr, *ws = nullptr;
+
+  // assembly (device)
+  double *ac = nullptr, *anb = nullptr, *bc = nullptr, *dphi = nullptr;
+  double *ac_int = nullptr, *bc_int = nullptr, *effdiv = nullptr;  // bc_int: 3N
+  double *pcoef = nullptr;                                         // F: p' face coefficient
+  // krylov work (device)
+  double *kx = nullptr, *kr = nullptr, *kr0 = nullptr, *kp = nullptr, *kv = nullptr, *ks = nullptr, *kt = nullptr;
+  double *kz = nullptr, *ky = nullptr;   // preconditioned vectors (AMG-BiCGSTAB)
+  // reductions
+  double *red = nullptr;        // RED_NQ * FS_RED_BLOCKS partials
+  int64_t *redi = nullptr;      // FS_RED_BLOCKS argmax partials
+  double *resblk = nullptr;     // device residual block, layout of fs_residuals' first 20 doubles + extras
+  int32_t *d_iters = nullptr;   // linear iterations per NF (5)
+  int32_t *d_status = nullptr;  // device-side status flags
+
+  // multigrid
+  fs_mg_dev *mg = nullptr;
+
+  // timing
+  cudaEvent_t ev[6] = {};
+  float phase_ms[5] = {};
+  int coop_grid = 0;            // blocks of a cooperative solver launch
+};
+
+// residual block layout on the device (double resblk[RB_SIZE])
+enum { RB_ABS = 0, RB_MAX = 5, RB_RMS = 10, RB_SCL = 15, RB_OVERALL = 20, RB_IMAX = 21, RB_SIZE = 24 };
+
+#define FS_CK(call)                                                          \
+  do {                                                                       \
+    cudaError_t e__ = (call);                                                \
+    if (e__ != cudaSuccess) {                                                \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e__);        \
+      return FS_E_CUDA;                                                      \
+    }                                                                        \
+  } while (0)
+
+#define FS_LAUNCH_CHECK()                                                    \
+  do {                                                                       \
+    ctx->launches++;                                                         \
+    cudaError_t e__ = cudaGetLastError();                                    \
+    if (e__ != cudaSuccess) {                                                \
+      ctx->err = std::string("launch: ") + cudaGetErrorString(e__);         \
+      return FS_E_CUDA;                                                      \
+    }                                                                        \
+  } while (0)
+
+static inline int fs_grid(long n, int block = FS_BLOCK) {
+  long g = (n + block - 1) / block;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// entry points shared between translation units
+int fs_geometry_build(fs_ctx *ctx, const fs_mesh_in *mi);
+int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const *phi,
+                    const double *const *bphi, double *const *g, double *const *bg,
+                    const int *method, const int *niter);
+int fs_momentum_assemble(fs_ctx *ctx, int comp);
+int fs_continuity_assemble(fs_ctx *ctx);
+int fs_continuity_correct(fs_ctx *ctx);
+int fs_residual_reduce(fs_ctx *ctx, int nf);   // CalculateResiduals partials -> resblk slot
+int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int solver);
+int fs_mg_build(fs_ctx *ctx);
+int fs_mg_free(fs_ctx *ctx);
+int fs_mg_vcycle_solve(fs_ctx *ctx, int nf, double rrf, double *iters_out);

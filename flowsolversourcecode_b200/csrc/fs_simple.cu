@@ -1,0 +1,884 @@
+// fs_simple.cu -- the per-face / per-cell kernels of one SIMPLE outer iteration.
+//
+// Every kernel is cell-centric gather (one thread per cell, looping over the
+// cell's face slots in slot order) or face-centric (one thread per face).  A
+// cell's slots hold its faces in increasing face index, so a gather visits a
+// cell's faces in the same order as the reference's face loops scatter into
+// that cell (AssembleGolbalElementAndFaceFluxes.for:60-98): sums are formed
+// in the reference's order without atomics, and with --fmad=false the
+// assembled coefficients are bit-identical to the CPU restatement.
+#include "fs_internal.cuh"
+
+namespace {
+
+constexpr double M23 = (double)(-2.0f / 3.0f);   // `-2./3.` is REAL(4) (AssembleBulkViscosity.for:36)
+constexpr double EPS9 = (double)1.e-9f;          // `1.e-9` is REAL(4) (AssembleHRSchemeCorrection.for:92)
+constexpr double TINY = 1.0e-15;                 // Constants1.F90
+
+// ------------------------------------------------------------ reductions
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+// deterministic block sum / max (fixed tree for a fixed blockDim); result valid in thread 0
+__device__ double block_sum(double v, double *sh) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.;
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.;
+    r = warp_sum(r);
+  }
+  return r;
+}
+__device__ double block_max(double v, double *sh) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = -1.0e300;
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : -1.0e300;
+    r = warp_max(r);
+  }
+  return r;
+}
+
+// per-cell residual statistics of CalculateResiduals (CalculateResidualsRoutine.for:30-67)
+// at dphi=0: r=|bc|.  Writes block partials.
+__device__ void residual_partials(double r, double acphi, double *red, int nblk) {
+  __shared__ double sh[32];
+  double s0 = block_sum(r, sh);
+  double s1 = block_sum(r * r, sh);
+  double m0 = block_max(r, sh);
+  double m1 = block_max(acphi, sh);
+  if (threadIdx.x == 0) {
+    red[RED_SUM0 * nblk + blockIdx.x] = s0;
+    red[RED_SUM1 * nblk + blockIdx.x] = s1;
+    red[RED_MAX0 * nblk + blockIdx.x] = m0;
+    red[RED_MAX1 * nblk + blockIdx.x] = m1;
+  }
+}
+
+// single block: partials -> residual block slot q (ResorAbs/Max/RMS/Scaled)
+__global__ void k_residual_final(const double *red, int nblk, int N, int q, double *rb) {
+  __shared__ double sh[32];
+  double s0 = 0., s1 = 0., m0 = -1., m1 = -1.;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    s0 += red[RED_SUM0 * nblk + b];
+    s1 += red[RED_SUM1 * nblk + b];
+    m0 = fmax(m0, red[RED_MAX0 * nblk + b]);
+    m1 = fmax(m1, red[RED_MAX1 * nblk + b]);
+  }
+  s0 = block_sum(s0, sh); s1 = block_sum(s1, sh);
+  m0 = block_max(m0, sh); m1 = block_max(m1, sh);
+  if (threadIdx.x == 0) {
+    rb[RB_ABS + q] = s0;
+    rb[RB_MAX + q] = m0;
+    rb[RB_RMS + q] = sqrt(s1 / N);
+    rb[RB_SCL + q] = (q == 3) ? 0. : m0 / (m1 + TINY);
+  }
+}
+
+// ------------------------------------------------------------ gradients
+struct GradJob {
+  int nfld;
+  const double *phi[4];
+  const double *bphi[4];
+  double *out[4];      // 3N destination of this pass
+  const double *in[4]; // 3N gradient of the previous pass (correction passes)
+};
+
+// StandardGreenGauss / first pass of StandardGreenGaussFaceCorrection1
+// (StandardGreenGaussGradient.for:35-79; StandardGreenGaussCorrection1Gradient.for:47-96)
+__global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B,
+    const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot,
+    const int32_t *__restrict__ fown, const int32_t *__restrict__ fnbr,
+    const double *__restrict__ gf, const double *__restrict__ sf,
+    const double *__restrict__ bsf, const double *__restrict__ vol) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int nc = ncf[i];
+  double V = vol[i];
+  for (int q = 0; q < J.nfld; q++) {
+    const double *phi = J.phi[q], *bphi = J.bphi[q];
+    double gx = 0., gy = 0., gz = 0.;
+    for (int j = 0; j < nc; j++) {
+      int s = slot[(long)j * N + i];
+      int f = s >> 1;
+      if (f < F) {
+        int o = fown[f], n = fnbr[f];
+        double g = gf[f];
+        double fip = phi[o] * g + phi[n] * (1. - g);
+        double fx = fip * sf[f], fy = fip * sf[F + f], fz = fip * sf[2L * F + f];
+        if (s & 1) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
+        else { gx = gx + fx; gy = gy + fy; gz = gz + fz; }
+      } else {
+        int b = f - F;
+        double bp = bphi[b];
+        gx = gx + bp * bsf[b]; gy = gy + bp * bsf[B + b]; gz = gz + bp * bsf[2L * B + b];
+      }
+    }
+    double *o = J.out[q];
+    o[i] = gx / V; o[N + i] = gy / V; o[2L * N + i] = gz / V;
+  }
+}
+
+// correction pass of StandardGreenGaussFaceCorrection1 (:98-172)
+__global__ void __launch_bounds__(FS_BLOCK) k_gg_corr(GradJob J, int N, int F, int B,
+    const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot,
+    const int32_t *__restrict__ fown, const int32_t *__restrict__ fnbr,
+    const double *__restrict__ gf, const double *__restrict__ sf, const double *__restrict__ dfp,
+    const double *__restrict__ bsf, const double *__restrict__ vol) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int nc = ncf[i];
+  double V = vol[i];
+  for (int q = 0; q < J.nfld; q++) {
+    const double *phi = J.phi[q], *bphi = J.bphi[q], *gi = J.in[q];
+    double gx = 0., gy = 0., gz = 0.;
+    for (int j = 0; j < nc; j++) {
+      int s = slot[(long)j * N + i];
+      int f = s >> 1;
+      if (f < F) {
+        int o = fown[f], n = fnbr[f];
+        double g = gf[f];
+        double fip = phi[o] * g + phi[n] * (1. - g);
+        double cx = gi[o] * g + gi[n] * (1. - g); cx = cx * dfp[f];
+        double cy = gi[N + o] * g + gi[N + n] * (1. - g); cy = cy * dfp[F + f];
+        double cz = gi[2L * N + o] * g + gi[2L * N + n] * (1. - g); cz = cz * dfp[2L * F + f];
+        double phif = fip + cx + cy + cz;
+        double fx = phif * sf[f], fy = phif * sf[F + f], fz = phif * sf[2L * F + f];
+        if (s & 1) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
+        else { gx = gx + fx; gy = gy + fy; gz = gz + fz; }
+      } else {
+        int b = f - F;
+        double bp = bphi[b];
+        gx = gx + bp * bsf[b]; gy = gy + bp * bsf[B + b]; gz = gz + bp * bsf[2L * B + b];
+      }
+    }
+    double *o = J.out[q];
+    o[i] = gx / V; o[N + i] = gy / V; o[2L * N + i] = gz / V;
+  }
+}
+
+// boundary gradients: owner value, then the CorrectGradients.for projections
+struct BGradJob { int nfld; int var[4]; const double *g[4]; double *bg[4]; };
+__global__ void k_bgrad(BGradJob J, int N, int B, const int32_t *__restrict__ bown,
+                        const int32_t *__restrict__ btype, const double *__restrict__ bnf,
+                        const double *__restrict__ bnzii) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  int k = bown[b], t = btype[b];
+  double nx = bnf[b], ny = bnf[B + b], nz = bnf[2L * B + b], nzi = bnzii[b];
+  for (int q = 0; q < J.nfld; q++) {
+    const double *g = J.g[q];
+    double gx = g[k], gy = g[N + k], gz = g[2L * N + k];
+    double ox = gx, oy = gy, oz = gz;
+    int var = J.var[q];
+    bool vel = (var == FS_VAR_U || var == FS_VAR_V || var == FS_VAR_W);
+    if ((vel && t == FS_BC_OUTLET_FD) || (var == FS_VAR_P && t == FS_BC_SYMMETRY)) {
+      // CorrectGradientAtOulet / CorrectPressureGradientAtSymmetryBoundary, nz=BFaceAreanz(i,i)
+      ox = gx * (1. - nx * nx) - gy * nx * ny - gz * nx * nzi;
+      oy = gy * (1. - ny * ny) - gx * ny * nx - gz * ny * nzi;
+      oz = gz * (1. - nzi * nzi) - gx * nzi * nx - gy * nzi * ny;
+    } else if (var == FS_VAR_P && (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP)) {
+      // CorrectPresureGradientAtWalls (CorrectGradients.for:34-56)
+      ox = (1 - nx * nx) * gx - nx * ny * gy - nx * nz * gz;
+      oy = (1 - ny * ny) * gy - ny * nx * gx - ny * nz * gz;
+      oz = (1 - nz * nz) * gz - nz * nx * gx - nz * ny * gy;
+    }
+    double *bg = J.bg[q];
+    bg[b] = ox; bg[B + b] = oy; bg[2L * B + b] = oz;
+  }
+}
+
+// ------------------------------------------------------------ interpolation helpers
+// InterpolateGradientToFace (InterpolateGradientFromElementToFace.for:3-100),
+// owner-perspective: o = owner gradient, n = neighbour gradient.
+__device__ __forceinline__ void face_grad(int scheme, double g, double md, double phio, double phin,
+                                          double d, double ex, double ey, double ez,
+                                          double ox, double oy, double oz, double nx, double ny, double nz,
+                                          double &fx, double &fy, double &fz) {
+  double gg = g;
+  if (scheme == FS_GI_UPWIND) gg = (md > 0.) ? 1. : 0.;
+  else if (scheme == FS_GI_DOWNWIND) gg = (md > 0.) ? 0. : 1.;
+  fx = gg * ox + (1. - gg) * nx;
+  fy = gg * oy + (1. - gg) * ny;
+  fz = gg * oz + (1. - gg) * nz;
+  if (scheme == FS_GI_AVERAGECORRECTED) {
+    double c = (phin - phio) / d;
+    c = c - (fx * ex + fy * ey + fz * ez);
+    fx = fx + c * ex; fy = fy + c * ey; fz = fz + c * ez;
+  }
+}
+
+// TVDLimiter (Convection/LimitersTVDType.for:4)
+__device__ __forceinline__ double tvd_psi(int s, double rf) {
+  switch (s) {
+  case FS_TVD_UPWIND: return 0.;
+  case FS_TVD_DOWNWIND: return 2.;
+  case FS_TVD_FROMM: return 0.5 * (1. + rf);
+  case FS_TVD_SOU: return rf;
+  case FS_TVD_CD: return 1.;
+  case FS_TVD_QUICK: return (3. + rf) / 4.;
+  case FS_TVD_SUPERBEE: return fmax(fmax(0., fmin(1., 2. * rf)), fmin(2., rf));
+  case FS_TVD_MINMOD: return fmax(0., fmin(1., rf));
+  case FS_TVD_OSHER: return fmax(0., fmin(2., rf));
+  case FS_TVD_VANLEER: return (rf + fabs(rf)) / (1. + fabs(rf));
+  case FS_TVD_MUSCL: return fmax(0., fmin(fmin(2. * rf, 0.5 * (1. + rf)), 2.));
+  case FS_TVD_SMART: return fmax(0., fmin(fmin(2. * rf, 0.75 * rf + 0.25), 4.));
+  case FS_TVD_HQUICK: return 2. * (rf + fabs(rf)) / (rf + 3.);
+  case FS_TVD_UMIST: return fmax(0., fmin(fmin(fmin(2. * rf, 0.25 + 0.75 * rf), 0.75 + 0.25 * rf), 2.));
+  case FS_TVD_CHARM: return (rf <= 0.) ? 0. : rf * (3. * rf + 1.) / ((rf + 1.) * (rf + 1.));
+  }
+  return 0.;
+}
+
+// HRSchemesCorrections (AssembleHRSchemeCorrection.for:36-134), TVD framework, cpf=1
+__device__ __forceinline__ double hr_flux(int scheme, double bleed, double md, double phio, double phin,
+                                          const double go[3], const double gn[3], double dx, double dy, double dz) {
+  double phic, phid, gx, gy, gz;
+  if (md > 0.) { phic = phio; phid = phin; gx = go[0]; gy = go[1]; gz = go[2]; }
+  else { phic = phin; phid = phio; gx = gn[0]; gy = gn[1]; gz = gn[2]; dx = -dx; dy = -dy; dz = -dz; }
+  double phiu = phid - 2. * (gx * dx + gy * dy + gz * dz);
+  double diff = phid - phic, rf;
+  if (fabs(diff) < EPS9) rf = 0.; else rf = (phic - phiu) / diff;
+  double psi = tvd_psi(scheme, rf);
+  double phiHR = phic + 0.5 * psi * diff;
+  phiHR = (1. - bleed) * phiHR + bleed * phic;
+  return md * (phiHR - phic) * 1.;
+}
+
+// ------------------------------------------------------------ momentum
+struct MomArgs {
+  int N, F, B;
+  const int32_t *ncf, *slot, *fown, *fnbr, *bown, *btype;
+  const double *gf, *sf, *dcfv, *dcf, *gdiff, *tf, *vol;
+  const double *bsf, *bfa, *bnf, *bdv, *bgdiff, *btf;
+  const double *u, *v, *w, *mdot, *bmdot, *bu, *bv, *bw;
+  const double *ug, *vg, *wg, *pg, *bug, *bvg, *bwg;
+  double mu, bleed, urf;
+  int gi_scheme, hr_on, conv_scheme, inviscid, relax, simplec;
+  // outputs
+  double *ac_int, *anb, *bc_int, *effdiv;
+  double *ac, *bc, *d1, *d2, *star;
+  double *red; int nblk;
+};
+
+// Interior-face part of SolveMomentumX/Y/Z for all three components at once:
+// diffusion (AssembleIsotropicDiffusion.for:99-117), transpose diffusion
+// (AssembleExplicitDiffusion.for:22-44), bulk viscosity (AssembleBulkViscosity.for:22-44),
+// upwind convection + HR deferred correction (AssembleConvection.for:72-88,153-162)
+// and the effective divergence (CalculateEffectiveDivergence.for:20-45).
+// FluxCf/FluxFf (and so ac, anb) are shared by u, v, w; bc differs.
+__global__ void __launch_bounds__(FS_BLOCK) k_mom_interior(MomArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  const int N = a.N, F = a.F;
+  const long N2 = 2L * N, F2 = 2L * F;
+  int nc = a.ncf[i];
+  const double mu = a.mu;
+  double ac = 0., bcu = 0., bcv = 0., bcw = 0., ed = 0.;
+  for (int j = 0; j < nc; j++) {
+    int s = a.slot[(long)j * N + i];
+    int f = s >> 1;
+    if (f >= F) { ed = ed + a.bmdot[f - F]; continue; }
+    int o = a.fown[f], n = a.fnbr[f];
+    double g = a.gf[f], md = a.mdot[f];
+    double sx = a.sf[f], sy = a.sf[F + f], sz = a.sf[F2 + f];
+    double uo = a.u[o], un = a.u[n], vo = a.v[o], vn = a.v[n], wo = a.w[o], wn = a.w[n];
+    double guo[3] = {a.ug[o], a.ug[N + o], a.ug[N2 + o]}, gun[3] = {a.ug[n], a.ug[N + n], a.ug[N2 + n]};
+    double gvo[3] = {a.vg[o], a.vg[N + o], a.vg[N2 + o]}, gvn[3] = {a.vg[n], a.vg[N + n], a.vg[N2 + n]};
+    double gwo[3] = {a.wg[o], a.wg[N + o], a.wg[N2 + o]}, gwn[3] = {a.wg[n], a.wg[N + n], a.wg[N2 + n]};
+    double dx = a.dcfv[f], dy = a.dcfv[F + f], dz = a.dcfv[F2 + f], d = a.dcf[f];
+    double ex = dx / d, ey = dy / d, ez = dz / d;
+    double fcf = 0., fff = 0., tu = 0., tv = 0., tw = 0.;
+    if (!a.inviscid) {
+      double gamf = g * mu + (1. - g) * mu;
+      double gd = a.gdiff[f];
+      double tx = a.tf[f], ty = a.tf[F + f], tz = a.tf[F2 + f];
+      double fu[3], fv[3], fw[3];
+      face_grad(a.gi_scheme, g, md, uo, un, d, ex, ey, ez, guo[0], guo[1], guo[2], gun[0], gun[1], gun[2], fu[0], fu[1], fu[2]);
+      face_grad(a.gi_scheme, g, md, vo, vn, d, ex, ey, ez, gvo[0], gvo[1], gvo[2], gvn[0], gvn[1], gvn[2], fv[0], fv[1], fv[2]);
+      face_grad(a.gi_scheme, g, md, wo, wn, d, ex, ey, ez, gwo[0], gwo[1], gwo[2], gwn[0], gwn[1], gwn[2], fw[0], fw[1], fw[2]);
+      double fcl = gamf * gd, ffl = -gamf * gd;
+      fcf = fcl; fff = ffl;
+      tu = fcl * uo + ffl * un + -(gamf * (fu[0] * tx + fu[1] * ty + fu[2] * tz));
+      tv = fcl * vo + ffl * vn + -(gamf * (fv[0] * tx + fv[1] * ty + fv[2] * tz));
+      tw = fcl * wo + ffl * wn + -(gamf * (fw[0] * tx + fw[1] * ty + fw[2] * tz));
+      // transpose term
+      tu = tu + -(gamf * (fu[0] * sx + fv[0] * sy + fw[0] * sz));
+      tv = tv + -(gamf * (fu[1] * sx + fv[1] * sy + fw[1] * sz));
+      tw = tw + -(gamf * (fu[2] * sx + fv[2] * sy + fw[2] * sz));
+      // bulk viscosity
+      double div = fu[0] + fv[1] + fw[2];
+      tu = tu + -(M23 * gamf * div * sx);
+      tv = tv + -(M23 * gamf * div * sy);
+      tw = tw + -(M23 * gamf * div * sz);
+    }
+    double cc = fmax(md, 0.), cn = -fmax(-md, 0.);
+    fcf = fcf + cc; fff = fff + cn;
+    tu = tu + (cc * uo + cn * un);
+    tv = tv + (cc * vo + cn * vn);
+    tw = tw + (cc * wo + cn * wn);
+    if (a.hr_on) {
+      tu = tu + hr_flux(a.conv_scheme, a.bleed, md, uo, un, guo, gun, dx, dy, dz);
+      tv = tv + hr_flux(a.conv_scheme, a.bleed, md, vo, vn, gvo, gvn, dx, dy, dz);
+      tw = tw + hr_flux(a.conv_scheme, a.bleed, md, wo, wn, gwo, gwn, dx, dy, dz);
+    }
+    if (s & 1) {   // this cell is the neighbour
+      ac = ac - fff;
+      a.anb[(long)j * N + i] = 0. - fcf;
+      bcu = bcu + tu; bcv = bcv + tv; bcw = bcw + tw;
+      ed = ed - md;
+    } else {
+      ac = ac + fcf;
+      a.anb[(long)j * N + i] = 0. + fff;
+      bcu = bcu - tu; bcv = bcv - tv; bcw = bcw - tw;
+      ed = ed + md;
+    }
+  }
+  a.ac_int[i] = ac;
+  a.bc_int[i] = bcu; a.bc_int[N + i] = bcv; a.bc_int[N2 + i] = bcw;
+  a.effdiv[i] = ed;
+}
+
+// Boundary faces, element terms, under-relaxation and D of one component:
+// AssembleIsotropicDiffusion.for:123-627 (walls/symmetry/inlet), explicit and bulk
+// boundary terms, AssembleConvection.for:165-178 + 263-556, AssemblePressureGradient.for,
+// AssembleGolbalElementAndFaceFluxes.for:83-98 + 4-30, UnderRelaxation.for:21,
+// StoreTheDValues.for:20-48, and the residual partials of CalculateResiduals.
+__global__ void __launch_bounds__(FS_BLOCK) k_mom_finish(MomArgs a, int comp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = i < a.N;
+  double r = 0., acphi = -1.;
+  if (live) {
+    const int N = a.N, F = a.F, B = a.B;
+    const long N2 = 2L * N, B2 = 2L * B;
+    const double mu = a.mu;
+    const double *fi = comp == 0 ? a.u : comp == 1 ? a.v : a.w;
+    const double *bfi = comp == 0 ? a.bu : comp == 1 ? a.bv : a.bw;
+    const double *bfg = comp == 0 ? a.bug : comp == 1 ? a.bvg : a.bwg;
+    double phi = fi[i];
+    double ac = a.ac_int[i], bc = a.bc_int[(long)comp * N + i];
+    int nc = a.ncf[i];
+    for (int j = 0; j < nc; j++) {
+      int f = a.slot[(long)j * N + i] >> 1;
+      if (f < F) continue;
+      int b = f - F, t = a.btype[b];
+      double fcf = 0., tf = 0.;
+      double bsx = a.bsf[b], bsy = a.bsf[B + b], bsz = a.bsf[B2 + b];
+      double bp = bfi[b];
+      if (!a.inviscid) {
+        double gamf = mu;
+        if (t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
+          double nx = a.bnf[b], ny = a.bnf[B + b], nz = a.bnf[B2 + b];
+          double dN = a.bdv[b] * nx + a.bdv[B + b] * ny + a.bdv[B2 + b] * nz;
+          double area = a.bfa[b], fcl, fvl;
+          if (t == FS_BC_WALL_NOSLIP) {
+            if (comp == 0) {
+              fcl = gamf * area * (1. - nx * nx) / dN;
+              fvl = -((gamf * area / dN) * (bp * (1. - nx * nx) + (a.v[i] - a.bv[b]) * nx * ny + (a.w[i] - a.bw[b]) * nx * nz));
+            } else if (comp == 1) {
+              fcl = gamf * area * (1. - ny * ny) / dN;
+              fvl = -((gamf * area / dN) * ((a.u[i] - a.bu[b]) * nx * ny + bp * (1. - ny * ny) + (a.w[i] - a.bw[b]) * nz * ny));
+            } else {
+              fcl = gamf * area * (1. - nz * nz) / dN;
+              fvl = -((gamf * area / dN) * ((a.u[i] - a.bu[b]) * nx * nz + (a.v[i] - a.bv[b]) * ny * nz + bp * (1. - nz * nz)));
+            }
+          } else {
+            if (comp == 0) { fcl = 2. * gamf * area * (nx * nx) / dN; fvl = -((-2. * gamf * area / dN) * (a.v[i] * ny + a.w[i] * nz) * nx); }
+            else if (comp == 1) { fcl = 2. * gamf * area * (ny * ny) / dN; fvl = -((-2. * gamf * area / dN) * (a.u[i] * nx + a.w[i] * nz) * ny); }
+            else { fcl = 2. * gamf * area * (nz * nz) / dN; fvl = -((-2. * gamf * area / dN) * (a.u[i] * nx + a.v[i] * ny) * nz); }
+          }
+          fcf = fcl;
+          tf = fcl * phi + 0. * bp + fvl;
+        } else if (t == FS_BC_INLET_VEL) {
+          double fcl = gamf * a.bgdiff[b], ffl = -gamf * a.bgdiff[b];
+          double fvl = -(gamf * (bfg[b] * a.btf[b] + bfg[B + b] * a.btf[B + b] + bfg[B2 + b] * a.btf[B2 + b]));
+          fcf = fcl;
+          tf = fcl * phi + ffl * bp + fvl;
+        }
+        // transpose (explicit) diffusion, all boundary faces
+        double gxc = a.bug[(long)comp * B + b], gyc = a.bvg[(long)comp * B + b], gzc = a.bwg[(long)comp * B + b];
+        tf = tf + -(gamf * (gxc * bsx + gyc * bsy + gzc * bsz));
+        // bulk viscosity, all boundary faces
+        double div = a.bug[b] + a.bvg[B + b] + a.bwg[B2 + b];
+        double sc = comp == 0 ? bsx : comp == 1 ? bsy : bsz;
+        tf = tf + -(M23 * gamf * div * sc);
+      }
+      if (t == FS_BC_INLET_VEL) {
+        double bm = a.bmdot[b];
+        double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
+        fcf = fcf + fcl;
+        tf = tf + (fcl * phi + ffl * bp);
+      } else if (t == FS_BC_OUTLET_FD) {
+        double bm = a.bmdot[b];
+        double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
+        double fvl = bm * (bfg[b] * a.bdv[b] + bfg[B + b] * a.bdv[B + b] + bfg[B2 + b] * a.bdv[B2 + b]);
+        fcf = fcf + fcl;
+        tf = tf + (fcl * phi + ffl * bp + fvl);
+      }
+      ac = ac + fcf;
+      bc = bc - tf;
+    }
+    // element terms: effective divergence (AssembleConvection.for:165-178) and pressure gradient
+    double e = a.effdiv[i];
+    double fce = fmax(e, 0.0) - e;
+    double fve = -(fmax(e, 0.0) * phi);
+    double fte = fce * phi + fve;
+    fte = fte + a.pg[(long)comp * N + i] * a.vol[i];
+    ac = ac + fce;
+    bc = bc - fte;
+    if (a.relax) ac = ac / a.urf;
+    double V = a.vol[i];
+    double d1 = V / ac, d2 = d1;
+    if (a.simplec) {
+      double sa = ac;
+      for (int j = 0; j < nc; j++) sa = sa + a.anb[(long)j * N + i];
+      d2 = V / sa;
+    }
+    a.ac[i] = ac; a.bc[i] = bc; a.d1[i] = d1; a.d2[i] = d2; a.star[i] = phi;
+    r = fabs(bc);
+    acphi = fabs(ac * phi);
+  }
+  residual_partials(r, acphi, a.red, a.nblk);
+}
+
+// ------------------------------------------------------------ continuity
+struct ContArgs {
+  int N, F, B, msd, relax, gi_scheme;
+  double rho, urf;
+  const int32_t *ncf, *slot, *fown, *fnbr, *bown, *btype;
+  const double *gf, *sf, *dcfv, *dcf;
+  const double *u, *v, *w, *p, *us, *vs, *ws, *pg;
+  const double *du1, *dv1, *dw1, *du2, *dv2, *dw2;
+  double *mdot, *pcoef, *bmdot;
+  const double *bu, *bv, *bw, *bsf;
+  double *ac, *anb, *bc;
+  double *red; int nblk;
+};
+
+__device__ __forceinline__ double geo_diff(int msd, double du, double dv, double dw, double sx, double sy, double sz,
+                                           double ex, double ey, double ez, double cf,
+                                           double &tx, double &ty, double &tz) {
+  double DuSf = du * sx, DvSf = dv * sy, DwSf = dw * sz, DuEf, DvEf, DwEf;
+  if (msd == 1) {
+    double dp = ex * DuSf + ey * DvSf + ez * DwSf;
+    DuEf = dp * ex; DvEf = dp * ey; DwEf = dp * ez;
+  } else if (msd == 2) {
+    double mag = sqrt(DuSf * DuSf + DvSf * DvSf + DwSf * DwSf);
+    DuEf = ex * mag; DvEf = ey * mag; DwEf = ez * mag;
+  } else {
+    double mag = sqrt(DuSf * DuSf + DvSf * DvSf + DwSf * DwSf);
+    double eu = DuSf / mag, ev = DvSf / mag, ew = DwSf / mag;
+    double dp = ex * eu + ey * ev + ez * ew;
+    DuEf = mag * ex / dp; DvEf = mag * ey / dp; DwEf = mag * ez / dp;
+  }
+  tx = DuSf - DuEf; ty = DvSf - DvEf; tz = DwSf - DwEf;
+  return sqrt(DuEf * DuEf + DvEf * DvEf + DwEf * DwEf) / cf;
+}
+
+// Rhie-Chow mdot (AssembleMdotUsingRhieChow.for:554-759) and the p' face
+// coefficient rho*geoDiff(D2) (AssemblePressureCorrectionFluxes.for:85-153)
+__global__ void __launch_bounds__(FS_BLOCK) k_mdot(ContArgs a) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.F) return;
+  const int N = a.N, F = a.F;
+  const long N2 = 2L * N, F2 = 2L * F;
+  int i = a.fown[k], j = a.fnbr[k];
+  double g = a.gf[k], g1 = 1. - g;
+  double rhof = a.rho;
+  double sx = a.sf[k], sy = a.sf[F + k], sz = a.sf[F2 + k];
+  double dx = a.dcfv[k], dy = a.dcfv[F + k], dz = a.dcfv[F2 + k], cf = a.dcf[k];
+  double ex = dx / cf, ey = dy / cf, ez = dz / cf;
+  double du = g * a.du1[i] + g1 * a.du1[j];
+  double dv = g * a.dv1[i] + g1 * a.dv1[j];
+  double dw = g * a.dw1[i] + g1 * a.dw1[j];
+  double ub = g * a.u[i] + g1 * a.u[j], vb = g * a.v[i] + g1 * a.v[j], wb = g * a.w[i] + g1 * a.w[j];
+  double fvl = rhof * (ub * sx + vb * sy + wb * sz);
+  double tx, ty, tz;
+  double gd = geo_diff(a.msd, du, dv, dw, sx, sy, sz, ex, ey, ez, cf, tx, ty, tz);
+  double fcl = rhof * gd, ffl = -rhof * gd;
+  double pi = a.p[i], pj = a.p[j];
+  double gox = a.pg[i], goy = a.pg[N + i], goz = a.pg[N2 + i];
+  double gnx = a.pg[j], gny = a.pg[N + j], gnz = a.pg[N2 + j];
+  double pfx, pfy, pfz;   // PressGradf (GradientInterpolationSchemeContinuity)
+  face_grad(a.gi_scheme, g, a.mdot[k], pi, pj, cf, ex, ey, ez, gox, goy, goz, gnx, gny, gnz, pfx, pfy, pfz);
+  double pbx = g * gox + g1 * gnx, pby = g * goy + g1 * gny, pbz = g * goz + g1 * gnz;  // PressGradBar ('average')
+  fvl = fvl - rhof * (pfx * tx + pfy * ty + pfz * tz);
+  fvl = fvl + rhof * (pbx * (du * sx) + pby * (dv * sy) + pbz * (dw * sz));
+  double mold = a.mdot[k];
+  if (a.relax) {
+    double ms = rhof * ((g * a.us[i] + g1 * a.us[j]) * sx + (g * a.vs[i] + g1 * a.vs[j]) * sy + (g * a.ws[i] + g1 * a.ws[j]) * sz);
+    fvl = fvl + (1. - a.urf) * (mold - ms);
+  }
+  a.mdot[k] = fcl * pi + ffl * pj + fvl;
+  // p' coefficient with D2 (SIMPLEC) -- identical to D1 for SIMPLE
+  double du2 = g * a.du2[i] + g1 * a.du2[j];
+  double dv2 = g * a.dv2[i] + g1 * a.dv2[j];
+  double dw2 = g * a.dw2[i] + g1 * a.dw2[j];
+  double t2x, t2y, t2z;
+  a.pcoef[k] = rhof * geo_diff(a.msd, du2, dv2, dw2, sx, sy, sz, ex, ey, ez, cf, t2x, t2y, t2z);
+}
+
+// specified-velocity inlets: Bmdot = rho*Ub.S (AssembleMdotUsingRhieChow.for:2054-2075)
+__global__ void k_bmdot_inlet(ContArgs a) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.B) return;
+  if (a.btype[b] != FS_BC_INLET_VEL) return;
+  const int B = a.B;
+  a.bmdot[b] = a.rho * (a.bu[b] * a.bsf[b] + a.bv[b] * a.bsf[B + b] + a.bw[b] * a.bsf[2L * B + b]);
+}
+
+// p' system (AssemblePressureCorrectionFluxes.for + global assembly): ac = sum coef,
+// anb = -coef, bc = -(net outflow)
+__global__ void __launch_bounds__(FS_BLOCK) k_pc_assemble(ContArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double r = 0.;
+  if (i < a.N) {
+    const int N = a.N, F = a.F;
+    int nc = a.ncf[i];
+    double ac = 0., bc = 0.;
+    for (int j = 0; j < nc; j++) {
+      int s = a.slot[(long)j * N + i];
+      int f = s >> 1;
+      if (f < F) {
+        double c = a.pcoef[f], fff = -c, md = a.mdot[f];
+        if (s & 1) { ac = ac - fff; a.anb[(long)j * N + i] = 0. - c; bc = bc + md; }
+        else { ac = ac + c; a.anb[(long)j * N + i] = 0. + fff; bc = bc - md; }
+      } else {
+        ac = ac + 0.;
+        bc = bc - a.bmdot[f - F];
+      }
+    }
+    ac = ac + 0.; bc = bc - 0.;
+    a.ac[i] = ac; a.bc[i] = bc;
+    r = fabs(bc);
+  }
+  residual_partials(r, 0., a.red, a.nblk);
+}
+
+// ------------------------------------------------------------ corrections
+struct CorrArgs {
+  int N, F, B, ref_cell, set_ref;
+  double urfp;
+  const int32_t *ncf, *slot, *fown, *fnbr, *bown, *btype;
+  const double *bdv, *bnf, *pcoef, *du2, *dv2, *dw2, *pcg, *bpg;
+  double *u, *v, *w, *p, *pc, *mdot, *bp, *bpc, *bu, *bv, *bw, *bmdot;
+  double *red; int64_t *redi; int nblk; double *rb;
+};
+
+// UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for)
+__global__ void k_bpc(CorrArgs a) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < a.B) a.bpc[b] = a.pc[a.bown[b]];
+}
+// CorrectPressure (CorrectPressure.for:21-42)
+__global__ void k_corr_p(CorrArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  double rpc = (a.ref_cell >= 0) ? a.pc[a.ref_cell] : 0.;
+  if (a.set_ref) rpc = 0.;
+  a.p[i] = a.p[i] + a.urfp * (a.pc[i] - rpc);
+}
+// CorrectVelocity (CorrectMdotandVelocity.for:773-779)
+__global__ void k_corr_u(CorrArgs a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.N) return;
+  const int N = a.N;
+  a.u[i] = a.u[i] - a.du2[i] * a.pcg[i];
+  a.v[i] = a.v[i] - a.dv2[i] * a.pcg[N + i];
+  a.w[i] = a.w[i] - a.dw2[i] * a.pcg[2L * N + i];
+}
+// Correctmdot (CorrectMdotandVelocity.for:55-63)
+__global__ void k_corr_mdot(CorrArgs a) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.F) return;
+  double c = a.pcoef[k];
+  a.mdot[k] = a.mdot[k] + c * a.pc[a.fown[k]] + (-c) * a.pc[a.fnbr[k]];
+}
+// UpdateBoundaryPressure (CorrectPressure.for:49-190), UpdateSymmetry
+// (SymmetryAndAxisBoundary.for:4-33), UpdateSlipWallBoundary (SlipWallBoundary.for:4)
+__global__ void k_bcorr(CorrArgs a) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.B) return;
+  const int B = a.B;
+  const long B2 = 2L * B;
+  int t = a.btype[b], i1 = a.bown[b];
+  if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
+    a.bp[b] = a.p[i1] + a.bpg[b] * a.bdv[b] + a.bpg[B + b] * a.bdv[B + b] + a.bpg[B2 + b] * a.bdv[B2 + b];
+  } else {
+    double rpc = (a.ref_cell >= 0) ? a.pc[a.ref_cell] : 0.;
+    if (a.set_ref) rpc = 0.;
+    a.bp[b] = a.bp[b] + a.urfp * (a.bpc[b] - rpc);
+  }
+  if (t == FS_BC_SYMMETRY || t == FS_BC_WALL_SLIP) {
+    double nx = a.bnf[b], ny = a.bnf[B + b], nz = a.bnf[B2 + b];
+    double q = a.u[i1] * nx + a.v[i1] * ny + a.w[i1] * nz;
+    a.bu[b] = a.u[i1] - q * nx; a.bv[b] = a.v[i1] - q * ny; a.bw[b] = a.w[i1] - q * nz;
+  }
+}
+
+// mass imbalance per cell (CalculateContinuityResiduals.for:130-183): partial sums,
+// max |m| and the largest index attaining it (iMaxImbalance)
+__global__ void __launch_bounds__(FS_BLOCK) k_mass_imbalance(CorrArgs a) {
+  __shared__ double sh[32];
+  __shared__ int64_t shi[FS_BLOCK];
+  __shared__ double shm[FS_BLOCK];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double m = 0.;
+  if (i < a.N) {
+    const int N = a.N, F = a.F;
+    int nc = a.ncf[i];
+    for (int j = 0; j < nc; j++) {
+      int s = a.slot[(long)j * N + i];
+      int f = s >> 1;
+      if (f < F) m = (s & 1) ? m - a.mdot[f] : m + a.mdot[f];
+      else m = m + a.bmdot[f - F];
+    }
+  }
+  double s0 = block_sum(m, sh);
+  double s1 = block_sum(fabs(m), sh);
+  double s2 = block_sum(m * m, sh);
+  double am = (i < a.N) ? fabs(m) : -1.;
+  shm[threadIdx.x] = am; shi[threadIdx.x] = (i < a.N) ? i : -1;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      double x = shm[threadIdx.x], y = shm[threadIdx.x + o];
+      int64_t ix = shi[threadIdx.x], iy = shi[threadIdx.x + o];
+      if (y > x || (y == x && iy > ix)) { shm[threadIdx.x] = y; shi[threadIdx.x] = iy; }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    a.red[RED_SUM0 * a.nblk + blockIdx.x] = s0;
+    a.red[RED_SUM1 * a.nblk + blockIdx.x] = s1;
+    a.red[RED_SUM2 * a.nblk + blockIdx.x] = s2;
+    a.red[RED_MAX0 * a.nblk + blockIdx.x] = shm[0];
+    a.redi[blockIdx.x] = shi[0];
+  }
+}
+
+__global__ void k_mass_final(CorrArgs a, double mdot_in) {
+  __shared__ double sh[32];
+  __shared__ int64_t shi[1024];
+  __shared__ double shm[1024];
+  double s0 = 0., s1 = 0., s2 = 0., mx = -1.; int64_t im = -1;
+  for (int b = threadIdx.x; b < a.nblk; b += blockDim.x) {
+    s0 += a.red[RED_SUM0 * a.nblk + b];
+    s1 += a.red[RED_SUM1 * a.nblk + b];
+    s2 += a.red[RED_SUM2 * a.nblk + b];
+    double y = a.red[RED_MAX0 * a.nblk + b]; int64_t iy = a.redi[b];
+    if (y > mx || (y == mx && iy > im)) { mx = y; im = iy; }
+  }
+  s0 = block_sum(s0, sh); s1 = block_sum(s1, sh); s2 = block_sum(s2, sh);
+  shm[threadIdx.x] = mx; shi[threadIdx.x] = im;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      double x = shm[threadIdx.x], y = shm[threadIdx.x + o];
+      int64_t ix = shi[threadIdx.x], iy = shi[threadIdx.x + o];
+      if (y > x || (y == x && iy > ix)) { shm[threadIdx.x] = y; shi[threadIdx.x] = iy; }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double mxv = shm[0] < 0. ? 0. : shm[0];
+    a.rb[RB_ABS + 4] = s1;
+    a.rb[RB_MAX + 4] = mxv;
+    a.rb[RB_RMS + 4] = sqrt(s2 / a.N);
+    a.rb[RB_SCL + 4] = (mdot_in == 0.) ? 0. : mxv / fabs(mdot_in);
+    a.rb[RB_OVERALL] = s0;
+    a.rb[RB_IMAX] = (double)shi[0];
+  }
+}
+
+__global__ void k_sum_inlet(int B, const int32_t *btype, const double *bmdot, double *out) {
+  // serial on purpose: a handful of inlet faces, deterministic order
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.;
+    for (int b = 0; b < B; b++) if (btype[b] == FS_BC_INLET_VEL) s += bmdot[b];
+    *out = s;
+  }
+}
+
+}  // namespace
+
+// ======================================================================
+// host drivers
+// ======================================================================
+int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const *phi,
+                    const double *const *bphi, double *const *g, double *const *bg,
+                    const int *method, const int *niter) {
+  const int N = ctx->N, F = ctx->F, B = ctx->B;
+  int passes[4], maxp = 0;
+  for (int q = 0; q < nfld; q++) {
+    passes[q] = 1 + (method[q] == 2 ? niter[q] : 0);
+    if (method[q] != 1 && method[q] != 2) { ctx->err = "only MethodCalcGradient 1 and 2 are implemented"; return FS_E_UNSUPPORTED; }
+    maxp = passes[q] > maxp ? passes[q] : maxp;
+  }
+  // pass p of field q writes g if (passes-1-p) is even, else the scratch buffer
+  for (int pidx = 0; pidx < maxp; pidx++) {
+    GradJob J{};
+    int n = 0;
+    for (int q = 0; q < nfld; q++) {
+      if (pidx >= passes[q]) continue;
+      double *tmp = ctx->gtmp + 3L * N * q;
+      bool to_final = ((passes[q] - 1 - pidx) % 2) == 0;
+      J.phi[n] = phi[q]; J.bphi[n] = bphi[q];
+      J.out[n] = to_final ? g[q] : tmp;
+      J.in[n] = to_final ? tmp : g[q];
+      n++;
+    }
+    J.nfld = n;
+    if (pidx == 0)
+      k_gg0<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->fown, ctx->fnbr, ctx->gf, ctx->sf, ctx->bsf, ctx->vol);
+    else
+      k_gg_corr<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->fown, ctx->fnbr, ctx->gf, ctx->sf, ctx->dfp, ctx->bsf, ctx->vol);
+    FS_LAUNCH_CHECK();
+  }
+  if (B) {
+    BGradJob BJ{};
+    BJ.nfld = nfld;
+    for (int q = 0; q < nfld; q++) { BJ.var[q] = vars[q]; BJ.g[q] = g[q]; BJ.bg[q] = bg[q]; }
+    k_bgrad<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(BJ, N, B, ctx->bown, ctx->btype, ctx->bnf, ctx->bnzii);
+    FS_LAUNCH_CHECK();
+  }
+  return FS_OK;
+}
+
+static MomArgs mom_args(fs_ctx *ctx) {
+  MomArgs a{};
+  const fs_case &c = ctx->cfg;
+  a.N = ctx->N; a.F = ctx->F; a.B = ctx->B;
+  a.ncf = ctx->ncf; a.slot = ctx->slot; a.fown = ctx->fown; a.fnbr = ctx->fnbr; a.bown = ctx->bown; a.btype = ctx->btype;
+  a.gf = ctx->gf; a.sf = ctx->sf; a.dcfv = ctx->dcfv; a.dcf = ctx->dcf; a.gdiff = ctx->gdiff; a.tf = ctx->tf; a.vol = ctx->vol;
+  a.bsf = ctx->bsf; a.bfa = ctx->bfa; a.bnf = ctx->bnf; a.bdv = ctx->bdv; a.bgdiff = ctx->bgdiff; a.btf = ctx->btf;
+  a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.mdot = ctx->mdot; a.bmdot = ctx->bmdot; a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw;
+  a.ug = ctx->ug; a.vg = ctx->vg; a.wg = ctx->wg; a.pg = ctx->pg; a.bug = ctx->bug; a.bvg = ctx->bvg; a.bwg = ctx->bwg;
+  a.mu = c.mu; a.bleed = c.bleed; a.urf = c.urf_momentum;
+  a.gi_scheme = c.grad_interp_mom;
+  a.hr_on = (c.hr_framework == FS_HR_TVD && ctx->nIter >= c.niter_start_hr && c.conv_scheme != FS_TVD_UPWIND) ? 1 : 0;
+  a.conv_scheme = c.conv_scheme; a.inviscid = c.inviscid; a.relax = c.relax_momentum; a.simplec = c.algorithm == FS_SIMPLEC;
+  a.ac_int = ctx->ac_int; a.anb = ctx->anb; a.bc_int = ctx->bc_int; a.effdiv = ctx->effdiv;
+  a.ac = ctx->ac; a.bc = ctx->bc; a.red = ctx->red; a.nblk = fs_grid(ctx->N);
+  return a;
+}
+
+// SolveMomentumX/Y/Z up to (not including) SolveEquation
+int fs_momentum_assemble(fs_ctx *ctx, int comp) {
+  const fs_case &c = ctx->cfg;
+  const int N = ctx->N;
+  if (comp == 0) {
+    int vars[4] = {FS_VAR_U, FS_VAR_V, FS_VAR_W, FS_VAR_P};
+    const double *phi[4] = {ctx->u, ctx->v, ctx->w, ctx->p};
+    const double *bphi[4] = {ctx->bu, ctx->bv, ctx->bw, ctx->bp};
+    double *g[4] = {ctx->ug, ctx->vg, ctx->wg, ctx->pg};
+    double *bg[4] = {ctx->bug, ctx->bvg, ctx->bwg, ctx->bpg};
+    int meth[4] = {c.method_grad_mom, c.method_grad_mom, c.method_grad_mom, c.method_grad_cont};
+    int nit[4] = {c.niter_grad_mom, c.niter_grad_mom, c.niter_grad_mom, c.niter_grad_cont};
+    int rc = fs_gradient_dev(ctx, 4, vars, phi, bphi, g, bg, meth, nit);
+    if (rc) return rc;
+    MomArgs a = mom_args(ctx);
+    k_mom_interior<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
+    FS_LAUNCH_CHECK();
+  }
+  MomArgs a = mom_args(ctx);
+  a.d1 = comp == 0 ? ctx->du1 : comp == 1 ? ctx->dv1 : ctx->dw1;
+  a.d2 = comp == 0 ? ctx->du2 : comp == 1 ? ctx->dv2 : ctx->dw2;
+  a.star = comp == 0 ? ctx->us : comp == 1 ? ctx->vs : ctx->ws;
+  k_mom_finish<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a, comp);
+  FS_LAUNCH_CHECK();
+  k_residual_final<<<1, 1024, 0, ctx->st>>>(ctx->red, a.nblk, N, comp, ctx->resblk);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+static ContArgs cont_args(fs_ctx *ctx) {
+  ContArgs a{};
+  const fs_case &c = ctx->cfg;
+  a.N = ctx->N; a.F = ctx->F; a.B = ctx->B; a.msd = c.method_decompose_s; a.relax = c.relax_momentum;
+  a.gi_scheme = c.grad_interp_cont; a.rho = c.rho; a.urf = c.urf_momentum;
+  a.ncf = ctx->ncf; a.slot = ctx->slot; a.fown = ctx->fown; a.fnbr = ctx->fnbr; a.bown = ctx->bown; a.btype = ctx->btype;
+  a.gf = ctx->gf; a.sf = ctx->sf; a.dcfv = ctx->dcfv; a.dcf = ctx->dcf;
+  a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.p = ctx->p; a.us = ctx->us; a.vs = ctx->vs; a.ws = ctx->ws; a.pg = ctx->pg;
+  a.du1 = ctx->du1; a.dv1 = ctx->dv1; a.dw1 = ctx->dw1; a.du2 = ctx->du2; a.dv2 = ctx->dv2; a.dw2 = ctx->dw2;
+  a.mdot = ctx->mdot; a.pcoef = ctx->pcoef; a.bmdot = ctx->bmdot;
+  a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bsf = ctx->bsf;
+  a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc; a.red = ctx->red; a.nblk = fs_grid(ctx->N);
+  return a;
+}
+
+// SolveContinuity up to (not including) SolveEquation
+int fs_continuity_assemble(fs_ctx *ctx) {
+  const int N = ctx->N, F = ctx->F, B = ctx->B;
+  FS_CK(cudaMemsetAsync(ctx->pc, 0, sizeof(double) * N, ctx->st));   // InitializePressureCorrection
+  ContArgs a = cont_args(ctx);
+  if (F) { k_mdot<<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  if (B) { k_bmdot_inlet<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  k_pc_assemble<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
+  FS_LAUNCH_CHECK();
+  k_residual_final<<<1, 1024, 0, ctx->st>>>(ctx->red, a.nblk, N, 3, ctx->resblk);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+static CorrArgs corr_args(fs_ctx *ctx) {
+  CorrArgs a{};
+  const fs_case &c = ctx->cfg;
+  a.N = ctx->N; a.F = ctx->F; a.B = ctx->B; a.ref_cell = c.ref_pressure_cell; a.set_ref = c.set_reference_pressure;
+  a.urfp = c.urf_pressure;
+  a.ncf = ctx->ncf; a.slot = ctx->slot; a.fown = ctx->fown; a.fnbr = ctx->fnbr; a.bown = ctx->bown; a.btype = ctx->btype;
+  a.bdv = ctx->bdv; a.bnf = ctx->bnf; a.pcoef = ctx->pcoef; a.du2 = ctx->du2; a.dv2 = ctx->dv2; a.dw2 = ctx->dw2;
+  a.pcg = ctx->pcg; a.bpg = ctx->bpg;
+  a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.p = ctx->p; a.pc = ctx->pc; a.mdot = ctx->mdot; a.bp = ctx->bp; a.bpc = ctx->bpc;
+  a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bmdot = ctx->bmdot;
+  a.red = ctx->red; a.redi = ctx->redi; a.nblk = fs_grid(ctx->N); a.rb = ctx->resblk;
+  return a;
+}
+
+// SolveContinuity after SolveEquation: corrections, residuals, symmetry update
+int fs_continuity_correct(fs_ctx *ctx) {
+  const int N = ctx->N, F = ctx->F, B = ctx->B;
+  const fs_case &c = ctx->cfg;
+  CorrArgs a = corr_args(ctx);
+  if (B) { k_bpc<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  k_corr_p<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
+  FS_LAUNCH_CHECK();
+  int var = FS_VAR_PC, meth = c.method_grad_cont, nit = c.niter_grad_cont;
+  const double *phi = ctx->pc, *bphi = ctx->bpc;
+  double *g = ctx->pcg, *bg = ctx->bpcg;
+  int rc = fs_gradient_dev(ctx, 1, &var, &phi, &bphi, &g, &bg, &meth, &nit);
+  if (rc) return rc;
+  k_corr_u<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
+  FS_LAUNCH_CHECK();
+  if (F) { k_corr_mdot<<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  if (B) { k_bcorr<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  k_mass_imbalance<<<a.nblk, FS_BLOCK, 0, ctx->st>>>(a);
+  FS_LAUNCH_CHECK();
+  double mdot_in = 0.;
+  bool has_inlet = false;
+  for (int s = 0; s < ctx->NS; s++) if (c.patch_type[s] == FS_BC_INLET_VEL) has_inlet = true;
+  if (has_inlet) {
+    // inlet mass flow is needed on the host only through ResorScaled(5)
+    double *d = ctx->resblk + RB_SIZE - 1;
+    k_sum_inlet<<<1, 32, 0, ctx->st>>>(B, ctx->btype, ctx->bmdot, d);
+    FS_LAUNCH_CHECK();
+    FS_CK(cudaMemcpyAsync(&mdot_in, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    FS_CK(cudaStreamSynchronize(ctx->st));
+  }
+  k_mass_final<<<1, 1024, 0, ctx->st>>>(a, mdot_in);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}

@@ -1,0 +1,248 @@
+// fs_solvers.cu -- SolveEquation (AlgebraicSolvers/SolveAlegbraicEquations.for:4-180)
+// on the GPU.
+//
+// Each solve is ONE persistent cooperative kernel (one or more CTAs per SM,
+// grid-wide barriers between dependent steps), so an entire BiCGSTAB or
+// Gauss-Seidel solve including its convergence test runs without a host
+// round trip.  Dot products and norms are FP64 and deterministic: every CTA
+// writes a partial, and after the barrier every CTA sums the same partials
+// in the same fixed order, so all CTAs hold the same value.
+//
+// Matrix: ac (N), anb (W*N slot-major), neighbour table cn (W*N), i.e. the
+// reference's Variables2 layout.  The product row i: ac_i x_i + sum_j anb_ij
+// x_cn(i,j) in slot order is the CSR row order of matrixSolverOMP.f90:517-583.
+#include "fs_internal.cuh"
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+struct SolveArgs {
+  int N, W;
+  const int32_t *ncf, *cn;
+  const double *ac, *anb, *bc;
+  double *x, *r, *r0, *p, *v, *s, *t, *dphi;
+  double *part;        // 8 * grid partial slots
+  const double *ires;  // IResiduals (ResorAbs of the system at dphi=0)
+  double rrf, tol;
+  int itmax;
+  const int32_t *color_rows;
+  const int32_t *color_ptr;  // device copy (ncolors+1)
+  int ncolors;
+  int32_t *iters;
+  double *diag;        // [0]=final residual norm, [1]=normb
+};
+
+__device__ __forceinline__ double row_ax(const SolveArgs &a, int i, const double *x) {
+  double t = 0.0;
+  t = t + a.ac[i] * x[i];
+  int nc = a.ncf[i];
+  for (int j = 0; j < nc; j++) {
+    int k = a.cn[(long)j * a.N + i];
+    if (k >= 0) t = t + a.anb[(long)j * a.N + i] * x[k];
+  }
+  return t;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block sum of per-thread values, broadcast to every thread of the block
+__device__ double block_sum_all(double v) {
+  __shared__ double sh[33];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.;
+    r = warp_sum(r);
+    if (lane == 0) sh[32] = r;
+  }
+  __syncthreads();
+  double r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+// grid-deterministic reduction of up to 2 values: write partials at slot `buf`,
+// barrier, then every CTA sums all partials in the same order
+__device__ void grid_sum2(cg::grid_group &grid, double *part, int buf, double a0, double a1,
+                          double &o0, double &o1) {
+  int G = gridDim.x;
+  double b0 = block_sum_all(a0), b1 = block_sum_all(a1);
+  if (threadIdx.x == 0) { part[(2 * buf) * G + blockIdx.x] = b0; part[(2 * buf + 1) * G + blockIdx.x] = b1; }
+  grid.sync();
+  double s0 = 0., s1 = 0.;
+  for (int q = threadIdx.x; q < G; q += blockDim.x) { s0 += part[(2 * buf) * G + q]; s1 += part[(2 * buf + 1) * G + q]; }
+  o0 = block_sum_all(s0);
+  o1 = block_sum_all(s1);
+}
+
+// BICGSTAB_OMP (matrixSolverOMP.f90:306-386): unpreconditioned, x kept between
+// calls (the reference's module vector x), stop when sqrt|r.r0| <= tol*|b|
+// or after maxit-1 iterations.
+__global__ void __launch_bounds__(FS_BLOCK) k_bicgstab(SolveArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  const int N = a.N;
+  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+  double l0 = 0., l1 = 0.;
+  for (long i = tid0; i < N; i += nth) {
+    double r0 = a.bc[i] - row_ax(a, (int)i, a.x);
+    a.r0[i] = r0; a.r[i] = r0; a.p[i] = r0;
+    l0 += r0 * r0;
+    l1 += a.bc[i] * a.bc[i];
+  }
+  double rhoPrev, bb;
+  grid_sum2(grid, a.part, 0, l0, l1, rhoPrev, bb);
+  double resnorm = sqrt(fabs(rhoPrev)), normb = sqrt(bb);
+  int k = 1;
+  int buf = 1;
+  while (k < a.itmax && resnorm > a.tol * normb) {
+    k = k + 1;
+    // v = A p ; dp0 = v.r0
+    l0 = 0.;
+    for (long i = tid0; i < N; i += nth) { double vi = row_ax(a, (int)i, a.p); a.v[i] = vi; l0 += vi * a.r0[i]; }
+    double dp0, dum;
+    grid_sum2(grid, a.part, buf, l0, 0., dp0, dum); buf ^= 3;
+    double alpha = rhoPrev / dp0;
+    for (long i = tid0; i < N; i += nth) a.s[i] = a.r[i] - alpha * a.v[i];
+    grid.sync();
+    // As = A s ; dp1 = As.s ; dp2 = As.As
+    l0 = 0.; l1 = 0.;
+    for (long i = tid0; i < N; i += nth) { double ti = row_ax(a, (int)i, a.s); a.t[i] = ti; l0 += ti * a.s[i]; l1 += ti * ti; }
+    double dp1, dp2;
+    grid_sum2(grid, a.part, buf, l0, l1, dp1, dp2); buf ^= 3;
+    double omega = dp1 / dp2;
+    l0 = 0.;
+    for (long i = tid0; i < N; i += nth) {
+      a.x[i] = a.x[i] + alpha * a.p[i] + omega * a.s[i];
+      double ri = a.s[i] - omega * a.t[i];
+      a.r[i] = ri;
+      l0 += ri * a.r0[i];
+    }
+    double rho;
+    grid_sum2(grid, a.part, buf, l0, 0., rho, dum); buf ^= 3;
+    double beta = (rho / rhoPrev) * (alpha / omega);
+    rhoPrev = rho;
+    for (long i = tid0; i < N; i += nth) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+    resnorm = sqrt(fabs(rho));
+    grid.sync();
+  }
+  for (long i = tid0; i < N; i += nth) a.dphi[i] = a.x[i];
+  if (tid0 == 0) { *a.iters = k - 1; a.diag[0] = resnorm; a.diag[1] = normb; }
+}
+
+// SolveEquationsUsingSOR sweeps (SORMethod.for:20-60) in multicolour order:
+// forward over colours 0..C-1, backward C-1..0, each colour an independent
+// set, then CheckConvergence (CheckConvergenceRoutine.for:3) -- until
+// sum|r| <= rrF * IResiduals or itmax sweeps (SolveAlegbraicEquations.for:108-117).
+__global__ void __launch_bounds__(FS_BLOCK) k_sor(SolveArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  const int N = a.N;
+  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+  double ires = *a.ires, fres = ires;
+  int iter = 0, buf = 0;
+  while (fres > a.rrf * ires && iter < a.itmax) {
+    for (int pass = 0; pass < 2; pass++) {
+      for (int cc = 0; cc < a.ncolors; cc++) {
+        int c = pass == 0 ? cc : a.ncolors - 1 - cc;
+        int r0 = a.color_ptr[c], r1 = a.color_ptr[c + 1];
+        for (long q = r0 + tid0; q < r1; q += nth) {
+          int i = a.color_rows[q];
+          double l = a.bc[i];
+          int nc = a.ncf[i];
+          for (int j = 0; j < nc; j++) {
+            int k = a.cn[(long)j * N + i];
+            if (k >= 0) l = l - a.anb[(long)j * N + i] * a.dphi[k];
+          }
+          a.dphi[i] = l / a.ac[i];
+        }
+        grid.sync();
+      }
+    }
+    double l0 = 0., dum;
+    for (long i = tid0; i < N; i += nth) {
+      double r = a.bc[i] - a.ac[i] * a.dphi[i];
+      int nc = a.ncf[i];
+      for (int j = 0; j < nc; j++) {
+        int k = a.cn[(long)j * N + i];
+        if (k >= 0) r = r - a.anb[(long)j * N + i] * a.dphi[k];
+      }
+      l0 += fabs(r);
+    }
+    grid_sum2(grid, a.part, buf, l0, 0., fres, dum); buf ^= 1;
+    iter++;
+  }
+  if (tid0 == 0) { *a.iters = iter; a.diag[0] = fres; a.diag[1] = ires; }
+}
+
+__global__ void k_axpy_field(int N, double *fi, const double *dphi) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) fi[i] = fi[i] + dphi[i];
+}
+
+}  // namespace
+
+static int coop_launch(fs_ctx *ctx, void *fn, SolveArgs &a) {
+  if (ctx->coop_grid <= 0) {
+    // one grid size for every cooperative solver kernel: the smallest co-resident count
+    int per_sm = 0, per_sm2 = 0;
+    FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void *)k_bicgstab, FS_BLOCK, 0));
+    FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (void *)k_sor, FS_BLOCK, 0));
+    if (per_sm2 < per_sm) per_sm = per_sm2;
+    if (per_sm < 1) { ctx->err = "cooperative kernel does not fit on an SM"; return FS_E_CUDA; }
+    ctx->coop_grid = ctx->num_sms * (per_sm > 4 ? 4 : per_sm);
+  }
+  int G = ctx->coop_grid;
+  long need = (ctx->N + FS_BLOCK - 1) / FS_BLOCK;
+  if (need < G) G = (int)(need < 1 ? 1 : need);
+  void *args[] = {&a};
+  FS_CK(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+static SolveArgs solve_args(fs_ctx *ctx, int nf, double rrf, int itmax) {
+  SolveArgs a{};
+  a.N = ctx->N; a.W = ctx->W; a.ncf = ctx->ncf; a.cn = ctx->cn;
+  a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc;
+  a.x = ctx->kx; a.r = ctx->kr; a.r0 = ctx->kr0; a.p = ctx->kp; a.v = ctx->kv; a.s = ctx->ks; a.t = ctx->kt;
+  a.dphi = ctx->dphi;
+  a.part = ctx->red;
+  a.ires = ctx->resblk + RB_ABS + (nf - 1);
+  a.rrf = rrf; a.itmax = itmax; a.tol = ctx->cfg.krylov_tol;
+  a.color_rows = ctx->color_rows;
+  a.ncolors = ctx->ncolors;
+  a.iters = ctx->d_iters + (nf - 1);
+  a.diag = ctx->resblk + 22;
+  return a;
+}
+
+int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int solver) {
+  const int N = ctx->N;
+  FS_CK(cudaMemsetAsync(ctx->dphi, 0, sizeof(double) * N, ctx->st));
+  SolveArgs a = solve_args(ctx, nf, rrf, itmax);
+  int rc = FS_OK;
+  if (solver == FS_SOLVER_SOR) {
+    a.color_ptr = ctx->color_rows + N;  // colour offsets live right after the row list
+    rc = coop_launch(ctx, (void *)k_sor, a);
+  } else if (solver == FS_SOLVER_BICGS) {
+    a.itmax = ctx->cfg.krylov_maxit;
+    rc = coop_launch(ctx, (void *)k_bicgstab, a);
+  } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS) {
+    double it = 0;
+    rc = fs_mg_vcycle_solve(ctx, nf, rrf, &it);
+  } else {
+    ctx->err = "unknown solver";
+    return FS_E_ARG;
+  }
+  if (rc) return rc;
+  k_axpy_field<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, fi, ctx->dphi);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}

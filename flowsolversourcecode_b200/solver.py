@@ -1,0 +1,195 @@
+"""Host mirror of the reference's SIMPLE-loop subroutines over the C ABI.
+
+Method names follow the Fortran subroutines they replace so a driver reads
+like MainProgram/MainProgram.for:257-348:
+
+    s = Solver(mesh, case)
+    for nIter in range(1, IterMax + 1):
+        s.SolveMomentumX(); s.SolveMomentumY(); s.SolveMomentumZ()
+        s.SolveContinuity()
+        source = s.PrintConvergenceHistory()
+        if source < case.max_residual: break
+
+Variables are the reference's ``character*10`` names ('velx', 'vely', 'velz',
+'pressc', 'press').  All state lives on the GPU; nothing here computes on
+the CPU, and every call raises :class:`FsError` on a non-zero status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .case import Case
+from .mesh import PolyMesh
+
+VARIABLE = {"velx": L.VAR_U, "vely": L.VAR_V, "velz": L.VAR_W, "pressc": L.VAR_PC, "press": L.VAR_P}
+
+
+class Solver:
+    def __init__(self, mesh: PolyMesh, case: Case, device: int = 0):
+        self.lib = L.load()
+        self.mesh = mesh
+        self.case = case
+        self._cfg = case.struct(mesh)
+        ms, self._keep = L.mesh_struct(mesh)
+        h = C.c_void_p()
+        rc = self.lib.fs_create(C.byref(ms), C.byref(self._cfg), device, C.byref(h))
+        L.check(rc, None, "fs_create")
+        self.ctx = h
+        n, f, b, w = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        self.lib.fs_sizes(self.ctx, C.byref(n), C.byref(f), C.byref(b), C.byref(w))
+        self.N, self.F, self.B, self.W = n.value, f.value, b.value, w.value
+        self.nIter = 0
+        self.residuals: dict | None = None
+
+    # ------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.fs_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc, what):
+        L.check(rc, self.ctx, what)
+
+    # ------------------------------------------------------------ drivers
+    def SolveMomentumX(self):
+        self._chk(self.lib.fs_solve_momentum(self.ctx, 0), "SolveMomentumX")
+
+    def SolveMomentumY(self):
+        self._chk(self.lib.fs_solve_momentum(self.ctx, 1), "SolveMomentumY")
+
+    def SolveMomentumZ(self):
+        self._chk(self.lib.fs_solve_momentum(self.ctx, 2), "SolveMomentumZ")
+
+    def SolveContinuity(self):
+        self._chk(self.lib.fs_solve_continuity(self.ctx), "SolveContinuity")
+
+    def assemble_momentum(self, comp: int):
+        self._chk(self.lib.fs_assemble_momentum(self.ctx, comp), "assemble_momentum")
+
+    def assemble_continuity(self):
+        self._chk(self.lib.fs_assemble_continuity(self.ctx), "assemble_continuity")
+
+    def correct_continuity(self):
+        self._chk(self.lib.fs_correct_continuity(self.ctx), "correct_continuity")
+
+    def set_iteration(self, n: int):
+        self.nIter = n
+        self._chk(self.lib.fs_set_iteration(self.ctx, n), "set_iteration")
+
+    def PrintConvergenceHistory(self) -> float:
+        """Residual block + stop metric `source` (PrintConvergenceToFileAndScreen.for:613-700)."""
+        r = L.FsResiduals()
+        self._chk(self.lib.fs_residuals_get(self.ctx, C.byref(r)), "residuals")
+        self.residuals = r.as_dict()
+        return r.source
+
+    def simple_iteration(self) -> dict:
+        """One outer iteration (MainProgram.for:257-325) as a single C call."""
+        r = L.FsResiduals()
+        self.nIter += 1
+        self._chk(self.lib.fs_simple_iteration(self.ctx, C.byref(r)), "fs_simple_iteration")
+        self.residuals = r.as_dict()
+        return self.residuals
+
+    def simple_iteration_host(self, state: dict) -> dict:
+        """One outer iteration on host-owned state arrays (copied in and out)."""
+        r = L.FsResiduals()
+        self.nIter += 1
+        a = [state[k] for k in ("u", "v", "w", "p", "mdot", "bu", "bv", "bw", "bp", "bmdot")]
+        self._chk(self.lib.fs_simple_iteration_host(self.ctx, *[L.dptr(x) for x in a], C.byref(r)),
+                  "fs_simple_iteration_host")
+        self.residuals = r.as_dict()
+        return self.residuals
+
+    def run(self, itermax: int, tol: float | None = None, callback=None) -> list[dict]:
+        """Outer loop with the reference's stop test (MainProgram.for:322-325)."""
+        tol = self.case.max_residual if tol is None else tol
+        hist = []
+        for _ in range(itermax):
+            r = self.simple_iteration()
+            hist.append(r)
+            if callback:
+                callback(self.nIter, r)
+            if r["source"] < tol:
+                break
+        return hist
+
+    # ------------------------------------------------------------ leaf routines
+    def Gradient(self, variable: str, method: int, n_iter: int):
+        self._chk(self.lib.fs_gradient(self.ctx, VARIABLE[variable], method, n_iter), "Gradient")
+
+    def gradient_host(self, variable: str, method: int, n_iter: int, phi: np.ndarray, bphi: np.ndarray):
+        phi = np.ascontiguousarray(phi, np.float64)
+        bphi = np.ascontiguousarray(bphi, np.float64)
+        g = np.zeros(3 * self.N)
+        bg = np.zeros(3 * self.B)
+        self._chk(self.lib.fs_gradient_host(self.ctx, VARIABLE[variable], method, n_iter, L.dptr(phi),
+                                            L.dptr(bphi), L.dptr(g), L.dptr(bg)), "fs_gradient_host")
+        return g, bg
+
+    def UnderRelaxEquation(self, urf: float):
+        self._chk(self.lib.fs_under_relax(self.ctx, urf), "UnderRelaxEquation")
+
+    def SolveEquation(self, variable: str, rrf: float, itmax: int, solver: str):
+        self._chk(self.lib.fs_solve_equation(self.ctx, VARIABLE[variable], rrf, itmax, L.SOLVER[solver]),
+                  "SolveEquation")
+
+    def solve_system(self, ac, anb, bc, rrf=0.1, itmax=100, solver="bicgs"):
+        ac = np.ascontiguousarray(ac, np.float64)
+        anb = np.ascontiguousarray(anb, np.float64)
+        bc = np.ascontiguousarray(bc, np.float64)
+        x = np.zeros(self.N)
+        it = C.c_int()
+        self._chk(self.lib.fs_solve_system_host(self.ctx, L.dptr(ac), L.dptr(anb), L.dptr(bc), L.dptr(x), rrf,
+                                                itmax, L.SOLVER[solver], C.byref(it)), "fs_solve_system_host")
+        return x, it.value
+
+    # ------------------------------------------------------------ state
+    def _size(self, name: str) -> int:
+        N, F, B, W = self.N, self.F, self.B, self.W
+        sizes = {"mdot": F, "gfactor": F, "gdiff": F, "sf": 3 * F, "ft": 3 * F, "anb": W * N,
+                 "bu": B, "bv": B, "bw": B, "bp": B, "bpc": B, "bmdot": B, "bsf": 3 * B, "xc": 3 * N}
+        if name.endswith("grad"):
+            return 3 * N
+        return sizes.get(name, N)
+
+    def get(self, name: str) -> np.ndarray:
+        a = np.zeros(self._size(name))
+        self._chk(self.lib.fs_get_field(self.ctx, L.FIELD_ID[name], L.dptr(a), a.shape[0]), f"get {name}")
+        return a
+
+    def set(self, name: str, arr) -> None:
+        a = np.ascontiguousarray(arr, np.float64)
+        self._chk(self.lib.fs_set_field(self.ctx, L.FIELD_ID[name], L.dptr(a), a.shape[0]), f"set {name}")
+
+    def state(self) -> dict:
+        return {k: self.get(k) for k in ("u", "v", "w", "p", "mdot", "bu", "bv", "bw", "bp", "bmdot")}
+
+    def connectivity(self) -> dict:
+        N, W, F = self.N, self.W, self.F
+        out = {"ncf": np.zeros(N, np.int32), "cf": np.zeros(N * W, np.int32), "cn": np.zeros(N * W, np.int32),
+               "own_slot": np.zeros(F, np.int32), "nbr_slot": np.zeros(F, np.int32)}
+        self._chk(self.lib.fs_get_connectivity(self.ctx, *[L.iptr(out[k]) for k in
+                                                           ("ncf", "cf", "cn", "own_slot", "nbr_slot")]),
+                  "connectivity")
+        return out
+
+    def phase_times(self) -> list[float]:
+        a = (C.c_float * 5)()
+        self.lib.fs_phase_times(self.ctx, a)
+        return list(a)
+
+    def launch_count(self) -> int:
+        return int(self.lib.fs_launch_count(self.ctx))
+
+    def sync(self):
+        self._chk(self.lib.fs_sync(self.ctx), "sync")

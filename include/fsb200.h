@@ -1,0 +1,264 @@
+/*
+ * fsb200.h -- C ABI of the B200 (sm_100a) SIMPLE inner loop.
+ *
+ * The entry points below replace the leaf and driver subroutines that the
+ * Fortran solver fadlmoukalled/FlowSolverSourceCode calls once per outer
+ * iteration (MainProgram/MainProgram.for:257-348).  Each declaration names
+ * the reference interface it stands in for.  All state lives on the GPU in
+ * an opaque context; Fortran (through ISO_C_BINDING) or
+ * C/C++/Python (ctypes) hold only the context pointer and plain host arrays.
+ *
+ * Conventions
+ *   - Indices are 0-based here (the reference is 1-based).  Face and cell
+ *     numbering is the polyMesh order: interior faces first, then boundary
+ *     faces patch by patch (ReadFoamMesh.f90:277-297).  The linear boundary
+ *     face index b = sum(NBFaces(s<set)) + j is the reference's
+ *     i4-NIFaces (AssembleGolbalElementAndFaceFluxes.for:83-92).
+ *   - Every call returns an int status: FS_OK (0) or a negative FS_E_* code.
+ *     Nothing traps; device waits are bounded and report FS_E_TIMEOUT.
+ *   - Character dummies of the reference (Variable, solver, schemes) become
+ *     the integer enums below.
+ *   - One context is single-caller and non-reentrant (one CUDA stream).
+ */
+#ifndef FSB200_H
+#define FSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------------- status */
+#define FS_OK             0
+#define FS_E_ARG         -1   /* bad argument / size */
+#define FS_E_CUDA        -2   /* CUDA runtime error */
+#define FS_E_NOMEM       -3   /* device allocation failed */
+#define FS_E_NAN         -4   /* NaN/Inf detected in a residual */
+#define FS_E_DIVERGED    -5   /* residual grew by > 1e6 */
+#define FS_E_TIMEOUT     -6   /* bounded device wait gave up */
+#define FS_E_MESH        -7   /* inconsistent mesh */
+#define FS_E_UNSUPPORTED -8   /* option not implemented */
+
+/* ------------------------------------------------------- variable ids (NF)
+ * GetNFfromVariable (AlgebraicSolvers/AssignNFvaluesToVariables.for:4):
+ * velx=1, vely=2, velz=3, pressc=4, continuity residual slot 5. */
+#define FS_VAR_U      1
+#define FS_VAR_V      2
+#define FS_VAR_W      3
+#define FS_VAR_PC     4
+#define FS_VAR_MASS   5
+#define FS_VAR_P      6   /* 'press' (pressure itself, gradient calls only) */
+
+/* ------------------------------------------------------ field ids (get/set) */
+enum fs_field {
+  FS_F_U = 0, FS_F_V, FS_F_W, FS_F_P, FS_F_PC,      /* cell fields (N) */
+  FS_F_MDOT,                                         /* interior faces (F) */
+  FS_F_BU, FS_F_BV, FS_F_BW, FS_F_BP, FS_F_BPC,      /* boundary faces (B) */
+  FS_F_BMDOT,
+  FS_F_AC, FS_F_BC, FS_F_ANB,                        /* last assembled system (N, N, W*N slot-major) */
+  FS_F_DU1, FS_F_DV1, FS_F_DW1, FS_F_DU2, FS_F_DV2, FS_F_DW2,
+  FS_F_UGRAD, FS_F_VGRAD, FS_F_WGRAD, FS_F_PGRAD, FS_F_PCGRAD, /* 3N each: x block, y block, z block */
+  FS_F_VOLUME, FS_F_XC,                              /* N, 3N geometry */
+  FS_F_GFACTOR, FS_F_SF, FS_F_GDIFF, FS_F_FT,        /* F, 3F, F, 3F */
+  FS_F_BSF,                                          /* 3B */
+  FS_F_DPHI,                                         /* N: last linear solution */
+  FS_F_COUNT
+};
+
+/* -------------------------------------------------------- boundary types
+ * BCType + wallTypeMomentum / inletTypeMomentum / outletTypeMomentum
+ * (SetBoundaryPatches/SetBoundaryConditionPatches.for:88-200). */
+enum fs_bc {
+  FS_BC_WALL_NOSLIP = 0,   /* 'wall','noslip' (velocity given per patch: lid) */
+  FS_BC_WALL_SLIP   = 1,   /* 'wall','slip' */
+  FS_BC_SYMMETRY    = 2,   /* 'symmetry' */
+  FS_BC_INLET_VEL   = 3,   /* 'inlet','specifiedvelocity' */
+  FS_BC_OUTLET_FD   = 4    /* 'outlet','fullydeveloped' */
+};
+
+/* ---------------------------------------------------------- scheme enums */
+enum fs_gradinterp { FS_GI_AVERAGE = 0, FS_GI_UPWIND, FS_GI_DOWNWIND, FS_GI_AVERAGECORRECTED };
+enum fs_hr { FS_HR_NONE = 0, FS_HR_TVD = 1 };
+/* TVDLimiter (Convection/LimitersTVDType.for:4) scheme names */
+enum fs_tvd {
+  FS_TVD_UPWIND = 0, FS_TVD_DOWNWIND, FS_TVD_FROMM, FS_TVD_SOU, FS_TVD_CD,
+  FS_TVD_QUICK, FS_TVD_SUPERBEE, FS_TVD_MINMOD, FS_TVD_OSHER, FS_TVD_VANLEER,
+  FS_TVD_MUSCL, FS_TVD_SMART, FS_TVD_HQUICK, FS_TVD_UMIST, FS_TVD_CHARM
+};
+/* ASSolver* (SolveAlegbraicEquations.for:105-175) plus the GPU-only forms */
+enum fs_solver {
+  FS_SOLVER_SOR = 0,       /* 'sor': symmetric Gauss-Seidel sweeps (GPU: multicolour order) */
+  FS_SOLVER_BICGS = 1,     /* 'bicgs': BICGSTAB_OMP restated (matrixSolverOMP.f90:306) */
+  FS_SOLVER_AMG = 2,       /* LMultigrid=.true., MGType='geometricelement' */
+  FS_SOLVER_AMG_BICGS = 3, /* FP64 BiCGSTAB right-preconditioned by one AMG V-cycle (no reference row) */
+  FS_SOLVER_AMG32_BICGS = 4/* same with an FP32 AMG hierarchy (iterative refinement, no reference row) */
+};
+enum fs_algorithm { FS_SIMPLE = 0, FS_SIMPLEC = 1 };
+
+#define FS_MAX_PATCHES 32
+
+/* Case description: the knobs of User0.F90 / DescribeProblem that the inner
+ * loop reads (ProblemDescriptionRoutine.for:201-524). */
+typedef struct fs_case {
+  double rho;                    /* Density (constant) */
+  double mu;                     /* Viscosity (constant, laminar) */
+  int    algorithm;              /* Algorithm: FS_SIMPLE / FS_SIMPLEC */
+  int    relax_momentum;         /* LRelaxMomentum */
+  double urf_momentum;           /* urfMomentum */
+  double urf_pressure;           /* urfPressure (always applied, CorrectPressure.for:42) */
+  int    method_grad_mom;        /* MethodCalcGradientMomentum (1 or 2) */
+  int    method_grad_cont;       /* MethodCalcGradientContinuity (1 or 2) */
+  int    niter_grad_mom;         /* nIterGradientMomentum */
+  int    niter_grad_cont;        /* nIterGradientContinuity */
+  int    grad_interp_mom;        /* GradientInterpolationSchemeMomentum */
+  int    grad_interp_cont;       /* GradientInterpolationSchemeContinuity */
+  int    method_decompose_s;     /* MethodDecomposeS (1,2,3); geometry + Rhie-Chow */
+  int    hr_framework;           /* HRFrameworkMomentum */
+  int    conv_scheme;            /* ConvectionSchemeMomentum (fs_tvd) */
+  int    niter_start_hr;         /* nIterStartApplyingHR */
+  double bleed;                  /* BleedMomentum */
+  int    solver_mom;             /* ASSolverMomentum / LMultigridMomentum */
+  int    solver_cont;            /* ASSolverContinuity / LMultigridContinuity */
+  double rrf_mom, rrf_cont;      /* rrFMomentum, rrFContinuity */
+  int    itmax_mom, itmax_cont;  /* ASIterMomentum, ASIterContinuity */
+  int    nstop_type;             /* NstopType 1..4 */
+  double max_residual;           /* maximumResidual */
+  int    ref_pressure_cell;      /* ReferencePressureLocation (0-based) */
+  int    set_reference_pressure; /* LSetReferencePressure (0/1) */
+  int    inviscid;               /* Linviscid */
+  /* multigrid (MultiGrid*, ProblemDescriptionRoutine.for:392-430) */
+  int    mg_cycle;               /* 0 V, 1 F, 2 W  (MultiGridCycleType) */
+  int    mg_pre, mg_post;        /* MultiGridpreSweep / MultiGridpostSweep */
+  int    mg_max_cycles;          /* MaxMultiGridCycles */
+  int    mg_min_parents;         /* minNumberofParents */
+  int    mg_max_levels;          /* maxNumberofCoarseLevels */
+  double mg_rrf;                 /* MultiGridrrf */
+  /* krylov (BICGSTAB_OMP(N,100,1.d-5)) */
+  int    krylov_maxit;
+  double krylov_tol;
+  /* patches, in polyMesh boundary order */
+  int    n_patches;
+  int    patch_type[FS_MAX_PATCHES];      /* fs_bc */
+  double patch_vel[FS_MAX_PATCHES][3];    /* wall / inlet velocity */
+} fs_case;
+
+/* Mesh in polyMesh form (0-based), the input Readit parses
+ * (GridAndGeometry/ReadFoamMesh.f90:31-297). */
+typedef struct fs_mesh_in {
+  int32_t        n_nodes;
+  const double  *points;      /* 3*n_nodes, xyz interleaved */
+  int32_t        n_faces;     /* all faces */
+  const int32_t *face_ptr;    /* n_faces+1 offsets into face_nodes */
+  const int32_t *face_nodes;
+  const int32_t *owner;       /* n_faces */
+  int32_t        n_internal;  /* faces [0,n_internal) have a neighbour */
+  const int32_t *neighbour;   /* n_internal */
+  int32_t        n_patches;
+  const int32_t *patch_start; /* n_patches, face index of first patch face */
+  const int32_t *patch_size;  /* n_patches */
+} fs_mesh_in;
+
+/* Residual block (Residuals1.F90), indexed by NF-1 for NF=1..5. */
+typedef struct fs_residuals {
+  double abs_[5], max_[5], rms[5], scaled[5];
+  double overall_imbalance;   /* OverallImbalance */
+  int    imax_imbalance;      /* iMaxImbalance (0-based) */
+  int    lin_iters[5];        /* linear iterations spent per NF this outer iteration */
+  double source;              /* stop metric of PrintConvergenceHistory */
+} fs_residuals;
+
+typedef struct fs_ctx fs_ctx;
+
+/* ---------------------------------------------------------- lifetime
+ * Replaces Grid + allocateStorage + SetBCPatches + CalculateInitialmdot
+ * (MainProgram.for:57-73,142).  Builds connectivity on the host (bit-exact
+ * with Readit), computes geometry on the GPU (ProcessGeometryRoutine.for:3),
+ * sets the initial state u=v=w=p=0 with patch velocities on the boundary,
+ * and the initial mdot (InitializaMdot.for:4). */
+int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **out);
+int fs_destroy(fs_ctx *ctx);
+int fs_sizes(const fs_ctx *ctx, int32_t *n_cells, int32_t *n_ifaces,
+             int32_t *n_bfaces, int32_t *max_faces);
+const char *fs_last_error(const fs_ctx *ctx);
+
+/* ------------------------------------------------------- driver routines */
+/* SolveMomentumX/Y/Z (Momentum/SolveXMomentumEquation.for:4,
+ * SolveYMomentumEquation.for:4, SolveZMomentumEquation.for:4). comp=0,1,2. */
+int fs_solve_momentum(fs_ctx *ctx, int comp);
+/* SolveContinuity (ContinuityEquation/SolveContinuityEquation.for:4). */
+int fs_solve_continuity(fs_ctx *ctx);
+/* One outer iteration of MainProgram.for:257-325 (momentum x,y,z,
+ * continuity, PrintConvergenceHistory's stop metric). */
+int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res);
+/* Same, but the state arrays live on the HOST: they are copied in, the
+ * iteration runs, and they are copied back (the Fortran-owned layout of a
+ * drop-in: u,v,w,p [N], mdot [F], bu,bv,bw,bp,bmdot [B]). */
+int fs_simple_iteration_host(fs_ctx *ctx, double *u, double *v, double *w,
+                             double *p, double *mdot, double *bu, double *bv,
+                             double *bw, double *bp, double *bmdot,
+                             fs_residuals *res);
+
+/* The two halves of each driver around its SolveEquation call, for callers
+ * that run their own solver (and for per-kernel parity checks):
+ * fs_assemble_momentum = SolveXMomentumEquation.for:177-292 (fluxes,
+ * gradients in X, assembly, UnderRelaxEquation, storeDvalues);
+ * fs_assemble_continuity = SolveContinuityEquation.for:37-74;
+ * fs_correct_continuity = SolveContinuityEquation.for:79-100. */
+int fs_assemble_momentum(fs_ctx *ctx, int comp);
+int fs_assemble_continuity(fs_ctx *ctx);
+int fs_correct_continuity(fs_ctx *ctx);
+/* MultiGrid2 nIter (gates nIterStartApplyingHR). */
+int fs_set_iteration(fs_ctx *ctx, int n_iter);
+
+/* ---------------------------------------------------------- leaf routines */
+/* Gradient (GradientFiles/CalculateGradients.for:3) of field var
+ * (FS_VAR_U/V/W/P/PC) into its gradient arrays, method 1 or 2. */
+int fs_gradient(fs_ctx *ctx, int var, int method, int n_iter);
+/* Gradient of host arrays phi [N] / bphi [B] -> grad [3N] / bgrad [3B]
+ * (x block, y block, z block).  var selects the boundary corrections. */
+int fs_gradient_host(fs_ctx *ctx, int var, int method, int n_iter,
+                     const double *phi, const double *bphi,
+                     double *grad, double *bgrad);
+/* UnderRelaxEquation (UnderRelaxVariables/UnderRelaxation.for:4) on the
+ * currently assembled system. */
+int fs_under_relax(fs_ctx *ctx, double urf);
+/* SolveEquation (AlgebraicSolvers/SolveAlegbraicEquations.for:4) on the
+ * currently assembled system for variable var; updates the field by dphi. */
+int fs_solve_equation(fs_ctx *ctx, int var, double rrf, int itmax, int solver);
+/* Solve a host-given system ac [N], anb [W*N slot-major], bc [N] for dphi [N]
+ * with the given solver (the matrix layout of Variables2.F90). */
+int fs_solve_system_host(fs_ctx *ctx, const double *ac, const double *anb,
+                         const double *bc, double *dphi, double rrf, int itmax,
+                         int solver, int *iters);
+/* CalculateResiduals (CalculateResidualsRoutine.for:3) of the assembled
+ * system at dphi=0 for field var; fills res slot var-1. */
+int fs_residuals_get(fs_ctx *ctx, fs_residuals *res);
+
+/* ----------------------------------------------------- state transfer */
+int fs_get_field(fs_ctx *ctx, int field, double *host, size_t n);
+int fs_set_field(fs_ctx *ctx, int field, const double *host, size_t n);
+/* Connectivity produced by the Readit restatement (0-based):
+ * n_cell_faces [N], cell_faces [W*N slot-major, -1 unused],
+ * cell_nbr [W*N, -1 boundary/unused], own_slot [F], nbr_slot [F]. */
+int fs_get_connectivity(fs_ctx *ctx, int32_t *n_cell_faces, int32_t *cell_faces,
+                        int32_t *cell_nbr, int32_t *own_slot, int32_t *nbr_slot);
+/* Multigrid hierarchy (geometric-element agglomeration): number of levels,
+ * level sizes, and the parent map of level l -> l+1 (0-based). */
+int fs_mg_levels(fs_ctx *ctx, int32_t *n_levels, int32_t *level_sizes, int max_levels);
+int fs_mg_parents(fs_ctx *ctx, int level, int32_t *parents, size_t n);
+
+/* Timing of the last outer iteration's phases in milliseconds (CUDA events):
+ * [0] momentum assembly, [1] momentum solves, [2] continuity assembly,
+ * [3] p' solve, [4] corrections+residuals. */
+int fs_phase_times(fs_ctx *ctx, float *ms5);
+/* Number of kernel launches issued by this context since creation. */
+int64_t fs_launch_count(const fs_ctx *ctx);
+/* Synchronise the context stream. */
+int fs_sync(fs_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FSB200_H */

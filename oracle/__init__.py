@@ -1,0 +1,148 @@
+"""ctypes access to the CPU restatement of the reference SIMPLE loop.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs.  The product never imports it.
+Parity is unpinned (see oracle.h): the reference is Fortran with no compiler
+in this image and ships no golden vectors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    r = subprocess.run(["make", "-s", "-C", HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = C.CDLL(LIB)
+        lib.om_create.restype = C.c_void_p
+        lib.om_create.argtypes = [C.c_void_p, C.c_void_p]
+        lib.om_destroy.argtypes = [C.c_void_p]
+        lib.om_array.restype = C.c_void_p
+        lib.om_array.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_long), C.POINTER(C.c_int)]
+        lib.om_sizes.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 4
+        for n in ("om_momentum", "om_assemble_momentum"):
+            getattr(lib, n).argtypes = [C.c_void_p, C.c_int]
+        for n in ("om_continuity", "om_assemble_continuity", "om_correct_continuity"):
+            getattr(lib, n).argtypes = [C.c_void_p]
+        lib.om_simple_iteration.restype = C.c_double
+        lib.om_simple_iteration.argtypes = [C.c_void_p]
+        lib.om_set_iter.argtypes = [C.c_void_p, C.c_int]
+        lib.om_residuals.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.om_lin_iters.argtypes = [C.c_void_p, C.c_int]
+        lib.om_gradient.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 4
+        lib.om_solve_equation.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_int]
+        lib.om_bicgstab.restype = C.c_int
+        lib.om_bicgstab.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        lib.om_calc_residuals.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        lib.om_mg_setup.restype = C.c_int
+        lib.om_mg_setup.argtypes = [C.c_void_p]
+        lib.om_mg_level_size.restype = C.c_int
+        lib.om_mg_level_size.argtypes = [C.c_void_p, C.c_int]
+        lib.om_mg_parents.restype = C.POINTER(C.c_int)
+        lib.om_mg_parents.argtypes = [C.c_void_p, C.c_int]
+        _lib = lib
+    return _lib
+
+
+class Oracle:
+    """The sequential FP64 restatement for one mesh + case."""
+
+    def __init__(self, mesh, case):
+        from flowsolversourcecode_b200 import _lib as L
+        self.lib = load()
+        self._cfg = case.struct(mesh)
+        ms, self._keep = L.mesh_struct(mesh)
+        self.h = self.lib.om_create(C.byref(ms), C.byref(self._cfg))
+        n, f, b, w = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self.lib.om_sizes(self.h, C.byref(n), C.byref(f), C.byref(b), C.byref(w))
+        self.N, self.F, self.B, self.W = n.value, f.value, b.value, w.value
+        self.nIter = 0
+
+    def arr(self, name: str) -> np.ndarray:
+        """Live numpy view of an internal array (writes go to the oracle)."""
+        ln, isint = C.c_long(), C.c_int()
+        p = self.lib.om_array(self.h, name.encode(), C.byref(ln), C.byref(isint))
+        if not p:
+            raise KeyError(name)
+        t = C.c_int32 if isint.value else C.c_double
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(t)), shape=(ln.value,))
+
+    def get(self, name):
+        return self.arr(name).copy()
+
+    def set(self, name, values):
+        self.arr(name)[:] = values
+
+    def simple_iteration(self) -> float:
+        self.nIter += 1
+        return self.lib.om_simple_iteration(self.h)
+
+    def momentum(self, comp: int):
+        self.lib.om_momentum(self.h, comp)
+
+    def assemble_momentum(self, comp: int):
+        self.lib.om_assemble_momentum(self.h, comp)
+
+    def continuity(self):
+        self.lib.om_continuity(self.h)
+
+    def assemble_continuity(self):
+        self.lib.om_assemble_continuity(self.h)
+
+    def correct_continuity(self):
+        self.lib.om_correct_continuity(self.h)
+
+    def set_iter(self, n: int):
+        self.nIter = n
+        self.lib.om_set_iter(self.h, n)
+
+    def residuals(self) -> dict:
+        a = (C.c_double * 20)()
+        self.lib.om_residuals(self.h, a)
+        a = list(a)
+        return {"abs": a[0:5], "max": a[5:10], "rms": a[10:15], "scaled": a[15:20]}
+
+    def lin_iters(self, nf: int) -> int:
+        return self.lib.om_lin_iters(self.h, nf)
+
+    def gradient(self, var: int, method: int, niter: int, phi, bphi):
+        phi = np.ascontiguousarray(phi, np.float64)
+        bphi = np.ascontiguousarray(bphi, np.float64)
+        g = np.zeros(3 * self.N)
+        bg = np.zeros(3 * self.B)
+        self.lib.om_gradient(self.h, var, method, niter, phi.ctypes.data, bphi.ctypes.data, g.ctypes.data,
+                             bg.ctypes.data)
+        return g, bg
+
+    def bicgstab(self, maxit=100, tol=1e-5) -> int:
+        return self.lib.om_bicgstab(self.h, maxit, tol)
+
+    def mg_setup(self) -> int:
+        return self.lib.om_mg_setup(self.h)
+
+    def mg_parents(self, level: int) -> np.ndarray:
+        n = self.lib.om_mg_level_size(self.h, level)
+        p = self.lib.om_mg_parents(self.h, level)
+        return np.ctypeslib.as_array(p, shape=(n,)).copy()
+
+    def close(self):
+        if self.h:
+            self.lib.om_destroy(self.h)
+            self.h = None
