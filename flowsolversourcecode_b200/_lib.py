@@ -110,6 +110,9 @@ PROTOTYPES = {
     "fs_mg_levels": (C.c_int, [_V, _I, _I, C.c_int]),
     "fs_mg_parents": (C.c_int, [_V, C.c_int, _I, C.c_size_t]),
     "fs_phase_times": (C.c_int, [_V, C.POINTER(C.c_float)]),
+    "fs_timer_start": (C.c_int, [_V]),
+    "fs_timer_stop": (C.c_int, [_V, C.POINTER(C.c_float)]),
+    "fs_solver_stats": (C.c_int, [_V, C.POINTER(C.c_float), _I, _I, C.c_int]),
     "fs_launch_count": (C.c_int64, [_V]),
     "fs_sync": (C.c_int, [_V]),
 }

@@ -164,6 +164,8 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(FS_E_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   for (auto &e : ctx->ev) cudaEventCreate(&e);
+  for (auto &e : ctx->tev) cudaEventCreate(&e);
+  for (auto &pr : ctx->sev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
   if (ctx->cfg.set_reference_pressure < 0) ctx->cfg.set_reference_pressure = 0;  // no pressure-specified patch types
   if ((rc = fs_geometry_build(ctx, mesh))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
   const size_t N = ctx->N, F = ctx->F, B = ctx->B, W = ctx->W;
@@ -219,6 +221,8 @@ int fs_destroy(fs_ctx *ctx) {
   fs_mg_free(ctx);
   free_all(ctx);
   for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
+  for (auto &e : ctx->tev) if (e) cudaEventDestroy(e);
+  for (auto &pr : ctx->sev) { if (pr[0]) cudaEventDestroy(pr[0]); if (pr[1]) cudaEventDestroy(pr[1]); }
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
   return FS_OK;
@@ -270,6 +274,7 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   FS_CK(cudaMemcpyAsync(rb, ctx->resblk, sizeof(rb), cudaMemcpyDeviceToHost, ctx->st));
   FS_CK(cudaMemcpyAsync(it, ctx->d_iters, sizeof(it), cudaMemcpyDeviceToHost, ctx->st));
   FS_CK(cudaStreamSynchronize(ctx->st));
+  fs_solver_stats_collect(ctx);
   fs_residuals r{};
   for (int q = 0; q < 5; q++) {
     r.abs_[q] = rb[RB_ABS + q]; r.max_[q] = rb[RB_MAX + q]; r.rms[q] = rb[RB_RMS + q]; r.scaled[q] = rb[RB_SCL + q];
@@ -464,6 +469,33 @@ int fs_phase_times(fs_ctx *ctx, float *ms5) {
 }
 
 int64_t fs_launch_count(const fs_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int fs_timer_start(fs_ctx *ctx) {
+  if (!ctx) return FS_E_ARG;
+  FS_CK(cudaEventRecord(ctx->tev[0], ctx->st));
+  return FS_OK;
+}
+
+int fs_timer_stop(fs_ctx *ctx, float *ms) {
+  if (!ctx || !ms) return FS_E_ARG;
+  FS_CK(cudaEventRecord(ctx->tev[1], ctx->st));
+  FS_CK(cudaEventSynchronize(ctx->tev[1]));
+  FS_CK(cudaEventElapsedTime(ms, ctx->tev[0], ctx->tev[1]));
+  return FS_OK;
+}
+
+int fs_solver_stats(fs_ctx *ctx, float *ms5, int32_t *iters5, int32_t *calls5, int reset) {
+  if (!ctx) return FS_E_ARG;
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  fs_solver_stats_collect(ctx);
+  for (int q = 0; q < 5; q++) {
+    if (ms5) ms5[q] = ctx->s_ms[q];
+    if (iters5) iters5[q] = ctx->s_its[q];
+    if (calls5) calls5[q] = ctx->s_calls[q];
+    if (reset) { ctx->s_ms[q] = 0.f; ctx->s_its[q] = 0; ctx->s_calls[q] = 0; }
+  }
+  return FS_OK;
+}
 
 int fs_sync(fs_ctx *ctx) {
   if (!ctx) return FS_E_ARG;

@@ -81,6 +81,11 @@ struct fs_ctx {
   fs_mg_dev *mg = nullptr;
 
   // timing
+  cudaEvent_t tev[2] = {};                 // fs_timer_start / fs_timer_stop
+  cudaEvent_t sev[5][2] = {};              // around the solver launch of each NF
+  bool s_pending[5] = {};
+  float s_ms[5] = {};
+  int32_t s_its[5] = {}, s_calls[5] = {};
   cudaEvent_t ev[6] = {};
   float phase_ms[5] = {};
   int coop_grid = 0;            // blocks of a cooperative solver launch
@@ -126,3 +131,4 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
 int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);
 int fs_mg_vcycle_solve(fs_ctx *ctx, int nf, double rrf, double *iters_out);
+int fs_solver_stats_collect(fs_ctx *ctx);   // after a stream sync: fold pending solver events

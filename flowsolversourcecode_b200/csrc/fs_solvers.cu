@@ -228,6 +228,8 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
   FS_CK(cudaMemsetAsync(ctx->dphi, 0, sizeof(double) * N, ctx->st));
   SolveArgs a = solve_args(ctx, nf, rrf, itmax);
   int rc = FS_OK;
+  if (ctx->s_pending[nf - 1]) { FS_CK(cudaStreamSynchronize(ctx->st)); fs_solver_stats_collect(ctx); }
+  FS_CK(cudaEventRecord(ctx->sev[nf - 1][0], ctx->st));
   if (solver == FS_SOLVER_SOR) {
     a.color_ptr = ctx->color_rows + N;  // colour offsets live right after the row list
     rc = coop_launch(ctx, (void *)k_sor, a);
@@ -242,7 +244,25 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     return FS_E_ARG;
   }
   if (rc) return rc;
+  FS_CK(cudaEventRecord(ctx->sev[nf - 1][1], ctx->st));
+  ctx->s_pending[nf - 1] = true;
   k_axpy_field<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, fi, ctx->dphi);
   FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+int fs_solver_stats_collect(fs_ctx *ctx) {
+  int32_t it[8];
+  bool any = false;
+  for (int q = 0; q < 5; q++) any |= ctx->s_pending[q];
+  if (!any) return FS_OK;
+  FS_CK(cudaMemcpy(it, ctx->d_iters, sizeof(it), cudaMemcpyDeviceToHost));
+  for (int q = 0; q < 5; q++) {
+    if (!ctx->s_pending[q]) continue;
+    float ms = 0.f;
+    FS_CK(cudaEventElapsedTime(&ms, ctx->sev[q][0], ctx->sev[q][1]));
+    ctx->s_ms[q] += ms; ctx->s_its[q] += it[q]; ctx->s_calls[q] += 1;
+    ctx->s_pending[q] = false;
+  }
   return FS_OK;
 }

@@ -188,6 +188,21 @@ class Solver:
         self.lib.fs_phase_times(self.ctx, a)
         return list(a)
 
+    def timer_start(self):
+        self._chk(self.lib.fs_timer_start(self.ctx), "timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        self._chk(self.lib.fs_timer_stop(self.ctx, C.byref(ms)), "timer_stop")
+        return ms.value
+
+    def solver_stats(self, reset: bool = True) -> dict:
+        ms = (C.c_float * 5)()
+        it = np.zeros(5, np.int32)
+        calls = np.zeros(5, np.int32)
+        self._chk(self.lib.fs_solver_stats(self.ctx, ms, L.iptr(it), L.iptr(calls), int(reset)), "solver_stats")
+        return {"ms": list(ms), "iters": it.tolist(), "calls": calls.tolist()}
+
     def launch_count(self) -> int:
         return int(self.lib.fs_launch_count(self.ctx))
 

@@ -253,6 +253,15 @@ int fs_mg_parents(fs_ctx *ctx, int level, int32_t *parents, size_t n);
  * [0] momentum assembly, [1] momentum solves, [2] continuity assembly,
  * [3] p' solve, [4] corrections+residuals. */
 int fs_phase_times(fs_ctx *ctx, float *ms5);
+/* CUDA-event timer on the context stream: fs_timer_start records the start
+ * event; fs_timer_stop records the stop event, waits for it and returns the
+ * elapsed device time in milliseconds. */
+int fs_timer_start(fs_ctx *ctx);
+int fs_timer_stop(fs_ctx *ctx, float *ms);
+/* Linear-solver statistics accumulated since the last reset, per NF 1..5:
+ * device time of the solver kernels (CUDA events around each launch, in ms),
+ * solver iterations, and calls.  reset=1 clears them after reading. */
+int fs_solver_stats(fs_ctx *ctx, float *ms5, int32_t *iters5, int32_t *calls5, int reset);
 /* Number of kernel launches issued by this context since creation. */
 int64_t fs_launch_count(const fs_ctx *ctx);
 /* Synchronise the context stream. */
