@@ -190,7 +190,7 @@ def test_outer_iterations_bicgs():
             # residuals at round-off level (the 1e-10 Krylov solves leave ~1e-17
             # mass imbalance) are compared against an absolute floor
             floor = 1e-12 * max(ro["max"][0], ro["max"][1], ro["max"][2])
-            assert abs(r["max"][q] - ro["max"][q]) <= 1e-6 * max(ro["max"][q], floor), (it, q)
+            assert abs(r["max"][q] - ro["max"][q]) <= max(1e-6 * ro["max"][q], floor), (it, q)
     for k in ("u", "v", "w", "p", "mdot"):
         assert _rel(s.get(k), o.get(k)) <= 1e-7, k
 
