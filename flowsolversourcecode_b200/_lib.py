@@ -19,6 +19,8 @@ FS_MAX_PATCHES = 32
 # status codes
 FS_OK, FS_E_ARG, FS_E_CUDA, FS_E_NOMEM, FS_E_NAN, FS_E_DIVERGED, FS_E_TIMEOUT, FS_E_MESH, FS_E_UNSUPPORTED = (
     0, -1, -2, -3, -4, -5, -6, -7, -8)
+FS_E_TOO_LARGE = -9
+FS_NOALLOC_MAX_ROWS = 262144
 # variable ids (GetNFfromVariable)
 VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
 # boundary types
@@ -115,6 +117,7 @@ PROTOTYPES = {
     "fs_solver_stats": (C.c_int, [_V, C.POINTER(C.c_float), _I, _I, C.c_int]),
     "fs_launch_count": (C.c_int64, [_V]),
     "fs_sync": (C.c_int, [_V]),
+    "fs_bicgstab_noalloc": (C.c_int, [C.c_int32, C.c_int32, _V, _V, _V, _V, _V, _V, C.c_int32, C.c_double, _V, _V]),
 }
 
 _lib = None

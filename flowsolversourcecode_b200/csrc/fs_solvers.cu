@@ -266,3 +266,90 @@ int fs_solver_stats_collect(fs_ctx *ctx) {
   }
   return FS_OK;
 }
+
+// ======================================================================
+// fs_bicgstab_noalloc: the BiCGSTAB solve for callers that cannot allocate.
+//
+// Some callers cannot call cudaMalloc at all: a Fortran host that must stay
+// inside a memory budget fixed by another framework's allocator, code running
+// while a CUDA graph is being captured elsewhere in the process, or a plugin
+// host that forbids device allocations after start-up.  They still own the
+// matrix, the right-hand side and the solution in device memory, but not the
+// six Krylov work vectors.  This entry point runs the same k_bicgstab kernel
+// with its work vectors, partial sums and counters in one fixed file-scope
+// device array, so it allocates nothing.
+//
+// Limits and rules:
+//   - at most FS_NOALLOC_MAX_ROWS rows; larger systems are rejected with
+//     FS_E_TOO_LARGE before anything is launched;
+//   - the array is shared by every call on a device: two calls whose kernels
+//     overlap on the GPU (different streams, or different host threads on one
+//     device) race on it and give wrong answers; serialise them;
+//   - nothing in the array has to start at zero: the kernel writes every work
+//     entry (r0, r, p first, then v, s, t, then the partial sums) before it
+//     reads it in the same call, so the previous call's contents are ignored;
+//   - the first call on a device looks up the array's device address with
+//     cudaGetSymbolAddress (with that device current) and caches it; make that
+//     first call before any stream capture that should contain the solve.
+// ======================================================================
+#define FS_NOALLOC_VECS 6
+#define FS_NOALLOC_PARTS (6 * FS_RED_BLOCKS)
+
+static __device__ __align__(256) double g_noalloc_scratch[FS_NOALLOC_VECS * (size_t)FS_NOALLOC_MAX_ROWS +
+                                                          FS_NOALLOC_PARTS + 16];
+
+#include <mutex>
+namespace {
+struct NoallocDev { double *base = nullptr; int grid = 0; };
+std::mutex g_noalloc_mu;
+NoallocDev g_noalloc_dev[64];
+}  // namespace
+
+extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, const int32_t *cn,
+                                   const double *ac, const double *anb, const double *bc, double *x,
+                                   int32_t maxit, double tol, int32_t *iters, void *stream) {
+  if (n <= 0 || w <= 0 || !ncf || !cn || !ac || !anb || !bc || !x || maxit < 1) return FS_E_ARG;
+  if (n > FS_NOALLOC_MAX_ROWS) return FS_E_TOO_LARGE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FS_E_CUDA;
+  NoallocDev d;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_dev[dev].base) {
+      // once per device, with that device current: the symbol's device address
+      double *ptr = nullptr;
+      if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return FS_E_CUDA;
+      int per_sm = 0, per_sm2 = 0, sms = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_bicgstab, FS_BLOCK, 0) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void *)k_sor, FS_BLOCK, 0) != cudaSuccess ||
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return FS_E_CUDA;
+      if (per_sm2 < per_sm) per_sm = per_sm2;
+      if (per_sm < 1) return FS_E_CUDA;
+      int g = sms * (per_sm > 4 ? 4 : per_sm);   // the grid the context solvers use
+      if (g > FS_RED_BLOCKS) g = FS_RED_BLOCKS;
+      g_noalloc_dev[dev].base = ptr;
+      g_noalloc_dev[dev].grid = g;
+    }
+    d = g_noalloc_dev[dev];
+  }
+  const size_t M = (size_t)FS_NOALLOC_MAX_ROWS;
+  double *base = d.base;
+  SolveArgs a{};
+  a.N = n; a.W = w; a.ncf = ncf; a.cn = cn; a.ac = ac; a.anb = anb; a.bc = bc;
+  a.x = x; a.dphi = x;
+  a.r = base; a.r0 = base + M; a.p = base + 2 * M; a.v = base + 3 * M; a.s = base + 4 * M; a.t = base + 5 * M;
+  a.part = base + FS_NOALLOC_VECS * M;
+  a.diag = a.part + FS_NOALLOC_PARTS;
+  a.iters = iters ? iters : (int32_t *)(a.diag + 4);
+  a.ires = a.diag;
+  a.tol = tol; a.itmax = maxit;
+  int G = d.grid;
+  long need = ((long)n + FS_BLOCK - 1) / FS_BLOCK;
+  if (need < G) G = (int)need;
+  void *args[] = {&a};
+  if (cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(G), dim3(FS_BLOCK), args, 0,
+                                  (cudaStream_t)stream) != cudaSuccess)
+    return FS_E_CUDA;
+  return FS_OK;
+}

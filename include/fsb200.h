@@ -40,6 +40,7 @@ extern "C" {
 #define FS_E_TIMEOUT     -6   /* bounded device wait gave up */
 #define FS_E_MESH        -7   /* inconsistent mesh */
 #define FS_E_UNSUPPORTED -8   /* option not implemented */
+#define FS_E_TOO_LARGE   -9   /* problem larger than a fixed-size scratch allows */
 
 /* ------------------------------------------------------- variable ids (NF)
  * GetNFfromVariable (AlgebraicSolvers/AssignNFvaluesToVariables.for:4):
@@ -266,6 +267,25 @@ int fs_solver_stats(fs_ctx *ctx, float *ms5, int32_t *iters5, int32_t *calls5, i
 int64_t fs_launch_count(const fs_ctx *ctx);
 /* Synchronise the context stream. */
 int fs_sync(fs_ctx *ctx);
+
+/* BiCGSTAB without any device allocation.  No counterpart in the reference:
+ * it is the k_bicgstab solve of fs_solve_system_host for callers that cannot
+ * call cudaMalloc (a host whose device memory is owned by another allocator,
+ * or that must not allocate once running).  All pointers are device memory
+ * owned by the caller, in the layout of fs_solve_system_host: ncf [n],
+ * cn and anb [w*n slot-major], ac and bc [n]; x [n] holds the initial guess on
+ * entry and the solution on return; iters (device int32, may be NULL) gets
+ * the iteration count.  The work vectors live in one fixed device array of
+ * the library, so n may not exceed FS_NOALLOC_MAX_ROWS (FS_E_TOO_LARGE
+ * otherwise).  The solve is queued on `stream` (a cudaStream_t, NULL for the
+ * default stream) and the call returns without waiting.  Every call on a
+ * device shares that array: calls that overlap on the GPU race on it.  The
+ * first call on a device looks the array's address up (cudaGetSymbolAddress)
+ * and should come before any stream capture that is meant to contain it. */
+#define FS_NOALLOC_MAX_ROWS 262144
+int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, const int32_t *cn,
+                        const double *ac, const double *anb, const double *bc, double *x,
+                        int32_t maxit, double tol, int32_t *iters, void *stream);
 
 #ifdef __cplusplus
 }
