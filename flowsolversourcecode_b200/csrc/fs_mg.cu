@@ -168,6 +168,44 @@ __device__ double residual(Sync &S, const Scope &sc, const LevelDev<R> &L, const
   return scope_sum(S, sc, s);
 }
 
+// damped Jacobi (omega = 2/3 on the diagonal ac): the preconditioner's smoother on
+// coarse levels that the whole grid processes -- 2 grid barriers per sweep instead
+// of 2 per colour (agglomerated levels need ~10 colours)
+template <class R>
+__device__ void jacobi(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, R *x, R *r, int sweeps) {
+  const int n = L.n;
+  const R omega = (R)(2.0 / 3.0);
+  for (int it = 0; it < sweeps; it++) {
+    for (long i = sc.tid0(); i < n; i += sc.nth()) {
+      R t = b[i] - L.ac[i] * x[i];
+      int nc = L.ncf[i];
+      for (int j = 0; j < nc; j++) {
+        int k = L.nbr[(long)j * n + i];
+        if (k >= 0) t = t - L.anb[(long)j * n + i] * x[k];
+      }
+      r[i] = t;
+    }
+    scope_sync(S, sc);
+    for (long i = sc.tid0(); i < n; i += sc.nth()) x[i] = x[i] + omega * r[i] / L.ac[i];
+    scope_sync(S, sc);
+  }
+}
+
+// r = b - A x without the norm (the preconditioner needs no convergence test)
+template <class R>
+__device__ void residual_only(const Scope &sc, const LevelDev<R> &L, const R *b, const R *x, R *r) {
+  const int n = L.n;
+  for (long i = sc.tid0(); i < n; i += sc.nth()) {
+    R t = b[i] - L.ac[i] * x[i];
+    int nc = L.ncf[i];
+    for (int j = 0; j < nc; j++) {
+      int k = L.nbr[(long)j * n + i];
+      if (k >= 0) t = t - L.anb[(long)j * n + i] * x[k];
+    }
+    r[i] = t;
+  }
+}
+
 // SolveEquationMG: sweeps until sum|r| <= rrF*IRes or itmax (checked=true), or
 // exactly itmax sweeps (checked=false, preconditioner)
 template <class R>
@@ -211,6 +249,8 @@ struct Cycle {
   int pre, post;
   bool checked;
   bool last_grid;   // scope of the previous operation
+  bool prec;        // preconditioner: Jacobi on grid-wide coarse levels, no norms
+  int coarse_sweeps;
   __device__ const R *B(int l) const { return l == 0 ? b0 : lev[l].b; }
   __device__ R *X(int l) const { return l == 0 ? x0 : lev[l].x; }
   __device__ R *Rr(int l) const { return l == 0 ? r0 : lev[l].r; }
@@ -223,12 +263,14 @@ struct Cycle {
   __device__ void op_smooth(int l, int itmax) {
     Scope sc = scope_of(lev[l]);
     enter(sc);
-    if (sc.active()) smooth(S, sc, lev[l], B(l), X(l), Rr(l), rrf, ires, itmax, checked);
+    if (prec && l > 0 && sc.grid) jacobi(S, sc, lev[l], B(l), X(l), Rr(l), itmax);
+    else if (sc.active()) smooth(S, sc, lev[l], B(l), X(l), Rr(l), rrf, ires, itmax, checked);
   }
   __device__ void op_residual(int l) {
     Scope sc = scope_of(lev[l]);
     enter(sc);
-    if (sc.active()) residual(S, sc, lev[l], B(l), X(l), Rr(l));
+    if (prec) { if (sc.active()) residual_only(sc, lev[l], B(l), X(l), Rr(l)); }
+    else if (sc.active()) residual(S, sc, lev[l], B(l), X(l), Rr(l));
   }
   __device__ void op_restrict(int l) {   // Restrict(l): smooth, residual, coarse rhs
     op_smooth(l, pre);
@@ -249,8 +291,8 @@ struct Cycle {
   __device__ void run(int type) {
     int L = nlev - 1;
     for (int l = 0; l < L; l++) op_restrict(l);
-    op_smooth(L, post);
-    op_residual(L);
+    op_smooth(L, prec ? coarse_sweeps : post);
+    if (!prec) op_residual(L);
     if (type != 0) {
       for (int l1 = L - 1; l1 >= 1; l1--) {
         for (int l = L; l >= l1 + 1; l--) op_prolong(l);
@@ -292,7 +334,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_mg_solve(MgSolveArgs a) {
   }
   S.all();
   double ires = *a.ires, fres = ires;
-  Cycle<double> C{S, a.lev, a.nlev, a.b0, a.x0, a.r0, a.rrf, ires, a.pre, a.post, true, true};
+  Cycle<double> C{S, a.lev, a.nlev, a.b0, a.x0, a.r0, a.rrf, ires, a.pre, a.post, true, true, false, 0};
   int ncycle = 1;
   while (ncycle <= a.maxcycles && fres > a.rrf * ires) {
     C.last_grid = true;
@@ -312,7 +354,7 @@ __device__ void vcycle_prec(Sync &S, const LevelDev<R> *lev, int nlev, const R *
     R *x = l == 0 ? x0 : lev[l].x;
     for (long i = g.tid0(); i < lev[l].n; i += g.nth()) x[i] = 0.;
   }
-  Cycle<R> C{S, lev, nlev, b0, x0, r0, 0., 0., pre, post, false, true};
+  Cycle<R> C{S, lev, nlev, b0, x0, r0, 0., 0., pre, post, false, true, true, 20};
   C.run(0);
 }
 
@@ -730,7 +772,8 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.N = ctx->N; a.ncf = ctx->ncf; a.cn = ctx->cn; a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc;
     a.x = ctx->kx; a.r = ctx->kr; a.r0 = ctx->kr0; a.p = ctx->kp; a.v = ctx->kv; a.s = ctx->ks; a.t = ctx->kt;
     a.y = ctx->ky; a.z = ctx->kz; a.dphi = ctx->dphi;
-    a.nlev = M->nlev; a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_post);
+    // one V-cycle per application: one pre- and one post-sweep (MultiGridpreSweep)
+    a.nlev = M->nlev; a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_pre);
     a.maxit = ctx->cfg.krylov_maxit; a.tol = ctx->cfg.krylov_tol; a.part = M->red;
     a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + 22;
   };
