@@ -143,7 +143,8 @@ static void free_all(fs_ctx *c) {
                   c->du1, c->dv1, c->dw1, c->du2, c->dv2, c->dw2, c->us, c->vs, c->ws,
                   c->ac, c->anb, c->bc, c->dphi, c->ac_int, c->bc_int, c->effdiv, c->pcoef,
                   c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky,
-                  c->red, c->redi, c->resblk, c->d_iters, c->d_status};
+                  c->red, c->redi, c->resblk, c->d_iters, c->d_status,
+                  c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP};
   for (void *p : ptrs) if (p) cudaFree(p);
 }
 
@@ -175,6 +176,9 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
                       &ctx->ac_int, &ctx->effdiv, &ctx->kx, &ctx->kr, &ctx->kr0, &ctx->kp, &ctx->kv, &ctx->ks,
                       &ctx->kt, &ctx->kz, &ctx->ky};
   for (auto p : cellv) if ((rc = alloc0(ctx, p, N))) return fail(rc);
+  if ((rc = alloc0(ctx, &ctx->acP, N)) || (rc = alloc0(ctx, &ctx->bcP, N)) || (rc = alloc0(ctx, &ctx->dphiP, N)) ||
+      (rc = alloc0(ctx, &ctx->anbP, W * N)))
+    return fail(rc);
   double **cell3[] = {&ctx->ug, &ctx->vg, &ctx->wg, &ctx->pg, &ctx->pcg, &ctx->bc_int};
   for (auto p : cell3) if ((rc = alloc0(ctx, p, 3 * N))) return fail(rc);
   if ((rc = alloc0(ctx, &ctx->gtmp, 12 * N))) return fail(rc);

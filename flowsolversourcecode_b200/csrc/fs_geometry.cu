@@ -296,6 +296,21 @@ int fs_geometry_build(fs_ctx *ctx, const fs_mesh_in *mi) {
   if ((rc = up(ctx, &ctx->fnbr, ctx->h_fnbr.data(), (size_t)F))) return rc;
   if ((rc = up(ctx, &ctx->bown, ctx->h_bown.data(), (size_t)B))) return rc;
   if ((rc = up(ctx, &ctx->btype, ctx->h_btype.data(), (size_t)B))) return rc;
+  {  // colour-major index maps for the permuted Gauss-Seidel matrix
+    std::vector<int32_t> pos(N), cnP((size_t)W * N, -1), ncfP(N);
+    for (int q = 0; q < N; q++) pos[ctx->h_color_rows[q]] = q;
+    for (int q = 0; q < N; q++) {
+      int i = ctx->h_color_rows[q];
+      ncfP[q] = ncf[i];
+      for (int j = 0; j < ncf[i]; j++) {
+        int k = ctx->h_cn[(size_t)j * N + i];
+        cnP[(size_t)j * N + q] = k >= 0 ? pos[k] : -1;
+      }
+    }
+    if ((rc = up(ctx, &ctx->cposP, pos.data(), pos.size()))) return rc;
+    if ((rc = up(ctx, &ctx->cnP, cnP.data(), cnP.size()))) return rc;
+    if ((rc = up(ctx, &ctx->ncfP, ncfP.data(), ncfP.size()))) return rc;
+  }
   {  // colour row lists followed by the colour offsets (ncolors+1)
     std::vector<int32_t> cr(ctx->h_color_rows);
     cr.insert(cr.end(), ctx->h_color_ptr.begin(), ctx->h_color_ptr.end());

@@ -47,6 +47,10 @@ struct fs_ctx {
   int32_t *slot = nullptr, *cn = nullptr, *ncf = nullptr;
   int32_t *fown = nullptr, *fnbr = nullptr, *bown = nullptr, *btype = nullptr;
   int32_t *color_rows = nullptr;
+  // colour-major copy of the matrix for the Gauss-Seidel sweeps: position p holds
+  // row color_rows[p]; cnP/ncfP are fixed per mesh, acP/bcP/anbP/dphiP per solve
+  int32_t *cposP = nullptr, *cnP = nullptr, *ncfP = nullptr;
+  double *acP = nullptr, *bcP = nullptr, *anbP = nullptr, *dphiP = nullptr;
 
   // geometry (device)
   double *vol = nullptr, *xc = nullptr;                     // xc: 3N
