@@ -42,6 +42,23 @@ def peaks():
     return HBM_FALLBACK_GBS, "fallback"
 
 
+def reduce_max(ms: float, dist=None, device="cpu") -> float:
+    """Max of a per-rank device time over all ranks (the slowest replica sets
+    the aggregate rate).  With no process group it is the local value."""
+    if dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, steps: int, ms_max: float) -> float:
+    """Whole-job SIMPLE iterations per second: every rank runs `steps`
+    iterations of its own replica; the job takes the slowest rank's time."""
+    return world * steps / (ms_max * 1e-3)
+
+
 def workload(n: int):
     from flowsolversourcecode_b200 import case as cs
     mesh, case = cs.cavity3d(n, solver_mom="sor", solver_cont="bicgs")
@@ -245,10 +262,7 @@ def main():
     clocks = clk.summary()
     stats = s.solver_stats(reset=True)
     phases = s.phase_times()
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = reduce_max(ms, dist, f"cuda:{local}")
 
     # ---------------- end-to-end leg (host buffers through the C ABI)
     st = s.state()
@@ -266,10 +280,7 @@ def main():
     for _ in range(args.steps):
         s.simple_iteration_host(host)
     e2e_ms = s.timer_stop()
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_max = float(t.item())
+    e2e_max = reduce_max(e2e_ms, dist, f"cuda:{local}")
     io_bytes = 8 * sum(a.shape[0] for a in host.values())
 
     if rank == 0:
@@ -285,7 +296,7 @@ def main():
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline_sample(mesh, case)
-        value = world * args.steps / (ms_max * 1e-3)
+        value = aggregate_rate(world, args.steps, ms_max)
         line = {
             "metric": "SIMPLE iters/s", "value": value, "unit": "iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": warm, "ms_per_step": ms_max / args.steps,
@@ -301,7 +312,7 @@ def main():
                        "phase_ms_last_step": [round(x, 3) for x in phases]},
             "roofline": roof,
             "cpu_baseline": cpu,
-            "e2e": {"value": world * args.steps / (e2e_max * 1e-3), "unit": "iter/s",
+            "e2e": {"value": aggregate_rate(world, args.steps, e2e_max), "unit": "iter/s",
                     "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
             "gpu_launches": launches,
             "clocks": clocks,

@@ -20,7 +20,7 @@ SOURCES = ["fs_geometry.cu", "fs_simple.cu", "fs_solvers.cu", "fs_mg.cu", "fs_ca
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC,-O2",
-         "-I", os.path.join(HERE, "..", "include")]
+         "-I", os.path.join(HERE, "..", "include")] + os.environ.get("FSB200_NVCC_FLAGS", "").split()
 
 
 def _stale(out: str, deps: list[str]) -> bool:

@@ -142,7 +142,7 @@ static void free_all(fs_ctx *c) {
                   c->ug, c->vg, c->wg, c->pg, c->pcg, c->bug, c->bvg, c->bwg, c->bpg, c->bpcg, c->gtmp,
                   c->du1, c->dv1, c->dw1, c->du2, c->dv2, c->dw2, c->us, c->vs, c->ws,
                   c->ac, c->anb, c->bc, c->dphi, c->ac_int, c->bc_int, c->effdiv, c->pcoef,
-                  c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky,
+                  c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky, c->sysx,
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
                   c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP};
   for (void *p : ptrs) if (p) cudaFree(p);
@@ -174,7 +174,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   double **cellv[] = {&ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->pc, &ctx->du1, &ctx->dv1, &ctx->dw1, &ctx->du2,
                       &ctx->dv2, &ctx->dw2, &ctx->us, &ctx->vs, &ctx->ws, &ctx->ac, &ctx->bc, &ctx->dphi,
                       &ctx->ac_int, &ctx->effdiv, &ctx->kx, &ctx->kr, &ctx->kr0, &ctx->kp, &ctx->kv, &ctx->ks,
-                      &ctx->kt, &ctx->kz, &ctx->ky};
+                      &ctx->kt, &ctx->kz, &ctx->ky, &ctx->sysx};
   for (auto p : cellv) if ((rc = alloc0(ctx, p, N))) return fail(rc);
   if ((rc = alloc0(ctx, &ctx->acP, N)) || (rc = alloc0(ctx, &ctx->bcP, N)) || (rc = alloc0(ctx, &ctx->dphiP, N)) ||
       (rc = alloc0(ctx, &ctx->anbP, W * N)))
@@ -416,7 +416,7 @@ int fs_solve_system_host(fs_ctx *ctx, const double *ac, const double *anb, const
   FS_CK(cudaMemcpyAsync(ctx->anb, anb, sizeof(double) * N * W, cudaMemcpyHostToDevice, ctx->st));
   FS_CK(cudaMemcpyAsync(ctx->bc, bc, sizeof(double) * N, cudaMemcpyHostToDevice, ctx->st));
   // solve into a zero field so the update equals dphi
-  double *fz = ctx->ky;
+  double *fz = ctx->sysx;
   FS_CK(cudaMemsetAsync(fz, 0, sizeof(double) * N, ctx->st));
   int rc = residual_of_system(ctx, FS_VAR_PC, fz);
   if (rc) return rc;

@@ -20,6 +20,9 @@
 #include <cstdint>
 
 #define FS_BLOCK 256
+#ifndef FS_COOP_BLOCK
+#define FS_COOP_BLOCK 256            // threads per CTA of the persistent cooperative solvers
+#endif
 #define FS_RED_BLOCKS 1184           // 148 SMs x 8: partial-sum slots of the grid reductions
 
 // reduction slots in ctx->red (double); each quantity has FS_RED_BLOCKS partials
@@ -74,6 +77,7 @@ struct fs_ctx {
   // krylov work (device)
   double *kx = nullptr, *kr = nullptr, *kr0 = nullptr, *kp = nullptr, *kv = nullptr, *ks = nullptr, *kt = nullptr;
   double *kz = nullptr, *ky = nullptr;   // preconditioned vectors (AMG-BiCGSTAB)
+  double *sysx = nullptr;                // fs_solve_system_host: the field the update is added to
   // reductions
   double *red = nullptr;        // RED_NQ * FS_RED_BLOCKS partials
   int64_t *redi = nullptr;      // FS_RED_BLOCKS argmax partials

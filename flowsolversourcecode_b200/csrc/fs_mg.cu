@@ -324,7 +324,7 @@ struct MgSolveArgs {
 };
 
 // AlgebraicMultigrid cycle loop (AlgebraicMultiGridMainRoutine.for:330-345)
-__global__ void __launch_bounds__(FS_BLOCK) k_mg_solve(MgSolveArgs a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
   Sync S(a.part);
   // dphiMG = 0 on every level
   for (int l = 0; l < a.nlev; l++) {
@@ -401,7 +401,7 @@ __device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, doub
 
 // right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle
 template <class R>
-__global__ void __launch_bounds__(FS_BLOCK) k_amg_bicgstab(AmgKArgs<R> a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK) k_amg_bicgstab(AmgKArgs<R> a) {
   Sync S(a.part);
   const int N = a.N;
   Scope g; g.grid = true;
@@ -706,9 +706,9 @@ int fs_mg_build(fs_ctx *ctx) {
   FS_CK(cudaMalloc(&M->red, sizeof(double) * 6 * FS_RED_BLOCKS));
   // cooperative grid: smallest co-resident count of the three kernels, <= 4 CTAs/SM
   int a = 0, b = 0, c = 0;
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_mg_solve, FS_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double>, FS_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float>, FS_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_mg_solve, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double>, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float>, FS_COOP_BLOCK, 0));
   int per = std::min(a, std::min(b, c));
   if (per < 1) { ctx->err = "multigrid kernels do not fit on an SM"; return FS_E_CUDA; }
   M->grid = ctx->num_sms * std::min(per, 4);
@@ -764,7 +764,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.maxcycles = ctx->cfg.mg_max_cycles; a.b0 = ctx->bc; a.x0 = ctx->dphi; a.r0 = M->r[0];
     a.rrf = rrf; a.ires = ctx->resblk + RB_ABS + (nf - 1); a.part = M->red; a.iters = ctx->d_iters + (nf - 1);
     void *args[] = {&a};
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_mg_solve, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+    FS_CK(cudaLaunchCooperativeKernel((void *)k_mg_solve, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
     FS_LAUNCH_CHECK();
     return FS_OK;
   }
@@ -782,13 +782,13 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     fill(a);
     a.lev = M->lev64; a.b32 = nullptr; a.x32 = nullptr; a.r32 = M->r[0];
     void *args[] = {&a};
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<double>, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<double>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
   } else {
     AmgKArgs<float> a{};
     fill(a);
     a.lev = M->lev32; a.b32 = M->bf[0]; a.x32 = M->xf[0]; a.r32 = M->rf[0];
     void *args[] = {&a};
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<float>, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<float>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
   }
   FS_LAUNCH_CHECK();
   (void)rrf;

@@ -98,10 +98,12 @@ struct GradJob {
 };
 
 // StandardGreenGauss / first pass of StandardGreenGaussFaceCorrection1
-// (StandardGreenGaussGradient.for:35-79; StandardGreenGaussCorrection1Gradient.for:47-96)
+// (StandardGreenGaussGradient.for:35-79; StandardGreenGaussCorrection1Gradient.for:47-96).
+// A cell's own values stay in registers; the other cell of each interior face
+// comes from the slot-major neighbour table cn (one coalesced index load), so
+// each slot costs one gathered value per field.
 __global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B,
-    const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot,
-    const int32_t *__restrict__ fown, const int32_t *__restrict__ fnbr,
+    const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot, const int32_t *__restrict__ cn,
     const double *__restrict__ gf, const double *__restrict__ sf,
     const double *__restrict__ bsf, const double *__restrict__ vol) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -109,17 +111,21 @@ __global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B
   int nc = ncf[i];
   double V = vol[i];
   for (int q = 0; q < J.nfld; q++) {
-    const double *phi = J.phi[q], *bphi = J.bphi[q];
+    const double *__restrict__ phi = J.phi[q];
+    const double *__restrict__ bphi = J.bphi[q];
+    const double pself = phi[i];
     double gx = 0., gy = 0., gz = 0.;
     for (int j = 0; j < nc; j++) {
       int s = slot[(long)j * N + i];
       int f = s >> 1;
       if (f < F) {
-        int o = fown[f], n = fnbr[f];
         double g = gf[f];
-        double fip = phi[o] * g + phi[n] * (1. - g);
+        double pk = phi[cn[(long)j * N + i]];
+        bool nbr_side = s & 1;
+        double po = nbr_side ? pk : pself, pn = nbr_side ? pself : pk;
+        double fip = po * g + pn * (1. - g);
         double fx = fip * sf[f], fy = fip * sf[F + f], fz = fip * sf[2L * F + f];
-        if (s & 1) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
+        if (nbr_side) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
         else { gx = gx + fx; gy = gy + fy; gz = gz + fz; }
       } else {
         int b = f - F;
@@ -134,8 +140,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B
 
 // correction pass of StandardGreenGaussFaceCorrection1 (:98-172)
 __global__ void __launch_bounds__(FS_BLOCK) k_gg_corr(GradJob J, int N, int F, int B,
-    const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot,
-    const int32_t *__restrict__ fown, const int32_t *__restrict__ fnbr,
+    const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot, const int32_t *__restrict__ cn,
     const double *__restrict__ gf, const double *__restrict__ sf, const double *__restrict__ dfp,
     const double *__restrict__ bsf, const double *__restrict__ vol) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -143,21 +148,30 @@ __global__ void __launch_bounds__(FS_BLOCK) k_gg_corr(GradJob J, int N, int F, i
   int nc = ncf[i];
   double V = vol[i];
   for (int q = 0; q < J.nfld; q++) {
-    const double *phi = J.phi[q], *bphi = J.bphi[q], *gi = J.in[q];
+    const double *__restrict__ phi = J.phi[q];
+    const double *__restrict__ bphi = J.bphi[q];
+    const double *__restrict__ gi = J.in[q];
+    const double ps = phi[i], gsx = gi[i], gsy = gi[N + i], gsz = gi[2L * N + i];
     double gx = 0., gy = 0., gz = 0.;
     for (int j = 0; j < nc; j++) {
       int s = slot[(long)j * N + i];
       int f = s >> 1;
       if (f < F) {
-        int o = fown[f], n = fnbr[f];
+        int k = cn[(long)j * N + i];
         double g = gf[f];
-        double fip = phi[o] * g + phi[n] * (1. - g);
-        double cx = gi[o] * g + gi[n] * (1. - g); cx = cx * dfp[f];
-        double cy = gi[N + o] * g + gi[N + n] * (1. - g); cy = cy * dfp[F + f];
-        double cz = gi[2L * N + o] * g + gi[2L * N + n] * (1. - g); cz = cz * dfp[2L * F + f];
+        double pk = phi[k], gkx = gi[k], gky = gi[N + k], gkz = gi[2L * N + k];
+        bool nb = s & 1;
+        double po = nb ? pk : ps, pn = nb ? ps : pk;
+        double gox = nb ? gkx : gsx, gnx = nb ? gsx : gkx;
+        double goy = nb ? gky : gsy, gny = nb ? gsy : gky;
+        double goz = nb ? gkz : gsz, gnz = nb ? gsz : gkz;
+        double fip = po * g + pn * (1. - g);
+        double cx = gox * g + gnx * (1. - g); cx = cx * dfp[f];
+        double cy = goy * g + gny * (1. - g); cy = cy * dfp[F + f];
+        double cz = goz * g + gnz * (1. - g); cz = cz * dfp[2L * F + f];
         double phif = fip + cx + cy + cz;
         double fx = phif * sf[f], fy = phif * sf[F + f], fz = phif * sf[2L * F + f];
-        if (s & 1) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
+        if (nb) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
         else { gx = gx + fx; gy = gy + fy; gz = gz + fz; }
       } else {
         int b = f - F;
@@ -261,7 +275,7 @@ __device__ __forceinline__ double hr_flux(int scheme, double bleed, double md, d
 // ------------------------------------------------------------ momentum
 struct MomArgs {
   int N, F, B;
-  const int32_t *ncf, *slot, *fown, *fnbr, *bown, *btype;
+  const int32_t *ncf, *slot, *fown, *fnbr, *bown, *btype, *cn;
   const double *gf, *sf, *dcfv, *dcf, *gdiff, *tf, *vol;
   const double *bsf, *bfa, *bnf, *bdv, *bgdiff, *btf;
   const double *u, *v, *w, *mdot, *bmdot, *bu, *bv, *bw;
@@ -287,18 +301,34 @@ __global__ void __launch_bounds__(FS_BLOCK) k_mom_interior(MomArgs a) {
   const long N2 = 2L * N, F2 = 2L * F;
   int nc = a.ncf[i];
   const double mu = a.mu;
+  // this cell's values stay in registers; the other cell of a face is cn(i,j)
+  const double us = a.u[i], vs = a.v[i], ws = a.w[i];
+  const double gus[3] = {a.ug[i], a.ug[N + i], a.ug[N2 + i]};
+  const double gvs[3] = {a.vg[i], a.vg[N + i], a.vg[N2 + i]};
+  const double gws[3] = {a.wg[i], a.wg[N + i], a.wg[N2 + i]};
   double ac = 0., bcu = 0., bcv = 0., bcw = 0., ed = 0.;
   for (int j = 0; j < nc; j++) {
     int s = a.slot[(long)j * N + i];
     int f = s >> 1;
     if (f >= F) { ed = ed + a.bmdot[f - F]; continue; }
-    int o = a.fown[f], n = a.fnbr[f];
+    const bool nb = s & 1;                 // this cell is the face's neighbour
+    const int k = a.cn[(long)j * N + i];
     double g = a.gf[f], md = a.mdot[f];
     double sx = a.sf[f], sy = a.sf[F + f], sz = a.sf[F2 + f];
-    double uo = a.u[o], un = a.u[n], vo = a.v[o], vn = a.v[n], wo = a.w[o], wn = a.w[n];
-    double guo[3] = {a.ug[o], a.ug[N + o], a.ug[N2 + o]}, gun[3] = {a.ug[n], a.ug[N + n], a.ug[N2 + n]};
-    double gvo[3] = {a.vg[o], a.vg[N + o], a.vg[N2 + o]}, gvn[3] = {a.vg[n], a.vg[N + n], a.vg[N2 + n]};
-    double gwo[3] = {a.wg[o], a.wg[N + o], a.wg[N2 + o]}, gwn[3] = {a.wg[n], a.wg[N + n], a.wg[N2 + n]};
+    const double uk = a.u[k], vk = a.v[k], wk = a.w[k];
+    const double guk[3] = {a.ug[k], a.ug[N + k], a.ug[N2 + k]};
+    const double gvk[3] = {a.vg[k], a.vg[N + k], a.vg[N2 + k]};
+    const double gwk[3] = {a.wg[k], a.wg[N + k], a.wg[N2 + k]};
+    // owner (o) / neighbour (n) values in the face's orientation
+    double uo = nb ? uk : us, un = nb ? us : uk;
+    double vo = nb ? vk : vs, vn = nb ? vs : vk;
+    double wo = nb ? wk : ws, wn = nb ? ws : wk;
+    double guo[3], gun[3], gvo[3], gvn[3], gwo[3], gwn[3];
+    for (int d = 0; d < 3; d++) {
+      guo[d] = nb ? guk[d] : gus[d]; gun[d] = nb ? gus[d] : guk[d];
+      gvo[d] = nb ? gvk[d] : gvs[d]; gvn[d] = nb ? gvs[d] : gvk[d];
+      gwo[d] = nb ? gwk[d] : gws[d]; gwn[d] = nb ? gws[d] : gwk[d];
+    }
     double dx = a.dcfv[f], dy = a.dcfv[F + f], dz = a.dcfv[F2 + f], d = a.dcf[f];
     double ex = dx / d, ey = dy / d, ez = dz / d;
     double fcf = 0., fff = 0., tu = 0., tv = 0., tw = 0.;
@@ -325,17 +355,17 @@ __global__ void __launch_bounds__(FS_BLOCK) k_mom_interior(MomArgs a) {
       tv = tv + -(M23 * gamf * div * sy);
       tw = tw + -(M23 * gamf * div * sz);
     }
-    double cc = fmax(md, 0.), cn = -fmax(-md, 0.);
-    fcf = fcf + cc; fff = fff + cn;
-    tu = tu + (cc * uo + cn * un);
-    tv = tv + (cc * vo + cn * vn);
-    tw = tw + (cc * wo + cn * wn);
+    double cc = fmax(md, 0.), cn_ = -fmax(-md, 0.);
+    fcf = fcf + cc; fff = fff + cn_;
+    tu = tu + (cc * uo + cn_ * un);
+    tv = tv + (cc * vo + cn_ * vn);
+    tw = tw + (cc * wo + cn_ * wn);
     if (a.hr_on) {
       tu = tu + hr_flux(a.conv_scheme, a.bleed, md, uo, un, guo, gun, dx, dy, dz);
       tv = tv + hr_flux(a.conv_scheme, a.bleed, md, vo, vn, gvo, gvn, dx, dy, dz);
       tw = tw + hr_flux(a.conv_scheme, a.bleed, md, wo, wn, gwo, gwn, dx, dy, dz);
     }
-    if (s & 1) {   // this cell is the neighbour
+    if (nb) {
       ac = ac - fff;
       a.anb[(long)j * N + i] = 0. - fcf;
       bcu = bcu + tu; bcv = bcv + tv; bcw = bcw + tw;
@@ -743,9 +773,9 @@ int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const 
     }
     J.nfld = n;
     if (pidx == 0)
-      k_gg0<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->fown, ctx->fnbr, ctx->gf, ctx->sf, ctx->bsf, ctx->vol);
+      k_gg0<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf, ctx->sf, ctx->bsf, ctx->vol);
     else
-      k_gg_corr<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->fown, ctx->fnbr, ctx->gf, ctx->sf, ctx->dfp, ctx->bsf, ctx->vol);
+      k_gg_corr<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf, ctx->sf, ctx->dfp, ctx->bsf, ctx->vol);
     FS_LAUNCH_CHECK();
   }
   if (B) {
@@ -763,6 +793,7 @@ static MomArgs mom_args(fs_ctx *ctx) {
   const fs_case &c = ctx->cfg;
   a.N = ctx->N; a.F = ctx->F; a.B = ctx->B;
   a.ncf = ctx->ncf; a.slot = ctx->slot; a.fown = ctx->fown; a.fnbr = ctx->fnbr; a.bown = ctx->bown; a.btype = ctx->btype;
+  a.cn = ctx->cn;
   a.gf = ctx->gf; a.sf = ctx->sf; a.dcfv = ctx->dcfv; a.dcf = ctx->dcf; a.gdiff = ctx->gdiff; a.tf = ctx->tf; a.vol = ctx->vol;
   a.bsf = ctx->bsf; a.bfa = ctx->bfa; a.bnf = ctx->bnf; a.bdv = ctx->bdv; a.bgdiff = ctx->bgdiff; a.btf = ctx->btf;
   a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.mdot = ctx->mdot; a.bmdot = ctx->bmdot; a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw;

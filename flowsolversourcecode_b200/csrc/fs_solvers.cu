@@ -87,7 +87,7 @@ __device__ void grid_sum2(cg::grid_group &grid, double *part, int buf, double a0
 // BICGSTAB_OMP (matrixSolverOMP.f90:306-386): unpreconditioned, x kept between
 // calls (the reference's module vector x), stop when sqrt|r.r0| <= tol*|b|
 // or after maxit-1 iterations.
-__global__ void __launch_bounds__(FS_BLOCK) k_bicgstab(SolveArgs a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK) k_bicgstab(SolveArgs a) {
   cg::grid_group grid = cg::this_grid();
   const int N = a.N;
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
@@ -138,98 +138,11 @@ __global__ void __launch_bounds__(FS_BLOCK) k_bicgstab(SolveArgs a) {
   if (tid0 == 0) { *a.iters = k - 1; a.diag[0] = resnorm; a.diag[1] = normb; }
 }
 
-// The same BICGSTAB_OMP iteration with three grid barriers instead of five.
-// s = r - alpha*v is formed where it is used (second SpMV, x/r update), and the
-// p update of iteration k is folded into the first SpMV of iteration k+1, where
-// every neighbour value p_new(j) = r(j) + beta*(p(j) - omega*v(j)) is formed on
-// the fly (p and v double-buffered).  Each element is the same expression as in
-// the reference, so iterates equal k_bicgstab's bit for bit; dot products are
-// summed in the same per-thread and per-CTA order.
-__global__ void __launch_bounds__(FS_BLOCK) k_bicgstab3(SolveArgs a, double *pb, double *vb) {
-  cg::grid_group grid = cg::this_grid();
-  const int N = a.N;
-  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
-  double *pA = a.p, *pB = pb, *vA = a.v, *vB = vb;   // old / new buffers, swapped each iteration
-  double l0 = 0., l1 = 0.;
-  for (long i = tid0; i < N; i += nth) {
-    double r0 = a.bc[i] - row_ax(a, (int)i, a.x);
-    a.r0[i] = r0; a.r[i] = r0; pA[i] = 0.; vA[i] = 0.;
-    l0 += r0 * r0;
-    l1 += a.bc[i] * a.bc[i];
-  }
-  double rhoPrev, bb;
-  grid_sum2(grid, a.part, 0, l0, l1, rhoPrev, bb);
-  double resnorm = sqrt(fabs(rhoPrev)), normb = sqrt(bb);
-  // first iteration: p = r0 exactly (beta = 0 on zero p and v)
-  double beta = 0., omega = 1.;
-  int k = 1;
-  int buf = 1;
-  const int32_t *__restrict__ ncf = a.ncf;
-  const int32_t *__restrict__ cn = a.cn;
-  const double *__restrict__ ac = a.ac;
-  const double *__restrict__ anb = a.anb;
-  while (k < a.itmax && resnorm > a.tol * normb) {
-    k = k + 1;
-    // A: p_new = r + beta*(p - omega*v); v_new = A p_new; dp0 = v_new.r0
-    l0 = 0.;
-    for (long i = tid0; i < N; i += nth) {
-      double pi = a.r[i] + beta * (pA[i] - omega * vA[i]);
-      double t = 0.0;
-      t = t + ac[i] * pi;
-      int nc = ncf[i];
-      for (int j = 0; j < nc; j++) {
-        int q = cn[(long)j * N + i];
-        if (q >= 0) t = t + anb[(long)j * N + i] * (a.r[q] + beta * (pA[q] - omega * vA[q]));
-      }
-      pB[i] = pi; vB[i] = t;
-      l0 += t * a.r0[i];
-    }
-    double dp0, dum;
-    grid_sum2(grid, a.part, buf, l0, 0., dp0, dum); buf ^= 3;
-    double alpha = rhoPrev / dp0;
-    // B: t = A s with s = r - alpha*v_new; dp1 = t.s, dp2 = t.t
-    l0 = 0.; l1 = 0.;
-    for (long i = tid0; i < N; i += nth) {
-      double si = a.r[i] - alpha * vB[i];
-      double t = 0.0;
-      t = t + ac[i] * si;
-      int nc = ncf[i];
-      for (int j = 0; j < nc; j++) {
-        int q = cn[(long)j * N + i];
-        if (q >= 0) t = t + anb[(long)j * N + i] * (a.r[q] - alpha * vB[q]);
-      }
-      a.t[i] = t;
-      l0 += t * si; l1 += t * t;
-    }
-    double dp1, dp2;
-    grid_sum2(grid, a.part, buf, l0, l1, dp1, dp2); buf ^= 3;
-    omega = dp1 / dp2;
-    // C: x += alpha p + omega s ; r = s - omega t ; rho = r.r0
-    l0 = 0.;
-    for (long i = tid0; i < N; i += nth) {
-      double si = a.r[i] - alpha * vB[i];
-      a.x[i] = a.x[i] + alpha * pB[i] + omega * si;
-      double ri = si - omega * a.t[i];
-      a.r[i] = ri;
-      l0 += ri * a.r0[i];
-    }
-    double rho;
-    grid_sum2(grid, a.part, buf, l0, 0., rho, dum); buf ^= 3;
-    beta = (rho / rhoPrev) * (alpha / omega);
-    rhoPrev = rho;
-    resnorm = sqrt(fabs(rho));
-    double *tp = pA; pA = pB; pB = tp;
-    double *tv = vA; vA = vB; vB = tv;
-  }
-  for (long i = tid0; i < N; i += nth) a.dphi[i] = a.x[i];
-  if (tid0 == 0) { *a.iters = k - 1; a.diag[0] = resnorm; a.diag[1] = normb; }
-}
-
 // SolveEquationsUsingSOR sweeps (SORMethod.for:20-60) in multicolour order:
 // forward over colours 0..C-1, backward C-1..0, each colour an independent
 // set, then CheckConvergence (CheckConvergenceRoutine.for:3) -- until
 // sum|r| <= rrF * IResiduals or itmax sweeps (SolveAlegbraicEquations.for:108-117).
-__global__ void __launch_bounds__(FS_BLOCK) k_sor(SolveArgs a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor(SolveArgs a) {
   cg::grid_group grid = cg::this_grid();
   const int N = a.N;
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
@@ -284,7 +197,7 @@ struct SorPArgs {
   double *diag;
 };
 
-__global__ void __launch_bounds__(FS_BLOCK) k_sor_colour(SorPArgs a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor_colour(SorPArgs a) {
   cg::grid_group grid = cg::this_grid();
   const int N = a.N;
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
@@ -356,12 +269,10 @@ __global__ void k_axpy_field(int N, double *fi, const double *dphi) {
 static int coop_grid_size(fs_ctx *ctx) {
   if (ctx->coop_grid > 0) return FS_OK;
   int a = 0, b = 0, c = 0;
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_bicgstab, FS_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_sor, FS_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_bicgstab3, FS_BLOCK, 0));
-  int d = 0;
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, (void *)k_sor_colour, FS_BLOCK, 0));
-  int per_sm = std::min(std::min(a, d), std::min(b, c));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_bicgstab, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_sor, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_sor_colour, FS_COOP_BLOCK, 0));
+  int per_sm = std::min(a, std::min(b, c));
   if (per_sm < 1) { ctx->err = "cooperative kernel does not fit on an SM"; return FS_E_CUDA; }
   ctx->coop_grid = ctx->num_sms * (per_sm > 4 ? 4 : per_sm);
   return FS_OK;
@@ -371,22 +282,10 @@ static int coop_launch(fs_ctx *ctx, void *fn, SolveArgs &a) {
   int rc = coop_grid_size(ctx);
   if (rc) return rc;
   int G = ctx->coop_grid;
-  long need = (ctx->N + FS_BLOCK - 1) / FS_BLOCK;
+  long need = (ctx->N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
   if (need < G) G = (int)(need < 1 ? 1 : need);
   void *args[] = {&a};
-  FS_CK(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
-  FS_LAUNCH_CHECK();
-  return FS_OK;
-}
-
-static int coop_launch3(fs_ctx *ctx, SolveArgs &a, double *pb, double *vb) {
-  int rc = coop_grid_size(ctx);
-  if (rc) return rc;
-  int G = ctx->coop_grid;
-  long need = (ctx->N + FS_BLOCK - 1) / FS_BLOCK;
-  if (need < G) G = (int)(need < 1 ? 1 : need);
-  void *args[] = {&a, &pb, &vb};
-  FS_CK(cudaLaunchCooperativeKernel((void *)k_bicgstab3, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+  FS_CK(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
   FS_LAUNCH_CHECK();
   return FS_OK;
 }
@@ -425,16 +324,16 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     sp.ac = ctx->acP; sp.anb = ctx->anbP; sp.bc = ctx->bcP; sp.x = ctx->dphiP; sp.part = ctx->red;
     sp.ires = a.ires; sp.rrf = rrf; sp.itmax = itmax; sp.ncolors = ctx->ncolors; sp.iters = a.iters; sp.diag = a.diag;
     int G = ctx->coop_grid;
-    long need = (N + FS_BLOCK - 1) / FS_BLOCK;
+    long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
     if (need < G) G = (int)(need < 1 ? 1 : need);
     void *args[] = {&sp};
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_sor_colour, dim3(G), dim3(FS_BLOCK), args, 0, ctx->st));
+    FS_CK(cudaLaunchCooperativeKernel((void *)k_sor_colour, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
     FS_LAUNCH_CHECK();
     k_from_colour<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->dphiP, ctx->dphi);
     FS_LAUNCH_CHECK();
   } else if (solver == FS_SOLVER_BICGS) {
     a.itmax = ctx->cfg.krylov_maxit;
-    rc = coop_launch3(ctx, a, ctx->ky, ctx->kz);
+    rc = coop_launch(ctx, (void *)k_bicgstab, a);
   } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS) {
     rc = fs_mg_solve(ctx, nf, rrf, solver);
   } else {
@@ -518,8 +417,8 @@ extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, con
       double *ptr = nullptr;
       if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return FS_E_CUDA;
       int per_sm = 0, per_sm2 = 0, sms = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_bicgstab, FS_BLOCK, 0) != cudaSuccess ||
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void *)k_sor, FS_BLOCK, 0) != cudaSuccess ||
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_bicgstab, FS_COOP_BLOCK, 0) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void *)k_sor, FS_COOP_BLOCK, 0) != cudaSuccess ||
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return FS_E_CUDA;
       if (per_sm2 < per_sm) per_sm = per_sm2;
@@ -543,10 +442,10 @@ extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, con
   a.ires = a.diag;
   a.tol = tol; a.itmax = maxit;
   int G = d.grid;
-  long need = ((long)n + FS_BLOCK - 1) / FS_BLOCK;
+  long need = ((long)n + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
   if (need < G) G = (int)need;
   void *args[] = {&a};
-  if (cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(G), dim3(FS_BLOCK), args, 0,
+  if (cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(G), dim3(FS_COOP_BLOCK), args, 0,
                                   (cudaStream_t)stream) != cudaSuccess)
     return FS_E_CUDA;
   return FS_OK;

@@ -1,0 +1,48 @@
+"""bench.py's multi-GPU path on CPU: world_size 2 over gloo.  Each rank runs an
+independent replica (the single-mesh path does not shard), the job time is
+the max over ranks and the rate aggregates the ranks' iterations; the
+reference arm runs on rank 0 only."""
+import os
+import socket
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    ms = [12.0, 15.0][rank]                      # rank 1 is the slow replica
+    m = bench.reduce_max(ms, dist, "cpu")
+    out[rank] = (m, bench.aggregate_rate(world, 10, m))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_aggregate_rate():
+    world = 2
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn", join=True)
+    assert out[0] == out[1]
+    m, rate = out[0]
+    assert m == 15.0
+    assert abs(rate - 2 * 10 / 0.015) < 1e-9
+
+
+def test_reference_arm_only_on_rank0(monkeypatch, capsys):
+    import argparse
+    import bench
+    args = argparse.Namespace(n=8, steps=2, warmup=1, gpus=2, impl="reference")
+    bench.run_reference(args, rank=1)
+    assert capsys.readouterr().out == ""
