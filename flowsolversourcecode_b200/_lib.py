@@ -58,6 +58,7 @@ class FsCase(C.Structure):
         ("krylov_maxit", C.c_int), ("krylov_tol", C.c_double),
         ("n_patches", C.c_int), ("patch_type", C.c_int * FS_MAX_PATCHES),
         ("patch_vel", (C.c_double * 3) * FS_MAX_PATCHES),
+        ("batched_momentum", C.c_int),
     ]
 
 

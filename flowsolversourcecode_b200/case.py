@@ -68,6 +68,8 @@ class Case:
     mg_min_parents: int = 10
     mg_max_levels: int = 10
     mg_rrf: float = 0.1
+    # multi-RHS momentum (X, Y, Z solved together; no reference counterpart)
+    batched_momentum: bool = False
     # patches: name -> (type, (u,v,w))
     patches: dict = field(default_factory=dict)
 
@@ -97,6 +99,7 @@ class Case:
         c.mg_pre, c.mg_post, c.mg_max_cycles = self.mg_pre, self.mg_post, self.mg_max_cycles
         c.mg_min_parents, c.mg_max_levels, c.mg_rrf = self.mg_min_parents, self.mg_max_levels, self.mg_rrf
         c.krylov_maxit, c.krylov_tol = self.krylov_maxit, self.krylov_tol
+        c.batched_momentum = int(self.batched_momentum)
         c.n_patches = len(mesh.patch_names)
         bct = {"wall": L.BC_WALL_NOSLIP, "slip": L.BC_WALL_SLIP, "symmetry": L.BC_SYMMETRY,
                "inlet": L.BC_INLET_VEL, "outlet": L.BC_OUTLET_FD}

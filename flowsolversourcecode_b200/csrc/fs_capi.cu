@@ -144,7 +144,8 @@ static void free_all(fs_ctx *c) {
                   c->ac, c->anb, c->bc, c->dphi, c->ac_int, c->bc_int, c->effdiv, c->pcoef,
                   c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky, c->sysx,
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
-                  c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP};
+                  c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP,
+                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P};
   for (void *p : ptrs) if (p) cudaFree(p);
 }
 
@@ -178,6 +179,10 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (auto p : cellv) if ((rc = alloc0(ctx, p, N))) return fail(rc);
   if ((rc = alloc0(ctx, &ctx->acP, N)) || (rc = alloc0(ctx, &ctx->bcP, N)) || (rc = alloc0(ctx, &ctx->dphiP, N)) ||
       (rc = alloc0(ctx, &ctx->anbP, W * N)))
+    return fail(rc);
+  if (ctx->cfg.batched_momentum &&
+      ((rc = alloc0(ctx, &ctx->ac3, 3 * N)) || (rc = alloc0(ctx, &ctx->bc3, 3 * N)) || (rc = alloc0(ctx, &ctx->ac3P, 3 * N)) ||
+       (rc = alloc0(ctx, &ctx->bc3P, 3 * N)) || (rc = alloc0(ctx, &ctx->x3P, 3 * N))))
     return fail(rc);
   double **cell3[] = {&ctx->ug, &ctx->vg, &ctx->wg, &ctx->pg, &ctx->pcg, &ctx->bc_int};
   for (auto p : cell3) if ((rc = alloc0(ctx, p, 3 * N))) return fail(rc);
@@ -305,10 +310,16 @@ int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res) {
   ctx->nIter++;
   int rc;
   cudaEventRecord(ctx->ev[0], ctx->st);
-  for (int c = 0; c < 3; c++) {
-    if ((rc = fs_momentum_assemble(ctx, c))) return rc;
-    double *fi = c == 0 ? ctx->u : c == 1 ? ctx->v : ctx->w;
-    if ((rc = fs_linear_solve(ctx, c + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom))) return rc;
+  if (ctx->cfg.batched_momentum && ctx->cfg.solver_mom == FS_SOLVER_SOR) {
+    for (int c = 0; c < 3; c++)
+      if ((rc = fs_momentum_assemble_to(ctx, c, ctx->ac3 + (size_t)c * ctx->N, ctx->bc3 + (size_t)c * ctx->N))) return rc;
+    if ((rc = fs_momentum_batched_solve(ctx))) return rc;
+  } else {
+    for (int c = 0; c < 3; c++) {
+      if ((rc = fs_momentum_assemble(ctx, c))) return rc;
+      double *fi = c == 0 ? ctx->u : c == 1 ? ctx->v : ctx->w;
+      if ((rc = fs_linear_solve(ctx, c + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom))) return rc;
+    }
   }
   cudaEventRecord(ctx->ev[1], ctx->st);
   if ((rc = fs_continuity_assemble(ctx))) return rc;

@@ -54,6 +54,8 @@ struct fs_ctx {
   // row color_rows[p]; cnP/ncfP are fixed per mesh, acP/bcP/anbP/dphiP per solve
   int32_t *cposP = nullptr, *cnP = nullptr, *ncfP = nullptr;
   double *acP = nullptr, *bcP = nullptr, *anbP = nullptr, *dphiP = nullptr;
+  // multi-RHS momentum: the three systems (3N each) in cell and colour-major order
+  double *ac3 = nullptr, *bc3 = nullptr, *ac3P = nullptr, *bc3P = nullptr, *x3P = nullptr;
 
   // geometry (device)
   double *vol = nullptr, *xc = nullptr;                     // xc: 3N
@@ -132,6 +134,8 @@ int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const 
                     const double *const *bphi, double *const *g, double *const *bg,
                     const int *method, const int *niter);
 int fs_momentum_assemble(fs_ctx *ctx, int comp);
+int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac, double *bc);
+int fs_momentum_batched_solve(fs_ctx *ctx);
 int fs_continuity_assemble(fs_ctx *ctx);
 int fs_continuity_correct(fs_ctx *ctx);
 int fs_residual_reduce(fs_ctx *ctx, int nf);   // CalculateResiduals partials -> resblk slot

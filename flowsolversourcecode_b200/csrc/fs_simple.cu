@@ -99,9 +99,11 @@ struct GradJob {
 
 // StandardGreenGauss / first pass of StandardGreenGaussFaceCorrection1
 // (StandardGreenGaussGradient.for:35-79; StandardGreenGaussCorrection1Gradient.for:47-96).
-// A cell's own values stay in registers; the other cell of each interior face
-// comes from the slot-major neighbour table cn (one coalesced index load), so
-// each slot costs one gathered value per field.
+// All NF fields of a call are done in one slot loop, so a face's geometry and
+// index are read once per cell for all fields.  A cell's own values stay in
+// registers; the other cell of each interior face comes from the slot-major
+// neighbour table cn.
+template <int NF>
 __global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B,
     const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot, const int32_t *__restrict__ cn,
     const double *__restrict__ gf, const double *__restrict__ sf,
@@ -110,35 +112,44 @@ __global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B
   if (i >= N) return;
   int nc = ncf[i];
   double V = vol[i];
-  for (int q = 0; q < J.nfld; q++) {
-    const double *__restrict__ phi = J.phi[q];
-    const double *__restrict__ bphi = J.bphi[q];
-    const double pself = phi[i];
-    double gx = 0., gy = 0., gz = 0.;
-    for (int j = 0; j < nc; j++) {
-      int s = slot[(long)j * N + i];
-      int f = s >> 1;
-      if (f < F) {
-        double g = gf[f];
-        double pk = phi[cn[(long)j * N + i]];
-        bool nbr_side = s & 1;
-        double po = nbr_side ? pk : pself, pn = nbr_side ? pself : pk;
+  double ps[NF], gx[NF], gy[NF], gz[NF];
+#pragma unroll
+  for (int q = 0; q < NF; q++) { ps[q] = J.phi[q][i]; gx[q] = 0.; gy[q] = 0.; gz[q] = 0.; }
+  for (int j = 0; j < nc; j++) {
+    int s = slot[(long)j * N + i];
+    int f = s >> 1;
+    if (f < F) {
+      int k = cn[(long)j * N + i];
+      double g = gf[f], sx = sf[f], sy = sf[F + f], sz = sf[2L * F + f];
+      bool nb = s & 1;
+#pragma unroll
+      for (int q = 0; q < NF; q++) {
+        double pk = J.phi[q][k];
+        double po = nb ? pk : ps[q], pn = nb ? ps[q] : pk;
         double fip = po * g + pn * (1. - g);
-        double fx = fip * sf[f], fy = fip * sf[F + f], fz = fip * sf[2L * F + f];
-        if (nbr_side) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
-        else { gx = gx + fx; gy = gy + fy; gz = gz + fz; }
-      } else {
-        int b = f - F;
-        double bp = bphi[b];
-        gx = gx + bp * bsf[b]; gy = gy + bp * bsf[B + b]; gz = gz + bp * bsf[2L * B + b];
+        double fx = fip * sx, fy = fip * sy, fz = fip * sz;
+        if (nb) { gx[q] = gx[q] - fx; gy[q] = gy[q] - fy; gz[q] = gz[q] - fz; }
+        else { gx[q] = gx[q] + fx; gy[q] = gy[q] + fy; gz[q] = gz[q] + fz; }
+      }
+    } else {
+      int b = f - F;
+      double bx = bsf[b], by = bsf[B + b], bz = bsf[2L * B + b];
+#pragma unroll
+      for (int q = 0; q < NF; q++) {
+        double bp = J.bphi[q][b];
+        gx[q] = gx[q] + bp * bx; gy[q] = gy[q] + bp * by; gz[q] = gz[q] + bp * bz;
       }
     }
+  }
+#pragma unroll
+  for (int q = 0; q < NF; q++) {
     double *o = J.out[q];
-    o[i] = gx / V; o[N + i] = gy / V; o[2L * N + i] = gz / V;
+    o[i] = gx[q] / V; o[N + i] = gy[q] / V; o[2L * N + i] = gz[q] / V;
   }
 }
 
 // correction pass of StandardGreenGaussFaceCorrection1 (:98-172)
+template <int NF>
 __global__ void __launch_bounds__(FS_BLOCK) k_gg_corr(GradJob J, int N, int F, int B,
     const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot, const int32_t *__restrict__ cn,
     const double *__restrict__ gf, const double *__restrict__ sf, const double *__restrict__ dfp,
@@ -147,40 +158,53 @@ __global__ void __launch_bounds__(FS_BLOCK) k_gg_corr(GradJob J, int N, int F, i
   if (i >= N) return;
   int nc = ncf[i];
   double V = vol[i];
-  for (int q = 0; q < J.nfld; q++) {
-    const double *__restrict__ phi = J.phi[q];
-    const double *__restrict__ bphi = J.bphi[q];
-    const double *__restrict__ gi = J.in[q];
-    const double ps = phi[i], gsx = gi[i], gsy = gi[N + i], gsz = gi[2L * N + i];
-    double gx = 0., gy = 0., gz = 0.;
-    for (int j = 0; j < nc; j++) {
-      int s = slot[(long)j * N + i];
-      int f = s >> 1;
-      if (f < F) {
-        int k = cn[(long)j * N + i];
-        double g = gf[f];
-        double pk = phi[k], gkx = gi[k], gky = gi[N + k], gkz = gi[2L * N + k];
-        bool nb = s & 1;
-        double po = nb ? pk : ps, pn = nb ? ps : pk;
-        double gox = nb ? gkx : gsx, gnx = nb ? gsx : gkx;
-        double goy = nb ? gky : gsy, gny = nb ? gsy : gky;
-        double goz = nb ? gkz : gsz, gnz = nb ? gsz : gkz;
-        double fip = po * g + pn * (1. - g);
-        double cx = gox * g + gnx * (1. - g); cx = cx * dfp[f];
-        double cy = goy * g + gny * (1. - g); cy = cy * dfp[F + f];
-        double cz = goz * g + gnz * (1. - g); cz = cz * dfp[2L * F + f];
+  double ps[NF], gsx[NF], gsy[NF], gsz[NF], gx[NF], gy[NF], gz[NF];
+#pragma unroll
+  for (int q = 0; q < NF; q++) {
+    ps[q] = J.phi[q][i];
+    gsx[q] = J.in[q][i]; gsy[q] = J.in[q][N + i]; gsz[q] = J.in[q][2L * N + i];
+    gx[q] = 0.; gy[q] = 0.; gz[q] = 0.;
+  }
+  for (int j = 0; j < nc; j++) {
+    int s = slot[(long)j * N + i];
+    int f = s >> 1;
+    if (f < F) {
+      int k = cn[(long)j * N + i];
+      double g = gf[f], g1 = 1. - g;
+      double sx = sf[f], sy = sf[F + f], sz = sf[2L * F + f];
+      double dx = dfp[f], dy = dfp[F + f], dz = dfp[2L * F + f];
+      bool nb = s & 1;
+#pragma unroll
+      for (int q = 0; q < NF; q++) {
+        const double *__restrict__ gi = J.in[q];
+        double pk = J.phi[q][k], gkx = gi[k], gky = gi[N + k], gkz = gi[2L * N + k];
+        double po = nb ? pk : ps[q], pn = nb ? ps[q] : pk;
+        double gox = nb ? gkx : gsx[q], gnx = nb ? gsx[q] : gkx;
+        double goy = nb ? gky : gsy[q], gny = nb ? gsy[q] : gky;
+        double goz = nb ? gkz : gsz[q], gnz = nb ? gsz[q] : gkz;
+        double fip = po * g + pn * g1;
+        double cx = gox * g + gnx * g1; cx = cx * dx;
+        double cy = goy * g + gny * g1; cy = cy * dy;
+        double cz = goz * g + gnz * g1; cz = cz * dz;
         double phif = fip + cx + cy + cz;
-        double fx = phif * sf[f], fy = phif * sf[F + f], fz = phif * sf[2L * F + f];
-        if (nb) { gx = gx - fx; gy = gy - fy; gz = gz - fz; }
-        else { gx = gx + fx; gy = gy + fy; gz = gz + fz; }
-      } else {
-        int b = f - F;
-        double bp = bphi[b];
-        gx = gx + bp * bsf[b]; gy = gy + bp * bsf[B + b]; gz = gz + bp * bsf[2L * B + b];
+        double fx = phif * sx, fy = phif * sy, fz = phif * sz;
+        if (nb) { gx[q] = gx[q] - fx; gy[q] = gy[q] - fy; gz[q] = gz[q] - fz; }
+        else { gx[q] = gx[q] + fx; gy[q] = gy[q] + fy; gz[q] = gz[q] + fz; }
+      }
+    } else {
+      int b = f - F;
+      double bx = bsf[b], by = bsf[B + b], bz = bsf[2L * B + b];
+#pragma unroll
+      for (int q = 0; q < NF; q++) {
+        double bp = J.bphi[q][b];
+        gx[q] = gx[q] + bp * bx; gy[q] = gy[q] + bp * by; gz[q] = gz[q] + bp * bz;
       }
     }
+  }
+#pragma unroll
+  for (int q = 0; q < NF; q++) {
     double *o = J.out[q];
-    o[i] = gx / V; o[N + i] = gy / V; o[2L * N + i] = gz / V;
+    o[i] = gx[q] / V; o[N + i] = gy[q] / V; o[2L * N + i] = gz[q] / V;
   }
 }
 
@@ -772,10 +796,22 @@ int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const 
       n++;
     }
     J.nfld = n;
-    if (pidx == 0)
-      k_gg0<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf, ctx->sf, ctx->bsf, ctx->vol);
-    else
-      k_gg_corr<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf, ctx->sf, ctx->dfp, ctx->bsf, ctx->vol);
+#define FS_GG_LAUNCH(NFV)                                                                                           \
+  do {                                                                                                              \
+    if (pidx == 0)                                                                                                  \
+      k_gg0<NFV><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf, ctx->sf,  \
+                                                       ctx->bsf, ctx->vol);                                         \
+    else                                                                                                            \
+      k_gg_corr<NFV><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf,       \
+                                                           ctx->sf, ctx->dfp, ctx->bsf, ctx->vol);                  \
+  } while (0)
+    switch (n) {
+    case 1: FS_GG_LAUNCH(1); break;
+    case 2: FS_GG_LAUNCH(2); break;
+    case 3: FS_GG_LAUNCH(3); break;
+    default: FS_GG_LAUNCH(4); break;
+    }
+#undef FS_GG_LAUNCH
     FS_LAUNCH_CHECK();
   }
   if (B) {
@@ -808,7 +844,10 @@ static MomArgs mom_args(fs_ctx *ctx) {
 }
 
 // SolveMomentumX/Y/Z up to (not including) SolveEquation
-int fs_momentum_assemble(fs_ctx *ctx, int comp) {
+int fs_momentum_assemble(fs_ctx *ctx, int comp) { return fs_momentum_assemble_to(ctx, comp, ctx->ac, ctx->bc); }
+
+// the same, writing the component's ac/bc to the given arrays
+int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac_out, double *bc_out) {
   const fs_case &c = ctx->cfg;
   const int N = ctx->N;
   if (comp == 0) {
@@ -826,6 +865,7 @@ int fs_momentum_assemble(fs_ctx *ctx, int comp) {
     FS_LAUNCH_CHECK();
   }
   MomArgs a = mom_args(ctx);
+  a.ac = ac_out; a.bc = bc_out;
   a.d1 = comp == 0 ? ctx->du1 : comp == 1 ? ctx->dv1 : ctx->dw1;
   a.d2 = comp == 0 ? ctx->du2 : comp == 1 ? ctx->dv2 : ctx->dw2;
   a.star = comp == 0 ? ctx->us : comp == 1 ? ctx->vs : ctx->ws;

@@ -257,6 +257,107 @@ __global__ void k_from_colour(int N, const int32_t *__restrict__ pos, const doub
   if (i < N) dphi[i] = xP[pos[i]];
 }
 
+// multi-RHS momentum: X, Y, Z systems share anb/cn; each keeps its own ac, bc
+// and convergence test (SolveAlegbraicEquations.for:108-117 per component)
+struct Sor3Args {
+  int N;
+  const int32_t *ncf, *cn, *color_ptr;
+  const double *ac3, *anb, *bc3;
+  double *x3;
+  double *part;
+  const double *ires3;   // ResorAbs of the three systems
+  double rrf;
+  int itmax, ncolors;
+  int32_t *iters3;
+};
+
+__global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor3_colour(Sor3Args a) {
+  cg::grid_group grid = cg::this_grid();
+  const int N = a.N;
+  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+  const int32_t *__restrict__ ncf = a.ncf;
+  const int32_t *__restrict__ cn = a.cn;
+  const double *__restrict__ anb = a.anb;
+  double ires[3], fres[3];
+  int iters[3];
+  for (int c = 0; c < 3; c++) { ires[c] = a.ires3[c]; fres[c] = ires[c]; iters[c] = 0; }
+  int buf = 0;
+  for (;;) {
+    bool act[3];
+    bool any = false;
+    for (int c = 0; c < 3; c++) { act[c] = fres[c] > a.rrf * ires[c] && iters[c] < a.itmax; any |= act[c]; }
+    if (!any) break;
+    for (int pass = 0; pass < 2; pass++) {
+      for (int cc = 0; cc < a.ncolors; cc++) {
+        int col = pass == 0 ? cc : a.ncolors - 1 - cc;
+        int r0 = a.color_ptr[col], r1 = a.color_ptr[col + 1];
+        for (long i = r0 + tid0; i < r1; i += nth) {
+          double l0 = a.bc3[i], l1 = a.bc3[N + i], l2 = a.bc3[2L * N + i];
+          int nc = ncf[i];
+          for (int j = 0; j < nc; j++) {
+            int k = cn[(long)j * N + i];
+            if (k >= 0) {
+              double w = anb[(long)j * N + i];
+              l0 = l0 - w * a.x3[k]; l1 = l1 - w * a.x3[N + k]; l2 = l2 - w * a.x3[2L * N + k];
+            }
+          }
+          if (act[0]) a.x3[i] = l0 / a.ac3[i];
+          if (act[1]) a.x3[N + i] = l1 / a.ac3[N + i];
+          if (act[2]) a.x3[2L * N + i] = l2 / a.ac3[2L * N + i];
+        }
+        grid.sync();
+      }
+    }
+    double s0 = 0., s1 = 0., s2 = 0.;
+    for (long i = tid0; i < N; i += nth) {
+      double r0 = a.bc3[i] - a.ac3[i] * a.x3[i];
+      double r1 = a.bc3[N + i] - a.ac3[N + i] * a.x3[N + i];
+      double r2 = a.bc3[2L * N + i] - a.ac3[2L * N + i] * a.x3[2L * N + i];
+      int nc = ncf[i];
+      for (int j = 0; j < nc; j++) {
+        int k = cn[(long)j * N + i];
+        if (k >= 0) {
+          double w = anb[(long)j * N + i];
+          r0 = r0 - w * a.x3[k]; r1 = r1 - w * a.x3[N + k]; r2 = r2 - w * a.x3[2L * N + k];
+        }
+      }
+      s0 += fabs(r0); s1 += fabs(r1); s2 += fabs(r2);
+    }
+    double o0, o1, o2, d;
+    grid_sum2(grid, a.part, buf, s0, s1, o0, o1);
+    grid_sum2(grid, a.part, buf + 1, s2, 0., o2, d);
+    buf = buf == 0 ? 2 : 0;
+    double o[3] = {o0, o1, o2};
+    for (int c = 0; c < 3; c++) if (act[c]) { fres[c] = o[c]; iters[c]++; }
+  }
+  if (tid0 == 0) for (int c = 0; c < 3; c++) a.iters3[c] = iters[c];
+}
+
+__global__ void k_to_colour3(int N, const int32_t *__restrict__ rows, const int32_t *__restrict__ ncfP,
+                             const double *__restrict__ ac3, const double *__restrict__ bc3,
+                             const double *__restrict__ anb, double *ac3P, double *bc3P, double *anbP, double *x3P) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  int i = rows[q];
+  for (int c = 0; c < 3; c++) {
+    ac3P[(long)c * N + q] = ac3[(long)c * N + i];
+    bc3P[(long)c * N + q] = bc3[(long)c * N + i];
+    x3P[(long)c * N + q] = 0.;
+  }
+  int nc = ncfP[q];
+  for (int j = 0; j < nc; j++) anbP[(long)j * N + q] = anb[(long)j * N + i];
+}
+
+__global__ void k_from_colour3(int N, const int32_t *__restrict__ pos, const double *__restrict__ x3P,
+                               double *u, double *v, double *w) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int q = pos[i];
+  u[i] = u[i] + x3P[q];
+  v[i] = v[i] + x3P[N + q];
+  w[i] = w[i] + x3P[2L * N + q];
+}
+
 __global__ void k_axpy_field(int N, double *fi, const double *dphi) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < N) fi[i] = fi[i] + dphi[i];
@@ -272,7 +373,9 @@ static int coop_grid_size(fs_ctx *ctx) {
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_bicgstab, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_sor, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_sor_colour, FS_COOP_BLOCK, 0));
-  int per_sm = std::min(a, std::min(b, c));
+  int d = 0;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, (void *)k_sor3_colour, FS_COOP_BLOCK, 0));
+  int per_sm = std::min(std::min(a, d), std::min(b, c));
   if (per_sm < 1) { ctx->err = "cooperative kernel does not fit on an SM"; return FS_E_CUDA; }
   ctx->coop_grid = ctx->num_sms * (per_sm > 4 ? 4 : per_sm);
   return FS_OK;
@@ -448,5 +551,35 @@ extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, con
   if (cudaLaunchCooperativeKernel((const void *)k_bicgstab, dim3(G), dim3(FS_COOP_BLOCK), args, 0,
                                   (cudaStream_t)stream) != cudaSuccess)
     return FS_E_CUDA;
+  return FS_OK;
+}
+
+// the three momentum solves in one cooperative launch (multi-RHS form)
+int fs_momentum_batched_solve(fs_ctx *ctx) {
+  const int N = ctx->N;
+  int rc = coop_grid_size(ctx);
+  if (rc) return rc;
+  for (int c = 0; c < 3; c++) {
+    if (ctx->s_pending[c]) { FS_CK(cudaStreamSynchronize(ctx->st)); fs_solver_stats_collect(ctx); }
+  }
+  FS_CK(cudaEventRecord(ctx->sev[0][0], ctx->st));
+  k_to_colour3<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->color_rows, ctx->ncfP, ctx->ac3, ctx->bc3, ctx->anb,
+                                                    ctx->ac3P, ctx->bc3P, ctx->anbP, ctx->x3P);
+  FS_LAUNCH_CHECK();
+  Sor3Args a{};
+  a.N = N; a.ncf = ctx->ncfP; a.cn = ctx->cnP; a.color_ptr = ctx->color_rows + N;
+  a.ac3 = ctx->ac3P; a.anb = ctx->anbP; a.bc3 = ctx->bc3P; a.x3 = ctx->x3P; a.part = ctx->red;
+  a.ires3 = ctx->resblk + RB_ABS; a.rrf = ctx->cfg.rrf_mom; a.itmax = ctx->cfg.itmax_mom; a.ncolors = ctx->ncolors;
+  a.iters3 = ctx->d_iters;
+  int G = ctx->coop_grid;
+  long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
+  if (need < G) G = (int)(need < 1 ? 1 : need);
+  void *args[] = {&a};
+  FS_CK(cudaLaunchCooperativeKernel((void *)k_sor3_colour, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
+  FS_LAUNCH_CHECK();
+  k_from_colour3<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->x3P, ctx->u, ctx->v, ctx->w);
+  FS_LAUNCH_CHECK();
+  FS_CK(cudaEventRecord(ctx->sev[0][1], ctx->st));
+  ctx->s_pending[0] = true;
   return FS_OK;
 }

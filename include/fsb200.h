@@ -143,6 +143,11 @@ typedef struct fs_case {
   int    n_patches;
   int    patch_type[FS_MAX_PATCHES];      /* fs_bc */
   double patch_vel[FS_MAX_PATCHES][3];    /* wall / inlet velocity */
+  /* multi-RHS momentum (no reference row): assemble X, Y and Z from the same
+   * velocities and solve them together (one Gauss-Seidel kernel, shared anb);
+   * the Y/Z wall cross terms then use the previous iteration's u, v.  Only
+   * with solver_mom = FS_SOLVER_SOR. */
+  int    batched_momentum;
 } fs_case;
 
 /* Mesh in polyMesh form (0-based), the input Readit parses

@@ -303,3 +303,19 @@ def test_simple_iterations_with_amg_bicgs():
     hist = [s.simple_iteration()["source"] for _ in range(30)]
     assert np.isfinite(hist).all()
     assert hist[-1] < hist[1]
+
+
+def test_batched_momentum_same_fixed_point():
+    # X, Y, Z solved together: the per-iteration wall cross terms lag, the
+    # converged field is the same
+    from flowsolversourcecode_b200.solver import Solver
+    mesh, case = cs.cavity(12, nz=10, re=100.0, nstop_type=3)
+    _, case_b = cs.cavity(12, nz=10, re=100.0, nstop_type=3, batched_momentum=True)
+    a, b = Solver(mesh, case), Solver(mesh, case_b)
+    for _ in range(400):
+        ra = a.simple_iteration()
+        rb = b.simple_iteration()
+    assert ra["source"] < 1e-11 and rb["source"] < 1e-11
+    for k in ("u", "v", "w"):
+        x, y = a.get(k), b.get(k)
+        assert np.linalg.norm(x - y) <= 1e-8 * np.linalg.norm(x), k
