@@ -144,3 +144,82 @@ int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);
 int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);
 int fs_solver_stats_collect(fs_ctx *ctx);   // after a stream sync: fold pending solver events
+
+#ifdef __CUDACC__
+// Row i of a slot-major ELL table (n rows, width w; unused slots hold index -1):
+// acc (+ or -) coef_ij * x(k_ij) over the valid slots in ascending slot order,
+// i.e. the summation order of the sequential slot loop, so results are
+// bit-identical to it.  U slots per round: the index and coefficient loads of
+// a round are issued before its gathers, so a row costs about two memory
+// latencies per round rather than two per slot.
+template <int U, bool SUB, class T, class XF>
+__device__ __forceinline__ T ell_acc(T acc, long n, int w, const int32_t *__restrict__ idx,
+                                     const T *__restrict__ coef, long i, XF &&xv) {
+  for (int j0 = 0; j0 < w; j0 += U) {
+    int k[U];
+    T a[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int j = j0 + u;
+      k[u] = j < w ? idx[(long)j * n + i] : -1;
+      a[u] = j < w ? coef[(long)j * n + i] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (k[u] >= 0) acc = SUB ? acc - a[u] * xv(k[u]) : acc + a[u] * xv(k[u]);
+  }
+  return acc;
+}
+
+// the slots j = q, q+G, ... of row i (lane q of a G-lane group); a partial sum
+template <int G, int U, class T, class XF>
+__device__ __forceinline__ T ell_part(long n, int w, const int32_t *__restrict__ idx, const T *__restrict__ coef,
+                                      long i, int q, XF &&xv) {
+  T acc = (T)0;
+  for (int j0 = q; j0 < w; j0 += U * G) {
+    int k[U];
+    T a[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int j = j0 + u * G;
+      k[u] = j < w ? idx[(long)j * n + i] : -1;
+      a[u] = j < w ? coef[(long)j * n + i] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (k[u] >= 0) acc = acc + a[u] * xv(k[u]);
+  }
+  return acc;
+}
+#endif
+
+#ifdef __CUDACC__
+// Rows i and i2 (i2 = i + stride, valid when h2) of the ELL product at once:
+// the index and coefficient loads of both rows are issued before their
+// gathers.  Inside the persistent cooperative kernels a grid-stride loop of
+// one row per step runs well below the bandwidth a plain launch reaches; two
+// independent rows per step restore the memory-level parallelism.  Per-row
+// summation order is that of ell_acc.
+template <int U, bool SUB, class T, class XF>
+__device__ __forceinline__ void ell_acc2(T &acc1, T &acc2, long n, int w, const int32_t *__restrict__ idx,
+                                         const T *__restrict__ coef, long i, long i2, bool h2, XF &&xv) {
+  for (int j0 = 0; j0 < w; j0 += U) {
+    int k1[U], k2[U];
+    T a1[U], a2[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int j = j0 + u;
+      const bool in = j < w, in2 = in && h2;
+      k1[u] = in ? idx[(long)j * n + i] : -1;
+      a1[u] = in ? coef[(long)j * n + i] : (T)0;
+      k2[u] = in2 ? idx[(long)j * n + i2] : -1;
+      a2[u] = in2 ? coef[(long)j * n + i2] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (k1[u] >= 0) acc1 = SUB ? acc1 - a1[u] * xv(k1[u]) : acc1 + a1[u] * xv(k1[u]);
+      if (k2[u] >= 0) acc2 = SUB ? acc2 - a2[u] * xv(k2[u]) : acc2 + a2[u] * xv(k2[u]);
+    }
+  }
+}
+#endif

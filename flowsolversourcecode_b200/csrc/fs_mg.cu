@@ -15,7 +15,9 @@
 // Cycles run inside ONE persistent cooperative kernel.  Levels with more than
 // FS_MG_SMALL rows are processed by the whole grid (grid barriers between
 // colours of the Gauss-Seidel sweeps); smaller levels by CTA 0 alone with
-// block barriers, so the coarse tail of a cycle costs no grid barriers.
+// block barriers, so the coarse tail of a cycle costs no grid barriers.  A
+// phase of a latency-bound sweep costs about one dependent-load chain per row a
+// thread handles, so CTA 0 wins below ~8 rows per thread (2048 rows).
 //   k_mg_solve      : AlgebraicMultigrid (AlgebraicMultiGridMainRoutine.for:330-345)
 //                     with V/F/W cycles (MultiGridCycle.for), smoothing sweeps
 //                     that stop on sum|r| <= rrF*IResiduals (SolveEquationsWithMultiGrid.for),
@@ -23,24 +25,40 @@
 //                     sequential sweep, coarse corrections kept between cycles
 //                     as the reference does.
 //   k_amg_bicgstab  : FP64 BiCGSTAB right-preconditioned by one V-cycle
-//                     (zero coarse guesses, fixed sweeps) -- no reference row;
-//                     templated on the V-cycle precision (double, or float with
-//                     FP32 copies of every level's matrix: iterative refinement).
+//                     (PCycle: damped Jacobi, fused restrict/prolong phases,
+//                     dense FP64 inverse of the coarsest level) -- no reference
+//                     row; templated on the V-cycle precision (double, or float
+//                     with FP32 copies of every level's matrix: iterative
+//                     refinement).
 #include "fs_internal.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
+#include <type_traits>
 
 namespace cg = cooperative_groups;
 
-#define FS_MG_SMALL 8192
+#define FS_MG_SMALL 2048
+#define FS_MG_DIRECT 160   // largest coarsest level inverted densely (n^2 doubles in shared memory)
 #define FS_MG_MAXLEV 16
+// preconditioner V-cycle: Jacobi weight and coarse-correction factor
+// (over-correction compensates the energy of piecewise-constant prolongation)
+#ifndef FS_MG_OMEGA
+#define FS_MG_OMEGA 0.8
+#endif
+// CTAs per SM the preconditioned Krylov kernel is compiled for (register cap)
+#ifndef FS_AMG_MINB
+#define FS_AMG_MINB 4
+#endif
+#ifndef FS_MG_ALPHA
+#define FS_MG_ALPHA 1.8
+#endif
 
 template <class R>
 struct LevelDev {
   int n, w, ncolors;
   const int32_t *ncf, *nbr, *color_ptr, *color_rows;
   const R *ac, *anb;
-  R *b, *x, *r;
+  R *b, *x, *r, *t;
   const int32_t *parent;        // this level -> next coarser (nullptr on the coarsest)
   const int32_t *rptr, *rlist;  // restriction into this level: finer rows per coarse row, ascending
 };
@@ -55,7 +73,12 @@ struct fs_mg_dev {
   int32_t *rptr[FS_MG_MAXLEV] = {}, *rlist[FS_MG_MAXLEV] = {};
   int32_t *colors[FS_MG_MAXLEV] = {};   // rows by colour, then ncol+1 offsets
   double *ac[FS_MG_MAXLEV] = {}, *anb[FS_MG_MAXLEV] = {}, *b[FS_MG_MAXLEV] = {}, *x[FS_MG_MAXLEV] = {}, *r[FS_MG_MAXLEV] = {};
+  double *t[FS_MG_MAXLEV] = {};
   float *acf[FS_MG_MAXLEV] = {}, *anbf[FS_MG_MAXLEV] = {}, *bf[FS_MG_MAXLEV] = {}, *xf[FS_MG_MAXLEV] = {}, *rf[FS_MG_MAXLEV] = {};
+  float *tf[FS_MG_MAXLEV] = {};
+  int lc = 0;                           // coarsest level of the preconditioner
+  bool direct = false;                  // lev[lc] inverted densely
+  double *sinv = nullptr;
   LevelDev<double> *lev64 = nullptr;
   LevelDev<float> *lev32 = nullptr;
   double *red = nullptr;                // partial sums
@@ -130,7 +153,7 @@ __device__ double scope_sum(Sync &S, const Scope &sc, double v) {
 
 // one symmetric multicolour Gauss-Seidel sweep (SORMultiGrid.for:20-66)
 template <class R>
-__device__ void gs_sweep(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, R *x) {
+__device__ void gs_sweep(Sync &S, const Scope &sc, const LevelDev<R> L, const R *b, R *x) {
   const int n = L.n;
   for (int pass = 0; pass < 2; pass++)
     for (int cc = 0; cc < L.ncolors; cc++) {
@@ -138,12 +161,7 @@ __device__ void gs_sweep(Sync &S, const Scope &sc, const LevelDev<R> &L, const R
       int r0 = L.color_ptr[c], r1 = L.color_ptr[c + 1];
       for (long q = r0 + sc.tid0(); q < r1; q += sc.nth()) {
         int i = L.color_rows[q];
-        R l = b[i];
-        int nc = L.ncf[i];
-        for (int j = 0; j < nc; j++) {
-          int k = L.nbr[(long)j * n + i];
-          if (k >= 0) l = l - L.anb[(long)j * n + i] * x[k];
-        }
+        R l = ell_acc<8, true>(b[i], n, L.w, L.nbr, L.anb, i, [&](int k) { return x[k]; });
         x[i] = l / L.ac[i];
       }
       scope_sync(S, sc);
@@ -152,62 +170,19 @@ __device__ void gs_sweep(Sync &S, const Scope &sc, const LevelDev<R> &L, const R
 
 // r = b - A x on a level; returns sum |r| (CalculateResidualsMG + CheckConvergenceMG)
 template <class R>
-__device__ double residual(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, const R *x, R *r) {
+__device__ double residual(Sync &S, const Scope &sc, const LevelDev<R> L, const R *b, const R *x, R *r) {
   const int n = L.n;
   double s = 0.;
   for (long i = sc.tid0(); i < n; i += sc.nth()) {
-    R t = b[i] - L.ac[i] * x[i];
-    int nc = L.ncf[i];
-    for (int j = 0; j < nc; j++) {
-      int k = L.nbr[(long)j * n + i];
-      if (k >= 0) t = t - L.anb[(long)j * n + i] * x[k];
-    }
+    R t = ell_acc<8, true>(b[i] - L.ac[i] * x[i], n, L.w, L.nbr, L.anb, i, [&](int k) { return x[k]; });
     r[i] = t;
     s += fabs((double)t);
   }
   return scope_sum(S, sc, s);
 }
 
-// damped Jacobi (omega = 2/3 on the diagonal ac): the preconditioner's smoother on
-// coarse levels that the whole grid processes -- 2 grid barriers per sweep instead
-// of 2 per colour (agglomerated levels need ~10 colours)
-template <class R>
-__device__ void jacobi(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, R *x, R *r, int sweeps) {
-  const int n = L.n;
-  const R omega = (R)(2.0 / 3.0);
-  for (int it = 0; it < sweeps; it++) {
-    for (long i = sc.tid0(); i < n; i += sc.nth()) {
-      R t = b[i] - L.ac[i] * x[i];
-      int nc = L.ncf[i];
-      for (int j = 0; j < nc; j++) {
-        int k = L.nbr[(long)j * n + i];
-        if (k >= 0) t = t - L.anb[(long)j * n + i] * x[k];
-      }
-      r[i] = t;
-    }
-    scope_sync(S, sc);
-    for (long i = sc.tid0(); i < n; i += sc.nth()) x[i] = x[i] + omega * r[i] / L.ac[i];
-    scope_sync(S, sc);
-  }
-}
-
-// r = b - A x without the norm (the preconditioner needs no convergence test)
-template <class R>
-__device__ void residual_only(const Scope &sc, const LevelDev<R> &L, const R *b, const R *x, R *r) {
-  const int n = L.n;
-  for (long i = sc.tid0(); i < n; i += sc.nth()) {
-    R t = b[i] - L.ac[i] * x[i];
-    int nc = L.ncf[i];
-    for (int j = 0; j < nc; j++) {
-      int k = L.nbr[(long)j * n + i];
-      if (k >= 0) t = t - L.anb[(long)j * n + i] * x[k];
-    }
-    r[i] = t;
-  }
-}
-
 // SolveEquationMG: sweeps until sum|r| <= rrF*IRes or itmax (checked=true), or
-// exactly itmax sweeps (checked=false, preconditioner)
+// exactly itmax sweeps (checked=false)
 template <class R>
 __device__ void smooth(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, R *x, R *r,
                        double rrf, double ires, int itmax, bool checked) {
@@ -249,8 +224,6 @@ struct Cycle {
   int pre, post;
   bool checked;
   bool last_grid;   // scope of the previous operation
-  bool prec;        // preconditioner: Jacobi on grid-wide coarse levels, no norms
-  int coarse_sweeps;
   __device__ const R *B(int l) const { return l == 0 ? b0 : lev[l].b; }
   __device__ R *X(int l) const { return l == 0 ? x0 : lev[l].x; }
   __device__ R *Rr(int l) const { return l == 0 ? r0 : lev[l].r; }
@@ -263,14 +236,12 @@ struct Cycle {
   __device__ void op_smooth(int l, int itmax) {
     Scope sc = scope_of(lev[l]);
     enter(sc);
-    if (prec && l > 0 && sc.grid) jacobi(S, sc, lev[l], B(l), X(l), Rr(l), itmax);
-    else if (sc.active()) smooth(S, sc, lev[l], B(l), X(l), Rr(l), rrf, ires, itmax, checked);
+    if (sc.active()) smooth(S, sc, lev[l], B(l), X(l), Rr(l), rrf, ires, itmax, checked);
   }
   __device__ void op_residual(int l) {
     Scope sc = scope_of(lev[l]);
     enter(sc);
-    if (prec) { if (sc.active()) residual_only(sc, lev[l], B(l), X(l), Rr(l)); }
-    else if (sc.active()) residual(S, sc, lev[l], B(l), X(l), Rr(l));
+    if (sc.active()) residual(S, sc, lev[l], B(l), X(l), Rr(l));
   }
   __device__ void op_restrict(int l) {   // Restrict(l): smooth, residual, coarse rhs
     op_smooth(l, pre);
@@ -291,8 +262,8 @@ struct Cycle {
   __device__ void run(int type) {
     int L = nlev - 1;
     for (int l = 0; l < L; l++) op_restrict(l);
-    op_smooth(L, prec ? coarse_sweeps : post);
-    if (!prec) op_residual(L);
+    op_smooth(L, post);
+    op_residual(L);
     if (type != 0) {
       for (int l1 = L - 1; l1 >= 1; l1--) {
         for (int l = L; l >= l1 + 1; l--) op_prolong(l);
@@ -334,7 +305,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
   }
   S.all();
   double ires = *a.ires, fres = ires;
-  Cycle<double> C{S, a.lev, a.nlev, a.b0, a.x0, a.r0, a.rrf, ires, a.pre, a.post, true, true, false, 0};
+  Cycle<double> C{S, a.lev, a.nlev, a.b0, a.x0, a.r0, a.rrf, ires, a.pre, a.post, true, true};
   int ncycle = 1;
   while (ncycle <= a.maxcycles && fres > a.rrf * ires) {
     C.last_grid = true;
@@ -346,62 +317,254 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.iters = ncycle - 1;
 }
 
-// one V-cycle as a preconditioner: x0 = M^-1 b0, zero guesses on every level
+// One V-cycle with zero initial guesses as the preconditioner M^-1 of the Krylov
+// solver.  Damped Jacobi (omega) on every level, so each sweep is one phase of
+// independent rows; the first pre-sweep from zero is fused into the restriction
+// that makes the level's rhs, and the coarsest level is solved by a dense FP64
+// inverse (k_mg_dense_inverse).  The coarse correction is over-weighted,
+// x += alpha*x_c[parent] with alpha > 1, which compensates the energy of
+// piecewise-constant prolongation.  On levels with a thread per row the
+// prolongation is a phase of its own before the first post-sweep; on levels
+// with G lanes per row it is formed on the fly inside the sweep for the row and
+// its neighbours.  A cycle over levels 0..lc costs 3*lc+2 barrier phases plus one
+// per thread-per-row level.  Level-0 rhs and result are FP64 in either
+// precision; up-leg results go to each level's r.
+//
+// Rows with fewer than two threads each are handled a thread per row, two rows
+// per step (ell_acc2).  Coarse rows have 10-30 neighbours and coarse levels
+// fewer rows than the grid has threads, so there a row is handled by G
+// consecutive lanes (G = 2..8 from the threads per row) that split its
+// neighbour loop and combine by shuffles.  Levels up to FS_PC_SMALL rows run on
+// CTA 0 alone.
+#define FS_PC_SMALL 256
+
 template <class R>
-__device__ void vcycle_prec(Sync &S, const LevelDev<R> *lev, int nlev, const R *b0, R *x0, R *r0, int pre, int post) {
-  Scope g; g.grid = true;
-  for (int l = 0; l < nlev; l++) {
-    R *x = l == 0 ? x0 : lev[l].x;
-    for (long i = g.tid0(); i < lev[l].n; i += g.nth()) x[i] = 0.;
+__device__ __forceinline__ Scope pc_scope(const LevelDev<R> &L) { Scope s; s.grid = L.n > FS_PC_SMALL; return s; }
+
+template <int G, class T>
+__device__ __forceinline__ T gsum(T v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// rows [0,n) by groups of G consecutive lanes; the trip count is uniform per
+// warp, so every lane reaches the group shuffles (f must not return early)
+template <int G, class F>
+__device__ __forceinline__ void group_rows(const Scope &sc, int n, F &f) {
+  constexpr int GPW = 32 / G;
+  const long w0 = sc.tid0() >> 5, nw = sc.nth() >> 5;
+  const int lane = threadIdx.x & 31, grp = lane / G, q = lane % G;
+  for (long wb = w0 * GPW; wb < n; wb += nw * GPW) {
+    long i = wb + grp;
+    f(std::integral_constant<int, G>{}, i, i < n, q);
   }
-  Cycle<R> C{S, lev, nlev, b0, x0, r0, 0., 0., pre, post, false, true, true, 20};
-  C.run(0);
+}
+
+// G from the threads per row (callers handle fewer than 2 threads per row)
+template <class F>
+__device__ __forceinline__ void level_rows(const Scope &sc, int n, int level, F &&f) {
+  const long per = sc.nth() / (n > 0 ? n : 1);
+  (void)level;
+  if (per < 4) group_rows<2>(sc, n, f);
+  else if (per < 8) group_rows<4>(sc, n, f);
+  else group_rows<8>(sc, n, f);
 }
 
 template <class R>
+struct PCycle {
+  Sync &S;
+  const LevelDev<R> *lev;
+  int lc;              // coarsest level used by the preconditioner
+  bool direct;         // coarsest by the dense inverse, else coarse_sweeps sweeps
+  const double *sinv;  // lev[lc].n^2, row-major
+  int pre, post, coarse_sweeps;
+  R omega, alpha;
+  bool last_grid;
+  __device__ void enter(const Scope &sc) {
+    if (sc.grid || last_grid) S.all(); else __syncthreads();
+    last_grid = sc.grid;
+  }
+  // r (into dst) = b - A x on level l; level 0 takes b from `in`
+  __device__ void residual(int l, const double *__restrict__ in, const R *__restrict__ x, R *__restrict__ dst) {
+    const LevelDev<R> L = lev[l];
+    Scope sc = pc_scope(L);
+    enter(sc);
+    if (!sc.active()) return;
+    if (l == 0 || sc.nth() < 2L * L.n) {   // a thread per row, two rows per step
+      const long t0 = sc.tid0(), nt = sc.nth();
+      for (long i = t0; i < L.n; i += 2 * nt) {
+        const long i2 = i + nt;
+        const bool h2 = i2 < L.n;
+        R t1 = 0., t2 = 0.;
+        ell_acc2<6, false>(t1, t2, L.n, L.w, L.nbr, L.anb, i, i2, h2, [&](int k) { return x[k]; });
+        dst[i] = (l == 0 ? (R)in[i] : L.b[i]) - L.ac[i] * x[i] - t1;
+        if (h2) dst[i2] = (l == 0 ? (R)in[i2] : L.b[i2]) - L.ac[i2] * x[i2] - t2;
+      }
+      return;
+    }
+    level_rows(sc, L.n, l, [&](auto g, long i, bool act, int q) {
+      constexpr int G = decltype(g)::value;
+      R t = 0.;
+      if (act) t = ell_part<G, G == 1 ? 8 : 4>(L.n, L.w, L.nbr, L.anb, i, q, [&](int k) { return x[k]; });
+      t = gsum<G>(t);
+      if (act && q == 0) dst[i] = (l == 0 ? (R)in[i] : L.b[i]) - L.ac[i] * x[i] - t;
+    });
+  }
+  // further Jacobi sweeps in place: residual into t, then the update
+  __device__ void sweeps(int l, const double *in, R *x, int n) {
+    const LevelDev<R> L = lev[l];
+    Scope sc = pc_scope(L);
+    for (int s = 0; s < n; s++) {
+      residual(l, in, x, L.t);
+      enter(sc);
+      if (sc.active()) for (long i = sc.tid0(); i < L.n; i += sc.nth()) x[i] = x[i] + omega * L.t[i] / L.ac[i];
+    }
+  }
+  // out = M^-1 in.  Callers have made `in` visible grid-wide.
+  __device__ void run(const double *__restrict__ in, double *__restrict__ out) {
+    Scope g; g.grid = true;
+    {
+      const LevelDev<R> L0 = lev[0];
+      for (long i = g.tid0(); i < L0.n; i += g.nth()) L0.x[i] = omega * (R)in[i] / L0.ac[i];
+    }
+    last_grid = true;
+    sweeps(0, in, lev[0].x, pre - 1);
+    for (int l = 0; l < lc; l++) {
+      const LevelDev<R> L = lev[l], C = lev[l + 1];
+      residual(l, in, L.x, L.r);
+      Scope scc = pc_scope(C);
+      enter(scc);
+      const bool first_sweep = l + 1 < lc || !direct;
+      if (scc.active() && scc.nth() < 2L * C.n) {   // a thread per coarse row
+        for (long P = scc.tid0(); P < C.n; P += scc.nth()) {
+          R s = 0.;
+          const int c0 = C.rptr[P], c1 = C.rptr[P + 1];
+          for (int c = c0; c < c1; c++) s = s + L.r[C.rlist[c]];
+          C.b[P] = s;
+          if (first_sweep) C.x[P] = omega * s / C.ac[P];
+        }
+      } else if (scc.active())
+        level_rows(scc, C.n, l + 1, [&](auto gg, long P, bool act, int q) {
+          constexpr int G = decltype(gg)::value;
+          R s = 0.;
+          if (act)
+            for (int c = C.rptr[P] + q; c < C.rptr[P + 1]; c += G) s = s + L.r[C.rlist[c]];
+          s = gsum<G>(s);
+          if (act && q == 0) {
+            C.b[P] = s;
+            if (first_sweep) C.x[P] = omega * s / C.ac[P];
+          }
+        });
+      if (l + 1 < lc) sweeps(l + 1, in, C.x, pre - 1);
+    }
+    const LevelDev<R> Cc = lev[lc];
+    if (direct) {
+      Scope c0; c0.grid = false;
+      enter(c0);
+      if (blockIdx.x == 0) {
+        const int n = Cc.n, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        for (int i = threadIdx.x >> 5; i < n; i += nw) {
+          double t = 0.;
+          for (int j = lane; j < n; j += 32) t += sinv[(long)i * n + j] * (double)Cc.b[j];
+          t = wsum(t);
+          if (lane == 0) Cc.r[i] = (R)t;
+        }
+      }
+    } else {
+      sweeps(lc, in, Cc.x, coarse_sweeps - 1);
+      Scope sc = pc_scope(Cc);
+      enter(sc);
+      if (sc.active()) for (long i = sc.tid0(); i < Cc.n; i += sc.nth()) Cc.r[i] = Cc.x[i];
+    }
+    for (int l = lc - 1; l >= 0; l--) {
+      const LevelDev<R> L = lev[l];
+      const R *__restrict__ xc = lev[l + 1].r;
+      Scope sl = pc_scope(L);
+      const bool to_out = l == 0 && post == 1;
+      enter(sl);
+      if (sl.active() && (l == 0 || sl.nth() < 2L * L.n)) {
+        // a thread per row: prolong in place (x += alpha x_c[parent], each row
+        // its own), then the smoothing sweep gathers x directly -- two memory
+        // latencies per slot round instead of three
+        const long t0 = sl.tid0(), nt = sl.nth();
+        for (long i = t0; i < L.n; i += nt) L.x[i] = L.x[i] + alpha * xc[L.parent[i]];
+        enter(sl);
+        for (long i = t0; i < L.n; i += 2 * nt) {
+          const long i2 = i + nt;
+          const bool h2 = i2 < L.n;
+          R t1 = 0., t2 = 0.;
+          ell_acc2<6, false>(t1, t2, L.n, L.w, L.nbr, L.anb, i, i2, h2, [&](int k) { return L.x[k]; });
+          R xi = L.x[i], bi = l == 0 ? (R)in[i] : L.b[i];
+          R xn = xi + omega * (bi - L.ac[i] * xi - t1) / L.ac[i];
+          if (to_out) out[i] = (double)xn; else L.r[i] = xn;
+          if (h2) {
+            R xj = L.x[i2], bj = l == 0 ? (R)in[i2] : L.b[i2];
+            R xm = xj + omega * (bj - L.ac[i2] * xj - t2) / L.ac[i2];
+            if (to_out) out[i2] = (double)xm; else L.r[i2] = xm;
+          }
+        }
+      } else if (sl.active())
+        level_rows(sl, L.n, l, [&](auto gg, long i, bool act, int q) {
+          constexpr int G = decltype(gg)::value;
+          R t = 0.;
+          if (act)
+            t = ell_part<G, G == 1 ? 8 : 4>(L.n, L.w, L.nbr, L.anb, i, q,
+                                            [&](int k) { return L.x[k] + alpha * xc[L.parent[k]]; });
+          t = gsum<G>(t);
+          if (act && q == 0) {
+            R xi = L.x[i] + alpha * xc[L.parent[i]];
+            R bi = l == 0 ? (R)in[i] : L.b[i];
+            R xn = xi + omega * (bi - L.ac[i] * xi - t) / L.ac[i];
+            if (to_out) out[i] = (double)xn; else L.r[i] = xn;
+          }
+        });
+      if (!to_out) sweeps(l, in, L.r, post - 1);
+    }
+    if (post > 1) {
+      enter(g);
+      const LevelDev<R> L0 = lev[0];
+      for (long i = g.tid0(); i < L0.n; i += g.nth()) out[i] = (double)L0.r[i];
+    }
+    enter(g);
+  }
+};
+
+template <class R>
 struct AmgKArgs {
-  int N;
+  int N, W;
   const int32_t *ncf, *cn;
   const double *ac, *anb, *bc;
   double *x, *r, *r0, *p, *v, *s, *t, *y, *z, *dphi;
-  R *b32, *x32, *r32;                 // level-0 vectors in the V-cycle precision
   const LevelDev<R> *lev;
-  int nlev, pre, post, maxit;
+  int lc, direct, pre, post, maxit;
+  const double *sinv;
   double tol;
   double *part;
   int32_t *iters;
   double *diag;
 };
 
-__device__ __forceinline__ double row_ax(int N, const int32_t *ncf, const int32_t *cn, const double *ac,
-                                         const double *anb, int i, const double *x) {
-  double t = 0.0;
-  t = t + ac[i] * x[i];
-  int nc = ncf[i];
-  for (int j = 0; j < nc; j++) {
-    int k = cn[(long)j * N + i];
-    if (k >= 0) t = t + anb[(long)j * N + i] * x[k];
-  }
-  return t;
+// rows i and i2 (when h2) of A x at once (ell_acc2)
+template <class A>
+__device__ __forceinline__ void row_ax2(const A &a, long i, long i2, bool h2, const double *x, double &t1, double &t2) {
+  t1 = 0.0;
+  t1 = t1 + a.ac[i] * x[i];
+  t2 = 0.0;
+  if (h2) t2 = t2 + a.ac[i2] * x[i2];
+  ell_acc2<6, false>(t1, t2, a.N, a.W, a.cn, a.anb, i, i2, h2, [&](int k) { return x[k]; });
 }
 
 // apply the preconditioner: out (FP64) = M^-1 in (FP64), via the R-precision V-cycle
 template <class R>
 __device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, double *out) {
-  Scope g; g.grid = true;
-  if (sizeof(R) == sizeof(double)) {
-    vcycle_prec<R>(S, a.lev, a.nlev, (const R *)in, (R *)out, a.r32, a.pre, a.post);
-  } else {
-    for (long i = g.tid0(); i < a.N; i += g.nth()) a.b32[i] = (R)in[i];
-    vcycle_prec<R>(S, a.lev, a.nlev, a.b32, a.x32, a.r32, a.pre, a.post);
-    for (long i = g.tid0(); i < a.N; i += g.nth()) out[i] = (double)a.x32[i];
-    S.all();
-  }
+  PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, true};
+  C.run(in, out);
 }
 
 // right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle
 template <class R>
-__global__ void __launch_bounds__(FS_COOP_BLOCK) k_amg_bicgstab(AmgKArgs<R> a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(AmgKArgs<R> a) {
   Sync S(a.part);
   const int N = a.N;
   Scope g; g.grid = true;
@@ -430,7 +593,14 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_amg_bicgstab(AmgKArgs<R> a) {
     S.all();
     apply_prec<R>(S, a, a.p, a.y);                                  // y = M^-1 p
     l0 = 0.;
-    for (long i = t0; i < N; i += nt) { double vi = row_ax(N, a.ncf, a.cn, a.ac, a.anb, (int)i, a.y); a.v[i] = vi; l0 += a.r0[i] * vi; }
+    for (long i = t0; i < N; i += 2 * nt) {
+      const long i2 = i + nt;
+      const bool h2 = i2 < N;
+      double v1, v2;
+      row_ax2(a, i, i2, h2, a.y, v1, v2);
+      a.v[i] = v1; l0 += a.r0[i] * v1;
+      if (h2) { a.v[i2] = v2; l0 += a.r0[i2] * v2; }
+    }
     double rv;
     S.sum2(l0, 0., rv, dum);
     alpha = rho / rv;
@@ -445,7 +615,14 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_amg_bicgstab(AmgKArgs<R> a) {
     }
     apply_prec<R>(S, a, a.s, a.z);                                  // z = M^-1 s
     l0 = 0.; l1 = 0.;
-    for (long i = t0; i < N; i += nt) { double ti = row_ax(N, a.ncf, a.cn, a.ac, a.anb, (int)i, a.z); a.t[i] = ti; l0 += ti * a.s[i]; l1 += ti * ti; }
+    for (long i = t0; i < N; i += 2 * nt) {
+      const long i2 = i + nt;
+      const bool h2 = i2 < N;
+      double t1, t2;
+      row_ax2(a, i, i2, h2, a.z, t1, t2);
+      a.t[i] = t1; l0 += t1 * a.s[i]; l1 += t1 * t1;
+      if (h2) { a.t[i2] = t2; l0 += t2 * a.s[i2]; l1 += t2 * t2; }
+    }
     double ts, tt;
     S.sum2(l0, l1, ts, tt);
     omega = ts / tt;
@@ -490,6 +667,57 @@ __global__ void k_mg_lhs(int nf, const int32_t *ncf_f, const double *ac_f, const
 __global__ void k_to_f32(long n, const double *a, float *b) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = (float)a[i];
+}
+
+// Dense inverse of the coarsest level (one CTA, matrix in shared memory):
+// in-place Gauss-Jordan without pivoting, two block barriers per pivot.  The
+// agglomerated matrices are diagonally dominant.  A pure-Neumann level (every
+// row sum ~0: the pressure correction with walls only) is singular with the
+// constant null space; its last equation is replaced by x_{n-1} = 0 and the last
+// column of the inverse is zeroed, so sinv*b solves the remaining equations --
+// the consistent systems the V-cycle restricts.  A zero pivot drops its unknown.
+__global__ void __launch_bounds__(1024) k_mg_dense_inverse(int n, const int32_t *ncf, const int32_t *nbr,
+                                                           const double *ac, const double *anb, double *sinv) {
+  extern __shared__ double sm[];
+  double *A = sm, *col = sm + (long)n * n;
+  __shared__ int singular;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int q = tid; q < n * n; q += nt) A[q] = 0.;
+  if (tid == 0) singular = 1;
+  __syncthreads();
+  for (int i = tid; i < n; i += nt) {
+    double d = ac[i], rs = d;
+    A[(long)i * n + i] = d;
+    for (int j = 0; j < ncf[i]; j++) {
+      int k = nbr[(long)j * n + i];
+      if (k >= 0) { double a = anb[(long)j * n + i]; A[(long)i * n + k] += a; rs += a; }
+    }
+    if (fabs(rs) > 1e-9 * fabs(d)) singular = 0;
+  }
+  __syncthreads();
+  const bool sing = singular != 0;
+  if (sing)
+    for (int j = tid; j < n; j += nt) A[(long)(n - 1) * n + j] = j == n - 1 ? 1. : 0.;
+  __syncthreads();
+  for (int k = 0; k < n; k++) {
+    const double d = A[(long)k * n + k];
+    const double p = d != 0. ? 1. / d : 0.;
+    __syncthreads();
+    for (int i = tid; i < n; i += nt)
+      if (i != k) col[i] = A[(long)i * n + k];
+    for (int j = tid; j < n; j += nt) A[(long)k * n + j] = j == k ? p : A[(long)k * n + j] * p;
+    __syncthreads();
+    for (int q = tid; q < n * n; q += nt) {
+      int i = q / n, j = q - i * n;
+      if (i == k) continue;
+      A[q] = j == k ? -col[i] * p : A[q] - col[i] * A[(long)k * n + j];
+    }
+    __syncthreads();
+  }
+  if (sing)
+    for (int i = tid; i < n; i += nt) A[(long)i * n + n - 1] = 0.;
+  __syncthreads();
+  for (int q = tid; q < n * n; q += nt) sinv[q] = A[q];
 }
 
 }  // namespace
@@ -678,6 +906,8 @@ int fs_mg_build(fs_ctx *ctx) {
     FS_CK(cudaMalloc(&M->b[q], sizeof(double) * n));
     FS_CK(cudaMalloc(&M->x[q], sizeof(double) * n));
     FS_CK(cudaMalloc(&M->r[q], sizeof(double) * n));
+    FS_CK(cudaMalloc(&M->t[q], sizeof(double) * n));
+    FS_CK(cudaMalloc(&M->tf[q], sizeof(float) * n));
     FS_CK(cudaMalloc(&M->acf[q], sizeof(float) * n));
     FS_CK(cudaMalloc(&M->anbf[q], sizeof(float) * nw));
     FS_CK(cudaMalloc(&M->bf[q], sizeof(float) * n));
@@ -689,13 +919,14 @@ int fs_mg_build(fs_ctx *ctx) {
     LevelDev<double> d{};
     d.n = M->n[q]; d.w = M->w[q]; d.ncolors = M->ncol[q];
     d.ncf = M->nnb[q]; d.nbr = M->nbr[q]; d.color_rows = cols; d.color_ptr = cols + M->n[q];
-    d.ac = M->ac[q]; d.anb = M->anb[q]; d.b = M->b[q]; d.x = M->x[q]; d.r = M->r[q];
+    d.ac = M->ac[q]; d.anb = M->anb[q]; d.b = M->b[q]; d.x = M->x[q]; d.r = M->r[q]; d.t = M->t[q];
     d.parent = (q + 1 < M->nlev) ? M->parent[q] : nullptr;
     d.rptr = M->rptr[q]; d.rlist = M->rlist[q];
     L64[q] = d;
     LevelDev<float> e{};
     e.n = d.n; e.w = d.w; e.ncolors = d.ncolors; e.ncf = d.ncf; e.nbr = d.nbr; e.color_rows = d.color_rows;
     e.color_ptr = d.color_ptr; e.ac = M->acf[q]; e.anb = M->anbf[q]; e.b = M->bf[q]; e.x = M->xf[q]; e.r = M->rf[q];
+    e.t = M->tf[q];
     e.parent = d.parent; e.rptr = d.rptr; e.rlist = d.rlist;
     L32[q] = e;
   }
@@ -704,6 +935,17 @@ int fs_mg_build(fs_ctx *ctx) {
   FS_CK(cudaMalloc(&M->lev32, sizeof(LevelDev<float>) * M->nlev));
   FS_CK(cudaMemcpy(M->lev32, L32.data(), sizeof(LevelDev<float>) * M->nlev, cudaMemcpyHostToDevice));
   FS_CK(cudaMalloc(&M->red, sizeof(double) * 6 * FS_RED_BLOCKS));
+  // preconditioner: stop at the first level small enough for the dense inverse
+  M->lc = M->nlev - 1;
+  for (int q = 0; q < M->nlev; q++)
+    if (q > 0 && M->n[q] <= FS_MG_DIRECT) { M->lc = q; break; }
+  M->direct = M->lc > 0 && M->n[M->lc] <= FS_MG_DIRECT;
+  if (M->direct) {
+    size_t nn = (size_t)M->n[M->lc] * M->n[M->lc];
+    FS_CK(cudaMalloc(&M->sinv, sizeof(double) * nn));
+    FS_CK(cudaFuncSetAttribute((const void *)k_mg_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(sizeof(double) * (nn + M->n[M->lc]))));
+  }
   // cooperative grid: smallest co-resident count of the three kernels, <= 4 CTAs/SM
   int a = 0, b = 0, c = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_mg_solve, FS_COOP_BLOCK, 0));
@@ -722,26 +964,27 @@ int fs_mg_free(fs_ctx *ctx) {
   for (int q = 0; q < M->nlev; q++) {
     void *p[] = {M->colors[q], q ? M->nnb[q] : nullptr, q ? M->nbr[q] : nullptr, M->parent[q], M->cptr[q], M->clist[q],
                  M->cmap[q], M->rptr[q], M->rlist[q], q ? M->ac[q] : nullptr, q ? M->anb[q] : nullptr, M->b[q], M->x[q],
-                 M->r[q], M->acf[q], M->anbf[q], M->bf[q], M->xf[q], M->rf[q]};
+                 M->r[q], M->acf[q], M->anbf[q], M->bf[q], M->xf[q], M->rf[q], M->t[q], M->tf[q]};
     for (void *x : p) if (x) cudaFree(x);
   }
-  cudaFree(M->lev64); cudaFree(M->lev32); cudaFree(M->red);
+  cudaFree(M->lev64); cudaFree(M->lev32); cudaFree(M->red); cudaFree(M->sinv);
   delete M;
   ctx->mg = nullptr;
   return FS_OK;
 }
 
-// coarse matrices for the current fine system (every call: the fine matrix changes)
-static int mg_coarse_matrices(fs_ctx *ctx, bool f32) {
+// coarse matrices of levels 1..last for the current fine system (every call:
+// the fine matrix changes), FP32 copies of levels 0..last when asked
+static int mg_coarse_matrices(fs_ctx *ctx, int last, bool f32) {
   fs_mg_dev *M = ctx->mg;
-  for (int q = 1; q < M->nlev; q++) {
+  for (int q = 1; q <= last; q++) {
     k_mg_lhs<<<fs_grid(M->n[q]), FS_BLOCK, 0, ctx->st>>>(M->n[q - 1], M->nnb[q - 1], M->ac[q - 1], M->anb[q - 1],
                                                         M->n[q], M->w[q], M->cptr[q], M->clist[q], M->cmap[q],
                                                         M->ac[q], M->anb[q]);
     FS_LAUNCH_CHECK();
   }
   if (f32)
-    for (int q = 0; q < M->nlev; q++) {
+    for (int q = 0; q <= last; q++) {
       long n = M->n[q], nw = (long)M->w[q] * M->n[q];
       k_to_f32<<<fs_grid(n), FS_BLOCK, 0, ctx->st>>>(n, M->ac[q], M->acf[q]);
       FS_LAUNCH_CHECK();
@@ -756,9 +999,9 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
   if (rc) return rc;
   fs_mg_dev *M = ctx->mg;
   const bool f32 = solver == FS_SOLVER_AMG32_BICGS;
-  if ((rc = mg_coarse_matrices(ctx, f32))) return rc;
   int G = M->grid;
   if (solver == FS_SOLVER_AMG) {
+    if ((rc = mg_coarse_matrices(ctx, M->nlev - 1, false))) return rc;
     MgSolveArgs a{};
     a.lev = M->lev64; a.nlev = M->nlev; a.type = ctx->cfg.mg_cycle; a.pre = ctx->cfg.mg_pre; a.post = ctx->cfg.mg_post;
     a.maxcycles = ctx->cfg.mg_max_cycles; a.b0 = ctx->bc; a.x0 = ctx->dphi; a.r0 = M->r[0];
@@ -768,25 +1011,33 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     FS_LAUNCH_CHECK();
     return FS_OK;
   }
+  if ((rc = mg_coarse_matrices(ctx, M->lc, f32))) return rc;
+  if (M->direct) {
+    const int n = M->n[M->lc];
+    k_mg_dense_inverse<<<1, 1024, sizeof(double) * ((size_t)n * n + n), ctx->st>>>(
+        n, M->nnb[M->lc], M->nbr[M->lc], M->ac[M->lc], M->anb[M->lc], M->sinv);
+    FS_LAUNCH_CHECK();
+  }
   auto fill = [&](auto &a) {
-    a.N = ctx->N; a.ncf = ctx->ncf; a.cn = ctx->cn; a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc;
+    a.N = ctx->N; a.W = ctx->W; a.ncf = ctx->ncf; a.cn = ctx->cn; a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc;
     a.x = ctx->kx; a.r = ctx->kr; a.r0 = ctx->kr0; a.p = ctx->kp; a.v = ctx->kv; a.s = ctx->ks; a.t = ctx->kt;
     a.y = ctx->ky; a.z = ctx->kz; a.dphi = ctx->dphi;
     // one V-cycle per application: one pre- and one post-sweep (MultiGridpreSweep)
-    a.nlev = M->nlev; a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_pre);
+    a.lc = M->lc; a.direct = M->direct; a.sinv = M->sinv;
+    a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_pre);
     a.maxit = ctx->cfg.krylov_maxit; a.tol = ctx->cfg.krylov_tol; a.part = M->red;
     a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + 22;
   };
   if (!f32) {
     AmgKArgs<double> a{};
     fill(a);
-    a.lev = M->lev64; a.b32 = nullptr; a.x32 = nullptr; a.r32 = M->r[0];
+    a.lev = M->lev64;
     void *args[] = {&a};
     FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<double>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
   } else {
     AmgKArgs<float> a{};
     fill(a);
-    a.lev = M->lev32; a.b32 = M->bf[0]; a.x32 = M->xf[0]; a.r32 = M->rf[0];
+    a.lev = M->lev32;
     void *args[] = {&a};
     FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<float>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
   }

@@ -17,6 +17,12 @@
 
 namespace cg = cooperative_groups;
 
+// CTAs per SM the BiCGSTAB kernel is compiled for (register cap: the shared
+// cooperative grid takes the smallest occupancy of the solver kernels)
+#ifndef FS_KRYLOV_MINB
+#define FS_KRYLOV_MINB 4
+#endif
+
 namespace {
 
 struct SolveArgs {
@@ -38,12 +44,17 @@ struct SolveArgs {
 __device__ __forceinline__ double row_ax(const SolveArgs &a, int i, const double *x) {
   double t = 0.0;
   t = t + a.ac[i] * x[i];
-  int nc = a.ncf[i];
-  for (int j = 0; j < nc; j++) {
-    int k = a.cn[(long)j * a.N + i];
-    if (k >= 0) t = t + a.anb[(long)j * a.N + i] * x[k];
-  }
-  return t;
+  return ell_acc<8, false>(t, a.N, a.W, a.cn, a.anb, i, [&](int k) { return x[k]; });
+}
+
+// rows i and i2 = i + stride (when h2) at once (ell_acc2)
+__device__ __forceinline__ void row_ax2(const SolveArgs &a, long i, long i2, bool h2, const double *x, double &t1,
+                                        double &t2) {
+  t1 = 0.0;
+  t1 = t1 + a.ac[i] * x[i];
+  t2 = 0.0;
+  if (h2) t2 = t2 + a.ac[i2] * x[i2];
+  ell_acc2<6, false>(t1, t2, a.N, a.W, a.cn, a.anb, i, i2, h2, [&](int k) { return x[k]; });
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -86,17 +97,29 @@ __device__ void grid_sum2(cg::grid_group &grid, double *part, int buf, double a0
 
 // BICGSTAB_OMP (matrixSolverOMP.f90:306-386): unpreconditioned, x kept between
 // calls (the reference's module vector x), stop when sqrt|r.r0| <= tol*|b|
-// or after maxit-1 iterations.
-__global__ void __launch_bounds__(FS_COOP_BLOCK) k_bicgstab(SolveArgs a) {
+// or after maxit-1 iterations.  Every row loop takes rows i and i + nth per
+// step (ell_acc2); a thread's partial sums still run over its rows in
+// ascending order.
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_bicgstab(SolveArgs a) {
   cg::grid_group grid = cg::this_grid();
   const int N = a.N;
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
   double l0 = 0., l1 = 0.;
-  for (long i = tid0; i < N; i += nth) {
-    double r0 = a.bc[i] - row_ax(a, (int)i, a.x);
+  for (long i = tid0; i < N; i += 2 * nth) {
+    const long i2 = i + nth;
+    const bool h2 = i2 < N;
+    double t1, t2;
+    row_ax2(a, i, i2, h2, a.x, t1, t2);
+    double r0 = a.bc[i] - t1;
     a.r0[i] = r0; a.r[i] = r0; a.p[i] = r0;
     l0 += r0 * r0;
     l1 += a.bc[i] * a.bc[i];
+    if (h2) {
+      double r2 = a.bc[i2] - t2;
+      a.r0[i2] = r2; a.r[i2] = r2; a.p[i2] = r2;
+      l0 += r2 * r2;
+      l1 += a.bc[i2] * a.bc[i2];
+    }
   }
   double rhoPrev, bb;
   grid_sum2(grid, a.part, 0, l0, l1, rhoPrev, bb);
@@ -107,30 +130,69 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_bicgstab(SolveArgs a) {
     k = k + 1;
     // v = A p ; dp0 = v.r0
     l0 = 0.;
-    for (long i = tid0; i < N; i += nth) { double vi = row_ax(a, (int)i, a.p); a.v[i] = vi; l0 += vi * a.r0[i]; }
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double v1, v2;
+      row_ax2(a, i, i2, h2, a.p, v1, v2);
+      a.v[i] = v1; l0 += v1 * a.r0[i];
+      if (h2) { a.v[i2] = v2; l0 += v2 * a.r0[i2]; }
+    }
     double dp0, dum;
     grid_sum2(grid, a.part, buf, l0, 0., dp0, dum); buf ^= 3;
     double alpha = rhoPrev / dp0;
-    for (long i = tid0; i < N; i += nth) a.s[i] = a.r[i] - alpha * a.v[i];
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double r1 = a.r[i], v1 = a.v[i], r2 = h2 ? a.r[i2] : 0., v2 = h2 ? a.v[i2] : 0.;
+      a.s[i] = r1 - alpha * v1;
+      if (h2) a.s[i2] = r2 - alpha * v2;
+    }
     grid.sync();
     // As = A s ; dp1 = As.s ; dp2 = As.As
     l0 = 0.; l1 = 0.;
-    for (long i = tid0; i < N; i += nth) { double ti = row_ax(a, (int)i, a.s); a.t[i] = ti; l0 += ti * a.s[i]; l1 += ti * ti; }
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double t1, t2;
+      row_ax2(a, i, i2, h2, a.s, t1, t2);
+      a.t[i] = t1; l0 += t1 * a.s[i]; l1 += t1 * t1;
+      if (h2) { a.t[i2] = t2; l0 += t2 * a.s[i2]; l1 += t2 * t2; }
+    }
     double dp1, dp2;
     grid_sum2(grid, a.part, buf, l0, l1, dp1, dp2); buf ^= 3;
     double omega = dp1 / dp2;
     l0 = 0.;
-    for (long i = tid0; i < N; i += nth) {
-      a.x[i] = a.x[i] + alpha * a.p[i] + omega * a.s[i];
-      double ri = a.s[i] - omega * a.t[i];
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double x1 = a.x[i], p1 = a.p[i], s1 = a.s[i], t1 = a.t[i], q1 = a.r0[i];
+      double x2 = 0., p2 = 0., s2 = 0., t2 = 0., q2 = 0.;
+      if (h2) { x2 = a.x[i2]; p2 = a.p[i2]; s2 = a.s[i2]; t2 = a.t[i2]; q2 = a.r0[i2]; }
+      a.x[i] = x1 + alpha * p1 + omega * s1;
+      double ri = s1 - omega * t1;
       a.r[i] = ri;
-      l0 += ri * a.r0[i];
+      l0 += ri * q1;
+      if (h2) {
+        a.x[i2] = x2 + alpha * p2 + omega * s2;
+        double rj = s2 - omega * t2;
+        a.r[i2] = rj;
+        l0 += rj * q2;
+      }
     }
     double rho;
     grid_sum2(grid, a.part, buf, l0, 0., rho, dum); buf ^= 3;
     double beta = (rho / rhoPrev) * (alpha / omega);
     rhoPrev = rho;
-    for (long i = tid0; i < N; i += nth) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double r1 = a.r[i], p1 = a.p[i], v1 = a.v[i];
+      double r2 = 0., p2 = 0., v2 = 0.;
+      if (h2) { r2 = a.r[i2]; p2 = a.p[i2]; v2 = a.v[i2]; }
+      a.p[i] = r1 + beta * (p1 - omega * v1);
+      if (h2) a.p[i2] = r2 + beta * (p2 - omega * v2);
+    }
     resnorm = sqrt(fabs(rho));
     grid.sync();
   }
@@ -142,7 +204,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_bicgstab(SolveArgs a) {
 // forward over colours 0..C-1, backward C-1..0, each colour an independent
 // set, then CheckConvergence (CheckConvergenceRoutine.for:3) -- until
 // sum|r| <= rrF * IResiduals or itmax sweeps (SolveAlegbraicEquations.for:108-117).
-__global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor(SolveArgs a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor(SolveArgs a) {
   cg::grid_group grid = cg::this_grid();
   const int N = a.N;
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
@@ -155,12 +217,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor(SolveArgs a) {
         int r0 = a.color_ptr[c], r1 = a.color_ptr[c + 1];
         for (long q = r0 + tid0; q < r1; q += nth) {
           int i = a.color_rows[q];
-          double l = a.bc[i];
-          int nc = a.ncf[i];
-          for (int j = 0; j < nc; j++) {
-            int k = a.cn[(long)j * N + i];
-            if (k >= 0) l = l - a.anb[(long)j * N + i] * a.dphi[k];
-          }
+          double l = ell_acc<8, true>(a.bc[i], N, a.W, a.cn, a.anb, i, [&](int k) { return a.dphi[k]; });
           a.dphi[i] = l / a.ac[i];
         }
         grid.sync();
@@ -168,12 +225,8 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor(SolveArgs a) {
     }
     double l0 = 0., dum;
     for (long i = tid0; i < N; i += nth) {
-      double r = a.bc[i] - a.ac[i] * a.dphi[i];
-      int nc = a.ncf[i];
-      for (int j = 0; j < nc; j++) {
-        int k = a.cn[(long)j * N + i];
-        if (k >= 0) r = r - a.anb[(long)j * N + i] * a.dphi[k];
-      }
+      double r = ell_acc<8, true>(a.bc[i] - a.ac[i] * a.dphi[i], N, a.W, a.cn, a.anb, i,
+                                  [&](int k) { return a.dphi[k]; });
       l0 += fabs(r);
     }
     grid_sum2(grid, a.part, buf, l0, 0., fres, dum); buf ^= 1;
@@ -185,7 +238,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor(SolveArgs a) {
 // the same sweeps on the colour-major copy: colour c occupies positions
 // [color_ptr[c], color_ptr[c+1]) contiguously, so every pass streams its rows
 struct SorPArgs {
-  int N;
+  int N, W;
   const int32_t *ncf, *cn, *color_ptr;
   const double *ac, *anb, *bc;
   double *x;
@@ -197,11 +250,10 @@ struct SorPArgs {
   double *diag;
 };
 
-__global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor_colour(SorPArgs a) {
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor_colour(SorPArgs a) {
   cg::grid_group grid = cg::this_grid();
   const int N = a.N;
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
-  const int32_t *__restrict__ ncf = a.ncf;
   const int32_t *__restrict__ cn = a.cn;
   const double *__restrict__ anb = a.anb;
   double ires = *a.ires, fres = ires;
@@ -211,27 +263,26 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor_colour(SorPArgs a) {
       for (int cc = 0; cc < a.ncolors; cc++) {
         int c = pass == 0 ? cc : a.ncolors - 1 - cc;
         int r0 = a.color_ptr[c], r1 = a.color_ptr[c + 1];
-        for (long i = r0 + tid0; i < r1; i += nth) {
-          double l = a.bc[i];
-          int nc = ncf[i];
-          for (int j = 0; j < nc; j++) {
-            int k = cn[(long)j * N + i];
-            if (k >= 0) l = l - anb[(long)j * N + i] * a.x[k];
-          }
-          a.x[i] = l / a.ac[i];
+        // rows of one colour are independent: two per step (ell_acc2)
+        for (long i = r0 + tid0; i < r1; i += 2 * nth) {
+          const long i2 = i + nth;
+          const bool h2 = i2 < r1;
+          double l1 = a.bc[i], l2 = h2 ? a.bc[i2] : 0.;
+          ell_acc2<6, true>(l1, l2, N, a.W, cn, anb, i, i2, h2, [&](int k) { return a.x[k]; });
+          a.x[i] = l1 / a.ac[i];
+          if (h2) a.x[i2] = l2 / a.ac[i2];
         }
         grid.sync();
       }
     }
     double l0 = 0., dum;
-    for (long i = tid0; i < N; i += nth) {
-      double r = a.bc[i] - a.ac[i] * a.x[i];
-      int nc = ncf[i];
-      for (int j = 0; j < nc; j++) {
-        int k = cn[(long)j * N + i];
-        if (k >= 0) r = r - anb[(long)j * N + i] * a.x[k];
-      }
-      l0 += fabs(r);
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double q1 = a.bc[i] - a.ac[i] * a.x[i], q2 = h2 ? a.bc[i2] - a.ac[i2] * a.x[i2] : 0.;
+      ell_acc2<6, true>(q1, q2, N, a.W, cn, anb, i, i2, h2, [&](int k) { return a.x[k]; });
+      l0 += fabs(q1);
+      if (h2) l0 += fabs(q2);
     }
     grid_sum2(grid, a.part, buf, l0, 0., fres, dum); buf ^= 1;
     iter++;
@@ -260,7 +311,7 @@ __global__ void k_from_colour(int N, const int32_t *__restrict__ pos, const doub
 // multi-RHS momentum: X, Y, Z systems share anb/cn; each keeps its own ac, bc
 // and convergence test (SolveAlegbraicEquations.for:108-117 per component)
 struct Sor3Args {
-  int N;
+  int N, W;
   const int32_t *ncf, *cn, *color_ptr;
   const double *ac3, *anb, *bc3;
   double *x3;
@@ -271,11 +322,38 @@ struct Sor3Args {
   int32_t *iters3;
 };
 
-__global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor3_colour(Sor3Args a) {
+// l_c -= anb_ij x_c[k_ij] (m for row i2) for the three components sharing
+// anb, slots in ascending order, rows i and i2 (when h2) at once
+__device__ __forceinline__ void sub3x2(long N, int W, const int32_t *__restrict__ cn, const double *__restrict__ anb,
+                                       long i, long i2, bool h2, const double *x3, double *l, double *m) {
+  for (int j0 = 0; j0 < W; j0 += 4) {
+    int k[4], k2[4];
+    double w[4], w2[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int j = j0 + u;
+      const bool in = j < W, in2 = in && h2;
+      k[u] = in ? cn[(long)j * N + i] : -1;
+      w[u] = in ? anb[(long)j * N + i] : 0.;
+      k2[u] = in2 ? cn[(long)j * N + i2] : -1;
+      w2[u] = in2 ? anb[(long)j * N + i2] : 0.;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (k[u] >= 0) {
+        l[0] = l[0] - w[u] * x3[k[u]]; l[1] = l[1] - w[u] * x3[N + k[u]]; l[2] = l[2] - w[u] * x3[2 * N + k[u]];
+      }
+      if (k2[u] >= 0) {
+        m[0] = m[0] - w2[u] * x3[k2[u]]; m[1] = m[1] - w2[u] * x3[N + k2[u]]; m[2] = m[2] - w2[u] * x3[2 * N + k2[u]];
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor3_colour(Sor3Args a) {
   cg::grid_group grid = cg::this_grid();
   const int N = a.N;
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
-  const int32_t *__restrict__ ncf = a.ncf;
   const int32_t *__restrict__ cn = a.cn;
   const double *__restrict__ anb = a.anb;
   double ires[3], fres[3];
@@ -291,37 +369,35 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_sor3_colour(Sor3Args a) {
       for (int cc = 0; cc < a.ncolors; cc++) {
         int col = pass == 0 ? cc : a.ncolors - 1 - cc;
         int r0 = a.color_ptr[col], r1 = a.color_ptr[col + 1];
-        for (long i = r0 + tid0; i < r1; i += nth) {
-          double l0 = a.bc3[i], l1 = a.bc3[N + i], l2 = a.bc3[2L * N + i];
-          int nc = ncf[i];
-          for (int j = 0; j < nc; j++) {
-            int k = cn[(long)j * N + i];
-            if (k >= 0) {
-              double w = anb[(long)j * N + i];
-              l0 = l0 - w * a.x3[k]; l1 = l1 - w * a.x3[N + k]; l2 = l2 - w * a.x3[2L * N + k];
-            }
+        for (long i = r0 + tid0; i < r1; i += 2 * nth) {
+          const long i2 = i + nth;
+          const bool h2 = i2 < r1;
+          double l[3] = {a.bc3[i], a.bc3[N + i], a.bc3[2L * N + i]};
+          double m[3] = {0., 0., 0.};
+          if (h2) { m[0] = a.bc3[i2]; m[1] = a.bc3[N + i2]; m[2] = a.bc3[2L * N + i2]; }
+          sub3x2(N, a.W, cn, anb, i, i2, h2, a.x3, l, m);
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            if (act[c]) a.x3[c * (long)N + i] = l[c] / a.ac3[c * (long)N + i];
+            if (act[c] && h2) a.x3[c * (long)N + i2] = m[c] / a.ac3[c * (long)N + i2];
           }
-          if (act[0]) a.x3[i] = l0 / a.ac3[i];
-          if (act[1]) a.x3[N + i] = l1 / a.ac3[N + i];
-          if (act[2]) a.x3[2L * N + i] = l2 / a.ac3[2L * N + i];
         }
         grid.sync();
       }
     }
     double s0 = 0., s1 = 0., s2 = 0.;
-    for (long i = tid0; i < N; i += nth) {
-      double r0 = a.bc3[i] - a.ac3[i] * a.x3[i];
-      double r1 = a.bc3[N + i] - a.ac3[N + i] * a.x3[N + i];
-      double r2 = a.bc3[2L * N + i] - a.ac3[2L * N + i] * a.x3[2L * N + i];
-      int nc = ncf[i];
-      for (int j = 0; j < nc; j++) {
-        int k = cn[(long)j * N + i];
-        if (k >= 0) {
-          double w = anb[(long)j * N + i];
-          r0 = r0 - w * a.x3[k]; r1 = r1 - w * a.x3[N + k]; r2 = r2 - w * a.x3[2L * N + k];
-        }
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double l[3], m[3] = {0., 0., 0.};
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        l[c] = a.bc3[c * (long)N + i] - a.ac3[c * (long)N + i] * a.x3[c * (long)N + i];
+        if (h2) m[c] = a.bc3[c * (long)N + i2] - a.ac3[c * (long)N + i2] * a.x3[c * (long)N + i2];
       }
-      s0 += fabs(r0); s1 += fabs(r1); s2 += fabs(r2);
+      sub3x2(N, a.W, cn, anb, i, i2, h2, a.x3, l, m);
+      s0 += fabs(l[0]); s1 += fabs(l[1]); s2 += fabs(l[2]);
+      if (h2) { s0 += fabs(m[0]); s1 += fabs(m[1]); s2 += fabs(m[2]); }
     }
     double o0, o1, o2, d;
     grid_sum2(grid, a.part, buf, s0, s1, o0, o1);
@@ -423,7 +499,7 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     FS_LAUNCH_CHECK();
     if ((rc = coop_grid_size(ctx))) return rc;
     SorPArgs sp{};
-    sp.N = N; sp.ncf = ctx->ncfP; sp.cn = ctx->cnP; sp.color_ptr = ctx->color_rows + N;
+    sp.N = N; sp.W = ctx->W; sp.ncf = ctx->ncfP; sp.cn = ctx->cnP; sp.color_ptr = ctx->color_rows + N;
     sp.ac = ctx->acP; sp.anb = ctx->anbP; sp.bc = ctx->bcP; sp.x = ctx->dphiP; sp.part = ctx->red;
     sp.ires = a.ires; sp.rrf = rrf; sp.itmax = itmax; sp.ncolors = ctx->ncolors; sp.iters = a.iters; sp.diag = a.diag;
     int G = ctx->coop_grid;
@@ -567,7 +643,7 @@ int fs_momentum_batched_solve(fs_ctx *ctx) {
                                                     ctx->ac3P, ctx->bc3P, ctx->anbP, ctx->x3P);
   FS_LAUNCH_CHECK();
   Sor3Args a{};
-  a.N = N; a.ncf = ctx->ncfP; a.cn = ctx->cnP; a.color_ptr = ctx->color_rows + N;
+  a.N = N; a.W = ctx->W; a.ncf = ctx->ncfP; a.cn = ctx->cnP; a.color_ptr = ctx->color_rows + N;
   a.ac3 = ctx->ac3P; a.anb = ctx->anbP; a.bc3 = ctx->bc3P; a.x3 = ctx->x3P; a.part = ctx->red;
   a.ires3 = ctx->resblk + RB_ABS; a.rrf = ctx->cfg.rrf_mom; a.itmax = ctx->cfg.itmax_mom; a.ncolors = ctx->ncolors;
   a.iters3 = ctx->d_iters;
