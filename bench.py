@@ -5,16 +5,28 @@ assembly and solves, Rhie-Chow + p' assembly, p' solve, corrections,
 residuals) on the 2,097,152-cell cavity (Re=1000, SOU deferred correction,
 SIMPLEC, urf 0.7/0.7).  Synthetic mesh, generated here.
 
+Forms (same case, same initial state):
+  fp64   the plain FP64 GPU path: momentum by multicolour SOR, p' by FP64
+         BiCGSTAB right-preconditioned with one element-agglomeration AMG
+         V-cycle (coarsest level inverted densely), tolerance 1e-8.  `value`.
+  mixed  the chosen forms: FP32 V-cycle (FP32 coarse matrices) inside the
+         FP64 BiCGSTAB, the three momentum components as one multi-RHS solve.
+         Reported under "mixed" with its field error against fp64.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--ttr MAXIT]
 
 b200 arm: `value` is device-timed (CUDA events on the solver's stream) with
-the state resident in HBM; `e2e` runs the same steps through the C ABI
+the state resident in HBM; `e2e` runs the fp64 steps through the C ABI
 fs_simple_iteration_host with the state in pinned host buffers, copies inside
-the timed region.  N>1 (torchrun) runs one independent replica per GPU (the
-single-mesh path does not shard) and reports the aggregate over ranks with the
-max-over-ranks time.  reference arm: the CPU restatement of the reference's
-loop (the Fortran reference cannot be compiled in this image) timed on the
-host, rank 0 only.
+the timed region.  `--ttr MAXIT` adds the time to residual 1e-6 of both forms
+from the initial state (at 128^3 this takes thousands of iterations).  N>1
+(torchrun) runs one independent replica per GPU (the single-mesh path does not
+shard) and reports the aggregate over ranks with the max-over-ranks time.
+reference arm: the CPU restatement of the reference's loop with the
+reference's own p' solver (unpreconditioned BiCGSTAB, same 1e-8 tolerance;
+the Fortran reference cannot be compiled in this image), timed on the host,
+rank 0 only.
 """
 from __future__ import annotations
 
@@ -31,6 +43,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 HBM_FALLBACK_GBS = 6650.0
+
+FORMS = {
+    "fp64": dict(solver_mom="sor", solver_cont="amg_bicgs", krylov_tol=1e-8, krylov_maxit=200),
+    "mixed": dict(solver_mom="sor", solver_cont="amg32_bicgs", krylov_tol=1e-8, krylov_maxit=200,
+                  batched_momentum=True),
+}
+REFERENCE_SOLVERS = dict(solver_mom="sor", solver_cont="bicgs", krylov_tol=1e-8, krylov_maxit=300)
 
 
 def peaks():
@@ -59,10 +78,10 @@ def aggregate_rate(world: int, steps: int, ms_max: float) -> float:
     return world * steps / (ms_max * 1e-3)
 
 
-def workload(n: int):
+def workload(n: int, form: str = "fp64"):
     from flowsolversourcecode_b200 import case as cs
-    mesh, case = cs.cavity3d(n, solver_mom="sor", solver_cont="bicgs")
-    return mesh, case
+    kw = REFERENCE_SOLVERS if form == "reference" else FORMS[form]
+    return cs.cavity3d(n, **kw)
 
 
 class Clocks:
@@ -116,53 +135,112 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def solver_roofline(stats: dict, N: int, W: int, hbm: float, ncu_traffic: dict | None):
-    """Achieved HBM bandwidth of the solver kernel with the most device time.
+# ---------------------------------------------------------------- algorithmic bytes
+def row_bytes(w: int, r: int) -> int:
+    """One ELL row: diagonal (r bytes), w coefficients (r) and w int32 indices.
+    The fixed-width row loops read all w slots (padded slots hold index -1)."""
+    return r + (r + 4) * w
 
-    Algorithmic bytes per matrix row (FP64 values, int32 indices, W slots):
-      matrix row          = 8 (ac) + 8W (anb) + 4W (cn) + 4 (ncf)
-      BiCGSTAB iteration  = 2 SpMV x (row + 8 x_i + 8 y) + 8 (r0 in v.r0)
-                            + 24 (s) + 48 (x, r) + 8 (r0) + 32 (p)
-      BiCGSTAB set-up     = row + 8 (b) + 8 (x) + 24 (r0, r, p) + 8 (dphi)
-      SOR sweep (fwd+bwd) = 2 x (row + 8 bc + 8 dphi + 4 colour list) + residual (row + 16)
-    """
-    row = 8 + 8 * W + 4 * W + 4
-    per = {"bicgstab": 2 * (row + 16) + 8 + 24 + 48 + 8 + 32, "sor": 2 * (row + 20) + row + 16}
+
+def vcycle_bytes(mg: dict, W: int, N: int, r: int) -> float:
+    """Compulsory HBM bytes of one preconditioner V-cycle (PCycle, one pre- and
+    one post-sweep): every array a phase touches is read or written once.
+      level 0   x0 = w in/ac          : in 8 + ac r + x r
+                residual              : row + in 8 + x r + r r
+                prolong (own phase)   : x r (read) + x r (write) + parent 4
+                sweep to `out` (FP64) : row + in 8 + x r + out 8
+      level l   restrict into l       : per fine row r_{l-1} r + rlist 4;
+                                        per row rptr 4 + b r + ac r + x r
+                residual, prolong+sweep as level 0 with b r instead of in 8,
+                                        the result into r (r bytes)
+      coarsest  restrict as above; dense solve n_c^2 x 8 + b r + x r
+    Gathers of neighbour values are L2 traffic and are not counted."""
+    sizes, widths, lc = mg["sizes"], mg["widths"], mg["prec_coarsest"]
+    total = 0.0
+    for l in range(lc + 1):
+        n, w = sizes[l], (W if l == 0 else widths[l])
+        row = row_bytes(w, r)
+        if l == 0:
+            total += n * (8 + 2 * r)                                  # x0 = omega in / ac
+            total += n * (row + 8 + 2 * r)                            # residual
+            total += n * (2 * r + 4)                                  # prolong
+            total += n * (row + 8 + r + 8)                            # sweep into out
+            continue
+        total += sizes[l - 1] * (r + 4) + n * (4 + 3 * r)            # restrict into l
+        if l == lc and mg["direct"]:
+            total += n * n * 8 + n * 2 * r
+            continue
+        total += n * (row + 3 * r)                                    # residual
+        total += n * (2 * r + 4) + n * (row + 3 * r)                  # prolong + sweep
+    return total
+
+
+def amg_bicgstab_bytes(mg: dict, W: int, N: int, r: int, iters: int, calls: int) -> float:
+    """k_amg_bicgstab: per BiCGSTAB iteration the Krylov algebra
+      r0.r 16, p 32, v = A y (row + y 8 + v 8 + r0 8), s 24,
+      t = A z (row + z 8 + t 8 + s 8), x/r update 56
+    = 176 + 2 row bytes per row (FP64 matrix), plus two V-cycles; per launch
+    the set-up (b, r, r0, p, v, x: 48) and dphi (8)."""
+    row0 = row_bytes(W, 8)
+    per_it = N * (176 + 2 * row0) + 2 * vcycle_bytes(mg, W, N, r)
+    return per_it * iters + N * 56.0 * calls
+
+
+def sor_bytes(W: int, N: int, sweeps: int, rhs: int = 1) -> float:
+    """k_sor_colour (rhs=1) / k_sor3_colour (rhs=3) on the colour-major copy:
+    a symmetric sweep visits every row twice (row + rhs x (bc 8 + x 8)), and
+    the residual check once more (row + rhs x 16)."""
+    row = row_bytes(W, 8) + (rhs - 1) * 8                # ac per component
+    per_sweep = N * (2 * (row + rhs * 16) + row + rhs * 16)
+    return per_sweep * sweeps
+
+
+def solver_roofline(stats: dict, mg: dict | None, N: int, W: int, hbm: float, form: str,
+                    ncu_traffic: dict | None):
+    """Achieved HBM bandwidth of the solver kernel with the most device time
+    (CUDA events around that kernel alone, on the solver stream)."""
     best = None
     for q in range(5):
-        ms, its, calls = stats["ms"][q], stats["iters"][q], stats["calls"][q]
-        if calls == 0 or ms <= 0:
+        kms, its, calls = stats["kernel_ms"][q], stats["iters"][q], stats["calls"][q]
+        if calls == 0 or kms <= 0:
             continue
-        kind = "bicgstab" if q == 3 else "sor"
-        setup = (row + 48) if kind == "bicgstab" else 0
-        nbytes = N * (per[kind] * its + setup * calls)
-        if best is None or ms > best["ms"]:
-            best = {"kernel": "k_bicgstab" if kind == "bicgstab" else "k_sor", "ms": ms, "bytes": nbytes,
-                    "calls": calls, "iters": its}
+        if q == 3:
+            r = 4 if form == "mixed" else 8
+            name = "k_amg_bicgstab<float>" if r == 4 else "k_amg_bicgstab<double>"
+            nbytes = amg_bicgstab_bytes(mg, W, N, r, its, calls)
+        elif form == "mixed" and q == 0:
+            name, nbytes = "k_sor3_colour", sor_bytes(W, N, its, rhs=3)
+        else:
+            name, nbytes = "k_sor_colour", sor_bytes(W, N, its)
+        if best is None or kms > best["ms"]:
+            best = {"kernel": name, "ms": kms, "bytes": nbytes, "calls": calls, "iters": its}
     if best is None:
         return None
     achieved = best["bytes"] / (best["ms"] * 1e-3) / 1e9
     traffic = None
     if ncu_traffic and best["kernel"] in ncu_traffic:
         t = ncu_traffic[best["kernel"]]
-        # measured bytes per row-iteration on a smaller case, scaled to these launches
+        # DRAM bytes per (row x linear iteration) measured by ncu on a smaller
+        # case of the same kernel, scaled to one launch here
         traffic = t["bytes_per_row_iter"] * N * best["iters"] / best["calls"]
     return {"bound": "hbm", "kernel": best["kernel"], "achieved": round(achieved, 1), "peak": hbm,
-            "unit": "GB/s", "frac": round(achieved / hbm, 4),
-            "traffic": traffic, "algorithmic_bytes_per_launch": best["bytes"] / best["calls"],
-            "launches": best["calls"], "avg_launch_ms": best["ms"] / best["calls"]}
+            "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": traffic,
+            "algorithmic_bytes_per_launch": best["bytes"] / best["calls"], "launches": best["calls"],
+            "avg_launch_ms": best["ms"] / best["calls"],
+            "iters_per_launch": best["iters"] / best["calls"]}
 
 
-def cpu_baseline_sample(mesh, case) -> dict:
+def cpu_baseline_sample(n: int) -> dict:
     import oracle
+    mesh, case = workload(n, "reference")
     o = oracle.Oracle(mesh, case)
-    o.simple_iteration()                 # first iteration (CSR set-up), untimed
     t0 = time.perf_counter()
     o.simple_iteration()
     dt = time.perf_counter() - t0
     o.close()
     return {"value": 1.0 / dt, "unit": "iter/s", "cores": 1, "kind": "port",
-            "sample": "1 SIMPLE outer iteration (the 2nd) of the same 128^3 case on the CPU restatement, 1 thread"}
+            "sample": f"the 1st SIMPLE outer iteration of the same {n}^3 case on the sequential CPU "
+                      f"restatement (p' by the reference's unpreconditioned BiCGSTAB to 1e-8), 1 thread"}
 
 
 def run_reference(args, rank: int) -> None:
@@ -170,10 +248,11 @@ def run_reference(args, rank: int) -> None:
         return
     import oracle
     oracle.build()
-    mesh, case = workload(args.n)
+    mesh, case = workload(args.n, "reference")
     o = oracle.Oracle(mesh, case)
+    warm = 1
     t0 = time.perf_counter()
-    for _ in range(max(1, min(args.warmup, 1))):
+    for _ in range(warm):
         o.simple_iteration()
     t_warm = time.perf_counter() - t0
     budget = 150.0
@@ -190,18 +269,57 @@ def run_reference(args, rank: int) -> None:
     val = k_run / total
     line = {
         "impl": "reference", "metric": "SIMPLE iters/s", "value": val, "unit": "iter/s", "n_gpus": args.gpus,
-        "steps": k_run, "warmup": max(1, min(args.warmup, 1)), "ms_per_step": 1e3 * total / k_run,
+        "steps": k_run, "warmup": warm, "ms_per_step": 1e3 * total / k_run,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"cavity3d_{args.n} lid-driven cavity, {mesh.n_cells} cells, Re=1000, SOU, SIMPLEC",
-                   "cells": mesh.n_cells, "solvers": "momentum sor, p' bicgs"},
+                   "cells": mesh.n_cells,
+                   "solvers": "momentum sor, p' bicgs (the reference's unpreconditioned BiCGSTAB) to 1e-8"},
         "cpu_baseline": {"value": val, "unit": "iter/s", "cores": 1, "kind": "port",
-                         "sample": f"{k_run} of {args.steps} requested SIMPLE iterations (time budget {budget:.0f}s) "
-                                   f"on the sequential CPU restatement; reference Fortran build unavailable "
-                                   f"(no Fortran compiler in the image)"},
+                         "sample": f"{k_run} of {args.steps} requested SIMPLE iterations after {warm} untimed "
+                                   f"(time budget {budget:.0f}s) on the sequential CPU restatement; reference "
+                                   f"Fortran build unavailable (no Fortran compiler in the image)"},
         "e2e": {"value": val, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "warmup_s": t_warm,
     }
     print(json.dumps(line), flush=True)
+
+
+def device_leg(s, steps: int, warm: int, barrier, local: int):
+    """Warm up, then time `steps` SIMPLE iterations with CUDA events on the
+    solver stream; clocks sampled during the timed region."""
+    for _ in range(warm):
+        s.simple_iteration()
+    s.sync()
+    s.solver_stats(reset=True)
+    barrier()
+    l0 = s.launch_count()
+    with Clocks(local) as clk:
+        s.timer_start()
+        last = None
+        for _ in range(steps):
+            last = s.simple_iteration()
+        ms = s.timer_stop()
+    return {"ms": ms, "launches": s.launch_count() - l0, "clocks": clk.summary(),
+            "stats": s.solver_stats(reset=True), "phases": s.phase_times(), "last": last}
+
+
+def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e-6) -> dict:
+    """Device time from the initial state until the stop metric drops below tol."""
+    s = Solver(mesh, case, device=local)
+    s.timer_start()
+    total, it, src = 0.0, 0, None
+    for it in range(1, maxit + 1):
+        r = s.simple_iteration()
+        src = r["source"]
+        if it % 200 == 0:
+            total += s.timer_stop()
+            s.timer_start()
+        if src < tol:
+            break
+    total += s.timer_stop()
+    s.close()
+    return {"seconds": total * 1e-3, "iterations": it, "reached": bool(src is not None and src < tol),
+            "final_source": src}
 
 
 def main():
@@ -211,6 +329,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--ttr", type=int, default=0, help="max iterations of the time-to-1e-6 leg (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -236,35 +355,22 @@ def main():
     fb.build()
     from flowsolversourcecode_b200.solver import Solver
 
-    mesh, case = workload(args.n)
-    s = Solver(mesh, case, device=local)
-    N, W = s.N, s.W
-    warm = max(args.warmup, 3)
-
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # ---------------- device-resident leg
-    for _ in range(warm):
-        s.simple_iteration()
-    s.sync()
-    s.solver_stats(reset=True)
-    barrier()
-    l0 = s.launch_count()
-    with Clocks(local) as clk:
-        s.timer_start()
-        last = None
-        for _ in range(args.steps):
-            last = s.simple_iteration()
-        ms = s.timer_stop()
-    launches = s.launch_count() - l0
-    clocks = clk.summary()
-    stats = s.solver_stats(reset=True)
-    phases = s.phase_times()
-    ms_max = reduce_max(ms, dist, f"cuda:{local}")
+    warm = max(args.warmup, 3)
+    mesh, case = workload(args.n, "fp64")
 
-    # ---------------- end-to-end leg (host buffers through the C ABI)
+    # ---------------- fp64 form: device-resident leg
+    s = Solver(mesh, case, device=local)
+    N, W, F = s.N, s.W, s.F
+    mg = s.mg_info()
+    d64 = device_leg(s, args.steps, warm, barrier, local)
+    ms_max = reduce_max(d64["ms"], dist, f"cuda:{local}")
+    fields64 = {k: s.get(k) for k in ("u", "v", "w", "p")}
+
+    # ---------------- fp64 form: end-to-end leg (host buffers through the C ABI)
     st = s.state()
     pinned = {}
     for k, v in st.items():
@@ -282,6 +388,23 @@ def main():
     e2e_ms = s.timer_stop()
     e2e_max = reduce_max(e2e_ms, dist, f"cuda:{local}")
     io_bytes = 8 * sum(a.shape[0] for a in host.values())
+    s.close()
+
+    # ---------------- mixed form: same case and initial state
+    _, case_m = workload(args.n, "mixed")
+    sm = Solver(mesh, case_m, device=local)
+    dmx = device_leg(sm, args.steps, warm, barrier, local)
+    msm_max = reduce_max(dmx["ms"], dist, f"cuda:{local}")
+    err = {}
+    for k, ref in fields64.items():
+        x = sm.get(k)
+        err[k] = float(np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300))
+    sm.close()
+
+    ttr = None
+    if args.ttr > 0:
+        ttr = {"fp64": time_to_residual(Solver, mesh, case, local, args.ttr),
+               "mixed": time_to_residual(Solver, mesh, case_m, local, args.ttr)}
 
     if rank == 0:
         hbm, src = peaks()
@@ -290,35 +413,50 @@ def main():
         if os.path.exists(tp):
             with open(tp) as f:
                 ncu_t = json.load(f)
-        roof = solver_roofline(stats, N, W, hbm, ncu_t)
-        if roof:
-            roof["peak_source"] = f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback 6.65 TB/s"
+        roof = solver_roofline(d64["stats"], mg, N, W, hbm, "fp64", ncu_t)
+        roof_m = solver_roofline(dmx["stats"], mg, N, W, hbm, "mixed", ncu_t)
+        for rf in (roof, roof_m):
+            if rf:
+                rf["peak_source"] = "measured (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else \
+                    "fallback 6.65 TB/s"
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline_sample(mesh, case)
+            cpu = cpu_baseline_sample(args.n)
         value = aggregate_rate(world, args.steps, ms_max)
         line = {
             "metric": "SIMPLE iters/s", "value": value, "unit": "iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": warm, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"cavity3d_{args.n} lid-driven cavity, {N} cells, {s.F} interior faces, "
+            "config": {"workload": f"cavity3d_{args.n} lid-driven cavity, {N} cells, {F} interior faces, "
                                    f"Re=1000, SOU deferred correction, SIMPLEC urf 0.7/0.7",
-                       "cells": N, "faces": s.F, "solvers": "momentum sor (multicolour), p' bicgs",
+                       "cells": N, "faces": F,
+                       "solvers": "momentum: multicolour SOR (rrF 0.01, 30 sweeps); p': FP64 BiCGSTAB "
+                                  "right-preconditioned by one element-agglomeration AMG V-cycle, tol 1e-8",
+                       "mg_levels": mg["sizes"], "mg_prec_coarsest": mg["prec_coarsest"],
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "inputs larger than L2 (working set ~1.7 GB)",
-                       "lin_iters_last_step": last["lin_iters"] if last else None,
-                       "solver_ms_per_step": [round(x / args.steps, 3) for x in stats["ms"]],
-                       "phase_ms_last_step": [round(x, 3) for x in phases]},
+                       "l2": "inputs larger than L2 (working set ~2 GB)",
+                       "lin_iters_last_step": d64["last"]["lin_iters"] if d64["last"] else None,
+                       "solver_ms_per_step": [round(x / args.steps, 3) for x in d64["stats"]["ms"]],
+                       "phase_ms_last_step": [round(x, 3) for x in d64["phases"]]},
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": aggregate_rate(world, args.steps, e2e_max), "unit": "iter/s",
                     "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-            "gpu_launches": launches,
-            "clocks": clocks,
+            "gpu_launches": d64["launches"],
+            "clocks": d64["clocks"],
+            "mixed": {"form": "FP32 AMG V-cycle (FP32 coarse matrices) inside FP64 BiCGSTAB to 1e-8; "
+                              "multi-RHS momentum SOR",
+                      "value": aggregate_rate(world, args.steps, msm_max), "unit": "iter/s",
+                      "ms_per_step": msm_max / args.steps,
+                      "time_vs_fp64": msm_max / ms_max,
+                      "field_rel_l2_vs_fp64": err,
+                      "solver_ms_per_step": [round(x / args.steps, 3) for x in dmx["stats"]["ms"]],
+                      "lin_iters_last_step": dmx["last"]["lin_iters"] if dmx["last"] else None,
+                      "roofline": roof_m, "gpu_launches": dmx["launches"], "clocks": dmx["clocks"]},
+            "time_to_1e-6": ttr,
         }
         print(json.dumps(line), flush=True)
-    s.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

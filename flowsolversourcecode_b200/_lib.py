@@ -112,6 +112,8 @@ PROTOTYPES = {
     "fs_get_connectivity": (C.c_int, [_V, _I, _I, _I, _I, _I]),
     "fs_mg_levels": (C.c_int, [_V, _I, _I, C.c_int]),
     "fs_mg_parents": (C.c_int, [_V, C.c_int, _I, C.c_size_t]),
+    "fs_mg_info": (C.c_int, [_V, _I, C.c_int, _I, _I]),
+    "fs_solver_kernel_ms": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "fs_phase_times": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "fs_timer_start": (C.c_int, [_V]),
     "fs_timer_stop": (C.c_int, [_V, C.POINTER(C.c_float)]),

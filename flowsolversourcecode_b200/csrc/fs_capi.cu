@@ -168,6 +168,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (auto &e : ctx->ev) cudaEventCreate(&e);
   for (auto &e : ctx->tev) cudaEventCreate(&e);
   for (auto &pr : ctx->sev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
+  for (auto &pr : ctx->kev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
   if (ctx->cfg.set_reference_pressure < 0) ctx->cfg.set_reference_pressure = 0;  // no pressure-specified patch types
   if ((rc = fs_geometry_build(ctx, mesh))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
   const size_t N = ctx->N, F = ctx->F, B = ctx->B, W = ctx->W;
@@ -232,6 +233,7 @@ int fs_destroy(fs_ctx *ctx) {
   for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto &e : ctx->tev) if (e) cudaEventDestroy(e);
   for (auto &pr : ctx->sev) { if (pr[0]) cudaEventDestroy(pr[0]); if (pr[1]) cudaEventDestroy(pr[1]); }
+  for (auto &pr : ctx->kev) { if (pr[0]) cudaEventDestroy(pr[0]); if (pr[1]) cudaEventDestroy(pr[1]); }
   if (ctx->st) cudaStreamDestroy(ctx->st);
   delete ctx;
   return FS_OK;
@@ -507,8 +509,16 @@ int fs_solver_stats(fs_ctx *ctx, float *ms5, int32_t *iters5, int32_t *calls5, i
     if (ms5) ms5[q] = ctx->s_ms[q];
     if (iters5) iters5[q] = ctx->s_its[q];
     if (calls5) calls5[q] = ctx->s_calls[q];
-    if (reset) { ctx->s_ms[q] = 0.f; ctx->s_its[q] = 0; ctx->s_calls[q] = 0; }
+    if (reset) { ctx->s_ms[q] = 0.f; ctx->s_its[q] = 0; ctx->s_calls[q] = 0; ctx->k_ms[q] = 0.f; }
   }
+  return FS_OK;
+}
+
+int fs_solver_kernel_ms(fs_ctx *ctx, float *ms5) {
+  if (!ctx || !ms5) return FS_E_ARG;
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  fs_solver_stats_collect(ctx);
+  for (int q = 0; q < 5; q++) ms5[q] = ctx->k_ms[q];
   return FS_OK;
 }
 

@@ -95,6 +95,8 @@ struct fs_ctx {
   cudaEvent_t sev[5][2] = {};              // around the solver launch of each NF
   bool s_pending[5] = {};
   float s_ms[5] = {};
+  cudaEvent_t kev[5][2] = {};              // around the main cooperative kernel of each solve
+  float k_ms[5] = {};
   int32_t s_its[5] = {}, s_calls[5] = {};
   cudaEvent_t ev[6] = {};
   float phase_ms[5] = {};

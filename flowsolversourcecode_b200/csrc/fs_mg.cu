@@ -1007,8 +1007,10 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.maxcycles = ctx->cfg.mg_max_cycles; a.b0 = ctx->bc; a.x0 = ctx->dphi; a.r0 = M->r[0];
     a.rrf = rrf; a.ires = ctx->resblk + RB_ABS + (nf - 1); a.part = M->red; a.iters = ctx->d_iters + (nf - 1);
     void *args[] = {&a};
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
     FS_CK(cudaLaunchCooperativeKernel((void *)k_mg_solve, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
     FS_LAUNCH_CHECK();
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
     return FS_OK;
   }
   if ((rc = mg_coarse_matrices(ctx, M->lc, f32))) return rc;
@@ -1033,15 +1035,18 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     fill(a);
     a.lev = M->lev64;
     void *args[] = {&a};
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
     FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<double>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
   } else {
     AmgKArgs<float> a{};
     fill(a);
     a.lev = M->lev32;
     void *args[] = {&a};
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
     FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<float>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
   }
   FS_LAUNCH_CHECK();
+  FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
   (void)rrf;
   return FS_OK;
 }
@@ -1062,5 +1067,16 @@ extern "C" int fs_mg_parents(fs_ctx *ctx, int level, int32_t *parents, size_t n)
   if (rc) return rc;
   if (level < 0 || level + 1 >= ctx->mg->nlev || n != ctx->mg->h_parent[level].size()) return FS_E_ARG;
   memcpy(parents, ctx->mg->h_parent[level].data(), sizeof(int32_t) * n);
+  return FS_OK;
+}
+
+extern "C" int fs_mg_info(fs_ctx *ctx, int32_t *widths, int max_levels, int32_t *prec_coarsest, int32_t *direct) {
+  if (!ctx) return FS_E_ARG;
+  int rc = fs_mg_build(ctx);
+  if (rc) return rc;
+  if (widths)
+    for (int q = 0; q < ctx->mg->nlev && q < max_levels; q++) widths[q] = ctx->mg->w[q];
+  if (prec_coarsest) *prec_coarsest = ctx->mg->lc;
+  if (direct) *direct = ctx->mg->direct ? 1 : 0;
   return FS_OK;
 }

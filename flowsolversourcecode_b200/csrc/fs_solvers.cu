@@ -506,13 +506,17 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
     if (need < G) G = (int)(need < 1 ? 1 : need);
     void *args[] = {&sp};
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
     FS_CK(cudaLaunchCooperativeKernel((void *)k_sor_colour, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
     FS_LAUNCH_CHECK();
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
     k_from_colour<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->dphiP, ctx->dphi);
     FS_LAUNCH_CHECK();
   } else if (solver == FS_SOLVER_BICGS) {
     a.itmax = ctx->cfg.krylov_maxit;
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
     rc = coop_launch(ctx, (void *)k_bicgstab, a);
+    FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
   } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS) {
     rc = fs_mg_solve(ctx, nf, rrf, solver);
   } else {
@@ -538,6 +542,9 @@ int fs_solver_stats_collect(fs_ctx *ctx) {
     float ms = 0.f;
     FS_CK(cudaEventElapsedTime(&ms, ctx->sev[q][0], ctx->sev[q][1]));
     ctx->s_ms[q] += ms; ctx->s_its[q] += it[q]; ctx->s_calls[q] += 1;
+    float kms = 0.f;
+    if (cudaEventElapsedTime(&kms, ctx->kev[q][0], ctx->kev[q][1]) == cudaSuccess) ctx->k_ms[q] += kms;
+    else cudaGetLastError();
     ctx->s_pending[q] = false;
   }
   return FS_OK;
@@ -651,7 +658,9 @@ int fs_momentum_batched_solve(fs_ctx *ctx) {
   long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
   if (need < G) G = (int)(need < 1 ? 1 : need);
   void *args[] = {&a};
+  FS_CK(cudaEventRecord(ctx->kev[0][0], ctx->st));
   FS_CK(cudaLaunchCooperativeKernel((void *)k_sor3_colour, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
+  FS_CK(cudaEventRecord(ctx->kev[0][1], ctx->st));
   FS_LAUNCH_CHECK();
   k_from_colour3<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->x3P, ctx->u, ctx->v, ctx->w);
   FS_LAUNCH_CHECK();

@@ -183,6 +183,19 @@ class Solver:
                   "connectivity")
         return out
 
+    def mg_info(self) -> dict:
+        """Multigrid hierarchy shapes: level sizes and ELL widths, and the
+        coarsest level of the AMG preconditioner (dense inverse when direct)."""
+        n = C.c_int()
+        sizes = np.zeros(16, np.int32)
+        widths = np.zeros(16, np.int32)
+        lc, direct = C.c_int(), C.c_int()
+        self._chk(self.lib.fs_mg_levels(self.ctx, C.byref(n), L.iptr(sizes), 16), "mg_levels")
+        self._chk(self.lib.fs_mg_info(self.ctx, L.iptr(widths), 16, C.byref(lc), C.byref(direct)), "mg_info")
+        k = n.value
+        return {"sizes": sizes[:k].tolist(), "widths": widths[:k].tolist(), "prec_coarsest": lc.value,
+                "direct": bool(direct.value)}
+
     def phase_times(self) -> list[float]:
         a = (C.c_float * 5)()
         self.lib.fs_phase_times(self.ctx, a)
@@ -197,11 +210,16 @@ class Solver:
         return ms.value
 
     def solver_stats(self, reset: bool = True) -> dict:
+        """Per NF (u, v, w, p', -): solve milliseconds (set-up kernels
+        included), linear iterations and calls since the last reset, and
+        `kernel_ms`, the main cooperative solver kernel alone."""
         ms = (C.c_float * 5)()
+        kms = (C.c_float * 5)()
         it = np.zeros(5, np.int32)
         calls = np.zeros(5, np.int32)
+        self._chk(self.lib.fs_solver_kernel_ms(self.ctx, kms), "solver_kernel_ms")
         self._chk(self.lib.fs_solver_stats(self.ctx, ms, L.iptr(it), L.iptr(calls), int(reset)), "solver_stats")
-        return {"ms": list(ms), "iters": it.tolist(), "calls": calls.tolist()}
+        return {"ms": list(ms), "iters": it.tolist(), "calls": calls.tolist(), "kernel_ms": list(kms)}
 
     def launch_count(self) -> int:
         return int(self.lib.fs_launch_count(self.ctx))

@@ -254,6 +254,10 @@ int fs_get_connectivity(fs_ctx *ctx, int32_t *n_cell_faces, int32_t *cell_faces,
  * level sizes, and the parent map of level l -> l+1 (0-based). */
 int fs_mg_levels(fs_ctx *ctx, int32_t *n_levels, int32_t *level_sizes, int max_levels);
 int fs_mg_parents(fs_ctx *ctx, int level, int32_t *parents, size_t n);
+/* Level shapes (no reference counterpart; diagnostics and the byte counts of
+ * the bench roofline): ELL width of each level and the coarsest level the
+ * AMG preconditioner cycles to (inverted densely when *direct is 1). */
+int fs_mg_info(fs_ctx *ctx, int32_t *widths, int max_levels, int32_t *prec_coarsest, int32_t *direct);
 
 /* Timing of the last outer iteration's phases in milliseconds (CUDA events):
  * [0] momentum assembly, [1] momentum solves, [2] continuity assembly,
@@ -268,6 +272,10 @@ int fs_timer_stop(fs_ctx *ctx, float *ms);
  * device time of the solver kernels (CUDA events around each launch, in ms),
  * solver iterations, and calls.  reset=1 clears them after reading. */
 int fs_solver_stats(fs_ctx *ctx, float *ms5, int32_t *iters5, int32_t *calls5, int reset);
+/* Milliseconds of the main cooperative solver kernel alone (no set-up
+ * kernels) per NF, accumulated like fs_solver_stats and reset with it.  No
+ * reference counterpart (roofline timing). */
+int fs_solver_kernel_ms(fs_ctx *ctx, float *ms5);
 /* Number of kernel launches issued by this context since creation. */
 int64_t fs_launch_count(const fs_ctx *ctx);
 /* Synchronise the context stream. */
