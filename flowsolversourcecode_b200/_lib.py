@@ -21,6 +21,7 @@ FS_OK, FS_E_ARG, FS_E_CUDA, FS_E_NOMEM, FS_E_NAN, FS_E_DIVERGED, FS_E_TIMEOUT, F
     0, -1, -2, -3, -4, -5, -6, -7, -8)
 FS_E_TOO_LARGE = -9
 FS_NOALLOC_MAX_ROWS = 262144
+FS_NN_NPARAM = 33665
 # variable ids (GetNFfromVariable)
 VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
 # boundary types
@@ -114,6 +115,14 @@ PROTOTYPES = {
     "fs_mg_parents": (C.c_int, [_V, C.c_int, _I, C.c_size_t]),
     "fs_mg_info": (C.c_int, [_V, _I, C.c_int, _I, _I]),
     "fs_solver_kernel_ms": (C.c_int, [_V, C.POINTER(C.c_float)]),
+    "fs_nn_create": (C.c_int, [_V, C.c_int, C.c_uint64]),
+    "fs_nn_mode": (C.c_int, [_V, C.c_int, C.c_int]),
+    "fs_nn_snapshots": (C.c_int, [_V, _I]),
+    "fs_nn_train": (C.c_int, [_V, C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "fs_nn_params": (C.c_int, [_V, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_size_t]),
+    "fs_nn_eval_host": (C.c_int, [_V] + [C.POINTER(C.c_float)] * 6),
+    "fs_nn_stats": (C.c_int, [_V, _I, _I]),
+    "fs_nn_policy": (C.c_int, [_V, _D, _D, _I]),
     "fs_phase_times": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "fs_timer_start": (C.c_int, [_V]),
     "fs_timer_stop": (C.c_int, [_V, C.POINTER(C.c_float)]),
@@ -150,6 +159,13 @@ def dptr(a: np.ndarray):
 def iptr(a: np.ndarray):
     assert a.dtype == np.int32 and a.flags.c_contiguous
     return a.ctypes.data_as(_I)
+
+
+def fptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
 class FsError(RuntimeError):

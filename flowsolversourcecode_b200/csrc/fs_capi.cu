@@ -229,6 +229,7 @@ int fs_destroy(fs_ctx *ctx) {
   cudaSetDevice(ctx->dev);
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   fs_mg_free(ctx);
+  fs_nn_free(ctx);
   free_all(ctx);
   for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto &e : ctx->tev) if (e) cudaEventDestroy(e);
@@ -258,12 +259,23 @@ int fs_solve_momentum(fs_ctx *ctx, int comp) {
   return fs_linear_solve(ctx, comp + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom);
 }
 
+// the p' solve, with the learned initial guess when one is enabled
+static int pc_solve(fs_ctx *ctx) {
+  const double *x0 = nullptr;
+  int rc = fs_nn_before_pc(ctx, &x0);
+  if (rc) return rc;
+  ctx->pc_guess = x0;
+  rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
+  ctx->pc_guess = nullptr;
+  if (rc) return rc;
+  return fs_nn_after_pc(ctx);
+}
+
 int fs_solve_continuity(fs_ctx *ctx) {
   if (!ctx) return FS_E_ARG;
   int rc = fs_continuity_assemble(ctx);
   if (rc) return rc;
-  rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
-  if (rc) return rc;
+  if ((rc = pc_solve(ctx))) return rc;
   return fs_continuity_correct(ctx);
 }
 
@@ -291,6 +303,7 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
     r.abs_[q] = rb[RB_ABS + q]; r.max_[q] = rb[RB_MAX + q]; r.rms[q] = rb[RB_RMS + q]; r.scaled[q] = rb[RB_SCL + q];
     r.lin_iters[q] = it[q];
   }
+  if (ctx->nn) fs_nn_note_iters(ctx, it[FS_VAR_PC - 1]);
   r.overall_imbalance = rb[RB_OVERALL];
   r.imax_imbalance = (int)rb[RB_IMAX];
   // PrintConvergenceHistory stop metric (PrintConvergenceToFileAndScreen.for:613-700)
@@ -326,7 +339,7 @@ int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res) {
   cudaEventRecord(ctx->ev[1], ctx->st);
   if ((rc = fs_continuity_assemble(ctx))) return rc;
   cudaEventRecord(ctx->ev[2], ctx->st);
-  if ((rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont))) return rc;
+  if ((rc = pc_solve(ctx))) return rc;
   cudaEventRecord(ctx->ev[3], ctx->st);
   if ((rc = fs_continuity_correct(ctx))) return rc;
   cudaEventRecord(ctx->ev[4], ctx->st);

@@ -29,6 +29,7 @@
 enum { RED_SUM0 = 0, RED_SUM1, RED_SUM2, RED_MAX0, RED_MAX1, RED_NQ };
 
 struct fs_mg_dev;  // multigrid hierarchy (fs_mg.cu)
+struct fs_nn;      // learned p' initial guess (fs_nn.cu)
 
 struct fs_ctx {
   int dev = 0;
@@ -89,6 +90,9 @@ struct fs_ctx {
 
   // multigrid
   fs_mg_dev *mg = nullptr;
+  // learned initial guess of the p' solve (nullptr: zero guess)
+  fs_nn *nn = nullptr;
+  const double *pc_guess = nullptr;   // set around the p' solve only
 
   // timing
   cudaEvent_t tev[2] = {};                 // fs_timer_start / fs_timer_stop
@@ -145,7 +149,12 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
 int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);
 int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);
-int fs_solver_stats_collect(fs_ctx *ctx);   // after a stream sync: fold pending solver events
+int fs_solver_stats_collect(fs_ctx *ctx);
+int fs_nn_before_pc(fs_ctx *ctx, const double **x0);   // features (+ guess) before the p' solve
+int fs_nn_after_pc(fs_ctx *ctx);                        // snapshot capture, previous p'
+void fs_nn_free(fs_ctx *ctx);
+int32_t *fs_nn_counters(fs_ctx *ctx);                   // device [fallbacks, uses] or nullptr
+void fs_nn_note_iters(fs_ctx *ctx, int pc_iters);       // iterations of the last p' solve (policy)   // after a stream sync: fold pending solver events
 
 #ifdef __CUDACC__
 // Row i of a slot-major ELL table (n rows, width w; unused slots hold index -1):

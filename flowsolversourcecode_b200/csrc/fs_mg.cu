@@ -543,6 +543,8 @@ struct AmgKArgs {
   double *part;
   int32_t *iters;
   double *diag;
+  const double *x0;   // initial guess (nullptr: zero)
+  int32_t *nncnt;     // [fallbacks, uses] of the initial guess, or nullptr
 };
 
 // rows i and i2 (when h2) of A x at once (ell_acc2)
@@ -569,18 +571,45 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   const int N = a.N;
   Scope g; g.grid = true;
   const long t0 = g.tid0(), nt = g.nth();
-  double l0 = 0., l1 = 0.;
+  // start from the initial guess scaled by the c that minimises |b - c A x0|
+  // (c = (A x0 . b) / (A x0 . A x0), so |r0| <= |b|), or from zero.  A guess
+  // with c not finite or zero falls back to the zero start (same decision in
+  // every CTA: the sums are grid-deterministic).  Whether guesses pay is judged
+  // on iteration counts by the host policy (fs_nn.cu).
+  double l0 = 0., l1 = 0., l2 = 0.;
+  for (long i = t0; i < N; i += 2 * nt) {
+    const long i2 = i + nt;
+    const bool h2 = i2 < N;
+    double q1 = 0., q2 = 0.;
+    if (a.x0) row_ax2(a, i, i2, h2, a.x0, q1, q2);
+    const double b1 = a.bc[i];
+    a.r[i] = q1;
+    l0 += q1 * b1; l1 += q1 * q1; l2 += b1 * b1;
+    if (h2) {
+      const double b2 = a.bc[i2];
+      a.r[i2] = q2;
+      l0 += q2 * b2; l1 += q2 * q2; l2 += b2 * b2;
+    }
+  }
+  double qb, qq, bb, dum;
+  S.sum2(l0, l1, qb, qq);
+  S.sum2(l2, 0., bb, dum);
+  double c = (a.x0 && qq > 0.) ? qb / qq : 0.;
+  if (!isfinite(c)) c = 0.;
+  const bool fell_back = a.x0 && c == 0.;
+  l0 = 0.;
   for (long i = t0; i < N; i += nt) {
-    a.x[i] = 0.;
-    double ri = a.bc[i];
-    a.r[i] = ri; a.r0[i] = ri; a.p[i] = 0.; a.v[i] = 0.;
+    const double xi = a.x0 ? c * a.x0[i] : 0.;
+    const double ri = a.bc[i] - c * a.r[i];
+    a.x[i] = xi; a.r[i] = ri; a.r0[i] = ri; a.p[i] = 0.; a.v[i] = 0.;
     l0 += ri * ri;
   }
-  double rr, dum;
+  double rr;
   S.sum2(l0, 0., rr, dum);
-  double normb = sqrt(rr), rho = 1., alpha = 1., omega = 1.;
+  if (a.nncnt && a.x0 && blockIdx.x == 0 && threadIdx.x == 0) { a.nncnt[1] += 1; if (fell_back) a.nncnt[0] += 1; }
+  double normb = sqrt(bb), rho = 1., alpha = 1., omega = 1.;
   int k = 0;
-  double resn = normb;
+  double resn = sqrt(rr);
   while (k < a.maxit && resn > a.tol * normb && normb > 0.) {
     k++;
     l0 = 0.;
@@ -1029,6 +1058,8 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_pre);
     a.maxit = ctx->cfg.krylov_maxit; a.tol = ctx->cfg.krylov_tol; a.part = M->red;
     a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + 22;
+    a.x0 = nf == FS_VAR_PC ? ctx->pc_guess : nullptr;
+    a.nncnt = fs_nn_counters(ctx);
   };
   if (!f32) {
     AmgKArgs<double> a{};

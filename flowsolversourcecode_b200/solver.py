@@ -196,6 +196,54 @@ class Solver:
         return {"sizes": sizes[:k].tolist(), "widths": widths[:k].tolist(), "prec_coarsest": lc.value,
                 "direct": bool(direct.value)}
 
+    # ------------------------------------------------------------ learned p' guess
+    def nn_create(self, snapshot_capacity: int = 0, seed: int = 0):
+        """Network for the learned p' initial guess, with room for
+        `snapshot_capacity` training snapshots of this mesh."""
+        self._chk(self.lib.fs_nn_create(self.ctx, snapshot_capacity, seed), "fs_nn_create")
+
+    def nn_mode(self, capture: bool = False, use: bool = False):
+        self._chk(self.lib.fs_nn_mode(self.ctx, int(capture), int(use)), "fs_nn_mode")
+
+    def nn_snapshots(self) -> int:
+        n = C.c_int32()
+        self._chk(self.lib.fs_nn_snapshots(self.ctx, C.byref(n)), "fs_nn_snapshots")
+        return n.value
+
+    def nn_train(self, epochs: int, lr: float = 1e-3, seed: int = 0) -> tuple[float, float]:
+        a, b = C.c_float(), C.c_float()
+        self._chk(self.lib.fs_nn_train(self.ctx, epochs, lr, seed, C.byref(a), C.byref(b)), "fs_nn_train")
+        return a.value, b.value
+
+    def nn_params(self, set: np.ndarray | None = None) -> np.ndarray:
+        out = np.zeros(L.FS_NN_NPARAM, np.float32)
+        s = None if set is None else np.ascontiguousarray(set, np.float32)
+        self._chk(self.lib.fs_nn_params(self.ctx, L.fptr(out), L.fptr(s), L.FS_NN_NPARAM), "fs_nn_params")
+        return out
+
+    def nn_eval(self, X: np.ndarray, wgt: np.ndarray, target: np.ndarray | None = None) -> dict:
+        """Forward (and with a target, loss and gradient) on host inputs."""
+        X = np.ascontiguousarray(X, np.float32)
+        wgt = np.ascontiguousarray(wgt, np.float32)
+        t = None if target is None else np.ascontiguousarray(target, np.float32)
+        loss = np.zeros(1, np.float32)
+        grad = np.zeros(L.FS_NN_NPARAM, np.float32)
+        y = np.zeros(self.N, np.float32)
+        self._chk(self.lib.fs_nn_eval_host(self.ctx, L.fptr(X), L.fptr(wgt), L.fptr(t), L.fptr(loss),
+                                           L.fptr(grad), L.fptr(y)), "fs_nn_eval_host")
+        return {"y": y, "loss": float(loss[0]) if t is not None else None, "grad": grad if t is not None else None}
+
+    def nn_stats(self) -> dict:
+        """Guessed p' solves, guesses dropped by the residual guard, the
+        policy's average iterations with the guess and from zero, and how
+        often the guess was parked for not reducing iterations."""
+        u, f = C.c_int32(), C.c_int32()
+        g, z, p = C.c_double(), C.c_double(), C.c_int32()
+        self._chk(self.lib.fs_nn_stats(self.ctx, C.byref(u), C.byref(f)), "fs_nn_stats")
+        self._chk(self.lib.fs_nn_policy(self.ctx, C.byref(g), C.byref(z), C.byref(p)), "fs_nn_policy")
+        return {"uses": u.value, "fallbacks": f.value, "avg_iters_guessed": g.value, "avg_iters_zero": z.value,
+                "parked": p.value}
+
     def phase_times(self) -> list[float]:
         a = (C.c_float * 5)()
         self.lib.fs_phase_times(self.ctx, a)

@@ -259,6 +259,40 @@ int fs_mg_parents(fs_ctx *ctx, int level, int32_t *parents, size_t n);
  * AMG preconditioner cycles to (inverted densely when *direct is 1). */
 int fs_mg_info(fs_ctx *ctx, int32_t *widths, int max_levels, int32_t *prec_coarsest, int32_t *direct);
 
+/* ----------------------------------------------------- learned p' initial guess
+ * No reference counterpart: the reference starts every p' solve from zero.
+ * A 4-layer message-passing network on the cell graph (hidden width 64, BF16
+ * tensor-core layer products with FP32 accumulation) maps features of the p'
+ * system (mass imbalance, coefficients, velocity-gradient diagonal, previous
+ * p') to an initial guess for the AMG-preconditioned BiCGSTAB solvers, which
+ * scale it by the c minimising |b - c A x0| (so |r0| <= |b|) and still
+ * iterate to their tolerance relative to |b|.
+ *   fs_nn_create     network (seeded init, untrained guess = 0) and room for
+ *                    snapshot_capacity training snapshots of this mesh
+ *   fs_nn_mode       capture: store (features, edge weights, converged p')
+ *                    after every p' solve; use: seed the p' solves
+ *   fs_nn_train      epochs of Adam over the stored snapshots on the GPU;
+ *                    mean relative loss of the first and last epoch
+ *   fs_nn_params     copy the FS_NN_NPARAM parameters out (get) and/or in (set)
+ *   fs_nn_eval_host  forward (and, with target, loss + gradient) on host
+ *                    inputs X [N x 8], edge weights [W*N slot-major], target [N]
+ *   fs_nn_stats      p' solves seeded by the network, and how many fell back
+ *                    to zero (scale c zero or not finite)
+ *   fs_nn_policy     the guess is used only while it reduces iterations
+ *                    against zero-start probes (every 4th solve): average
+ *                    p' iterations with the guess and from zero, and how often
+ *                    the guess was parked */
+#define FS_NN_NPARAM 33665
+int fs_nn_create(fs_ctx *ctx, int snapshot_capacity, uint64_t seed);
+int fs_nn_mode(fs_ctx *ctx, int capture, int use);
+int fs_nn_snapshots(fs_ctx *ctx, int32_t *count);
+int fs_nn_train(fs_ctx *ctx, int epochs, float lr, uint64_t seed, float *loss_first, float *loss_last);
+int fs_nn_params(fs_ctx *ctx, float *get, const float *set, size_t n);
+int fs_nn_eval_host(fs_ctx *ctx, const float *X, const float *wgt, const float *target, float *loss, float *grad,
+                    float *y);
+int fs_nn_stats(fs_ctx *ctx, int32_t *uses, int32_t *fallbacks);
+int fs_nn_policy(fs_ctx *ctx, double *avg_guessed, double *avg_zero, int32_t *parked);
+
 /* Timing of the last outer iteration's phases in milliseconds (CUDA events):
  * [0] momentum assembly, [1] momentum solves, [2] continuity assembly,
  * [3] p' solve, [4] corrections+residuals. */
