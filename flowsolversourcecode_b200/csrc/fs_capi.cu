@@ -291,6 +291,16 @@ int fs_set_iteration(fs_ctx *ctx, int n_iter) {
   return FS_OK;
 }
 
+// PrintConvergenceHistory stop metric (PrintConvergenceToFileAndScreen.for:613-700)
+// from a device residual block
+static double stop_metric(const fs_case &c, const double *rb) {
+  const int o = c.nstop_type == 1 ? RB_ABS : c.nstop_type == 2 ? RB_MAX : c.nstop_type == 3 ? RB_RMS : RB_SCL;
+  double s = 0.;
+  s = fmax(s, fmax(fabs(rb[o]), fmax(fabs(rb[o + 1]), fabs(rb[o + 2]))));
+  s = fmax(s, fabs(rb[o + 4]));
+  return s;
+}
+
 static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   double rb[RB_SIZE];
   int32_t it[8];
@@ -306,25 +316,17 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   if (ctx->nn) fs_nn_note_iters(ctx, it[FS_VAR_PC - 1]);
   r.overall_imbalance = rb[RB_OVERALL];
   r.imax_imbalance = (int)rb[RB_IMAX];
-  // PrintConvergenceHistory stop metric (PrintConvergenceToFileAndScreen.for:613-700)
-  const double *v = ctx->cfg.nstop_type == 1 ? r.abs_ : ctx->cfg.nstop_type == 2 ? r.max_ :
-                    ctx->cfg.nstop_type == 3 ? r.rms : r.scaled;
-  double s = 0.;
-  s = fmax(s, fmax(fabs(v[0]), fmax(fabs(v[1]), fabs(v[2]))));
-  s = fmax(s, fabs(v[4]));
-  r.source = s;
+  r.source = stop_metric(ctx->cfg, rb);
   if (res) *res = r;
   for (int q = 0; q < 5; q++)
     if (!std::isfinite(r.abs_[q])) { ctx->err = "NaN/Inf residual"; return FS_E_NAN; }
   return FS_OK;
 }
 
-int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res) {
-  if (!ctx) return FS_E_ARG;
-  cudaSetDevice(ctx->dev);
-  ctx->nIter++;
+// one SIMPLE outer iteration enqueued on the context stream (MainProgram.for:257-325)
+static int iteration_body(fs_ctx *ctx) {
   int rc;
-  cudaEventRecord(ctx->ev[0], ctx->st);
+  FS_TIMING(cudaEventRecord(ctx->ev[0], ctx->st));
   if (ctx->cfg.batched_momentum && ctx->cfg.solver_mom == FS_SOLVER_SOR) {
     for (int c = 0; c < 3; c++)
       if ((rc = fs_momentum_assemble_to(ctx, c, ctx->ac3 + (size_t)c * ctx->N, ctx->bc3 + (size_t)c * ctx->N))) return rc;
@@ -336,13 +338,32 @@ int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res) {
       if ((rc = fs_linear_solve(ctx, c + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom))) return rc;
     }
   }
-  cudaEventRecord(ctx->ev[1], ctx->st);
+  FS_TIMING(cudaEventRecord(ctx->ev[1], ctx->st));
   if ((rc = fs_continuity_assemble(ctx))) return rc;
-  cudaEventRecord(ctx->ev[2], ctx->st);
-  if ((rc = pc_solve(ctx))) return rc;
-  cudaEventRecord(ctx->ev[3], ctx->st);
+  FS_TIMING(cudaEventRecord(ctx->ev[2], ctx->st));
+  // the learned guess needs host-side bookkeeping per solve: not in captured graphs
+  if (ctx->graph_mode)
+    rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
+  else
+    rc = pc_solve(ctx);
+  if (rc) return rc;
+  FS_TIMING(cudaEventRecord(ctx->ev[3], ctx->st));
   if ((rc = fs_continuity_correct(ctx))) return rc;
-  cudaEventRecord(ctx->ev[4], ctx->st);
+  FS_TIMING(cudaEventRecord(ctx->ev[4], ctx->st));
+  return FS_OK;
+}
+
+static int iteration_enqueue(fs_ctx *ctx) {
+  ctx->nIter++;
+  return iteration_body(ctx);
+}
+
+int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res) {
+  if (!ctx) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  ctx->nIter++;
+  int rc = iteration_body(ctx);
+  if (rc) return rc;
   rc = read_residuals(ctx, res);
   cudaEventElapsedTime(&ctx->phase_ms[0], ctx->ev[0], ctx->ev[1]);
   cudaEventElapsedTime(&ctx->phase_ms[2], ctx->ev[1], ctx->ev[2]);
@@ -538,6 +559,111 @@ int fs_solver_kernel_ms(fs_ctx *ctx, float *ms5) {
 int fs_sync(fs_ctx *ctx) {
   if (!ctx) return FS_E_ARG;
   FS_CK(cudaStreamSynchronize(ctx->st));
+  return FS_OK;
+}
+
+// Ensemble of independent cases (no reference counterpart): `iters` SIMPLE
+// iterations of every case captured into ONE CUDA graph -- the cases in
+// sequence, so their cooperative solver kernels never run concurrently -- and
+// the graph launched `launches` times, one host synchronisation per launch.
+// Residual blocks and linear iteration counts of every captured iteration go to
+// pinned host memory by copies inside the graph.  source_out[q*T + t] is the
+// stop metric of case q after its t-th run iteration (T = iters*launches),
+// pc_iters_out (optional) the p' iterations, ms_out the device time of the
+// launches.  The learned guess is not used inside the graph.
+int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
+                    float *ms_out) {
+  if (!cs || n < 1 || iters < 1 || launches < 1 || !source_out) return FS_E_ARG;
+  fs_ctx *c0 = cs[0];
+  for (int q = 0; q < n; q++)
+    if (!cs[q] || cs[q]->dev != c0->dev) return FS_E_ARG;
+  cudaSetDevice(c0->dev);
+  fs_ctx *ctx = c0;  // FS_CK reports into the first context
+  // one ordinary iteration per case builds hierarchies, colourings and grids
+  // (nothing may allocate during capture); the HR start must already be passed
+  for (int q = 0; q < n; q++) {
+    fs_ctx *c = cs[q];
+    do {
+      fs_residuals r;
+      int rc = fs_simple_iteration(c, &r);
+      if (rc) { if (c != ctx) ctx->err = c->err; return rc; }
+    } while (c->nIter < c->cfg.niter_start_hr);
+  }
+  const size_t slot = RB_SIZE + 4;  // residual block, then 8 int32 iteration counts
+  double *h = nullptr;
+  FS_CK(cudaHostAlloc((void **)&h, sizeof(double) * slot * n * iters, cudaHostAllocDefault));
+  cudaStream_t S = nullptr;
+  cudaEvent_t ej = nullptr, e0 = nullptr, e1 = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  std::vector<int> nit0(n);
+  int rc = FS_OK;
+  auto cleanup = [&]() {
+    if (x) cudaGraphExecDestroy(x);
+    if (g) cudaGraphDestroy(g);
+    if (ej) cudaEventDestroy(ej);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (S) cudaStreamDestroy(S);
+    cudaFreeHost(h);
+  };
+  auto fail = [&](const char *what, cudaError_t e) {
+    ctx->err = std::string(what) + ": " + cudaGetErrorString(e);
+    cleanup();
+    return FS_E_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&S, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", e);
+  if ((e = cudaEventCreateWithFlags(&ej, cudaEventDisableTiming)) != cudaSuccess) return fail("event", e);
+  if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) return fail("event", e);
+  for (int q = 0; q < n; q++) nit0[q] = cs[q]->nIter;
+  for (int q = 0; q < n; q++)
+    if ((e = cudaStreamSynchronize(cs[q]->st)) != cudaSuccess) return fail("before capture", e);
+  (void)cudaGetLastError();  // no stale error may be reported by a launch check inside the capture
+  if ((e = cudaStreamBeginCapture(S, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return fail("capture", e);
+  const char *what = nullptr;
+  for (int t = 0; t < iters && rc == FS_OK && !what; t++)
+    for (int q = 0; q < n && rc == FS_OK && !what; q++) {
+      fs_ctx *c = cs[q];
+      if ((e = cudaEventRecord(ej, S)) != cudaSuccess) { what = "join record"; break; }
+      if ((e = cudaStreamWaitEvent(c->st, ej, 0)) != cudaSuccess) { what = "join wait"; break; }
+      c->graph_mode = true;
+      rc = iteration_enqueue(c);
+      c->graph_mode = false;
+      if (rc != FS_OK) { if (c != ctx) ctx->err = c->err; break; }
+      double *d = h + ((size_t)q * iters + t) * slot;
+      if ((e = cudaMemcpyAsync(d, c->resblk, sizeof(double) * RB_SIZE, cudaMemcpyDeviceToHost, c->st)) != cudaSuccess ||
+          (e = cudaMemcpyAsync(d + RB_SIZE, c->d_iters, sizeof(int32_t) * 8, cudaMemcpyDeviceToHost, c->st)) !=
+              cudaSuccess) { what = "residual copy"; break; }
+      if ((e = cudaEventRecord(ej, c->st)) != cudaSuccess) { what = "rejoin record"; break; }
+      if ((e = cudaStreamWaitEvent(S, ej, 0)) != cudaSuccess) { what = "rejoin wait"; break; }
+    }
+  cudaError_t ec = cudaStreamEndCapture(S, &g);
+  for (int q = 0; q < n; q++) cs[q]->nIter = nit0[q];
+  if (what) return fail(what, e);
+  if (rc != FS_OK) { cleanup(); return rc; }
+  if (ec != cudaSuccess) return fail("capture", ec);
+  if ((e = cudaGraphInstantiate(&x, g, 0)) != cudaSuccess) return fail("instantiate", e);
+  const int T = iters * launches;
+  cudaEventRecord(e0, S);
+  for (int L = 0; L < launches; L++) {
+    if ((e = cudaGraphLaunch(x, S)) != cudaSuccess) return fail("graph launch", e);
+    if ((e = cudaStreamSynchronize(S)) != cudaSuccess) return fail("graph run", e);
+    for (int q = 0; q < n; q++)
+      for (int t = 0; t < iters; t++) {
+        const double *d = h + ((size_t)q * iters + t) * slot;
+        const int k = L * iters + t;
+        source_out[(size_t)q * T + k] = stop_metric(cs[q]->cfg, d);
+        if (pc_iters_out) pc_iters_out[(size_t)q * T + k] = ((const int32_t *)(d + RB_SIZE))[FS_VAR_PC - 1];
+      }
+  }
+  cudaEventRecord(e1, S);
+  if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return fail("graph run", e);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  if (ms_out) *ms_out = ms;
+  for (int q = 0; q < n; q++) cs[q]->nIter = nit0[q] + T;
+  cleanup();
   return FS_OK;
 }
 

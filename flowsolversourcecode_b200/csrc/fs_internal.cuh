@@ -105,7 +105,15 @@ struct fs_ctx {
   cudaEvent_t ev[6] = {};
   float phase_ms[5] = {};
   int coop_grid = 0;            // blocks of a cooperative solver launch
+  int coop_per_sm = 0;          // launch shape: cooperative CTAs per SM (0: up to 4; fs_set_launch_shape)
+  bool graph_mode = false;      // enqueueing for stream capture: no host syncs, no timing events
 };
+
+// timing events and their host-side bookkeeping are skipped while a graph is captured
+#define FS_TIMING(stmt)                                                      \
+  do {                                                                       \
+    if (!ctx->graph_mode) { stmt; }                                          \
+  } while (0)
 
 // residual block layout on the device (double resblk[RB_SIZE])
 enum { RB_ABS = 0, RB_MAX = 5, RB_RMS = 10, RB_SCL = 15, RB_OVERALL = 20, RB_IMAX = 21, RB_SIZE = 24 };
@@ -119,15 +127,33 @@ enum { RB_ABS = 0, RB_MAX = 5, RB_RMS = 10, RB_SCL = 15, RB_OVERALL = 20, RB_IMA
     }                                                                        \
   } while (0)
 
+#define FS_STR2(x) #x
+#define FS_STR(x) FS_STR2(x)
 #define FS_LAUNCH_CHECK()                                                    \
   do {                                                                       \
     ctx->launches++;                                                         \
     cudaError_t e__ = cudaGetLastError();                                    \
     if (e__ != cudaSuccess) {                                                \
-      ctx->err = std::string("launch: ") + cudaGetErrorString(e__);         \
+      ctx->err = std::string("launch (" __FILE__ ":" FS_STR(__LINE__) "): ") + cudaGetErrorString(e__); \
       return FS_E_CUDA;                                                      \
     }                                                                        \
   } while (0)
+
+// A cooperative (grid-synchronising) launch in the form stream capture
+// accepts: cudaLaunchKernelExC with the cooperative launch attribute.
+static inline cudaError_t fs_coop_launch(const void *fn, int grid, int block, void **args, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, fn, args);
+}
 
 static inline int fs_grid(long n, int block = FS_BLOCK) {
   long g = (n + block - 1) / block;
@@ -150,6 +176,7 @@ int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);
 int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);
 int fs_solver_stats_collect(fs_ctx *ctx);
+int fs_coop_per_sm(fs_ctx *ctx, int occupancy);         // CTAs per SM for a cooperative launch
 int fs_nn_before_pc(fs_ctx *ctx, const double **x0);   // features (+ guess) before the p' solve
 int fs_nn_after_pc(fs_ctx *ctx);                        // snapshot capture, previous p'
 void fs_nn_free(fs_ctx *ctx);

@@ -82,7 +82,7 @@ struct fs_mg_dev {
   LevelDev<double> *lev64 = nullptr;
   LevelDev<float> *lev32 = nullptr;
   double *red = nullptr;                // partial sums
-  int grid = 0;
+  int per_sm = 0;                       // co-resident CTAs per SM of the multigrid kernels
 };
 
 namespace {
@@ -972,8 +972,10 @@ int fs_mg_build(fs_ctx *ctx) {
   if (M->direct) {
     size_t nn = (size_t)M->n[M->lc] * M->n[M->lc];
     FS_CK(cudaMalloc(&M->sinv, sizeof(double) * nn));
+    // the attribute belongs to the function, shared by every context of the
+    // process: set it for the largest coarsest level any context may have
     FS_CK(cudaFuncSetAttribute((const void *)k_mg_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(sizeof(double) * (nn + M->n[M->lc]))));
+                               (int)(sizeof(double) * ((size_t)FS_MG_DIRECT * FS_MG_DIRECT + FS_MG_DIRECT))));
   }
   // cooperative grid: smallest co-resident count of the three kernels, <= 4 CTAs/SM
   int a = 0, b = 0, c = 0;
@@ -982,8 +984,7 @@ int fs_mg_build(fs_ctx *ctx) {
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float>, FS_COOP_BLOCK, 0));
   int per = std::min(a, std::min(b, c));
   if (per < 1) { ctx->err = "multigrid kernels do not fit on an SM"; return FS_E_CUDA; }
-  M->grid = ctx->num_sms * std::min(per, 4);
-  M->grid = std::min(M->grid, FS_RED_BLOCKS);
+  M->per_sm = per;   // occupancy limit; the grid follows the launch shape at each solve
   return FS_OK;
 }
 
@@ -1028,7 +1029,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
   if (rc) return rc;
   fs_mg_dev *M = ctx->mg;
   const bool f32 = solver == FS_SOLVER_AMG32_BICGS;
-  int G = M->grid;
+  const int G = std::min(ctx->num_sms * fs_coop_per_sm(ctx, M->per_sm), FS_RED_BLOCKS);
   if (solver == FS_SOLVER_AMG) {
     if ((rc = mg_coarse_matrices(ctx, M->nlev - 1, false))) return rc;
     MgSolveArgs a{};
@@ -1036,10 +1037,10 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.maxcycles = ctx->cfg.mg_max_cycles; a.b0 = ctx->bc; a.x0 = ctx->dphi; a.r0 = M->r[0];
     a.rrf = rrf; a.ires = ctx->resblk + RB_ABS + (nf - 1); a.part = M->red; a.iters = ctx->d_iters + (nf - 1);
     void *args[] = {&a};
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_mg_solve, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
+    FS_CK(fs_coop_launch((const void *)k_mg_solve, G, FS_COOP_BLOCK, args, ctx->st));
     FS_LAUNCH_CHECK();
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
     return FS_OK;
   }
   if ((rc = mg_coarse_matrices(ctx, M->lc, f32))) return rc;
@@ -1066,18 +1067,18 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     fill(a);
     a.lev = M->lev64;
     void *args[] = {&a};
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<double>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
+    FS_CK(fs_coop_launch((const void *)k_amg_bicgstab<double>, G, FS_COOP_BLOCK, args, ctx->st));
   } else {
     AmgKArgs<float> a{};
     fill(a);
     a.lev = M->lev32;
     void *args[] = {&a};
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_amg_bicgstab<float>, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
+    FS_CK(fs_coop_launch((const void *)k_amg_bicgstab<float>, G, FS_COOP_BLOCK, args, ctx->st));
   }
   FS_LAUNCH_CHECK();
-  FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
+  FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
   (void)rrf;
   return FS_OK;
 }

@@ -724,7 +724,8 @@ __global__ void __launch_bounds__(FS_BLOCK) k_mass_imbalance(CorrArgs a) {
   }
 }
 
-__global__ void k_mass_final(CorrArgs a, double mdot_in) {
+// mdot_in_dev: inlet mass flow on the device (nullptr: no inlet)
+__global__ void k_mass_final(CorrArgs a, const double *mdot_in_dev) {
   __shared__ double sh[32];
   __shared__ int64_t shi[1024];
   __shared__ double shm[1024];
@@ -748,6 +749,7 @@ __global__ void k_mass_final(CorrArgs a, double mdot_in) {
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+    const double mdot_in = mdot_in_dev ? *mdot_in_dev : 0.;
     double mxv = shm[0] < 0. ? 0. : shm[0];
     a.rb[RB_ABS + 4] = s1;
     a.rb[RB_MAX + 4] = mxv;
@@ -938,18 +940,16 @@ int fs_continuity_correct(fs_ctx *ctx) {
   if (B) { k_bcorr<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   k_mass_imbalance<<<a.nblk, FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();
-  double mdot_in = 0.;
   bool has_inlet = false;
   for (int s = 0; s < ctx->NS; s++) if (c.patch_type[s] == FS_BC_INLET_VEL) has_inlet = true;
+  double *d_in = nullptr;
   if (has_inlet) {
-    // inlet mass flow is needed on the host only through ResorScaled(5)
-    double *d = ctx->resblk + RB_SIZE - 1;
-    k_sum_inlet<<<1, 32, 0, ctx->st>>>(B, ctx->btype, ctx->bmdot, d);
+    // inlet mass flow, used only through ResorScaled(5); stays on the device
+    d_in = ctx->resblk + RB_SIZE - 1;
+    k_sum_inlet<<<1, 32, 0, ctx->st>>>(B, ctx->btype, ctx->bmdot, d_in);
     FS_LAUNCH_CHECK();
-    FS_CK(cudaMemcpyAsync(&mdot_in, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-    FS_CK(cudaStreamSynchronize(ctx->st));
   }
-  k_mass_final<<<1, 1024, 0, ctx->st>>>(a, mdot_in);
+  k_mass_final<<<1, 1024, 0, ctx->st>>>(a, d_in);
   FS_LAUNCH_CHECK();
   return FS_OK;
 }

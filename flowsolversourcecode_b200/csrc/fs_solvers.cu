@@ -453,7 +453,21 @@ static int coop_grid_size(fs_ctx *ctx) {
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, (void *)k_sor3_colour, FS_COOP_BLOCK, 0));
   int per_sm = std::min(std::min(a, d), std::min(b, c));
   if (per_sm < 1) { ctx->err = "cooperative kernel does not fit on an SM"; return FS_E_CUDA; }
-  ctx->coop_grid = ctx->num_sms * (per_sm > 4 ? 4 : per_sm);
+  ctx->coop_grid = ctx->num_sms * fs_coop_per_sm(ctx, per_sm);
+  return FS_OK;
+}
+
+// CTAs per SM of a cooperative launch: the occupancy limit, capped at 4 or at
+// the launch shape chosen with fs_set_launch_shape
+int fs_coop_per_sm(fs_ctx *ctx, int occupancy) {
+  int cap = ctx->coop_per_sm > 0 ? ctx->coop_per_sm : 4;
+  return std::max(1, std::min(occupancy, cap));
+}
+
+extern "C" int fs_set_launch_shape(fs_ctx *ctx, int ctas_per_sm) {
+  if (!ctx || ctas_per_sm < 0 || ctas_per_sm > 8) return FS_E_ARG;
+  ctx->coop_per_sm = ctas_per_sm;
+  ctx->coop_grid = 0;   // recomputed at the next solve
   return FS_OK;
 }
 
@@ -464,7 +478,7 @@ static int coop_launch(fs_ctx *ctx, void *fn, SolveArgs &a) {
   long need = (ctx->N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
   if (need < G) G = (int)(need < 1 ? 1 : need);
   void *args[] = {&a};
-  FS_CK(cudaLaunchCooperativeKernel(fn, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
+  FS_CK(fs_coop_launch(fn, G, FS_COOP_BLOCK, args, ctx->st));
   FS_LAUNCH_CHECK();
   return FS_OK;
 }
@@ -490,8 +504,8 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
   FS_CK(cudaMemsetAsync(ctx->dphi, 0, sizeof(double) * N, ctx->st));
   SolveArgs a = solve_args(ctx, nf, rrf, itmax);
   int rc = FS_OK;
-  if (ctx->s_pending[nf - 1]) { FS_CK(cudaStreamSynchronize(ctx->st)); fs_solver_stats_collect(ctx); }
-  FS_CK(cudaEventRecord(ctx->sev[nf - 1][0], ctx->st));
+  if (ctx->s_pending[nf - 1] && !ctx->graph_mode) { FS_CK(cudaStreamSynchronize(ctx->st)); fs_solver_stats_collect(ctx); }
+  FS_TIMING(FS_CK(cudaEventRecord(ctx->sev[nf - 1][0], ctx->st)));
   if (solver == FS_SOLVER_SOR) {
     // colour-major copy, sweeps on it, back to cell order
     k_to_colour<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->W, ctx->color_rows, ctx->ncfP, ctx->ac, ctx->bc,
@@ -506,17 +520,17 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
     if (need < G) G = (int)(need < 1 ? 1 : need);
     void *args[] = {&sp};
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
-    FS_CK(cudaLaunchCooperativeKernel((void *)k_sor_colour, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
+    FS_CK(fs_coop_launch((const void *)k_sor_colour, G, FS_COOP_BLOCK, args, ctx->st));
     FS_LAUNCH_CHECK();
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
     k_from_colour<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->dphiP, ctx->dphi);
     FS_LAUNCH_CHECK();
   } else if (solver == FS_SOLVER_BICGS) {
     a.itmax = ctx->cfg.krylov_maxit;
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     rc = coop_launch(ctx, (void *)k_bicgstab, a);
-    FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st));
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
   } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS) {
     rc = fs_mg_solve(ctx, nf, rrf, solver);
   } else {
@@ -524,8 +538,7 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     return FS_E_ARG;
   }
   if (rc) return rc;
-  FS_CK(cudaEventRecord(ctx->sev[nf - 1][1], ctx->st));
-  ctx->s_pending[nf - 1] = true;
+  FS_TIMING(FS_CK(cudaEventRecord(ctx->sev[nf - 1][1], ctx->st)); ctx->s_pending[nf - 1] = true);
   k_axpy_field<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, fi, ctx->dphi);
   FS_LAUNCH_CHECK();
   return FS_OK;
@@ -643,9 +656,9 @@ int fs_momentum_batched_solve(fs_ctx *ctx) {
   int rc = coop_grid_size(ctx);
   if (rc) return rc;
   for (int c = 0; c < 3; c++) {
-    if (ctx->s_pending[c]) { FS_CK(cudaStreamSynchronize(ctx->st)); fs_solver_stats_collect(ctx); }
+    if (ctx->s_pending[c] && !ctx->graph_mode) { FS_CK(cudaStreamSynchronize(ctx->st)); fs_solver_stats_collect(ctx); }
   }
-  FS_CK(cudaEventRecord(ctx->sev[0][0], ctx->st));
+  FS_TIMING(FS_CK(cudaEventRecord(ctx->sev[0][0], ctx->st)));
   k_to_colour3<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->color_rows, ctx->ncfP, ctx->ac3, ctx->bc3, ctx->anb,
                                                     ctx->ac3P, ctx->bc3P, ctx->anbP, ctx->x3P);
   FS_LAUNCH_CHECK();
@@ -658,13 +671,12 @@ int fs_momentum_batched_solve(fs_ctx *ctx) {
   long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
   if (need < G) G = (int)(need < 1 ? 1 : need);
   void *args[] = {&a};
-  FS_CK(cudaEventRecord(ctx->kev[0][0], ctx->st));
-  FS_CK(cudaLaunchCooperativeKernel((void *)k_sor3_colour, dim3(G), dim3(FS_COOP_BLOCK), args, 0, ctx->st));
-  FS_CK(cudaEventRecord(ctx->kev[0][1], ctx->st));
+  FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[0][0], ctx->st)));
+  FS_CK(fs_coop_launch((const void *)k_sor3_colour, G, FS_COOP_BLOCK, args, ctx->st));
+  FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[0][1], ctx->st)));
   FS_LAUNCH_CHECK();
   k_from_colour3<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->x3P, ctx->u, ctx->v, ctx->w);
   FS_LAUNCH_CHECK();
-  FS_CK(cudaEventRecord(ctx->sev[0][1], ctx->st));
-  ctx->s_pending[0] = true;
+  FS_TIMING(FS_CK(cudaEventRecord(ctx->sev[0][1], ctx->st)); ctx->s_pending[0] = true);
   return FS_OK;
 }

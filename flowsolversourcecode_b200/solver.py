@@ -196,6 +196,10 @@ class Solver:
         return {"sizes": sizes[:k].tolist(), "widths": widths[:k].tolist(), "prec_coarsest": lc.value,
                 "direct": bool(direct.value)}
 
+    def set_launch_shape(self, ctas_per_sm: int):
+        """Cooperative CTAs per SM of the persistent solver kernels (0: default)."""
+        self._chk(self.lib.fs_set_launch_shape(self.ctx, ctas_per_sm), "fs_set_launch_shape")
+
     # ------------------------------------------------------------ learned p' guess
     def nn_create(self, snapshot_capacity: int = 0, seed: int = 0):
         """Network for the learned p' initial guess, with room for

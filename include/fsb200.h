@@ -293,6 +293,23 @@ int fs_nn_eval_host(fs_ctx *ctx, const float *X, const float *wgt, const float *
 int fs_nn_stats(fs_ctx *ctx, int32_t *uses, int32_t *fallbacks);
 int fs_nn_policy(fs_ctx *ctx, double *avg_guessed, double *avg_zero, int32_t *parked);
 
+/* ----------------------------------------------------- ensemble and launch shape
+ * No reference counterparts.
+ * fs_set_launch_shape: cooperative CTAs per SM of the persistent solver
+ *   kernels (1..8; 0 = occupancy limit capped at 4); the project's autotuner
+ *   (flowsolversourcecode_b200/ensemble.py) picks it per case by timing.
+ * fs_ensemble_run: `iters` SIMPLE iterations of each of n independent cases
+ *   (contexts on one GPU) captured into one CUDA graph, cases in sequence so
+ *   their cooperative kernels never overlap, launched `launches` times with one
+ *   host synchronisation per launch.  source_out [n * iters * launches]
+ *   (case-major) receives the stop metric after every iteration, pc_iters_out
+ *   (optional, same shape) the p' iterations, ms_out the device time.  One
+ *   ordinary iteration per case runs first (hierarchies, colourings, grids);
+ *   the learned guess is not used inside the graph. */
+int fs_set_launch_shape(fs_ctx *ctx, int ctas_per_sm);
+int fs_ensemble_run(fs_ctx **ctxs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
+                    float *ms_out);
+
 /* Timing of the last outer iteration's phases in milliseconds (CUDA events):
  * [0] momentum assembly, [1] momentum solves, [2] continuity assembly,
  * [3] p' solve, [4] corrections+residuals. */
