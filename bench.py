@@ -359,7 +359,7 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
         line = {
             "metric": "ensemble cell-iterations/s", "value": total_cells * T / (ms * 1e-3), "unit": "cell-iter/s",
             "n_gpus": world, "steps": T, "warmup": args.steps, "ms_per_step": ms / T, "higher_is_better": True,
-            "scaling": "weak" if world > 1 else "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"ensemble of {len(specs)} lid-driven cavities, edges U{{32..96}}, lid U[0.5,2], "
                                    f"Re log-U[100,2000], seed 0",
                        "cases": len(specs), "cells_total": sum(s.cells for s in specs), "cases_rank0": len(mine),

@@ -145,7 +145,7 @@ static void free_all(fs_ctx *c) {
                   c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky, c->sysx,
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
                   c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP,
-                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P};
+                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm};
   for (void *p : ptrs) if (p) cudaFree(p);
 }
 

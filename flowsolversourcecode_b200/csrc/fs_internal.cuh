@@ -81,6 +81,7 @@ struct fs_ctx {
   double *kx = nullptr, *kr = nullptr, *kr0 = nullptr, *kp = nullptr, *kv = nullptr, *ks = nullptr, *kt = nullptr;
   double *kz = nullptr, *ky = nullptr;   // preconditioned vectors (AMG-BiCGSTAB)
   double *sysx = nullptr;                // fs_solve_system_host: the field the update is added to
+  double *gm = nullptr;                  // GMRES work: 21 Krylov vectors + 7 (allocated on first use)
   // reductions
   double *red = nullptr;        // RED_NQ * FS_RED_BLOCKS partials
   int64_t *redi = nullptr;      // FS_RED_BLOCKS argmax partials

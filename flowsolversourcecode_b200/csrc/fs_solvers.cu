@@ -443,15 +443,192 @@ __global__ void k_axpy_field(int N, double *fi, const double *dphi) {
 
 // one grid size for every cooperative solver kernel of a context: the smallest
 // co-resident CTA count of the three, at most 4 per SM
+
+// GMRES_RESTARTED_OMP_RETURNR (matrixSolverOMP.f90:48-304) with the caller's
+// GMRES_ninner = 20, GMRES_tol = 1e-9 (:4-6, :604), as one cooperative kernel:
+// the system normalised by |b|; restart lengths mm = 5, 10, 15, 20, each round
+// from x = 0 (resetFlag is never cleared, :81,120); Arnoldi with modified
+// Gram-Schmidt (one grid reduction per projection) and Givens rotations; the
+// best iterate kept; the restart length reduced by 5 (above 10) or 1 when a
+// cycle gains less than 10 % or loses; a round with m = 1 ends when a cycle
+// gains less than 1 % or after 100 cycles; the next round only if this one
+// improved the best residual.  Every CTA keeps the Hessenberg matrix, the
+// rotations and the least-squares solution in shared memory, updated by its
+// thread 0 from the same grid-deterministic sums, so all CTAs take the same
+// branches.  A zero right-hand side gives x = 0 (the reference divides by
+// |b| = 0).  As the reference's module vector x, the result also stays in x.
+#define FS_GM_M 20
+#define FS_GM_CYCLES 20000   // bound on cycles per round (the reference's loop always ends; this only bounds a kernel)
+struct GmresArgs {
+  int N, W;
+  const int32_t *cn;
+  const double *ac, *anb, *bc;
+  double *V, *w, *x1, *xOpt, *rOpt, *xG, *rG, *bn, *x, *r, *dphi;
+  double *part;
+  int32_t *iters;
+  double *diag;
+};
+
+__device__ __forceinline__ void gm_ax2(const GmresArgs &a, long i, long i2, bool h2, const double *x, double &t1,
+                                       double &t2) {
+  t1 = 0.0;
+  t1 = t1 + a.ac[i] * x[i];
+  t2 = 0.0;
+  if (h2) t2 = t2 + a.ac[i2] * x[i2];
+  ell_acc2<6, false>(t1, t2, a.N, a.W, a.cn, a.anb, i, i2, h2, [&](int k) { return x[k]; });
+}
+
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_gmres(GmresArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  const int N = a.N;
+  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+  __shared__ double H[FS_GM_M + 1][FS_GM_M], g[FS_GM_M + 1], c[FS_GM_M], s[FS_GM_M], y[FS_GM_M];
+  const double res = 1.0e-9, normb = 1.0;
+  int buf = 1;
+  double l0 = 0., dum;
+  for (long i = tid0; i < N; i += nth) l0 += a.bc[i] * a.bc[i];
+  double bb;
+  grid_sum2(grid, a.part, 0, l0, 0., bb, dum);
+  const double normb0 = sqrt(bb);
+  if (normb0 == 0.) {
+    for (long i = tid0; i < N; i += nth) { a.x[i] = 0.; a.dphi[i] = 0.; }
+    if (tid0 == 0) { *a.iters = 0; a.diag[0] = 0.; a.diag[1] = 0.; }
+    return;
+  }
+  for (long i = tid0; i < N; i += nth) a.bn[i] = a.bc[i] / normb0;
+  int total = 0, mm = 5;
+  double normminG = 1.0e30;
+  while (mm <= FS_GM_M) {
+    double normmin = 1.0e30;
+    int mcur = mm, iter = 0, leave = 0, cycles = 0;
+    l0 = 0.;
+    for (long i = tid0; i < N; i += nth) { a.x[i] = 0.; const double ri = a.bn[i]; a.r[i] = ri; l0 += ri * ri; }
+    double rr;
+    grid_sum2(grid, a.part, buf, l0, 0., rr, dum); buf ^= 3;
+    double normr = sqrt(rr), normrPrev = normr;
+    while (normmin > res * normb && leave == 0 && cycles < FS_GM_CYCLES) {
+      cycles++;
+      iter++;
+      int mloc = mcur;
+      for (long i = tid0; i < N; i += nth) a.V[i] = a.r[i] / normr;
+      if (threadIdx.x == 0) {
+        for (int p = 0; p <= FS_GM_M; p++) { g[p] = 0.; for (int q = 0; q < FS_GM_M; q++) H[p][q] = 0.; }
+        g[0] = normr;
+      }
+      __syncthreads();
+      for (int j = 0; j < mloc; j++) {
+        total++;
+        const double *vj = a.V + (size_t)j * N;
+        grid.sync();   // v_j complete before its neighbours are gathered
+        for (long i = tid0; i < N; i += 2 * nth) {
+          const long i2 = i + nth;
+          const bool h2 = i2 < N;
+          double t1, t2;
+          gm_ax2(a, i, i2, h2, vj, t1, t2);
+          a.w[i] = t1;
+          if (h2) a.w[i2] = t2;
+        }
+        for (int i = 0; i <= j; i++) {
+          const double *vi = a.V + (size_t)i * N;
+          l0 = 0.;
+          for (long q = tid0; q < N; q += nth) l0 += a.w[q] * vi[q];
+          double h;
+          grid_sum2(grid, a.part, buf, l0, 0., h, dum); buf ^= 3;
+          for (long q = tid0; q < N; q += nth) a.w[q] = a.w[q] - h * vi[q];
+          if (threadIdx.x == 0) H[i][j] = h;
+        }
+        l0 = 0.;
+        for (long q = tid0; q < N; q += nth) l0 += a.w[q] * a.w[q];
+        double ww;
+        grid_sum2(grid, a.part, buf, l0, 0., ww, dum); buf ^= 3;
+        const double hn = sqrt(ww);
+        if (threadIdx.x == 0) H[j + 1][j] = hn;
+        if (hn == 0.) { mloc = j + 1; __syncthreads(); break; }
+        double *vn = a.V + (size_t)(j + 1) * N;
+        for (long q = tid0; q < N; q += nth) vn[q] = a.w[q] / hn;
+        if (threadIdx.x == 0) {
+          for (int i = 0; i < j; i++) {
+            double hi = c[i] * H[i][j] + s[i] * H[i + 1][j], hi1 = -s[i] * H[i][j] + c[i] * H[i + 1][j];
+            H[i][j] = hi; H[i + 1][j] = hi1;
+          }
+          double d = sqrt(H[j][j] * H[j][j] + H[j + 1][j] * H[j + 1][j]);
+          s[j] = H[j + 1][j] / d; c[j] = H[j][j] / d;
+          for (int q = 0; q < mloc; q++) {
+            double hj = c[j] * H[j][q] + s[j] * H[j + 1][q], hj1 = -s[j] * H[j][q] + c[j] * H[j + 1][q];
+            H[j][q] = hj; H[j + 1][q] = hj1;
+          }
+          double gj = c[j] * g[j] + s[j] * g[j + 1], gj1 = -s[j] * g[j] + c[j] * g[j + 1];
+          g[j] = gj; g[j + 1] = gj1;
+        }
+        __syncthreads();
+      }
+      mcur = mloc;
+      if (threadIdx.x == 0) {
+        y[mcur - 1] = g[mcur - 1] / H[mcur - 1][mcur - 1];
+        for (int j = mcur - 2; j >= 0; j--) {
+          double dp = 0.;
+          for (int q = j + 1; q < mcur; q++) dp += H[j][q] * y[q];
+          y[j] = (g[j] - dp) / H[j][j];
+        }
+      }
+      __syncthreads();
+      for (long i = tid0; i < N; i += nth) {
+        double t = 0.;
+        for (int q = 0; q < mcur; q++) t += a.V[(size_t)q * N + i] * y[q];
+        a.x1[i] = a.x[i] + t;
+      }
+      grid.sync();   // x1 complete before its neighbours are gathered
+      l0 = 0.;
+      for (long i = tid0; i < N; i += 2 * nth) {
+        const long i2 = i + nth;
+        const bool h2 = i2 < N;
+        double t1, t2;
+        gm_ax2(a, i, i2, h2, a.x1, t1, t2);
+        const double r1 = a.bn[i] - t1;
+        a.r[i] = r1;
+        l0 += r1 * r1;
+        if (h2) { const double r2 = a.bn[i2] - t2; a.r[i2] = r2; l0 += r2 * r2; }
+      }
+      grid_sum2(grid, a.part, buf, l0, 0., rr, dum); buf ^= 3;
+      normr = sqrt(rr);
+      if ((normr - normrPrev) / normrPrev > -0.01 && mcur == 1) leave = 1;
+      if (mcur == 1 && iter > 100) leave = 1;
+      const bool best = normr < normmin, step = normr < normrPrev;
+      if (best) normmin = normr;
+      for (long i = tid0; i < N; i += nth) {
+        if (best) { a.xOpt[i] = a.x1[i]; a.rOpt[i] = a.r[i]; }
+        if (step) a.x[i] = a.x1[i];
+        else { a.x[i] = a.xOpt[i]; a.r[i] = a.rOpt[i]; }
+      }
+      if ((fabs((normr - normrPrev) / normr) < 0.1 || normr > normrPrev) && mcur > 1) {
+        mcur = mcur > 10 ? mcur - 5 : mcur - 1;
+        iter = 0;
+      }
+      normrPrev = normr;
+    }
+    if (normmin < normminG) {
+      normminG = normmin;
+      for (long i = tid0; i < N; i += nth) { a.xG[i] = a.xOpt[i]; a.rG[i] = a.rOpt[i]; }
+      mm += 5;
+    } else {
+      mm = FS_GM_M + 5;
+    }
+    if (normminG <= res) mm = FS_GM_M + 5;
+  }
+  for (long i = tid0; i < N; i += nth) { const double xi = a.xG[i] * normb0; a.x[i] = xi; a.dphi[i] = xi; }
+  if (tid0 == 0) { *a.iters = total; a.diag[0] = normminG * normb0; a.diag[1] = normb0; }
+}
+
 static int coop_grid_size(fs_ctx *ctx) {
   if (ctx->coop_grid > 0) return FS_OK;
   int a = 0, b = 0, c = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_bicgstab, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_sor, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_sor_colour, FS_COOP_BLOCK, 0));
-  int d = 0;
+  int d = 0, e = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, (void *)k_sor3_colour, FS_COOP_BLOCK, 0));
-  int per_sm = std::min(std::min(a, d), std::min(b, c));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, (void *)k_gmres, FS_COOP_BLOCK, 0));
+  int per_sm = std::min(std::min(std::min(a, d), std::min(b, c)), e);
   if (per_sm < 1) { ctx->err = "cooperative kernel does not fit on an SM"; return FS_E_CUDA; }
   ctx->coop_grid = ctx->num_sms * fs_coop_per_sm(ctx, per_sm);
   return FS_OK;
@@ -530,6 +707,25 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     a.itmax = ctx->cfg.krylov_maxit;
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     rc = coop_launch(ctx, (void *)k_bicgstab, a);
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
+  } else if (solver == FS_SOLVER_GMRES) {
+    if (!ctx->gm) FS_CK(cudaMalloc(&ctx->gm, sizeof(double) * (size_t)(FS_GM_M + 8) * N));
+    GmresArgs g{};
+    g.N = N; g.W = ctx->W; g.cn = ctx->cn; g.ac = ctx->ac; g.anb = ctx->anb; g.bc = ctx->bc;
+    double *p = ctx->gm;
+    g.V = p; p += (size_t)(FS_GM_M + 1) * N;
+    g.w = p; p += N; g.x1 = p; p += N; g.xOpt = p; p += N; g.rOpt = p; p += N;
+    g.xG = p; p += N; g.rG = p; p += N; g.bn = p;
+    g.x = ctx->kx; g.r = ctx->kr; g.dphi = ctx->dphi; g.part = ctx->red;
+    g.iters = a.iters; g.diag = a.diag;
+    if ((rc = coop_grid_size(ctx))) return rc;
+    int G = ctx->coop_grid;
+    long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
+    if (need < G) G = (int)(need < 1 ? 1 : need);
+    void *args[] = {&g};
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
+    FS_CK(fs_coop_launch((const void *)k_gmres, G, FS_COOP_BLOCK, args, ctx->st));
+    FS_LAUNCH_CHECK();
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
   } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS) {
     rc = fs_mg_solve(ctx, nf, rrf, solver);

@@ -94,7 +94,8 @@ enum fs_solver {
   FS_SOLVER_BICGS = 1,     /* 'bicgs': BICGSTAB_OMP restated (matrixSolverOMP.f90:306) */
   FS_SOLVER_AMG = 2,       /* LMultigrid=.true., MGType='geometricelement' */
   FS_SOLVER_AMG_BICGS = 3, /* FP64 BiCGSTAB right-preconditioned by one AMG V-cycle (no reference row) */
-  FS_SOLVER_AMG32_BICGS = 4/* same with an FP32 AMG hierarchy (iterative refinement, no reference row) */
+  FS_SOLVER_AMG32_BICGS = 4,/* same with an FP32 AMG hierarchy (iterative refinement, no reference row) */
+  FS_SOLVER_GMRES = 5      /* 'gmres': GMRES_RESTARTED_OMP_RETURNR restated (matrixSolverOMP.f90:48) */
 };
 enum fs_algorithm { FS_SIMPLE = 0, FS_SIMPLEC = 1 };
 

@@ -50,6 +50,8 @@ def load():
         lib.om_solve_equation.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_int]
         lib.om_bicgstab.restype = C.c_int
         lib.om_bicgstab.argtypes = [C.c_void_p, C.c_int, C.c_double]
+        lib.om_gmres.restype = C.c_int
+        lib.om_gmres.argtypes = [C.c_void_p]
         lib.om_calc_residuals.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         lib.om_mg_setup.restype = C.c_int
         lib.om_mg_setup.argtypes = [C.c_void_p]
@@ -133,6 +135,10 @@ class Oracle:
 
     def bicgstab(self, maxit=100, tol=1e-5) -> int:
         return self.lib.om_bicgstab(self.h, maxit, tol)
+
+    def gmres(self) -> int:
+        """GMRES_RESTARTED_OMP_RETURNR on the current system; dphi holds x."""
+        return self.lib.om_gmres(self.h)
 
     def mg_setup(self) -> int:
         return self.lib.om_mg_setup(self.h)

@@ -934,6 +934,123 @@ int om_bicgstab(om *m, int nIter, double res)
   return k - 1;
 }
 
+/* GMRES_RESTARTED_OMP_RETURNR (matrixSolverOMP.f90:48-304) with the caller's
+ * parameters GMRES_ninner=20, GMRES_nouter=1000, GMRES_tol=1e-9
+ * (matrixSolverOMP.f90:4-6,604): the system is normalised by |b|; restart
+ * lengths mm = 5, 10, 15, 20 (each round from x = 0: resetFlag is never
+ * cleared, :81,120); within a round, Arnoldi with modified Gram-Schmidt and
+ * Givens rotations (:145-181), the best iterate kept (:219-229), and the
+ * restart length reduced by 5 (above 10) or 1 when a cycle gains less than
+ * 10 % or loses (:231-238); a round with m = 1 ends when a cycle gains less
+ * than 1 % or after 100 cycles (:215-216).  The next round runs only if this
+ * one improved the best residual (:256-263).  A zero right-hand side gives
+ * x = 0 (the reference divides by |b| = 0).  Returns the Arnoldi steps. */
+int om_gmres(om *m)
+{
+  const int n = m->N, mMax = 20;
+  const double res = 1.0e-9;
+  csr_build(m);
+  double *b = dz_(n), *x = m->kx, *r = m->kr;
+  memcpy(b, m->bc, sizeof(double) * n);
+  double normb0 = sqrt(dot(b, b, n));
+  int total = 0;
+  if (normb0 == 0.) {
+    memset(x, 0, sizeof(double) * n);
+    memcpy(m->dphi, x, sizeof(double) * n);
+    free(b);
+    return 0;
+  }
+  for (int i = 0; i < n; i++) b[i] = b[i] / normb0;
+  const double normb = 1.0;
+  double *w = dz_(n), *x1 = dz_(n), *xOpt = dz_(n), *rOpt = dz_(n), *xG = dz_(n), *rG = dz_(n);
+  double *V = dz_((size_t)n * (mMax + 1));
+  double H[21][20], g[21], c[20], s[20], y[20];
+  double normminG = 1.0e30;
+  int mm = 5;
+  while (mm <= mMax) {
+    double normmin = 1.0e30;
+    int mcur = mm, iter = 0, leave = 0;
+    memset(x, 0, sizeof(double) * n);
+    memcpy(r, b, sizeof(double) * n);
+    double normr = sqrt(dot(r, r, n));
+    double normrPrev = normr;
+    while (normmin > res * normb && leave == 0) {
+      iter++;
+      int mloc = mcur;
+      for (int i = 0; i < n; i++) V[i] = r[i] / normr;
+      for (int a = 0; a <= mMax; a++) { g[a] = 0.; for (int q = 0; q < mMax; q++) H[a][q] = 0.; }
+      g[0] = normr;
+      for (int j = 0; j < mloc; j++) {
+        total++;
+        axomp(m, V + (size_t)j * n, w);
+        for (int i = 0; i <= j; i++) {
+          H[i][j] = dot(w, V + (size_t)i * n, n);
+          const double h = H[i][j], *vi = V + (size_t)i * n;
+          for (int q = 0; q < n; q++) w[q] = w[q] - h * vi[q];
+        }
+        H[j + 1][j] = sqrt(dot(w, w, n));
+        if (H[j + 1][j] == 0.) { mloc = j + 1; break; }
+        for (int q = 0; q < n; q++) V[(size_t)(j + 1) * n + q] = w[q] / H[j + 1][j];
+        for (int i = 0; i < j; i++) {
+          double hi = c[i] * H[i][j] + s[i] * H[i + 1][j], hi1 = -s[i] * H[i][j] + c[i] * H[i + 1][j];
+          H[i][j] = hi; H[i + 1][j] = hi1;
+        }
+        double d = sqrt(H[j][j] * H[j][j] + H[j + 1][j] * H[j + 1][j]);
+        s[j] = H[j + 1][j] / d; c[j] = H[j][j] / d;
+        for (int q = 0; q < mloc; q++) {
+          double hj = c[j] * H[j][q] + s[j] * H[j + 1][q], hj1 = -s[j] * H[j][q] + c[j] * H[j + 1][q];
+          H[j][q] = hj; H[j + 1][q] = hj1;
+        }
+        double gj = c[j] * g[j] + s[j] * g[j + 1], gj1 = -s[j] * g[j] + c[j] * g[j + 1];
+        g[j] = gj; g[j + 1] = gj1;
+      }
+      mcur = mloc;
+      y[mcur - 1] = g[mcur - 1] / H[mcur - 1][mcur - 1];
+      for (int j = mcur - 2; j >= 0; j--) {
+        double dp = 0.;
+        for (int q = j + 1; q < mcur; q++) dp += H[j][q] * y[q];
+        y[j] = (g[j] - dp) / H[j][j];
+      }
+      for (int i = 0; i < n; i++) {
+        double t = 0.;
+        for (int q = 0; q < mcur; q++) t += V[(size_t)q * n + i] * y[q];
+        w[i] = t;
+      }
+      for (int i = 0; i < n; i++) x1[i] = x[i] + w[i];
+      axomp(m, x1, r);
+      for (int i = 0; i < n; i++) r[i] = b[i] - r[i];
+      normr = sqrt(dot(r, r, n));
+      if ((normr - normrPrev) / normrPrev > -0.01 && mcur == 1) leave = 1;
+      if (mcur == 1 && iter > 100) leave = 1;
+      if (normr < normmin) {
+        normmin = normr;
+        memcpy(xOpt, x1, sizeof(double) * n);
+        memcpy(rOpt, r, sizeof(double) * n);
+      }
+      if (normr < normrPrev) memcpy(x, x1, sizeof(double) * n);
+      else { memcpy(x, xOpt, sizeof(double) * n); memcpy(r, rOpt, sizeof(double) * n); }
+      if ((fabs((normr - normrPrev) / normr) < 0.1 || normr > normrPrev) && mcur > 1) {
+        mcur = mcur > 10 ? mcur - 5 : mcur - 1;
+        iter = 0;
+      }
+      normrPrev = normr;
+    }
+    if (normmin < normminG) {
+      normminG = normmin;
+      memcpy(xG, xOpt, sizeof(double) * n);
+      memcpy(rG, rOpt, sizeof(double) * n);
+      mm += 5;
+    } else {
+      mm = mMax + 5;
+    }
+    if (normminG <= res) mm = mMax + 5;
+  }
+  for (int i = 0; i < n; i++) x[i] = xG[i] * normb0;
+  memcpy(m->dphi, x, sizeof(double) * n);     /* dphi=x */
+  free(b); free(w); free(x1); free(xOpt); free(rOpt); free(xG); free(rG); free(V);
+  return total;
+}
+
 int om_mg_solve(om *m, double rrF, double IRes);   /* below */
 
 /* SolveEquation (SolveAlegbraicEquations.for:4-180) */
@@ -950,6 +1067,8 @@ void om_solve_equation(om *m, int nf, double *fi, double rrf, int itmax, int sol
     iter = om_bicgstab(m, m->cfg.krylov_maxit, m->cfg.krylov_tol);
   } else if (solver == FS_SOLVER_AMG) {
     iter = om_mg_solve(m, rrf, IRes);
+  } else if (solver == FS_SOLVER_GMRES) {
+    iter = om_gmres(m);
   } else {
     fprintf(stderr, "oracle: solver %d not restated\n", solver);
   }

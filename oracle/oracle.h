@@ -49,6 +49,7 @@ void   om_assemble_continuity(om *m);          /* SolveContinuity up to the p' s
 void   om_correct_continuity(om *m);           /* SolveContinuity after the p' solve */
 void   om_solve_equation(om *m, int nf, double *fi, double rrf, int itmax, int solver);
 int    om_bicgstab(om *m, int maxit, double tol); /* returns iterations */
+int    om_gmres(om *m);                            /* returns Arnoldi steps */
 void   om_calc_residuals(om *m, int nf, const double *fi);
 
 /* geometric-element agglomeration multigrid */

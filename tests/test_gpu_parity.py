@@ -162,6 +162,41 @@ def test_bicgstab_parity():
     assert _rel(x_g, x_o) <= 1e-6
 
 
+def test_gmres_parity():
+    # GMRES_RESTARTED_OMP_RETURNR on a momentum system (non-symmetric: SOU
+    # convection) and on the p' system; the GPU's dot products sum in another
+    # order, so both reach the 1e-9 normalised residual along slightly
+    # different paths
+    mesh, case = cs.cavity(12, nz=10, jitter=0.2, seed=3, conv_scheme="sou", niter_start_hr=1)
+    s, o = _pair(mesh, case)
+    for _ in range(3):
+        o.simple_iteration()
+    o.set_iter(4)
+    for assemble in (lambda: o.assemble_momentum(0), o.assemble_continuity):
+        assemble()
+        ac, anb, bc = o.get("ac"), o.get("anb"), o.get("bc")
+        it_o = o.gmres()
+        x_o = o.get("dphi")
+        x_g, it_g = s.solve_system(ac, anb, bc, solver="gmres")
+        assert it_g > 0 and abs(it_g - it_o) <= max(5, it_o // 5), (it_g, it_o)
+        assert _rel(x_g, x_o) <= 1e-6
+
+
+def test_outer_iterations_gmres():
+    # p' by GMRES through SolveEquation for three SIMPLE iterations; momentum by
+    # BiCGSTAB to 1e-10 from a non-zero state, as in test_outer_iterations_bicgs
+    # (multicolour SOR at rrF 0.01 would differ from the sequential sweep)
+    mesh, case = cs.cavity(10, nz=8, jitter=0.2, seed=2, solver_mom="bicgs", solver_cont="gmres",
+                           krylov_tol=1e-10, krylov_maxit=400)
+    s, o = _pair(mesh, case)
+    _random_state(s, o, seed=5, scale=0.05)
+    for _ in range(3):
+        s.simple_iteration()
+        o.simple_iteration()
+    for k in ("u", "v", "w", "p"):
+        assert _rel(s.get(k), o.get(k)) <= 1e-6, k
+
+
 def test_sor_solution():
     mesh, case = cs.cavity(12, nz=10, jitter=0.2, seed=3)
     s, o = _pair(mesh, case)

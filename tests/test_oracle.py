@@ -150,6 +150,12 @@ def test_solvers_match_direct(oracle_lib):
     assert it < 400
     assert np.abs(x - x_direct).max() <= 1e-8 * np.abs(x_direct).max()
     assert np.array_equal(o.get("u"), u0)
+    # GMRES_RESTARTED_OMP_RETURNR: relative residual 1e-9 of the normalised system
+    steps = o.gmres()
+    x = o.get("dphi")
+    assert 0 < steps
+    assert np.linalg.norm(A @ x - b) <= 2e-9 * np.linalg.norm(b)
+    assert np.abs(x - x_direct).max() <= 1e-7 * np.abs(x_direct).max()
 
 
 def test_connectivity_slot_order(oracle_lib):
