@@ -153,11 +153,16 @@ __device__ double scope_sum(Sync &S, const Scope &sc, double v) {
 
 // one symmetric multicolour Gauss-Seidel sweep (SORMultiGrid.for:20-66)
 template <class R>
-__device__ void gs_sweep(Sync &S, const Scope &sc, const LevelDev<R> L, const R *b, R *x) {
+// `last`: colour of the previous pass over x; a pass repeating it (the
+// backward pass's first colour, the next sweep's first) would rewrite the same
+// values -- rows of one colour read only other colours -- and is skipped
+__device__ void gs_sweep(Sync &S, const Scope &sc, const LevelDev<R> L, const R *b, R *x, int &last) {
   const int n = L.n;
   for (int pass = 0; pass < 2; pass++)
     for (int cc = 0; cc < L.ncolors; cc++) {
       int c = pass == 0 ? cc : L.ncolors - 1 - cc;
+      if (c == last) continue;
+      last = c;
       int r0 = L.color_ptr[c], r1 = L.color_ptr[c + 1];
       for (long q = r0 + sc.tid0(); q < r1; q += sc.nth()) {
         int i = L.color_rows[q];
@@ -187,9 +192,9 @@ template <class R>
 __device__ void smooth(Sync &S, const Scope &sc, const LevelDev<R> &L, const R *b, R *x, R *r,
                        double rrf, double ires, int itmax, bool checked) {
   double fres = ires;
-  int iter = 0;
+  int iter = 0, last = -1;
   while ((!checked || fres > rrf * ires) && iter < itmax) {
-    gs_sweep(S, sc, L, b, x);
+    gs_sweep(S, sc, L, b, x, last);
     if (checked) fres = residual(S, sc, L, b, x, r);
     iter++;
   }

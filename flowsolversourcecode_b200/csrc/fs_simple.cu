@@ -97,6 +97,23 @@ struct GradJob {
   const double *in[4]; // 3N gradient of the previous pass (correction passes)
 };
 
+// CTAs per SM the wide gather kernels are compiled for (register caps):
+// uncapped, k_mom_interior took 162 registers (one CTA per SM) and
+// k_gg_corr<4> 128; these latency-bound gathers run faster with more resident
+// warps even at the cost of a few spilled registers
+#ifndef FS_MOM_MINB
+#define FS_MOM_MINB 2
+#endif
+#ifndef FS_GG_MINB
+#define FS_GG_MINB 3
+#endif
+#ifndef FS_GG0_MINB
+#define FS_GG0_MINB 3
+#endif
+#ifndef FS_FACE_MINB
+#define FS_FACE_MINB 4
+#endif
+
 // StandardGreenGauss / first pass of StandardGreenGaussFaceCorrection1
 // (StandardGreenGaussGradient.for:35-79; StandardGreenGaussCorrection1Gradient.for:47-96).
 // All NF fields of a call are done in one slot loop, so a face's geometry and
@@ -104,7 +121,7 @@ struct GradJob {
 // registers; the other cell of each interior face comes from the slot-major
 // neighbour table cn.
 template <int NF>
-__global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B,
+__global__ void __launch_bounds__(FS_BLOCK, FS_GG0_MINB) k_gg0(GradJob J, int N, int F, int B,
     const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot, const int32_t *__restrict__ cn,
     const double *__restrict__ gf, const double *__restrict__ sf,
     const double *__restrict__ bsf, const double *__restrict__ vol) {
@@ -150,7 +167,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_gg0(GradJob J, int N, int F, int B
 
 // correction pass of StandardGreenGaussFaceCorrection1 (:98-172)
 template <int NF>
-__global__ void __launch_bounds__(FS_BLOCK) k_gg_corr(GradJob J, int N, int F, int B,
+__global__ void __launch_bounds__(FS_BLOCK, FS_GG_MINB) k_gg_corr(GradJob J, int N, int F, int B,
     const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot, const int32_t *__restrict__ cn,
     const double *__restrict__ gf, const double *__restrict__ sf, const double *__restrict__ dfp,
     const double *__restrict__ bsf, const double *__restrict__ vol) {
@@ -318,7 +335,7 @@ struct MomArgs {
 // upwind convection + HR deferred correction (AssembleConvection.for:72-88,153-162)
 // and the effective divergence (CalculateEffectiveDivergence.for:20-45).
 // FluxCf/FluxFf (and so ac, anb) are shared by u, v, w; bc differs.
-__global__ void __launch_bounds__(FS_BLOCK) k_mom_interior(MomArgs a) {
+__global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.N) return;
   const int N = a.N, F = a.F;
@@ -411,7 +428,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_mom_interior(MomArgs a) {
 // boundary terms, AssembleConvection.for:165-178 + 263-556, AssemblePressureGradient.for,
 // AssembleGolbalElementAndFaceFluxes.for:83-98 + 4-30, UnderRelaxation.for:21,
 // StoreTheDValues.for:20-48, and the residual partials of CalculateResiduals.
-__global__ void __launch_bounds__(FS_BLOCK) k_mom_finish(MomArgs a, int comp) {
+__global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a, int comp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool live = i < a.N;
   double r = 0., acphi = -1.;
@@ -544,7 +561,7 @@ __device__ __forceinline__ double geo_diff(int msd, double du, double dv, double
 
 // Rhie-Chow mdot (AssembleMdotUsingRhieChow.for:554-759) and the p' face
 // coefficient rho*geoDiff(D2) (AssemblePressureCorrectionFluxes.for:85-153)
-__global__ void __launch_bounds__(FS_BLOCK) k_mdot(ContArgs a) {
+__global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mdot(ContArgs a) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.F) return;
   const int N = a.N, F = a.F;

@@ -210,10 +210,16 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor(SolveArgs
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
   double ires = *a.ires, fres = ires;
   int iter = 0, buf = 0;
+  // a pass repeating the previous pass's colour (the backward pass's first
+  // colour, the next sweep's first) would rewrite the same values -- rows of
+  // one colour read only other colours -- and is skipped: results unchanged
+  int last = -1;
   while (fres > a.rrf * ires && iter < a.itmax) {
     for (int pass = 0; pass < 2; pass++) {
       for (int cc = 0; cc < a.ncolors; cc++) {
         int c = pass == 0 ? cc : a.ncolors - 1 - cc;
+        if (c == last) continue;
+        last = c;
         int r0 = a.color_ptr[c], r1 = a.color_ptr[c + 1];
         for (long q = r0 + tid0; q < r1; q += nth) {
           int i = a.color_rows[q];
@@ -258,10 +264,16 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor_colour(So
   const double *__restrict__ anb = a.anb;
   double ires = *a.ires, fres = ires;
   int iter = 0, buf = 0;
+  // a pass repeating the previous pass's colour (the backward pass's first
+  // colour, the next sweep's first) would rewrite the same values -- rows of
+  // one colour read only other colours -- and is skipped: results unchanged
+  int last = -1;
   while (fres > a.rrf * ires && iter < a.itmax) {
     for (int pass = 0; pass < 2; pass++) {
       for (int cc = 0; cc < a.ncolors; cc++) {
         int c = pass == 0 ? cc : a.ncolors - 1 - cc;
+        if (c == last) continue;
+        last = c;
         int r0 = a.color_ptr[c], r1 = a.color_ptr[c + 1];
         // rows of one colour are independent: two per step (ell_acc2)
         for (long i = r0 + tid0; i < r1; i += 2 * nth) {
@@ -360,6 +372,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor3_colour(S
   int iters[3];
   for (int c = 0; c < 3; c++) { ires[c] = a.ires3[c]; fres[c] = ires[c]; iters[c] = 0; }
   int buf = 0;
+  int last = -1;   // repeated colour passes are skipped, as in k_sor_colour
   for (;;) {
     bool act[3];
     bool any = false;
@@ -368,6 +381,8 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor3_colour(S
     for (int pass = 0; pass < 2; pass++) {
       for (int cc = 0; cc < a.ncolors; cc++) {
         int col = pass == 0 ? cc : a.ncolors - 1 - cc;
+        if (col == last) continue;
+        last = col;
         int r0 = a.color_ptr[col], r1 = a.color_ptr[col + 1];
         for (long i = r0 + tid0; i < r1; i += 2 * nth) {
           const long i2 = i + nth;
