@@ -294,14 +294,32 @@ def device_leg(s, steps: int, warm: int, barrier, local: int):
     s.solver_stats(reset=True)
     barrier()
     l0 = s.launch_count()
+    ph = [0.0] * 5
     with Clocks(local) as clk:
         s.timer_start()
         last = None
         for _ in range(steps):
             last = s.simple_iteration()
+            ph = [a + b for a, b in zip(ph, s.phase_times())]
         ms = s.timer_stop()
     return {"ms": ms, "launches": s.launch_count() - l0, "clocks": clk.summary(),
-            "stats": s.solver_stats(reset=True), "phases": s.phase_times(), "last": last}
+            "stats": s.solver_stats(reset=True), "phases": s.phase_times(), "phase_sum": ph, "last": last}
+
+
+def assembly_roofline(leg: dict, N: int, F: int, steps: int, hbm: float) -> dict:
+    """HBM fraction of everything in a SIMPLE iteration except the linear
+    solves: gradients, momentum assembly with urf and D, Rhie-Chow + p'
+    assembly, corrections and residuals.  Algorithmic bytes per iteration
+    576 per interior face + 1432 per cell (each array read or written once per
+    data-dependent phase, same-shape work sharing geometry); time = the
+    momentum phase minus its solves, the continuity assembly phase, and the
+    correction phase (CUDA events on the solver stream)."""
+    ph, st = leg["phase_sum"], leg["stats"]
+    ms = (ph[0] - sum(st["ms"][:3])) + ph[2] + ph[4]
+    nbytes = (576.0 * F + 1432.0 * N) * steps
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "bytes_per_step": nbytes / steps, "ms_per_step": ms / steps}
 
 
 def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e-6) -> dict:
@@ -502,6 +520,7 @@ def main():
                        "solver_ms_per_step": [round(x / args.steps, 3) for x in d64["stats"]["ms"]],
                        "phase_ms_last_step": [round(x, 3) for x in d64["phases"]]},
             "roofline": roof,
+            "assembly_roofline": assembly_roofline(d64, N, F, args.steps, hbm),
             "cpu_baseline": cpu,
             "e2e": {"value": aggregate_rate(world, args.steps, e2e_max), "unit": "iter/s",
                     "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},

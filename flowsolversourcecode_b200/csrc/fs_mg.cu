@@ -733,6 +733,9 @@ __global__ void __launch_bounds__(1024) k_mg_dense_inverse(int n, const int32_t 
   if (sing)
     for (int j = tid; j < n; j += nt) A[(long)(n - 1) * n + j] = j == n - 1 ? 1. : 0.;
   __syncthreads();
+  // warps take rows, lanes take columns: the pivot row is read with unit
+  // stride across a warp and no index division is needed
+  const int lane = tid & 31, wid = tid >> 5, nwarp = nt >> 5;
   for (int k = 0; k < n; k++) {
     const double d = A[(long)k * n + k];
     const double p = d != 0. ? 1. / d : 0.;
@@ -741,10 +744,12 @@ __global__ void __launch_bounds__(1024) k_mg_dense_inverse(int n, const int32_t 
       if (i != k) col[i] = A[(long)i * n + k];
     for (int j = tid; j < n; j += nt) A[(long)k * n + j] = j == k ? p : A[(long)k * n + j] * p;
     __syncthreads();
-    for (int q = tid; q < n * n; q += nt) {
-      int i = q / n, j = q - i * n;
+    const double *rk = A + (long)k * n;
+    for (int i = wid; i < n; i += nwarp) {
       if (i == k) continue;
-      A[q] = j == k ? -col[i] * p : A[q] - col[i] * A[(long)k * n + j];
+      const double ci = col[i];
+      double *ri = A + (long)i * n;
+      for (int j = lane; j < n; j += 32) ri[j] = j == k ? -ci * p : ri[j] - ci * rk[j];
     }
     __syncthreads();
   }
