@@ -43,7 +43,7 @@ namespace cg = cooperative_groups;
 // preconditioner V-cycle: Jacobi weight and coarse-correction factor
 // (over-correction compensates the energy of piecewise-constant prolongation)
 #ifndef FS_MG_OMEGA
-#define FS_MG_OMEGA 0.8
+#define FS_MG_OMEGA 0.9
 #endif
 // CTAs per SM the preconditioned Krylov kernel is compiled for (register cap)
 #ifndef FS_AMG_MINB
@@ -51,6 +51,13 @@ namespace cg = cooperative_groups;
 #endif
 #ifndef FS_MG_ALPHA
 #define FS_MG_ALPHA 1.8
+#endif
+// level 0 (the fine matrix) may take its own weight and correction factor
+#ifndef FS_MG_OMEGA0
+#define FS_MG_OMEGA0 0.8
+#endif
+#ifndef FS_MG_ALPHA0
+#define FS_MG_ALPHA0 FS_MG_ALPHA
 #endif
 
 template <class R>
@@ -384,8 +391,11 @@ struct PCycle {
   bool direct;         // coarsest by the dense inverse, else coarse_sweeps sweeps
   const double *sinv;  // lev[lc].n^2, row-major
   int pre, post, coarse_sweeps;
-  R omega, alpha;
+  R omega, alpha;        // Jacobi weight and coarse-correction factor on levels >= 1
   bool last_grid;
+  R omega0, alpha0;      // the same on level 0
+  __device__ R om(int l) const { return l == 0 ? omega0 : omega; }
+  __device__ R al(int l) const { return l == 0 ? alpha0 : alpha; }
   __device__ void enter(const Scope &sc) {
     if (sc.grid || last_grid) S.all(); else __syncthreads();
     last_grid = sc.grid;
@@ -423,7 +433,7 @@ struct PCycle {
     for (int s = 0; s < n; s++) {
       residual(l, in, x, L.t);
       enter(sc);
-      if (sc.active()) for (long i = sc.tid0(); i < L.n; i += sc.nth()) x[i] = x[i] + omega * L.t[i] / L.ac[i];
+      if (sc.active()) for (long i = sc.tid0(); i < L.n; i += sc.nth()) x[i] = x[i] + om(l) * L.t[i] / L.ac[i];
     }
   }
   // out = M^-1 in.  Callers have made `in` visible grid-wide.
@@ -431,7 +441,7 @@ struct PCycle {
     Scope g; g.grid = true;
     {
       const LevelDev<R> L0 = lev[0];
-      for (long i = g.tid0(); i < L0.n; i += g.nth()) L0.x[i] = omega * (R)in[i] / L0.ac[i];
+      for (long i = g.tid0(); i < L0.n; i += g.nth()) L0.x[i] = omega0 * (R)in[i] / L0.ac[i];
     }
     last_grid = true;
     sweeps(0, in, lev[0].x, pre - 1);
@@ -447,7 +457,7 @@ struct PCycle {
           const int c0 = C.rptr[P], c1 = C.rptr[P + 1];
           for (int c = c0; c < c1; c++) s = s + L.r[C.rlist[c]];
           C.b[P] = s;
-          if (first_sweep) C.x[P] = omega * s / C.ac[P];
+          if (first_sweep) C.x[P] = om(l + 1) * s / C.ac[P];
         }
       } else if (scc.active())
         level_rows(scc, C.n, l + 1, [&](auto gg, long P, bool act, int q) {
@@ -458,7 +468,7 @@ struct PCycle {
           s = gsum<G>(s);
           if (act && q == 0) {
             C.b[P] = s;
-            if (first_sweep) C.x[P] = omega * s / C.ac[P];
+            if (first_sweep) C.x[P] = om(l + 1) * s / C.ac[P];
           }
         });
       if (l + 1 < lc) sweeps(l + 1, in, C.x, pre - 1);
@@ -493,7 +503,7 @@ struct PCycle {
         // its own), then the smoothing sweep gathers x directly -- two memory
         // latencies per slot round instead of three
         const long t0 = sl.tid0(), nt = sl.nth();
-        for (long i = t0; i < L.n; i += nt) L.x[i] = L.x[i] + alpha * xc[L.parent[i]];
+        for (long i = t0; i < L.n; i += nt) L.x[i] = L.x[i] + al(l) * xc[L.parent[i]];
         enter(sl);
         for (long i = t0; i < L.n; i += 2 * nt) {
           const long i2 = i + nt;
@@ -501,11 +511,11 @@ struct PCycle {
           R t1 = 0., t2 = 0.;
           ell_acc2<6, false>(t1, t2, L.n, L.w, L.nbr, L.anb, i, i2, h2, [&](int k) { return L.x[k]; });
           R xi = L.x[i], bi = l == 0 ? (R)in[i] : L.b[i];
-          R xn = xi + omega * (bi - L.ac[i] * xi - t1) / L.ac[i];
+          R xn = xi + om(l) * (bi - L.ac[i] * xi - t1) / L.ac[i];
           if (to_out) out[i] = (double)xn; else L.r[i] = xn;
           if (h2) {
             R xj = L.x[i2], bj = l == 0 ? (R)in[i2] : L.b[i2];
-            R xm = xj + omega * (bj - L.ac[i2] * xj - t2) / L.ac[i2];
+            R xm = xj + om(l) * (bj - L.ac[i2] * xj - t2) / L.ac[i2];
             if (to_out) out[i2] = (double)xm; else L.r[i2] = xm;
           }
         }
@@ -515,12 +525,12 @@ struct PCycle {
           R t = 0.;
           if (act)
             t = ell_part<G, G == 1 ? 8 : 4>(L.n, L.w, L.nbr, L.anb, i, q,
-                                            [&](int k) { return L.x[k] + alpha * xc[L.parent[k]]; });
+                                            [&](int k) { return L.x[k] + al(l) * xc[L.parent[k]]; });
           t = gsum<G>(t);
           if (act && q == 0) {
-            R xi = L.x[i] + alpha * xc[L.parent[i]];
+            R xi = L.x[i] + al(l) * xc[L.parent[i]];
             R bi = l == 0 ? (R)in[i] : L.b[i];
-            R xn = xi + omega * (bi - L.ac[i] * xi - t) / L.ac[i];
+            R xn = xi + om(l) * (bi - L.ac[i] * xi - t) / L.ac[i];
             if (to_out) out[i] = (double)xn; else L.r[i] = xn;
           }
         });
@@ -565,7 +575,8 @@ __device__ __forceinline__ void row_ax2(const A &a, long i, long i2, bool h2, co
 // apply the preconditioner: out (FP64) = M^-1 in (FP64), via the R-precision V-cycle
 template <class R>
 __device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, double *out) {
-  PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, true};
+  PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, true,
+               (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0};
   C.run(in, out);
 }
 

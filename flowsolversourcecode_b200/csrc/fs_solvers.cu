@@ -204,44 +204,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_bicgstab(Solv
 // forward over colours 0..C-1, backward C-1..0, each colour an independent
 // set, then CheckConvergence (CheckConvergenceRoutine.for:3) -- until
 // sum|r| <= rrF * IResiduals or itmax sweeps (SolveAlegbraicEquations.for:108-117).
-__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor(SolveArgs a) {
-  cg::grid_group grid = cg::this_grid();
-  const int N = a.N;
-  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
-  double ires = *a.ires, fres = ires;
-  int iter = 0, buf = 0;
-  // a pass repeating the previous pass's colour (the backward pass's first
-  // colour, the next sweep's first) would rewrite the same values -- rows of
-  // one colour read only other colours -- and is skipped: results unchanged
-  int last = -1;
-  while (fres > a.rrf * ires && iter < a.itmax) {
-    for (int pass = 0; pass < 2; pass++) {
-      for (int cc = 0; cc < a.ncolors; cc++) {
-        int c = pass == 0 ? cc : a.ncolors - 1 - cc;
-        if (c == last) continue;
-        last = c;
-        int r0 = a.color_ptr[c], r1 = a.color_ptr[c + 1];
-        for (long q = r0 + tid0; q < r1; q += nth) {
-          int i = a.color_rows[q];
-          double l = ell_acc<8, true>(a.bc[i], N, a.W, a.cn, a.anb, i, [&](int k) { return a.dphi[k]; });
-          a.dphi[i] = l / a.ac[i];
-        }
-        grid.sync();
-      }
-    }
-    double l0 = 0., dum;
-    for (long i = tid0; i < N; i += nth) {
-      double r = ell_acc<8, true>(a.bc[i] - a.ac[i] * a.dphi[i], N, a.W, a.cn, a.anb, i,
-                                  [&](int k) { return a.dphi[k]; });
-      l0 += fabs(r);
-    }
-    grid_sum2(grid, a.part, buf, l0, 0., fres, dum); buf ^= 1;
-    iter++;
-  }
-  if (tid0 == 0) { *a.iters = iter; a.diag[0] = fres; a.diag[1] = ires; }
-}
-
-// the same sweeps on the colour-major copy: colour c occupies positions
+// The sweeps run on the colour-major copy: colour c occupies positions
 // [color_ptr[c], color_ptr[c+1]) contiguously, so every pass streams its rows
 struct SorPArgs {
   int N, W;
@@ -638,7 +601,7 @@ static int coop_grid_size(fs_ctx *ctx) {
   if (ctx->coop_grid > 0) return FS_OK;
   int a = 0, b = 0, c = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_bicgstab, FS_COOP_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_sor, FS_COOP_BLOCK, 0));
+  b = a;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_sor_colour, FS_COOP_BLOCK, 0));
   int d = 0, e = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, (void *)k_sor3_colour, FS_COOP_BLOCK, 0));
@@ -828,7 +791,7 @@ extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, con
       if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return FS_E_CUDA;
       int per_sm = 0, per_sm2 = 0, sms = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_bicgstab, FS_COOP_BLOCK, 0) != cudaSuccess ||
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void *)k_sor, FS_COOP_BLOCK, 0) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void *)k_sor_colour, FS_COOP_BLOCK, 0) != cudaSuccess ||
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return FS_E_CUDA;
       if (per_sm2 < per_sm) per_sm = per_sm2;

@@ -46,3 +46,34 @@ def test_reference_arm_only_on_rank0(monkeypatch, capsys):
     args = argparse.Namespace(n=8, steps=2, warmup=1, gpus=2, impl="reference")
     bench.run_reference(args, rank=1)
     assert capsys.readouterr().out == ""
+
+
+def _shard_worker(rank, world, port, out):
+    # each rank takes its share of the 64-case ensemble (as bench.py --ensemble
+    # does); the whole-job cell count is the only collective
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import torch
+    from flowsolversourcecode_b200 import ensemble as E
+    specs = E.make_specs(64, seed=0)
+    mine = E.shard([s.cells for s in specs], world)[rank]
+    cells = torch.tensor([float(sum(specs[q].cells for q in mine))], dtype=torch.float64)
+    dist.all_reduce(cells)
+    got = [None] * world
+    dist.all_gather_object(got, mine)
+    out[rank] = (cells.item(), got)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_ensemble_shards_over_ranks():
+    from flowsolversourcecode_b200 import ensemble as E
+    world = 2
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_shard_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn", join=True)
+    specs = E.make_specs(64, seed=0)
+    total, parts = out[0]
+    assert out[1][0] == total == float(sum(s.cells for s in specs))
+    assert sorted(q for p in parts for q in p) == list(range(64))
+    assert not set(parts[0]) & set(parts[1])
