@@ -16,6 +16,7 @@ Forms (same case, same initial state):
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                   [--ttr MAXIT]
   python bench.py --ensemble 64 [--gpus N]     the batched-ensemble configuration
+  python bench.py --case distorted             the same cavity on the jittered mesh
 
 b200 arm: `value` is device-timed (CUDA events on the solver's stream) with
 the state resident in HBM; `e2e` runs the fp64 steps through the C ABI
@@ -79,10 +80,17 @@ def aggregate_rate(world: int, steps: int, ms_max: float) -> float:
     return world * steps / (ms_max * 1e-3)
 
 
-def workload(n: int, form: str = "fp64"):
+def workload(n: int, form: str = "fp64", distorted: bool = False):
+    """The n^3 cavity (Re 1000, SOU); distorted: interior nodes jittered by
+    U(-0.2h, 0.2h) from seed 0 (non-orthogonal correction is always on:
+    MethodCalcGradient 2 and MethodDecomposeS 3)."""
     from flowsolversourcecode_b200 import case as cs
     kw = REFERENCE_SOLVERS if form == "reference" else FORMS[form]
-    return cs.cavity3d(n, **kw)
+    return cs.cavity3d_distorted(n, seed=0, **kw) if distorted else cs.cavity3d(n, **kw)
+
+
+def workload_name(n: int, distorted: bool) -> str:
+    return f"cavity3d_{n}" + ("_distorted (interior nodes jittered +-20% h, seed 0)" if distorted else "")
 
 
 class Clocks:
@@ -231,9 +239,9 @@ def solver_roofline(stats: dict, mg: dict | None, N: int, W: int, hbm: float, fo
             "iters_per_launch": best["iters"] / best["calls"]}
 
 
-def cpu_baseline_sample(n: int) -> dict:
+def cpu_baseline_sample(n: int, distorted: bool = False) -> dict:
     import oracle
-    mesh, case = workload(n, "reference")
+    mesh, case = workload(n, "reference", distorted)
     o = oracle.Oracle(mesh, case)
     t0 = time.perf_counter()
     o.simple_iteration()
@@ -249,7 +257,7 @@ def run_reference(args, rank: int) -> None:
         return
     import oracle
     oracle.build()
-    mesh, case = workload(args.n, "reference")
+    mesh, case = workload(args.n, "reference", args.case == "distorted")
     o = oracle.Oracle(mesh, case)
     warm = 1
     t0 = time.perf_counter()
@@ -272,7 +280,8 @@ def run_reference(args, rank: int) -> None:
         "impl": "reference", "metric": "SIMPLE iters/s", "value": val, "unit": "iter/s", "n_gpus": args.gpus,
         "steps": k_run, "warmup": warm, "ms_per_step": 1e3 * total / k_run,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"cavity3d_{args.n} lid-driven cavity, {mesh.n_cells} cells, Re=1000, SOU, SIMPLEC",
+        "config": {"workload": f"{workload_name(args.n, args.case == 'distorted')} lid-driven cavity, "
+                               f"{mesh.n_cells} cells, Re=1000, SOU, SIMPLEC",
                    "cells": mesh.n_cells,
                    "solvers": "momentum sor, p' bicgs (the reference's unpreconditioned BiCGSTAB) to 1e-8"},
         "cpu_baseline": {"value": val, "unit": "iter/s", "cores": 1, "kind": "port",
@@ -401,6 +410,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--case", default="cubic", choices=["cubic", "distorted"])
     ap.add_argument("--ttr", type=int, default=0, help="max iterations of the time-to-1e-6 leg (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", type=int, default=0, help="run the batched-ensemble configuration with this many cases")
@@ -440,7 +450,8 @@ def main():
             dist.barrier()
 
     warm = max(args.warmup, 3)
-    mesh, case = workload(args.n, "fp64")
+    distorted = args.case == "distorted"
+    mesh, case = workload(args.n, "fp64", distorted)
 
     # ---------------- fp64 form: device-resident leg
     s = Solver(mesh, case, device=local)
@@ -471,7 +482,7 @@ def main():
     s.close()
 
     # ---------------- mixed form: same case and initial state
-    _, case_m = workload(args.n, "mixed")
+    _, case_m = workload(args.n, "mixed", distorted)
     sm = Solver(mesh, case_m, device=local)
     dmx = device_leg(sm, args.steps, warm, barrier, local)
     msm_max = reduce_max(dmx["ms"], dist, f"cuda:{local}")
@@ -501,14 +512,14 @@ def main():
                     "fallback 6.65 TB/s"
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline_sample(args.n)
+            cpu = cpu_baseline_sample(args.n, distorted)
         value = aggregate_rate(world, args.steps, ms_max)
         line = {
             "metric": "SIMPLE iters/s", "value": value, "unit": "iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": warm, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"cavity3d_{args.n} lid-driven cavity, {N} cells, {F} interior faces, "
+            "config": {"workload": f"{workload_name(args.n, distorted)} lid-driven cavity, {N} cells, {F} interior faces, "
                                    f"Re=1000, SOU deferred correction, SIMPLEC urf 0.7/0.7",
                        "cells": N, "faces": F,
                        "solvers": "momentum: multicolour SOR (rrF 0.01, 30 sweeps); p': FP64 BiCGSTAB "
