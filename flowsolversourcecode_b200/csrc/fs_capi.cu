@@ -306,7 +306,15 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   int32_t it[8];
   FS_CK(cudaMemcpyAsync(rb, ctx->resblk, sizeof(rb), cudaMemcpyDeviceToHost, ctx->st));
   FS_CK(cudaMemcpyAsync(it, ctx->d_iters, sizeof(it), cudaMemcpyDeviceToHost, ctx->st));
+  int32_t status = 0;
+  FS_CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->st));
   FS_CK(cudaStreamSynchronize(ctx->st));
+  if (status) {
+    // a bounded device wait gave up: the iteration's results are not valid
+    FS_CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t), ctx->st));
+    ctx->err = "a bounded device wait (multigrid team barrier) timed out";
+    return FS_E_TIMEOUT;
+  }
   fs_solver_stats_collect(ctx);
   fs_residuals r{};
   for (int q = 0; q < 5; q++) {

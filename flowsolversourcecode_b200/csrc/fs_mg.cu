@@ -138,11 +138,20 @@ struct Sync {
 };
 
 // which threads work on a level, and how they synchronise
+// the first FS_PC_TEAM CTAs: mid-sized preconditioner levels (PCycle)
+#define FS_PC_TEAM 32
+__device__ __forceinline__ int team_size() { return gridDim.x < FS_PC_TEAM ? (int)gridDim.x : FS_PC_TEAM; }
+
 struct Scope {
-  bool grid;   // whole grid, else CTA 0 only
-  __device__ bool active() const { return grid || blockIdx.x == 0; }
-  __device__ long tid0() const { return grid ? (long)blockIdx.x * blockDim.x + threadIdx.x : (long)threadIdx.x; }
-  __device__ long nth() const { return grid ? (long)gridDim.x * blockDim.x : (long)blockDim.x; }
+  bool grid = false;   // whole grid
+  bool team = false;   // else the first team_size() CTAs; else CTA 0 only
+  __device__ bool active() const { return grid || (team ? (int)blockIdx.x < team_size() : blockIdx.x == 0); }
+  __device__ long tid0() const {
+    return (grid || team) ? (long)blockIdx.x * blockDim.x + threadIdx.x : (long)threadIdx.x;
+  }
+  __device__ long nth() const {
+    return grid ? (long)gridDim.x * blockDim.x : team ? (long)team_size() * blockDim.x : (long)blockDim.x;
+  }
 };
 
 template <class R>
@@ -347,11 +356,23 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
 // fewer rows than the grid has threads, so there a row is handled by G
 // consecutive lanes (G = 2..8 from the threads per row) that split its
 // neighbour loop and combine by shuffles.  Levels up to FS_PC_SMALL rows run on
-// CTA 0 alone.
+// CTA 0 alone; levels up to FS_PC_TEAM_MAX rows on a team of the first
+// FS_PC_TEAM CTAs with a bounded barrier of their own in global memory -- a
+// barrier over all CTAs costs several microseconds, and those phases have too
+// little work to use the whole grid anyway.
 #define FS_PC_SMALL 256
+#ifndef FS_PC_TEAM_MAX
+#define FS_PC_TEAM_MAX 4096   // levels up to this many rows run on the CTA team
+#endif
+#define FS_PC_SPIN_LIMIT (1L << 20)   // polls of a team barrier before it reports a timeout
 
 template <class R>
-__device__ __forceinline__ Scope pc_scope(const LevelDev<R> &L) { Scope s; s.grid = L.n > FS_PC_SMALL; return s; }
+__device__ __forceinline__ Scope pc_scope(const LevelDev<R> &L) {
+  Scope s;
+  s.grid = L.n > FS_PC_TEAM_MAX;
+  s.team = !s.grid && L.n > FS_PC_SMALL;
+  return s;
+}
 
 template <int G, class T>
 __device__ __forceinline__ T gsum(T v) {
@@ -392,13 +413,48 @@ struct PCycle {
   const double *sinv;  // lev[lc].n^2, row-major
   int pre, post, coarse_sweeps;
   R omega, alpha;        // Jacobi weight and coarse-correction factor on levels >= 1
-  bool last_grid;
+  Scope last;            // scope of the previous phase
   R omega0, alpha0;      // the same on level 0
+  unsigned *bar;         // team barrier: [0] arrivals, [1] generation (zero at launch)
+  int32_t *status;       // [0] set when a team barrier timed out
+  unsigned gen;          // generation this CTA waits to leave
   __device__ R om(int l) const { return l == 0 ? omega0 : omega; }
   __device__ R al(int l) const { return l == 0 ? alpha0 : alpha; }
+  // barrier among the team CTAs: the arrival count in global memory, the last
+  // arrival resets it and bumps the generation the others poll; polls are
+  // bounded, and a timeout is recorded (later team barriers then stop
+  // waiting).  Out of line: inlined at every phase it doubled the kernel's
+  // register spills.
+  __device__ __noinline__ void team_sync() {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned g = gen, T = (unsigned)team_size();
+      if (atomicAdd(&bar[0], 1u) == T - 1) {
+        atomicExch(&bar[0], 0u);
+        __threadfence();
+        atomicAdd(&bar[1], 1u);
+      } else {
+        const volatile unsigned *vg = bar + 1;
+        const volatile int32_t *vs = status;
+        long spins = 0;
+        while (*vg == g && *vs == 0) {
+          if (++spins > FS_PC_SPIN_LIMIT) { atomicExch(status, 1); break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    gen++;
+    __syncthreads();
+  }
+  // the barrier before a phase: grid-wide when the grid is involved on either
+  // side, among the team when the team is, else within CTA 0
   __device__ void enter(const Scope &sc) {
-    if (sc.grid || last_grid) S.all(); else __syncthreads();
-    last_grid = sc.grid;
+    if (sc.grid || last.grid) S.all();
+    else if (sc.team || last.team) { if ((int)blockIdx.x < team_size()) team_sync(); }
+    else __syncthreads();
+    last = sc;
   }
   // r (into dst) = b - A x on level l; level 0 takes b from `in`
   __device__ void residual(int l, const double *__restrict__ in, const R *__restrict__ x, R *__restrict__ dst) {
@@ -443,7 +499,8 @@ struct PCycle {
       const LevelDev<R> L0 = lev[0];
       for (long i = g.tid0(); i < L0.n; i += g.nth()) L0.x[i] = omega0 * (R)in[i] / L0.ac[i];
     }
-    last_grid = true;
+    last.grid = true;
+    last.team = false;
     sweeps(0, in, lev[0].x, pre - 1);
     for (int l = 0; l < lc; l++) {
       const LevelDev<R> L = lev[l], C = lev[l + 1];
@@ -560,6 +617,8 @@ struct AmgKArgs {
   double *diag;
   const double *x0;   // initial guess (nullptr: zero)
   int32_t *nncnt;     // [fallbacks, uses] of the initial guess, or nullptr
+  unsigned *teambar;  // team barrier words of the V-cycle (zeroed before the launch)
+  int32_t *status;    // [0] team-barrier timeout flag
 };
 
 // rows i and i2 (when h2) of A x at once (ell_acc2)
@@ -574,16 +633,20 @@ __device__ __forceinline__ void row_ax2(const A &a, long i, long i2, bool h2, co
 
 // apply the preconditioner: out (FP64) = M^-1 in (FP64), via the R-precision V-cycle
 template <class R>
-__device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, double *out) {
-  PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, true,
-               (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0};
+__device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, double *out, unsigned &gen) {
+  Scope all;
+  all.grid = true;
+  PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, all,
+               (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0, a.teambar, a.status, gen};
   C.run(in, out);
+  gen = C.gen;
 }
 
 // right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle
 template <class R>
 __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(AmgKArgs<R> a) {
   Sync S(a.part);
+  unsigned gen = 0;   // team-barrier generation (the counters are zeroed before the launch)
   const int N = a.N;
   Scope g; g.grid = true;
   const long t0 = g.tid0(), nt = g.nth();
@@ -636,7 +699,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     rho = rho1;
     for (long i = t0; i < N; i += nt) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
     S.all();
-    apply_prec<R>(S, a, a.p, a.y);                                  // y = M^-1 p
+    apply_prec<R>(S, a, a.p, a.y, gen);                             // y = M^-1 p
     l0 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
       const long i2 = i + nt;
@@ -658,7 +721,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
       resn = sqrt(ss);
       break;
     }
-    apply_prec<R>(S, a, a.s, a.z);                                  // z = M^-1 s
+    apply_prec<R>(S, a, a.s, a.z, gen);                             // z = M^-1 s
     l0 = 0.; l1 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
       const long i2 = i + nt;
@@ -1065,6 +1128,8 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     return FS_OK;
   }
   if ((rc = mg_coarse_matrices(ctx, M->lc, f32))) return rc;
+  // team-barrier counters of the V-cycle start at zero for every launch
+  FS_CK(cudaMemsetAsync(ctx->d_status + 4, 0, sizeof(int32_t) * 2, ctx->st));
   if (M->direct) {
     const int n = M->n[M->lc];
     k_mg_dense_inverse<<<1, 1024, sizeof(double) * ((size_t)n * n + n), ctx->st>>>(
@@ -1082,6 +1147,8 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + 22;
     a.x0 = nf == FS_VAR_PC ? ctx->pc_guess : nullptr;
     a.nncnt = fs_nn_counters(ctx);
+    a.teambar = (unsigned *)(ctx->d_status + 4);
+    a.status = ctx->d_status;
   };
   if (!f32) {
     AmgKArgs<double> a{};
