@@ -108,6 +108,7 @@ struct fs_ctx {
   int coop_grid = 0;            // blocks of a cooperative solver launch
   int coop_per_sm = 0;          // launch shape: cooperative CTAs per SM (0: up to 4; fs_set_launch_shape)
   bool graph_mode = false;      // enqueueing for stream capture: no host syncs, no timing events
+  int test_wait_extra = 0;      // fs_test_wait_timeout: extra arrivals the team barrier waits for
 };
 
 // timing events and their host-side bookkeeping are skipped while a graph is captured

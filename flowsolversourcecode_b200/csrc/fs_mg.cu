@@ -418,6 +418,7 @@ struct PCycle {
   unsigned *bar;         // team barrier: [0] arrivals, [1] generation (zero at launch)
   int32_t *status;       // [0] set when a team barrier timed out
   unsigned gen;          // generation this CTA waits to leave
+  int extra;             // arrivals waited for beyond the team (0; >0 only to test the timeout)
   __device__ R om(int l) const { return l == 0 ? omega0 : omega; }
   __device__ R al(int l) const { return l == 0 ? alpha0 : alpha; }
   // barrier among the team CTAs: the arrival count in global memory, the last
@@ -429,7 +430,7 @@ struct PCycle {
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
-      const unsigned g = gen, T = (unsigned)team_size();
+      const unsigned g = gen, T = (unsigned)(team_size() + extra);
       if (atomicAdd(&bar[0], 1u) == T - 1) {
         atomicExch(&bar[0], 0u);
         __threadfence();
@@ -619,6 +620,7 @@ struct AmgKArgs {
   int32_t *nncnt;     // [fallbacks, uses] of the initial guess, or nullptr
   unsigned *teambar;  // team barrier words of the V-cycle (zeroed before the launch)
   int32_t *status;    // [0] team-barrier timeout flag
+  int team_extra;     // fs_test_wait_timeout
 };
 
 // rows i and i2 (when h2) of A x at once (ell_acc2)
@@ -637,7 +639,7 @@ __device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, doub
   Scope all;
   all.grid = true;
   PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, all,
-               (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0, a.teambar, a.status, gen};
+               (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0, a.teambar, a.status, gen, a.team_extra};
   C.run(in, out);
   gen = C.gen;
 }
@@ -1149,6 +1151,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.nncnt = fs_nn_counters(ctx);
     a.teambar = (unsigned *)(ctx->d_status + 4);
     a.status = ctx->d_status;
+    a.team_extra = ctx->test_wait_extra;
   };
   if (!f32) {
     AmgKArgs<double> a{};
@@ -1198,5 +1201,14 @@ extern "C" int fs_mg_info(fs_ctx *ctx, int32_t *widths, int max_levels, int32_t 
     for (int q = 0; q < ctx->mg->nlev && q < max_levels; q++) widths[q] = ctx->mg->w[q];
   if (prec_coarsest) *prec_coarsest = ctx->mg->lc;
   if (direct) *direct = ctx->mg->direct ? 1 : 0;
+  return FS_OK;
+}
+
+// Test of the bounded device waits (no reference counterpart): with extra > 0
+// the multigrid team barriers wait for more CTAs than the team has, so their
+// polls run out; the solve then ends and the iteration reports FS_E_TIMEOUT.
+extern "C" int fs_test_wait_timeout(fs_ctx *ctx, int extra) {
+  if (!ctx || extra < 0 || extra > 64) return FS_E_ARG;
+  ctx->test_wait_extra = extra;
   return FS_OK;
 }

@@ -308,6 +308,12 @@ int fs_nn_policy(fs_ctx *ctx, double *avg_guessed, double *avg_zero, int32_t *pa
  *   ordinary iteration per case runs first (hierarchies, colourings, grids);
  *   the learned guess is not used inside the graph. */
 int fs_set_launch_shape(fs_ctx *ctx, int ctas_per_sm);
+/* Test of the bounded device waits (no reference counterpart): with extra > 0
+ * the AMG preconditioner's team barriers wait for `extra` more CTAs than take
+ * part, so their bounded polls run out (well under a second); the iteration
+ * then returns FS_E_TIMEOUT and its results are not valid.  0 restores normal
+ * operation. */
+int fs_test_wait_timeout(fs_ctx *ctx, int extra);
 int fs_ensemble_run(fs_ctx **ctxs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
                     float *ms_out);
 

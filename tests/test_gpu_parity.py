@@ -354,3 +354,32 @@ def test_batched_momentum_same_fixed_point():
     for k in ("u", "v", "w"):
         x, y = a.get(k), b.get(k)
         assert np.linalg.norm(x - y) <= 1e-8 * np.linalg.norm(x), k
+
+
+def test_bounded_wait_runs_out_and_reports_timeout():
+    # Failure detection without a GPU fault: the AMG preconditioner's team
+    # barriers are made to wait for one CTA more than takes part, so their
+    # bounded polls run out; the iteration must come back with FS_E_TIMEOUT in
+    # about a second, and the device and the library must stay usable.
+    import ctypes as C
+    import time
+    from flowsolversourcecode_b200 import _lib as Lb
+    from flowsolversourcecode_b200.solver import Solver
+    mesh, case = cs.cavity(12, nz=12, solver_cont="amg_bicgs", krylov_tol=1e-8, krylov_maxit=50)
+    s = Solver(mesh, case)
+    s.simple_iteration()
+    assert s.lib.fs_test_wait_timeout(s.ctx, 1) == 0
+    r = Lb.FsResiduals()
+    t0 = time.time()
+    rc = s.lib.fs_simple_iteration(s.ctx, C.byref(r))
+    dt = time.time() - t0
+    assert rc == Lb.FS_E_TIMEOUT, rc
+    assert dt < 10.0, dt
+    assert b"timed out" in s.lib.fs_last_error(s.ctx)
+    assert s.lib.fs_test_wait_timeout(s.ctx, 0) == 0
+    s.close()
+    t = Solver(mesh, case)
+    for _ in range(2):
+        res = t.simple_iteration()
+    assert np.isfinite(res["source"])
+    t.close()
