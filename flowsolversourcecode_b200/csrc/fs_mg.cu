@@ -139,7 +139,9 @@ struct Sync {
 
 // which threads work on a level, and how they synchronise
 // the first FS_PC_TEAM CTAs: mid-sized preconditioner levels (PCycle)
+#ifndef FS_PC_TEAM
 #define FS_PC_TEAM 32
+#endif
 __device__ __forceinline__ int team_size() { return gridDim.x < FS_PC_TEAM ? (int)gridDim.x : FS_PC_TEAM; }
 
 struct Scope {
@@ -424,9 +426,15 @@ struct PCycle {
   // barrier among the team CTAs: the arrival count in global memory, the last
   // arrival resets it and bumps the generation the others poll; polls are
   // bounded, and a timeout is recorded (later team barriers then stop
-  // waiting).  Out of line: inlined at every phase it doubled the kernel's
-  // register spills.
-  __device__ __noinline__ void team_sync() {
+  // waiting).  The FP64 cycle calls it out of line (inlined at every phase it
+  // doubled that kernel's register spills); the FP32 cycle, with fewer live
+  // registers, runs faster with it inline.
+  __device__ __noinline__ void team_sync_call() { team_sync_body(); }
+  __device__ __forceinline__ void team_sync() {
+    if (sizeof(R) == sizeof(double)) team_sync_call();
+    else team_sync_body();
+  }
+  __device__ __forceinline__ void team_sync_body() {
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
