@@ -24,6 +24,7 @@ FS_NOALLOC_MAX_ROWS = 262144
 FS_NN_NPARAM = 33665
 # variable ids (GetNFfromVariable)
 VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
+VAR_TKE, VAR_TED, VAR_RHOK = 8, 9, 10
 # boundary types
 BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD = 0, 1, 2, 3, 4
 # gradient interpolation
@@ -36,7 +37,8 @@ SIMPLE, SIMPLEC = 0, 1
 
 FIELDS = ["u", "v", "w", "p", "pc", "mdot", "bu", "bv", "bw", "bp", "bpc", "bmdot", "ac", "bc", "anb",
           "du1", "dv1", "dw1", "du2", "dv2", "dw2", "ugrad", "vgrad", "wgrad", "pgrad", "pcgrad",
-          "volume", "xc", "gfactor", "sf", "gdiff", "ft", "bsf", "dphi"]
+          "volume", "xc", "gfactor", "sf", "gdiff", "ft", "bsf", "dphi",
+          "tke", "ted", "mut", "btke", "bted", "bmut"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
 
@@ -60,6 +62,14 @@ class FsCase(C.Structure):
         ("n_patches", C.c_int), ("patch_type", C.c_int * FS_MAX_PATCHES),
         ("patch_vel", (C.c_double * 3) * FS_MAX_PATCHES),
         ("batched_momentum", C.c_int),
+        ("mass_flow_fraction", C.c_double * FS_MAX_PATCHES),
+        ("turbulence", C.c_int), ("solver_turb", C.c_int),
+        ("rrf_tke", C.c_double), ("rrf_ted", C.c_double),
+        ("itmax_tke", C.c_int), ("itmax_ted", C.c_int),
+        ("urf_tke", C.c_double), ("urf_ted", C.c_double), ("urf_tvisc", C.c_double),
+        ("max_visc_ratio", C.c_double), ("limit_production", C.c_int),
+        ("conv_scheme_tke", C.c_int), ("conv_scheme_ted", C.c_int),
+        ("inlet_intensity", C.c_double * FS_MAX_PATCHES), ("inlet_length", C.c_double * FS_MAX_PATCHES),
     ]
 
 
@@ -77,12 +87,16 @@ class FsResiduals(C.Structure):
         ("abs_", C.c_double * 5), ("max_", C.c_double * 5), ("rms", C.c_double * 5), ("scaled", C.c_double * 5),
         ("overall_imbalance", C.c_double), ("imax_imbalance", C.c_int), ("lin_iters", C.c_int * 5),
         ("source", C.c_double),
+        ("turb_abs", C.c_double * 2), ("turb_max", C.c_double * 2), ("turb_rms", C.c_double * 2),
+        ("turb_scaled", C.c_double * 2), ("turb_lin_iters", C.c_int * 2),
     ]
 
     def as_dict(self) -> dict:
         return {"abs": list(self.abs_), "max": list(self.max_), "rms": list(self.rms), "scaled": list(self.scaled),
                 "overall_imbalance": self.overall_imbalance, "imax_imbalance": self.imax_imbalance,
-                "lin_iters": list(self.lin_iters), "source": self.source}
+                "lin_iters": list(self.lin_iters), "source": self.source,
+                "turb_abs": list(self.turb_abs), "turb_max": list(self.turb_max), "turb_rms": list(self.turb_rms),
+                "turb_scaled": list(self.turb_scaled), "turb_lin_iters": list(self.turb_lin_iters)}
 
 
 # every entry point of include/fsb200.h with its argument types
@@ -102,6 +116,7 @@ PROTOTYPES = {
     "fs_assemble_continuity": (C.c_int, [_V]),
     "fs_correct_continuity": (C.c_int, [_V]),
     "fs_set_iteration": (C.c_int, [_V, C.c_int]),
+    "fs_initialize_mdot": (C.c_int, [_V]),
     "fs_gradient": (C.c_int, [_V, C.c_int, C.c_int, C.c_int]),
     "fs_gradient_host": (C.c_int, [_V, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D]),
     "fs_under_relax": (C.c_int, [_V, C.c_double]),

@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib as L
-from .mesh import BOX_PATCHES, PolyMesh, box_mesh
+from .mesh import BFS_PATCHES, BOX_PATCHES, PolyMesh, bfs_mesh, box_mesh, uniform01
 
 
 def ref_real(x: float) -> float:
@@ -72,6 +72,24 @@ class Case:
     batched_momentum: bool = False
     # patches: name -> (type, (u,v,w))
     patches: dict = field(default_factory=dict)
+    # 'fullydeveloped' outlets: patch name -> MassFlowFraction (default 1)
+    mass_flow_fraction: dict = field(default_factory=dict)
+    # k-epsilon (TurbulenceModel='kepsilon', equilibrium 'standard' wall functions)
+    turbulence: bool = False
+    solver_turb: str = "sor"               # ASSolverTKE = ASSolverTED
+    rrf_tke: float = 0.1                   # rrfTKE
+    rrf_ted: float = 0.1                   # rrfTED
+    itmax_tke: int = 10                    # ASIterTKE
+    itmax_ted: int = 3                     # ASIterTED
+    urf_tke: float = 0.5                   # urfTKE
+    urf_ted: float = 0.5                   # urfTED
+    urf_tvisc: float = 0.5                 # urfTViscosity
+    max_visc_ratio: float = 1.0e6          # MaximumViscosityRatio
+    limit_production: bool = True          # LimitTurbulenceProduction
+    conv_scheme_tke: str = "upwind"        # ConvectionSchemeTKE
+    conv_scheme_ted: str = "minmod"        # ConvectionSchemeTED
+    # inlet patch name -> (inletTurbulenceIntensity, inletTurbulenceLengthScale), 'specifiedil'
+    inlet_turbulence: dict = field(default_factory=dict)
 
     def struct(self, mesh: PolyMesh) -> L.FsCase:
         c = L.FsCase()
@@ -108,6 +126,16 @@ class Case:
             c.patch_type[s] = bct[t]
             for q in range(3):
                 c.patch_vel[s][q] = float(vel[q])
+            c.mass_flow_fraction[s] = float(self.mass_flow_fraction.get(name, 1.0))
+            it, il = self.inlet_turbulence.get(name, (0.0, 1.0))
+            c.inlet_intensity[s], c.inlet_length[s] = float(it), float(il)
+        c.turbulence = int(self.turbulence)
+        c.solver_turb = L.SOLVER[self.solver_turb]
+        c.rrf_tke, c.rrf_ted = self.rrf_tke, self.rrf_ted
+        c.itmax_tke, c.itmax_ted = self.itmax_tke, self.itmax_ted
+        c.urf_tke, c.urf_ted, c.urf_tvisc = self.urf_tke, self.urf_ted, self.urf_tvisc
+        c.max_visc_ratio, c.limit_production = self.max_visc_ratio, int(self.limit_production)
+        c.conv_scheme_tke, c.conv_scheme_ted = L.TVD[self.conv_scheme_tke], L.TVD[self.conv_scheme_ted]
         return c
 
 
@@ -149,3 +177,54 @@ def cavity3d_distorted(n: int = 128, seed: int = 0, **kw):
     kw.setdefault("conv_scheme", "sou")
     kw.setdefault("niter_start_hr", 1)
     return cavity(n, re=1000.0, jitter=0.2, seed=seed, **kw)
+
+
+def bfs(nx: int = 512, ny: int = 96, nz: int = 48, re_h: float = 5000.0, intensity: float = 0.05,
+        length: float = 0.1, **kw) -> tuple[PolyMesh, Case]:
+    """3-D backward-facing step, steady RANS k-epsilon with wall functions.
+
+    Channel 30H x 3H x 2H (H = 1), step wall at x = 0 for y < H, inlet at
+    x = 0 for y >= H with u = 1, outlet 'fullydeveloped' at x = 30H, no-slip
+    walls elsewhere; rho = 1, mu = 1/Re_H.  Inlet turbulence 'specifiedil'
+    with the given intensity and length scale.  Second-order upwind deferred
+    correction for momentum from iteration 1.  Use :func:`bfs_initial_state`
+    for the initial fields (perturbed inlet profile)."""
+    mesh = bfs_mesh(nx, ny, nz)
+    patches = {p: ("wall", (0.0, 0.0, 0.0)) for p in BFS_PATCHES}
+    patches["inlet"] = ("inlet", (1.0, 0.0, 0.0))
+    patches["xmax"] = ("outlet", (0.0, 0.0, 0.0))
+    kw.setdefault("conv_scheme", "sou")
+    kw.setdefault("niter_start_hr", 1)
+    kw.setdefault("turbulence", True)
+    case = Case(mu=1.0 / re_h, patches=patches, inlet_turbulence={"inlet": (intensity, length)}, **kw)
+    return mesh, case
+
+
+def bfs_initial_state(mesh: PolyMesh, case: Case, seed: int = 0, perturbation: float = 0.05) -> dict:
+    """Initial fields of the step case: u = 1 in every cell and on the outlet,
+    inlet faces u = 1 + perturbation * U(-1, 1) (splitmix64 from `seed`, one
+    draw per inlet face in boundary order), k and epsilon uniform at the
+    inlet-turbulence values of a unit velocity (k = 1.5 I^2, eps =
+    Cmu^0.75 k^1.5 / L) and mu_t = Cmu rho k^2 / eps, on cells and boundary faces.
+    Apply with ``obj.set(name, value)`` for every item, then
+    ``obj.initialize_mdot()``."""
+    N = mesh.n_cells
+    B = mesh.n_faces - mesh.n_internal
+    F = mesh.n_internal
+    s_in = mesh.patch("inlet")
+    b0 = int(mesh.patch_start[s_in]) - F
+    nin = int(mesh.patch_size[s_in])
+    bu = np.zeros(B)
+    s_out = mesh.patch("xmax")
+    o0 = int(mesh.patch_start[s_out]) - F
+    bu[o0:o0 + int(mesh.patch_size[s_out])] = 1.0
+    bu[b0:b0 + nin] = 1.0 + perturbation * (2.0 * uniform01(seed, nin) - 1.0)
+    it, ln = case.inlet_turbulence.get("inlet", (0.05, 0.1))
+    k0 = 1.5 * 1.0 * it * it
+    cmu = float(np.float32(0.09))
+    cmu75 = np.sqrt(np.sqrt(cmu)) ** 3
+    e0 = cmu75 * k0 ** 1.5 / ln
+    mut0 = cmu * case.rho * k0 * k0 / e0
+    return {"u": np.ones(N), "bu": bu,
+            "tke": np.full(N, k0), "ted": np.full(N, e0), "mut": np.full(N, mut0),
+            "btke": np.full(B, k0), "bted": np.full(B, e0), "bmut": np.full(B, mut0)}

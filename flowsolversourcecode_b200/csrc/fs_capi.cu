@@ -123,6 +123,8 @@ static double *field_ptr(fs_ctx *c, int f, size_t *n) {
   case FS_F_FT: *n = 3 * F; return c->tf;
   case FS_F_BSF: *n = 3 * B; return c->bsf;
   case FS_F_DPHI: *n = N; return c->dphi;
+  case FS_F_TKE: case FS_F_TED: case FS_F_MUT: case FS_F_BTKE: case FS_F_BTED: case FS_F_BMUT:
+    return fs_turb_field(c, f, n);
   }
   *n = 0;
   return nullptr;
@@ -145,7 +147,7 @@ static void free_all(fs_ctx *c) {
                   c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky, c->sysx,
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
                   c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP,
-                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm};
+                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm, c->d_bset, c->flow};
   for (void *p : ptrs) if (p) cudaFree(p);
 }
 
@@ -161,7 +163,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   ctx->cfg = *cfg;
   ctx->dev = device;
   int rc = FS_OK;
-  auto fail = [&](int r) { free_all(ctx); if (ctx->st) cudaStreamDestroy(ctx->st); delete ctx; return r; };
+  auto fail = [&](int r) { fs_turb_free(ctx); free_all(ctx); if (ctx->st) cudaStreamDestroy(ctx->st); delete ctx; return r; };
   if (cudaSetDevice(device) != cudaSuccess) return fail(FS_E_CUDA);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(FS_E_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -199,10 +201,14 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   if ((rc = alloc0(ctx, &ctx->red, nred))) return fail(rc);
   if (cudaMalloc(&ctx->redi, sizeof(int64_t) * (nblk > FS_RED_BLOCKS ? nblk : FS_RED_BLOCKS)) != cudaSuccess) return fail(FS_E_NOMEM);
   if ((rc = alloc0(ctx, &ctx->resblk, RB_SIZE))) return fail(rc);
-  if (cudaMalloc(&ctx->d_iters, sizeof(int32_t) * 8) != cudaSuccess) return fail(FS_E_NOMEM);
-  cudaMemsetAsync(ctx->d_iters, 0, sizeof(int32_t) * 8, ctx->st);
+  if (cudaMalloc(&ctx->d_iters, sizeof(int32_t) * FS_NITERS) != cudaSuccess) return fail(FS_E_NOMEM);
+  cudaMemsetAsync(ctx->d_iters, 0, sizeof(int32_t) * FS_NITERS, ctx->st);
   if (cudaMalloc(&ctx->d_status, sizeof(int32_t) * 8) != cudaSuccess) return fail(FS_E_NOMEM);
   cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t) * 8, ctx->st);
+  if ((rc = alloc0(ctx, &ctx->flow, 1 + 2 * FS_MAX_PATCHES))) return fail(rc);
+  if (cudaMalloc(&ctx->d_bset, sizeof(int32_t) * (B ? B : 1)) != cudaSuccess) return fail(FS_E_NOMEM);
+  if (B) cudaMemcpyAsync(ctx->d_bset, ctx->h_bset.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice, ctx->st);
+  if ((rc = fs_turb_create(ctx))) return fail(rc);
   // boundary values from the patches (setBoundaryConditions): wall / inlet velocities
   std::vector<double> hb(3 * B, 0.);
   for (size_t b = 0; b < B; b++) {
@@ -230,6 +236,7 @@ int fs_destroy(fs_ctx *ctx) {
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   fs_mg_free(ctx);
   fs_nn_free(ctx);
+  fs_turb_free(ctx);
   free_all(ctx);
   for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto &e : ctx->tev) if (e) cudaEventDestroy(e);
@@ -291,6 +298,17 @@ int fs_set_iteration(fs_ctx *ctx, int n_iter) {
   return FS_OK;
 }
 
+int fs_initialize_mdot(fs_ctx *ctx) {
+  if (!ctx) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  const int N = ctx->N, F = ctx->F, B = ctx->B;
+  k_initial_mdot<<<fs_grid((long)F + B), FS_BLOCK, 0, ctx->st>>>(N, F, B, ctx->cfg.rho, ctx->fown, ctx->fnbr,
+      ctx->gf, ctx->sf, ctx->u, ctx->v, ctx->w, ctx->mdot, ctx->btype, ctx->bsf, ctx->bu, ctx->bv, ctx->bw, ctx->bmdot);
+  FS_LAUNCH_CHECK();
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  return FS_OK;
+}
+
 // PrintConvergenceHistory stop metric (PrintConvergenceToFileAndScreen.for:613-700)
 // from a device residual block
 static double stop_metric(const fs_case &c, const double *rb) {
@@ -298,12 +316,13 @@ static double stop_metric(const fs_case &c, const double *rb) {
   double s = 0.;
   s = fmax(s, fmax(fabs(rb[o]), fmax(fabs(rb[o + 1]), fabs(rb[o + 2]))));
   s = fmax(s, fabs(rb[o + 4]));
+  if (c.turbulence) { s = fmax(s, fabs(rb[o + FS_VAR_TKE - 1])); s = fmax(s, fabs(rb[o + FS_VAR_TED - 1])); }
   return s;
 }
 
 static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   double rb[RB_SIZE];
-  int32_t it[8];
+  int32_t it[FS_NITERS];
   FS_CK(cudaMemcpyAsync(rb, ctx->resblk, sizeof(rb), cudaMemcpyDeviceToHost, ctx->st));
   FS_CK(cudaMemcpyAsync(it, ctx->d_iters, sizeof(it), cudaMemcpyDeviceToHost, ctx->st));
   int32_t status = 0;
@@ -321,6 +340,11 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
     r.abs_[q] = rb[RB_ABS + q]; r.max_[q] = rb[RB_MAX + q]; r.rms[q] = rb[RB_RMS + q]; r.scaled[q] = rb[RB_SCL + q];
     r.lin_iters[q] = it[q];
   }
+  for (int q = 0; q < 2; q++) {
+    const int e = FS_VAR_TKE - 1 + q;
+    r.turb_abs[q] = rb[RB_ABS + e]; r.turb_max[q] = rb[RB_MAX + e]; r.turb_rms[q] = rb[RB_RMS + e];
+    r.turb_scaled[q] = rb[RB_SCL + e]; r.turb_lin_iters[q] = it[e];
+  }
   if (ctx->nn) fs_nn_note_iters(ctx, it[FS_VAR_PC - 1]);
   r.overall_imbalance = rb[RB_OVERALL];
   r.imax_imbalance = (int)rb[RB_IMAX];
@@ -328,6 +352,9 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   if (res) *res = r;
   for (int q = 0; q < 5; q++)
     if (!std::isfinite(r.abs_[q])) { ctx->err = "NaN/Inf residual"; return FS_E_NAN; }
+  if (ctx->cfg.turbulence)
+    for (int q = 0; q < 2; q++)
+      if (!std::isfinite(r.turb_abs[q])) { ctx->err = "NaN/Inf residual"; return FS_E_NAN; }
   return FS_OK;
 }
 
@@ -357,6 +384,8 @@ static int iteration_body(fs_ctx *ctx) {
   if (rc) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[3], ctx->st));
   if ((rc = fs_continuity_correct(ctx))) return rc;
+  // CalculateEffectsOfTurbulence (MainProgram.for:275-277)
+  if ((rc = fs_turb_effects(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[4], ctx->st));
   return FS_OK;
 }
@@ -597,7 +626,7 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
       if (rc) { if (c != ctx) ctx->err = c->err; return rc; }
     } while (c->nIter < c->cfg.niter_start_hr);
   }
-  const size_t slot = RB_SIZE + 4;  // residual block, then 8 int32 iteration counts
+  const size_t slot = RB_SIZE + FS_NITERS / 2;  // residual block, then the int32 iteration counts
   double *h = nullptr;
   FS_CK(cudaHostAlloc((void **)&h, sizeof(double) * slot * n * iters, cudaHostAllocDefault));
   cudaStream_t S = nullptr;
@@ -641,7 +670,7 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
       if (rc != FS_OK) { if (c != ctx) ctx->err = c->err; break; }
       double *d = h + ((size_t)q * iters + t) * slot;
       if ((e = cudaMemcpyAsync(d, c->resblk, sizeof(double) * RB_SIZE, cudaMemcpyDeviceToHost, c->st)) != cudaSuccess ||
-          (e = cudaMemcpyAsync(d + RB_SIZE, c->d_iters, sizeof(int32_t) * 8, cudaMemcpyDeviceToHost, c->st)) !=
+          (e = cudaMemcpyAsync(d + RB_SIZE, c->d_iters, sizeof(int32_t) * FS_NITERS, cudaMemcpyDeviceToHost, c->st)) !=
               cudaSuccess) { what = "residual copy"; break; }
       if ((e = cudaEventRecord(ej, c->st)) != cudaSuccess) { what = "rejoin record"; break; }
       if ((e = cudaStreamWaitEvent(S, ej, 0)) != cudaSuccess) { what = "rejoin wait"; break; }

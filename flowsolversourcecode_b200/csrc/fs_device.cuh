@@ -1,0 +1,145 @@
+// fs_device.cuh -- device helpers shared by the assembly kernels of
+// fs_simple.cu and fs_turb.cu: reference constants, deterministic block
+// reductions, the residual statistics of CalculateResiduals, face-gradient
+// interpolation and the TVD deferred correction.  Everything is internal to
+// the including translation unit.
+#pragma once
+#include "fs_internal.cuh"
+
+namespace {
+
+constexpr double M23 = (double)(-2.0f / 3.0f);   // `-2./3.` is REAL(4) (AssembleBulkViscosity.for:36)
+constexpr double EPS9 = (double)1.e-9f;          // `1.e-9` is REAL(4) (AssembleHRSchemeCorrection.for:92)
+constexpr double TINY = 1.0e-15;                 // Constants1.F90
+
+// ------------------------------------------------------------ reductions
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+// deterministic block sum / max (fixed tree for a fixed blockDim); result valid in thread 0
+__device__ double block_sum(double v, double *sh) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.;
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.;
+    r = warp_sum(r);
+  }
+  return r;
+}
+__device__ double block_max(double v, double *sh) {
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = -1.0e300;
+  if (wid == 0) {
+    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : -1.0e300;
+    r = warp_max(r);
+  }
+  return r;
+}
+
+// per-cell residual statistics of CalculateResiduals (CalculateResidualsRoutine.for:30-67)
+// at dphi=0: r=|bc|.  Writes block partials.
+__device__ void residual_partials(double r, double acphi, double *red, int nblk) {
+  __shared__ double sh[32];
+  double s0 = block_sum(r, sh);
+  double s1 = block_sum(r * r, sh);
+  double m0 = block_max(r, sh);
+  double m1 = block_max(acphi, sh);
+  if (threadIdx.x == 0) {
+    red[RED_SUM0 * nblk + blockIdx.x] = s0;
+    red[RED_SUM1 * nblk + blockIdx.x] = s1;
+    red[RED_MAX0 * nblk + blockIdx.x] = m0;
+    red[RED_MAX1 * nblk + blockIdx.x] = m1;
+  }
+}
+
+// single block: partials -> residual block slot q (ResorAbs/Max/RMS/Scaled)
+__global__ void k_residual_final(const double *red, int nblk, int N, int q, double *rb) {
+  __shared__ double sh[32];
+  double s0 = 0., s1 = 0., m0 = -1., m1 = -1.;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    s0 += red[RED_SUM0 * nblk + b];
+    s1 += red[RED_SUM1 * nblk + b];
+    m0 = fmax(m0, red[RED_MAX0 * nblk + b]);
+    m1 = fmax(m1, red[RED_MAX1 * nblk + b]);
+  }
+  s0 = block_sum(s0, sh); s1 = block_sum(s1, sh);
+  m0 = block_max(m0, sh); m1 = block_max(m1, sh);
+  if (threadIdx.x == 0) {
+    rb[RB_ABS + q] = s0;
+    rb[RB_MAX + q] = m0;
+    rb[RB_RMS + q] = sqrt(s1 / N);
+    rb[RB_SCL + q] = (q == 3) ? 0. : m0 / (m1 + TINY);
+  }
+}
+
+// ------------------------------------------------------------ interpolation helpers
+// InterpolateGradientToFace (InterpolateGradientFromElementToFace.for:3-100),
+// owner-perspective: o = owner gradient, n = neighbour gradient.
+__device__ __forceinline__ void face_grad(int scheme, double g, double md, double phio, double phin,
+                                          double d, double ex, double ey, double ez,
+                                          double ox, double oy, double oz, double nx, double ny, double nz,
+                                          double &fx, double &fy, double &fz) {
+  double gg = g;
+  if (scheme == FS_GI_UPWIND) gg = (md > 0.) ? 1. : 0.;
+  else if (scheme == FS_GI_DOWNWIND) gg = (md > 0.) ? 0. : 1.;
+  fx = gg * ox + (1. - gg) * nx;
+  fy = gg * oy + (1. - gg) * ny;
+  fz = gg * oz + (1. - gg) * nz;
+  if (scheme == FS_GI_AVERAGECORRECTED) {
+    double c = (phin - phio) / d;
+    c = c - (fx * ex + fy * ey + fz * ez);
+    fx = fx + c * ex; fy = fy + c * ey; fz = fz + c * ez;
+  }
+}
+
+// TVDLimiter (Convection/LimitersTVDType.for:4)
+__device__ __forceinline__ double tvd_psi(int s, double rf) {
+  switch (s) {
+  case FS_TVD_UPWIND: return 0.;
+  case FS_TVD_DOWNWIND: return 2.;
+  case FS_TVD_FROMM: return 0.5 * (1. + rf);
+  case FS_TVD_SOU: return rf;
+  case FS_TVD_CD: return 1.;
+  case FS_TVD_QUICK: return (3. + rf) / 4.;
+  case FS_TVD_SUPERBEE: return fmax(fmax(0., fmin(1., 2. * rf)), fmin(2., rf));
+  case FS_TVD_MINMOD: return fmax(0., fmin(1., rf));
+  case FS_TVD_OSHER: return fmax(0., fmin(2., rf));
+  case FS_TVD_VANLEER: return (rf + fabs(rf)) / (1. + fabs(rf));
+  case FS_TVD_MUSCL: return fmax(0., fmin(fmin(2. * rf, 0.5 * (1. + rf)), 2.));
+  case FS_TVD_SMART: return fmax(0., fmin(fmin(2. * rf, 0.75 * rf + 0.25), 4.));
+  case FS_TVD_HQUICK: return 2. * (rf + fabs(rf)) / (rf + 3.);
+  case FS_TVD_UMIST: return fmax(0., fmin(fmin(fmin(2. * rf, 0.25 + 0.75 * rf), 0.75 + 0.25 * rf), 2.));
+  case FS_TVD_CHARM: return (rf <= 0.) ? 0. : rf * (3. * rf + 1.) / ((rf + 1.) * (rf + 1.));
+  }
+  return 0.;
+}
+
+// HRSchemesCorrections (AssembleHRSchemeCorrection.for:36-134), TVD framework, cpf=1
+__device__ __forceinline__ double hr_flux(int scheme, double bleed, double md, double phio, double phin,
+                                          const double go[3], const double gn[3], double dx, double dy, double dz) {
+  double phic, phid, gx, gy, gz;
+  if (md > 0.) { phic = phio; phid = phin; gx = go[0]; gy = go[1]; gz = go[2]; }
+  else { phic = phin; phid = phio; gx = gn[0]; gy = gn[1]; gz = gn[2]; dx = -dx; dy = -dy; dz = -dz; }
+  double phiu = phid - 2. * (gx * dx + gy * dy + gz * dz);
+  double diff = phid - phic, rf;
+  if (fabs(diff) < EPS9) rf = 0.; else rf = (phic - phiu) / diff;
+  double psi = tvd_psi(scheme, rf);
+  double phiHR = phic + 0.5 * psi * diff;
+  phiHR = (1. - bleed) * phiHR + bleed * phic;
+  return md * (phiHR - phic) * 1.;
+}
+
+}  // namespace

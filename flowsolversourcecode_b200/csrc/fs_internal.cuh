@@ -29,7 +29,11 @@
 enum { RED_SUM0 = 0, RED_SUM1, RED_SUM2, RED_MAX0, RED_MAX1, RED_NQ };
 
 struct fs_mg_dev;  // multigrid hierarchy (fs_mg.cu)
+struct fs_turb;    // k-epsilon state (fs_turb.cu)
 struct fs_nn;      // learned p' initial guess (fs_nn.cu)
+
+#define FS_NEQ 9        // equations with residual slots: NF 1..9
+#define FS_NITERS 16     // int32 iteration-count slots (NF - 1 indexed)
 
 struct fs_ctx {
   int dev = 0;
@@ -86,9 +90,15 @@ struct fs_ctx {
   double *red = nullptr;        // RED_NQ * FS_RED_BLOCKS partials
   int64_t *redi = nullptr;      // FS_RED_BLOCKS argmax partials
   double *resblk = nullptr;     // device residual block, layout of fs_residuals' first 20 doubles + extras
-  int32_t *d_iters = nullptr;   // linear iterations per NF (5)
+  int32_t *d_iters = nullptr;   // linear iterations per NF (FS_NITERS slots, NF 1..9 used)
   int32_t *d_status = nullptr;  // device-side status flags
 
+  // boundary patch per boundary face (device), outlet mass-flow scratch:
+  // [0] mdotIn, [1 + s] mdot1(s), [1 + FS_MAX_PATCHES + s] mdotOut(s)
+  int32_t *d_bset = nullptr;
+  double *flow = nullptr;
+  // k-epsilon (nullptr: laminar)
+  fs_turb *turb = nullptr;
   // multigrid
   fs_mg_dev *mg = nullptr;
   // learned initial guess of the p' solve (nullptr: zero guess)
@@ -97,12 +107,12 @@ struct fs_ctx {
 
   // timing
   cudaEvent_t tev[2] = {};                 // fs_timer_start / fs_timer_stop
-  cudaEvent_t sev[5][2] = {};              // around the solver launch of each NF
-  bool s_pending[5] = {};
-  float s_ms[5] = {};
-  cudaEvent_t kev[5][2] = {};              // around the main cooperative kernel of each solve
-  float k_ms[5] = {};
-  int32_t s_its[5] = {}, s_calls[5] = {};
+  cudaEvent_t sev[FS_NEQ][2] = {};         // around the solver launch of each NF
+  bool s_pending[FS_NEQ] = {};
+  float s_ms[FS_NEQ] = {};
+  cudaEvent_t kev[FS_NEQ][2] = {};         // around the main cooperative kernel of each solve
+  float k_ms[FS_NEQ] = {};
+  int32_t s_its[FS_NEQ] = {}, s_calls[FS_NEQ] = {};
   cudaEvent_t ev[6] = {};
   float phase_ms[5] = {};
   int coop_grid = 0;            // blocks of a cooperative solver launch
@@ -117,8 +127,11 @@ struct fs_ctx {
     if (!ctx->graph_mode) { stmt; }                                          \
   } while (0)
 
-// residual block layout on the device (double resblk[RB_SIZE])
-enum { RB_ABS = 0, RB_MAX = 5, RB_RMS = 10, RB_SCL = 15, RB_OVERALL = 20, RB_IMAX = 21, RB_SIZE = 24 };
+// residual block layout on the device (double resblk[RB_SIZE]): four norms of
+// NF 1..9 (u, v, w, p', mass, -, -, k, epsilon), the overall imbalance and its
+// cell, then two scratch slots
+enum { RB_ABS = 0, RB_MAX = 9, RB_RMS = 18, RB_SCL = 27, RB_OVERALL = 36, RB_IMAX = 37,
+       RB_DIAG = 38, RB_MDOTIN = 39, RB_SIZE = 40 };
 
 #define FS_CK(call)                                                          \
   do {                                                                       \
@@ -174,6 +187,15 @@ int fs_continuity_assemble(fs_ctx *ctx);
 int fs_continuity_correct(fs_ctx *ctx);
 int fs_residual_reduce(fs_ctx *ctx, int nf);   // CalculateResiduals partials -> resblk slot
 int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int solver);
+// k-epsilon and outlets (fs_turb.cu)
+int fs_turb_create(fs_ctx *ctx);
+void fs_turb_free(fs_ctx *ctx);
+double *fs_turb_field(fs_ctx *ctx, int field, size_t *n);
+void fs_turb_momentum_ptrs(fs_ctx *ctx, const double **mut, const double **bedif, const double **drk);
+int fs_turb_wall_functions(fs_ctx *ctx);
+int fs_turb_rhok_gradient(fs_ctx *ctx);
+int fs_turb_effects(fs_ctx *ctx);
+int fs_flow_in_out(fs_ctx *ctx);
 int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);
 int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);

@@ -1154,7 +1154,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.lc = M->lc; a.direct = M->direct; a.sinv = M->sinv;
     a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_pre);
     a.maxit = ctx->cfg.krylov_maxit; a.tol = ctx->cfg.krylov_tol; a.part = M->red;
-    a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + 22;
+    a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + RB_DIAG;
     a.x0 = nf == FS_VAR_PC ? ctx->pc_guess : nullptr;
     a.nncnt = fs_nn_counters(ctx);
     a.teambar = (unsigned *)(ctx->d_status + 4);

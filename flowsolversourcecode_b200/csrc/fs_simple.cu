@@ -8,85 +8,9 @@
 // in the reference's order without atomics, and with --fmad=false the
 // assembled coefficients are bit-identical to the CPU restatement.
 #include "fs_internal.cuh"
+#include "fs_device.cuh"
 
 namespace {
-
-constexpr double M23 = (double)(-2.0f / 3.0f);   // `-2./3.` is REAL(4) (AssembleBulkViscosity.for:36)
-constexpr double EPS9 = (double)1.e-9f;          // `1.e-9` is REAL(4) (AssembleHRSchemeCorrection.for:92)
-constexpr double TINY = 1.0e-15;                 // Constants1.F90
-
-// ------------------------------------------------------------ reductions
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-__device__ __forceinline__ double warp_max(double v) {
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-  return v;
-}
-// deterministic block sum / max (fixed tree for a fixed blockDim); result valid in thread 0
-__device__ double block_sum(double v, double *sh) {
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  v = warp_sum(v);
-  __syncthreads();
-  if (lane == 0) sh[wid] = v;
-  __syncthreads();
-  double r = 0.;
-  if (wid == 0) {
-    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.;
-    r = warp_sum(r);
-  }
-  return r;
-}
-__device__ double block_max(double v, double *sh) {
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  v = warp_max(v);
-  __syncthreads();
-  if (lane == 0) sh[wid] = v;
-  __syncthreads();
-  double r = -1.0e300;
-  if (wid == 0) {
-    r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : -1.0e300;
-    r = warp_max(r);
-  }
-  return r;
-}
-
-// per-cell residual statistics of CalculateResiduals (CalculateResidualsRoutine.for:30-67)
-// at dphi=0: r=|bc|.  Writes block partials.
-__device__ void residual_partials(double r, double acphi, double *red, int nblk) {
-  __shared__ double sh[32];
-  double s0 = block_sum(r, sh);
-  double s1 = block_sum(r * r, sh);
-  double m0 = block_max(r, sh);
-  double m1 = block_max(acphi, sh);
-  if (threadIdx.x == 0) {
-    red[RED_SUM0 * nblk + blockIdx.x] = s0;
-    red[RED_SUM1 * nblk + blockIdx.x] = s1;
-    red[RED_MAX0 * nblk + blockIdx.x] = m0;
-    red[RED_MAX1 * nblk + blockIdx.x] = m1;
-  }
-}
-
-// single block: partials -> residual block slot q (ResorAbs/Max/RMS/Scaled)
-__global__ void k_residual_final(const double *red, int nblk, int N, int q, double *rb) {
-  __shared__ double sh[32];
-  double s0 = 0., s1 = 0., m0 = -1., m1 = -1.;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-    s0 += red[RED_SUM0 * nblk + b];
-    s1 += red[RED_SUM1 * nblk + b];
-    m0 = fmax(m0, red[RED_MAX0 * nblk + b]);
-    m1 = fmax(m1, red[RED_MAX1 * nblk + b]);
-  }
-  s0 = block_sum(s0, sh); s1 = block_sum(s1, sh);
-  m0 = block_max(m0, sh); m1 = block_max(m1, sh);
-  if (threadIdx.x == 0) {
-    rb[RB_ABS + q] = s0;
-    rb[RB_MAX + q] = m0;
-    rb[RB_RMS + q] = sqrt(s1 / N);
-    rb[RB_SCL + q] = (q == 3) ? 0. : m0 / (m1 + TINY);
-  }
-}
 
 // ------------------------------------------------------------ gradients
 struct GradJob {
@@ -256,63 +180,6 @@ __global__ void k_bgrad(BGradJob J, int N, int B, const int32_t *__restrict__ bo
   }
 }
 
-// ------------------------------------------------------------ interpolation helpers
-// InterpolateGradientToFace (InterpolateGradientFromElementToFace.for:3-100),
-// owner-perspective: o = owner gradient, n = neighbour gradient.
-__device__ __forceinline__ void face_grad(int scheme, double g, double md, double phio, double phin,
-                                          double d, double ex, double ey, double ez,
-                                          double ox, double oy, double oz, double nx, double ny, double nz,
-                                          double &fx, double &fy, double &fz) {
-  double gg = g;
-  if (scheme == FS_GI_UPWIND) gg = (md > 0.) ? 1. : 0.;
-  else if (scheme == FS_GI_DOWNWIND) gg = (md > 0.) ? 0. : 1.;
-  fx = gg * ox + (1. - gg) * nx;
-  fy = gg * oy + (1. - gg) * ny;
-  fz = gg * oz + (1. - gg) * nz;
-  if (scheme == FS_GI_AVERAGECORRECTED) {
-    double c = (phin - phio) / d;
-    c = c - (fx * ex + fy * ey + fz * ez);
-    fx = fx + c * ex; fy = fy + c * ey; fz = fz + c * ez;
-  }
-}
-
-// TVDLimiter (Convection/LimitersTVDType.for:4)
-__device__ __forceinline__ double tvd_psi(int s, double rf) {
-  switch (s) {
-  case FS_TVD_UPWIND: return 0.;
-  case FS_TVD_DOWNWIND: return 2.;
-  case FS_TVD_FROMM: return 0.5 * (1. + rf);
-  case FS_TVD_SOU: return rf;
-  case FS_TVD_CD: return 1.;
-  case FS_TVD_QUICK: return (3. + rf) / 4.;
-  case FS_TVD_SUPERBEE: return fmax(fmax(0., fmin(1., 2. * rf)), fmin(2., rf));
-  case FS_TVD_MINMOD: return fmax(0., fmin(1., rf));
-  case FS_TVD_OSHER: return fmax(0., fmin(2., rf));
-  case FS_TVD_VANLEER: return (rf + fabs(rf)) / (1. + fabs(rf));
-  case FS_TVD_MUSCL: return fmax(0., fmin(fmin(2. * rf, 0.5 * (1. + rf)), 2.));
-  case FS_TVD_SMART: return fmax(0., fmin(fmin(2. * rf, 0.75 * rf + 0.25), 4.));
-  case FS_TVD_HQUICK: return 2. * (rf + fabs(rf)) / (rf + 3.);
-  case FS_TVD_UMIST: return fmax(0., fmin(fmin(fmin(2. * rf, 0.25 + 0.75 * rf), 0.75 + 0.25 * rf), 2.));
-  case FS_TVD_CHARM: return (rf <= 0.) ? 0. : rf * (3. * rf + 1.) / ((rf + 1.) * (rf + 1.));
-  }
-  return 0.;
-}
-
-// HRSchemesCorrections (AssembleHRSchemeCorrection.for:36-134), TVD framework, cpf=1
-__device__ __forceinline__ double hr_flux(int scheme, double bleed, double md, double phio, double phin,
-                                          const double go[3], const double gn[3], double dx, double dy, double dz) {
-  double phic, phid, gx, gy, gz;
-  if (md > 0.) { phic = phio; phid = phin; gx = go[0]; gy = go[1]; gz = go[2]; }
-  else { phic = phin; phid = phio; gx = gn[0]; gy = gn[1]; gz = gn[2]; dx = -dx; dy = -dy; dz = -dz; }
-  double phiu = phid - 2. * (gx * dx + gy * dy + gz * dz);
-  double diff = phid - phic, rf;
-  if (fabs(diff) < EPS9) rf = 0.; else rf = (phic - phiu) / diff;
-  double psi = tvd_psi(scheme, rf);
-  double phiHR = phic + 0.5 * psi * diff;
-  phiHR = (1. - bleed) * phiHR + bleed * phic;
-  return md * (phiHR - phic) * 1.;
-}
-
 // ------------------------------------------------------------ momentum
 struct MomArgs {
   int N, F, B;
@@ -321,6 +188,7 @@ struct MomArgs {
   const double *bsf, *bfa, *bnf, *bdv, *bgdiff, *btf;
   const double *u, *v, *w, *mdot, *bmdot, *bu, *bv, *bw;
   const double *ug, *vg, *wg, *pg, *bug, *bvg, *bwg;
+  const double *mut, *bedif, *drk;      // k-epsilon: mu_t (N), BeDiffCoefficient (B), grad(2/3 rho k) (3N)
   double mu, bleed, urf;
   int gi_scheme, hr_on, conv_scheme, inviscid, relax, simplec;
   // outputs
@@ -335,6 +203,8 @@ struct MomArgs {
 // upwind convection + HR deferred correction (AssembleConvection.for:72-88,153-162)
 // and the effective divergence (CalculateEffectiveDivergence.for:20-45).
 // FluxCf/FluxFf (and so ac, anb) are shared by u, v, w; bc differs.
+// TURB: eDiffCoefficient = mu + mu_t (ComputeEffectiveDiffusionCoefficient.for:30-32)
+template <bool TURB>
 __global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.N) return;
@@ -344,6 +214,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs 
   const double mu = a.mu;
   // this cell's values stay in registers; the other cell of a face is cn(i,j)
   const double us = a.u[i], vs = a.v[i], ws = a.w[i];
+  const double mts = TURB ? a.mut[i] : 0.;
   const double gus[3] = {a.ug[i], a.ug[N + i], a.ug[N2 + i]};
   const double gvs[3] = {a.vg[i], a.vg[N + i], a.vg[N2 + i]};
   const double gws[3] = {a.wg[i], a.wg[N + i], a.wg[N2 + i]};
@@ -374,7 +245,13 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs 
     double ex = dx / d, ey = dy / d, ez = dz / d;
     double fcf = 0., fff = 0., tu = 0., tv = 0., tw = 0.;
     if (!a.inviscid) {
-      double gamf = g * mu + (1. - g) * mu;
+      double gamf;
+      if (TURB) {
+        const double mtk = a.mut[k];
+        gamf = g * (mu + (nb ? mtk : mts)) + (1. - g) * (mu + (nb ? mts : mtk));
+      } else {
+        gamf = g * mu + (1. - g) * mu;
+      }
       double gd = a.gdiff[f];
       double tx = a.tf[f], ty = a.tf[F + f], tz = a.tf[F2 + f];
       double fu[3], fv[3], fw[3];
@@ -428,6 +305,9 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs 
 // boundary terms, AssembleConvection.for:165-178 + 263-556, AssemblePressureGradient.for,
 // AssembleGolbalElementAndFaceFluxes.for:83-98 + 4-30, UnderRelaxation.for:21,
 // StoreTheDValues.for:20-48, and the residual partials of CalculateResiduals.
+// TURB: boundary faces diffuse with BeDiffCoefficient (wall functions on no-slip
+// walls) and FluxTE takes MinusTwoThirdsRhoK (AssembleMinusTwoThirdsRhoK.for:96-110).
+template <bool TURB>
 __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a, int comp) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool live = i < a.N;
@@ -450,7 +330,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
       double bsx = a.bsf[b], bsy = a.bsf[B + b], bsz = a.bsf[B2 + b];
       double bp = bfi[b];
       if (!a.inviscid) {
-        double gamf = mu;
+        double gamf = TURB ? a.bedif[b] : mu;
         if (t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
           double nx = a.bnf[b], ny = a.bnf[B + b], nz = a.bnf[B2 + b];
           double dN = a.bdv[b] * nx + a.bdv[B + b] * ny + a.bdv[B2 + b] * nz;
@@ -508,6 +388,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
     double fve = -(fmax(e, 0.0) * phi);
     double fte = fce * phi + fve;
     fte = fte + a.pg[(long)comp * N + i] * a.vol[i];
+    if (TURB) fte = fte + a.drk[(long)comp * N + i] * a.vol[i];
     ac = ac + fce;
     bc = bc - fte;
     if (a.relax) ac = ac / a.urf;
@@ -777,13 +658,13 @@ __global__ void k_mass_final(CorrArgs a, const double *mdot_in_dev) {
   }
 }
 
+// inlet mass flow: one CTA, strided per-thread sums then a fixed tree (deterministic)
 __global__ void k_sum_inlet(int B, const int32_t *btype, const double *bmdot, double *out) {
-  // serial on purpose: a handful of inlet faces, deterministic order
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double s = 0.;
-    for (int b = 0; b < B; b++) if (btype[b] == FS_BC_INLET_VEL) s += bmdot[b];
-    *out = s;
-  }
+  __shared__ double sh[32];
+  double s = 0.;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) if (btype[b] == FS_BC_INLET_VEL) s += bmdot[b];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) *out = s;
 }
 
 }  // namespace
@@ -854,6 +735,7 @@ static MomArgs mom_args(fs_ctx *ctx) {
   a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.mdot = ctx->mdot; a.bmdot = ctx->bmdot; a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw;
   a.ug = ctx->ug; a.vg = ctx->vg; a.wg = ctx->wg; a.pg = ctx->pg; a.bug = ctx->bug; a.bvg = ctx->bvg; a.bwg = ctx->bwg;
   a.mu = c.mu; a.bleed = c.bleed; a.urf = c.urf_momentum;
+  fs_turb_momentum_ptrs(ctx, &a.mut, &a.bedif, &a.drk);
   a.gi_scheme = c.grad_interp_mom;
   a.hr_on = (c.hr_framework == FS_HR_TVD && ctx->nIter >= c.niter_start_hr && c.conv_scheme != FS_TVD_UPWIND) ? 1 : 0;
   a.conv_scheme = c.conv_scheme; a.inviscid = c.inviscid; a.relax = c.relax_momentum; a.simplec = c.algorithm == FS_SIMPLEC;
@@ -879,16 +761,23 @@ int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac_out, double *bc_ou
     int nit[4] = {c.niter_grad_mom, c.niter_grad_mom, c.niter_grad_mom, c.niter_grad_cont};
     int rc = fs_gradient_dev(ctx, 4, vars, phi, bphi, g, bg, meth, nit);
     if (rc) return rc;
+    if (ctx->turb && (rc = fs_turb_rhok_gradient(ctx))) return rc;
     MomArgs a = mom_args(ctx);
-    k_mom_interior<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
+    if (ctx->turb) k_mom_interior<true><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
+    else k_mom_interior<false><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
     FS_LAUNCH_CHECK();
+  }
+  if (ctx->turb && !c.inviscid) {
+    int rc = fs_turb_wall_functions(ctx);
+    if (rc) return rc;
   }
   MomArgs a = mom_args(ctx);
   a.ac = ac_out; a.bc = bc_out;
   a.d1 = comp == 0 ? ctx->du1 : comp == 1 ? ctx->dv1 : ctx->dw1;
   a.d2 = comp == 0 ? ctx->du2 : comp == 1 ? ctx->dv2 : ctx->dw2;
   a.star = comp == 0 ? ctx->us : comp == 1 ? ctx->vs : ctx->ws;
-  k_mom_finish<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a, comp);
+  if (ctx->turb) k_mom_finish<true><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a, comp);
+  else k_mom_finish<false><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a, comp);
   FS_LAUNCH_CHECK();
   k_residual_final<<<1, 1024, 0, ctx->st>>>(ctx->red, a.nblk, N, comp, ctx->resblk);
   FS_LAUNCH_CHECK();
@@ -914,6 +803,8 @@ static ContArgs cont_args(fs_ctx *ctx) {
 int fs_continuity_assemble(fs_ctx *ctx) {
   const int N = ctx->N, F = ctx->F, B = ctx->B;
   FS_CK(cudaMemsetAsync(ctx->pc, 0, sizeof(double) * N, ctx->st));   // InitializePressureCorrection
+  int rc = fs_flow_in_out(ctx);                                        // FlowIn, FlowOut, AdjustFlow
+  if (rc) return rc;
   ContArgs a = cont_args(ctx);
   if (F) { k_mdot<<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   if (B) { k_bmdot_inlet<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
@@ -962,8 +853,8 @@ int fs_continuity_correct(fs_ctx *ctx) {
   double *d_in = nullptr;
   if (has_inlet) {
     // inlet mass flow, used only through ResorScaled(5); stays on the device
-    d_in = ctx->resblk + RB_SIZE - 1;
-    k_sum_inlet<<<1, 32, 0, ctx->st>>>(B, ctx->btype, ctx->bmdot, d_in);
+    d_in = ctx->resblk + RB_MDOTIN;
+    k_sum_inlet<<<1, 1024, 0, ctx->st>>>(B, ctx->btype, ctx->bmdot, d_in);
     FS_LAUNCH_CHECK();
   }
   k_mass_final<<<1, 1024, 0, ctx->st>>>(a, d_in);

@@ -650,7 +650,7 @@ static SolveArgs solve_args(fs_ctx *ctx, int nf, double rrf, int itmax) {
   a.color_rows = ctx->color_rows;
   a.ncolors = ctx->ncolors;
   a.iters = ctx->d_iters + (nf - 1);
-  a.diag = ctx->resblk + 22;
+  a.diag = ctx->resblk + RB_DIAG;
   return a;
 }
 
@@ -719,12 +719,12 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
 }
 
 int fs_solver_stats_collect(fs_ctx *ctx) {
-  int32_t it[8];
+  int32_t it[FS_NITERS];
   bool any = false;
-  for (int q = 0; q < 5; q++) any |= ctx->s_pending[q];
+  for (int q = 0; q < FS_NEQ; q++) any |= ctx->s_pending[q];
   if (!any) return FS_OK;
   FS_CK(cudaMemcpy(it, ctx->d_iters, sizeof(it), cudaMemcpyDeviceToHost));
-  for (int q = 0; q < 5; q++) {
+  for (int q = 0; q < FS_NEQ; q++) {
     if (!ctx->s_pending[q]) continue;
     float ms = 0.f;
     FS_CK(cudaEventElapsedTime(&ms, ctx->sev[q][0], ctx->sev[q][1]));

@@ -156,11 +156,33 @@ def box_mesh(nx: int, ny: int, nz: int, lx: float = 1.0, ly: float = 1.0, lz: fl
                     patch_start=pstart, patch_size=np.array(psz, np.int32))
 
 
+BFS_PATCHES = ("inlet", "step", "xmax", "ymin", "ymax", "zmin", "zmax")
+
+
 def bfs_mesh(nx: int, ny: int, nz: int, H: float = 1.0) -> PolyMesh:
-    """Backward-facing-step channel 30H x 3H x 2H (step height H at x=0,
-    y<H) as a box whose xmin patch is later split by the case into inlet
-    (y>=H) and step wall (y<H).  Returned as a plain box; see cases.py."""
-    return box_mesh(nx, ny, nz, 30.0 * H, 3.0 * H, 2.0 * H)
+    """Backward-facing-step channel 30H x 3H x 2H: the box of ``box_mesh``
+    whose xmin patch is split into ``inlet`` (cells with y >= H) and ``step``
+    (the wall of the step face, y < H), each in cell order.  ny must be a
+    multiple of 3 so that y = H is a grid line.  Patches: inlet, step, xmax
+    (the outlet), ymin, ymax, zmin, zmax."""
+    if ny % 3:
+        raise ValueError("ny must be a multiple of 3 (y = H on a grid line)")
+    m = box_mesh(nx, ny, nz, 30.0 * H, 3.0 * H, 2.0 * H)
+    s0, n0 = int(m.patch_start[0]), int(m.patch_size[0])
+    own = m.owner[s0:s0 + n0]
+    j = (own // nx) % ny
+    up = np.nonzero(j >= ny // 3)[0]
+    lo = np.nonzero(j < ny // 3)[0]
+    order = np.concatenate([up, lo])
+    fn = m.face_nodes.reshape(-1, 4).copy()
+    fn[s0:s0 + n0] = fn[s0 + order]
+    owner = m.owner.copy()
+    owner[s0:s0 + n0] = own[order]
+    psz = [len(up), len(lo)] + [int(x) for x in m.patch_size[1:]]
+    pstart = np.cumsum([s0] + psz[:-1]).astype(np.int32)
+    return PolyMesh(points=m.points, face_ptr=m.face_ptr, face_nodes=fn.ravel(), owner=owner,
+                    neighbour=m.neighbour, patch_names=list(BFS_PATCHES),
+                    patch_start=pstart, patch_size=np.array(psz, np.int32))
 
 
 # --------------------------------------------------------------------------

@@ -81,6 +81,10 @@ class Solver:
     def correct_continuity(self):
         self._chk(self.lib.fs_correct_continuity(self.ctx), "correct_continuity")
 
+    def initialize_mdot(self):
+        """CalculateInitialmdot from the current velocity fields (after set())."""
+        self._chk(self.lib.fs_initialize_mdot(self.ctx), "initialize_mdot")
+
     def set_iteration(self, n: int):
         self.nIter = n
         self._chk(self.lib.fs_set_iteration(self.ctx, n), "set_iteration")
@@ -157,7 +161,8 @@ class Solver:
     def _size(self, name: str) -> int:
         N, F, B, W = self.N, self.F, self.B, self.W
         sizes = {"mdot": F, "gfactor": F, "gdiff": F, "sf": 3 * F, "ft": 3 * F, "anb": W * N,
-                 "bu": B, "bv": B, "bw": B, "bp": B, "bpc": B, "bmdot": B, "bsf": 3 * B, "xc": 3 * N}
+                 "bu": B, "bv": B, "bw": B, "bp": B, "bpc": B, "bmdot": B, "bsf": 3 * B, "xc": 3 * N,
+                 "btke": B, "bted": B, "bmut": B}
         if name.endswith("grad"):
             return 3 * N
         return sizes.get(name, N)

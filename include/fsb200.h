@@ -51,6 +51,9 @@ extern "C" {
 #define FS_VAR_PC     4
 #define FS_VAR_MASS   5
 #define FS_VAR_P      6   /* 'press' (pressure itself, gradient calls only) */
+#define FS_VAR_TKE    8   /* 'tke' (AssignNFvaluesToVariables.for:55) */
+#define FS_VAR_TED    9   /* 'ted' (AssignNFvaluesToVariables.for:60) */
+#define FS_VAR_RHOK  10   /* 'rhok' = 2/3 rho k (gradient calls only, AssembleMinusTwoThirdsRhoK.for) */
 
 /* ------------------------------------------------------ field ids (get/set) */
 enum fs_field {
@@ -65,6 +68,8 @@ enum fs_field {
   FS_F_GFACTOR, FS_F_SF, FS_F_GDIFF, FS_F_FT,        /* F, 3F, F, 3F */
   FS_F_BSF,                                          /* 3B */
   FS_F_DPHI,                                         /* N: last linear solution */
+  FS_F_TKE, FS_F_TED, FS_F_MUT,                      /* N: k, epsilon, turbulent viscosity */
+  FS_F_BTKE, FS_F_BTED, FS_F_BMUT,                   /* B */
   FS_F_COUNT
 };
 
@@ -149,6 +154,22 @@ typedef struct fs_case {
    * the Y/Z wall cross terms then use the previous iteration's u, v.  Only
    * with solver_mom = FS_SOLVER_SOR. */
   int    batched_momentum;
+  /* outlets 'fullydeveloped': MassFlowFraction per patch (AdjustFlowAtOuletBoundary.for:38-55) */
+  double mass_flow_fraction[FS_MAX_PATCHES];
+  /* k-epsilon (TurbulenceModel='kepsilon', WallTreatment='wallfunctions',
+   * WallFunctionKind='equilibrium', MomentumWallFunctionType='standard';
+   * SolveSelectedTurbulenceModelEquations.for:21-30).  0 = laminar. */
+  int    turbulence;
+  int    solver_turb;            /* ASSolverTKE = ASSolverTED */
+  double rrf_tke, rrf_ted;       /* rrfTKE, rrfTED */
+  int    itmax_tke, itmax_ted;   /* ASIterTKE, ASIterTED */
+  double urf_tke, urf_ted;       /* urfTKE, urfTED (LRelaxTKE/TED) */
+  double urf_tvisc;              /* urfTViscosity */
+  double max_visc_ratio;         /* MaximumViscosityRatio */
+  int    limit_production;       /* LimitTurbulenceProduction */
+  int    conv_scheme_tke, conv_scheme_ted; /* ConvectionSchemeTKE/TED (fs_tvd; HR framework tvd) */
+  double inlet_intensity[FS_MAX_PATCHES];  /* inletTurbulenceIntensity, inletTypeT='specifiedil' */
+  double inlet_length[FS_MAX_PATCHES];     /* inletTurbulenceLengthScale */
 } fs_case;
 
 /* Mesh in polyMesh form (0-based), the input Readit parses
@@ -174,6 +195,9 @@ typedef struct fs_residuals {
   int    imax_imbalance;      /* iMaxImbalance (0-based) */
   int    lin_iters[5];        /* linear iterations spent per NF this outer iteration */
   double source;              /* stop metric of PrintConvergenceHistory */
+  /* k and epsilon equations (NF 8, 9), filled when the case is turbulent */
+  double turb_abs[2], turb_max[2], turb_rms[2], turb_scaled[2];
+  int    turb_lin_iters[2];
 } fs_residuals;
 
 typedef struct fs_ctx fs_ctx;
@@ -218,6 +242,10 @@ int fs_assemble_continuity(fs_ctx *ctx);
 int fs_correct_continuity(fs_ctx *ctx);
 /* MultiGrid2 nIter (gates nIterStartApplyingHR). */
 int fs_set_iteration(fs_ctx *ctx, int n_iter);
+/* CalculateInitialmdot (ContinuityEquation/InitializaMdot.for:4): mdot and
+ * Bmdot from the current cell and boundary velocities, for a caller that set
+ * an initial field with fs_set_field (fs_create already ran it once). */
+int fs_initialize_mdot(fs_ctx *ctx);
 
 /* ---------------------------------------------------------- leaf routines */
 /* Gradient (GradientFiles/CalculateGradients.for:3) of field var

@@ -53,6 +53,8 @@ def load():
         lib.om_gmres.restype = C.c_int
         lib.om_gmres.argtypes = [C.c_void_p]
         lib.om_calc_residuals.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        lib.om_residuals_turb.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.om_initialize_mdot.argtypes = [C.c_void_p]
         lib.om_mg_setup.restype = C.c_int
         lib.om_mg_setup.argtypes = [C.c_void_p]
         lib.om_mg_level_size.restype = C.c_int
@@ -120,6 +122,17 @@ class Oracle:
         self.lib.om_residuals(self.h, a)
         a = list(a)
         return {"abs": a[0:5], "max": a[5:10], "rms": a[10:15], "scaled": a[15:20]}
+
+    def residuals_turb(self) -> dict:
+        """Residual norms of the k (index 0) and epsilon (index 1) equations."""
+        a = (C.c_double * 8)()
+        self.lib.om_residuals_turb(self.h, a)
+        a = list(a)
+        return {"abs": a[0:2], "max": a[2:4], "rms": a[4:6], "scaled": a[6:8]}
+
+    def initialize_mdot(self):
+        """CalculateInitialmdot from the current velocity fields."""
+        self.lib.om_initialize_mdot(self.h)
 
     def lin_iters(self, nf: int) -> int:
         return self.lib.om_lin_iters(self.h, nf)

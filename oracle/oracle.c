@@ -27,6 +27,7 @@
 #define OM_M23   ((double)(-2.0f / 3.0f))
 #define OM_EPS9  ((double)1.e-9f)
 #define OM_TINY  1.0e-15              /* Constants1.F90: tiny=1.d-15 */
+#define OM_TWOTHIRD ((double)(2.0f / 3.0f))   /* Constants1.F90:12 TwoThird, a REAL(4) literal */
 
 struct om {
   fs_case cfg;
@@ -68,10 +69,21 @@ struct om {
   double *fce, *fte;                        /* FluxCE, FluxTE [N] */
   double *effdiv;
   double *ac, *anb, *bc, *dphi;
-  /* residuals (Residuals1.F90) */
-  double rabs[5], rmax[5], rrms[5], rscl[5];
+  /* residuals (Residuals1.F90), NF 1..9 */
+  double rabs[9], rmax[9], rrms[9], rscl[9];
   double overall_imbalance; int imax_imbalance;
-  int lin_iters[5];
+  int lin_iters[9];
+  /* outlets (FlowInOut1.F90) */
+  double mdot_in, *mdot1, *mdot_out;        /* mdotIn, mdot1(NS), mdotOut(NS) */
+  /* k-epsilon (Variables1, PhysicalProperties1, Turbulence1, WallDistance1) */
+  double *tke, *ted, *mut, *btke, *bted, *bmut;
+  double *tkeg, *tedg, *btkeg, *btedg, *tkegf, *tedgf;
+  double *edif, *bedif;                     /* eDiffCoefficient, BeDiffCoefficient */
+  double *prod, *bprod;                     /* TurbulenceProduction, BTurbulenceProduction */
+  double *s11, *s12, *s13, *s22, *s23, *s33;
+  double *rhok, *brhok, *drk, *bdrk;        /* MinusTwoThirdsRhoK */
+  double *wdist; int *itau;                 /* WallDistance, iTau (boundary index) */
+  double *utau, *yplus, *uplus, *dupdyp, *tauw, *wallvisc;   /* per wall face */
   /* BICGSTAB_OMP persistent storage (SparseMatricesVariables) */
   int csr_built; long *csr_ptr; int *csr_j; int *csr_slot; double *csr_val;
   double *kx, *kr, *kb;
@@ -80,6 +92,7 @@ struct om {
 };
 
 static double *dz_(long n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
+static void om_momentum_wall_functions(om *m);   /* oracle_turb.inc */
 static int *iz_(long n) { return (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int)); }
 
 /* ===================================================================== */
@@ -508,11 +521,21 @@ void om_assemble_momentum(om *m, int comp)
   }
   const double *fgx = fgf, *fgy = fgf + F, *fgz = fgf + 2 * (long)F;
   if (!c->inviscid) {
+    /* CalculateEffectiveDiffusionCoefficient('vel?') (ComputeEffectiveDiffusionCoefficient.for:24-48,
+     * 580-596): mu (+ mu_t and the momentum wall functions when turbulent) */
+    if (c->turbulence) {
+      for (int i = 0; i < N; i++) m->edif[i] = c->mu + m->mut[i];
+      for (int b = 0; b < B; b++) m->bedif[b] = c->mu + m->bmut[b];
+      om_momentum_wall_functions(m);
+    } else {
+      for (int i = 0; i < N; i++) m->edif[i] = c->mu;
+      for (int b = 0; b < B; b++) m->bedif[b] = c->mu;
+    }
     /* AssembleDiffusionTerm interior (AssembleIsotropicDiffusion.for:99-117);
-     * GamaFace = 'average' of eDiffCoefficient=Viscosity (ComputeEffectiveDiffusionCoefficient.for:580-596) */
+     * GamaFace = 'average' of eDiffCoefficient (InterpolateGamaFromCentroidToFace.for) */
     for (int k = 0; k < F; k++) {
       int i = m->if_own[k], j = m->if_nbr[k];
-      double gamf = m->gf[k] * c->mu + (1. - m->gf[k]) * c->mu;
+      double gamf = m->gf[k] * m->edif[i] + (1. - m->gf[k]) * m->edif[j];
       double fcl = gamf * m->gdiff[k], ffl = -gamf * m->gdiff[k];
       double fvl = -(gamf * (fgx[k] * m->Tx[k] + fgy[k] * m->Ty[k] + fgz[k] * m->Tz[k]));
       m->fcf[k] += fcl; m->fff[k] += ffl; m->fvf[k] += fvl;
@@ -522,7 +545,7 @@ void om_assemble_momentum(om *m, int comp)
     for (int b = 0; b < B; b++) {
       int i1 = m->bf_own[b], t = m->btype[b];
       long i4 = F + b;
-      double gamf = c->mu;
+      double gamf = m->bedif[b];
       if (t == FS_BC_WALL_NOSLIP) {
         double dN = m->bdx[b] * m->bnx[b] + m->bdy[b] * m->bny[b] + m->bdz[b] * m->bnz[b];
         double area = m->bfa[b], nx = m->bnx[b], ny = m->bny[b], nz = m->bnz[b];
@@ -561,7 +584,7 @@ void om_assemble_momentum(om *m, int comp)
     const double *Gy = comp == 0 ? m->vgf : comp == 1 ? m->vgf + F : m->vgf + 2 * (long)F;
     const double *Gz = comp == 0 ? m->wgf : comp == 1 ? m->wgf + F : m->wgf + 2 * (long)F;
     for (int k = 0; k < F; k++) {
-      double gamf = m->gf[k] * c->mu + (1. - m->gf[k]) * c->mu;
+      double gamf = m->gf[k] * m->edif[m->if_own[k]] + (1. - m->gf[k]) * m->edif[m->if_nbr[k]];
       double fvl = -(gamf * (Gx[k] * m->sx[k] + Gy[k] * m->sy[k] + Gz[k] * m->sz[k]));
       m->fvf[k] += fvl; m->ftf[k] += fvl;
     }
@@ -569,20 +592,20 @@ void om_assemble_momentum(om *m, int comp)
     const double *BGy = comp == 0 ? m->bvg : comp == 1 ? m->bvg + B : m->bvg + 2 * (long)B;
     const double *BGz = comp == 0 ? m->bwg : comp == 1 ? m->bwg + B : m->bwg + 2 * (long)B;
     for (int b = 0; b < B; b++) {
-      double gamf = c->mu;
+      double gamf = m->bedif[b];
       double fvl = -(gamf * (BGx[b] * m->bsx[b] + BGy[b] * m->bsy[b] + BGz[b] * m->bsz[b]));
       m->fvf[F + b] += fvl; m->ftf[F + b] += fvl;
     }
     /* AssembleBulkViscosityTerm (AssembleBulkViscosity.for:22-172) */
     for (int k = 0; k < F; k++) {
-      double gamf = m->gf[k] * c->mu + (1. - m->gf[k]) * c->mu;
+      double gamf = m->gf[k] * m->edif[m->if_own[k]] + (1. - m->gf[k]) * m->edif[m->if_nbr[k]];
       double div = m->ugf[k] + m->vgf[F + k] + m->wgf[2 * (long)F + k];
       double s = comp == 0 ? m->sx[k] : comp == 1 ? m->sy[k] : m->sz[k];
       double fvl = -(OM_M23 * gamf * div * s);
       m->fvf[k] += fvl; m->ftf[k] += fvl;
     }
     for (int b = 0; b < B; b++) {
-      double gamf = c->mu;
+      double gamf = m->bedif[b];
       double div = m->bug[b] + m->bvg[B + b] + m->bwg[2 * (long)B + b];
       double s = comp == 0 ? m->bsx[b] : comp == 1 ? m->bsy[b] : m->bsz[b];
       double fvl = -(OM_M23 * gamf * div * s);
@@ -640,6 +663,16 @@ void om_assemble_momentum(om *m, int comp)
   /* AssemblePressureGradientTerm (AssemblePressureGradient.for:17-22) */
   const double *dp = m->pg + (long)comp * N;
   for (int i = 0; i < N; i++) m->fte[i] += dp[i] * m->vol[i];
+  /* MinusTwoThirdsRhoK (AssembleMinusTwoThirdsRhoK.for:40-110): gradient of 2/3 rho k in X */
+  if (c->turbulence) {
+    if (comp == 0) {
+      for (int i = 0; i < N; i++) m->rhok[i] = OM_TWOTHIRD * c->rho * m->tke[i];
+      for (int b = 0; b < B; b++) m->brhok[b] = OM_TWOTHIRD * c->rho * m->btke[b];
+      om_gradient(m, FS_VAR_RHOK, c->method_grad_mom, c->niter_grad_mom, m->rhok, m->brhok, m->drk, m->bdrk);
+    }
+    const double *dk = m->drk + (long)comp * N;
+    for (int i = 0; i < N; i++) m->fte[i] += dk[i] * m->vol[i];
+  }
   global_assembly(m);
   /* UnderRelaxEquation (UnderRelaxation.for:21) */
   if (c->relax_momentum) for (int i = 0; i < N; i++) m->ac[i] = m->ac[i] / c->urf_momentum;
@@ -690,12 +723,58 @@ static double geo_diff(int msd, double Du, double Dv, double Dw, double sx, doub
   return gd;
 }
 
+/* FlowIn (CalculateFlowIn.for:4-40), FlowOut (CalculateFlowOut.for:4-55) and
+ * AdjustFlow (AdjustFlowAtOuletBoundary.for:4-75), incompressible, when every
+ * outlet is 'fullydeveloped' */
+static void om_flow_in_out(om *m)
+{
+  int NS = m->NS, F = m->F;
+  const fs_case *c = &m->cfg;
+  int nfd = 0;
+  for (int s = 0; s < NS; s++) {
+    if (c->patch_type[s] == FS_BC_OUTLET_FD) nfd++;
+  }
+  if (nfd == 0) return;   /* FlowOut/AdjustFlow return at once; FlowIn's sum is unused */
+  m->mdot_in = 0.;
+  for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_INLET_VEL)
+    for (int j = 0; j < m->bset_n[s]; j++) m->mdot_in = m->mdot_in + m->bmdot[m->bset_start[s] + j];
+  for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_FD) {
+    m->mdot1[s] = 0.;
+    for (int j = 0; j < m->bset_n[s]; j++) {
+      int b = m->bset_start[s] + j;
+      m->bmdot[b] = c->rho * (m->bu[b] * m->bsx[b] + m->bv[b] * m->bsy[b] + m->bw[b] * m->bsz[b]);
+      if (m->bmdot[b] < m->mdot1[s]) m->mdot1[s] = m->bmdot[b];
+    }
+    m->mdot1[s] = fabs(m->mdot1[s]);
+  }
+  for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_FD) {
+    m->mdot_out[s] = 0.;
+    for (int j = 0; j < m->bset_n[s]; j++) m->mdot_out[s] = m->mdot_out[s] + m->mdot1[s] + m->bmdot[m->bset_start[s] + j];
+  }
+  double tff = 0.;
+  for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_FD) tff = tff + c->mass_flow_fraction[s];
+  for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_FD) {
+    double ratio = (c->mass_flow_fraction[s] / (tff + OM_TINY)) * fabs(m->mdot_in / (m->mdot_out[s] + OM_TINY));
+    for (int j = 0; j < m->bset_n[s]; j++) {
+      int b = m->bset_start[s] + j, k = m->bf_own[b];
+      m->bmdot[b] = ratio * (m->bmdot[b] + m->mdot1[s]);
+      /* boundary velocity from the owner and the boundary gradient; AssembleMdot
+       * overwrites it with the owner velocity right after */
+      m->bu[b] = m->u[k] + (m->bug[b] * m->bdx[b] + m->bug[m->B + b] * m->bdy[b] + m->bug[2L * m->B + b] * m->bdz[b]);
+      m->bv[b] = m->v[k] + (m->bvg[b] * m->bdx[b] + m->bvg[m->B + b] * m->bdy[b] + m->bvg[2L * m->B + b] * m->bdz[b]);
+      m->bw[b] = m->w[k] + (m->bwg[b] * m->bdx[b] + m->bwg[m->B + b] * m->bdy[b] + m->bwg[2L * m->B + b] * m->bdz[b]);
+    }
+  }
+  (void)F;
+}
+
 void om_assemble_continuity(om *m)
 {
   int N = m->N, F = m->F, B = m->B;
   const fs_case *c = &m->cfg;
   init_fluxes(m);
   memset(m->pc, 0, sizeof(double) * N);          /* InitializePressureCorrection */
+  om_flow_in_out(m);                             /* FlowIn, FlowOut, AdjustFlow */
   /* AssembleMdot (AssembleMdotUsingRhieChow.for:262-292, 554-759) */
   double *pgbar = dz_(3 * (long)F);
   om_interp_grad(m, FS_GI_AVERAGE, m->p, m->pg, pgbar);
@@ -722,6 +801,11 @@ void om_assemble_continuity(om *m)
   /* inlet specified velocity Bmdot (AssembleMdotUsingRhieChow.for:2054-2075) */
   for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_VEL)
     m->bmdot[b] = c->rho * (m->bu[b] * m->bsx[b] + m->bv[b] * m->bsy[b] + m->bw[b] * m->bsz[b]);
+  /* fully developed outlet velocity (AssembleMdotUsingRhieChow.for:2033-2050) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_FD) {
+    int i1 = m->bf_own[b];
+    m->bu[b] = m->u[i1]; m->bv[b] = m->v[i1]; m->bw[b] = m->w[i1];
+  }
   /* AssemblePressureCorrection (AssemblePressureCorrectionFluxes.for:85-164) */
   for (int k = 0; k < F; k++) {
     double du = avgf(m, k, m->du2), dv = avgf(m, k, m->dv2), dw = avgf(m, k, m->dw2);
@@ -1077,6 +1161,11 @@ void om_solve_equation(om *m, int nf, double *fi, double rrf, int itmax, int sol
 }
 
 /* ===================================================================== */
+/*  k-epsilon (Turbulence/)                                               */
+/* ===================================================================== */
+#include "oracle_turb.inc"
+
+/* ===================================================================== */
 /*  Stop metric (PrintConvergenceToFileAndScreen.for:613-700)             */
 /* ===================================================================== */
 static double stop_metric(om *m)
@@ -1086,6 +1175,7 @@ static double stop_metric(om *m)
   double s = 0.;
   s = fmax(s, fmax(fabs(r[0]), fmax(fabs(r[1]), fabs(r[2]))));
   s = fmax(s, fabs(r[4]));
+  if (m->cfg.turbulence) { s = fmax(s, fabs(r[7])); s = fmax(s, fabs(r[8])); }
   return s;
 }
 
@@ -1094,7 +1184,29 @@ double om_simple_iteration(om *m)
   m->nIter++;
   om_momentum(m, 0); om_momentum(m, 1); om_momentum(m, 2);
   om_continuity(m);
+  if (m->cfg.turbulence) om_effects_of_turbulence(m);
   return stop_metric(m);
+}
+
+void om_residuals_turb(om *m, double out[8])
+{
+  for (int q = 0; q < 2; q++) { out[q] = m->rabs[7 + q]; out[2 + q] = m->rmax[7 + q]; out[4 + q] = m->rrms[7 + q]; out[6 + q] = m->rscl[7 + q]; }
+}
+
+/* CalculateInitialmdot (InitializaMdot.for:20-60), Densityf = rho */
+void om_initialize_mdot(om *m)
+{
+  const fs_case *cfg = &m->cfg;
+  for (int k = 0; k < m->F; k++) {
+    double uf = m->gf[k] * m->u[m->if_own[k]] + (1. - m->gf[k]) * m->u[m->if_nbr[k]];
+    double vf = m->gf[k] * m->v[m->if_own[k]] + (1. - m->gf[k]) * m->v[m->if_nbr[k]];
+    double wf = m->gf[k] * m->w[m->if_own[k]] + (1. - m->gf[k]) * m->w[m->if_nbr[k]];
+    m->mdot[k] = cfg->rho * (uf * m->sx[k] + vf * m->sy[k] + wf * m->sz[k]);
+  }
+  for (int b = 0; b < m->B; b++) {
+    if (m->btype[b] == FS_BC_WALL_NOSLIP || m->btype[b] == FS_BC_WALL_SLIP) m->bmdot[b] = 0.;
+    else m->bmdot[b] = cfg->rho * (m->bsx[b] * m->bu[b] + m->bsy[b] * m->bv[b] + m->bsz[b] * m->bw[b]);
+  }
 }
 
 void om_set_iter(om *m, int nIter) { m->nIter = nIter; }
@@ -1142,17 +1254,18 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
   m->fcf = dz_(F + B); m->fff = dz_(F + B); m->fvf = dz_(F + B); m->ftf = dz_(F + B);
   m->fce = dz_(N); m->fte = dz_(N); m->effdiv = dz_(N);
   m->ac = dz_(N); m->bc = dz_(N); m->dphi = dz_(N); m->anb = dz_((long)N * m->W);
-  /* CalculateInitialmdot (InitializaMdot.for:20-60), Densityf = rho */
-  for (int k = 0; k < F; k++) {
-    double uf = m->gf[k] * m->u[m->if_own[k]] + (1. - m->gf[k]) * m->u[m->if_nbr[k]];
-    double vf = m->gf[k] * m->v[m->if_own[k]] + (1. - m->gf[k]) * m->v[m->if_nbr[k]];
-    double wf = m->gf[k] * m->w[m->if_own[k]] + (1. - m->gf[k]) * m->w[m->if_nbr[k]];
-    m->mdot[k] = cfg->rho * (uf * m->sx[k] + vf * m->sy[k] + wf * m->sz[k]);
-  }
-  for (int b = 0; b < B; b++) {
-    if (m->btype[b] == FS_BC_WALL_NOSLIP || m->btype[b] == FS_BC_WALL_SLIP) m->bmdot[b] = 0.;
-    else m->bmdot[b] = cfg->rho * (m->bsx[b] * m->bu[b] + m->bsy[b] * m->bv[b] + m->bsz[b] * m->bw[b]);
-  }
+  m->mdot1 = dz_(m->NS); m->mdot_out = dz_(m->NS);
+  m->edif = dz_(N); m->bedif = dz_(B);
+  m->tke = dz_(N); m->ted = dz_(N); m->mut = dz_(N); m->btke = dz_(B); m->bted = dz_(B); m->bmut = dz_(B);
+  m->tkeg = dz_(3L*N); m->tedg = dz_(3L*N); m->btkeg = dz_(3L*B); m->btedg = dz_(3L*B);
+  m->tkegf = dz_(3L*F); m->tedgf = dz_(3L*F);
+  m->prod = dz_(N); m->bprod = dz_(B);
+  m->s11 = dz_(N); m->s12 = dz_(N); m->s13 = dz_(N); m->s22 = dz_(N); m->s23 = dz_(N); m->s33 = dz_(N);
+  m->rhok = dz_(N); m->brhok = dz_(B); m->drk = dz_(3L*N); m->bdrk = dz_(3L*B);
+  m->wdist = dz_(N); m->itau = iz_(N);
+  m->utau = dz_(B); m->yplus = dz_(B); m->uplus = dz_(B); m->dupdyp = dz_(B); m->tauw = dz_(B); m->wallvisc = dz_(B);
+  om_wall_distance(m);
+  om_initialize_mdot(m);
   return m;
 }
 
@@ -1196,6 +1309,13 @@ void *om_array(om *m, const char *name, long *len, int *is_int)
     {"own_slot", m->own_slot, F, 1}, {"nbr_slot", m->nbr_slot, F, 1},
     {"if_own", m->if_own, F, 1}, {"if_nbr", m->if_nbr, F, 1}, {"bf_own", m->bf_own, B, 1},
     {"btype", m->btype, B, 1}, {"kx", m->kx, m->kx ? N : 0, 0},
+    {"tke", m->tke, N, 0}, {"ted", m->ted, N, 0}, {"mut", m->mut, N, 0},
+    {"btke", m->btke, B, 0}, {"bted", m->bted, B, 0}, {"bmut", m->bmut, B, 0},
+    {"tkeg", m->tkeg, 3*N, 0}, {"tedg", m->tedg, 3*N, 0}, {"prod", m->prod, N, 0},
+    {"edif", m->edif, N, 0}, {"bedif", m->bedif, B, 0}, {"drk", m->drk, 3*N, 0},
+    {"wdist", m->wdist, N, 0}, {"itau", m->itau, N, 1},
+    {"utau", m->utau, B, 0}, {"yplus", m->yplus, B, 0}, {"uplus", m->uplus, B, 0},
+    {"dupdyp", m->dupdyp, B, 0}, {"wallvisc", m->wallvisc, B, 0}, {"bprod", m->bprod, B, 0},
   };
   for (unsigned q = 0; q < sizeof(t) / sizeof(t[0]); q++)
     if (strcmp(t[q].n, name) == 0) { *len = t[q].len; *is_int = t[q].isint; return t[q].p; }
