@@ -17,6 +17,7 @@ Forms (same case, same initial state):
                   [--ttr MAXIT]
   python bench.py --ensemble 64 [--gpus N]     the batched-ensemble configuration
   python bench.py --case distorted             the same cavity on the jittered mesh
+  python bench.py --case bfs                   the k-epsilon backward-facing step (512x96x48)
 
 b200 arm: `value` is device-timed (CUDA events on the solver's stream) with
 the state resident in HBM; `e2e` runs the fp64 steps through the C ABI
@@ -80,17 +81,38 @@ def aggregate_rate(world: int, steps: int, ms_max: float) -> float:
     return world * steps / (ms_max * 1e-3)
 
 
-def workload(n: int, form: str = "fp64", distorted: bool = False):
+def workload(n: int, form: str = "fp64", kind: str = "cubic"):
     """The n^3 cavity (Re 1000, SOU); distorted: interior nodes jittered by
     U(-0.2h, 0.2h) from seed 0 (non-orthogonal correction is always on:
-    MethodCalcGradient 2 and MethodDecomposeS 3)."""
+    MethodCalcGradient 2 and MethodDecomposeS 3); bfs: the backward-facing
+    step 4n x 3n/4 x 3n/8 (512x96x48 at n=128), k-epsilon with wall functions,
+    Re_H 5000, inlet u = 1 + 5% U(-1,1) from seed 0.  Returns (mesh, case,
+    initial state or None)."""
     from flowsolversourcecode_b200 import case as cs
-    kw = REFERENCE_SOLVERS if form == "reference" else FORMS[form]
-    return cs.cavity3d_distorted(n, seed=0, **kw) if distorted else cs.cavity3d(n, **kw)
+    kw = dict(REFERENCE_SOLVERS if form == "reference" else FORMS[form])
+    if kind == "bfs":
+        kw.pop("batched_momentum", None)      # k-epsilon runs the per-component momentum solves
+        mesh, case = cs.bfs(4 * n, 3 * n // 4, 3 * n // 8, **kw)
+        return mesh, case, cs.bfs_initial_state(mesh, case, seed=0)
+    mesh, case = cs.cavity3d_distorted(n, seed=0, **kw) if kind == "distorted" else cs.cavity3d(n, **kw)
+    return mesh, case, None
 
 
-def workload_name(n: int, distorted: bool) -> str:
-    return f"cavity3d_{n}" + ("_distorted (interior nodes jittered +-20% h, seed 0)" if distorted else "")
+def workload_name(n: int, kind: str) -> str:
+    if kind == "bfs":
+        return (f"bfs_{4 * n}x{3 * n // 4}x{3 * n // 8} backward-facing step, channel 30H x 3H x 2H, k-epsilon "
+                f"with equilibrium wall functions, Re_H=5000, inlet u=1+5% U(-1,1) seed 0")
+    return (f"cavity3d_{n}" + ("_distorted (interior nodes jittered +-20% h, seed 0)" if kind == "distorted" else "")
+            + " lid-driven cavity, Re=1000")
+
+
+def start(obj, init):
+    """Apply an initial state (set every field, then CalculateInitialmdot)."""
+    if init:
+        for k, v in init.items():
+            obj.set(k, v)
+        obj.initialize_mdot()
+    return obj
 
 
 class Clocks:
@@ -239,17 +261,17 @@ def solver_roofline(stats: dict, mg: dict | None, N: int, W: int, hbm: float, fo
             "iters_per_launch": best["iters"] / best["calls"]}
 
 
-def cpu_baseline_sample(n: int, distorted: bool = False) -> dict:
+def cpu_baseline_sample(n: int, kind: str = "cubic") -> dict:
     import oracle
-    mesh, case = workload(n, "reference", distorted)
-    o = oracle.Oracle(mesh, case)
+    mesh, case, init = workload(n, "reference", kind)
+    o = start(oracle.Oracle(mesh, case), init)
     t0 = time.perf_counter()
     o.simple_iteration()
     dt = time.perf_counter() - t0
     o.close()
     return {"value": 1.0 / dt, "unit": "iter/s", "cores": 1, "kind": "port",
-            "sample": f"the 1st SIMPLE outer iteration of the same {n}^3 case on the sequential CPU "
-                      f"restatement (p' by the reference's unpreconditioned BiCGSTAB to 1e-8), 1 thread"}
+            "sample": f"the 1st SIMPLE outer iteration of the same {mesh.n_cells}-cell case on the sequential "
+                      f"CPU restatement (p' by the reference's unpreconditioned BiCGSTAB to 1e-8), 1 thread"}
 
 
 def run_reference(args, rank: int) -> None:
@@ -257,8 +279,8 @@ def run_reference(args, rank: int) -> None:
         return
     import oracle
     oracle.build()
-    mesh, case = workload(args.n, "reference", args.case == "distorted")
-    o = oracle.Oracle(mesh, case)
+    mesh, case, init = workload(args.n, "reference", args.case)
+    o = start(oracle.Oracle(mesh, case), init)
     warm = 1
     t0 = time.perf_counter()
     for _ in range(warm):
@@ -280,8 +302,7 @@ def run_reference(args, rank: int) -> None:
         "impl": "reference", "metric": "SIMPLE iters/s", "value": val, "unit": "iter/s", "n_gpus": args.gpus,
         "steps": k_run, "warmup": warm, "ms_per_step": 1e3 * total / k_run,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{workload_name(args.n, args.case == 'distorted')} lid-driven cavity, "
-                               f"{mesh.n_cells} cells, Re=1000, SOU, SIMPLEC",
+        "config": {"workload": f"{workload_name(args.n, args.case)}, {mesh.n_cells} cells, SOU, SIMPLEC",
                    "cells": mesh.n_cells,
                    "solvers": "momentum sor, p' bicgs (the reference's unpreconditioned BiCGSTAB) to 1e-8"},
         "cpu_baseline": {"value": val, "unit": "iter/s", "cores": 1, "kind": "port",
@@ -331,9 +352,9 @@ def assembly_roofline(leg: dict, N: int, F: int, steps: int, hbm: float) -> dict
             "frac": round(achieved / hbm, 4), "bytes_per_step": nbytes / steps, "ms_per_step": ms / steps}
 
 
-def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e-6) -> dict:
+def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e-6, init=None) -> dict:
     """Device time from the initial state until the stop metric drops below tol."""
-    s = Solver(mesh, case, device=local)
+    s = start(Solver(mesh, case, device=local), init)
     s.timer_start()
     total, it, src = 0.0, 0, None
     for it in range(1, maxit + 1):
@@ -410,7 +431,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=128)
-    ap.add_argument("--case", default="cubic", choices=["cubic", "distorted"])
+    ap.add_argument("--case", default="cubic", choices=["cubic", "distorted", "bfs"])
     ap.add_argument("--ttr", type=int, default=0, help="max iterations of the time-to-1e-6 leg (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", type=int, default=0, help="run the batched-ensemble configuration with this many cases")
@@ -450,16 +471,17 @@ def main():
             dist.barrier()
 
     warm = max(args.warmup, 3)
-    distorted = args.case == "distorted"
-    mesh, case = workload(args.n, "fp64", distorted)
+    kind = args.case
+    mesh, case, init = workload(args.n, "fp64", kind)
 
     # ---------------- fp64 form: device-resident leg
-    s = Solver(mesh, case, device=local)
+    s = start(Solver(mesh, case, device=local), init)
     N, W, F = s.N, s.W, s.F
     mg = s.mg_info()
     d64 = device_leg(s, args.steps, warm, barrier, local)
     ms_max = reduce_max(d64["ms"], dist, f"cuda:{local}")
-    fields64 = {k: s.get(k) for k in ("u", "v", "w", "p")}
+    fkeys = ("u", "v", "w", "p") + (("tke", "ted") if case.turbulence else ())
+    fields64 = {k: s.get(k) for k in fkeys}
 
     # ---------------- fp64 form: end-to-end leg (host buffers through the C ABI)
     st = s.state()
@@ -482,8 +504,8 @@ def main():
     s.close()
 
     # ---------------- mixed form: same case and initial state
-    _, case_m = workload(args.n, "mixed", distorted)
-    sm = Solver(mesh, case_m, device=local)
+    _, case_m, _ = workload(args.n, "mixed", kind)
+    sm = start(Solver(mesh, case_m, device=local), init)
     dmx = device_leg(sm, args.steps, warm, barrier, local)
     msm_max = reduce_max(dmx["ms"], dist, f"cuda:{local}")
     err = {}
@@ -494,8 +516,8 @@ def main():
 
     ttr = None
     if args.ttr > 0:
-        ttr = {"fp64": time_to_residual(Solver, mesh, case, local, args.ttr),
-               "mixed": time_to_residual(Solver, mesh, case_m, local, args.ttr)}
+        ttr = {"fp64": time_to_residual(Solver, mesh, case, local, args.ttr, init=init),
+               "mixed": time_to_residual(Solver, mesh, case_m, local, args.ttr, init=init)}
 
     if rank == 0:
         hbm, src = peaks()
@@ -512,22 +534,24 @@ def main():
                     "fallback 6.65 TB/s"
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline_sample(args.n, distorted)
+            cpu = cpu_baseline_sample(args.n, kind)
         value = aggregate_rate(world, args.steps, ms_max)
         line = {
             "metric": "SIMPLE iters/s", "value": value, "unit": "iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": warm, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"{workload_name(args.n, distorted)} lid-driven cavity, {N} cells, {F} interior faces, "
-                                   f"Re=1000, SOU deferred correction, SIMPLEC urf 0.7/0.7",
+            "config": {"workload": f"{workload_name(args.n, kind)}, {N} cells, {F} interior faces, "
+                                   f"SOU deferred correction, SIMPLEC urf 0.7/0.7",
                        "cells": N, "faces": F,
                        "solvers": "momentum: multicolour SOR (rrF 0.01, 30 sweeps); p': FP64 BiCGSTAB "
-                                  "right-preconditioned by one element-agglomeration AMG V-cycle, tol 1e-8",
+                                  "right-preconditioned by one element-agglomeration AMG V-cycle, tol 1e-8"
+                                  + ("; k, epsilon: multicolour SOR (rrF 0.1, 10 / 3 sweeps)" if case.turbulence else ""),
                        "mg_levels": mg["sizes"], "mg_prec_coarsest": mg["prec_coarsest"],
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (working set ~2 GB)",
                        "lin_iters_last_step": d64["last"]["lin_iters"] if d64["last"] else None,
+                       "turb_lin_iters_last_step": d64["last"]["turb_lin_iters"] if case.turbulence and d64["last"] else None,
                        "solver_ms_per_step": [round(x / args.steps, 3) for x in d64["stats"]["ms"]],
                        "phase_ms_last_step": [round(x, 3) for x in d64["phases"]]},
             "roofline": roof,
@@ -537,8 +561,8 @@ def main():
                     "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
             "gpu_launches": d64["launches"],
             "clocks": d64["clocks"],
-            "mixed": {"form": "FP32 AMG V-cycle (FP32 coarse matrices) inside FP64 BiCGSTAB to 1e-8; "
-                              "multi-RHS momentum SOR",
+            "mixed": {"form": "FP32 AMG V-cycle (FP32 coarse matrices) inside FP64 BiCGSTAB to 1e-8"
+                              + ("" if case.turbulence else "; multi-RHS momentum SOR"),
                       "value": aggregate_rate(world, args.steps, msm_max), "unit": "iter/s",
                       "ms_per_step": msm_max / args.steps,
                       "time_vs_fp64": msm_max / ms_max,
