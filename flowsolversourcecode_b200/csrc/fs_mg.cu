@@ -761,25 +761,56 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
 }
 
 // coarse matrix of level lc from level lc-1 (AssembleElementBasedAgglomoratedLHS.for:45-150)
-__global__ void k_mg_lhs(int nf, const int32_t *ncf_f, const double *ac_f, const double *anb_f,
-                         int nc, int wc, const int32_t *cptr, const int32_t *clist, const int32_t *cmap,
-                         double *ac_c, double *anb_c) {
+// one thread per coarse row (AssembleElementBasedAgglomoratedLHS.for:45-150):
+// the children in list order, each child's diagonal then its neighbour slots in
+// slot order, so every coarse entry is summed in the reference's order.  The
+// coarse row's off-diagonal sums live in shared memory (wc doubles per thread,
+// column-major across the block).  WF > 0 bounds the fine width: a child's
+// slots are then loaded all at once (independent loads in flight) before the
+// additions, instead of one dependent load chain per slot.
+template <int WF>
+__global__ void k_mg_lhs(int nf, const int32_t *__restrict__ ncf_f, const double *__restrict__ ac_f,
+                         const double *__restrict__ anb_f, int nc, int wc, const int32_t *__restrict__ cptr,
+                         const int32_t *__restrict__ clist, const int32_t *__restrict__ cmap,
+                         double *__restrict__ ac_c, double *__restrict__ anb_c) {
+  extern __shared__ double sacc[];
   int P = blockIdx.x * blockDim.x + threadIdx.x;
+  const int T = blockDim.x;
+  double *acc_nb = sacc + threadIdx.x;
+  for (int k = 0; k < wc; k++) acc_nb[(long)k * T] = 0.;
   if (P >= nc) return;
   double acc = 0.;
-  for (int k = 0; k < wc; k++) anb_c[(long)k * nc + P] = 0.;
-  for (int q = cptr[P]; q < cptr[P + 1]; q++) {
-    int c = clist[q];
-    acc = acc + ac_f[c];
-    int nn = ncf_f[c];
-    for (int j = 0; j < nn; j++) {
-      int t = cmap[(long)j * nf + c];
-      double a = anb_f[(long)j * nf + c];
-      if (t == -2) acc = acc + a;
-      else if (t >= 0) anb_c[(long)t * nc + P] = anb_c[(long)t * nc + P] + a;
+  const int q0 = cptr[P], q1 = cptr[P + 1];
+  for (int q = q0; q < q1; q++) {
+    const int c = clist[q];
+    const double a0 = ac_f[c];
+    const int nn = ncf_f[c];
+    if (WF > 0) {
+      int t[WF > 0 ? WF : 1];
+      double a[WF > 0 ? WF : 1];
+#pragma unroll
+      for (int j = 0; j < WF; j++) {
+        t[j] = -1; a[j] = 0.;
+        if (j < nn) { t[j] = cmap[(long)j * nf + c]; a[j] = anb_f[(long)j * nf + c]; }
+      }
+      acc = acc + a0;
+#pragma unroll
+      for (int j = 0; j < WF; j++) {
+        if (t[j] == -2) acc = acc + a[j];
+        else if (t[j] >= 0) acc_nb[(long)t[j] * T] = acc_nb[(long)t[j] * T] + a[j];
+      }
+    } else {
+      acc = acc + a0;
+      for (int j = 0; j < nn; j++) {
+        const int tj = cmap[(long)j * nf + c];
+        const double aj = anb_f[(long)j * nf + c];
+        if (tj == -2) acc = acc + aj;
+        else if (tj >= 0) acc_nb[(long)tj * T] = acc_nb[(long)tj * T] + aj;
+      }
     }
   }
   ac_c[P] = acc;
+  for (int k = 0; k < wc; k++) anb_c[(long)k * nc + P] = acc_nb[(long)k * T];
 }
 
 __global__ void k_to_f32(long n, const double *a, float *b) {
@@ -817,23 +848,32 @@ __global__ void __launch_bounds__(1024) k_mg_dense_inverse(int n, const int32_t 
   if (sing)
     for (int j = tid; j < n; j += nt) A[(long)(n - 1) * n + j] = j == n - 1 ? 1. : 0.;
   __syncthreads();
-  // warps take rows, lanes take columns: the pivot row is read with unit
-  // stride across a warp and no index division is needed
+  // warps take rows, lanes take columns.  The pivot row and column of step k
+  // are read from buffers (prow/pcol, double-buffered by the parity of k) that
+  // the update of step k-1 filled, so one block barrier per pivot suffices;
+  // every entry goes through the same operations as an in-place elimination.
   const int lane = tid & 31, wid = tid >> 5, nwarp = nt >> 5;
+  double *prow = col + n, *pcol = prow + 2 * n;   // [2][n] each
+  for (int j = tid; j < n; j += nt) { prow[j] = A[j]; pcol[j] = A[(long)j * n]; }
+  __syncthreads();
   for (int k = 0; k < n; k++) {
-    const double d = A[(long)k * n + k];
+    const int b = k & 1;
+    const double *pr = prow + b * n, *pc = pcol + b * n;
+    double *nr = prow + (b ^ 1) * n, *nc = pcol + (b ^ 1) * n;
+    const double d = pr[k];
     const double p = d != 0. ? 1. / d : 0.;
-    __syncthreads();
-    for (int i = tid; i < n; i += nt)
-      if (i != k) col[i] = A[(long)i * n + k];
-    for (int j = tid; j < n; j += nt) A[(long)k * n + j] = j == k ? p : A[(long)k * n + j] * p;
-    __syncthreads();
-    const double *rk = A + (long)k * n;
     for (int i = wid; i < n; i += nwarp) {
-      if (i == k) continue;
-      const double ci = col[i];
       double *ri = A + (long)i * n;
-      for (int j = lane; j < n; j += 32) ri[j] = j == k ? -ci * p : ri[j] - ci * rk[j];
+      const double ci = pc[i];
+      for (int j = lane; j < n; j += 32) {
+        const double rkj = j == k ? p : pr[j] * p;
+        double v;
+        if (i == k) v = rkj;
+        else v = j == k ? -ci * p : ri[j] - ci * rkj;
+        ri[j] = v;
+        if (i == k + 1) nr[j] = v;
+        if (j == k + 1) nc[i] = v;
+      }
     }
     __syncthreads();
   }
@@ -1069,7 +1109,7 @@ int fs_mg_build(fs_ctx *ctx) {
     // the attribute belongs to the function, shared by every context of the
     // process: set it for the largest coarsest level any context may have
     FS_CK(cudaFuncSetAttribute((const void *)k_mg_dense_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(sizeof(double) * ((size_t)FS_MG_DIRECT * FS_MG_DIRECT + FS_MG_DIRECT))));
+                               (int)(sizeof(double) * ((size_t)FS_MG_DIRECT * FS_MG_DIRECT + 5 * FS_MG_DIRECT))));
   }
   // cooperative grid: smallest co-resident count of the three kernels, <= 4 CTAs/SM
   int a = 0, b = 0, c = 0;
@@ -1102,9 +1142,18 @@ int fs_mg_free(fs_ctx *ctx) {
 static int mg_coarse_matrices(fs_ctx *ctx, int last, bool f32) {
   fs_mg_dev *M = ctx->mg;
   for (int q = 1; q <= last; q++) {
-    k_mg_lhs<<<fs_grid(M->n[q]), FS_BLOCK, 0, ctx->st>>>(M->n[q - 1], M->nnb[q - 1], M->ac[q - 1], M->anb[q - 1],
-                                                        M->n[q], M->w[q], M->cptr[q], M->clist[q], M->cmap[q],
-                                                        M->ac[q], M->anb[q]);
+    // block of T threads with T * w doubles of shared accumulators (<= 48 KB)
+    int T = 128;
+    while (T > 32 && (size_t)T * M->w[q] * sizeof(double) > 48 * 1024) T /= 2;
+    const size_t sm = (size_t)T * M->w[q] * sizeof(double);
+    if (sm > 48 * 1024) { ctx->err = "coarse level too wide for the coarse-matrix kernel"; return FS_E_UNSUPPORTED; }
+    const int wf = M->w[q - 1];
+#define FS_LHS_ARGS M->n[q - 1], M->nnb[q - 1], M->ac[q - 1], M->anb[q - 1], M->n[q], M->w[q], M->cptr[q], \
+                    M->clist[q], M->cmap[q], M->ac[q], M->anb[q]
+    if (wf <= 8) k_mg_lhs<8><<<fs_grid(M->n[q], T), T, sm, ctx->st>>>(FS_LHS_ARGS);
+    else if (wf <= 32) k_mg_lhs<32><<<fs_grid(M->n[q], T), T, sm, ctx->st>>>(FS_LHS_ARGS);
+    else k_mg_lhs<0><<<fs_grid(M->n[q], T), T, sm, ctx->st>>>(FS_LHS_ARGS);
+#undef FS_LHS_ARGS
     FS_LAUNCH_CHECK();
   }
   if (f32)
@@ -1142,7 +1191,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
   FS_CK(cudaMemsetAsync(ctx->d_status + 4, 0, sizeof(int32_t) * 2, ctx->st));
   if (M->direct) {
     const int n = M->n[M->lc];
-    k_mg_dense_inverse<<<1, 1024, sizeof(double) * ((size_t)n * n + n), ctx->st>>>(
+    k_mg_dense_inverse<<<1, 1024, sizeof(double) * ((size_t)n * n + 5 * (size_t)n), ctx->st>>>(
         n, M->nnb[M->lc], M->nbr[M->lc], M->ac[M->lc], M->anb[M->lc], M->sinv);
     FS_LAUNCH_CHECK();
   }
