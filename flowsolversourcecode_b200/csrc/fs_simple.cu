@@ -56,11 +56,10 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_GG0_MINB) k_gg0(GradJob J, int N,
   double ps[NF], gx[NF], gy[NF], gz[NF];
 #pragma unroll
   for (int q = 0; q < NF; q++) { ps[q] = J.phi[q][i]; gx[q] = 0.; gy[q] = 0.; gz[q] = 0.; }
-  for (int j = 0; j < nc; j++) {
-    int s = slot[(long)j * N + i];
+  FS_SLOT_PREFETCH(nc, slot, cn, N, i);
+  auto face = [&](int s, int k) {
     int f = s >> 1;
     if (f < F) {
-      int k = cn[(long)j * N + i];
       double g = gf[f], sx = sf[f], sy = sf[F + f], sz = sf[2L * F + f];
       bool nb = s & 1;
 #pragma unroll
@@ -81,7 +80,8 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_GG0_MINB) k_gg0(GradJob J, int N,
         gx[q] = gx[q] + bp * bx; gy[q] = gy[q] + bp * by; gz[q] = gz[q] + bp * bz;
       }
     }
-  }
+  };
+  FS_SLOT_LOOP(nc, slot, cn, N, i, face);
 #pragma unroll
   for (int q = 0; q < NF; q++) {
     double *o = J.out[q];
@@ -106,11 +106,10 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_GG_MINB) k_gg_corr(GradJob J, int
     gsx[q] = J.in[q][i]; gsy[q] = J.in[q][N + i]; gsz[q] = J.in[q][2L * N + i];
     gx[q] = 0.; gy[q] = 0.; gz[q] = 0.;
   }
-  for (int j = 0; j < nc; j++) {
-    int s = slot[(long)j * N + i];
+  FS_SLOT_PREFETCH(nc, slot, cn, N, i);
+  auto face = [&](int s, int k) {
     int f = s >> 1;
     if (f < F) {
-      int k = cn[(long)j * N + i];
       double g = gf[f], g1 = 1. - g;
       double sx = sf[f], sy = sf[F + f], sz = sf[2L * F + f];
       double dx = dfp[f], dy = dfp[F + f], dz = dfp[2L * F + f];
@@ -141,7 +140,8 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_GG_MINB) k_gg_corr(GradJob J, int
         gx[q] = gx[q] + bp * bx; gy[q] = gy[q] + bp * by; gz[q] = gz[q] + bp * bz;
       }
     }
-  }
+  };
+  FS_SLOT_LOOP(nc, slot, cn, N, i, face);
 #pragma unroll
   for (int q = 0; q < NF; q++) {
     double *o = J.out[q];
@@ -658,11 +658,14 @@ __global__ void k_mass_final(CorrArgs a, const double *mdot_in_dev) {
   }
 }
 
-// inlet mass flow: one CTA, strided per-thread sums then a fixed tree (deterministic)
-__global__ void k_sum_inlet(int B, const int32_t *btype, const double *bmdot, double *out) {
+// inlet mass flow: one CTA over the inlet patches' face ranges, strided
+// per-thread sums then a fixed tree (deterministic)
+struct InletRanges { int n; int start[FS_MAX_PATCHES], cnt[FS_MAX_PATCHES]; };
+__global__ void k_sum_inlet(InletRanges r, const double *bmdot, double *out) {
   __shared__ double sh[32];
   double s = 0.;
-  for (int b = threadIdx.x; b < B; b += blockDim.x) if (btype[b] == FS_BC_INLET_VEL) s += bmdot[b];
+  for (int q = 0; q < r.n; q++)
+    for (int j = threadIdx.x; j < r.cnt[q]; j += blockDim.x) s += bmdot[r.start[q] + j];
   s = block_sum(s, sh);
   if (threadIdx.x == 0) *out = s;
 }
@@ -848,13 +851,14 @@ int fs_continuity_correct(fs_ctx *ctx) {
   if (B) { k_bcorr<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   k_mass_imbalance<<<a.nblk, FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();
-  bool has_inlet = false;
-  for (int s = 0; s < ctx->NS; s++) if (c.patch_type[s] == FS_BC_INLET_VEL) has_inlet = true;
+  InletRanges ir{};
+  for (int s = 0; s < ctx->NS; s++)
+    if (c.patch_type[s] == FS_BC_INLET_VEL) { ir.start[ir.n] = ctx->h_bset_start[s]; ir.cnt[ir.n] = ctx->h_bset_n[s]; ir.n++; }
   double *d_in = nullptr;
-  if (has_inlet) {
+  if (ir.n) {
     // inlet mass flow, used only through ResorScaled(5); stays on the device
     d_in = ctx->resblk + RB_MDOTIN;
-    k_sum_inlet<<<1, 1024, 0, ctx->st>>>(B, ctx->btype, ctx->bmdot, d_in);
+    k_sum_inlet<<<1, 1024, 0, ctx->st>>>(ir, ctx->bmdot, d_in);
     FS_LAUNCH_CHECK();
   }
   k_mass_final<<<1, 1024, 0, ctx->st>>>(a, d_in);
