@@ -6,6 +6,23 @@
 #pragma once
 #include "fs_internal.cuh"
 
+// Slot loops of the cell-centric gathers: the first FS_PF (face, neighbour)
+// pairs of a cell are loaded up front, so a face's data loads no longer wait
+// behind its own index loads; faces are still visited in slot order.
+#define FS_PF 6
+#define FS_SLOT_PREFETCH(nc, slot, cn, N, i)                                    \
+  int pf_s_[FS_PF], pf_k_[FS_PF];                                               \
+  _Pragma("unroll") for (int j_ = 0; j_ < FS_PF; j_++) {                        \
+    pf_s_[j_] = j_ < (nc) ? (slot)[(long)j_ * (N) + (i)] : 0;                   \
+    pf_k_[j_] = j_ < (nc) ? (cn)[(long)j_ * (N) + (i)] : 0;                     \
+  }
+#define FS_SLOT_LOOP(nc, slot, cn, N, i, fn)                                    \
+  do {                                                                          \
+    _Pragma("unroll") for (int j_ = 0; j_ < FS_PF; j_++)                        \
+      if (j_ < (nc)) fn(pf_s_[j_], pf_k_[j_]);                                  \
+    for (int j_ = FS_PF; j_ < (nc); j_++) fn((slot)[(long)j_ * (N) + (i)], (cn)[(long)j_ * (N) + (i)]); \
+  } while (0)
+
 namespace {
 
 constexpr double M23 = (double)(-2.0f / 3.0f);   // `-2./3.` is REAL(4) (AssembleBulkViscosity.for:36)
