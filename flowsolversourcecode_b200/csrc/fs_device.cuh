@@ -22,6 +22,17 @@
       if (j_ < (nc)) fn(pf_s_[j_], pf_k_[j_]);                                  \
     for (int j_ = FS_PF; j_ < (nc); j_++) fn((slot)[(long)j_ * (N) + (i)], (cn)[(long)j_ * (N) + (i)]); \
   } while (0)
+// a rolled loop over the prefetched pairs, passing the slot index too:
+// fn(j, slot, neighbour); for bodies too large to unroll (the prefetched
+// pairs then sit in thread-local memory, an L1 hit per slot)
+#define FS_SLOT_LOOP_J(nc, slot, cn, N, i, fn)                                  \
+  do {                                                                          \
+    _Pragma("unroll 1") for (int j_ = 0; j_ < (nc); j_++) {                     \
+      const int s_ = j_ < FS_PF ? pf_s_[j_] : (slot)[(long)j_ * (N) + (i)];     \
+      const int k_ = j_ < FS_PF ? pf_k_[j_] : (cn)[(long)j_ * (N) + (i)];       \
+      fn(j_, s_, k_);                                                           \
+    }                                                                           \
+  } while (0)
 
 namespace {
 

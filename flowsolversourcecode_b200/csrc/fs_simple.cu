@@ -219,12 +219,11 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs 
   const double gvs[3] = {a.vg[i], a.vg[N + i], a.vg[N2 + i]};
   const double gws[3] = {a.wg[i], a.wg[N + i], a.wg[N2 + i]};
   double ac = 0., bcu = 0., bcv = 0., bcw = 0., ed = 0.;
-  for (int j = 0; j < nc; j++) {
-    int s = a.slot[(long)j * N + i];
+  FS_SLOT_PREFETCH(nc, a.slot, a.cn, N, i);
+  auto face = [&](int j, int s, int k) {
     int f = s >> 1;
-    if (f >= F) { ed = ed + a.bmdot[f - F]; continue; }
+    if (f >= F) { ed = ed + a.bmdot[f - F]; return; }
     const bool nb = s & 1;                 // this cell is the face's neighbour
-    const int k = a.cn[(long)j * N + i];
     double g = a.gf[f], md = a.mdot[f];
     double sx = a.sf[f], sy = a.sf[F + f], sz = a.sf[F2 + f];
     const double uk = a.u[k], vk = a.v[k], wk = a.w[k];
@@ -294,7 +293,8 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs 
       bcu = bcu - tu; bcv = bcv - tv; bcw = bcw - tw;
       ed = ed + md;
     }
-  }
+  };
+  FS_SLOT_LOOP_J(nc, a.slot, a.cn, N, i, face);
   a.ac_int[i] = ac;
   a.bc_int[i] = bcu; a.bc_int[N + i] = bcv; a.bc_int[N2 + i] = bcw;
   a.effdiv[i] = ed;
@@ -501,8 +501,8 @@ __global__ void __launch_bounds__(FS_BLOCK) k_pc_assemble(ContArgs a) {
     const int N = a.N, F = a.F;
     int nc = a.ncf[i];
     double ac = 0., bc = 0.;
-    for (int j = 0; j < nc; j++) {
-      int s = a.slot[(long)j * N + i];
+    FS_SLOT_PREFETCH(nc, a.slot, a.slot, N, i);
+    auto face = [&](int j, int s, int) {
       int f = s >> 1;
       if (f < F) {
         double c = a.pcoef[f], fff = -c, md = a.mdot[f];
@@ -512,7 +512,8 @@ __global__ void __launch_bounds__(FS_BLOCK) k_pc_assemble(ContArgs a) {
         ac = ac + 0.;
         bc = bc - a.bmdot[f - F];
       }
-    }
+    };
+    FS_SLOT_LOOP_J(nc, a.slot, a.slot, N, i, face);
     ac = ac + 0.; bc = bc - 0.;
     a.ac[i] = ac; a.bc[i] = bc;
     r = fabs(bc);

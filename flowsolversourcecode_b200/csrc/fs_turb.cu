@@ -213,8 +213,8 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
     }
     // ---- faces, slot order = the reference's face order for this cell
     double ac = 0., bc = 0., ed = 0.;
-    for (int j = 0; j < nc; j++) {
-      int s = a.slot[(long)j * N + i];
+    FS_SLOT_PREFETCH(nc, a.slot, a.cn, N, i);
+    auto face = [&](int j, int s, int k) {
       int f = s >> 1;
       if (f >= F) {
         int b = f - F, t = a.btype[b];
@@ -236,10 +236,9 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
         }
         ac = ac + fcf;
         bc = bc - tf;
-        continue;
+        return;
       }
       const bool nb = s & 1;
-      const int k = a.cn[(long)j * N + i];
       const double g = a.gf[f], md = a.mdot[f];
       const double pk = a.phi[k];
       const double gk[3] = {a.phig[k], a.phig[N + k], a.phig[2L * N + k]};
@@ -273,7 +272,8 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
         bc = bc - tf;
         ed = ed + md;
       }
-    }
+    };
+    FS_SLOT_LOOP_J(nc, a.slot, a.cn, N, i, face);
     // effective divergence (AssembleConvection.for:165-178)
     double fce2 = fmax(ed, 0.0) - ed;
     double fve = -(fmax(ed, 0.0) * ps);
