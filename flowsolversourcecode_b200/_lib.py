@@ -70,6 +70,7 @@ class FsCase(C.Structure):
         ("max_visc_ratio", C.c_double), ("limit_production", C.c_int),
         ("conv_scheme_tke", C.c_int), ("conv_scheme_ted", C.c_int),
         ("inlet_intensity", C.c_double * FS_MAX_PATCHES), ("inlet_length", C.c_double * FS_MAX_PATCHES),
+        ("wall_function", C.c_int),
     ]
 
 

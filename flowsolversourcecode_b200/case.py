@@ -88,6 +88,7 @@ class Case:
     limit_production: bool = True          # LimitTurbulenceProduction
     conv_scheme_tke: str = "upwind"        # ConvectionSchemeTKE
     conv_scheme_ted: str = "minmod"        # ConvectionSchemeTED
+    wall_function: str = "standard"        # MomentumWallFunctionType: 'standard' or 'scalable'
     # inlet patch name -> (inletTurbulenceIntensity, inletTurbulenceLengthScale), 'specifiedil'
     inlet_turbulence: dict = field(default_factory=dict)
 
@@ -136,6 +137,7 @@ class Case:
         c.urf_tke, c.urf_ted, c.urf_tvisc = self.urf_tke, self.urf_ted, self.urf_tvisc
         c.max_visc_ratio, c.limit_production = self.max_visc_ratio, int(self.limit_production)
         c.conv_scheme_tke, c.conv_scheme_ted = L.TVD[self.conv_scheme_tke], L.TVD[self.conv_scheme_ted]
+        c.wall_function = {"standard": 0, "scalable": 1}[self.wall_function]
         return c
 
 

@@ -1,5 +1,5 @@
-// fs_turb.cu -- standard k-epsilon with equilibrium 'standard' momentum wall
-// functions (Turbulence/ of the reference, TurbulenceModel='kepsilon'), and
+// fs_turb.cu -- standard k-epsilon with equilibrium 'standard' or 'scalable'
+// momentum wall functions (Turbulence/ of the reference, TurbulenceModel='kepsilon'), and
 // the 'fullydeveloped' outlet mass-flow adjustment of SolveContinuity.
 //
 // The k and epsilon equations go through one cell-centric gather kernel each
@@ -47,7 +47,7 @@ constexpr double TWOTHIRD = (double)(2.0f / 3.0f);              // Constants1.F9
 struct TurbArgs {
   int N, F, B;
   double rho, mu, urf, bleed, cmu75, tvisc_urf, max_ratio;
-  int scheme, hr_on, limit, first;
+  int scheme, hr_on, limit, first, scalable;
   const int32_t *ncf, *slot, *cn, *bown, *btype, *bset;
   const double *gf, *sf, *dcfv, *gdiff, *tf, *vol;
   const double *bsf, *bnf, *bdv, *bgdiff, *btf;
@@ -96,7 +96,8 @@ __global__ void k_wall_distance(TurbArgs a) {
 
 // CalculateEffectiveDiffusionCoefficient('vel?') boundary part
 // (ComputeEffectiveDiffusionCoefficient.for:34-46) and
-// EquilibriumMomentumWallFunctions, 'standard' (WallFunctions.for:1846-1935)
+// EquilibriumMomentumWallFunctions (WallFunctions.for:1846-1993): 'standard'
+// (:1918-1960) or 'scalable' (:1961-1993, y+ clipped to ctrans + tiny)
 __global__ void k_wall_fn(TurbArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= a.B) return;
@@ -109,9 +110,17 @@ __global__ void k_wall_fn(TurbArgs a) {
     a.yplus[b] = rho * a.utau[b] * dn / mu;
   }
   double yp1 = dn * rho * a.utau[b] / mu;
-  double yp = fmax(yp1, KE_YPMIN), up, ut, dd;
-  if (yp < KE_CTRANS) { up = yp; ut = wv / up; dd = 1.; }
-  else { up = log(yp) / KE_KAPPA + KE_CC; ut = wv / up; dd = 1. / (KE_KAPPA * yp); }
+  double yp, up, ut, dd;
+  if (a.scalable) {
+    yp = fmax(yp1, KE_CTRANS + TINY);
+    dd = 1. / (KE_KAPPA * yp);
+    up = log(yp) / KE_KAPPA + KE_CC;
+    ut = wv / up;
+  } else {
+    yp = fmax(yp1, KE_YPMIN);
+    if (yp < KE_CTRANS) { up = yp; ut = wv / up; dd = 1.; }
+    else { up = log(yp) / KE_KAPPA + KE_CC; ut = wv / up; dd = 1. / (KE_KAPPA * yp); }
+  }
   a.yplus[b] = yp; a.uplus[b] = up; a.utau[b] = ut; a.dupdyp[b] = dd;
   double tw = rho * ut * ut;
   double wvis = tw * dn / fmax(wv, TINY);
@@ -139,14 +148,17 @@ __global__ void k_inlet_turb(TurbArgs a) {
   a.bmut[b] = (1. - a.tvisc_urf) * a.bmut[b] + KE_CMU * a.tvisc_urf * a.rho * (k * k) / fmax(e, TINY);
 }
 
-// wall-adjacent epsilon (AssembleTEDSources.for:78-95): the cell's last wall face decides
+// wall-adjacent epsilon (AssembleTEDSources.for:78-120): the cell's last wall face decides
 __global__ void k_ted_wall(TurbArgs a) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.N) return;
   int b = a.itau[i];
   if (b < 0) return;
   double dn = a.wdist[i], k = fmax(a.tke[i], 0.);
-  if (a.yplus[b] < KE_CTRANS) a.ted[i] = 2. * a.mu * k / (a.rho * (dn * dn));
+  if (a.scalable) {
+    dn = a.yplus[b] * a.mu / (a.rho * a.utau[b]);
+    a.ted[i] = a.cmu75 * pow(k, 1.5) / (KE_KAPPA * dn);
+  } else if (a.yplus[b] < KE_CTRANS) a.ted[i] = 2. * a.mu * k / (a.rho * (dn * dn));
   else a.ted[i] = a.cmu75 * pow(k, 1.5) / (KE_KAPPA * dn);
 }
 
@@ -392,6 +404,7 @@ TurbArgs turb_args(fs_ctx *ctx) {
   a.rho = c.rho; a.mu = c.mu; a.bleed = c.bleed;
   a.cmu75 = sqrt(sqrt(KE_CMU)); a.cmu75 = a.cmu75 * a.cmu75 * a.cmu75;
   a.tvisc_urf = c.urf_tvisc; a.max_ratio = c.max_visc_ratio; a.limit = c.limit_production;
+  a.scalable = c.wall_function == 1;
   a.ncf = ctx->ncf; a.slot = ctx->slot; a.cn = ctx->cn; a.bown = ctx->bown; a.btype = ctx->btype; a.bset = ctx->d_bset;
   a.gf = ctx->gf; a.sf = ctx->sf; a.dcfv = ctx->dcfv; a.gdiff = ctx->gdiff; a.tf = ctx->tf; a.vol = ctx->vol;
   a.bsf = ctx->bsf; a.bnf = ctx->bnf; a.bdv = ctx->bdv; a.bgdiff = ctx->bgdiff; a.btf = ctx->btf;

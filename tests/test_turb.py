@@ -107,10 +107,11 @@ def test_oracle_wall_function_law():
 
 # ------------------------------------------------------------------- GPU
 @pytest.mark.gpu
-def test_kepsilon_step_matches_oracle():
+@pytest.mark.parametrize("wall_function", ["standard", "scalable"])
+def test_kepsilon_step_matches_oracle(wall_function):
     import oracle
     from flowsolversourcecode_b200.solver import Solver
-    m, c = cs.bfs(24, 9, 6, **_tight())
+    m, c = cs.bfs(24, 9, 6, **_tight(wall_function=wall_function))
     o = oracle.Oracle(m, c)
     g = Solver(m, c)
     _setup(o, m, c)
