@@ -55,6 +55,7 @@ def load():
         lib.om_calc_residuals.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         lib.om_residuals_turb.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         lib.om_initialize_mdot.argtypes = [C.c_void_p]
+        lib.om_turb_production.argtypes = [C.c_void_p]
         lib.om_mg_setup.restype = C.c_int
         lib.om_mg_setup.argtypes = [C.c_void_p]
         lib.om_mg_level_size.restype = C.c_int
@@ -129,6 +130,11 @@ class Oracle:
         self.lib.om_residuals_turb(self.h, a)
         a = list(a)
         return {"abs": a[0:2], "max": a[2:4], "rms": a[4:6], "scaled": a[6:8]}
+
+    def turb_production(self) -> np.ndarray:
+        """k-epsilon production from the current gradients, k, epsilon, mu_t."""
+        self.lib.om_turb_production(self.h)
+        return self.get("prod")
 
     def initialize_mdot(self):
         """CalculateInitialmdot from the current velocity fields."""

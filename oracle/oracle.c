@@ -1188,6 +1188,10 @@ double om_simple_iteration(om *m)
   return stop_metric(m);
 }
 
+/* CalculateStrainRateTensor + CalculateTurbulenceProduction on the current
+ * velocity gradients, k, epsilon and mu_t (into "prod"), for the unit tests */
+void om_turb_production(om *m) { om_strain_rate(m); om_production(m); }
+
 void om_residuals_turb(om *m, double out[8])
 {
   for (int q = 0; q < 2; q++) { out[q] = m->rabs[7 + q]; out[2 + q] = m->rmax[7 + q]; out[4 + q] = m->rrms[7 + q]; out[6 + q] = m->rscl[7 + q]; }

@@ -78,6 +78,24 @@ def test_oracle_kepsilon_step():
     assert o.lin_iters(8) >= 1 and o.lin_iters(9) >= 1
 
 
+def test_oracle_inlet_turbulence():
+    """'specifiedil' inlets: k = 1.5 |U|^2 I^2, eps = Cmu^0.75 k^1.5 / L on
+    every inlet face (CalculateTurbulenceAtBoundary.for:20-30)."""
+    import oracle
+    m, c = cs.bfs(12, 6, 4, solver_cont="bicgs", krylov_tol=1e-8, krylov_maxit=200)
+    o = oracle.Oracle(m, c)
+    _setup(o, m, c)
+    o.simple_iteration()
+    sl = _patch_slice(m, "inlet")
+    bu = o.get("bu")[sl]
+    I, L = c.inlet_turbulence["inlet"]
+    k = 1.5 * (bu * bu) * (I * I)
+    cmu = float(np.float32(0.09))
+    cmu75 = np.sqrt(np.sqrt(cmu)) ** 3
+    assert np.allclose(o.get("btke")[sl], k, rtol=1e-15, atol=0)
+    assert np.allclose(o.get("bted")[sl], cmu75 * k ** 1.5 / L, rtol=1e-14, atol=0)
+
+
 def test_oracle_wall_function_law():
     """After an iteration every no-slip wall face obeys the standard
     equilibrium wall function: u+ = y+ below y+ = 11.63, else
@@ -103,6 +121,33 @@ def test_oracle_wall_function_law():
     # momentum pass left mu_t,wall = max(mu_wall - mu, 0) in bmut until
     # CalculateTurbulentViscosity recomputed it; only bounds are checked here
     assert np.all(np.isfinite(bedif[walls]))
+
+
+def test_oracle_production_of_simple_shear():
+    """Uniform shear u = gamma*y: S12 = gamma/2, and the kepsilon shear stress
+    uses mu + mu_t (calculateShearStress), so P = (mu + mu_t) gamma^2 exactly;
+    with LimitTurbulenceProduction P is capped at 10 rho eps."""
+    import oracle
+    m, c = cs.bfs(12, 6, 4)
+    o = oracle.Oracle(m, c)
+    N = m.n_cells
+    gamma = 3.0
+    ug = np.zeros(3 * N)
+    ug[N:2 * N] = gamma
+    o.set("ug", ug)
+    o.set("vg", np.zeros(3 * N))
+    o.set("wg", np.zeros(3 * N))
+    mut = np.linspace(0.001, 0.01, N)
+    o.set("mut", mut)
+    o.set("tke", np.full(N, 0.2))
+    o.set("ted", np.full(N, 1e3))
+    P = o.turb_production()
+    ref = (mut + c.mu) * 2.0 * (0.5 * gamma) * gamma
+    assert np.allclose(P, ref, rtol=1e-15, atol=0)
+    o.set("ted", np.full(N, 1e-3))
+    P = o.turb_production()
+    cap = float(np.float32(10.0)) * c.rho * 1e-3
+    assert np.allclose(P, np.minimum(ref, cap), rtol=1e-15, atol=0)
 
 
 # ------------------------------------------------------------------- GPU
