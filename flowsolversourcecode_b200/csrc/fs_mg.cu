@@ -772,7 +772,8 @@ template <int WF>
 __global__ void k_mg_lhs(int nf, const int32_t *__restrict__ ncf_f, const double *__restrict__ ac_f,
                          const double *__restrict__ anb_f, int nc, int wc, const int32_t *__restrict__ cptr,
                          const int32_t *__restrict__ clist, const int32_t *__restrict__ cmap,
-                         double *__restrict__ ac_c, double *__restrict__ anb_c) {
+                         double *__restrict__ ac_c, double *__restrict__ anb_c,
+                         float *__restrict__ acf_c, float *__restrict__ anbf_c) {
   extern __shared__ double sacc[];
   int P = blockIdx.x * blockDim.x + threadIdx.x;
   const int T = blockDim.x;
@@ -811,6 +812,10 @@ __global__ void k_mg_lhs(int nf, const int32_t *__restrict__ ncf_f, const double
   }
   ac_c[P] = acc;
   for (int k = 0; k < wc; k++) anb_c[(long)k * nc + P] = acc_nb[(long)k * T];
+  if (acf_c) {   // the FP32 copy of the coarse level, when the preconditioner is FP32
+    acf_c[P] = (float)acc;
+    for (int k = 0; k < wc; k++) anbf_c[(long)k * nc + P] = (float)acc_nb[(long)k * T];
+  }
 }
 
 __global__ void k_to_f32(long n, const double *a, float *b) {
@@ -1149,7 +1154,7 @@ static int mg_coarse_matrices(fs_ctx *ctx, int last, bool f32) {
     if (sm > 48 * 1024) { ctx->err = "coarse level too wide for the coarse-matrix kernel"; return FS_E_UNSUPPORTED; }
     const int wf = M->w[q - 1];
 #define FS_LHS_ARGS M->n[q - 1], M->nnb[q - 1], M->ac[q - 1], M->anb[q - 1], M->n[q], M->w[q], M->cptr[q], \
-                    M->clist[q], M->cmap[q], M->ac[q], M->anb[q]
+                    M->clist[q], M->cmap[q], M->ac[q], M->anb[q], f32 ? M->acf[q] : nullptr, f32 ? M->anbf[q] : nullptr
     if (wf <= 8) k_mg_lhs<8><<<fs_grid(M->n[q], T), T, sm, ctx->st>>>(FS_LHS_ARGS);
     else if (wf <= 32) k_mg_lhs<32><<<fs_grid(M->n[q], T), T, sm, ctx->st>>>(FS_LHS_ARGS);
     else k_mg_lhs<0><<<fs_grid(M->n[q], T), T, sm, ctx->st>>>(FS_LHS_ARGS);
@@ -1157,7 +1162,7 @@ static int mg_coarse_matrices(fs_ctx *ctx, int last, bool f32) {
     FS_LAUNCH_CHECK();
   }
   if (f32)
-    for (int q = 0; q <= last; q++) {
+    for (int q = 0; q <= 0; q++) {   // coarse levels got their FP32 copy from k_mg_lhs
       long n = M->n[q], nw = (long)M->w[q] * M->n[q];
       k_to_f32<<<fs_grid(n), FS_BLOCK, 0, ctx->st>>>(n, M->ac[q], M->acf[q]);
       FS_LAUNCH_CHECK();
