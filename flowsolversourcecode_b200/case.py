@@ -137,7 +137,7 @@ class Case:
         c.urf_tke, c.urf_ted, c.urf_tvisc = self.urf_tke, self.urf_ted, self.urf_tvisc
         c.max_visc_ratio, c.limit_production = self.max_visc_ratio, int(self.limit_production)
         c.conv_scheme_tke, c.conv_scheme_ted = L.TVD[self.conv_scheme_tke], L.TVD[self.conv_scheme_ted]
-        c.wall_function = {"standard": 0, "scalable": 1}[self.wall_function]
+        c.wall_function = {"standard": 0, "scalable": 1, "automatic": 2}[self.wall_function]
         return c
 
 
@@ -188,16 +188,20 @@ def bfs(nx: int = 512, ny: int = 96, nz: int = 48, re_h: float = 5000.0, intensi
     Channel 30H x 3H x 2H (H = 1), step wall at x = 0 for y < H, inlet at
     x = 0 for y >= H with u = 1, outlet 'fullydeveloped' at x = 30H, no-slip
     walls elsewhere; rho = 1, mu = 1/Re_H.  Inlet turbulence 'specifiedil'
-    with the given intensity and length scale.  Second-order upwind deferred
-    correction for momentum from iteration 1.  Use :func:`bfs_initial_state`
-    for the initial fields (perturbed inlet profile)."""
+    with the given intensity and length scale.  Momentum wall functions
+    'automatic' (the reference's default type) and the bounded minmod TVD
+    scheme for momentum from iteration 1: with 'standard' wall functions or
+    unbounded second-order upwind the outer iteration settles into a limit
+    cycle instead of converging.  Use :func:`bfs_initial_state` for the
+    initial fields (perturbed inlet profile)."""
     mesh = bfs_mesh(nx, ny, nz)
     patches = {p: ("wall", (0.0, 0.0, 0.0)) for p in BFS_PATCHES}
     patches["inlet"] = ("inlet", (1.0, 0.0, 0.0))
     patches["xmax"] = ("outlet", (0.0, 0.0, 0.0))
-    kw.setdefault("conv_scheme", "sou")
+    kw.setdefault("conv_scheme", "minmod")
     kw.setdefault("niter_start_hr", 1)
     kw.setdefault("turbulence", True)
+    kw.setdefault("wall_function", "automatic")
     case = Case(mu=1.0 / re_h, patches=patches, inlet_turbulence={"inlet": (intensity, length)}, **kw)
     return mesh, case
 

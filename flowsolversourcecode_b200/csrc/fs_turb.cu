@@ -1,5 +1,5 @@
-// fs_turb.cu -- standard k-epsilon with equilibrium 'standard' or 'scalable'
-// momentum wall functions (Turbulence/ of the reference, TurbulenceModel='kepsilon'), and
+// fs_turb.cu -- standard k-epsilon with equilibrium 'standard', 'scalable' or
+// 'automatic' momentum wall functions (Turbulence/ of the reference, TurbulenceModel='kepsilon'), and
 // the 'fullydeveloped' outlet mass-flow adjustment of SolveContinuity.
 //
 // The k and epsilon equations go through one cell-centric gather kernel each
@@ -47,7 +47,7 @@ constexpr double TWOTHIRD = (double)(2.0f / 3.0f);              // Constants1.F9
 struct TurbArgs {
   int N, F, B;
   double rho, mu, urf, bleed, cmu75, tvisc_urf, max_ratio;
-  int scheme, hr_on, limit, first, scalable;
+  int scheme, hr_on, limit, first, wfun;   // wfun: 0 standard, 1 scalable, 2 automatic
   const int32_t *ncf, *slot, *cn, *bown, *btype, *bset;
   const double *gf, *sf, *dcfv, *gdiff, *tf, *vol;
   const double *bsf, *bnf, *bdv, *bgdiff, *btf;
@@ -96,8 +96,9 @@ __global__ void k_wall_distance(TurbArgs a) {
 
 // CalculateEffectiveDiffusionCoefficient('vel?') boundary part
 // (ComputeEffectiveDiffusionCoefficient.for:34-46) and
-// EquilibriumMomentumWallFunctions (WallFunctions.for:1846-1993): 'standard'
-// (:1918-1960) or 'scalable' (:1961-1993, y+ clipped to ctrans + tiny)
+// EquilibriumMomentumWallFunctions (WallFunctions.for:1846-2025): 'standard'
+// (:1918-1960), 'scalable' (:1961-1993, y+ clipped to ctrans + tiny) or
+// 'automatic' (:1994-2025, viscous and log u_tau blended by fourth powers)
 __global__ void k_wall_fn(TurbArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= a.B) return;
@@ -111,7 +112,17 @@ __global__ void k_wall_fn(TurbArgs a) {
   }
   double yp1 = dn * rho * a.utau[b] / mu;
   double yp, up, ut, dd;
-  if (a.scalable) {
+  if (a.wfun == 2) {
+    const double utv = sqrt(mu * wv / (rho * dn));
+    const double utl = wv / (log(a.yplus[b]) / KE_KAPPA + KE_CC);
+    const double v2 = utv * utv, l2 = utl * utl;
+    ut = pow(v2 * v2 + l2 * l2, (double)0.25f);
+    up = wv / fmax(ut, TINY);
+    yp = rho * ut * dn / mu;
+    const double y2 = yp * yp;
+    const double factor = (double)0.01f * (y2 * y2) / (1. + 5. * yp) + TINY;
+    dd = 1. * exp(-factor) + (1. / (KE_KAPPA * yp)) * exp(-1. / factor);
+  } else if (a.wfun == 1) {
     yp = fmax(yp1, KE_CTRANS + TINY);
     dd = 1. / (KE_KAPPA * yp);
     up = log(yp) / KE_KAPPA + KE_CC;
@@ -154,8 +165,9 @@ __global__ void k_ted_wall(TurbArgs a) {
   if (i >= a.N) return;
   int b = a.itau[i];
   if (b < 0) return;
+  if (a.wfun == 2) return;   // 'automatic': no branch sets the wall-cell epsilon
   double dn = a.wdist[i], k = fmax(a.tke[i], 0.);
-  if (a.scalable) {
+  if (a.wfun == 1) {
     dn = a.yplus[b] * a.mu / (a.rho * a.utau[b]);
     a.ted[i] = a.cmu75 * pow(k, 1.5) / (KE_KAPPA * dn);
   } else if (a.yplus[b] < KE_CTRANS) a.ted[i] = 2. * a.mu * k / (a.rho * (dn * dn));
@@ -404,7 +416,7 @@ TurbArgs turb_args(fs_ctx *ctx) {
   a.rho = c.rho; a.mu = c.mu; a.bleed = c.bleed;
   a.cmu75 = sqrt(sqrt(KE_CMU)); a.cmu75 = a.cmu75 * a.cmu75 * a.cmu75;
   a.tvisc_urf = c.urf_tvisc; a.max_ratio = c.max_visc_ratio; a.limit = c.limit_production;
-  a.scalable = c.wall_function == 1;
+  a.wfun = c.wall_function;
   a.ncf = ctx->ncf; a.slot = ctx->slot; a.cn = ctx->cn; a.bown = ctx->bown; a.btype = ctx->btype; a.bset = ctx->d_bset;
   a.gf = ctx->gf; a.sf = ctx->sf; a.dcfv = ctx->dcfv; a.gdiff = ctx->gdiff; a.tf = ctx->tf; a.vol = ctx->vol;
   a.bsf = ctx->bsf; a.bnf = ctx->bnf; a.bdv = ctx->bdv; a.bgdiff = ctx->bgdiff; a.btf = ctx->btf;

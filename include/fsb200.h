@@ -157,7 +157,7 @@ typedef struct fs_case {
   /* outlets 'fullydeveloped': MassFlowFraction per patch (AdjustFlowAtOuletBoundary.for:38-55) */
   double mass_flow_fraction[FS_MAX_PATCHES];
   /* k-epsilon (TurbulenceModel='kepsilon', WallTreatment='wallfunctions',
-   * WallFunctionKind='equilibrium', MomentumWallFunctionType 'standard' or 'scalable';
+   * WallFunctionKind='equilibrium', MomentumWallFunctionType 'standard', 'scalable' or 'automatic';
    * SolveSelectedTurbulenceModelEquations.for:21-30).  0 = laminar. */
   int    turbulence;
   int    solver_turb;            /* ASSolverTKE = ASSolverTED */
@@ -170,7 +170,7 @@ typedef struct fs_case {
   int    conv_scheme_tke, conv_scheme_ted; /* ConvectionSchemeTKE/TED (fs_tvd; HR framework tvd) */
   double inlet_intensity[FS_MAX_PATCHES];  /* inletTurbulenceIntensity, inletTypeT='specifiedil' */
   double inlet_length[FS_MAX_PATCHES];     /* inletTurbulenceLengthScale */
-  int    wall_function;          /* MomentumWallFunctionType: 0 'standard', 1 'scalable' */
+  int    wall_function;          /* MomentumWallFunctionType: 0 'standard', 1 'scalable', 2 'automatic' */
 } fs_case;
 
 /* Mesh in polyMesh form (0-based), the input Readit parses
