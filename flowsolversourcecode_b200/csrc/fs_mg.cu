@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   // start from the initial guess scaled by the c that minimises |b - c A x0|
   // (c = (A x0 . b) / (A x0 . A x0), so |r0| <= |b|), or from zero.  A guess
   // with c not finite or zero falls back to the zero start (same decision in
-  // every CTA: the sums are grid-deterministic).  Whether guesses pay is judged
+  // every CTA: the sums are grid-deterministic).  Whether guesses pay is decided
   // on iteration counts by the host policy (fs_nn.cu).
   double l0 = 0., l1 = 0., l2 = 0.;
   for (long i = t0; i < N; i += 2 * nt) {

@@ -317,7 +317,7 @@ def test_multigrid_solvers_momentum_system(solver, tol):
 
 @pytest.mark.parametrize("solver", ["amg_bicgs", "amg32_bicgs", "amg"])
 def test_multigrid_pressure_correction_residual(solver):
-    # the closed-cavity p' system is singular: judge the residual, and the
+    # the closed-cavity p' system is singular: check the residual, and the
     # solution up to the constant null vector
     mesh, case = cs.cavity(16, nz=14, jitter=0.2, seed=3, krylov_tol=1e-9, krylov_maxit=200, mg_max_cycles=200)
     s, o = _pair(mesh, case)
