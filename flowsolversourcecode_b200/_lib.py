@@ -38,7 +38,7 @@ SIMPLE, SIMPLEC = 0, 1
 FIELDS = ["u", "v", "w", "p", "pc", "mdot", "bu", "bv", "bw", "bp", "bpc", "bmdot", "ac", "bc", "anb",
           "du1", "dv1", "dw1", "du2", "dv2", "dw2", "ugrad", "vgrad", "wgrad", "pgrad", "pcgrad",
           "volume", "xc", "gfactor", "sf", "gdiff", "ft", "bsf", "dphi",
-          "tke", "ted", "mut", "btke", "bted", "bmut"]
+          "tke", "ted", "mut", "btke", "bted", "bmut", "kx", "utau", "yplus"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
 

@@ -123,7 +123,9 @@ static double *field_ptr(fs_ctx *c, int f, size_t *n) {
   case FS_F_FT: *n = 3 * F; return c->tf;
   case FS_F_BSF: *n = 3 * B; return c->bsf;
   case FS_F_DPHI: *n = N; return c->dphi;
+  case FS_F_KX: *n = N; return c->kx;
   case FS_F_TKE: case FS_F_TED: case FS_F_MUT: case FS_F_BTKE: case FS_F_BTED: case FS_F_BMUT:
+  case FS_F_UTAU: case FS_F_YPLUS:
     return fs_turb_field(c, f, n);
   }
   *n = 0;

@@ -484,6 +484,8 @@ double *fs_turb_field(fs_ctx *ctx, int field, size_t *n) {
   case FS_F_BTKE: *n = ctx->B; return T->btke;
   case FS_F_BTED: *n = ctx->B; return T->bted;
   case FS_F_BMUT: *n = ctx->B; return T->bmut;
+  case FS_F_UTAU: *n = ctx->B; return T->utau;
+  case FS_F_YPLUS: *n = ctx->B; return T->yplus;
   }
   return nullptr;
 }

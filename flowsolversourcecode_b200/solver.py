@@ -162,7 +162,7 @@ class Solver:
         N, F, B, W = self.N, self.F, self.B, self.W
         sizes = {"mdot": F, "gfactor": F, "gdiff": F, "sf": 3 * F, "ft": 3 * F, "anb": W * N,
                  "bu": B, "bv": B, "bw": B, "bp": B, "bpc": B, "bmdot": B, "bsf": 3 * B, "xc": 3 * N,
-                 "btke": B, "bted": B, "bmut": B}
+                 "btke": B, "bted": B, "bmut": B, "utau": B, "yplus": B}
         if name.endswith("grad"):
             return 3 * N
         return sizes.get(name, N)
@@ -175,6 +175,31 @@ class Solver:
     def set(self, name: str, arr) -> None:
         a = np.ascontiguousarray(arr, np.float64)
         self._chk(self.lib.fs_set_field(self.ctx, L.FIELD_ID[name], L.dptr(a), a.shape[0]), f"set {name}")
+
+    # fields that carry information from one outer iteration to the next
+    RESTART_FIELDS = ("u", "v", "w", "p", "mdot", "bu", "bv", "bw", "bp", "bmdot", "kx")
+    RESTART_TURB = ("tke", "ted", "mut", "btke", "bted", "bmut", "utau", "yplus")
+
+    def write_solution(self, path: str) -> None:
+        """writeSolution (WriteAndReadSolution/WriteSolutionToContinue.for:4):
+        every array an outer iteration reads from the previous one -- the
+        cell, face and boundary fields, BICGSTAB_OMP's persistent vector, the
+        k-epsilon fields and wall-function state -- and the iteration count,
+        to a .npz file.  Gradients, D, u* and the matrices are rebuilt by the
+        next iteration before they are read, so they are not stored."""
+        names = self.RESTART_FIELDS + (self.RESTART_TURB if self.case.turbulence else ())
+        data = {k: self.get(k) for k in names}
+        data["nIter"] = np.array([self.nIter], np.int64)
+        np.savez(path, **data)
+
+    def read_solution(self, path: str) -> None:
+        """readSolution: restore a state written by write_solution, so the
+        next outer iterations repeat those of the run that wrote it."""
+        with np.load(path) as f:
+            for k in f.files:
+                if k != "nIter":
+                    self.set(k, f[k])
+            self.set_iteration(int(f["nIter"][0]))
 
     def state(self) -> dict:
         return {k: self.get(k) for k in ("u", "v", "w", "p", "mdot", "bu", "bv", "bw", "bp", "bmdot")}

@@ -70,6 +70,8 @@ enum fs_field {
   FS_F_DPHI,                                         /* N: last linear solution */
   FS_F_TKE, FS_F_TED, FS_F_MUT,                      /* N: k, epsilon, turbulent viscosity */
   FS_F_BTKE, FS_F_BTED, FS_F_BMUT,                   /* B */
+  FS_F_KX,                                           /* N: BICGSTAB_OMP's persistent solution vector */
+  FS_F_UTAU, FS_F_YPLUS,                             /* B: wall-function state (uTau, yplus) */
   FS_F_COUNT
 };
 
