@@ -705,6 +705,9 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     for (long i = t0; i < N; i += nt) l0 += a.r0[i] * a.r[i];
     double rho1;
     S.sum2(l0, 0., rho1, dum);
+    // breakdown (r0 . r vanished: r at round-off): keep x.  Every CTA holds the
+    // same sums, so every CTA takes the same branch.
+    if (!(rho1 != 0.) || !isfinite(rho1)) break;
     double beta = (rho1 / rho) * (alpha / omega);
     rho = rho1;
     for (long i = t0; i < N; i += nt) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
@@ -721,6 +724,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     }
     double rv;
     S.sum2(l0, 0., rv, dum);
+    if (!(rv != 0.) || !isfinite(rho / rv)) break;
     alpha = rho / rv;
     l0 = 0.;
     for (long i = t0; i < N; i += nt) { double si = a.r[i] - alpha * a.v[i]; a.s[i] = si; l0 += si * si; }
@@ -743,6 +747,12 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     }
     double ts, tt;
     S.sum2(l0, l1, ts, tt);
+    if (!(tt > 0.) || !(ts != 0.) || !isfinite(ts / tt)) {
+      // t = A z vanished or is orthogonal to s: take the half step and stop
+      for (long i = t0; i < N; i += nt) a.x[i] = a.x[i] + alpha * a.y[i];
+      resn = sqrt(ss);
+      break;
+    }
     omega = ts / tt;
     l0 = 0.;
     for (long i = t0; i < N; i += nt) {

@@ -210,3 +210,35 @@ def test_kepsilon_step_outlet_balance_and_bounds():
     u = g.get("u").reshape(8, 12, 48)
     assert u[:, :4, 1:12].min() < 0
     g.close()
+
+
+@pytest.mark.gpu
+def test_kepsilon_step_converged_fields_match_oracle():
+    """The default GPU path (multicolour SOR for momentum, k and epsilon, FP64
+    AMG-BiCGSTAB for p') and the sequential oracle (SOR everywhere, the
+    reference's default continuity solver) converge the k-epsilon step to the
+    same fields: run both to the stop metric 1e-9 and compare."""
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    mo, co = cs.bfs(24, 9, 6, solver_cont="sor", rrf_cont=1e-3, itmax_cont=300)
+    o = oracle.Oracle(mo, co)
+    _setup(o, mo, co)
+    for it in range(8000):
+        if o.simple_iteration() < 1e-9:
+            break
+    assert it < 7999
+    mg, cg = cs.bfs(24, 9, 6, solver_cont="amg_bicgs", krylov_tol=1e-10, krylov_maxit=200)
+    g = Solver(mg, cg)
+    _setup(g, mg, cg)
+    for it in range(8000):
+        if g.simple_iteration()["source"] < 1e-9:
+            break
+    assert it < 7999
+    for k in ("u", "v", "w", "tke", "ted", "mut"):
+        x, ref = g.get(k), o.get(k)
+        err = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+        assert err <= 1e-6, (k, err)
+    # pressure: same field up to the level fixed at the reference cell
+    dp = (g.get("p") - g.get("p")[0]) - (o.get("p") - o.get("p")[0])
+    assert np.linalg.norm(dp) <= 1e-6 * np.linalg.norm(o.get("p") - o.get("p")[0])
+    g.close()
