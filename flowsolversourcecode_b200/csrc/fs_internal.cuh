@@ -192,6 +192,7 @@ int fs_turb_create(fs_ctx *ctx);
 void fs_turb_free(fs_ctx *ctx);
 double *fs_turb_field(fs_ctx *ctx, int field, size_t *n);
 void fs_turb_momentum_ptrs(fs_ctx *ctx, const double **mut, const double **bedif, const double **drk);
+void fs_turb_rhok_ptrs(fs_ctx *ctx, const double **rhok, const double **drk);
 int fs_turb_wall_functions(fs_ctx *ctx);
 int fs_turb_rhok_gradient(fs_ctx *ctx);
 int fs_turb_effects(fs_ctx *ctx);

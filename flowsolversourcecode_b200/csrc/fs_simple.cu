@@ -416,6 +416,7 @@ struct ContArgs {
   const double *du1, *dv1, *dw1, *du2, *dv2, *dw2;
   double *mdot, *pcoef, *bmdot;
   const double *bu, *bv, *bw, *bsf;
+  const double *rhok, *drk;   // k-epsilon: 2/3 rho k and its gradient (3N), nullptr when laminar
   double *ac, *anb, *bc;
   double *red; int nblk;
 };
@@ -442,6 +443,7 @@ __device__ __forceinline__ double geo_diff(int msd, double du, double dv, double
 
 // Rhie-Chow mdot (AssembleMdotUsingRhieChow.for:554-759) and the p' face
 // coefficient rho*geoDiff(D2) (AssemblePressureCorrectionFluxes.for:85-153)
+template <bool TURB>
 __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mdot(ContArgs a) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= a.F) return;
@@ -469,6 +471,18 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mdot(ContArgs a) {
   double pbx = g * gox + g1 * gnx, pby = g * goy + g1 * gny, pbz = g * goz + g1 * gnz;  // PressGradBar ('average')
   fvl = fvl - rhof * (pfx * tx + pfy * ty + pfz * tz);
   fvl = fvl + rhof * (pbx * (du * sx) + pby * (dv * sy) + pbz * (dw * sz));
+  if (TURB) {
+    // k-epsilon: the 2/3 rho k gradient like the pressure (AssembleMdotUsingRhieChow.for:296-305, 627-634)
+    const double ki = a.rhok[i], kj = a.rhok[j];
+    const double kox = a.drk[i], koy = a.drk[N + i], koz = a.drk[N2 + i];
+    const double knx = a.drk[j], kny = a.drk[N + j], knz = a.drk[N2 + j];
+    double rfx, rfy, rfz;
+    face_grad(FS_GI_AVERAGECORRECTED, g, a.mdot[k], ki, kj, cf, ex, ey, ez, kox, koy, koz, knx, kny, knz, rfx, rfy, rfz);
+    const double rbx = g * kox + g1 * knx, rby = g * koy + g1 * kny, rbz = g * koz + g1 * knz;
+    fvl = fvl - rhof * (rfx * tx + rfy * ty + rfz * tz);
+    fvl = fvl + rhof * (rbx * (du * sx) + rby * (dv * sy) + rbz * (dw * sz));
+    fvl = fvl + fcl * ki + ffl * kj;
+  }
   double mold = a.mdot[k];
   if (a.relax) {
     double ms = rhof * ((g * a.us[i] + g1 * a.us[j]) * sx + (g * a.vs[i] + g1 * a.vs[j]) * sy + (g * a.ws[i] + g1 * a.ws[j]) * sz);
@@ -799,6 +813,7 @@ static ContArgs cont_args(fs_ctx *ctx) {
   a.du1 = ctx->du1; a.dv1 = ctx->dv1; a.dw1 = ctx->dw1; a.du2 = ctx->du2; a.dv2 = ctx->dv2; a.dw2 = ctx->dw2;
   a.mdot = ctx->mdot; a.pcoef = ctx->pcoef; a.bmdot = ctx->bmdot;
   a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bsf = ctx->bsf;
+  fs_turb_rhok_ptrs(ctx, &a.rhok, &a.drk);
   a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc; a.red = ctx->red; a.nblk = fs_grid(ctx->N);
   return a;
 }
@@ -810,7 +825,11 @@ int fs_continuity_assemble(fs_ctx *ctx) {
   int rc = fs_flow_in_out(ctx);                                        // FlowIn, FlowOut, AdjustFlow
   if (rc) return rc;
   ContArgs a = cont_args(ctx);
-  if (F) { k_mdot<<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  if (F) {
+    if (a.rhok) k_mdot<true><<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a);
+    else k_mdot<false><<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a);
+    FS_LAUNCH_CHECK();
+  }
   if (B) { k_bmdot_inlet<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   k_pc_assemble<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();

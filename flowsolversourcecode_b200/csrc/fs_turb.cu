@@ -498,6 +498,13 @@ void fs_turb_momentum_ptrs(fs_ctx *ctx, const double **mut, const double **bedif
   *drk = T ? T->drk : nullptr;
 }
 
+// 2/3 rho k and its gradient for the Rhie-Chow interpolation (nullptr when laminar)
+void fs_turb_rhok_ptrs(fs_ctx *ctx, const double **rhok, const double **drk) {
+  fs_turb *T = ctx->turb;
+  *rhok = T ? T->rhok : nullptr;
+  *drk = T ? T->drk : nullptr;
+}
+
 // CalculateEffectiveDiffusionCoefficient('vel?') with the momentum wall
 // functions, before the boundary terms of each momentum component
 int fs_turb_wall_functions(fs_ctx *ctx) {

@@ -780,6 +780,15 @@ void om_assemble_continuity(om *m)
   om_interp_grad(m, FS_GI_AVERAGE, m->p, m->pg, pgbar);
   const double *pbx = pgbar, *pby = pgbar + F, *pbz = pgbar + 2 * (long)F;
   const double *pfx = m->pgf, *pfy = m->pgf + F, *pfz = m->pgf + 2 * (long)F;
+  /* k-epsilon: the 2/3 rho k gradient enters like the pressure
+   * (AssembleMdotUsingRhieChow.for:296-305, 627-634): 'average' and
+   * 'averagecorrected' face gradients of rhok from MinusTwoThirdsRhoK */
+  double *rkbar = NULL, *rkf = NULL;
+  if (c->turbulence) {
+    rkbar = dz_(3 * (long)F); rkf = dz_(3 * (long)F);
+    om_interp_grad(m, FS_GI_AVERAGE, m->rhok, m->drk, rkbar);
+    om_interp_grad(m, FS_GI_AVERAGECORRECTED, m->rhok, m->drk, rkf);
+  }
   for (int k = 0; k < F; k++) {
     int i = m->if_own[k], j = m->if_nbr[k];
     double rhof = c->rho, sx = m->sx[k], sy = m->sy[k], sz = m->sz[k];
@@ -791,13 +800,18 @@ void om_assemble_continuity(om *m)
     double fcl = rhof * gd, ffl = -rhof * gd;
     fvl = fvl - rhof * (pfx[k] * tx + pfy[k] * ty + pfz[k] * tz);
     fvl = fvl + rhof * (pbx[k] * (du * sx) + pby[k] * (dv * sy) + pbz[k] * (dw * sz));
+    if (c->turbulence) {
+      fvl = fvl - rhof * (rkf[k] * tx + rkf[F + k] * ty + rkf[2L * F + k] * tz);
+      fvl = fvl + rhof * (rkbar[k] * (du * sx) + rkbar[F + k] * (dv * sy) + rkbar[2L * F + k] * (dw * sz));
+      fvl = fvl + fcl * m->rhok[i] + ffl * m->rhok[j];
+    }
     if (c->relax_momentum) {
       double ms = rhof * (avgf(m, k, m->us) * sx + avgf(m, k, m->vs) * sy + avgf(m, k, m->ws) * sz);
       fvl = fvl + (1. - c->urf_momentum) * (m->mdot[k] - ms);
     }
     m->mdot[k] = fcl * m->p[i] + ffl * m->p[j] + fvl;
   }
-  free(pgbar);
+  free(pgbar); free(rkbar); free(rkf);
   /* inlet specified velocity Bmdot (AssembleMdotUsingRhieChow.for:2054-2075) */
   for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_VEL)
     m->bmdot[b] = c->rho * (m->bu[b] * m->bsx[b] + m->bv[b] * m->bsy[b] + m->bw[b] * m->bsz[b]);
