@@ -164,12 +164,13 @@ __global__ void k_bgrad(BGradJob J, int N, int B, const int32_t *__restrict__ bo
     double ox = gx, oy = gy, oz = gz;
     int var = J.var[q];
     bool vel = (var == FS_VAR_U || var == FS_VAR_V || var == FS_VAR_W);
-    if ((vel && t == FS_BC_OUTLET_FD) || (var == FS_VAR_P && t == FS_BC_SYMMETRY)) {
+    bool prs = (var == FS_VAR_P || var == FS_VAR_RHOK);   // 'press' and 'rhok' (CalculateGradients.for:266-271)
+    if ((vel && t == FS_BC_OUTLET_FD) || (prs && t == FS_BC_SYMMETRY)) {
       // CorrectGradientAtOulet / CorrectPressureGradientAtSymmetryBoundary, nz=BFaceAreanz(i,i)
       ox = gx * (1. - nx * nx) - gy * nx * ny - gz * nx * nzi;
       oy = gy * (1. - ny * ny) - gx * ny * nx - gz * ny * nzi;
       oz = gz * (1. - nzi * nzi) - gx * nzi * nx - gy * nzi * ny;
-    } else if (var == FS_VAR_P && (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP)) {
+    } else if (prs && (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP)) {
       // CorrectPresureGradientAtWalls (CorrectGradients.for:34-56)
       ox = (1 - nx * nx) * gx - nx * ny * gy - nx * nz * gz;
       oy = (1 - ny * ny) * gy - ny * nx * gx - ny * nz * gz;

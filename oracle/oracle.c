@@ -398,7 +398,7 @@ void om_gradient(om *m, int var, int method, int niter, const double *phi, const
       tproj(m->bnx[b], m->bny[b], nz_ii(m, s), gx[k], gy[k], gz[k], &bgx[b], &bgy[b], &bgz[b], 0);
     }
   }
-  if (var == FS_VAR_P) {
+  if (var == FS_VAR_P || var == FS_VAR_RHOK) {   /* 'press' and 'rhok' (CalculateGradients.for:266-271) */
     /* CorrectPressureGradientAtSymmetryBoundary (CorrectGradients.for:244-288) */
     for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_SYMMETRY) {
       int k = m->bf_own[b], s = m->bf_set[b];
