@@ -26,7 +26,7 @@ FS_NN_NPARAM = 33665
 VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
 VAR_TKE, VAR_TED, VAR_RHOK = 8, 9, 10
 # boundary types
-BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD = 0, 1, 2, 3, 4
+BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD, BC_OUTLET_SP = 0, 1, 2, 3, 4, 5
 # gradient interpolation
 GI_AVERAGE, GI_UPWIND, GI_DOWNWIND, GI_AVERAGECORRECTED = 0, 1, 2, 3
 HR_NONE, HR_TVD = 0, 1
@@ -71,6 +71,7 @@ class FsCase(C.Structure):
         ("conv_scheme_tke", C.c_int), ("conv_scheme_ted", C.c_int),
         ("inlet_intensity", C.c_double * FS_MAX_PATCHES), ("inlet_length", C.c_double * FS_MAX_PATCHES),
         ("wall_function", C.c_int),
+        ("patch_pressure", C.c_double * FS_MAX_PATCHES),
     ]
 
 

@@ -70,7 +70,7 @@ class Case:
     mg_rrf: float = 0.1
     # multi-RHS momentum (X, Y, Z solved together; no reference counterpart)
     batched_momentum: bool = False
-    # patches: name -> (type, (u,v,w))
+    # patches: name -> (type, (u,v,w)); type "pressure_outlet" takes (type, static pressure)
     patches: dict = field(default_factory=dict)
     # 'fullydeveloped' outlets: patch name -> MassFlowFraction (default 1)
     mass_flow_fraction: dict = field(default_factory=dict)
@@ -121,12 +121,15 @@ class Case:
         c.batched_momentum = int(self.batched_momentum)
         c.n_patches = len(mesh.patch_names)
         bct = {"wall": L.BC_WALL_NOSLIP, "slip": L.BC_WALL_SLIP, "symmetry": L.BC_SYMMETRY,
-               "inlet": L.BC_INLET_VEL, "outlet": L.BC_OUTLET_FD}
+               "inlet": L.BC_INLET_VEL, "outlet": L.BC_OUTLET_FD, "pressure_outlet": L.BC_OUTLET_SP}
         for s, name in enumerate(mesh.patch_names):
             t, vel = self.patches.get(name, ("wall", (0.0, 0.0, 0.0)))
             c.patch_type[s] = bct[t]
-            for q in range(3):
-                c.patch_vel[s][q] = float(vel[q])
+            if t == "pressure_outlet":   # (type, static pressure)
+                c.patch_pressure[s] = float(vel)
+            else:
+                for q in range(3):
+                    c.patch_vel[s][q] = float(vel[q])
             c.mass_flow_fraction[s] = float(self.mass_flow_fraction.get(name, 1.0))
             it, il = self.inlet_turbulence.get(name, (0.0, 1.0))
             c.inlet_intensity[s], c.inlet_length[s] = float(it), float(il)
@@ -211,8 +214,8 @@ def bfs_initial_state(mesh: PolyMesh, case: Case, seed: int = 0, perturbation: f
     inlet faces u = 1 + perturbation * U(-1, 1) (splitmix64 from `seed`, one
     draw per inlet face in boundary order), k and epsilon uniform at the
     inlet-turbulence values of a unit velocity (k = 1.5 I^2, eps =
-    Cmu^0.75 k^1.5 / L) and mu_t = Cmu rho k^2 / eps, on cells and boundary faces.
-    Apply with ``obj.set(name, value)`` for every item, then
+    Cmu^0.75 k^1.5 / L) and mu_t = Cmu rho k^2 / eps, on cells and boundary faces
+    (turbulent cases only).  Apply with ``obj.set(name, value)`` for every item, then
     ``obj.initialize_mdot()``."""
     N = mesh.n_cells
     B = mesh.n_faces - mesh.n_internal
@@ -231,6 +234,8 @@ def bfs_initial_state(mesh: PolyMesh, case: Case, seed: int = 0, perturbation: f
     cmu75 = np.sqrt(np.sqrt(cmu)) ** 3
     e0 = cmu75 * k0 ** 1.5 / ln
     mut0 = cmu * case.rho * k0 * k0 / e0
-    return {"u": np.ones(N), "bu": bu,
-            "tke": np.full(N, k0), "ted": np.full(N, e0), "mut": np.full(N, mut0),
-            "btke": np.full(B, k0), "bted": np.full(B, e0), "bmut": np.full(B, mut0)}
+    state = {"u": np.ones(N), "bu": bu}
+    if case.turbulence:
+        state.update({"tke": np.full(N, k0), "ted": np.full(N, e0), "mut": np.full(N, mut0),
+                      "btke": np.full(B, k0), "bted": np.full(B, e0), "bmut": np.full(B, mut0)})
+    return state

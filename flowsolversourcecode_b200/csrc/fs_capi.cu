@@ -145,7 +145,7 @@ static void free_all(fs_ctx *c) {
                   c->u, c->v, c->w, c->p, c->pc, c->mdot, c->bu, c->bv, c->bw, c->bp, c->bpc, c->bmdot,
                   c->ug, c->vg, c->wg, c->pg, c->pcg, c->bug, c->bvg, c->bwg, c->bpg, c->bpcg, c->gtmp,
                   c->du1, c->dv1, c->dw1, c->du2, c->dv2, c->dw2, c->us, c->vs, c->ws,
-                  c->ac, c->anb, c->bc, c->dphi, c->ac_int, c->bc_int, c->effdiv, c->pcoef,
+                  c->ac, c->anb, c->bc, c->dphi, c->ac_int, c->bc_int, c->effdiv, c->pcoef, c->bpcoef,
                   c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky, c->sysx,
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
                   c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP,
@@ -173,7 +173,9 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (auto &e : ctx->tev) cudaEventCreate(&e);
   for (auto &pr : ctx->sev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
   for (auto &pr : ctx->kev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
-  if (ctx->cfg.set_reference_pressure < 0) ctx->cfg.set_reference_pressure = 0;  // no pressure-specified patch types
+  for (int s = 0; s < ctx->cfg.n_patches; s++) ctx->has_sp |= ctx->cfg.patch_type[s] == FS_BC_OUTLET_SP;
+  // SetReferencePressure (ReferenceAndSetPressureRoutines.for:4-50): a pressure-specified patch fixes the level
+  if (ctx->cfg.set_reference_pressure < 0) ctx->cfg.set_reference_pressure = ctx->has_sp ? 1 : 0;
   if ((rc = fs_geometry_build(ctx, mesh))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
   const size_t N = ctx->N, F = ctx->F, B = ctx->B, W = ctx->W;
   if (ctx->cfg.ref_pressure_cell >= (int)N) return fail(FS_E_ARG);
@@ -193,7 +195,8 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (auto p : cell3) if ((rc = alloc0(ctx, p, 3 * N))) return fail(rc);
   if ((rc = alloc0(ctx, &ctx->gtmp, 12 * N))) return fail(rc);
   if ((rc = alloc0(ctx, &ctx->anb, W * N))) return fail(rc);
-  if ((rc = alloc0(ctx, &ctx->mdot, F)) || (rc = alloc0(ctx, &ctx->pcoef, F))) return fail(rc);
+  if ((rc = alloc0(ctx, &ctx->mdot, F)) || (rc = alloc0(ctx, &ctx->pcoef, F)) || (rc = alloc0(ctx, &ctx->bpcoef, B)))
+    return fail(rc);
   double **bnd[] = {&ctx->bu, &ctx->bv, &ctx->bw, &ctx->bp, &ctx->bpc, &ctx->bmdot};
   for (auto p : bnd) if ((rc = alloc0(ctx, p, B))) return fail(rc);
   double **bnd3[] = {&ctx->bug, &ctx->bvg, &ctx->bwg, &ctx->bpg, &ctx->bpcg};
@@ -219,7 +222,13 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
       hb[b] = ctx->cfg.patch_vel[s][0]; hb[B + b] = ctx->cfg.patch_vel[s][1]; hb[2 * B + b] = ctx->cfg.patch_vel[s][2];
     }
   }
+  std::vector<double> hp(B, 0.);   // static pressure of 'specifiedstaticpressure' outlets
+  for (size_t b = 0; b < B; b++) {
+    int s = ctx->h_bset[b];
+    if (ctx->cfg.patch_type[s] == FS_BC_OUTLET_SP) hp[b] = ctx->cfg.patch_pressure[s];
+  }
   if (B) {
+    cudaMemcpyAsync(ctx->bp, hp.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
     cudaMemcpyAsync(ctx->bu, hb.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
     cudaMemcpyAsync(ctx->bv, hb.data() + B, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
     cudaMemcpyAsync(ctx->bw, hb.data() + 2 * B, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);

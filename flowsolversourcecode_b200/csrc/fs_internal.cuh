@@ -81,6 +81,8 @@ struct fs_ctx {
   double *ac = nullptr, *anb = nullptr, *bc = nullptr, *dphi = nullptr;
   double *ac_int = nullptr, *bc_int = nullptr, *effdiv = nullptr;  // bc_int: 3N
   double *pcoef = nullptr;                                         // F: p' face coefficient
+  double *bpcoef = nullptr;                                        // B: p' coefficient of pressure outlets
+  bool has_sp = false;                                             // a 'specifiedstaticpressure' outlet exists
   // krylov work (device)
   double *kx = nullptr, *kr = nullptr, *kr0 = nullptr, *kp = nullptr, *kv = nullptr, *ks = nullptr, *kt = nullptr;
   double *kz = nullptr, *ky = nullptr;   // preconditioned vectors (AMG-BiCGSTAB)
@@ -193,6 +195,7 @@ void fs_turb_free(fs_ctx *ctx);
 double *fs_turb_field(fs_ctx *ctx, int field, size_t *n);
 void fs_turb_momentum_ptrs(fs_ctx *ctx, const double **mut, const double **bedif, const double **drk);
 void fs_turb_rhok_ptrs(fs_ctx *ctx, const double **rhok, const double **drk);
+void fs_turb_brhok_ptrs(fs_ctx *ctx, const double **brhok, const double **bdrk);
 int fs_turb_wall_functions(fs_ctx *ctx);
 int fs_turb_rhok_gradient(fs_ctx *ctx);
 int fs_turb_effects(fs_ctx *ctx);

@@ -165,7 +165,7 @@ __global__ void k_bgrad(BGradJob J, int N, int B, const int32_t *__restrict__ bo
     int var = J.var[q];
     bool vel = (var == FS_VAR_U || var == FS_VAR_V || var == FS_VAR_W);
     bool prs = (var == FS_VAR_P || var == FS_VAR_RHOK);   // 'press' and 'rhok' (CalculateGradients.for:266-271)
-    if ((vel && t == FS_BC_OUTLET_FD) || (prs && t == FS_BC_SYMMETRY)) {
+    if ((vel && (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP)) || (prs && t == FS_BC_SYMMETRY)) {
       // CorrectGradientAtOulet / CorrectPressureGradientAtSymmetryBoundary, nz=BFaceAreanz(i,i)
       ox = gx * (1. - nx * nx) - gy * nx * ny - gz * nx * nzi;
       oy = gy * (1. - ny * ny) - gx * ny * nx - gz * ny * nzi;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
         double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
         fcf = fcf + fcl;
         tf = tf + (fcl * phi + ffl * bp);
-      } else if (t == FS_BC_OUTLET_FD) {
+      } else if (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {
         double bm = a.bmdot[b];
         double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
         double fvl = bm * (bfg[b] * a.bdv[b] + bfg[B + b] * a.bdv[B + b] + bfg[B2 + b] * a.bdv[B2 + b]);
@@ -418,6 +418,9 @@ struct ContArgs {
   double *mdot, *pcoef, *bmdot;
   const double *bu, *bv, *bw, *bsf;
   const double *rhok, *drk;   // k-epsilon: 2/3 rho k and its gradient (3N), nullptr when laminar
+  // pressure outlets
+  double *bpcoef, *bu_w, *bv_w, *bw_w;
+  const double *bug, *bvg, *bwg, *bdv, *bpg, *bp, *brhok, *bdrk;
   double *ac, *anb, *bc;
   double *red; int nblk;
 };
@@ -507,6 +510,43 @@ __global__ void k_bmdot_inlet(ContArgs a) {
   a.bmdot[b] = a.rho * (a.bu[b] * a.bsf[b] + a.bv[b] * a.bsf[B + b] + a.bw[b] * a.bsf[2L * B + b]);
 }
 
+// 'specifiedstaticpressure' outlets: boundary velocity, Rhie-Chow Bmdot
+// (AssembleMdotUsingRhieChow.for:1441-1598) and the p' coefficient rho geoDiff(D2)
+// (AssemblePressureCorrectionFluxes.for:244-313)
+__global__ void k_bmdot_sp(ContArgs a) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.B || a.btype[b] != FS_BC_OUTLET_SP) return;
+  const int N = a.N, B = a.B;
+  const long N2 = 2L * N, B2 = 2L * B;
+  const int i1 = a.bown[b];
+  const double rhof = a.rho, sx = a.bsf[b], sy = a.bsf[B + b], sz = a.bsf[B2 + b];
+  const double dx = a.bdv[b], dy = a.bdv[B + b], dz = a.bdv[B2 + b];
+  a.bu_w[b] = a.u[i1] + (a.bug[b] * dx + a.bug[B + b] * dy + a.bug[B2 + b] * dz);
+  a.bv_w[b] = a.v[i1] + (a.bvg[b] * dx + a.bvg[B + b] * dy + a.bvg[B2 + b] * dz);
+  a.bw_w[b] = a.w[i1] + (a.bwg[b] * dx + a.bwg[B + b] * dy + a.bwg[B2 + b] * dz);
+  const double cf = sqrt(dx * dx + dy * dy + dz * dz);
+  const double ex = dx / cf, ey = dy / cf, ez = dz / cf;
+  double fvl = rhof * (a.u[i1] * sx + a.v[i1] * sy + a.w[i1] * sz);
+  const double du = a.du1[i1], dv = a.dv1[i1], dw = a.dw1[i1];
+  double tx, ty, tz;
+  const double gd = geo_diff(a.msd, du, dv, dw, sx, sy, sz, ex, ey, ez, cf, tx, ty, tz);
+  const double fcl = rhof * gd, ffl = -rhof * gd;
+  fvl = fvl - rhof * (a.bpg[b] * tx + a.bpg[B + b] * ty + a.bpg[B2 + b] * tz);
+  fvl = fvl + rhof * (a.pg[i1] * (du * sx) + a.pg[N + i1] * (dv * sy) + a.pg[N2 + i1] * (dw * sz));
+  if (a.rhok) {
+    fvl = fvl - rhof * (a.bdrk[b] * tx + a.bdrk[B + b] * ty + a.bdrk[B2 + b] * tz);
+    fvl = fvl + rhof * (a.drk[i1] * (du * sx) + a.drk[N + i1] * (dv * sy) + a.drk[N2 + i1] * (dw * sz));
+    fvl = fvl + fcl * a.rhok[i1] + ffl * a.brhok[b];
+  }
+  if (a.relax) {
+    const double ms = rhof * (a.us[i1] * sx + a.vs[i1] * sy + a.ws[i1] * sz);
+    fvl = fvl + (1. - a.urf) * (a.bmdot[b] - ms);
+  }
+  a.bmdot[b] = fcl * a.p[i1] + ffl * a.bp[b] + fvl;
+  double t2x, t2y, t2z;
+  a.bpcoef[b] = rhof * geo_diff(a.msd, a.du2[i1], a.dv2[i1], a.dw2[i1], sx, sy, sz, ex, ey, ez, cf, t2x, t2y, t2z);
+}
+
 // p' system (AssemblePressureCorrectionFluxes.for + global assembly): ac = sum coef,
 // anb = -coef, bc = -(net outflow)
 __global__ void __launch_bounds__(FS_BLOCK) k_pc_assemble(ContArgs a) {
@@ -524,7 +564,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_pc_assemble(ContArgs a) {
         if (s & 1) { ac = ac - fff; a.anb[(long)j * N + i] = 0. - c; bc = bc + md; }
         else { ac = ac + c; a.anb[(long)j * N + i] = 0. + fff; bc = bc - md; }
       } else {
-        ac = ac + 0.;
+        ac = ac + (a.btype[f - F] == FS_BC_OUTLET_SP ? a.bpcoef[f - F] : 0.);
         bc = bc - a.bmdot[f - F];
       }
     };
@@ -543,13 +583,14 @@ struct CorrArgs {
   const int32_t *ncf, *slot, *fown, *fnbr, *bown, *btype;
   const double *bdv, *bnf, *pcoef, *du2, *dv2, *dw2, *pcg, *bpg;
   double *u, *v, *w, *p, *pc, *mdot, *bp, *bpc, *bu, *bv, *bw, *bmdot;
+  const double *bpcoef;
   double *red; int64_t *redi; int nblk; double *rb;
 };
 
 // UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for)
 __global__ void k_bpc(CorrArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < a.B) a.bpc[b] = a.pc[a.bown[b]];
+  if (b < a.B) a.bpc[b] = a.btype[b] == FS_BC_OUTLET_SP ? 0. : a.pc[a.bown[b]];   // :126-130
 }
 // CorrectPressure (CorrectPressure.for:21-42)
 __global__ void k_corr_p(CorrArgs a) {
@@ -583,7 +624,14 @@ __global__ void k_bcorr(CorrArgs a) {
   const int B = a.B;
   const long B2 = 2L * B;
   int t = a.btype[b], i1 = a.bown[b];
-  if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
+  if (t == FS_BC_OUTLET_SP) {
+    // CorrectBoundarymdot (CorrectMdotandVelocity.for:264-280); the static pressure stays (CorrectPressure.for:162-166)
+    const int N = a.N;
+    a.bmdot[b] = a.bmdot[b] - a.bpcoef[b] * (a.bpc[b] - a.pc[i1]);
+    a.bu[b] = a.bu[b] - a.du2[i1] * a.pcg[i1];
+    a.bv[b] = a.bv[b] - a.dv2[i1] * a.pcg[N + i1];
+    a.bw[b] = a.bw[b] - a.dw2[i1] * a.pcg[2L * N + i1];
+  } else if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
     a.bp[b] = a.p[i1] + a.bpg[b] * a.bdv[b] + a.bpg[B + b] * a.bdv[B + b] + a.bpg[B2 + b] * a.bdv[B2 + b];
   } else {
     double rpc = (a.ref_cell >= 0) ? a.pc[a.ref_cell] : 0.;
@@ -815,6 +863,9 @@ static ContArgs cont_args(fs_ctx *ctx) {
   a.mdot = ctx->mdot; a.pcoef = ctx->pcoef; a.bmdot = ctx->bmdot;
   a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bsf = ctx->bsf;
   fs_turb_rhok_ptrs(ctx, &a.rhok, &a.drk);
+  fs_turb_brhok_ptrs(ctx, &a.brhok, &a.bdrk);
+  a.bpcoef = ctx->bpcoef; a.bu_w = ctx->bu; a.bv_w = ctx->bv; a.bw_w = ctx->bw;
+  a.bug = ctx->bug; a.bvg = ctx->bvg; a.bwg = ctx->bwg; a.bdv = ctx->bdv; a.bpg = ctx->bpg; a.bp = ctx->bp;
   a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc; a.red = ctx->red; a.nblk = fs_grid(ctx->N);
   return a;
 }
@@ -832,6 +883,7 @@ int fs_continuity_assemble(fs_ctx *ctx) {
     FS_LAUNCH_CHECK();
   }
   if (B) { k_bmdot_inlet<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  if (B && ctx->has_sp) { k_bmdot_sp<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   k_pc_assemble<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();
   k_residual_final<<<1, 1024, 0, ctx->st>>>(ctx->red, a.nblk, N, 3, ctx->resblk);
@@ -848,7 +900,7 @@ static CorrArgs corr_args(fs_ctx *ctx) {
   a.bdv = ctx->bdv; a.bnf = ctx->bnf; a.pcoef = ctx->pcoef; a.du2 = ctx->du2; a.dv2 = ctx->dv2; a.dw2 = ctx->dw2;
   a.pcg = ctx->pcg; a.bpg = ctx->bpg;
   a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.p = ctx->p; a.pc = ctx->pc; a.mdot = ctx->mdot; a.bp = ctx->bp; a.bpc = ctx->bpc;
-  a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bmdot = ctx->bmdot;
+  a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bmdot = ctx->bmdot; a.bpcoef = ctx->bpcoef;
   a.red = ctx->red; a.redi = ctx->redi; a.nblk = fs_grid(ctx->N); a.rb = ctx->resblk;
   return a;
 }

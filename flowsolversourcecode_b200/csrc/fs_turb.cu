@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
           fcf = fcl;
           tf = fcl * ps + ffl * a.bphi[b] + fvl;
         }
-        if (t == FS_BC_INLET_VEL || t == FS_BC_OUTLET_FD) {
+        if (t == FS_BC_INLET_VEL || t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {
           double cc = fmax(bm, 0.), cn_ = -fmax(-bm, 0.);
           fcf = fcf + cc;
           tf = tf + (cc * ps + cn_ * a.bphi[b]);
@@ -329,7 +329,7 @@ __global__ void k_turb_bound(int N, int B, const int32_t *bown, const int32_t *b
   if (t < N) phi[t] = fmax(phi[t], TINY);
   if (t < B) {
     int ty = btype[t];
-    if (ty == FS_BC_OUTLET_FD || ty == FS_BC_SYMMETRY) bphi[t] = fmax(phi[bown[t]], TINY);
+    if (ty == FS_BC_OUTLET_FD || ty == FS_BC_OUTLET_SP || ty == FS_BC_SYMMETRY) bphi[t] = fmax(phi[bown[t]], TINY);
     else bphi[t] = fmax(bphi[t], 0.);
   }
 }
@@ -505,6 +505,13 @@ void fs_turb_rhok_ptrs(fs_ctx *ctx, const double **rhok, const double **drk) {
   *drk = T ? T->drk : nullptr;
 }
 
+// boundary values of 2/3 rho k and of its gradient (nullptr when laminar)
+void fs_turb_brhok_ptrs(fs_ctx *ctx, const double **brhok, const double **bdrk) {
+  fs_turb *T = ctx->turb;
+  *brhok = T ? T->brhok : nullptr;
+  *bdrk = T ? T->bdrk : nullptr;
+}
+
 // CalculateEffectiveDiffusionCoefficient('vel?') with the momentum wall
 // functions, before the boundary terms of each momentum component
 int fs_turb_wall_functions(fs_ctx *ctx) {
@@ -584,9 +591,9 @@ int fs_turb_effects(fs_ctx *ctx) {
 // FlowIn / FlowOut / AdjustFlow when every outlet is 'fullydeveloped'
 int fs_flow_in_out(fs_ctx *ctx) {
   const fs_case &c = ctx->cfg;
-  int nfd = 0;
-  for (int s = 0; s < ctx->NS; s++) nfd += c.patch_type[s] == FS_BC_OUTLET_FD;
-  if (!nfd) return FS_OK;
+  int nfd = 0, other = 0;
+  for (int s = 0; s < ctx->NS; s++) { nfd += c.patch_type[s] == FS_BC_OUTLET_FD; other += c.patch_type[s] == FS_BC_OUTLET_SP; }
+  if (!nfd || other) return FS_OK;   // FlowOut / AdjustFlow act only when every outlet is fully developed
   FlowArgs a{};
   a.B = ctx->B; a.NS = ctx->NS; a.rho = c.rho;
   double tff = 0.;

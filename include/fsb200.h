@@ -83,7 +83,8 @@ enum fs_bc {
   FS_BC_WALL_SLIP   = 1,   /* 'wall','slip' */
   FS_BC_SYMMETRY    = 2,   /* 'symmetry' */
   FS_BC_INLET_VEL   = 3,   /* 'inlet','specifiedvelocity' */
-  FS_BC_OUTLET_FD   = 4    /* 'outlet','fullydeveloped' */
+  FS_BC_OUTLET_FD   = 4,   /* 'outlet','fullydeveloped' */
+  FS_BC_OUTLET_SP   = 5    /* 'outlet','specifiedstaticpressure' (patch_pressure) */
 };
 
 /* ---------------------------------------------------------- scheme enums */
@@ -173,6 +174,7 @@ typedef struct fs_case {
   double inlet_intensity[FS_MAX_PATCHES];  /* inletTurbulenceIntensity, inletTypeT='specifiedil' */
   double inlet_length[FS_MAX_PATCHES];     /* inletTurbulenceLengthScale */
   int    wall_function;          /* MomentumWallFunctionType: 0 'standard', 1 'scalable', 2 'automatic' */
+  double patch_pressure[FS_MAX_PATCHES];  /* static pressure of 'specifiedstaticpressure' outlets */
 } fs_case;
 
 /* Mesh in polyMesh form (0-based), the input Readit parses

@@ -393,7 +393,7 @@ void om_gradient(om *m, int var, int method, int niter, const double *phi, const
   /* RelaxGradient: all LrelaxGradient* are .false. (User0.F90:164-179) -> return */
   /* CorrectGradientAtOulet for velocities (CorrectGradients.for:188-238) */
   if (var == FS_VAR_U || var == FS_VAR_V || var == FS_VAR_W) {
-    for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_FD) {
+    for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_FD || m->btype[b] == FS_BC_OUTLET_SP) {
       int k = m->bf_own[b], s = m->bf_set[b];
       tproj(m->bnx[b], m->bny[b], nz_ii(m, s), gx[k], gy[k], gz[k], &bgx[b], &bgy[b], &bgz[b], 0);
     }
@@ -652,7 +652,7 @@ void om_assemble_momentum(om *m, int comp)
     if (t == FS_BC_INLET_VEL) {
       double fcl = fmax(m->bmdot[b], 0.), ffl = -fmax(-m->bmdot[b], 0.);
       m->fcf[i4] += fcl; m->fff[i4] += ffl; m->ftf[i4] += fcl * fi[i1] + ffl * bfi[b];
-    } else if (t == FS_BC_OUTLET_FD) {
+    } else if (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {   /* :421-448 the same for both */
       const double *bgx = bfg, *bgy = bfg + B, *bgz = bfg + 2 * (long)B;
       double fcl = fmax(m->bmdot[b], 0.), ffl = -fmax(-m->bmdot[b], 0.);
       double fvl = m->bmdot[b] * (bgx[b] * m->bdx[b] + bgy[b] * m->bdy[b] + bgz[b] * m->bdz[b]);
@@ -730,11 +730,13 @@ static void om_flow_in_out(om *m)
 {
   int NS = m->NS, F = m->F;
   const fs_case *c = &m->cfg;
-  int nfd = 0;
+  int nfd = 0, other = 0;
   for (int s = 0; s < NS; s++) {
     if (c->patch_type[s] == FS_BC_OUTLET_FD) nfd++;
+    if (c->patch_type[s] == FS_BC_OUTLET_SP) other++;
   }
-  if (nfd == 0) return;   /* FlowOut/AdjustFlow return at once; FlowIn's sum is unused */
+  /* FlowOut/AdjustFlow return at once unless every outlet is fully developed */
+  if (nfd == 0 || other) return;
   m->mdot_in = 0.;
   for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_INLET_VEL)
     for (int j = 0; j < m->bset_n[s]; j++) m->mdot_in = m->mdot_in + m->bmdot[m->bset_start[s] + j];
@@ -812,6 +814,31 @@ void om_assemble_continuity(om *m)
     m->mdot[k] = fcl * m->p[i] + ffl * m->p[j] + fvl;
   }
   free(pgbar); free(rkbar); free(rkf);
+  /* 'specifiedstaticpressure' outlets (AssembleMdotUsingRhieChow.for:1441-1598) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) {
+    int i1 = m->bf_own[b];
+    double rhof = c->rho, sx = m->bsx[b], sy = m->bsy[b], sz = m->bsz[b];
+    m->bu[b] = m->u[i1] + (m->bug[b] * m->bdx[b] + m->bug[B + b] * m->bdy[b] + m->bug[2L * B + b] * m->bdz[b]);
+    m->bv[b] = m->v[i1] + (m->bvg[b] * m->bdx[b] + m->bvg[B + b] * m->bdy[b] + m->bvg[2L * B + b] * m->bdz[b]);
+    m->bw[b] = m->w[i1] + (m->bwg[b] * m->bdx[b] + m->bwg[B + b] * m->bdy[b] + m->bwg[2L * B + b] * m->bdz[b]);
+    double mbar = m->u[i1] * sx + m->v[i1] * sy + m->w[i1] * sz;
+    double fvl = rhof * mbar;
+    double du = m->du1[i1], dv = m->dv1[i1], dw = m->dw1[i1], tx, ty, tz;
+    double gd = geo_diff(c->method_decompose_s, du, dv, dw, sx, sy, sz, m->bex[b], m->bey[b], m->bez[b], m->bd[b], &tx, &ty, &tz);
+    double fcl = rhof * gd, ffl = -rhof * gd;
+    fvl = fvl - rhof * (m->bpg[b] * tx + m->bpg[B + b] * ty + m->bpg[2L * B + b] * tz);
+    fvl = fvl + rhof * (m->pg[i1] * (du * sx) + m->pg[N + i1] * (dv * sy) + m->pg[2L * N + i1] * (dw * sz));
+    if (c->turbulence) {
+      fvl = fvl - rhof * (m->bdrk[b] * tx + m->bdrk[B + b] * ty + m->bdrk[2L * B + b] * tz);
+      fvl = fvl + rhof * (m->drk[i1] * (du * sx) + m->drk[N + i1] * (dv * sy) + m->drk[2L * N + i1] * (dw * sz));
+      fvl = fvl + fcl * m->rhok[i1] + ffl * m->brhok[b];
+    }
+    if (c->relax_momentum) {
+      double ms = rhof * (m->us[i1] * sx + m->vs[i1] * sy + m->ws[i1] * sz);
+      fvl = fvl + (1. - c->urf_momentum) * (m->bmdot[b] - ms);
+    }
+    m->bmdot[b] = fcl * m->p[i1] + ffl * m->bp[b] + fvl;
+  }
   /* inlet specified velocity Bmdot (AssembleMdotUsingRhieChow.for:2054-2075) */
   for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_VEL)
     m->bmdot[b] = c->rho * (m->bu[b] * m->bsx[b] + m->bv[b] * m->bsy[b] + m->bw[b] * m->bsz[b]);
@@ -827,6 +854,14 @@ void om_assemble_continuity(om *m)
     m->fcf[k] = c->rho * gd; m->fff[k] = -(c->rho * gd); m->ftf[k] = m->mdot[k];
   }
   for (int b = 0; b < B; b++) m->ftf[F + b] = m->bmdot[b];
+  /* 'specifiedstaticpressure' outlets: p'_b = 0, FluxCf = FluxFf = rho geoDiff(D2)
+   * (AssemblePressureCorrectionFluxes.for:244-313) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) {
+    int i1 = m->bf_own[b];
+    double gd = geo_diff(c->method_decompose_s, m->du2[i1], m->dv2[i1], m->dw2[i1], m->bsx[b], m->bsy[b], m->bsz[b],
+                         m->bex[b], m->bey[b], m->bez[b], m->bd[b], 0, 0, 0);
+    m->fcf[F + b] = c->rho * gd; m->fff[F + b] = c->rho * gd;
+  }
   /* specified-velocity inlet: FluxCf=FluxFf=0 (AssemblePressureCorrectionFluxes.for:545-563) */
   global_assembly(m);
   if (0) {   /* LfixPressure (FixPressure, ReferenceAndSetPressureRoutines.for:64) is not used by these cases */
@@ -841,7 +876,8 @@ void om_correct_continuity(om *m)
   int N = m->N, F = m->F, B = m->B;
   const fs_case *c = &m->cfg;
   /* UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for) */
-  for (int b = 0; b < B; b++) m->bpc[b] = m->pc[m->bf_own[b]];
+  for (int b = 0; b < B; b++)
+    m->bpc[b] = m->btype[b] == FS_BC_OUTLET_SP ? 0. : m->pc[m->bf_own[b]];   /* :126-130 */
   /* CorrectPressure (CorrectPressure.for:4-42) */
   double rpc = (c->ref_pressure_cell >= 0) ? m->pc[c->ref_pressure_cell] : 0.;
   if (c->set_reference_pressure == 1) rpc = 0.;
@@ -856,6 +892,15 @@ void om_correct_continuity(om *m)
   /* Correctmdot (CorrectMdotandVelocity.for:55-63) */
   for (int k = 0; k < F; k++)
     m->mdot[k] = m->mdot[k] + m->fcf[k] * m->pc[m->if_own[k]] + m->fff[k] * m->pc[m->if_nbr[k]];
+  /* CorrectBoundarymdot, 'specifiedstaticpressure' (CorrectMdotandVelocity.for:264-280) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) {
+    int i1 = m->bf_own[b];
+    double gd = m->fff[F + b];
+    m->bmdot[b] = m->bmdot[b] - gd * (m->bpc[b] - m->pc[i1]);
+    m->bu[b] = m->bu[b] - m->du2[i1] * m->pcg[i1];
+    m->bv[b] = m->bv[b] - m->dv2[i1] * m->pcg[N + i1];
+    m->bw[b] = m->bw[b] - m->dw2[i1] * m->pcg[2L * N + i1];
+  }
   /* UpdateBoundaryPressure (CorrectPressure.for:49-190): walls and symmetry */
   for (int b = 0; b < B; b++) {
     int t = m->btype[b], i1 = m->bf_own[b];
@@ -1264,6 +1309,12 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
   }
   m->u = dz_(N); m->v = dz_(N); m->w = dz_(N); m->p = dz_(N); m->pc = dz_(N); m->mdot = dz_(F);
   m->bu = bvx; m->bv = bvy; m->bw = bvz; m->bp = dz_(B); m->bpc = dz_(B); m->bmdot = dz_(B);
+  /* specified static pressure on its outlets; SetReferencePressure
+   * (ReferenceAndSetPressureRoutines.for:4-50): a pressure-specified patch
+   * fixes the level, no reference cell */
+  int has_sp = 0;
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) { m->bp[b] = cfg->patch_pressure[m->bf_set[b]]; has_sp = 1; }
+  if (m->cfg.set_reference_pressure < 0) m->cfg.set_reference_pressure = has_sp;
   m->ug = dz_(3L*N); m->vg = dz_(3L*N); m->wg = dz_(3L*N); m->pg = dz_(3L*N); m->pcg = dz_(3L*N);
   m->bug = dz_(3L*B); m->bvg = dz_(3L*B); m->bwg = dz_(3L*B); m->bpg = dz_(3L*B); m->bpcg = dz_(3L*B);
   m->ugf = dz_(3L*F); m->vgf = dz_(3L*F); m->wgf = dz_(3L*F); m->pgf = dz_(3L*F);

@@ -163,6 +163,30 @@ def test_oracle_production_of_simple_shear():
     assert np.allclose(P, np.minimum(ref, cap), rtol=1e-15, atol=0)
 
 
+def _pressure_outlet(case):
+    case.patches["xmax"] = ("pressure_outlet", 0.0)
+    return case
+
+
+def test_oracle_pressure_outlet_step():
+    """'specifiedstaticpressure' outlet: the laminar step converges with the
+    outlet pressure held, and the outflow matches the inflow once converged."""
+    import oracle
+    m, c = cs.bfs(30, 12, 6, re_h=100.0, turbulence=False, solver_cont="sor", rrf_cont=1e-3, itmax_cont=300)
+    _pressure_outlet(c)
+    o = oracle.Oracle(m, c)
+    _setup(o, m, c)
+    for it in range(400):
+        s = o.simple_iteration()
+        if s < 1e-8:
+            break
+    assert s < 1e-8, s
+    bm = o.get("bmdot")
+    qin, qout = bm[_patch_slice(m, "inlet")].sum(), bm[_patch_slice(m, "xmax")].sum()
+    assert abs(qin + qout) <= 1e-5 * abs(qin)
+    assert np.all(o.get("bp")[_patch_slice(m, "xmax")] == 0.0)
+
+
 # ------------------------------------------------------------------- GPU
 @pytest.mark.gpu
 @pytest.mark.parametrize("wall_function", ["standard", "scalable", "automatic"])
@@ -241,4 +265,27 @@ def test_kepsilon_step_converged_fields_match_oracle():
     # pressure: same field up to the level fixed at the reference cell
     dp = (g.get("p") - g.get("p")[0]) - (o.get("p") - o.get("p")[0])
     assert np.linalg.norm(dp) <= 1e-6 * np.linalg.norm(o.get("p") - o.get("p")[0])
+    g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("turbulence", [False, True])
+def test_pressure_outlet_step_matches_oracle(turbulence):
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, re_h=100.0 if not turbulence else 5000.0, turbulence=turbulence, **_tight())
+    _pressure_outlet(c)
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
+    _setup(o, m, c)
+    _setup(g, m, c)
+    for it in range(6):
+        so = o.simple_iteration()
+        rg = g.simple_iteration()
+        assert abs(rg["source"] - so) <= 1e-6 * abs(so) + 1e-14, (it, rg["source"], so)
+    keys = ("u", "v", "w", "p", "bmdot", "bu", "bp") + (("tke", "ted", "mut") if turbulence else ())
+    for k in keys:
+        x, ref = g.get(k), o.get(k)
+        err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+        assert err <= 1e-9, (k, err)
     g.close()
