@@ -27,6 +27,7 @@ VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
 VAR_TKE, VAR_TED, VAR_RHOK = 8, 9, 10
 # boundary types
 BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD, BC_OUTLET_SP = 0, 1, 2, 3, 4, 5
+TRANSIENT = {"euler": 0, "cranknicolson1": 1, "cranknicolson2": 2, "adamsmoulton": 3}
 # gradient interpolation
 GI_AVERAGE, GI_UPWIND, GI_DOWNWIND, GI_AVERAGECORRECTED = 0, 1, 2, 3
 HR_NONE, HR_TVD = 0, 1
@@ -38,7 +39,8 @@ SIMPLE, SIMPLEC = 0, 1
 FIELDS = ["u", "v", "w", "p", "pc", "mdot", "bu", "bv", "bw", "bp", "bpc", "bmdot", "ac", "bc", "anb",
           "du1", "dv1", "dw1", "du2", "dv2", "dw2", "ugrad", "vgrad", "wgrad", "pgrad", "pcgrad",
           "volume", "xc", "gfactor", "sf", "gdiff", "ft", "bsf", "dphi",
-          "tke", "ted", "mut", "btke", "bted", "bmut", "kx", "utau", "yplus"]
+          "tke", "ted", "mut", "btke", "bted", "bmut", "kx", "utau", "yplus",
+          "old", "oldold", "bold"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
 
@@ -72,6 +74,7 @@ class FsCase(C.Structure):
         ("inlet_intensity", C.c_double * FS_MAX_PATCHES), ("inlet_length", C.c_double * FS_MAX_PATCHES),
         ("wall_function", C.c_int),
         ("patch_pressure", C.c_double * FS_MAX_PATCHES),
+        ("unsteady", C.c_int), ("transient_scheme", C.c_int), ("dt", C.c_double),
     ]
 
 
@@ -119,6 +122,9 @@ PROTOTYPES = {
     "fs_correct_continuity": (C.c_int, [_V]),
     "fs_set_iteration": (C.c_int, [_V, C.c_int]),
     "fs_initialize_mdot": (C.c_int, [_V]),
+    "fs_advance_time": (C.c_int, [_V, C.c_double]),
+    "fs_get_time": (C.c_int, [_V, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "fs_set_time": (C.c_int, [_V, C.POINTER(C.c_double), C.c_int32]),
     "fs_gradient": (C.c_int, [_V, C.c_int, C.c_int, C.c_int]),
     "fs_gradient_host": (C.c_int, [_V, C.c_int, C.c_int, C.c_int, _D, _D, _D, _D]),
     "fs_under_relax": (C.c_int, [_V, C.c_double]),

@@ -91,6 +91,10 @@ class Case:
     wall_function: str = "standard"        # MomentumWallFunctionType: 'standard' or 'scalable'
     # inlet patch name -> (inletTurbulenceIntensity, inletTurbulenceLengthScale), 'specifiedil'
     inlet_turbulence: dict = field(default_factory=dict)
+    # unsteady runs (LUnsteady, TransientScheme, dt); time steps through Solver.advance_time
+    unsteady: bool = False
+    transient_scheme: str = "euler"        # 'euler', 'cranknicolson1', 'cranknicolson2', 'adamsmoulton'
+    dt: float = 1.0e-2
 
     def struct(self, mesh: PolyMesh) -> L.FsCase:
         c = L.FsCase()
@@ -141,6 +145,7 @@ class Case:
         c.max_visc_ratio, c.limit_production = self.max_visc_ratio, int(self.limit_production)
         c.conv_scheme_tke, c.conv_scheme_ted = L.TVD[self.conv_scheme_tke], L.TVD[self.conv_scheme_ted]
         c.wall_function = {"standard": 0, "scalable": 1, "automatic": 2}[self.wall_function]
+        c.unsteady, c.transient_scheme, c.dt = int(self.unsteady), L.TRANSIENT[self.transient_scheme], float(self.dt)
         return c
 
 

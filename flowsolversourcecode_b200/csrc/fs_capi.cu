@@ -127,6 +127,9 @@ static double *field_ptr(fs_ctx *c, int f, size_t *n) {
   case FS_F_TKE: case FS_F_TED: case FS_F_MUT: case FS_F_BTKE: case FS_F_BTED: case FS_F_BMUT:
   case FS_F_UTAU: case FS_F_YPLUS:
     return fs_turb_field(c, f, n);
+  case FS_F_OLD: *n = c->old ? 6 * N : 0; return c->old;
+  case FS_F_OLDOLD: *n = c->oldold ? 6 * N : 0; return c->oldold;
+  case FS_F_BOLD: *n = c->bold ? 6 * B : 0; return c->bold;
   }
   *n = 0;
   return nullptr;
@@ -165,7 +168,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   ctx->cfg = *cfg;
   ctx->dev = device;
   int rc = FS_OK;
-  auto fail = [&](int r) { fs_turb_free(ctx); free_all(ctx); if (ctx->st) cudaStreamDestroy(ctx->st); delete ctx; return r; };
+  auto fail = [&](int r) { fs_transient_free(ctx); fs_turb_free(ctx); free_all(ctx); if (ctx->st) cudaStreamDestroy(ctx->st); delete ctx; return r; };
   if (cudaSetDevice(device) != cudaSuccess) return fail(FS_E_CUDA);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(FS_E_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -236,6 +239,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   k_initial_mdot<<<fs_grid((long)F + B), FS_BLOCK, 0, ctx->st>>>((int)N, (int)F, (int)B, ctx->cfg.rho, ctx->fown, ctx->fnbr,
       ctx->gf, ctx->sf, ctx->u, ctx->v, ctx->w, ctx->mdot, ctx->btype, ctx->bsf, ctx->bu, ctx->bv, ctx->bw, ctx->bmdot);
   ctx->launches++;
+  if ((rc = fs_transient_create(ctx))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
   if (cudaStreamSynchronize(ctx->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return fail(FS_E_CUDA);
   *out = ctx;
   return FS_OK;
@@ -248,6 +252,7 @@ int fs_destroy(fs_ctx *ctx) {
   fs_mg_free(ctx);
   fs_nn_free(ctx);
   fs_turb_free(ctx);
+  fs_transient_free(ctx);
   free_all(ctx);
   for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto &e : ctx->tev) if (e) cudaEventDestroy(e);

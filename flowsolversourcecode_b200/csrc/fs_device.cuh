@@ -170,4 +170,22 @@ __device__ __forceinline__ double hr_flux(int scheme, double bleed, double md, d
   return md * (phiHR - phic) * 1.;
 }
 
+// AssembleTransientTerm (AssembleTheTransientTerm.for:52-330) for time-level
+// block lvl (0..2 velocity, 4 k, 5 epsilon) of cell i: adds to the cell's
+// FluxCE and FluxTE sums in the reference's order.
+__device__ __forceinline__ void transient_term(const FsTransient &t, int lvl, long N, long i, double V, double phi,
+                                               double &fce, double &fte) {
+  const double po = t.old[lvl * N + i];
+  if (!t.three) {
+    const double fcl = t.rho * V / t.d, fcol = -(t.rho * V / t.d);
+    fce = fce + fcl;
+    fte = fte + fcl * phi + fcol * po;
+  } else {
+    const double poo = t.oldold[lvl * N + i];
+    const double fcl = t.f1 * t.rho * V, fcol = t.s2 * (t.f2 * t.rho * V), fcool = t.f3 * t.rho * V;
+    fce = fce + fcl;
+    fte = fte + fcl * phi + fcol * po + fcool * poo;
+  }
+}
+
 }  // namespace

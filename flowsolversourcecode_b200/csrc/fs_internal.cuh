@@ -99,6 +99,11 @@ struct fs_ctx {
   // [0] mdotIn, [1 + s] mdot1(s), [1 + FS_MAX_PATCHES + s] mdotOut(s)
   int32_t *d_bset = nullptr;
   double *flow = nullptr;
+  // unsteady runs: u v w p k epsilon at time levels n-1, n-2 (6N each), their
+  // boundary values at n-1 (6B), p at the last X-momentum gradient ('cranknicolson1')
+  double *old = nullptr, *oldold = nullptr, *bold = nullptr, *p_mx = nullptr;
+  double dt = 0., dto = 0., dtoo = 0., time = 0.;
+  int ndt = 0, tscheme = 0;      // tscheme: the TransientScheme in effect
   // k-epsilon (nullptr: laminar)
   fs_turb *turb = nullptr;
   // multigrid
@@ -190,6 +195,19 @@ int fs_continuity_correct(fs_ctx *ctx);
 int fs_residual_reduce(fs_ctx *ctx, int nf);   // CalculateResiduals partials -> resblk slot
 int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int solver);
 // k-epsilon and outlets (fs_turb.cu)
+// Transient term of one equation (AssembleTheTransientTerm.for:52-330), by value in kernel arguments:
+// two-level (three = 0): FluxCE = rho V / d, FluxCEold = -(rho V / d);
+// three-level: FluxCE = f1 rho V, FluxCEold = s2 (f2 rho V), FluxCEoldold = f3 rho V.
+struct FsTransient {
+  int on, three;
+  double rho, d, f1, f2, f3, s2;
+  const double *old, *oldold;    // 6N blocks: u v w p k epsilon
+};
+FsTransient fs_transient_args(const fs_ctx *ctx);
+double fs_drhodt(const fs_ctx *ctx);                   // d rho/dt of the continuity residual
+int fs_transient_create(fs_ctx *ctx);
+void fs_transient_free(fs_ctx *ctx);
+int fs_assemble_mdot(fs_ctx *ctx, const double *p_face);   // AssembleMdot alone
 int fs_turb_create(fs_ctx *ctx);
 void fs_turb_free(fs_ctx *ctx);
 double *fs_turb_field(fs_ctx *ctx, int field, size_t *n);

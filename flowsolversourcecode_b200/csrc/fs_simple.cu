@@ -196,6 +196,7 @@ struct MomArgs {
   double *ac_int, *anb, *bc_int, *effdiv;
   double *ac, *bc, *d1, *d2, *star;
   double *red; int nblk;
+  FsTransient tr;                        // unsteady runs (tr.on = 0: steady)
 };
 
 // Interior-face part of SolveMomentumX/Y/Z for all three components at once:
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
     double fce = fmax(e, 0.0) - e;
     double fve = -(fmax(e, 0.0) * phi);
     double fte = fce * phi + fve;
+    if (a.tr.on) transient_term(a.tr, comp, N, i, a.vol[i], phi, fce, fte);   // SolveXMomentumEquation.for:247-251
     fte = fte + a.pg[(long)comp * N + i] * a.vol[i];
     if (TURB) fte = fte + a.drk[(long)comp * N + i] * a.vol[i];
     ac = ac + fce;
@@ -414,6 +416,7 @@ struct ContArgs {
   const int32_t *ncf, *slot, *fown, *fnbr, *bown, *btype;
   const double *gf, *sf, *dcfv, *dcf;
   const double *u, *v, *w, *p, *us, *vs, *ws, *pg;
+  const double *pf;   // pressure of the 'averagecorrected' face gradient (fs_assemble_mdot)
   const double *du1, *dv1, *dw1, *du2, *dv2, *dw2;
   double *mdot, *pcoef, *bmdot;
   const double *bu, *bv, *bw, *bsf;
@@ -471,7 +474,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mdot(ContArgs a) {
   double gox = a.pg[i], goy = a.pg[N + i], goz = a.pg[N2 + i];
   double gnx = a.pg[j], gny = a.pg[N + j], gnz = a.pg[N2 + j];
   double pfx, pfy, pfz;   // PressGradf (GradientInterpolationSchemeContinuity)
-  face_grad(a.gi_scheme, g, a.mdot[k], pi, pj, cf, ex, ey, ez, gox, goy, goz, gnx, gny, gnz, pfx, pfy, pfz);
+  face_grad(a.gi_scheme, g, a.mdot[k], a.pf[i], a.pf[j], cf, ex, ey, ez, gox, goy, goz, gnx, gny, gnz, pfx, pfy, pfz);
   double pbx = g * gox + g1 * gnx, pby = g * goy + g1 * gny, pbz = g * goz + g1 * gnz;  // PressGradBar ('average')
   fvl = fvl - rhof * (pfx * tx + pfy * ty + pfz * tz);
   fvl = fvl + rhof * (pbx * (du * sx) + pby * (dv * sy) + pbz * (dw * sz));
@@ -585,6 +588,7 @@ struct CorrArgs {
   double *u, *v, *w, *p, *pc, *mdot, *bp, *bpc, *bu, *bv, *bw, *bmdot;
   const double *bpcoef;
   double *red; int64_t *redi; int nblk; double *rb;
+  const double *vol; double drhodt; int unsteady;   // + d rho/dt V in unsteady runs
 };
 
 // UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for)
@@ -662,6 +666,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_mass_imbalance(CorrArgs a) {
       if (f < F) m = (s & 1) ? m - a.mdot[f] : m + a.mdot[f];
       else m = m + a.bmdot[f - F];
     }
+    if (a.unsteady) m = m + a.drhodt * a.vol[i];   // CalculateContinuityResiduals.for:159-170
   }
   double s0 = block_sum(m, sh);
   double s1 = block_sum(fabs(m), sh);
@@ -795,6 +800,7 @@ static MomArgs mom_args(fs_ctx *ctx) {
   MomArgs a{};
   const fs_case &c = ctx->cfg;
   a.N = ctx->N; a.F = ctx->F; a.B = ctx->B;
+  a.tr = fs_transient_args(ctx);
   a.ncf = ctx->ncf; a.slot = ctx->slot; a.fown = ctx->fown; a.fnbr = ctx->fnbr; a.bown = ctx->bown; a.btype = ctx->btype;
   a.cn = ctx->cn;
   a.gf = ctx->gf; a.sf = ctx->sf; a.dcfv = ctx->dcfv; a.dcf = ctx->dcf; a.gdiff = ctx->gdiff; a.tf = ctx->tf; a.vol = ctx->vol;
@@ -828,6 +834,9 @@ int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac_out, double *bc_ou
     int nit[4] = {c.niter_grad_mom, c.niter_grad_mom, c.niter_grad_mom, c.niter_grad_cont};
     int rc = fs_gradient_dev(ctx, 4, vars, phi, bphi, g, bg, meth, nit);
     if (rc) return rc;
+    // 'cranknicolson1': the pressure PressGradf is interpolated from here on
+    // (SolveXMomentumEquation.for:214-217), kept for the AssembleMdot after an extrapolation
+    if (ctx->p_mx) FS_CK(cudaMemcpyAsync(ctx->p_mx, ctx->p, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->st));
     if (ctx->turb && (rc = fs_turb_rhok_gradient(ctx))) return rc;
     MomArgs a = mom_args(ctx);
     if (ctx->turb) k_mom_interior<true><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
@@ -859,6 +868,7 @@ static ContArgs cont_args(fs_ctx *ctx) {
   a.ncf = ctx->ncf; a.slot = ctx->slot; a.fown = ctx->fown; a.fnbr = ctx->fnbr; a.bown = ctx->bown; a.btype = ctx->btype;
   a.gf = ctx->gf; a.sf = ctx->sf; a.dcfv = ctx->dcfv; a.dcf = ctx->dcf;
   a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.p = ctx->p; a.us = ctx->us; a.vs = ctx->vs; a.ws = ctx->ws; a.pg = ctx->pg;
+  a.pf = ctx->p;
   a.du1 = ctx->du1; a.dv1 = ctx->dv1; a.dw1 = ctx->dw1; a.du2 = ctx->du2; a.dv2 = ctx->dv2; a.dw2 = ctx->dw2;
   a.mdot = ctx->mdot; a.pcoef = ctx->pcoef; a.bmdot = ctx->bmdot;
   a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bsf = ctx->bsf;
@@ -870,13 +880,14 @@ static ContArgs cont_args(fs_ctx *ctx) {
   return a;
 }
 
-// SolveContinuity up to (not including) SolveEquation
-int fs_continuity_assemble(fs_ctx *ctx) {
-  const int N = ctx->N, F = ctx->F, B = ctx->B;
-  FS_CK(cudaMemsetAsync(ctx->pc, 0, sizeof(double) * N, ctx->st));   // InitializePressureCorrection
-  int rc = fs_flow_in_out(ctx);                                        // FlowIn, FlowOut, AdjustFlow
-  if (rc) return rc;
+// AssembleMdot (AssembleMdotUsingRhieChow.for:262-759, 1441-1598, 2033-2075).
+// p_face: the pressure whose 'averagecorrected' face gradient PressGradf
+// enters (the X-momentum solve interpolated it, SolveXMomentumEquation.for:214-217);
+// the current pressure, except after a Crank-Nicolson extrapolation.
+int fs_assemble_mdot(fs_ctx *ctx, const double *p_face) {
+  const int F = ctx->F, B = ctx->B;
   ContArgs a = cont_args(ctx);
+  a.pf = p_face;
   if (F) {
     if (a.rhok) k_mdot<true><<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a);
     else k_mdot<false><<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a);
@@ -884,6 +895,18 @@ int fs_continuity_assemble(fs_ctx *ctx) {
   }
   if (B) { k_bmdot_inlet<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   if (B && ctx->has_sp) { k_bmdot_sp<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  return FS_OK;
+}
+
+// SolveContinuity up to (not including) SolveEquation
+int fs_continuity_assemble(fs_ctx *ctx) {
+  const int N = ctx->N, F = ctx->F, B = ctx->B;
+  FS_CK(cudaMemsetAsync(ctx->pc, 0, sizeof(double) * N, ctx->st));   // InitializePressureCorrection
+  int rc = fs_flow_in_out(ctx);                                        // FlowIn, FlowOut, AdjustFlow
+  if (rc) return rc;
+  rc = fs_assemble_mdot(ctx, ctx->p);
+  if (rc) return rc;
+  ContArgs a = cont_args(ctx);
   k_pc_assemble<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();
   k_residual_final<<<1, 1024, 0, ctx->st>>>(ctx->red, a.nblk, N, 3, ctx->resblk);
@@ -902,6 +925,7 @@ static CorrArgs corr_args(fs_ctx *ctx) {
   a.u = ctx->u; a.v = ctx->v; a.w = ctx->w; a.p = ctx->p; a.pc = ctx->pc; a.mdot = ctx->mdot; a.bp = ctx->bp; a.bpc = ctx->bpc;
   a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bmdot = ctx->bmdot; a.bpcoef = ctx->bpcoef;
   a.red = ctx->red; a.redi = ctx->redi; a.nblk = fs_grid(ctx->N); a.rb = ctx->resblk;
+  a.vol = ctx->vol; a.unsteady = c.unsteady; a.drhodt = c.unsteady ? fs_drhodt(ctx) : 0.;
   return a;
 }
 

@@ -61,6 +61,7 @@ struct TurbArgs {
   double *ac, *anb, *bc, *red;
   int nblk;
   double in_i[FS_MAX_PATCHES], in_l[FS_MAX_PATCHES];
+  FsTransient tr;                     // unsteady runs (tr.on = 0: steady)
 };
 
 // TangentialVelocity (NormalAndTangentialVelocities/CalculateTangentialVelocity.for:4-35)
@@ -304,6 +305,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
     double fte2 = fce2 * ps + fve;
     fce = fce + fce2;
     fte = fte + fte2;
+    if (a.tr.on) transient_term(a.tr, TED ? 5 : 4, N, i, V, ps, fce, fte);   // SolveTKE.for:194-199
     ac = ac + fce;
     bc = bc - fte;
     ac = ac / a.urf;
@@ -414,6 +416,7 @@ TurbArgs turb_args(fs_ctx *ctx) {
   fs_turb *T = ctx->turb;
   a.N = ctx->N; a.F = ctx->F; a.B = ctx->B;
   a.rho = c.rho; a.mu = c.mu; a.bleed = c.bleed;
+  a.tr = fs_transient_args(ctx);
   a.cmu75 = sqrt(sqrt(KE_CMU)); a.cmu75 = a.cmu75 * a.cmu75 * a.cmu75;
   a.tvisc_urf = c.urf_tvisc; a.max_ratio = c.max_visc_ratio; a.limit = c.limit_production;
   a.wfun = c.wall_function;

@@ -85,6 +85,31 @@ class Solver:
         """CalculateInitialmdot from the current velocity fields (after set())."""
         self._chk(self.lib.fs_initialize_mdot(self.ctx), "initialize_mdot")
 
+    # ------------------------------------------------------------ unsteady runs
+    def advance_time(self, dt_next: float | None = None):
+        """Time-step prologue of the unsteady loop (MainProgram.for:184-245):
+        scheme selection, Crank-Nicolson extrapolation, updateVariablesInTime,
+        dt bookkeeping, time += dt; the outer-iteration count restarts."""
+        dt_next = self.case.dt if dt_next is None else dt_next
+        self._chk(self.lib.fs_advance_time(self.ctx, float(dt_next)), "advance_time")
+        self.nIter = 0
+
+    def time_state(self) -> dict:
+        t = (C.c_double * 4)()
+        n = C.c_int32(0)
+        self._chk(self.lib.fs_get_time(self.ctx, t, C.byref(n)), "get_time")
+        return {"time": t[0], "dt": t[1], "dt_old": t[2], "dt_oldold": t[3], "ndt": n.value}
+
+    def set_time_state(self, time: float, dt: float, dt_old: float, dt_oldold: float, ndt: int):
+        t = (C.c_double * 4)(time, dt, dt_old, dt_oldold)
+        self._chk(self.lib.fs_set_time(self.ctx, t, int(ndt)), "set_time")
+
+    def run_time_step(self, itermax: int, tol: float | None = None, dt_next: float | None = None) -> list[dict]:
+        """One time step: advance_time, then outer iterations until the
+        stop metric falls below tol (do nIter=1,IterMax, MainProgram.for:257-325)."""
+        self.advance_time(dt_next)
+        return self.run(itermax, tol)
+
     def set_iteration(self, n: int):
         self.nIter = n
         self._chk(self.lib.fs_set_iteration(self.ctx, n), "set_iteration")
@@ -162,7 +187,8 @@ class Solver:
         N, F, B, W = self.N, self.F, self.B, self.W
         sizes = {"mdot": F, "gfactor": F, "gdiff": F, "sf": 3 * F, "ft": 3 * F, "anb": W * N,
                  "bu": B, "bv": B, "bw": B, "bp": B, "bpc": B, "bmdot": B, "bsf": 3 * B, "xc": 3 * N,
-                 "btke": B, "bted": B, "bmut": B, "utau": B, "yplus": B}
+                 "btke": B, "bted": B, "bmut": B, "utau": B, "yplus": B,
+                 "old": 6 * N, "oldold": 6 * N, "bold": 6 * B}
         if name.endswith("grad"):
             return 3 * N
         return sizes.get(name, N)
@@ -179,6 +205,8 @@ class Solver:
     # fields that carry information from one outer iteration to the next
     RESTART_FIELDS = ("u", "v", "w", "p", "mdot", "bu", "bv", "bw", "bp", "bmdot", "kx")
     RESTART_TURB = ("tke", "ted", "mut", "btke", "bted", "bmut", "utau", "yplus")
+    # unsteady runs: the old time levels (ReadSolutionToContinue.for:59-108)
+    RESTART_UNSTEADY = ("old", "oldold", "bold")
 
     def write_solution(self, path: str) -> None:
         """writeSolution (WriteAndReadSolution/WriteSolutionToContinue.for:4):
@@ -188,8 +216,13 @@ class Solver:
         to a .npz file.  Gradients, D, u* and the matrices are rebuilt by the
         next iteration before they are read, so they are not stored."""
         names = self.RESTART_FIELDS + (self.RESTART_TURB if self.case.turbulence else ())
+        names += self.RESTART_UNSTEADY if self.case.unsteady else ()
         data = {k: self.get(k) for k in names}
         data["nIter"] = np.array([self.nIter], np.int64)
+        if self.case.unsteady:
+            t = self.time_state()
+            data["time"] = np.array([t["time"], t["dt"], t["dt_old"], t["dt_oldold"]])
+            data["ndt"] = np.array([t["ndt"]], np.int64)
         np.savez(path, **data)
 
     def read_solution(self, path: str) -> None:
@@ -197,9 +230,11 @@ class Solver:
         next outer iterations repeat those of the run that wrote it."""
         with np.load(path) as f:
             for k in f.files:
-                if k != "nIter":
+                if k not in ("nIter", "time", "ndt"):
                     self.set(k, f[k])
             self.set_iteration(int(f["nIter"][0]))
+            if "time" in f.files:
+                self.set_time_state(*[float(x) for x in f["time"]], int(f["ndt"][0]))
 
     def state(self) -> dict:
         return {k: self.get(k) for k in ("u", "v", "w", "p", "mdot", "bu", "bv", "bw", "bp", "bmdot")}

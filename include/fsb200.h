@@ -72,6 +72,8 @@ enum fs_field {
   FS_F_BTKE, FS_F_BTED, FS_F_BMUT,                   /* B */
   FS_F_KX,                                           /* N: BICGSTAB_OMP's persistent solution vector */
   FS_F_UTAU, FS_F_YPLUS,                             /* B: wall-function state (uTau, yplus) */
+  FS_F_OLD, FS_F_OLDOLD,                             /* 6N: u v w p k epsilon at time levels n-1, n-2 (unsteady) */
+  FS_F_BOLD,                                         /* 6B: their boundary values at n-1 */
   FS_F_COUNT
 };
 
@@ -175,7 +177,22 @@ typedef struct fs_case {
   double inlet_length[FS_MAX_PATCHES];     /* inletTurbulenceLengthScale */
   int    wall_function;          /* MomentumWallFunctionType: 0 'standard', 1 'scalable', 2 'automatic' */
   double patch_pressure[FS_MAX_PATCHES];  /* static pressure of 'specifiedstaticpressure' outlets */
+  /* unsteady runs (LUnsteady, TransientScheme, dt; ProblemDescriptionRoutine.for:539):
+   * the transient term of the momentum, k and epsilon equations
+   * (AssembleTheTransientTerm.for:52-330).  Time steps are advanced by
+   * fs_advance_time; 0 = steady. */
+  int    unsteady;
+  int    transient_scheme;       /* fs_transient */
+  double dt;                     /* first time step */
 } fs_case;
+
+/* TransientScheme values (AssembleTheTransientTerm.for:52,124,199,290). */
+enum fs_transient {
+  FS_TRANSIENT_EULER          = 0,   /* 'euler' */
+  FS_TRANSIENT_CRANKNICOLSON1 = 1,   /* 'cranknicolson1': Euler over dt/2, then extrapolate */
+  FS_TRANSIENT_CRANKNICOLSON2 = 2,   /* 'cranknicolson2': three time levels */
+  FS_TRANSIENT_ADAMSMOULTON   = 3    /* 'adamsmoulton': three time levels */
+};
 
 /* Mesh in polyMesh form (0-based), the input Readit parses
  * (GridAndGeometry/ReadFoamMesh.f90:31-297). */
@@ -251,6 +268,22 @@ int fs_set_iteration(fs_ctx *ctx, int n_iter);
  * Bmdot from the current cell and boundary velocities, for a caller that set
  * an initial field with fs_set_field (fs_create already ran it once). */
 int fs_initialize_mdot(fs_ctx *ctx);
+
+/* Time-step prologue of the unsteady loop (MainProgram.for:184-245): the
+ * first step of 'cranknicolson2'/'adamsmoulton' runs as 'euler'; from the
+ * second step on 'cranknicolson1' first extrapolates every solved field
+ * (CrankNicolsonRoutine.for:4: phi = 2 phi - phiOld, boundary values too) and
+ * re-assembles the face mass fluxes (AssembleMdot); then the time levels are
+ * shifted (updateVariablesInTime, AdvanceVariablesInTime.for:4), dtOldOld =
+ * dtOld = dt, dt = dt_next, time += dt and the outer-iteration counter
+ * restarts (do nIter=1,IterMax).  Requires cfg.unsteady. */
+int fs_advance_time(fs_ctx *ctx, double dt_next);
+/* Time state: t[0] time, t[1] dt, t[2] dtOld, t[3] dtOldOld, and ndt (the
+ * number of time steps taken).  fs_set_time restores it for a restart
+ * (readSolution, ReadSolutionToContinue.for:59-108, restores the old time
+ * levels, which are the fields FS_F_OLD, FS_F_OLDOLD and FS_F_BOLD). */
+int fs_get_time(fs_ctx *ctx, double t[4], int32_t *n_steps);
+int fs_set_time(fs_ctx *ctx, const double t[4], int32_t n_steps);
 
 /* ---------------------------------------------------------- leaf routines */
 /* Gradient (GradientFiles/CalculateGradients.for:3) of field var

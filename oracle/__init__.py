@@ -56,6 +56,9 @@ def load():
         lib.om_residuals_turb.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         lib.om_initialize_mdot.argtypes = [C.c_void_p]
         lib.om_turb_production.argtypes = [C.c_void_p]
+        lib.om_advance_time.argtypes = [C.c_void_p, C.c_double]
+        lib.om_get_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        lib.om_set_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
         lib.om_mg_setup.restype = C.c_int
         lib.om_mg_setup.argtypes = [C.c_void_p]
         lib.om_mg_level_size.restype = C.c_int
@@ -139,6 +142,21 @@ class Oracle:
     def initialize_mdot(self):
         """CalculateInitialmdot from the current velocity fields."""
         self.lib.om_initialize_mdot(self.h)
+
+    def advance_time(self, dt_next: float):
+        """Time-step prologue of the unsteady loop (MainProgram.for:184-245)."""
+        self.lib.om_advance_time(self.h, float(dt_next))
+        self.nIter = 0
+
+    def get_time(self) -> dict:
+        t = (C.c_double * 4)()
+        n = C.c_int(0)
+        self.lib.om_get_time(self.h, t, C.byref(n))
+        return {"time": t[0], "dt": t[1], "dt_old": t[2], "dt_oldold": t[3], "ndt": n.value}
+
+    def set_time(self, time: float, dt: float, dt_old: float, dt_oldold: float, ndt: int):
+        t = (C.c_double * 4)(time, dt, dt_old, dt_oldold)
+        self.lib.om_set_time(self.h, t, int(ndt))
 
     def lin_iters(self, nf: int) -> int:
         return self.lib.om_lin_iters(self.h, nf)

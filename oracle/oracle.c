@@ -89,11 +89,16 @@ struct om {
   double *kx, *kr, *kb;
   /* multigrid */
   int mg_nlev; int mg_built; void *mgt;
+  /* unsteady (Variables1 ...Old and ...OldOld, Transient1 dt, dtOld, dtOldOld; time, ndt) */
+  double *old, *oldold, *bold;
+  double dt, dto, dtoo, time;
+  int ndt, tscheme;                         /* tscheme: the TransientScheme in effect */
 };
 
 static double *dz_(long n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
 static void om_momentum_wall_functions(om *m);   /* oracle_turb.inc */
 static int *iz_(long n) { return (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int)); }
+#include "oracle_transient.inc"
 
 /* ===================================================================== */
 /*  Connectivity: Readit (GridAndGeometry/ReadFoamMesh.f90:277-660)       */
@@ -659,6 +664,8 @@ void om_assemble_momentum(om *m, int comp)
       m->fcf[i4] += fcl; m->fff[i4] += ffl; m->ftf[i4] += fcl * fi[i1] + ffl * bfi[b] + fvl;
     }
   }
+  /* AssembleTransientTerm (SolveXMomentumEquation.for:247-251) */
+  om_transient_term(m, fi, comp);
   /* AssembleSourceTerm: Sc=Sb=0 for these cases (AssembleSources.for:20-33) adds nothing */
   /* AssemblePressureGradientTerm (AssemblePressureGradient.for:17-22) */
   const double *dp = m->pg + (long)comp * N;
@@ -770,14 +777,11 @@ static void om_flow_in_out(om *m)
   (void)F;
 }
 
-void om_assemble_continuity(om *m)
+/* AssembleMdot (AssembleMdotUsingRhieChow.for:262-292, 554-759, 1441-1598, 2033-2075) */
+static void om_assemble_mdot(om *m)
 {
   int N = m->N, F = m->F, B = m->B;
   const fs_case *c = &m->cfg;
-  init_fluxes(m);
-  memset(m->pc, 0, sizeof(double) * N);          /* InitializePressureCorrection */
-  om_flow_in_out(m);                             /* FlowIn, FlowOut, AdjustFlow */
-  /* AssembleMdot (AssembleMdotUsingRhieChow.for:262-292, 554-759) */
   double *pgbar = dz_(3 * (long)F);
   om_interp_grad(m, FS_GI_AVERAGE, m->p, m->pg, pgbar);
   const double *pbx = pgbar, *pby = pgbar + F, *pbz = pgbar + 2 * (long)F;
@@ -847,6 +851,16 @@ void om_assemble_continuity(om *m)
     int i1 = m->bf_own[b];
     m->bu[b] = m->u[i1]; m->bv[b] = m->v[i1]; m->bw[b] = m->w[i1];
   }
+}
+
+void om_assemble_continuity(om *m)
+{
+  int N = m->N, F = m->F, B = m->B;
+  const fs_case *c = &m->cfg;
+  init_fluxes(m);
+  memset(m->pc, 0, sizeof(double) * N);          /* InitializePressureCorrection */
+  om_flow_in_out(m);                             /* FlowIn, FlowOut, AdjustFlow */
+  om_assemble_mdot(m);
   /* AssemblePressureCorrection (AssemblePressureCorrectionFluxes.for:85-164) */
   for (int k = 0; k < F; k++) {
     double du = avgf(m, k, m->du2), dv = avgf(m, k, m->dv2), dw = avgf(m, k, m->dw2);
@@ -913,6 +927,10 @@ void om_correct_continuity(om *m)
   double *mi = dz_(N);
   for (int k = 0; k < F; k++) { mi[m->if_own[k]] += m->mdot[k]; mi[m->if_nbr[k]] -= m->mdot[k]; }
   for (int b = 0; b < B; b++) mi[m->bf_own[b]] += m->bmdot[b];
+  if (c->unsteady) {   /* + d rho/dt V (CalculateContinuityResiduals.for:159-170) */
+    double drhodt = om_drhodt(m);
+    for (int i = 0; i < N; i++) mi[i] = mi[i] + drhodt * m->vol[i];
+  }
   double mx = 0., ov = 0., ab = 0., rms = 0.; int imx = 0;
   for (int i = 0; i < N; i++) {
     ov += mi[i]; ab += fabs(mi[i]);
@@ -1335,6 +1353,7 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
   m->utau = dz_(B); m->yplus = dz_(B); m->uplus = dz_(B); m->dupdyp = dz_(B); m->tauw = dz_(B); m->wallvisc = dz_(B);
   om_wall_distance(m);
   om_initialize_mdot(m);
+  om_transient_init(m);
   return m;
 }
 
@@ -1385,6 +1404,7 @@ void *om_array(om *m, const char *name, long *len, int *is_int)
     {"wdist", m->wdist, N, 0}, {"itau", m->itau, N, 1},
     {"utau", m->utau, B, 0}, {"yplus", m->yplus, B, 0}, {"uplus", m->uplus, B, 0},
     {"dupdyp", m->dupdyp, B, 0}, {"wallvisc", m->wallvisc, B, 0}, {"bprod", m->bprod, B, 0},
+    {"old", m->old, 6*N, 0}, {"oldold", m->oldold, 6*N, 0}, {"bold", m->bold, 6*B, 0},
   };
   for (unsigned q = 0; q < sizeof(t) / sizeof(t[0]); q++)
     if (strcmp(t[q].n, name) == 0) { *len = t[q].len; *is_int = t[q].isint; return t[q].p; }
