@@ -504,11 +504,20 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mdot(ContArgs a) {
   a.pcoef[k] = rhof * geo_diff(a.msd, du2, dv2, dw2, sx, sy, sz, ex, ey, ez, cf, t2x, t2y, t2z);
 }
 
-// specified-velocity inlets: Bmdot = rho*Ub.S (AssembleMdotUsingRhieChow.for:2054-2075)
+// specified-velocity inlets: Bmdot = rho*Ub.S (AssembleMdotUsingRhieChow.for:2054-2075);
+// fully developed outlets: the boundary velocity
 __global__ void k_bmdot_inlet(ContArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= a.B) return;
-  if (a.btype[b] != FS_BC_INLET_VEL) return;
+  const int t = a.btype[b];
+  if (t == FS_BC_OUTLET_FD) {
+    // fully developed outlet velocity (AssembleMdotUsingRhieChow.for:2033-2050); k_flow_in_out
+    // set the same values just before, unless a Crank-Nicolson extrapolation came in between
+    const int i1 = a.bown[b];
+    a.bu_w[b] = a.u[i1]; a.bv_w[b] = a.v[i1]; a.bw_w[b] = a.w[i1];
+    return;
+  }
+  if (t != FS_BC_INLET_VEL) return;
   const int B = a.B;
   a.bmdot[b] = a.rho * (a.bu[b] * a.bsf[b] + a.bv[b] * a.bsf[B + b] + a.bw[b] * a.bsf[2L * B + b]);
 }
