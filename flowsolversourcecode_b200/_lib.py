@@ -84,6 +84,16 @@ class FsMeshIn(C.Structure):
         ("n_faces", C.c_int32), ("face_ptr", C.POINTER(C.c_int32)), ("face_nodes", C.POINTER(C.c_int32)),
         ("owner", C.POINTER(C.c_int32)), ("n_internal", C.c_int32), ("neighbour", C.POINTER(C.c_int32)),
         ("n_patches", C.c_int32), ("patch_start", C.POINTER(C.c_int32)), ("patch_size", C.POINTER(C.c_int32)),
+        ("cell_face_ptr", C.POINTER(C.c_int32)), ("cell_faces", C.POINTER(C.c_int32)),
+        ("cell_node_ptr", C.POINTER(C.c_int32)), ("cell_nodes", C.POINTER(C.c_int32)),
+    ]
+
+
+class FsNeuIn(C.Structure):
+    _fields_ = [
+        ("n_elements", C.c_int32), ("type", C.POINTER(C.c_int32)), ("node_ptr", C.POINTER(C.c_int32)),
+        ("nodes", C.POINTER(C.c_int32)), ("n_sets", C.c_int32), ("set_size", C.POINTER(C.c_int32)),
+        ("bc_element", C.POINTER(C.c_int32)), ("bc_face", C.POINTER(C.c_int32)),
     ]
 
 
@@ -123,6 +133,7 @@ PROTOTYPES = {
     "fs_set_iteration": (C.c_int, [_V, C.c_int]),
     "fs_initialize_mdot": (C.c_int, [_V]),
     "fs_advance_time": (C.c_int, [_V, C.c_double]),
+    "fs_neu_connectivity": (C.c_int, [C.POINTER(FsNeuIn)] + [C.POINTER(C.c_int32)] * 8),
     "fs_get_time": (C.c_int, [_V, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "fs_set_time": (C.c_int, [_V, C.POINTER(C.c_double), C.c_int32]),
     "fs_gradient": (C.c_int, [_V, C.c_int, C.c_int, C.c_int]),
@@ -220,4 +231,11 @@ def mesh_struct(mesh) -> tuple[FsMeshIn, list]:
     m = FsMeshIn(n_nodes=pts.shape[0] // 3, points=dptr(pts), n_faces=ow.shape[0], face_ptr=iptr(fp),
                  face_nodes=iptr(fn), owner=iptr(ow), n_internal=nb.shape[0], neighbour=iptr(nb),
                  n_patches=ps.shape[0], patch_start=iptr(ps), patch_size=iptr(pz))
+    # element-local face order and element node order of a neutral-file mesh
+    for name in ("cell_face_ptr", "cell_faces", "cell_node_ptr", "cell_nodes"):
+        a = getattr(mesh, name, None)
+        if a is not None:
+            a = np.ascontiguousarray(a, np.int32)
+            keep.append(a)
+            setattr(m, name, iptr(a))
     return m, keep

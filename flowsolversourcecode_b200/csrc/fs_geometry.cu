@@ -233,8 +233,13 @@ int fs_geometry_build(fs_ctx *ctx, const fs_mesh_in *mi) {
   // ---- Readit restatement (host, O(N)) ----
   std::vector<int32_t> &ncf = ctx->h_ncf;
   ncf.assign(N, 0);
-  for (int i = 0; i < F; i++) { ncf[mi->owner[i]]++; ncf[mi->neighbour[i]]++; }
-  for (int i = F; i < nf; i++) ncf[mi->owner[i]]++;
+  if (mi->cell_face_ptr) {   // the element-local order of GlobalConnectivity
+    if (!mi->cell_faces || mi->cell_face_ptr[0] != 0) { ctx->err = "cell_faces missing"; return FS_E_MESH; }
+    for (int i = 0; i < N; i++) ncf[i] = mi->cell_face_ptr[i + 1] - mi->cell_face_ptr[i];
+  } else {
+    for (int i = 0; i < F; i++) { ncf[mi->owner[i]]++; ncf[mi->neighbour[i]]++; }
+    for (int i = F; i < nf; i++) ncf[mi->owner[i]]++;
+  }
   int W = 0;
   for (int i = 0; i < N; i++) W = std::max(W, ncf[i]);
   ctx->W = W;
@@ -243,16 +248,41 @@ int fs_geometry_build(fs_ctx *ctx, const fs_mesh_in *mi) {
   ctx->h_own_slot.assign(F, 0);
   ctx->h_nbr_slot.assign(F, 0);
   std::vector<int32_t> cnt(N, 0), slotv((size_t)W * N, -1);
-  for (int k = 0; k < F; k++) {
-    int o = mi->owner[k], nb = mi->neighbour[k];
-    int jo = cnt[o]++, jn = cnt[nb]++;
-    ctx->h_cf[(size_t)jo * N + o] = k; ctx->h_cn[(size_t)jo * N + o] = nb; slotv[(size_t)jo * N + o] = k << 1;
-    ctx->h_cf[(size_t)jn * N + nb] = k; ctx->h_cn[(size_t)jn * N + nb] = o; slotv[(size_t)jn * N + nb] = (k << 1) | 1;
-    ctx->h_own_slot[k] = jo; ctx->h_nbr_slot[k] = jn;
-  }
-  for (int k = F; k < nf; k++) {
-    int o = mi->owner[k], j = cnt[o]++;
-    ctx->h_cf[(size_t)j * N + o] = k; slotv[(size_t)j * N + o] = k << 1;
+  if (mi->cell_face_ptr) {
+    // every interior face once on its owner's and once on its neighbour's list,
+    // every boundary face once on its owner's
+    std::vector<int8_t> seen((size_t)nf, 0);
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < ncf[i]; j++) {
+        int k = mi->cell_faces[mi->cell_face_ptr[i] + j];
+        if (k < 0 || k >= nf) { ctx->err = "cell_faces: face id out of range"; return FS_E_MESH; }
+        int side;
+        if (k < F && mi->owner[k] == i && !(seen[k] & 1)) side = 0;
+        else if (k < F && mi->neighbour[k] == i && !(seen[k] & 2)) side = 1;
+        else if (k >= F && mi->owner[k] == i && !seen[k]) side = 0;
+        else { ctx->err = "cell_faces: face not on this cell or listed twice"; return FS_E_MESH; }
+        seen[k] |= (int8_t)(1 << side);
+        ctx->h_cf[(size_t)j * N + i] = k;
+        slotv[(size_t)j * N + i] = (k << 1) | side;
+        if (k < F) {
+          ctx->h_cn[(size_t)j * N + i] = side ? mi->owner[k] : mi->neighbour[k];
+          (side ? ctx->h_nbr_slot : ctx->h_own_slot)[k] = j;
+        }
+      }
+    for (int k = 0; k < nf; k++)
+      if (seen[k] != (k < F ? 3 : 1)) { ctx->err = "cell_faces: a face is missing from its cells"; return FS_E_MESH; }
+  } else {
+    for (int k = 0; k < F; k++) {
+      int o = mi->owner[k], nb = mi->neighbour[k];
+      int jo = cnt[o]++, jn = cnt[nb]++;
+      ctx->h_cf[(size_t)jo * N + o] = k; ctx->h_cn[(size_t)jo * N + o] = nb; slotv[(size_t)jo * N + o] = k << 1;
+      ctx->h_cf[(size_t)jn * N + nb] = k; ctx->h_cn[(size_t)jn * N + nb] = o; slotv[(size_t)jn * N + nb] = (k << 1) | 1;
+      ctx->h_own_slot[k] = jo; ctx->h_nbr_slot[k] = jn;
+    }
+    for (int k = F; k < nf; k++) {
+      int o = mi->owner[k], j = cnt[o]++;
+      ctx->h_cf[(size_t)j * N + o] = k; slotv[(size_t)j * N + o] = k << 1;
+    }
   }
   ctx->h_fown.assign(mi->owner, mi->owner + F);
   ctx->h_fnbr.assign(mi->neighbour, mi->neighbour + F);
@@ -267,10 +297,16 @@ int fs_geometry_build(fs_ctx *ctx, const fs_mesh_in *mi) {
       ctx->h_bset[b] = s; ctx->h_btype[b] = ctx->cfg.patch_type[s];
     }
   }
-  // ordered cell node lists (ReadFoamMesh.f90:430-458)
+  // ordered cell node lists (ReadFoamMesh.f90:430-458), or as given (ListOfElementNodes of a neutral file)
   std::vector<int32_t> cptr(N + 1, 0), cnodes;
   cnodes.reserve((size_t)N * 8);
-  for (int i = 0; i < N; i++) {
+  if (mi->cell_node_ptr) {
+    if (!mi->cell_nodes || mi->cell_node_ptr[0] != 0) { ctx->err = "cell_nodes missing"; return FS_E_MESH; }
+    cptr.assign(mi->cell_node_ptr, mi->cell_node_ptr + N + 1);
+    cnodes.assign(mi->cell_nodes, mi->cell_nodes + cptr[N]);
+    for (int32_t nd : cnodes) if (nd < 0 || nd >= mi->n_nodes) { ctx->err = "cell node out of range"; return FS_E_MESH; }
+  }
+  for (int i = 0; i < N && !mi->cell_node_ptr; i++) {
     cptr[i] = (int32_t)cnodes.size();
     size_t start = cnodes.size();
     for (int j = 0; j < ncf[i]; j++) {
@@ -284,7 +320,7 @@ int fs_geometry_build(fs_ctx *ctx, const fs_mesh_in *mi) {
       }
     }
   }
-  cptr[N] = (int32_t)cnodes.size();
+  if (!mi->cell_node_ptr) cptr[N] = (int32_t)cnodes.size();
   build_colors(ctx);
 
   // ---- upload connectivity ----

@@ -208,7 +208,33 @@ typedef struct fs_mesh_in {
   int32_t        n_patches;
   const int32_t *patch_start; /* n_patches, face index of first patch face */
   const int32_t *patch_size;  /* n_patches */
+  /* Optional (NULL: the polyMesh order of Readit, ReadFoamMesh.f90:311-458).
+   * A mesh built by GlobalConnectivity (Gambit neutral files) keeps each
+   * element's faces in its local face order (NGlobalEFaces,
+   * GlobalGridConnectivity.for:125-345) and its nodes in file order
+   * (ListOfElementNodes, ReadGridFromNeutralFile.for): both set the order of
+   * the per-cell sums, so they are passed as given.  fs_neu_connectivity
+   * returns them. */
+  const int32_t *cell_face_ptr; /* n_cells+1 offsets into cell_faces */
+  const int32_t *cell_faces;    /* face ids, each interior face once per side, each boundary face once */
+  const int32_t *cell_node_ptr; /* n_cells+1 offsets into cell_nodes */
+  const int32_t *cell_nodes;
 } fs_mesh_in;
+
+/* Gambit neutral-file elements (ReadNeutralGrid, ReadGridFromNeutralFile.for)
+ * for fs_neu_connectivity.  0-based node and element ids; bc_face is the
+ * element-local face, 0-based, in the face numbering of GlobalConnectivity
+ * (GlobalGridConnectivity.for:21-120). */
+typedef struct fs_neu_in {
+  int32_t        n_elements;
+  const int32_t *type;          /* NTypeGeometry: 4 brick, 5 wedge, 6 tetrahedron, 7 pyramid */
+  const int32_t *node_ptr;      /* n_elements+1 offsets into nodes */
+  const int32_t *nodes;         /* element nodes in file order */
+  int32_t        n_sets;        /* NumberOfBCSets */
+  const int32_t *set_size;      /* NBCDataRecords per set */
+  const int32_t *bc_element;    /* NElementBC, sets concatenated */
+  const int32_t *bc_face;       /* NElementBCFace */
+} fs_neu_in;
 
 /* Residual block (Residuals1.F90), indexed by NF-1 for NF=1..5. */
 typedef struct fs_residuals {
@@ -268,6 +294,21 @@ int fs_set_iteration(fs_ctx *ctx, int n_iter);
  * Bmdot from the current cell and boundary velocities, for a caller that set
  * an initial field with fs_set_field (fs_create already ran it once). */
 int fs_initialize_mdot(fs_ctx *ctx);
+
+/* GlobalConnectivity (GlobalGridConnectivity.for:4-523) in O(N) with a hash
+ * of sorted face nodes instead of the O(N^2) search, the same face order:
+ * elements in order, local faces in order; a face not on a boundary record
+ * and not seen before becomes the next interior face (nodes in the creating
+ * element's local order, owner = lower element id); boundary faces follow,
+ * set by set, record by record.  Host-only (no GPU).  Outputs, sized by the
+ * caller for F_max = sum of local faces over elements: face_ptr (F_max+1),
+ * face_nodes (4 F_max), owner (F_max), neighbour (F_max), cell_face_ptr
+ * (n_elements+1), cell_faces (F_max); n_internal and n_faces are written.
+ * Returns FS_E_MESH for an unknown element type, a bad boundary record or a
+ * face shared by more than two elements. */
+int fs_neu_connectivity(const fs_neu_in *in, int32_t *n_internal, int32_t *n_faces,
+                        int32_t *face_ptr, int32_t *face_nodes, int32_t *owner, int32_t *neighbour,
+                        int32_t *cell_face_ptr, int32_t *cell_faces);
 
 /* Time-step prologue of the unsteady loop (MainProgram.for:184-245): the
  * first step of 'cranknicolson2'/'adamsmoulton' runs as 'euler'; from the

@@ -56,6 +56,8 @@ def load():
         lib.om_residuals_turb.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         lib.om_initialize_mdot.argtypes = [C.c_void_p]
         lib.om_turb_production.argtypes = [C.c_void_p]
+        lib.om_neu_connectivity_literal.restype = C.c_int
+        lib.om_neu_connectivity_literal.argtypes = [C.c_void_p] + [C.POINTER(C.c_int32)] * 8
         lib.om_advance_time.argtypes = [C.c_void_p, C.c_double]
         lib.om_get_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         lib.om_set_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]

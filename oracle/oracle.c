@@ -99,6 +99,7 @@ static double *dz_(long n) { return (double *)calloc((size_t)(n > 0 ? n : 1), si
 static void om_momentum_wall_functions(om *m);   /* oracle_turb.inc */
 static int *iz_(long n) { return (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int)); }
 #include "oracle_transient.inc"
+#include "oracle_neutral.inc"
 
 /* ===================================================================== */
 /*  Connectivity: Readit (GridAndGeometry/ReadFoamMesh.f90:277-660)       */
@@ -123,24 +124,33 @@ static void om_connectivity(om *m, const fs_mesh_in *mi)
       m->bf_own[k] = mi->owner[F + k]; m->bf_set[k] = s;
     }
   }
-  /* NumbOfElementFaces (ReadFoamMesh.f90:311-322) */
+  /* NumbOfElementFaces (ReadFoamMesh.f90:311-322); a neutral-file mesh
+   * gives its element-local face lists (NGlobalEFaces of GlobalConnectivity) */
   m->ncf = iz_(N);
-  for (int i = 0; i < F; i++) { m->ncf[mi->owner[i]]++; m->ncf[mi->neighbour[i]]++; }
-  for (int i = F; i < nf; i++) m->ncf[mi->owner[i]]++;
+  if (mi->cell_face_ptr) for (int i = 0; i < N; i++) m->ncf[i] = mi->cell_face_ptr[i + 1] - mi->cell_face_ptr[i];
+  else {
+    for (int i = 0; i < F; i++) { m->ncf[mi->owner[i]]++; m->ncf[mi->neighbour[i]]++; }
+    for (int i = F; i < nf; i++) m->ncf[mi->owner[i]]++;
+  }
   int W = -1;
   for (int i = 0; i < N; i++) if (m->ncf[i] > W) W = m->ncf[i];
   m->W = W;
   /* NGlobalEFaces: interior faces in file order, then boundary faces (:326-342) */
   m->cf = iz_((long)W * N); m->cn = iz_((long)W * N);
   for (long q = 0; q < (long)W * N; q++) { m->cf[q] = -1; m->cn[q] = -1; }
-  int *cnt = iz_(N);
-  for (int i = 0; i < F; i++) {
-    int o = mi->owner[i], nb = mi->neighbour[i];
-    m->cf[(long)cnt[o] * N + o] = i; cnt[o]++;
-    m->cf[(long)cnt[nb] * N + nb] = i; cnt[nb]++;
+  if (mi->cell_face_ptr) {
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < m->ncf[i]; j++) m->cf[(long)j * N + i] = mi->cell_faces[mi->cell_face_ptr[i] + j];
+  } else {
+    int *cnt = iz_(N);
+    for (int i = 0; i < F; i++) {
+      int o = mi->owner[i], nb = mi->neighbour[i];
+      m->cf[(long)cnt[o] * N + o] = i; cnt[o]++;
+      m->cf[(long)cnt[nb] * N + nb] = i; cnt[nb]++;
+    }
+    for (int i = F; i < nf; i++) { int o = mi->owner[i]; m->cf[(long)cnt[o] * N + o] = i; cnt[o]++; }
+    free(cnt);
   }
-  for (int i = F; i < nf; i++) { int o = mi->owner[i]; m->cf[(long)cnt[o] * N + o] = i; cnt[o]++; }
-  free(cnt);
   /* iOwnerNeighbor / iNeighborOwner / ElementNeighbor (:597-635) */
   m->own_slot = iz_(F); m->nbr_slot = iz_(F);
   for (int i = 0; i < F; i++) {
@@ -154,6 +164,12 @@ static void om_connectivity(om *m, const fs_mesh_in *mi)
    * face in face order, then new nodes of later faces.  The first pass
    * (:380-410) only counts unique nodes, which the second pass reproduces. */
   m->cnode_ptr = iz_(N + 1);
+  if (mi->cell_node_ptr) {   /* ListOfElementNodes as read from a neutral file */
+    memcpy(m->cnode_ptr, mi->cell_node_ptr, sizeof(int) * (N + 1));
+    m->cnodes = iz_(mi->cell_node_ptr[N]);
+    memcpy(m->cnodes, mi->cell_nodes, sizeof(int) * mi->cell_node_ptr[N]);
+    return;
+  }
   int cap = 0;
   for (int i = 0; i < N; i++) {
     int c = 0;

@@ -41,6 +41,9 @@ void   om_residuals(om *m, double out[20]);    /* ResorAbs/Max/RMS/Scaled x5 */
 int    om_lin_iters(om *m, int nf);            /* linear iterations last solve of NF */
 void   om_residuals_turb(om *m, double out[8]);/* abs/max/rms/scaled of k, epsilon (NF 8, 9) */
 void   om_initialize_mdot(om *m);              /* CalculateInitialmdot from the current fields */
+int    om_neu_connectivity_literal(const fs_neu_in *in, int *n_internal, int *n_faces, int *face_ptr,
+                                   int *face_nodes, int *owner, int *neighbour, int *cell_face_ptr,
+                                   int *cell_faces);   /* GlobalConnectivity, O(N^2) as written */
 void   om_advance_time(om *m, double dt_next);  /* time-step prologue (MainProgram.for:184-245) */
 void   om_get_time(om *m, double t[4], int *ndt);        /* time, dt, dtOld, dtOldOld; ndt */
 void   om_set_time(om *m, const double t[4], int ndt);
