@@ -22,7 +22,8 @@ __global__ void k_initial_mdot(int N, int F, int B, double rho, const int32_t *f
   } else if (t < (long)F + B) {
     int b = (int)(t - F), ty = btype[b];
     if (ty == FS_BC_WALL_NOSLIP || ty == FS_BC_WALL_SLIP) bmdot[b] = 0.;
-    else bmdot[b] = rho * (bsf[b] * bu[b] + bsf[B + b] * bv[b] + bsf[2L * B + b] * bw[b]);
+    else if (ty != FS_BC_INLET_MASS)   // a mass-flow inlet's Bmdot is specified (InitializaMdot.for:55)
+      bmdot[b] = rho * (bsf[b] * bu[b] + bsf[B + b] * bv[b] + bsf[2L * B + b] * bw[b]);
   }
 }
 
@@ -152,7 +153,7 @@ static void free_all(fs_ctx *c) {
                   c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky, c->sysx,
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
                   c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP,
-                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm, c->d_bset, c->flow};
+                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm, c->d_bset, c->flow, c->bdir};
   for (void *p : ptrs) if (p) cudaFree(p);
 }
 
@@ -229,6 +230,35 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (size_t b = 0; b < B; b++) {
     int s = ctx->h_bset[b];
     if (ctx->cfg.patch_type[s] == FS_BC_OUTLET_SP) hp[b] = ctx->cfg.patch_pressure[s];
+  }
+  // 'specifiedmassflowrate' inlets: Bmdot = -mdot |S_f| / sum |S| in face order, and the
+  // velocity AssembleMdot derives from it (AssembleMdotUsingRhieChow.for:2077-2100)
+  std::vector<double> hm(B, 0.);
+  bool has_mass = false;
+  for (int s = 0; s < ctx->cfg.n_patches; s++) has_mass |= ctx->cfg.patch_type[s] == FS_BC_INLET_MASS;
+  if (has_mass && B) {
+    std::vector<double> hfa(B), hsf(3 * B), hd(3 * B, 0.);
+    if (cudaStreamSynchronize(ctx->st) != cudaSuccess ||
+        cudaMemcpy(hfa.data(), ctx->bfa, sizeof(double) * B, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hsf.data(), ctx->bsf, sizeof(double) * 3 * B, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(FS_E_CUDA);
+    for (int s = 0; s < ctx->cfg.n_patches; s++) {
+      if (ctx->cfg.patch_type[s] != FS_BC_INLET_MASS) continue;
+      const int b0 = ctx->h_bset_start[s], nb = ctx->h_bset_n[s];
+      const double *d = ctx->cfg.patch_vel[s], rho = ctx->cfg.rho;
+      double area = 0.;
+      for (int j = 0; j < nb; j++) area = area + hfa[b0 + j];
+      for (int j = 0; j < nb; j++) {
+        const size_t b = b0 + j;
+        for (int q = 0; q < 3; q++) hd[3 * b + q] = d[q];
+        hm[b] = -(ctx->cfg.patch_mass_flow[s] * hfa[b] / area);
+        const double vm = hm[b] / (rho * (d[0] * hsf[b] + d[1] * hsf[B + b] + d[2] * hsf[2 * B + b]));
+        hb[b] = vm * d[0]; hb[B + b] = vm * d[1]; hb[2 * B + b] = vm * d[2];
+      }
+    }
+    if (cudaMalloc(&ctx->bdir, sizeof(double) * 3 * B) != cudaSuccess) return fail(FS_E_NOMEM);
+    cudaMemcpyAsync(ctx->bdir, hd.data(), sizeof(double) * 3 * B, cudaMemcpyHostToDevice, ctx->st);
+    cudaMemcpyAsync(ctx->bmdot, hm.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
   }
   if (B) {
     cudaMemcpyAsync(ctx->bp, hp.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);

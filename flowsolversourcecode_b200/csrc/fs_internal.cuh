@@ -19,6 +19,11 @@
 #include <vector>
 #include <cstdint>
 
+// 'specifiedvelocity' and 'specifiedmassflowrate' inlets share the momentum,
+// p' and k-epsilon treatment (AssembleIsotropicDiffusion.for:254-300,
+// AssembleConvection.for:260-300, AssemblePressureCorrectionFluxes.for:545-575)
+__host__ __device__ inline bool fs_is_inlet(int t) { return t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS; }
+
 #define FS_BLOCK 256
 #ifndef FS_COOP_BLOCK
 #define FS_COOP_BLOCK 256            // threads per CTA of the persistent cooperative solvers
@@ -83,6 +88,7 @@ struct fs_ctx {
   double *pcoef = nullptr;                                         // F: p' face coefficient
   double *bpcoef = nullptr;                                        // B: p' coefficient of pressure outlets
   bool has_sp = false;                                             // a 'specifiedstaticpressure' outlet exists
+  double *bdir = nullptr;                                          // 3B: direction of 'specifiedmassflowrate' inlets
   // krylov work (device)
   double *kx = nullptr, *kr = nullptr, *kr0 = nullptr, *kp = nullptr, *kv = nullptr, *ks = nullptr, *kt = nullptr;
   double *kz = nullptr, *ky = nullptr;   // preconditioned vectors (AMG-BiCGSTAB)

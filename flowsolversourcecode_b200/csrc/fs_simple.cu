@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
           }
           fcf = fcl;
           tf = fcl * phi + 0. * bp + fvl;
-        } else if (t == FS_BC_INLET_VEL) {
+        } else if (fs_is_inlet(t)) {
           double fcl = gamf * a.bgdiff[b], ffl = -gamf * a.bgdiff[b];
           double fvl = -(gamf * (bfg[b] * a.btf[b] + bfg[B + b] * a.btf[B + b] + bfg[B2 + b] * a.btf[B2 + b]));
           fcf = fcl;
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
         double sc = comp == 0 ? bsx : comp == 1 ? bsy : bsz;
         tf = tf + -(M23 * gamf * div * sc);
       }
-      if (t == FS_BC_INLET_VEL) {
+      if (fs_is_inlet(t)) {
         double bm = a.bmdot[b];
         double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
         fcf = fcf + fcl;
@@ -423,6 +423,7 @@ struct ContArgs {
   const double *rhok, *drk;   // k-epsilon: 2/3 rho k and its gradient (3N), nullptr when laminar
   // pressure outlets
   double *bpcoef, *bu_w, *bv_w, *bw_w;
+  const double *bdir;   // 3B direction of 'specifiedmassflowrate' inlets (nullptr: none)
   const double *bug, *bvg, *bwg, *bdv, *bpg, *bp, *brhok, *bdrk;
   double *ac, *anb, *bc;
   double *red; int nblk;
@@ -505,7 +506,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mdot(ContArgs a) {
 }
 
 // specified-velocity inlets: Bmdot = rho*Ub.S (AssembleMdotUsingRhieChow.for:2054-2075);
-// fully developed outlets: the boundary velocity
+// mass-flow inlets and fully developed outlets: the boundary velocity
 __global__ void k_bmdot_inlet(ContArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= a.B) return;
@@ -517,8 +518,15 @@ __global__ void k_bmdot_inlet(ContArgs a) {
     a.bu_w[b] = a.u[i1]; a.bv_w[b] = a.v[i1]; a.bw_w[b] = a.w[i1];
     return;
   }
-  if (t != FS_BC_INLET_VEL) return;
   const int B = a.B;
+  if (t == FS_BC_INLET_MASS) {
+    // velocity from the specified Bmdot along the given direction (AssembleMdotUsingRhieChow.for:2077-2100)
+    const double dx = a.bdir[3L * b], dy = a.bdir[3L * b + 1], dz = a.bdir[3L * b + 2];
+    const double vm = a.bmdot[b] / (a.rho * (dx * a.bsf[b] + dy * a.bsf[B + b] + dz * a.bsf[2L * B + b]));
+    a.bu_w[b] = vm * dx; a.bv_w[b] = vm * dy; a.bw_w[b] = vm * dz;
+    return;
+  }
+  if (t != FS_BC_INLET_VEL) return;
   a.bmdot[b] = a.rho * (a.bu[b] * a.bsf[b] + a.bv[b] * a.bsf[B + b] + a.bw[b] * a.bsf[2L * B + b]);
 }
 
@@ -650,6 +658,12 @@ __global__ void k_bcorr(CorrArgs a) {
     double rpc = (a.ref_cell >= 0) ? a.pc[a.ref_cell] : 0.;
     if (a.set_ref) rpc = 0.;
     a.bp[b] = a.bp[b] + a.urfp * (a.bpc[b] - rpc);
+    if (t == FS_BC_INLET_MASS) {   // CorrectBoundarymdot: the velocity only (CorrectMdotandVelocity.for:165-175)
+      const int N = a.N;
+      a.bu[b] = a.bu[b] - a.du2[i1] * a.pcg[i1];
+      a.bv[b] = a.bv[b] - a.dv2[i1] * a.pcg[N + i1];
+      a.bw[b] = a.bw[b] - a.dw2[i1] * a.pcg[2L * N + i1];
+    }
   }
   if (t == FS_BC_SYMMETRY || t == FS_BC_WALL_SLIP) {
     double nx = a.bnf[b], ny = a.bnf[B + b], nz = a.bnf[B2 + b];
@@ -883,7 +897,7 @@ static ContArgs cont_args(fs_ctx *ctx) {
   a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bsf = ctx->bsf;
   fs_turb_rhok_ptrs(ctx, &a.rhok, &a.drk);
   fs_turb_brhok_ptrs(ctx, &a.brhok, &a.bdrk);
-  a.bpcoef = ctx->bpcoef; a.bu_w = ctx->bu; a.bv_w = ctx->bv; a.bw_w = ctx->bw;
+  a.bpcoef = ctx->bpcoef; a.bu_w = ctx->bu; a.bv_w = ctx->bv; a.bw_w = ctx->bw; a.bdir = ctx->bdir;
   a.bug = ctx->bug; a.bvg = ctx->bvg; a.bwg = ctx->bwg; a.bdv = ctx->bdv; a.bpg = ctx->bpg; a.bp = ctx->bp;
   a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc; a.red = ctx->red; a.nblk = fs_grid(ctx->N);
   return a;
@@ -959,7 +973,7 @@ int fs_continuity_correct(fs_ctx *ctx) {
   FS_LAUNCH_CHECK();
   InletRanges ir{};
   for (int s = 0; s < ctx->NS; s++)
-    if (c.patch_type[s] == FS_BC_INLET_VEL) { ir.start[ir.n] = ctx->h_bset_start[s]; ir.cnt[ir.n] = ctx->h_bset_n[s]; ir.n++; }
+    if (fs_is_inlet(c.patch_type[s])) { ir.start[ir.n] = ctx->h_bset_start[s]; ir.cnt[ir.n] = ctx->h_bset_n[s]; ir.n++; }
   double *d_in = nullptr;
   if (ir.n) {
     // inlet mass flow, used only through ResorScaled(5); stays on the device

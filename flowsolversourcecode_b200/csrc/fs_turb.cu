@@ -150,7 +150,7 @@ __global__ void k_rhok(int N, int B, double rho, const double *tke, const double
 // CalculateInletTurbulence, 'specifiedil' (CalculateTurbulenceAtBoundary.for:20-40)
 __global__ void k_inlet_turb(TurbArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= a.B || a.btype[b] != FS_BC_INLET_VEL) return;
+  if (b >= a.B || !fs_is_inlet(a.btype[b])) return;
   int s = a.bset[b];
   double bv2 = a.bu[b] * a.bu[b] + a.bv[b] * a.bv[b] + a.bw[b] * a.bw[b];
   double in2 = a.in_i[s] * a.in_i[s];
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
         double bm = a.bmdot[b];
         ed = ed + bm;
         double fcf = 0., tf = 0.;
-        if (t == FS_BC_INLET_VEL) {
+        if (fs_is_inlet(t)) {
           double gamf = mu + a.bmut[b] / sig;          // BeDiffCoefficient of the equation
           double gd = a.bgdiff[b];
           double fcl = gamf * gd, ffl = -gamf * gd;
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
           fcf = fcl;
           tf = fcl * ps + ffl * a.bphi[b] + fvl;
         }
-        if (t == FS_BC_INLET_VEL || t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {
+        if (fs_is_inlet(t) || t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {
           double cc = fmax(bm, 0.), cn_ = -fmax(-bm, 0.);
           fcf = fcf + cc;
           tf = tf + (cc * ps + cn_ * a.bphi[b]);
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(1024) k_flow_in_out(FlowArgs a) {
   const int B = a.B;
   double s = 0.;
   for (int q = 0; q < a.NS; q++)
-    if (a.ptype[q] == FS_BC_INLET_VEL)
+    if (fs_is_inlet(a.ptype[q]))   // CalculateFlowIn.for:37-48
       for (int j = threadIdx.x; j < a.pn[q]; j += blockDim.x) s = s + a.bmdot[a.pstart[q] + j];
   s = block_sum(s, sh);
   if (threadIdx.x == 0) { a.flow[0] = s; bcast = s; }

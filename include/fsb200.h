@@ -86,7 +86,9 @@ enum fs_bc {
   FS_BC_SYMMETRY    = 2,   /* 'symmetry' */
   FS_BC_INLET_VEL   = 3,   /* 'inlet','specifiedvelocity' */
   FS_BC_OUTLET_FD   = 4,   /* 'outlet','fullydeveloped' */
-  FS_BC_OUTLET_SP   = 5    /* 'outlet','specifiedstaticpressure' (patch_pressure) */
+  FS_BC_OUTLET_SP   = 5,   /* 'outlet','specifiedstaticpressure' (patch_pressure) */
+  FS_BC_INLET_MASS  = 6    /* 'inlet','specifiedmassflowrate': patch_vel is the velocity
+                            * direction (xVeldirection...), patch_mass_flow the inflow */
 };
 
 /* ---------------------------------------------------------- scheme enums */
@@ -184,6 +186,10 @@ typedef struct fs_case {
   int    unsteady;
   int    transient_scheme;       /* fs_transient */
   double dt;                     /* first time step */
+  /* 'specifiedmassflowrate' inlets: mass flow into the domain per patch,
+   * spread over the faces by area as the initial Bmdot (the reference leaves
+   * the face values to DescribeProblem: set FS_F_BMDOT to override) */
+  double patch_mass_flow[FS_MAX_PATCHES];
 } fs_case;
 
 /* TransientScheme values (AssembleTheTransientTerm.for:52,124,199,290). */

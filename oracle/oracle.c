@@ -28,6 +28,10 @@
 #define OM_EPS9  ((double)1.e-9f)
 #define OM_TINY  1.0e-15              /* Constants1.F90: tiny=1.d-15 */
 #define OM_TWOTHIRD ((double)(2.0f / 3.0f))   /* Constants1.F90:12 TwoThird, a REAL(4) literal */
+/* 'specifiedvelocity' and 'specifiedmassflowrate' inlets take the same
+ * momentum, p' and k-epsilon treatment (AssembleIsotropicDiffusion.for:254-300,
+ * AssembleConvection.for:260-300, AssemblePressureCorrectionFluxes.for:545-575) */
+#define OM_INLET(t) ((t) == FS_BC_INLET_VEL || (t) == FS_BC_INLET_MASS)
 
 struct om {
   fs_case cfg;
@@ -83,6 +87,7 @@ struct om {
   double *s11, *s12, *s13, *s22, *s23, *s33;
   double *rhok, *brhok, *drk, *bdrk;        /* MinusTwoThirdsRhoK */
   double *wdist; int *itau;                 /* WallDistance, iTau (boundary index) */
+  double *bdir;                             /* xVeldirection.. of 'specifiedmassflowrate' inlets [3B] */
   double *utau, *yplus, *uplus, *dupdyp, *tauw, *wallvisc;   /* per wall face */
   /* BICGSTAB_OMP persistent storage (SparseMatricesVariables) */
   int csr_built; long *csr_ptr; int *csr_j; int *csr_slot; double *csr_val;
@@ -592,7 +597,7 @@ void om_assemble_momentum(om *m, int comp)
         else { fcl = 2. * gamf * area * (nz * nz) / dN; fvl = -((-2. * gamf * area / dN) * (m->u[i1] * nx + m->v[i1] * ny) * nz); }
         m->fcf[i4] += fcl; m->fvf[i4] += fvl;
         m->ftf[i4] += fcl * fi[i1] + 0. * bfi[b] + fvl;
-      } else if (t == FS_BC_INLET_VEL) {   /* :254-285 */
+      } else if (OM_INLET(t)) {   /* :254-300 */
         const double *bgx = bfg, *bgy = bfg + B, *bgz = bfg + 2 * (long)B;
         double fcl = gamf * m->bgdiff[b], ffl = -gamf * m->bgdiff[b];
         double fvl = -(gamf * (bgx[b] * m->bTx[b] + bgy[b] * m->bTy[b] + bgz[b] * m->bTz[b]));
@@ -670,7 +675,7 @@ void om_assemble_momentum(om *m, int comp)
   /* boundary convection (AssembleConvection.for:182-580): inlet specified velocity, outlet FD */
   for (int b = 0; b < B; b++) {
     int i1 = m->bf_own[b], t = m->btype[b]; long i4 = F + b;
-    if (t == FS_BC_INLET_VEL) {
+    if (OM_INLET(t)) {
       double fcl = fmax(m->bmdot[b], 0.), ffl = -fmax(-m->bmdot[b], 0.);
       m->fcf[i4] += fcl; m->fff[i4] += ffl; m->ftf[i4] += fcl * fi[i1] + ffl * bfi[b];
     } else if (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {   /* :421-448 the same for both */
@@ -761,7 +766,7 @@ static void om_flow_in_out(om *m)
   /* FlowOut/AdjustFlow return at once unless every outlet is fully developed */
   if (nfd == 0 || other) return;
   m->mdot_in = 0.;
-  for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_INLET_VEL)
+  for (int s = 0; s < NS; s++) if (OM_INLET(c->patch_type[s]))   /* CalculateFlowIn.for:37-48 */
     for (int j = 0; j < m->bset_n[s]; j++) m->mdot_in = m->mdot_in + m->bmdot[m->bset_start[s] + j];
   for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_FD) {
     m->mdot1[s] = 0.;
@@ -867,6 +872,13 @@ static void om_assemble_mdot(om *m)
     int i1 = m->bf_own[b];
     m->bu[b] = m->u[i1]; m->bv[b] = m->v[i1]; m->bw[b] = m->w[i1];
   }
+  /* 'specifiedmassflowrate' inlet velocity from Bmdot along the given
+   * direction (AssembleMdotUsingRhieChow.for:2077-2100) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_MASS) {
+    const double *d = m->bdir + 3L * b;
+    double vm = m->bmdot[b] / (c->rho * (d[0] * m->bsx[b] + d[1] * m->bsy[b] + d[2] * m->bsz[b]));
+    m->bu[b] = vm * d[0]; m->bv[b] = vm * d[1]; m->bw[b] = vm * d[2];
+  }
 }
 
 void om_assemble_continuity(om *m)
@@ -931,12 +943,19 @@ void om_correct_continuity(om *m)
     m->bv[b] = m->bv[b] - m->dv2[i1] * m->pcg[N + i1];
     m->bw[b] = m->bw[b] - m->dw2[i1] * m->pcg[2L * N + i1];
   }
+  /* CorrectBoundarymdot, 'specifiedmassflowrate' inlets: velocity only (CorrectMdotandVelocity.for:165-175) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_MASS) {
+    int i1 = m->bf_own[b];
+    m->bu[b] = m->bu[b] - m->du2[i1] * m->pcg[i1];
+    m->bv[b] = m->bv[b] - m->dv2[i1] * m->pcg[N + i1];
+    m->bw[b] = m->bw[b] - m->dw2[i1] * m->pcg[2L * N + i1];
+  }
   /* UpdateBoundaryPressure (CorrectPressure.for:49-190): walls and symmetry */
   for (int b = 0; b < B; b++) {
     int t = m->btype[b], i1 = m->bf_own[b];
     if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY)
       m->bp[b] = m->p[i1] + m->bpg[b] * m->bdx[b] + m->bpg[B + b] * m->bdy[b] + m->bpg[2 * (long)B + b] * m->bdz[b];
-    else if (t == FS_BC_INLET_VEL || t == FS_BC_OUTLET_FD)
+    else if (OM_INLET(t) || t == FS_BC_OUTLET_FD)   /* :120-138 */
       m->bp[b] = m->bp[b] + c->urf_pressure * (m->bpc[b] - rpc);
   }
   /* CalculateResidualsContinuity (CalculateContinuityResiduals.for:130-235) */
@@ -957,7 +976,7 @@ void om_correct_continuity(om *m)
   m->rmax[4] = mx; m->rabs[4] = ab; m->rrms[4] = sqrt(rms / N);
   m->overall_imbalance = ov; m->imax_imbalance = imx;
   double min_ = 0.;
-  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_VEL) min_ += m->bmdot[b];
+  for (int b = 0; b < B; b++) if (OM_INLET(m->btype[b])) min_ += m->bmdot[b];   /* every 'inlet' face (:195-203) */
   m->rscl[4] = (min_ == 0.) ? 0. : m->rmax[4] / fabs(min_);
   free(mi);
   /* UpdateSymmetry (SymmetryAndAxisBoundary.for:4-33), UpdateSlipWallBoundary */
@@ -1302,6 +1321,7 @@ void om_initialize_mdot(om *m)
   }
   for (int b = 0; b < m->B; b++) {
     if (m->btype[b] == FS_BC_WALL_NOSLIP || m->btype[b] == FS_BC_WALL_SLIP) m->bmdot[b] = 0.;
+    else if (m->btype[b] == FS_BC_INLET_MASS) continue;   /* specified, not from the velocity (InitializaMdot.for:55) */
     else m->bmdot[b] = cfg->rho * (m->bsx[b] * m->bu[b] + m->bsy[b] * m->bv[b] + m->bsz[b] * m->bw[b]);
   }
 }
@@ -1368,6 +1388,20 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
   m->wdist = dz_(N); m->itau = iz_(N);
   m->utau = dz_(B); m->yplus = dz_(B); m->uplus = dz_(B); m->dupdyp = dz_(B); m->tauw = dz_(B); m->wallvisc = dz_(B);
   om_wall_distance(m);
+  /* 'specifiedmassflowrate' inlets: direction per face, Bmdot = -mdot |S_f| / sum |S| in face order */
+  m->bdir = dz_(3L * B);
+  for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_INLET_MASS) {
+    double area = 0.;
+    for (int j = 0; j < m->bset_n[s]; j++) area = area + m->bfa[m->bset_start[s] + j];
+    for (int j = 0; j < m->bset_n[s]; j++) {
+      int b = m->bset_start[s] + j;
+      const double *d = m->bdir + 3L * b;
+      for (int q = 0; q < 3; q++) m->bdir[3L * b + q] = cfg->patch_vel[s][q];
+      m->bmdot[b] = -(cfg->patch_mass_flow[s] * m->bfa[b] / area);
+      double vm = m->bmdot[b] / (cfg->rho * (d[0] * m->bsx[b] + d[1] * m->bsy[b] + d[2] * m->bsz[b]));
+      m->bu[b] = vm * d[0]; m->bv[b] = vm * d[1]; m->bw[b] = vm * d[2];
+    }
+  }
   om_initialize_mdot(m);
   om_transient_init(m);
   return m;

@@ -1,0 +1,120 @@
+"""'specifiedmassflowrate' inlets (inletTypeM, AssembleMdotUsingRhieChow.for:2077-2100,
+CorrectMdotandVelocity.for:165-175, InitializaMdot.for:55, CalculateFlowIn.for:37-48):
+the restatement's invariants on the step case (CPU) and the GPU path against it."""
+
+import numpy as np
+import pytest
+
+from flowsolversourcecode_b200 import case as cs
+
+
+def _tight(**kw):
+    kw.setdefault("solver_mom", "bicgs")
+    kw.setdefault("solver_cont", "bicgs")
+    kw.setdefault("solver_turb", "bicgs")
+    kw.setdefault("krylov_tol", 1e-13)
+    kw.setdefault("krylov_maxit", 400)
+    return kw
+
+
+def _mass_inlet(mesh, case, u=1.0):
+    """The step's inlet as a mass-flow inlet carrying rho u A along +x."""
+    s = mesh.patch("inlet")
+    case.patches["inlet"] = ("mass_inlet", (1.0, 0.0, 0.0), case.rho * u * _patch_area(mesh, s))
+
+
+def _patch_area(mesh, s):
+    pts = mesh.points
+    area = 0.0
+    for f in range(int(mesh.patch_start[s]), int(mesh.patch_start[s] + mesh.patch_size[s])):
+        p = pts[mesh.face_nodes[mesh.face_ptr[f]:mesh.face_ptr[f + 1]]]
+        area += 0.5 * np.linalg.norm(np.cross(p[2] - p[0], p[3] - p[1]))
+    return area
+
+
+def _setup(obj, mesh, case, seed=0):
+    for k, v in cs.bfs_initial_state(mesh, case, seed=seed).items():
+        if k not in ("bu", "bv", "bw"):   # the inlet velocity follows from Bmdot
+            obj.set(k, v)
+    obj.initialize_mdot()
+
+
+def _inlet(mesh):
+    s = mesh.patch("inlet")
+    b0 = int(mesh.patch_start[s]) - mesh.n_internal
+    return slice(b0, b0 + int(mesh.patch_size[s]))
+
+
+# ------------------------------------------------------------------- CPU
+def test_oracle_mass_inlet_initial_state():
+    import oracle
+    m, c = cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, **_tight())
+    _mass_inlet(m, c, u=1.5)
+    o = oracle.Oracle(m, c)
+    sl = _inlet(m)
+    bm = o.get("bmdot")[sl]
+    mdot = c.patches["inlet"][2]
+    assert abs(bm.sum() + mdot) <= 1e-13 * mdot
+    np.testing.assert_allclose(o.get("bu")[sl], 1.5, rtol=1e-13)
+    assert np.abs(o.get("bv")[sl]).max() == 0.0 and np.abs(o.get("bw")[sl]).max() == 0.0
+    o.initialize_mdot()                                   # leaves the specified Bmdot alone
+    assert np.array_equal(o.get("bmdot")[sl], bm)
+
+
+@pytest.mark.parametrize("turbulence", [False, True])
+def test_oracle_mass_inlet_matches_velocity_inlet(turbulence):
+    """With the same inflow a mass-flow inlet converges to the velocity
+    inlet's solution (its boundary velocity correction vanishes with p'),
+    keeps the inflow fixed and balances it at the outlet."""
+    import oracle
+    kw = dict(re_h=100.0 if not turbulence else 5000.0, turbulence=turbulence, **_tight())
+    m, cv = cs.bfs(24, 9, 6, **kw)
+    _, cm = cs.bfs(24, 9, 6, **kw)
+    _mass_inlet(m, cm)
+    ov, om = oracle.Oracle(m, cv), oracle.Oracle(m, cm)
+    for o, c in ((ov, cv), (om, cm)):
+        for k, v in cs.bfs_initial_state(m, c, seed=0, perturbation=0.0).items():
+            o.set(k, v)
+        o.initialize_mdot()
+    sl = _inlet(m)
+    bm0 = om.get("bmdot")[sl].copy()
+    for o in (ov, om):
+        for it in range(4000):
+            if o.simple_iteration() < 1e-8:
+                break
+        assert it < 3999
+    assert np.array_equal(om.get("bmdot")[sl], bm0)
+    s_out = m.patch("xmax")
+    b0 = int(m.patch_start[s_out]) - m.n_internal
+    out = om.get("bmdot")[b0:b0 + int(m.patch_size[s_out])].sum()
+    assert abs(out + bm0.sum()) <= 1e-10 * abs(bm0.sum())
+    for k in ("u", "v", "w") + (("tke", "ted") if turbulence else ()):
+        ref = ov.get(k)
+        assert np.linalg.norm(om.get(k) - ref) <= 1e-5 * np.linalg.norm(ref), k
+
+
+# ------------------------------------------------------------------- GPU
+@pytest.mark.gpu
+@pytest.mark.parametrize("turbulence", [False, True])
+def test_mass_inlet_step_matches_oracle(turbulence):
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, re_h=100.0 if not turbulence else 5000.0, turbulence=turbulence, **_tight())
+    _mass_inlet(m, c)
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
+    sl = _inlet(m)
+    for k in ("bmdot", "bu"):
+        assert np.array_equal(g.get(k)[sl], o.get(k)[sl]), k
+    _setup(o, m, c)
+    _setup(g, m, c)
+    for it in range(6):
+        so = o.simple_iteration()
+        rg = g.simple_iteration()
+        assert abs(rg["source"] - so) <= 1e-6 * abs(so) + 1e-14, (it, rg["source"], so)
+    keys = ("u", "v", "w", "p", "bmdot", "bu", "bp") + (("tke", "ted", "mut", "btke") if turbulence else ())
+    for k in keys:
+        x, ref = g.get(k), o.get(k)
+        err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+        assert err <= 1e-9, (k, err)
+    g.close()
