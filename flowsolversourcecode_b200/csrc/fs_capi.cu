@@ -177,7 +177,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (auto &e : ctx->tev) cudaEventCreate(&e);
   for (auto &pr : ctx->sev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
   for (auto &pr : ctx->kev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
-  for (int s = 0; s < ctx->cfg.n_patches; s++) ctx->has_sp |= ctx->cfg.patch_type[s] == FS_BC_OUTLET_SP;
+  for (int s = 0; s < ctx->cfg.n_patches; s++) ctx->has_sp |= fs_is_pressure(ctx->cfg.patch_type[s]);
   // SetReferencePressure (ReferenceAndSetPressureRoutines.for:4-50): a pressure-specified patch fixes the level
   if (ctx->cfg.set_reference_pressure < 0) ctx->cfg.set_reference_pressure = ctx->has_sp ? 1 : 0;
   if ((rc = fs_geometry_build(ctx, mesh))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
@@ -229,13 +229,14 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   std::vector<double> hp(B, 0.);   // static pressure of 'specifiedstaticpressure' outlets
   for (size_t b = 0; b < B; b++) {
     int s = ctx->h_bset[b];
-    if (ctx->cfg.patch_type[s] == FS_BC_OUTLET_SP) hp[b] = ctx->cfg.patch_pressure[s];
+    if (fs_is_pressure(ctx->cfg.patch_type[s])) hp[b] = ctx->cfg.patch_pressure[s];
   }
   // 'specifiedmassflowrate' inlets: Bmdot = -mdot |S_f| / sum |S| in face order, and the
   // velocity AssembleMdot derives from it (AssembleMdotUsingRhieChow.for:2077-2100)
   std::vector<double> hm(B, 0.);
   bool has_mass = false;
-  for (int s = 0; s < ctx->cfg.n_patches; s++) has_mass |= ctx->cfg.patch_type[s] == FS_BC_INLET_MASS;
+  for (int s = 0; s < ctx->cfg.n_patches; s++)
+    has_mass |= ctx->cfg.patch_type[s] == FS_BC_INLET_MASS || ctx->cfg.patch_type[s] == FS_BC_INLET_SP;
   if (has_mass && B) {
     std::vector<double> hfa(B), hsf(3 * B), hd(3 * B, 0.);
     if (cudaStreamSynchronize(ctx->st) != cudaSuccess ||
@@ -243,9 +244,11 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
         cudaMemcpy(hsf.data(), ctx->bsf, sizeof(double) * 3 * B, cudaMemcpyDeviceToHost) != cudaSuccess)
       return fail(FS_E_CUDA);
     for (int s = 0; s < ctx->cfg.n_patches; s++) {
-      if (ctx->cfg.patch_type[s] != FS_BC_INLET_MASS) continue;
       const int b0 = ctx->h_bset_start[s], nb = ctx->h_bset_n[s];
       const double *d = ctx->cfg.patch_vel[s], rho = ctx->cfg.rho;
+      if (ctx->cfg.patch_type[s] == FS_BC_INLET_SP)   // direction only
+        for (int j = 0; j < nb; j++) for (int q = 0; q < 3; q++) hd[3 * (size_t)(b0 + j) + q] = d[q];
+      if (ctx->cfg.patch_type[s] != FS_BC_INLET_MASS) continue;
       double area = 0.;
       for (int j = 0; j < nb; j++) area = area + hfa[b0 + j];
       for (int j = 0; j < nb; j++) {

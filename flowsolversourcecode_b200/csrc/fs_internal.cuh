@@ -22,7 +22,19 @@
 // 'specifiedvelocity' and 'specifiedmassflowrate' inlets share the momentum,
 // p' and k-epsilon treatment (AssembleIsotropicDiffusion.for:254-300,
 // AssembleConvection.for:260-300, AssemblePressureCorrectionFluxes.for:545-575)
-__host__ __device__ inline bool fs_is_inlet(int t) { return t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS; }
+__host__ __device__ inline bool fs_is_inlet(int t) {
+  return t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS || t == FS_BC_INLET_SP;
+}
+// static pressure specified: Rhie-Chow boundary flux and p'_b = 0
+// (AssembleMdotUsingRhieChow.for:1441-1598, 2105-2283)
+__host__ __device__ inline bool fs_is_pressure(int t) { return t == FS_BC_OUTLET_SP || t == FS_BC_INLET_SP; }
+// the velocity follows from Bmdot along a given direction (AssembleMdotUsingRhieChow.for:2089-2099)
+__device__ __forceinline__ void fs_directed_velocity(const double *bdir, const double *bsf, double rho, int B, int b,
+                                                     double bm, double *bu, double *bv, double *bw) {
+  const double dx = bdir[3L * b], dy = bdir[3L * b + 1], dz = bdir[3L * b + 2];
+  const double vm = bm / (rho * (dx * bsf[b] + dy * bsf[B + b] + dz * bsf[2L * B + b]));
+  bu[b] = vm * dx; bv[b] = vm * dy; bw[b] = vm * dz;
+}
 
 #define FS_BLOCK 256
 #ifndef FS_COOP_BLOCK

@@ -521,9 +521,7 @@ __global__ void k_bmdot_inlet(ContArgs a) {
   const int B = a.B;
   if (t == FS_BC_INLET_MASS) {
     // velocity from the specified Bmdot along the given direction (AssembleMdotUsingRhieChow.for:2077-2100)
-    const double dx = a.bdir[3L * b], dy = a.bdir[3L * b + 1], dz = a.bdir[3L * b + 2];
-    const double vm = a.bmdot[b] / (a.rho * (dx * a.bsf[b] + dy * a.bsf[B + b] + dz * a.bsf[2L * B + b]));
-    a.bu_w[b] = vm * dx; a.bv_w[b] = vm * dy; a.bw_w[b] = vm * dz;
+    fs_directed_velocity(a.bdir, a.bsf, a.rho, B, b, a.bmdot[b], a.bu_w, a.bv_w, a.bw_w);
     return;
   }
   if (t != FS_BC_INLET_VEL) return;
@@ -535,15 +533,18 @@ __global__ void k_bmdot_inlet(ContArgs a) {
 // (AssemblePressureCorrectionFluxes.for:244-313)
 __global__ void k_bmdot_sp(ContArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= a.B || a.btype[b] != FS_BC_OUTLET_SP) return;
+  if (b >= a.B || !fs_is_pressure(a.btype[b])) return;
   const int N = a.N, B = a.B;
   const long N2 = 2L * N, B2 = 2L * B;
   const int i1 = a.bown[b];
+  const bool inlet = a.btype[b] == FS_BC_INLET_SP;   // :2105-2283, the same flux; velocity from Bmdot
   const double rhof = a.rho, sx = a.bsf[b], sy = a.bsf[B + b], sz = a.bsf[B2 + b];
   const double dx = a.bdv[b], dy = a.bdv[B + b], dz = a.bdv[B2 + b];
-  a.bu_w[b] = a.u[i1] + (a.bug[b] * dx + a.bug[B + b] * dy + a.bug[B2 + b] * dz);
-  a.bv_w[b] = a.v[i1] + (a.bvg[b] * dx + a.bvg[B + b] * dy + a.bvg[B2 + b] * dz);
-  a.bw_w[b] = a.w[i1] + (a.bwg[b] * dx + a.bwg[B + b] * dy + a.bwg[B2 + b] * dz);
+  if (!inlet) {
+    a.bu_w[b] = a.u[i1] + (a.bug[b] * dx + a.bug[B + b] * dy + a.bug[B2 + b] * dz);
+    a.bv_w[b] = a.v[i1] + (a.bvg[b] * dx + a.bvg[B + b] * dy + a.bvg[B2 + b] * dz);
+    a.bw_w[b] = a.w[i1] + (a.bwg[b] * dx + a.bwg[B + b] * dy + a.bwg[B2 + b] * dz);
+  }
   const double cf = sqrt(dx * dx + dy * dy + dz * dz);
   const double ex = dx / cf, ey = dy / cf, ez = dz / cf;
   double fvl = rhof * (a.u[i1] * sx + a.v[i1] * sy + a.w[i1] * sz);
@@ -563,6 +564,7 @@ __global__ void k_bmdot_sp(ContArgs a) {
     fvl = fvl + (1. - a.urf) * (a.bmdot[b] - ms);
   }
   a.bmdot[b] = fcl * a.p[i1] + ffl * a.bp[b] + fvl;
+  if (inlet) fs_directed_velocity(a.bdir, a.bsf, rhof, B, b, a.bmdot[b], a.bu_w, a.bv_w, a.bw_w);
   double t2x, t2y, t2z;
   a.bpcoef[b] = rhof * geo_diff(a.msd, a.du2[i1], a.dv2[i1], a.dw2[i1], sx, sy, sz, ex, ey, ez, cf, t2x, t2y, t2z);
 }
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_pc_assemble(ContArgs a) {
         if (s & 1) { ac = ac - fff; a.anb[(long)j * N + i] = 0. - c; bc = bc + md; }
         else { ac = ac + c; a.anb[(long)j * N + i] = 0. + fff; bc = bc - md; }
       } else {
-        ac = ac + (a.btype[f - F] == FS_BC_OUTLET_SP ? a.bpcoef[f - F] : 0.);
+        ac = ac + (fs_is_pressure(a.btype[f - F]) ? a.bpcoef[f - F] : 0.);
         bc = bc - a.bmdot[f - F];
       }
     };
@@ -606,12 +608,13 @@ struct CorrArgs {
   const double *bpcoef;
   double *red; int64_t *redi; int nblk; double *rb;
   const double *vol; double drhodt; int unsteady;   // + d rho/dt V in unsteady runs
+  const double *bdir, *bsf; double rho;             // inlets with a given velocity direction
 };
 
 // UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for)
 __global__ void k_bpc(CorrArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < a.B) a.bpc[b] = a.btype[b] == FS_BC_OUTLET_SP ? 0. : a.pc[a.bown[b]];   // :126-130
+  if (b < a.B) a.bpc[b] = fs_is_pressure(a.btype[b]) ? 0. : a.pc[a.bown[b]];   // :85-90, 126-130
 }
 // CorrectPressure (CorrectPressure.for:21-42)
 __global__ void k_corr_p(CorrArgs a) {
@@ -645,13 +648,18 @@ __global__ void k_bcorr(CorrArgs a) {
   const int B = a.B;
   const long B2 = 2L * B;
   int t = a.btype[b], i1 = a.bown[b];
-  if (t == FS_BC_OUTLET_SP) {
-    // CorrectBoundarymdot (CorrectMdotandVelocity.for:264-280); the static pressure stays (CorrectPressure.for:162-166)
+  if (fs_is_pressure(t)) {
+    // CorrectBoundarymdot (CorrectMdotandVelocity.for:264-280; inlets :180-205, the velocity
+    // again from Bmdot); the static pressure stays (CorrectPressure.for:146-150, 162-166)
     const int N = a.N;
     a.bmdot[b] = a.bmdot[b] - a.bpcoef[b] * (a.bpc[b] - a.pc[i1]);
-    a.bu[b] = a.bu[b] - a.du2[i1] * a.pcg[i1];
-    a.bv[b] = a.bv[b] - a.dv2[i1] * a.pcg[N + i1];
-    a.bw[b] = a.bw[b] - a.dw2[i1] * a.pcg[2L * N + i1];
+    if (t == FS_BC_INLET_SP) {
+      fs_directed_velocity(a.bdir, a.bsf, a.rho, B, b, a.bmdot[b], a.bu, a.bv, a.bw);
+    } else {
+      a.bu[b] = a.bu[b] - a.du2[i1] * a.pcg[i1];
+      a.bv[b] = a.bv[b] - a.dv2[i1] * a.pcg[N + i1];
+      a.bw[b] = a.bw[b] - a.dw2[i1] * a.pcg[2L * N + i1];
+    }
   } else if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
     a.bp[b] = a.p[i1] + a.bpg[b] * a.bdv[b] + a.bpg[B + b] * a.bdv[B + b] + a.bpg[B2 + b] * a.bdv[B2 + b];
   } else {
@@ -949,6 +957,7 @@ static CorrArgs corr_args(fs_ctx *ctx) {
   a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bmdot = ctx->bmdot; a.bpcoef = ctx->bpcoef;
   a.red = ctx->red; a.redi = ctx->redi; a.nblk = fs_grid(ctx->N); a.rb = ctx->resblk;
   a.vol = ctx->vol; a.unsteady = c.unsteady; a.drhodt = c.unsteady ? fs_drhodt(ctx) : 0.;
+  a.bdir = ctx->bdir; a.bsf = ctx->bsf; a.rho = c.rho;
   return a;
 }
 

@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(1024) k_flow_in_out(FlowArgs a) {
   const int B = a.B;
   double s = 0.;
   for (int q = 0; q < a.NS; q++)
-    if (fs_is_inlet(a.ptype[q]))   // CalculateFlowIn.for:37-48
+    if (a.ptype[q] == FS_BC_INLET_VEL || a.ptype[q] == FS_BC_INLET_MASS)   // CalculateFlowIn.for:37-48
       for (int j = threadIdx.x; j < a.pn[q]; j += blockDim.x) s = s + a.bmdot[a.pstart[q] + j];
   s = block_sum(s, sh);
   if (threadIdx.x == 0) { a.flow[0] = s; bcast = s; }

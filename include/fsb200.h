@@ -87,8 +87,10 @@ enum fs_bc {
   FS_BC_INLET_VEL   = 3,   /* 'inlet','specifiedvelocity' */
   FS_BC_OUTLET_FD   = 4,   /* 'outlet','fullydeveloped' */
   FS_BC_OUTLET_SP   = 5,   /* 'outlet','specifiedstaticpressure' (patch_pressure) */
-  FS_BC_INLET_MASS  = 6    /* 'inlet','specifiedmassflowrate': patch_vel is the velocity
+  FS_BC_INLET_MASS  = 6,   /* 'inlet','specifiedmassflowrate': patch_vel is the velocity
                             * direction (xVeldirection...), patch_mass_flow the inflow */
+  FS_BC_INLET_SP    = 7    /* 'inlet','specifiedstaticpressure': patch_pressure, and
+                            * patch_vel the velocity direction */
 };
 
 /* ---------------------------------------------------------- scheme enums */

@@ -31,7 +31,11 @@
 /* 'specifiedvelocity' and 'specifiedmassflowrate' inlets take the same
  * momentum, p' and k-epsilon treatment (AssembleIsotropicDiffusion.for:254-300,
  * AssembleConvection.for:260-300, AssemblePressureCorrectionFluxes.for:545-575) */
-#define OM_INLET(t) ((t) == FS_BC_INLET_VEL || (t) == FS_BC_INLET_MASS)
+#define OM_INLET(t) ((t) == FS_BC_INLET_VEL || (t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP)
+/* static pressure specified: Rhie-Chow boundary flux, p'_b = 0 (AssembleMdotUsingRhieChow.for:1441-1598, 2105-2283) */
+#define OM_PRESSURE(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_INLET_SP)
+/* the direction of the inlet velocity is given (xVeldirection...) */
+#define OM_DIRECTED(t) ((t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP)
 
 struct om {
   fs_case cfg;
@@ -766,7 +770,8 @@ static void om_flow_in_out(om *m)
   /* FlowOut/AdjustFlow return at once unless every outlet is fully developed */
   if (nfd == 0 || other) return;
   m->mdot_in = 0.;
-  for (int s = 0; s < NS; s++) if (OM_INLET(c->patch_type[s]))   /* CalculateFlowIn.for:37-48 */
+  for (int s = 0; s < NS; s++)   /* velocity and mass-flow inlets (CalculateFlowIn.for:37-48) */
+    if (c->patch_type[s] == FS_BC_INLET_VEL || c->patch_type[s] == FS_BC_INLET_MASS)
     for (int j = 0; j < m->bset_n[s]; j++) m->mdot_in = m->mdot_in + m->bmdot[m->bset_start[s] + j];
   for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_FD) {
     m->mdot1[s] = 0.;
@@ -798,7 +803,16 @@ static void om_flow_in_out(om *m)
   (void)F;
 }
 
-/* AssembleMdot (AssembleMdotUsingRhieChow.for:262-292, 554-759, 1441-1598, 2033-2075) */
+/* the velocity of an inlet with a given direction from its Bmdot
+ * (AssembleMdotUsingRhieChow.for:2089-2099) */
+static void om_directed_velocity(om *m, int b)
+{
+  const double *d = m->bdir + 3L * b;
+  double vm = m->bmdot[b] / (m->cfg.rho * (d[0] * m->bsx[b] + d[1] * m->bsy[b] + d[2] * m->bsz[b]));
+  m->bu[b] = vm * d[0]; m->bv[b] = vm * d[1]; m->bw[b] = vm * d[2];
+}
+
+/* AssembleMdot (AssembleMdotUsingRhieChow.for:262-292, 554-759, 1441-1598, 2033-2283) */
 static void om_assemble_mdot(om *m)
 {
   int N = m->N, F = m->F, B = m->B;
@@ -839,13 +853,17 @@ static void om_assemble_mdot(om *m)
     m->mdot[k] = fcl * m->p[i] + ffl * m->p[j] + fvl;
   }
   free(pgbar); free(rkbar); free(rkf);
-  /* 'specifiedstaticpressure' outlets (AssembleMdotUsingRhieChow.for:1441-1598) */
-  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) {
+  /* 'specifiedstaticpressure' outlets (AssembleMdotUsingRhieChow.for:1441-1598) and
+   * inlets (:2105-2283): the same Rhie-Chow boundary flux; the outlet first
+   * extrapolates its velocity, the inlet's follows from Bmdot along its direction */
+  for (int b = 0; b < B; b++) if (OM_PRESSURE(m->btype[b])) {
     int i1 = m->bf_own[b];
     double rhof = c->rho, sx = m->bsx[b], sy = m->bsy[b], sz = m->bsz[b];
-    m->bu[b] = m->u[i1] + (m->bug[b] * m->bdx[b] + m->bug[B + b] * m->bdy[b] + m->bug[2L * B + b] * m->bdz[b]);
-    m->bv[b] = m->v[i1] + (m->bvg[b] * m->bdx[b] + m->bvg[B + b] * m->bdy[b] + m->bvg[2L * B + b] * m->bdz[b]);
-    m->bw[b] = m->w[i1] + (m->bwg[b] * m->bdx[b] + m->bwg[B + b] * m->bdy[b] + m->bwg[2L * B + b] * m->bdz[b]);
+    if (m->btype[b] == FS_BC_OUTLET_SP) {
+      m->bu[b] = m->u[i1] + (m->bug[b] * m->bdx[b] + m->bug[B + b] * m->bdy[b] + m->bug[2L * B + b] * m->bdz[b]);
+      m->bv[b] = m->v[i1] + (m->bvg[b] * m->bdx[b] + m->bvg[B + b] * m->bdy[b] + m->bvg[2L * B + b] * m->bdz[b]);
+      m->bw[b] = m->w[i1] + (m->bwg[b] * m->bdx[b] + m->bwg[B + b] * m->bdy[b] + m->bwg[2L * B + b] * m->bdz[b]);
+    }
     double mbar = m->u[i1] * sx + m->v[i1] * sy + m->w[i1] * sz;
     double fvl = rhof * mbar;
     double du = m->du1[i1], dv = m->dv1[i1], dw = m->dw1[i1], tx, ty, tz;
@@ -863,6 +881,7 @@ static void om_assemble_mdot(om *m)
       fvl = fvl + (1. - c->urf_momentum) * (m->bmdot[b] - ms);
     }
     m->bmdot[b] = fcl * m->p[i1] + ffl * m->bp[b] + fvl;
+    if (m->btype[b] == FS_BC_INLET_SP) om_directed_velocity(m, b);   /* :2277-2282 */
   }
   /* inlet specified velocity Bmdot (AssembleMdotUsingRhieChow.for:2054-2075) */
   for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_VEL)
@@ -874,11 +893,7 @@ static void om_assemble_mdot(om *m)
   }
   /* 'specifiedmassflowrate' inlet velocity from Bmdot along the given
    * direction (AssembleMdotUsingRhieChow.for:2077-2100) */
-  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_MASS) {
-    const double *d = m->bdir + 3L * b;
-    double vm = m->bmdot[b] / (c->rho * (d[0] * m->bsx[b] + d[1] * m->bsy[b] + d[2] * m->bsz[b]));
-    m->bu[b] = vm * d[0]; m->bv[b] = vm * d[1]; m->bw[b] = vm * d[2];
-  }
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_MASS) om_directed_velocity(m, b);
 }
 
 void om_assemble_continuity(om *m)
@@ -896,9 +911,9 @@ void om_assemble_continuity(om *m)
     m->fcf[k] = c->rho * gd; m->fff[k] = -(c->rho * gd); m->ftf[k] = m->mdot[k];
   }
   for (int b = 0; b < B; b++) m->ftf[F + b] = m->bmdot[b];
-  /* 'specifiedstaticpressure' outlets: p'_b = 0, FluxCf = FluxFf = rho geoDiff(D2)
-   * (AssemblePressureCorrectionFluxes.for:244-313) */
-  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) {
+  /* 'specifiedstaticpressure' outlets and inlets: p'_b = 0, FluxCf = FluxFf = rho geoDiff(D2)
+   * (AssemblePressureCorrectionFluxes.for:244-313, 585-657) */
+  for (int b = 0; b < B; b++) if (OM_PRESSURE(m->btype[b])) {
     int i1 = m->bf_own[b];
     double gd = geo_diff(c->method_decompose_s, m->du2[i1], m->dv2[i1], m->dw2[i1], m->bsx[b], m->bsy[b], m->bsz[b],
                          m->bex[b], m->bey[b], m->bez[b], m->bd[b], 0, 0, 0);
@@ -919,7 +934,7 @@ void om_correct_continuity(om *m)
   const fs_case *c = &m->cfg;
   /* UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for) */
   for (int b = 0; b < B; b++)
-    m->bpc[b] = m->btype[b] == FS_BC_OUTLET_SP ? 0. : m->pc[m->bf_own[b]];   /* :126-130 */
+    m->bpc[b] = OM_PRESSURE(m->btype[b]) ? 0. : m->pc[m->bf_own[b]];   /* :85-90, 126-130 */
   /* CorrectPressure (CorrectPressure.for:4-42) */
   double rpc = (c->ref_pressure_cell >= 0) ? m->pc[c->ref_pressure_cell] : 0.;
   if (c->set_reference_pressure == 1) rpc = 0.;
@@ -934,11 +949,13 @@ void om_correct_continuity(om *m)
   /* Correctmdot (CorrectMdotandVelocity.for:55-63) */
   for (int k = 0; k < F; k++)
     m->mdot[k] = m->mdot[k] + m->fcf[k] * m->pc[m->if_own[k]] + m->fff[k] * m->pc[m->if_nbr[k]];
-  /* CorrectBoundarymdot, 'specifiedstaticpressure' (CorrectMdotandVelocity.for:264-280) */
-  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) {
+  /* CorrectBoundarymdot, 'specifiedstaticpressure' outlets (CorrectMdotandVelocity.for:264-280)
+   * and inlets (:180-205: the velocity again from Bmdot along its direction) */
+  for (int b = 0; b < B; b++) if (OM_PRESSURE(m->btype[b])) {
     int i1 = m->bf_own[b];
     double gd = m->fff[F + b];
     m->bmdot[b] = m->bmdot[b] - gd * (m->bpc[b] - m->pc[i1]);
+    if (m->btype[b] == FS_BC_INLET_SP) { om_directed_velocity(m, b); continue; }
     m->bu[b] = m->bu[b] - m->du2[i1] * m->pcg[i1];
     m->bv[b] = m->bv[b] - m->dv2[i1] * m->pcg[N + i1];
     m->bw[b] = m->bw[b] - m->dw2[i1] * m->pcg[2L * N + i1];
@@ -955,7 +972,7 @@ void om_correct_continuity(om *m)
     int t = m->btype[b], i1 = m->bf_own[b];
     if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY)
       m->bp[b] = m->p[i1] + m->bpg[b] * m->bdx[b] + m->bpg[B + b] * m->bdy[b] + m->bpg[2 * (long)B + b] * m->bdz[b];
-    else if (OM_INLET(t) || t == FS_BC_OUTLET_FD)   /* :120-138 */
+    else if (t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS || t == FS_BC_OUTLET_FD)   /* :120-138; static pressures stay */
       m->bp[b] = m->bp[b] + c->urf_pressure * (m->bpc[b] - rpc);
   }
   /* CalculateResidualsContinuity (CalculateContinuityResiduals.for:130-235) */
@@ -1367,7 +1384,7 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
    * (ReferenceAndSetPressureRoutines.for:4-50): a pressure-specified patch
    * fixes the level, no reference cell */
   int has_sp = 0;
-  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_SP) { m->bp[b] = cfg->patch_pressure[m->bf_set[b]]; has_sp = 1; }
+  for (int b = 0; b < B; b++) if (OM_PRESSURE(m->btype[b])) { m->bp[b] = cfg->patch_pressure[m->bf_set[b]]; has_sp = 1; }
   if (m->cfg.set_reference_pressure < 0) m->cfg.set_reference_pressure = has_sp;
   m->ug = dz_(3L*N); m->vg = dz_(3L*N); m->wg = dz_(3L*N); m->pg = dz_(3L*N); m->pcg = dz_(3L*N);
   m->bug = dz_(3L*B); m->bvg = dz_(3L*B); m->bwg = dz_(3L*B); m->bpg = dz_(3L*B); m->bpcg = dz_(3L*B);
@@ -1390,6 +1407,9 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
   om_wall_distance(m);
   /* 'specifiedmassflowrate' inlets: direction per face, Bmdot = -mdot |S_f| / sum |S| in face order */
   m->bdir = dz_(3L * B);
+  for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_INLET_SP)
+    for (int j = 0; j < m->bset_n[s]; j++)
+      for (int q = 0; q < 3; q++) m->bdir[3L * (m->bset_start[s] + j) + q] = cfg->patch_vel[s][q];
   for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_INLET_MASS) {
     double area = 0.;
     for (int j = 0; j < m->bset_n[s]; j++) area = area + m->bfa[m->bset_start[s] + j];

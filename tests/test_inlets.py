@@ -1,5 +1,7 @@
 """'specifiedmassflowrate' inlets (inletTypeM, AssembleMdotUsingRhieChow.for:2077-2100,
-CorrectMdotandVelocity.for:165-175, InitializaMdot.for:55, CalculateFlowIn.for:37-48):
+CorrectMdotandVelocity.for:165-175, InitializaMdot.for:55, CalculateFlowIn.for:37-48)
+and 'specifiedstaticpressure' inlets (AssembleMdotUsingRhieChow.for:2105-2283,
+AssemblePressureCorrectionFluxes.for:585-657, CorrectMdotandVelocity.for:180-205):
 the restatement's invariants on the step case (CPU) and the GPU path against it."""
 
 import numpy as np
@@ -106,6 +108,59 @@ def test_mass_inlet_step_matches_oracle(turbulence):
     sl = _inlet(m)
     for k in ("bmdot", "bu"):
         assert np.array_equal(g.get(k)[sl], o.get(k)[sl]), k
+    _setup(o, m, c)
+    _setup(g, m, c)
+    for it in range(6):
+        so = o.simple_iteration()
+        rg = g.simple_iteration()
+        assert abs(rg["source"] - so) <= 1e-6 * abs(so) + 1e-14, (it, rg["source"], so)
+    keys = ("u", "v", "w", "p", "bmdot", "bu", "bp") + (("tke", "ted", "mut", "btke") if turbulence else ())
+    for k in keys:
+        x, ref = g.get(k), o.get(k)
+        err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+        assert err <= 1e-9, (k, err)
+    g.close()
+
+
+# ------------------------------------------------ 'specifiedstaticpressure' inlets
+def _pressure_driven(case, p_in=1.0):
+    """Inlet at static pressure p_in along +x, outlet at 0: a pressure-driven step flow."""
+    case.patches["inlet"] = ("pressure_inlet", (1.0, 0.0, 0.0), p_in)
+    case.patches["xmax"] = ("pressure_outlet", 0.0)
+
+
+def test_oracle_pressure_inlet_step():
+    """The pressure drop drives a flow in through the inlet and out at the
+    outlet; the inlet velocity points along its direction, the boundary
+    pressures stay where they were set and the flow balances."""
+    import oracle
+    m, c = cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, **_tight())
+    _pressure_driven(c, 0.05)
+    o = oracle.Oracle(m, c)
+    for it in range(3000):
+        if o.simple_iteration() < 1e-8:
+            break
+    assert it < 2999
+    sl = _inlet(m)
+    bm_in = o.get("bmdot")[sl]
+    assert np.all(bm_in < 0.0)                         # inflow on every inlet face
+    np.testing.assert_array_equal(o.get("bp")[sl], 0.05)
+    assert np.abs(o.get("bv")[sl]).max() == 0.0 and np.all(o.get("bu")[sl] > 0.0)
+    s_out = m.patch("xmax")
+    b0 = int(m.patch_start[s_out]) - m.n_internal
+    out = o.get("bmdot")[b0:b0 + int(m.patch_size[s_out])].sum()
+    assert abs(out + bm_in.sum()) <= 1e-8 * abs(bm_in.sum())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("turbulence", [False, True])
+def test_pressure_inlet_step_matches_oracle(turbulence):
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, re_h=100.0 if not turbulence else 5000.0, turbulence=turbulence, **_tight())
+    _pressure_driven(c, 0.05)
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
     _setup(o, m, c)
     _setup(g, m, c)
     for it in range(6):
