@@ -26,7 +26,8 @@ FS_NN_NPARAM = 33665
 VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
 VAR_TKE, VAR_TED, VAR_RHOK = 8, 9, 10
 # boundary types
-BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD, BC_OUTLET_SP, BC_INLET_MASS, BC_INLET_SP = range(8)
+(BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD, BC_OUTLET_SP, BC_INLET_MASS, BC_INLET_SP,
+ BC_OUTLET_MASS) = range(9)
 TRANSIENT = {"euler": 0, "cranknicolson1": 1, "cranknicolson2": 2, "adamsmoulton": 3}
 # gradient interpolation
 GI_AVERAGE, GI_UPWIND, GI_DOWNWIND, GI_AVERAGECORRECTED = 0, 1, 2, 3

@@ -22,7 +22,7 @@ __global__ void k_initial_mdot(int N, int F, int B, double rho, const int32_t *f
   } else if (t < (long)F + B) {
     int b = (int)(t - F), ty = btype[b];
     if (ty == FS_BC_WALL_NOSLIP || ty == FS_BC_WALL_SLIP) bmdot[b] = 0.;
-    else if (ty != FS_BC_INLET_MASS)   // a mass-flow inlet's Bmdot is specified (InitializaMdot.for:55)
+    else if (ty != FS_BC_INLET_MASS && ty != FS_BC_OUTLET_MASS)   // specified mass flow (InitializaMdot.for:55,66)
       bmdot[b] = rho * (bsf[b] * bu[b] + bsf[B + b] * bv[b] + bsf[2L * B + b] * bw[b]);
   }
 }
@@ -236,7 +236,8 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   std::vector<double> hm(B, 0.);
   bool has_mass = false;
   for (int s = 0; s < ctx->cfg.n_patches; s++)
-    has_mass |= ctx->cfg.patch_type[s] == FS_BC_INLET_MASS || ctx->cfg.patch_type[s] == FS_BC_INLET_SP;
+    has_mass |= ctx->cfg.patch_type[s] == FS_BC_INLET_MASS || ctx->cfg.patch_type[s] == FS_BC_INLET_SP ||
+                ctx->cfg.patch_type[s] == FS_BC_OUTLET_MASS;
   if (has_mass && B) {
     std::vector<double> hfa(B), hsf(3 * B), hd(3 * B, 0.);
     if (cudaStreamSynchronize(ctx->st) != cudaSuccess ||
@@ -248,6 +249,11 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
       const double *d = ctx->cfg.patch_vel[s], rho = ctx->cfg.rho;
       if (ctx->cfg.patch_type[s] == FS_BC_INLET_SP)   // direction only
         for (int j = 0; j < nb; j++) for (int q = 0; q < 3; q++) hd[3 * (size_t)(b0 + j) + q] = d[q];
+      if (ctx->cfg.patch_type[s] == FS_BC_OUTLET_MASS) {   // outflow: Bmdot > 0; velocity from the first mdot assembly
+        double area = 0.;
+        for (int j = 0; j < nb; j++) area = area + hfa[b0 + j];
+        for (int j = 0; j < nb; j++) hm[b0 + j] = ctx->cfg.patch_mass_flow[s] * hfa[b0 + j] / area;
+      }
       if (ctx->cfg.patch_type[s] != FS_BC_INLET_MASS) continue;
       double area = 0.;
       for (int j = 0; j < nb; j++) area = area + hfa[b0 + j];

@@ -355,7 +355,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
           }
           fcf = fcl;
           tf = fcl * phi + 0. * bp + fvl;
-        } else if (fs_is_inlet(t)) {
+        } else if (fs_is_inlet(t) || t == FS_BC_OUTLET_MASS) {   // :254-300, 507-525
           double fcl = gamf * a.bgdiff[b], ffl = -gamf * a.bgdiff[b];
           double fvl = -(gamf * (bfg[b] * a.btf[b] + bfg[B + b] * a.btf[B + b] + bfg[B2 + b] * a.btf[B2 + b]));
           fcf = fcl;
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
         double sc = comp == 0 ? bsx : comp == 1 ? bsy : bsz;
         tf = tf + -(M23 * gamf * div * sc);
       }
-      if (fs_is_inlet(t)) {
+      if (fs_is_inlet(t) || t == FS_BC_OUTLET_MASS) {
         double bm = a.bmdot[b];
         double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
         fcf = fcf + fcl;
@@ -524,6 +524,16 @@ __global__ void k_bmdot_inlet(ContArgs a) {
     fs_directed_velocity(a.bdir, a.bsf, a.rho, B, b, a.bmdot[b], a.bu_w, a.bv_w, a.bw_w);
     return;
   }
+  if (t == FS_BC_OUTLET_MASS) {
+    // along the owner's velocity (AssembleMdotUsingRhieChow.for:1999-2031)
+    const int i1 = a.bown[b];
+    const double u = a.u[i1], v = a.v[i1], w = a.w[i1];
+    const double vel = sqrt(u * u + v * v + w * w);
+    const double dx = u / (vel + TINY), dy = v / (vel + TINY), dz = w / (vel + TINY);
+    const double vm = a.bmdot[b] / (a.rho * (dx * a.bsf[b] + dy * a.bsf[B + b] + dz * a.bsf[2L * B + b]));
+    a.bu_w[b] = vm * dx; a.bv_w[b] = vm * dy; a.bw_w[b] = vm * dz;
+    return;
+  }
   if (t != FS_BC_INLET_VEL) return;
   a.bmdot[b] = a.rho * (a.bu[b] * a.bsf[b] + a.bv[b] * a.bsf[B + b] + a.bw[b] * a.bsf[2L * B + b]);
 }
@@ -666,7 +676,7 @@ __global__ void k_bcorr(CorrArgs a) {
     double rpc = (a.ref_cell >= 0) ? a.pc[a.ref_cell] : 0.;
     if (a.set_ref) rpc = 0.;
     a.bp[b] = a.bp[b] + a.urfp * (a.bpc[b] - rpc);
-    if (t == FS_BC_INLET_MASS) {   // CorrectBoundarymdot: the velocity only (CorrectMdotandVelocity.for:165-175)
+    if (t == FS_BC_INLET_MASS || t == FS_BC_OUTLET_MASS) {   // CorrectBoundarymdot: the velocity only (:165-175, 354-364)
       const int N = a.N;
       a.bu[b] = a.bu[b] - a.du2[i1] * a.pcg[i1];
       a.bv[b] = a.bv[b] - a.dv2[i1] * a.pcg[N + i1];

@@ -89,8 +89,10 @@ enum fs_bc {
   FS_BC_OUTLET_SP   = 5,   /* 'outlet','specifiedstaticpressure' (patch_pressure) */
   FS_BC_INLET_MASS  = 6,   /* 'inlet','specifiedmassflowrate': patch_vel is the velocity
                             * direction (xVeldirection...), patch_mass_flow the inflow */
-  FS_BC_INLET_SP    = 7    /* 'inlet','specifiedstaticpressure': patch_pressure, and
+  FS_BC_INLET_SP    = 7,   /* 'inlet','specifiedstaticpressure': patch_pressure, and
                             * patch_vel the velocity direction */
+  FS_BC_OUTLET_MASS = 8    /* 'outlet','specifiedmassflowrate': patch_mass_flow leaves the
+                            * domain, along the owner cell's velocity */
 };
 
 /* ---------------------------------------------------------- scheme enums */
@@ -188,9 +190,10 @@ typedef struct fs_case {
   int    unsteady;
   int    transient_scheme;       /* fs_transient */
   double dt;                     /* first time step */
-  /* 'specifiedmassflowrate' inlets: mass flow into the domain per patch,
-   * spread over the faces by area as the initial Bmdot (the reference leaves
-   * the face values to DescribeProblem: set FS_F_BMDOT to override) */
+  /* 'specifiedmassflowrate' inlets and outlets: mass flow into (inlets) or
+   * out of (outlets) the domain per patch, spread over the faces by area as
+   * the initial Bmdot (the reference leaves the face values to
+   * DescribeProblem: set FS_F_BMDOT to override) */
   double patch_mass_flow[FS_MAX_PATCHES];
 } fs_case;
 

@@ -34,6 +34,9 @@
 #define OM_INLET(t) ((t) == FS_BC_INLET_VEL || (t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP)
 /* static pressure specified: Rhie-Chow boundary flux, p'_b = 0 (AssembleMdotUsingRhieChow.for:1441-1598, 2105-2283) */
 #define OM_PRESSURE(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_INLET_SP)
+/* Dirichlet momentum diffusion and plain upwind convection at the face
+ * (AssembleIsotropicDiffusion.for:254-300, 507-525; AssembleConvection.for:260-330, 505-520) */
+#define OM_GIVEN_FLOW(t) (OM_INLET(t) || (t) == FS_BC_OUTLET_MASS)
 /* the direction of the inlet velocity is given (xVeldirection...) */
 #define OM_DIRECTED(t) ((t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP)
 
@@ -601,7 +604,7 @@ void om_assemble_momentum(om *m, int comp)
         else { fcl = 2. * gamf * area * (nz * nz) / dN; fvl = -((-2. * gamf * area / dN) * (m->u[i1] * nx + m->v[i1] * ny) * nz); }
         m->fcf[i4] += fcl; m->fvf[i4] += fvl;
         m->ftf[i4] += fcl * fi[i1] + 0. * bfi[b] + fvl;
-      } else if (OM_INLET(t)) {   /* :254-300 */
+      } else if (OM_GIVEN_FLOW(t)) {   /* :254-300, 507-525 */
         const double *bgx = bfg, *bgy = bfg + B, *bgz = bfg + 2 * (long)B;
         double fcl = gamf * m->bgdiff[b], ffl = -gamf * m->bgdiff[b];
         double fvl = -(gamf * (bgx[b] * m->bTx[b] + bgy[b] * m->bTy[b] + bgz[b] * m->bTz[b]));
@@ -679,7 +682,7 @@ void om_assemble_momentum(om *m, int comp)
   /* boundary convection (AssembleConvection.for:182-580): inlet specified velocity, outlet FD */
   for (int b = 0; b < B; b++) {
     int i1 = m->bf_own[b], t = m->btype[b]; long i4 = F + b;
-    if (OM_INLET(t)) {
+    if (OM_GIVEN_FLOW(t)) {
       double fcl = fmax(m->bmdot[b], 0.), ffl = -fmax(-m->bmdot[b], 0.);
       m->fcf[i4] += fcl; m->fff[i4] += ffl; m->ftf[i4] += fcl * fi[i1] + ffl * bfi[b];
     } else if (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {   /* :421-448 the same for both */
@@ -765,7 +768,7 @@ static void om_flow_in_out(om *m)
   int nfd = 0, other = 0;
   for (int s = 0; s < NS; s++) {
     if (c->patch_type[s] == FS_BC_OUTLET_FD) nfd++;
-    if (c->patch_type[s] == FS_BC_OUTLET_SP) other++;
+    if (c->patch_type[s] == FS_BC_OUTLET_SP || c->patch_type[s] == FS_BC_OUTLET_MASS) other++;
   }
   /* FlowOut/AdjustFlow return at once unless every outlet is fully developed */
   if (nfd == 0 || other) return;
@@ -894,6 +897,14 @@ static void om_assemble_mdot(om *m)
   /* 'specifiedmassflowrate' inlet velocity from Bmdot along the given
    * direction (AssembleMdotUsingRhieChow.for:2077-2100) */
   for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_MASS) om_directed_velocity(m, b);
+  /* 'specifiedmassflowrate' outlets: along the owner's velocity (:1999-2031) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_MASS) {
+    int i1 = m->bf_own[b];
+    double vel = sqrt(m->u[i1] * m->u[i1] + m->v[i1] * m->v[i1] + m->w[i1] * m->w[i1]);
+    double dx = m->u[i1] / (vel + OM_TINY), dy = m->v[i1] / (vel + OM_TINY), dz = m->w[i1] / (vel + OM_TINY);
+    double vm = m->bmdot[b] / (c->rho * (dx * m->bsx[b] + dy * m->bsy[b] + dz * m->bsz[b]));
+    m->bu[b] = vm * dx; m->bv[b] = vm * dy; m->bw[b] = vm * dz;
+  }
 }
 
 void om_assemble_continuity(om *m)
@@ -960,8 +971,9 @@ void om_correct_continuity(om *m)
     m->bv[b] = m->bv[b] - m->dv2[i1] * m->pcg[N + i1];
     m->bw[b] = m->bw[b] - m->dw2[i1] * m->pcg[2L * N + i1];
   }
-  /* CorrectBoundarymdot, 'specifiedmassflowrate' inlets: velocity only (CorrectMdotandVelocity.for:165-175) */
-  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_MASS) {
+  /* CorrectBoundarymdot, 'specifiedmassflowrate' inlets and outlets: velocity only
+   * (CorrectMdotandVelocity.for:165-175, 354-364) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_MASS || m->btype[b] == FS_BC_OUTLET_MASS) {
     int i1 = m->bf_own[b];
     m->bu[b] = m->bu[b] - m->du2[i1] * m->pcg[i1];
     m->bv[b] = m->bv[b] - m->dv2[i1] * m->pcg[N + i1];
@@ -972,7 +984,7 @@ void om_correct_continuity(om *m)
     int t = m->btype[b], i1 = m->bf_own[b];
     if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY)
       m->bp[b] = m->p[i1] + m->bpg[b] * m->bdx[b] + m->bpg[B + b] * m->bdy[b] + m->bpg[2 * (long)B + b] * m->bdz[b];
-    else if (t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS || t == FS_BC_OUTLET_FD)   /* :120-138; static pressures stay */
+    else if (t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS || t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_MASS)   /* :120-138, 220-226; static pressures stay */
       m->bp[b] = m->bp[b] + c->urf_pressure * (m->bpc[b] - rpc);
   }
   /* CalculateResidualsContinuity (CalculateContinuityResiduals.for:130-235) */
@@ -1338,7 +1350,7 @@ void om_initialize_mdot(om *m)
   }
   for (int b = 0; b < m->B; b++) {
     if (m->btype[b] == FS_BC_WALL_NOSLIP || m->btype[b] == FS_BC_WALL_SLIP) m->bmdot[b] = 0.;
-    else if (m->btype[b] == FS_BC_INLET_MASS) continue;   /* specified, not from the velocity (InitializaMdot.for:55) */
+    else if (m->btype[b] == FS_BC_INLET_MASS || m->btype[b] == FS_BC_OUTLET_MASS) continue;   /* specified (InitializaMdot.for:55,66) */
     else m->bmdot[b] = cfg->rho * (m->bsx[b] * m->bu[b] + m->bsy[b] * m->bv[b] + m->bsz[b] * m->bw[b]);
   }
 }
@@ -1410,6 +1422,11 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
   for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_INLET_SP)
     for (int j = 0; j < m->bset_n[s]; j++)
       for (int q = 0; q < 3; q++) m->bdir[3L * (m->bset_start[s] + j) + q] = cfg->patch_vel[s][q];
+  for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_OUTLET_MASS) {   /* outflow: Bmdot > 0 */
+    double area = 0.;
+    for (int j = 0; j < m->bset_n[s]; j++) area = area + m->bfa[m->bset_start[s] + j];
+    for (int j = 0; j < m->bset_n[s]; j++) m->bmdot[m->bset_start[s] + j] = cfg->patch_mass_flow[s] * m->bfa[m->bset_start[s] + j] / area;
+  }
   for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_INLET_MASS) {
     double area = 0.;
     for (int j = 0; j < m->bset_n[s]; j++) area = area + m->bfa[m->bset_start[s] + j];

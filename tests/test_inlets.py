@@ -1,7 +1,9 @@
 """'specifiedmassflowrate' inlets (inletTypeM, AssembleMdotUsingRhieChow.for:2077-2100,
 CorrectMdotandVelocity.for:165-175, InitializaMdot.for:55, CalculateFlowIn.for:37-48)
 and 'specifiedstaticpressure' inlets (AssembleMdotUsingRhieChow.for:2105-2283,
-AssemblePressureCorrectionFluxes.for:585-657, CorrectMdotandVelocity.for:180-205):
+AssemblePressureCorrectionFluxes.for:585-657, CorrectMdotandVelocity.for:180-205),
+and 'specifiedmassflowrate' outlets (AssembleMdotUsingRhieChow.for:1999-2031,
+CorrectMdotandVelocity.for:354-364):
 the restatement's invariants on the step case (CPU) and the GPU path against it."""
 
 import numpy as np
@@ -163,6 +165,60 @@ def test_pressure_inlet_step_matches_oracle(turbulence):
     g = Solver(m, c)
     _setup(o, m, c)
     _setup(g, m, c)
+    for it in range(6):
+        so = o.simple_iteration()
+        rg = g.simple_iteration()
+        assert abs(rg["source"] - so) <= 1e-6 * abs(so) + 1e-14, (it, rg["source"], so)
+    keys = ("u", "v", "w", "p", "bmdot", "bu", "bp") + (("tke", "ted", "mut", "btke") if turbulence else ())
+    for k in keys:
+        x, ref = g.get(k), o.get(k)
+        err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+        assert err <= 1e-9, (k, err)
+    g.close()
+
+
+# ------------------------------------------------ 'specifiedmassflowrate' outlets
+def _mass_outlet(mesh, case):
+    """The step's outlet removes what the velocity inlet brings in (rho U A)."""
+    case.patches["xmax"] = ("mass_outlet", case.rho * 1.0 * _patch_area(mesh, mesh.patch("inlet")))
+
+
+def test_oracle_mass_outlet_step():
+    import oracle
+    m, c = cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, **_tight())
+    _mass_outlet(m, c)
+    o = oracle.Oracle(m, c)
+    for k, v in cs.bfs_initial_state(m, c, seed=0, perturbation=0.0).items():
+        o.set(k, v)
+    o.initialize_mdot()
+    s_out = m.patch("xmax")
+    b0 = int(m.patch_start[s_out]) - m.n_internal
+    sl = slice(b0, b0 + int(m.patch_size[s_out]))
+    bm0 = o.get("bmdot")[sl].copy()
+    assert np.all(bm0 > 0.0) and abs(bm0.sum() - c.patches["xmax"][1]) <= 1e-13 * bm0.sum()
+    for it in range(4000):
+        if o.simple_iteration() < 1e-8:
+            break
+    assert it < 3999
+    assert np.array_equal(o.get("bmdot")[sl], bm0)        # the outflow stays as specified
+    assert np.all(o.get("bu")[sl] > 0.0)                  # along the owners' velocity, out of the domain
+    r = o.residuals()
+    assert abs(r["max"][4]) < 1e-8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("turbulence", [False, True])
+def test_mass_outlet_step_matches_oracle(turbulence):
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, re_h=100.0 if not turbulence else 5000.0, turbulence=turbulence, **_tight())
+    _mass_outlet(m, c)
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
+    for obj in (o, g):
+        for k, v in cs.bfs_initial_state(m, c, seed=0).items():
+            obj.set(k, v)
+        obj.initialize_mdot()
     for it in range(6):
         so = o.simple_iteration()
         rg = g.simple_iteration()
