@@ -172,8 +172,10 @@ def write_neu(path: str, m: NeuMesh) -> None:
 def neu_box(nx: int, ny: int, nz: int, kind: str = "hex", lx: float = 1.0, ly: float = 1.0, lz: float = 1.0,
             jitter: float = 0.0, seed: int = 0) -> NeuMesh:
     """A box of nx*ny*nz hexahedra ('hex'), each split into 2 wedges along
-    the x-y diagonal ('wedge') or into 6 tetrahedra around its main
-    diagonal ('tet', conforming across cells), with the six sides as
+    the x-y diagonal ('wedge'), into 6 tetrahedra around its main diagonal
+    ('tet', conforming across cells) or into 6 pyramids on its faces with
+    the apex at its centre ('pyramid'; 'mixed' keeps every other hexahedron
+    whole, so bricks and pyramids share faces), with the six sides as
     boundary sets named like the polyMesh box (xmin ... zmax).  Interior
     nodes move by up to jitter/2 of a cell (seeded)."""
     I, J, K = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
@@ -211,6 +213,19 @@ def neu_box(nx: int, ny: int, nz: int, kind: str = "hex", lx: float = 1.0, ly: f
                         path.append(P[(1, 1, 1)])
                         types.append(6)
                         conn.append(path)
+                elif kind in ("pyramid", "mixed"):
+                    if kind == "mixed" and (i + j + k) % 2 == 0:
+                        types.append(4)
+                        conn.append(c)
+                        continue
+                    # six pyramids on the hex faces with the apex at the cell centre
+                    centre = len(pts)
+                    pts = np.vstack([pts, pts[c].mean(axis=0)])
+                    idx = np.vstack([idx, [i + 0.5, j + 0.5, k + 0.5]])
+                    for f in LOCAL_FACES[4]:
+                        q = [c[x] for x in f]               # a cycle: base nodes 1,2,4,3 in Gambit order
+                        types.append(7)
+                        conn.append([q[0], q[1], q[3], q[2], centre])
                 else:
                     raise ValueError(kind)
     etype = np.asarray(types, np.int32)

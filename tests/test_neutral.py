@@ -12,6 +12,7 @@ from flowsolversourcecode_b200 import case as cs
 from flowsolversourcecode_b200 import neutral as nm
 
 KINDS = ["hex", "wedge", "tet"]
+ALL_KINDS = KINDS + ["pyramid", "mixed"]   # 'mixed': bricks and pyramids sharing faces
 
 
 def _literal():
@@ -19,7 +20,7 @@ def _literal():
     return oracle.load().om_neu_connectivity_literal
 
 
-@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("kind", ALL_KINDS)
 def test_neu_write_read_roundtrip(kind, tmp_path):
     m = nm.neu_box(3, 4, 2, kind, jitter=0.3, seed=2)
     p = str(tmp_path / "m.neu")
@@ -34,7 +35,7 @@ def test_neu_write_read_roundtrip(kind, tmp_path):
     np.testing.assert_allclose(r2.points, m.points * [2.0, 1.0, 0.5], rtol=1e-10, atol=1e-12)
 
 
-@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("kind", ALL_KINDS)
 @pytest.mark.parametrize("shuffle", [False, True])
 def test_connectivity_matches_literal_global_connectivity(kind, shuffle):
     """Every array -- interior face order, face nodes, owner/neighbour,
@@ -102,12 +103,12 @@ def test_neu_hex_cavity_matches_polymesh_cavity():
         assert np.abs(a.get(k)[ia] - b.get(k)[ib]).max() <= 1e-9 * np.abs(b.get(k)).max(), k
 
 
-@pytest.mark.parametrize("kind", ["wedge", "tet"])
+@pytest.mark.parametrize("kind", ["wedge", "tet", "pyramid", "mixed"])
 def test_oracle_cavity_on_wedges_and_tetrahedra(kind):
     import oracle
     _, c = cs.cavity(5, nz=3, solver_mom="bicgs", solver_cont="bicgs", krylov_tol=1e-10, krylov_maxit=300)
     o = oracle.Oracle(nm.to_polymesh(nm.neu_box(5, 5, 3, kind, jitter=0.2, seed=3)), c)
-    r = [o.simple_iteration() for _ in range(40)]
+    r = [o.simple_iteration() for _ in range(60)]
     assert np.all(np.isfinite(r)) and r[-1] < 1e-3 * r[1]
     # the element volumes fill the unit box
     assert abs(o.get("vol").sum() - 1.0) < 1e-12
