@@ -239,3 +239,35 @@ def test_mass_outlet_step_matches_oracle(turbulence):
         err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
         assert err <= 1e-9, (k, err)
     g.close()
+
+
+@pytest.mark.gpu
+@GPU_PARITY_PENDING
+def test_mass_inlet_phases_match_oracle():
+    """Phase by phase through the first two outer iterations of the
+    mass-flow-inlet step (momentum X, Y, Z, then SolveContinuity), naming the
+    first phase and array where the GPU leaves the oracle."""
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, **_tight())
+    _mass_inlet(m, c)
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
+    _setup(o, m, c)
+    _setup(g, m, c)
+    fields = ("u", "v", "w", "p", "mdot", "bmdot", "bu", "bv", "bw", "bp")
+    phases = (("momentum X", g.SolveMomentumX, lambda: o.momentum(0)),
+              ("momentum Y", g.SolveMomentumY, lambda: o.momentum(1)),
+              ("momentum Z", g.SolveMomentumZ, lambda: o.momentum(2)),
+              ("continuity", g.SolveContinuity, o.continuity))
+    for it in (1, 2):
+        g.set_iteration(it)
+        o.set_iter(it)
+        for name, gpu_phase, oracle_phase in phases:
+            gpu_phase()
+            oracle_phase()
+            for k in fields:
+                x, ref = g.get(k), o.get(k)
+                err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+                assert err <= 1e-9, (it, name, k, err)
+    g.close()
