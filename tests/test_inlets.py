@@ -11,13 +11,6 @@ import pytest
 
 from flowsolversourcecode_b200 import case as cs
 
-# The first B200 run of the mass-flow-inlet step started from a zero outlet
-# velocity, which made the first p' system inconsistent (net inflow), and left
-# the oracle at the second outer iteration; the setup now starts from the
-# step's outlet velocity.  These parity tests have not run on a GPU since, so
-# they stay expected failures until a GPU run confirms them.
-GPU_PARITY_PENDING = pytest.mark.xfail(strict=False, reason="GPU parity of this boundary type not yet confirmed")
-
 
 def _tight(**kw):
     kw.setdefault("solver_mom", "bicgs")
@@ -113,7 +106,6 @@ def test_oracle_mass_inlet_matches_velocity_inlet(turbulence):
 
 # ------------------------------------------------------------------- GPU
 @pytest.mark.gpu
-@GPU_PARITY_PENDING
 @pytest.mark.parametrize("turbulence", [False, True])
 def test_mass_inlet_step_matches_oracle(turbulence):
     import oracle
@@ -170,7 +162,6 @@ def test_oracle_pressure_inlet_step():
 
 
 @pytest.mark.gpu
-@GPU_PARITY_PENDING
 @pytest.mark.parametrize("turbulence", [False, True])
 def test_pressure_inlet_step_matches_oracle(turbulence):
     import oracle
@@ -223,7 +214,6 @@ def test_oracle_mass_outlet_step():
 
 
 @pytest.mark.gpu
-@GPU_PARITY_PENDING
 @pytest.mark.parametrize("turbulence", [False, True])
 def test_mass_outlet_step_matches_oracle(turbulence):
     import oracle
@@ -233,7 +223,9 @@ def test_mass_outlet_step_matches_oracle(turbulence):
     o = oracle.Oracle(m, c)
     g = Solver(m, c)
     for obj in (o, g):
-        for k, v in cs.bfs_initial_state(m, c, seed=0).items():
+        # no inlet perturbation: the specified outflow must balance the inflow,
+        # or the closed p' system has a net source and no solution
+        for k, v in cs.bfs_initial_state(m, c, seed=0, perturbation=0.0).items():
             obj.set(k, v)
         obj.initialize_mdot()
     for it in range(6):
@@ -249,7 +241,6 @@ def test_mass_outlet_step_matches_oracle(turbulence):
 
 
 @pytest.mark.gpu
-@GPU_PARITY_PENDING
 def test_mass_inlet_phases_match_oracle():
     """Phase by phase through the first two outer iterations of the
     mass-flow-inlet step (momentum X, Y, Z, then SolveContinuity), naming the
@@ -273,8 +264,14 @@ def test_mass_inlet_phases_match_oracle():
         for name, gpu_phase, oracle_phase in phases:
             gpu_phase()
             oracle_phase()
+            ref = {k: o.get(k) for k in fields}
+            # a velocity component is measured against the velocity's scale:
+            # w after the first Z solve is rounding noise (|w| ~ 1e-16 against
+            # |u| ~ 30), which no solver reproduces digit for digit
+            vel = max(np.linalg.norm(ref[k]) for k in ("u", "v", "w"))
+            bvel = max(np.linalg.norm(ref[k]) for k in ("bu", "bv", "bw"))
             for k in fields:
-                x, ref = g.get(k), o.get(k)
-                err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+                scale = vel if k in ("u", "v", "w") else bvel if k in ("bu", "bv", "bw") else np.linalg.norm(ref[k])
+                err = np.linalg.norm(g.get(k) - ref[k]) / max(scale, 1e-300)
                 assert err <= 1e-9, (it, name, k, err)
     g.close()
