@@ -19,7 +19,7 @@ Forms (same case, same initial state):
          iteration count and the converged fields change.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--ttr MAXIT]
+                  [--ttr MAXIT] (default 6000; 0 skips the time-to-residual legs)
   python bench.py --ensemble 64 [--gpus N]     the batched-ensemble configuration
   python bench.py --case distorted             the same cavity on the jittered mesh
   python bench.py --case bfs                   the k-epsilon backward-facing step (512x96x48)
@@ -27,14 +27,18 @@ Forms (same case, same initial state):
 b200 arm: `value` is device-timed (CUDA events on the solver's stream) with
 the state resident in HBM; `e2e` runs the fp64 steps through the C ABI
 fs_simple_iteration_host with the state in pinned host buffers, copies inside
-the timed region.  `--ttr MAXIT` adds the time to residual 1e-6 of both forms
-from the initial state (at 128^3 this takes thousands of iterations).  N>1
+the timed region.  On one GPU the time to residual 1e-6 of the fp64 form,
+the fp64 form with the p' solve to 1e-3 (fp64_rrf), and both mixed forms
+follows, from the initial state, with each form's converged fields against
+the fp64 form's (at 128^3 about 3,300 outer iterations per form; `--ttr 0`
+skips it, `--ttr MAXIT` caps the iterations).  N>1
 (torchrun) runs one independent replica per GPU (the single-mesh path does not
 shard) and reports the aggregate over ranks with the max-over-ranks time.
 reference arm: the CPU restatement of the reference's loop with the
 reference's own p' solver (unpreconditioned BiCGSTAB, same 1e-8 tolerance;
-the Fortran reference cannot be compiled in this image), timed on the host,
-rank 0 only.
+the Fortran reference cannot be compiled: no Fortran compiler on the host),
+its AxOMP loop on every host core as the reference's OpenMP build runs it,
+timed on the host, rank 0 only, within a 240 s budget.
 """
 from __future__ import annotations
 
@@ -58,6 +62,9 @@ FORMS = {
                   batched_momentum=True),
     "mixed_rrf": dict(solver_mom="sor", solver_cont="amg32_bicgs", krylov_tol=1e-3, krylov_maxit=200,
                       batched_momentum=True),
+    # the fp64 form with the same inexact p' solve: separates the gain of the
+    # tolerance from the gain of the FP32 preconditioner in time to residual
+    "fp64_rrf": dict(solver_mom="sor", solver_cont="amg_bicgs", krylov_tol=1e-3, krylov_maxit=200),
 }
 REFERENCE_SOLVERS = dict(solver_mom="sor", solver_cont="bicgs", krylov_tol=1e-8, krylov_maxit=300)
 
@@ -268,17 +275,37 @@ def solver_roofline(stats: dict, mg: dict | None, N: int, W: int, hbm: float, fo
             "iters_per_launch": best["iters"] / best["calls"]}
 
 
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_baseline_sample(n: int, kind: str = "cubic") -> dict:
+    """The CPU restatement of the reference's loop on this host: the 2nd
+    SIMPLE iteration of the same case (the 1st, from rest, is untimed) with
+    the reference's OpenMP loop (AxOMP) on every host core, then the 3rd on
+    one thread."""
     import oracle
     mesh, case, init = workload(n, "reference", kind)
+    cores = host_cores()
     o = start(oracle.Oracle(mesh, case), init)
+    o.simple_iteration()
+    oracle.set_threads(cores)
     t0 = time.perf_counter()
     o.simple_iteration()
     dt = time.perf_counter() - t0
+    oracle.set_threads(1)
+    t0 = time.perf_counter()
+    o.simple_iteration()
+    dt1 = time.perf_counter() - t0
     o.close()
-    return {"value": 1.0 / dt, "unit": "iter/s", "cores": 1, "kind": "port",
-            "sample": f"the 1st SIMPLE outer iteration of the same {mesh.n_cells}-cell case on the sequential "
-                      f"CPU restatement (p' by the reference's unpreconditioned BiCGSTAB to 1e-8), 1 thread"}
+    return {"value": 1.0 / dt, "unit": "iter/s", "cores": cores, "kind": "port", "value_1thread": 1.0 / dt1,
+            "sample": f"the 2nd SIMPLE outer iteration of the same {mesh.n_cells}-cell case on the CPU "
+                      f"restatement (p' by the reference's unpreconditioned BiCGSTAB to 1e-8), its AxOMP loop "
+                      f"on {cores} threads (all host cores); value_1thread: the 3rd iteration on 1 thread. "
+                      f"Reference Fortran build unavailable (no Fortran compiler on the host)"}
 
 
 def run_reference(args, rank: int) -> None:
@@ -286,14 +313,21 @@ def run_reference(args, rank: int) -> None:
         return
     import oracle
     oracle.build()
+    cores = host_cores()
+    oracle.set_threads(cores)
     mesh, case, init = workload(args.n, "reference", args.case)
     o = start(oracle.Oracle(mesh, case), init)
-    warm = 1
+    warm = max(args.warmup, 3)
+    budget = 240.0           # seconds for warm-up and timed steps together
     t0 = time.perf_counter()
+    w_run = 0
     for _ in range(warm):
         o.simple_iteration()
+        w_run += 1
+        if time.perf_counter() - t0 > budget / 4:
+            break
     t_warm = time.perf_counter() - t0
-    budget = 150.0
+    budget -= t_warm
     k_run = args.steps
     times = []
     for k in range(args.steps):
@@ -307,15 +341,17 @@ def run_reference(args, rank: int) -> None:
     val = k_run / total
     line = {
         "impl": "reference", "metric": "SIMPLE iters/s", "value": val, "unit": "iter/s", "n_gpus": args.gpus,
-        "steps": k_run, "warmup": warm, "ms_per_step": 1e3 * total / k_run,
+        "steps": k_run, "warmup": w_run, "ms_per_step": 1e3 * total / k_run,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{workload_name(args.n, args.case)}, {mesh.n_cells} cells, SOU, SIMPLEC",
                    "cells": mesh.n_cells,
-                   "solvers": "momentum sor, p' bicgs (the reference's unpreconditioned BiCGSTAB) to 1e-8"},
-        "cpu_baseline": {"value": val, "unit": "iter/s", "cores": 1, "kind": "port",
-                         "sample": f"{k_run} of {args.steps} requested SIMPLE iterations after {warm} untimed "
-                                   f"(time budget {budget:.0f}s) on the sequential CPU restatement; reference "
-                                   f"Fortran build unavailable (no Fortran compiler in the image)"},
+                   "solvers": "momentum sor, p' bicgs (the reference's unpreconditioned BiCGSTAB) to 1e-8",
+                   "budget": f"{k_run} of {args.steps} requested timed steps and {w_run} of {warm} warm-up steps "
+                             f"fit the 240 s budget of this arm"},
+        "cpu_baseline": {"value": val, "unit": "iter/s", "cores": cores, "kind": "port",
+                         "sample": f"{k_run} SIMPLE iterations after {w_run} untimed on the CPU restatement, its "
+                                   f"AxOMP loop (the reference's OpenMP region) on {cores} threads, all host cores; "
+                                   f"reference Fortran build unavailable (no Fortran compiler on the host)"},
         "e2e": {"value": val, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "warmup_s": t_warm,
     }
@@ -359,8 +395,10 @@ def assembly_roofline(leg: dict, N: int, F: int, steps: int, hbm: float) -> dict
             "frac": round(achieved / hbm, 4), "bytes_per_step": nbytes / steps, "ms_per_step": ms / steps}
 
 
-def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e-6, init=None) -> dict:
-    """Device time from the initial state until the stop metric drops below tol."""
+def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e-6, init=None,
+                     keys=("u", "v", "w", "p")) -> tuple[dict, dict]:
+    """Device time from the initial state until the stop metric drops below
+    tol; returns the record and the fields reached."""
     s = start(Solver(mesh, case, device=local), init)
     s.timer_start()
     total, it, src = 0.0, 0, None
@@ -373,9 +411,10 @@ def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e
         if src < tol:
             break
     total += s.timer_stop()
+    fields = {k: s.get(k) for k in keys}
     s.close()
-    return {"seconds": total * 1e-3, "iterations": it, "reached": bool(src is not None and src < tol),
-            "final_source": src}
+    return ({"seconds": total * 1e-3, "iterations": it, "reached": bool(src is not None and src < tol),
+             "final_source": src}, fields)
 
 
 def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
@@ -511,7 +550,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--case", default="cubic", choices=["cubic", "distorted", "bfs"])
-    ap.add_argument("--ttr", type=int, default=0, help="max iterations of the time-to-1e-6 leg (0: skip)")
+    ap.add_argument("--ttr", type=int, default=6000, help="max iterations of the time-to-1e-6 legs (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--learned", action="store_true", help="with --case bfs: train and measure the learned p' guess")
     ap.add_argument("--ensemble", type=int, default=0, help="run the batched-ensemble configuration with this many cases")
@@ -612,12 +651,21 @@ def main():
     sr.close()
 
     ttr = None
-    if args.ttr > 0:
-        ttr = {"fp64": time_to_residual(Solver, mesh, case, local, args.ttr, init=init),
-               "mixed": time_to_residual(Solver, mesh, case_m, local, args.ttr, init=init),
-               "mixed_rrf": time_to_residual(Solver, mesh, case_r, local, args.ttr, init=init)}
-        for k in ("mixed", "mixed_rrf"):
-            ttr[k]["time_vs_fp64"] = ttr[k]["seconds"] / ttr["fp64"]["seconds"]
+    if args.ttr > 0 and world == 1:
+        # every form from the same initial state to the stop metric 1e-6; the
+        # converged fields of each against the fp64 form's, and the times
+        # against both fp64 legs (same p' tolerance 1e-8, and 1e-3)
+        _, case_f, _ = workload(args.n, "fp64_rrf", kind)
+        ttr, tf = {}, {}
+        for name, c in (("fp64", case), ("fp64_rrf", case_f), ("mixed", case_m), ("mixed_rrf", case_r)):
+            ttr[name], tf[name] = time_to_residual(Solver, mesh, c, local, args.ttr, init=init, keys=fkeys)
+        for name in ("fp64_rrf", "mixed", "mixed_rrf"):
+            ttr[name]["time_vs_fp64"] = ttr[name]["seconds"] / ttr["fp64"]["seconds"]
+            ttr[name]["field_rel_l2_vs_fp64"] = {
+                k: float(np.linalg.norm(tf[name][k] - tf["fp64"][k]) / max(np.linalg.norm(tf["fp64"][k]), 1e-300))
+                for k in fkeys}
+        ttr["mixed_rrf"]["time_vs_fp64_rrf"] = ttr["mixed_rrf"]["seconds"] / ttr["fp64_rrf"]["seconds"]
+        ttr["tolerance"] = "stop metric (NstopType 4, normalised residual) below 1e-6 from the initial state"
 
     if rank == 0:
         hbm, src = peaks()

@@ -27,14 +27,14 @@ VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
 VAR_TKE, VAR_TED, VAR_RHOK = 8, 9, 10
 # boundary types
 (BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD, BC_OUTLET_SP, BC_INLET_MASS, BC_INLET_SP,
- BC_OUTLET_MASS) = range(9)
+ BC_OUTLET_MASS, BC_OUTLET_ASP) = range(10)
 TRANSIENT = {"euler": 0, "cranknicolson1": 1, "cranknicolson2": 2, "adamsmoulton": 3}
 # gradient interpolation
 GI_AVERAGE, GI_UPWIND, GI_DOWNWIND, GI_AVERAGECORRECTED = 0, 1, 2, 3
 HR_NONE, HR_TVD = 0, 1
 TVD = {n: i for i, n in enumerate(["upwind", "downwind", "fromm", "sou", "cd", "quick", "superbee", "minmod",
                                     "osher", "vanleer", "muscl", "smart", "hquick", "umist", "charm"])}
-SOLVER = {"sor": 0, "bicgs": 1, "amg": 2, "amg_bicgs": 3, "amg32_bicgs": 4, "gmres": 5}
+SOLVER = {"sor": 0, "bicgs": 1, "amg": 2, "amg_bicgs": 3, "amg32_bicgs": 4, "gmres": 5, "ilu": 6}
 SIMPLE, SIMPLEC = 0, 1
 
 FIELDS = ["u", "v", "w", "p", "pc", "mdot", "bu", "bv", "bw", "bp", "bpc", "bmdot", "ac", "bc", "anb",
@@ -150,6 +150,7 @@ PROTOTYPES = {
     "fs_mg_levels": (C.c_int, [_V, _I, _I, C.c_int]),
     "fs_mg_parents": (C.c_int, [_V, C.c_int, _I, C.c_size_t]),
     "fs_mg_info": (C.c_int, [_V, _I, C.c_int, _I, _I]),
+    "fs_mg_coarse_matrix": (C.c_int, [_V, C.c_int, _D, _I, _I, _D, C.c_size_t, C.c_size_t]),
     "fs_solver_kernel_ms": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "fs_nn_create": (C.c_int, [_V, C.c_int, C.c_uint64]),
     "fs_nn_mode": (C.c_int, [_V, C.c_int, C.c_int]),
@@ -208,7 +209,11 @@ def fptr(a):
 
 
 class FsError(RuntimeError):
-    pass
+    """A non-zero status of a C-ABI call; `status` holds the FS_E_* code."""
+
+    def __init__(self, message: str, status: int = 0):
+        super().__init__(message)
+        self.status = status
 
 
 def check(rc: int, ctx=None, what: str = "") -> None:
@@ -217,7 +222,7 @@ def check(rc: int, ctx=None, what: str = "") -> None:
         if ctx is not None and _lib is not None:
             m = _lib.fs_last_error(ctx)
             msg = m.decode() if m else ""
-        raise FsError(f"{what} failed with status {rc}: {msg}")
+        raise FsError(f"{what} failed with status {rc}: {msg}", rc)
 
 
 def mesh_struct(mesh) -> tuple[FsMeshIn, list]:

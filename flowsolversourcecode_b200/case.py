@@ -73,7 +73,8 @@ class Case:
     # patches: name -> (type, (u,v,w)); type "pressure_outlet" takes (type, static pressure),
     # "mass_inlet" ('specifiedmassflowrate') takes (type, (direction x,y,z), mass flow into the domain),
     # "pressure_inlet" ('specifiedstaticpressure' inlet) takes (type, (direction x,y,z), static pressure),
-    # "mass_outlet" ('specifiedmassflowrate' outlet) takes (type, mass flow out of the domain)
+    # "mass_outlet" ('specifiedmassflowrate' outlet) takes (type, mass flow out of the domain),
+    # "average_pressure_outlet" ('specifiedaveragestaticpressure') takes (type, average static pressure)
     patches: dict = field(default_factory=dict)
     # 'fullydeveloped' outlets: patch name -> MassFlowFraction (default 1)
     mass_flow_fraction: dict = field(default_factory=dict)
@@ -129,12 +130,13 @@ class Case:
         c.n_patches = len(mesh.patch_names)
         bct = {"wall": L.BC_WALL_NOSLIP, "slip": L.BC_WALL_SLIP, "symmetry": L.BC_SYMMETRY,
                "inlet": L.BC_INLET_VEL, "outlet": L.BC_OUTLET_FD, "pressure_outlet": L.BC_OUTLET_SP,
-               "mass_inlet": L.BC_INLET_MASS, "pressure_inlet": L.BC_INLET_SP, "mass_outlet": L.BC_OUTLET_MASS}
+               "mass_inlet": L.BC_INLET_MASS, "pressure_inlet": L.BC_INLET_SP, "mass_outlet": L.BC_OUTLET_MASS,
+               "average_pressure_outlet": L.BC_OUTLET_ASP}
         for s, name in enumerate(mesh.patch_names):
             spec = self.patches.get(name, ("wall", (0.0, 0.0, 0.0)))
             t, vel = spec[0], spec[1]
             c.patch_type[s] = bct[t]
-            if t == "pressure_outlet":   # (type, static pressure)
+            if t in ("pressure_outlet", "average_pressure_outlet"):   # (type, static | average static pressure)
                 c.patch_pressure[s] = float(vel)
             elif t == "mass_outlet":     # (type, mass flow)
                 c.patch_mass_flow[s] = float(vel)

@@ -289,6 +289,7 @@ int fs_destroy(fs_ctx *ctx) {
   cudaSetDevice(ctx->dev);
   if (ctx->st) cudaStreamSynchronize(ctx->st);
   fs_mg_free(ctx);
+  fs_ilu_free(ctx);
   fs_nn_free(ctx);
   fs_turb_free(ctx);
   fs_transient_free(ctx);
@@ -410,6 +411,15 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   if (ctx->cfg.turbulence)
     for (int q = 0; q < 2; q++)
       if (!std::isfinite(r.turb_abs[q])) { ctx->err = "NaN/Inf residual"; return FS_E_NAN; }
+  // divergence: the stop metric grew past FS_DIVERGENCE_FACTOR times the largest
+  // one of the earlier outer iterations of the run (or of the time step)
+  if (std::isfinite(r.source) && r.source > 0.) {
+    if (ctx->div_ref > 0. && r.source > FS_DIVERGENCE_FACTOR * ctx->div_ref) {
+      ctx->err = "diverged: the stop metric grew by more than 1e6 over its largest earlier value";
+      return FS_E_DIVERGED;
+    }
+    ctx->div_ref = fmax(ctx->div_ref, r.source);
+  }
   return FS_OK;
 }
 

@@ -27,7 +27,12 @@ __host__ __device__ inline bool fs_is_inlet(int t) {
 }
 // static pressure specified: Rhie-Chow boundary flux and p'_b = 0
 // (AssembleMdotUsingRhieChow.for:1441-1598, 2105-2283)
-__host__ __device__ inline bool fs_is_pressure(int t) { return t == FS_BC_OUTLET_SP || t == FS_BC_INLET_SP; }
+__host__ __device__ inline bool fs_is_pressure(int t) {
+  return t == FS_BC_OUTLET_SP || t == FS_BC_INLET_SP || t == FS_BC_OUTLET_ASP;
+}
+// static-pressure and average-static-pressure outlets: one treatment in every
+// routine but CorrectPressure (the loops of the two types are the same text)
+__host__ __device__ inline bool fs_is_sp_outlet(int t) { return t == FS_BC_OUTLET_SP || t == FS_BC_OUTLET_ASP; }
 // the velocity follows from Bmdot along a given direction (AssembleMdotUsingRhieChow.for:2089-2099)
 __device__ __forceinline__ void fs_directed_velocity(const double *bdir, const double *bsf, double rho, int B, int b,
                                                      double bm, double *bu, double *bv, double *bw) {
@@ -48,6 +53,7 @@ enum { RED_SUM0 = 0, RED_SUM1, RED_SUM2, RED_MAX0, RED_MAX1, RED_NQ };
 struct fs_mg_dev;  // multigrid hierarchy (fs_mg.cu)
 struct fs_turb;    // k-epsilon state (fs_turb.cu)
 struct fs_nn;      // learned p' initial guess (fs_nn.cu)
+struct fs_ilu;     // D-ILU level schedule (fs_solvers.cu)
 
 #define FS_NEQ 9        // equations with residual slots: NF 1..9
 #define FS_NITERS 16     // int32 iteration-count slots (NF - 1 indexed)
@@ -58,6 +64,7 @@ struct fs_ctx {
   fs_case cfg{};
   int N = 0, F = 0, B = 0, W = 0, NS = 0;
   int nIter = 0;
+  double div_ref = 0.;   // largest stop metric so far (divergence check), 0 = none yet
   int64_t launches = 0;
   std::string err;
   int num_sms = 148;
@@ -126,6 +133,8 @@ struct fs_ctx {
   fs_turb *turb = nullptr;
   // multigrid
   fs_mg_dev *mg = nullptr;
+  // level schedule and factor of the 'ilu' solver (built on first use)
+  fs_ilu *ilu = nullptr;
   // learned initial guess of the p' solve (nullptr: zero guess)
   fs_nn *nn = nullptr;
   const double *pc_guess = nullptr;   // set around the p' solve only
@@ -238,6 +247,7 @@ int fs_turb_effects(fs_ctx *ctx);
 int fs_flow_in_out(fs_ctx *ctx);
 int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);
+void fs_ilu_free(fs_ctx *ctx);
 int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);
 int fs_solver_stats_collect(fs_ctx *ctx);
 int fs_coop_per_sm(fs_ctx *ctx, int occupancy);         // CTAs per SM for a cooperative launch

@@ -68,6 +68,11 @@ struct LevelDev {
   R *b, *x, *r, *t;
   const int32_t *parent;        // this level -> next coarser (nullptr on the coarsest)
   const int32_t *rptr, *rlist;  // restriction into this level: finer rows per coarse row, ascending
+  // warp chunks of this level's rows for the fused restriction into it:
+  // chunk k is rows [chunk[k], chunk[k+1]), at most 32 rows and, unless one
+  // row alone has more, at most 64 finer rows (children) in all
+  const int32_t *chunk;
+  int nchunk;
 };
 
 struct fs_mg_dev {
@@ -79,6 +84,8 @@ struct fs_mg_dev {
   int32_t *cptr[FS_MG_MAXLEV] = {}, *clist[FS_MG_MAXLEV] = {}, *cmap[FS_MG_MAXLEV] = {};
   int32_t *rptr[FS_MG_MAXLEV] = {}, *rlist[FS_MG_MAXLEV] = {};
   int32_t *colors[FS_MG_MAXLEV] = {};   // rows by colour, then ncol+1 offsets
+  int32_t *chunk[FS_MG_MAXLEV] = {};    // warp chunks of coarse rows (fused restriction)
+  int nchunk[FS_MG_MAXLEV] = {};
   double *ac[FS_MG_MAXLEV] = {}, *anb[FS_MG_MAXLEV] = {}, *b[FS_MG_MAXLEV] = {}, *x[FS_MG_MAXLEV] = {}, *r[FS_MG_MAXLEV] = {};
   double *t[FS_MG_MAXLEV] = {};
   float *acf[FS_MG_MAXLEV] = {}, *anbf[FS_MG_MAXLEV] = {}, *bf[FS_MG_MAXLEV] = {}, *xf[FS_MG_MAXLEV] = {}, *rf[FS_MG_MAXLEV] = {};
@@ -367,6 +374,9 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
 #define FS_PC_TEAM_MAX 4096   // levels up to this many rows run on the CTA team
 #endif
 #define FS_PC_SPIN_LIMIT (1L << 20)   // polls of a team barrier before it reports a timeout
+#ifndef FS_PC_FUSE_DOWN
+#define FS_PC_FUSE_DOWN 2     // restrictions from levels below this one form the residual on the fly
+#endif
 
 template <class R>
 __device__ __forceinline__ Scope pc_scope(const LevelDev<R> &L) {
@@ -421,6 +431,7 @@ struct PCycle {
   int32_t *status;       // [0] set when a team barrier timed out
   unsigned gen;          // generation this CTA waits to leave
   int extra;             // arrivals waited for beyond the team (0; >0 only to test the timeout)
+  bool synced;           // the next enter() needs no barrier (the caller has just passed one)
   __device__ R om(int l) const { return l == 0 ? omega0 : omega; }
   __device__ R al(int l) const { return l == 0 ? alpha0 : alpha; }
   // barrier among the team CTAs: the arrival count in global memory, the last
@@ -460,7 +471,8 @@ struct PCycle {
   // the barrier before a phase: grid-wide when the grid is involved on either
   // side, among the team when the team is, else within CTA 0
   __device__ void enter(const Scope &sc) {
-    if (sc.grid || last.grid) S.all();
+    if (synced) synced = false;
+    else if (sc.grid || last.grid) S.all();
     else if (sc.team || last.team) { if ((int)blockIdx.x < team_size()) team_sync(); }
     else __syncthreads();
     last = sc;
@@ -609,6 +621,184 @@ struct PCycle {
     }
     enter(g);
   }
+
+  // ------------------------------------------------------------ fused V-cycle
+  // The same V-cycle (one pre- and one post-sweep, dense coarsest inverse) in
+  // one barrier phase per level and leg, with the same arithmetic in the same
+  // order as run():
+  //   down: the restriction into level l+1 forms the residual of each child
+  //     on the fly (no residual array, no phase of its own) for the first
+  //     FS_PC_FUSE_DOWN levels; a warp takes a chunk of coarse rows, a lane
+  //     two children, and each coarse row sums its children's residuals in
+  //     ascending order through shuffles;
+  //   up: the sweep of a row of level l >= 1 scatters its new value, times
+  //     alpha, to the row's children on level l-1 (the prolongation: every
+  //     finer row has one parent, so no two writes meet), and the coarsest
+  //     level's dense solve does the same; level 0's sweep writes `out`.
+  // The caller has set x_0 = omega0 in / ac_0 and passed a grid barrier.
+  __device__ void restrict_fused(int l, const double *__restrict__ in) {
+    const LevelDev<R> L = lev[l], C = lev[l + 1];
+    Scope sc = pc_scope(L);
+    enter(sc);
+    if (!sc.active()) return;
+    const bool first_sweep = l + 1 < lc || !direct;
+    const R omc = om(l + 1);
+    const int lane = threadIdx.x & 31;
+    const long w0 = sc.tid0() >> 5, nw = sc.nth() >> 5;
+    for (long k = w0; k < C.nchunk; k += nw) {
+      const int P0 = C.chunk[k], P1 = C.chunk[k + 1];
+      const int e0 = C.rptr[P0], e1 = C.rptr[P1];
+      const int P = P0 + lane;
+      const bool hasP = P < P1;
+      const int ra0 = hasP ? C.rptr[P] : e1, ra1 = hasP ? C.rptr[P + 1] : e1;
+      R s = 0.;
+      for (int base = e0; base < e1; base += 64) {
+        const int ea = base + lane, eb = ea + 32;
+        const bool hb = eb < e1;
+        const long ia = C.rlist[ea < e1 ? ea : e0], ib = C.rlist[hb ? eb : e0];
+        R t1 = 0., t2 = 0.;
+        ell_acc2<6, false>(t1, t2, L.n, L.w, L.nbr, L.anb, ia, ib, hb, [&](int q) { return L.x[q]; });
+        const R va = (l == 0 ? (R)in[ia] : L.b[ia]) - L.ac[ia] * L.x[ia] - t1;
+        R vb = 0.;
+        if (hb) vb = (l == 0 ? (R)in[ib] : L.b[ib]) - L.ac[ib] * L.x[ib] - t2;
+        // this lane's coarse row: its children inside [base, base+64), in order
+        const int lo = ra0 > base ? ra0 : base, hi = ra1 < base + 64 ? ra1 : base + 64;
+        const int cnt = hi > lo ? hi - lo : 0;
+        const int mx = __reduce_max_sync(0xffffffffu, cnt);
+        for (int m = 0; m < mx; m++) {
+          const int off = lo + m - base;
+          const R xa = __shfl_sync(0xffffffffu, va, off & 31);
+          const R xb = __shfl_sync(0xffffffffu, vb, off & 31);
+          if (m < cnt) s = s + (off < 32 ? xa : xb);
+        }
+      }
+      if (hasP) {
+        C.b[P] = s;
+        if (first_sweep) C.x[P] = omc * s / C.ac[P];
+      }
+    }
+  }
+  // the residual phase and the restriction of run() (levels past FS_PC_FUSE_DOWN)
+  __device__ void restrict_plain(int l, const double *__restrict__ in) {
+    const LevelDev<R> L = lev[l], C = lev[l + 1];
+    residual(l, in, L.x, L.r);
+    Scope scc = pc_scope(C);
+    enter(scc);
+    if (!scc.active()) return;
+    const bool first_sweep = l + 1 < lc || !direct;
+    if (scc.nth() < 2L * C.n) {
+      for (long P = scc.tid0(); P < C.n; P += scc.nth()) {
+        R s = 0.;
+        const int c0 = C.rptr[P], c1 = C.rptr[P + 1];
+        for (int c = c0; c < c1; c++) s = s + L.r[C.rlist[c]];
+        C.b[P] = s;
+        if (first_sweep) C.x[P] = om(l + 1) * s / C.ac[P];
+      }
+    } else
+      level_rows(scc, C.n, l + 1, [&](auto gg, long P, bool act, int q) {
+        constexpr int G = decltype(gg)::value;
+        R s = 0.;
+        if (act)
+          for (int c = C.rptr[P] + q; c < C.rptr[P + 1]; c += G) s = s + L.r[C.rlist[c]];
+        s = gsum<G>(s);
+        if (act && q == 0) {
+          C.b[P] = s;
+          if (first_sweep) C.x[P] = om(l + 1) * s / C.ac[P];
+        }
+      });
+  }
+  // x_{l-1}[c] += d for the children c of row i of level l (d = alpha x_l[i])
+  __device__ __forceinline__ void scatter_children(const LevelDev<R> &L, R *__restrict__ xf, long i, R d, int q0,
+                                                   int step) {
+    const int c1 = L.rptr[i + 1];
+    for (int c = L.rptr[i] + q0; c < c1; c += 4 * step) {
+      int f[4];
+      R v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) f[u] = c + u * step < c1 ? L.rlist[c + u * step] : -1;
+#pragma unroll
+      for (int u = 0; u < 4; u++) if (f[u] >= 0) v[u] = xf[f[u]];
+#pragma unroll
+      for (int u = 0; u < 4; u++) if (f[u] >= 0) xf[f[u]] = v[u] + d;
+    }
+  }
+  // the post-sweep of level l, then its prolongation into level l-1 (l >= 1)
+  // or the result into `out` (l = 0)
+  __device__ void smooth_scatter(int l, const double *__restrict__ in, double *__restrict__ out) {
+    const LevelDev<R> L = lev[l];
+    Scope sl = pc_scope(L);
+    enter(sl);
+    if (!sl.active()) return;
+    R *__restrict__ xf = l > 0 ? lev[l - 1].x : nullptr;
+    const R af = l > 0 ? al(l - 1) : (R)0.;
+    if (l == 0 || sl.nth() < 2L * L.n) {   // a thread per row, two rows per step
+      const long t0 = sl.tid0(), nt = sl.nth();
+      for (long i = t0; i < L.n; i += 2 * nt) {
+        const long i2 = i + nt;
+        const bool h2 = i2 < L.n;
+        R t1 = 0., t2 = 0.;
+        ell_acc2<6, false>(t1, t2, L.n, L.w, L.nbr, L.anb, i, i2, h2, [&](int k) { return L.x[k]; });
+        R xi = L.x[i], bi = l == 0 ? (R)in[i] : L.b[i];
+        R xn = xi + om(l) * (bi - L.ac[i] * xi - t1) / L.ac[i];
+        R xm = 0.;
+        if (h2) {
+          R xj = L.x[i2], bj = l == 0 ? (R)in[i2] : L.b[i2];
+          xm = xj + om(l) * (bj - L.ac[i2] * xj - t2) / L.ac[i2];
+        }
+        if (l == 0) {
+          out[i] = (double)xn;
+          if (h2) out[i2] = (double)xm;
+        } else {
+          scatter_children(L, xf, i, af * xn, 0, 1);
+          if (h2) scatter_children(L, xf, i2, af * xm, 0, 1);
+        }
+      }
+      return;
+    }
+    level_rows(sl, L.n, l, [&](auto gg, long i, bool act, int q) {
+      constexpr int G = decltype(gg)::value;
+      R t = 0.;
+      if (act) t = ell_part<G, G == 1 ? 8 : 4>(L.n, L.w, L.nbr, L.anb, i, q, [&](int k) { return L.x[k]; });
+      t = gsum<G>(t);
+      if (act) {
+        R xi = L.x[i], bi = L.b[i];
+        R xn = xi + om(l) * (bi - L.ac[i] * xi - t) / L.ac[i];
+        scatter_children(L, xf, i, af * xn, q, G);
+      }
+    });
+  }
+  // the dense coarsest solve (CTA 0, warps on rows), scattered into level lc-1
+  __device__ void coarsest_scatter() {
+    Scope c0;
+    c0.grid = false;
+    enter(c0);
+    if (blockIdx.x != 0) return;
+    const LevelDev<R> Cc = lev[lc];
+    R *__restrict__ xf = lev[lc - 1].x;
+    const R af = al(lc - 1);
+    const int n = Cc.n, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x >> 5; i < n; i += nw) {
+      double t = 0.;
+      for (int j = lane; j < n; j += 32) t += sinv[(long)i * n + j] * (double)Cc.b[j];
+      t = wsum(t);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      scatter_children(Cc, xf, i, af * (R)t, lane, 32);
+    }
+  }
+  __device__ void run_fused(const double *__restrict__ in, double *__restrict__ out) {
+    Scope g;
+    g.grid = true;
+    last.grid = true;
+    last.team = false;
+    synced = true;   // the caller's grid barrier stands for the first phase's
+    for (int l = 0; l < lc; l++) {
+      if (l < FS_PC_FUSE_DOWN) restrict_fused(l, in);
+      else restrict_plain(l, in);
+    }
+    coarsest_scatter();
+    for (int l = lc - 1; l >= 0; l--) smooth_scatter(l, in, out);
+    enter(g);
+  }
 };
 
 template <class R>
@@ -641,19 +831,24 @@ __device__ __forceinline__ void row_ax2(const A &a, long i, long i2, bool h2, co
   ell_acc2<6, false>(t1, t2, a.N, a.W, a.cn, a.anb, i, i2, h2, [&](int k) { return x[k]; });
 }
 
-// apply the preconditioner: out (FP64) = M^-1 in (FP64), via the R-precision V-cycle
-template <class R>
+// apply the preconditioner: out (FP64) = M^-1 in (FP64), via the R-precision
+// V-cycle; `fused`: the caller has set x_0 = omega0 in / ac_0 (run_fused)
+template <class R, bool FUSED>
 __device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, double *out, unsigned &gen) {
   Scope all;
   all.grid = true;
   PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, all,
-               (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0, a.teambar, a.status, gen, a.team_extra};
-  C.run(in, out);
+               (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0, a.teambar, a.status, gen, a.team_extra, false};
+  if (FUSED) C.run_fused(in, out);
+  else C.run(in, out);
   gen = C.gen;
 }
 
-// right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle
-template <class R>
+// right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle;
+// FUSED: the fused V-cycle (one pre- and one post-sweep, dense coarsest
+// level), whose first sweep from zero, x_0 = omega0 in / ac_0, rides on the
+// loops that form p and s
+template <class R, bool FUSED>
 __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(AmgKArgs<R> a) {
   Sync S(a.part);
   unsigned gen = 0;   // team-barrier generation (the counters are zeroed before the launch)
@@ -699,20 +894,26 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   double normb = sqrt(bb), rho = 1., alpha = 1., omega = 1.;
   int k = 0;
   double resn = sqrt(rr);
+  R *__restrict__ x0v = a.lev[0].x;
+  const R *__restrict__ ac0 = a.lev[0].ac;
+  const R om0 = (R)FS_MG_OMEGA0;
+  // r0 . r of the next iteration, formed with the residual update (r = r0 at first)
+  double rho_next = rr;
   while (k < a.maxit && resn > a.tol * normb && normb > 0.) {
     k++;
-    l0 = 0.;
-    for (long i = t0; i < N; i += nt) l0 += a.r0[i] * a.r[i];
-    double rho1;
-    S.sum2(l0, 0., rho1, dum);
+    const double rho1 = rho_next;
     // breakdown (r0 . r vanished: r at round-off): keep x.  Every CTA holds the
     // same sums, so every CTA takes the same branch.
     if (!(rho1 != 0.) || !isfinite(rho1)) break;
     double beta = (rho1 / rho) * (alpha / omega);
     rho = rho1;
-    for (long i = t0; i < N; i += nt) a.p[i] = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+    for (long i = t0; i < N; i += nt) {
+      const double pi = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+      a.p[i] = pi;
+      if (FUSED) x0v[i] = om0 * (R)pi / ac0[i];
+    }
     S.all();
-    apply_prec<R>(S, a, a.p, a.y, gen);                             // y = M^-1 p
+    apply_prec<R, FUSED>(S, a, a.p, a.y, gen);                      // y = M^-1 p
     l0 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
       const long i2 = i + nt;
@@ -727,7 +928,12 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     if (!(rv != 0.) || !isfinite(rho / rv)) break;
     alpha = rho / rv;
     l0 = 0.;
-    for (long i = t0; i < N; i += nt) { double si = a.r[i] - alpha * a.v[i]; a.s[i] = si; l0 += si * si; }
+    for (long i = t0; i < N; i += nt) {
+      const double si = a.r[i] - alpha * a.v[i];
+      a.s[i] = si;
+      l0 += si * si;
+      if (FUSED) x0v[i] = om0 * (R)si / ac0[i];
+    }
     double ss;
     S.sum2(l0, 0., ss, dum);
     if (sqrt(ss) <= a.tol * normb) {
@@ -735,7 +941,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
       resn = sqrt(ss);
       break;
     }
-    apply_prec<R>(S, a, a.s, a.z, gen);                             // z = M^-1 s
+    apply_prec<R, FUSED>(S, a, a.s, a.z, gen);                      // z = M^-1 s
     l0 = 0.; l1 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
       const long i2 = i + nt;
@@ -754,15 +960,16 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
       break;
     }
     omega = ts / tt;
-    l0 = 0.;
+    l0 = 0.; l1 = 0.;
     for (long i = t0; i < N; i += nt) {
       a.x[i] = a.x[i] + alpha * a.y[i] + omega * a.z[i];
       double ri = a.s[i] - omega * a.t[i];
       a.r[i] = ri;
       l0 += ri * ri;
+      l1 += a.r0[i] * ri;
     }
     double rn;
-    S.sum2(l0, 0., rn, dum);
+    S.sum2(l0, l1, rn, rho_next);
     resn = sqrt(rn);
   }
   S.all();
@@ -1073,6 +1280,17 @@ int fs_mg_build(fs_ctx *ctx) {
       for (int i = 0; i < h.n; i++) rlist[pos[M->h_parent[q][i]]++] = i;
       if ((rc = upv(ctx, &M->rptr[q + 1], rptr))) return rc;
       if ((rc = upv(ctx, &M->rlist[q + 1], rlist))) return rc;
+      // warp chunks of the coarse rows: consecutive rows, <= 32 of them and
+      // <= 64 children in all (a row with more children is a chunk alone)
+      std::vector<int32_t> ck(1, 0);
+      for (int P = 0, rows = 0, kids = 0; P < c.n; P++) {
+        const int k = rptr[P + 1] - rptr[P];
+        if (rows > 0 && (rows == 32 || kids + k > 64)) { ck.push_back(P); rows = 0; kids = 0; }
+        rows++; kids += k;
+      }
+      ck.push_back(c.n);
+      M->nchunk[q + 1] = (int)ck.size() - 1;
+      if ((rc = upv(ctx, &M->chunk[q + 1], ck))) return rc;
     }
     size_t n = h.n, nw = (size_t)h.w * h.n;
     if (q == 0) { M->ac[0] = ctx->ac; M->anb[0] = ctx->anb; }
@@ -1100,12 +1318,14 @@ int fs_mg_build(fs_ctx *ctx) {
     d.ac = M->ac[q]; d.anb = M->anb[q]; d.b = M->b[q]; d.x = M->x[q]; d.r = M->r[q]; d.t = M->t[q];
     d.parent = (q + 1 < M->nlev) ? M->parent[q] : nullptr;
     d.rptr = M->rptr[q]; d.rlist = M->rlist[q];
+    d.chunk = M->chunk[q]; d.nchunk = M->nchunk[q];
     L64[q] = d;
     LevelDev<float> e{};
     e.n = d.n; e.w = d.w; e.ncolors = d.ncolors; e.ncf = d.ncf; e.nbr = d.nbr; e.color_rows = d.color_rows;
     e.color_ptr = d.color_ptr; e.ac = M->acf[q]; e.anb = M->anbf[q]; e.b = M->bf[q]; e.x = M->xf[q]; e.r = M->rf[q];
     e.t = M->tf[q];
     e.parent = d.parent; e.rptr = d.rptr; e.rlist = d.rlist;
+    e.chunk = d.chunk; e.nchunk = d.nchunk;
     L32[q] = e;
   }
   FS_CK(cudaMalloc(&M->lev64, sizeof(LevelDev<double>) * M->nlev));
@@ -1129,9 +1349,12 @@ int fs_mg_build(fs_ctx *ctx) {
   // cooperative grid: smallest co-resident count of the three kernels, <= 4 CTAs/SM
   int a = 0, b = 0, c = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_mg_solve, FS_COOP_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double>, FS_COOP_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float>, FS_COOP_BLOCK, 0));
-  int per = std::min(a, std::min(b, c));
+  int b2 = 0, c2 = 0;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double, false>, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float, false>, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, (void *)k_amg_bicgstab<double, true>, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c2, (void *)k_amg_bicgstab<float, true>, FS_COOP_BLOCK, 0));
+  int per = std::min(std::min(a, std::min(b, c)), std::min(b2, c2));
   if (per < 1) { ctx->err = "multigrid kernels do not fit on an SM"; return FS_E_CUDA; }
   M->per_sm = per;   // occupancy limit; the grid follows the launch shape at each solve
   return FS_OK;
@@ -1141,7 +1364,7 @@ int fs_mg_free(fs_ctx *ctx) {
   fs_mg_dev *M = ctx->mg;
   if (!M) return FS_OK;
   for (int q = 0; q < M->nlev; q++) {
-    void *p[] = {M->colors[q], q ? M->nnb[q] : nullptr, q ? M->nbr[q] : nullptr, M->parent[q], M->cptr[q], M->clist[q],
+    void *p[] = {M->colors[q], M->chunk[q], q ? M->nnb[q] : nullptr, q ? M->nbr[q] : nullptr, M->parent[q], M->cptr[q], M->clist[q],
                  M->cmap[q], M->rptr[q], M->rlist[q], q ? M->ac[q] : nullptr, q ? M->anb[q] : nullptr, M->b[q], M->x[q],
                  M->r[q], M->acf[q], M->anbf[q], M->bf[q], M->xf[q], M->rf[q], M->t[q], M->tf[q]};
     for (void *x : p) if (x) cudaFree(x);
@@ -1225,20 +1448,24 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.status = ctx->d_status;
     a.team_extra = ctx->test_wait_extra;
   };
+  // the fused V-cycle needs one pre- and one post-sweep and a dense coarsest level
+  const bool fused = std::max(1, ctx->cfg.mg_pre) == 1 && M->direct && M->lc > 0;
   if (!f32) {
     AmgKArgs<double> a{};
     fill(a);
     a.lev = M->lev64;
     void *args[] = {&a};
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
-    FS_CK(fs_coop_launch((const void *)k_amg_bicgstab<double>, G, FS_COOP_BLOCK, args, ctx->st));
+    FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<double, true> : (const void *)k_amg_bicgstab<double, false>,
+                         G, FS_COOP_BLOCK, args, ctx->st));
   } else {
     AmgKArgs<float> a{};
     fill(a);
     a.lev = M->lev32;
     void *args[] = {&a};
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
-    FS_CK(fs_coop_launch((const void *)k_amg_bicgstab<float>, G, FS_COOP_BLOCK, args, ctx->st));
+    FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<float, true> : (const void *)k_amg_bicgstab<float, false>,
+                         G, FS_COOP_BLOCK, args, ctx->st));
   }
   FS_LAUNCH_CHECK();
   FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
@@ -1273,6 +1500,23 @@ extern "C" int fs_mg_info(fs_ctx *ctx, int32_t *widths, int max_levels, int32_t 
     for (int q = 0; q < ctx->mg->nlev && q < max_levels; q++) widths[q] = ctx->mg->w[q];
   if (prec_coarsest) *prec_coarsest = ctx->mg->lc;
   if (direct) *direct = ctx->mg->direct ? 1 : 0;
+  return FS_OK;
+}
+
+extern "C" int fs_mg_coarse_matrix(fs_ctx *ctx, int level, double *ac, int32_t *n_nbr, int32_t *nbr, double *anb,
+                                   size_t n, size_t w) {
+  if (!ctx || !ac || !n_nbr || !nbr || !anb) return FS_E_ARG;
+  int rc = fs_mg_build(ctx);
+  if (rc) return rc;
+  fs_mg_dev *M = ctx->mg;
+  if (level < 1 || level >= M->nlev || n != (size_t)M->n[level] || w != (size_t)M->w[level]) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  if ((rc = mg_coarse_matrices(ctx, level, false))) return rc;
+  FS_CK(cudaMemcpyAsync(ac, M->ac[level], sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaMemcpyAsync(anb, M->anb[level], sizeof(double) * n * w, cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaMemcpyAsync(n_nbr, M->nnb[level], sizeof(int32_t) * n, cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaMemcpyAsync(nbr, M->nbr[level], sizeof(int32_t) * n * w, cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaStreamSynchronize(ctx->st));
   return FS_OK;
 }
 

@@ -165,7 +165,7 @@ __global__ void k_bgrad(BGradJob J, int N, int B, const int32_t *__restrict__ bo
     int var = J.var[q];
     bool vel = (var == FS_VAR_U || var == FS_VAR_V || var == FS_VAR_W);
     bool prs = (var == FS_VAR_P || var == FS_VAR_RHOK);   // 'press' and 'rhok' (CalculateGradients.for:266-271)
-    if ((vel && (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP)) || (prs && t == FS_BC_SYMMETRY)) {
+    if ((vel && (t == FS_BC_OUTLET_FD || fs_is_sp_outlet(t))) || (prs && t == FS_BC_SYMMETRY)) {
       // CorrectGradientAtOulet / CorrectPressureGradientAtSymmetryBoundary, nz=BFaceAreanz(i,i)
       ox = gx * (1. - nx * nx) - gy * nx * ny - gz * nx * nzi;
       oy = gy * (1. - ny * ny) - gx * ny * nx - gz * ny * nzi;
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
         double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
         fcf = fcf + fcl;
         tf = tf + (fcl * phi + ffl * bp);
-      } else if (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {
+      } else if (t == FS_BC_OUTLET_FD || fs_is_sp_outlet(t)) {
         double bm = a.bmdot[b];
         double fcl = fmax(bm, 0.), ffl = -fmax(-bm, 0.);
         double fvl = bm * (bfg[b] * a.bdv[b] + bfg[B + b] * a.bdv[B + b] + bfg[B2 + b] * a.bdv[B2 + b]);
@@ -670,6 +670,7 @@ __global__ void k_bcorr(CorrArgs a) {
       a.bv[b] = a.bv[b] - a.dv2[i1] * a.pcg[N + i1];
       a.bw[b] = a.bw[b] - a.dw2[i1] * a.pcg[2L * N + i1];
     }
+    if (t == FS_BC_OUTLET_ASP) a.bp[b] = a.p[i1];   // CorrectPressure.for:169-176; k_avg_pressure shifts it
   } else if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
     a.bp[b] = a.p[i1] + a.bpg[b] * a.bdv[b] + a.bpg[B + b] * a.bdv[B + b] + a.bpg[B2 + b] * a.bdv[B2 + b];
   } else {
@@ -688,6 +689,26 @@ __global__ void k_bcorr(CorrArgs a) {
     double q = a.u[i1] * nx + a.v[i1] * ny + a.w[i1] * nz;
     a.bu[b] = a.u[i1] - q * nx; a.bv[b] = a.v[i1] - q * ny; a.bw[b] = a.w[i1] - q * nz;
   }
+}
+
+// 'specifiedaveragestaticpressure' outlets (CorrectPressure.for:178-203): the
+// face pressures (the owners', set by k_bcorr) shifted so that their area
+// average is AverageOutletPressure; one CTA per patch, fixed-order sums
+struct AvgPatch { int n; int start[FS_MAX_PATCHES], cnt[FS_MAX_PATCHES]; double target[FS_MAX_PATCHES]; };
+__global__ void __launch_bounds__(1024) k_avg_pressure(AvgPatch ap, const double *__restrict__ bfa, double *bp) {
+  __shared__ double sh[32];
+  __shared__ double shift;
+  const int q = blockIdx.x;
+  if (q >= ap.n) return;
+  const int b0 = ap.start[q], n = ap.cnt[q];
+  double s = 0., ar = 0.;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) { s = s + bfa[b0 + j] * bp[b0 + j]; ar = ar + bfa[b0 + j]; }
+  s = block_sum(s, sh);
+  ar = block_sum(ar, sh);
+  if (threadIdx.x == 0) shift = ap.target[q] - s / (ar + 1.0e-15);
+  __syncthreads();
+  const double d = shift;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) bp[b0 + j] = bp[b0 + j] + d;
 }
 
 // mass imbalance per cell (CalculateContinuityResiduals.for:130-183): partial sums,
@@ -988,6 +1009,12 @@ int fs_continuity_correct(fs_ctx *ctx) {
   FS_LAUNCH_CHECK();
   if (F) { k_corr_mdot<<<fs_grid(F), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   if (B) { k_bcorr<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  AvgPatch ap{};
+  for (int s = 0; s < ctx->NS; s++)
+    if (c.patch_type[s] == FS_BC_OUTLET_ASP) {
+      ap.start[ap.n] = ctx->h_bset_start[s]; ap.cnt[ap.n] = ctx->h_bset_n[s]; ap.target[ap.n] = c.patch_pressure[s]; ap.n++;
+    }
+  if (ap.n) { k_avg_pressure<<<ap.n, 1024, 0, ctx->st>>>(ap, ctx->bfa, ctx->bp); FS_LAUNCH_CHECK(); }
   k_mass_imbalance<<<a.nblk, FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();
   InletRanges ir{};

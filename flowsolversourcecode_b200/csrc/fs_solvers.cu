@@ -14,6 +14,7 @@
 #include "fs_internal.cuh"
 #include <cooperative_groups.h>
 #include <algorithm>
+#include <array>
 
 namespace cg = cooperative_groups;
 
@@ -597,6 +598,9 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_gmres(GmresAr
   if (tid0 == 0) { *a.iters = total; a.diag[0] = normminG * normb0; a.diag[1] = normb0; }
 }
 
+struct IluArgs;
+__global__ void k_ilu(IluArgs a);
+
 static int coop_grid_size(fs_ctx *ctx) {
   if (ctx->coop_grid > 0) return FS_OK;
   int a = 0, b = 0, c = 0;
@@ -606,6 +610,7 @@ static int coop_grid_size(fs_ctx *ctx) {
   int d = 0, e = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, (void *)k_sor3_colour, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, (void *)k_gmres, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_ilu, FS_COOP_BLOCK, 0));
   int per_sm = std::min(std::min(std::min(a, d), std::min(b, c)), e);
   if (per_sm < 1) { ctx->err = "cooperative kernel does not fit on an SM"; return FS_E_CUDA; }
   ctx->coop_grid = ctx->num_sms * fs_coop_per_sm(ctx, per_sm);
@@ -636,6 +641,185 @@ static int coop_launch(fs_ctx *ctx, void *fn, SolveArgs &a) {
   FS_CK(fs_coop_launch(fn, G, FS_COOP_BLOCK, args, ctx->st));
   FS_LAUNCH_CHECK();
   return FS_OK;
+}
+
+// ======================================================================
+// 'ilu' (SolveAlegbraicEquations.for:122-133): ILUFactorization once
+// (FactorizeUsingILU.for:4-75), then SolveEquationsUsingILU sweeps
+// (ILUMethod.for:4-170) and CheckConvergence until sum|r| <= rrF*IResiduals
+// or itmax.  The factorisation and both substitutions are sequential in
+// element order; here each runs level by level (a row's level is one more
+// than that of the rows it waits for), one grid barrier per level, and every
+// row applies its terms in the order the sequential loops apply them, so the
+// factor and the sweeps are those of the element-order loops bit for bit.
+//   lower list of row j: entries (i, sj, si) for every slot si of an earlier
+//     neighbour i that points to j, sorted by (i, si); sj is the first slot
+//     of j pointing to i (the reference's search loops)
+//   forward levels: over the lower lists; backward levels: over the later
+//     neighbours in the slot table
+struct fs_ilu {
+  int nlf = 0, nlb = 0;
+  int32_t *lo_ptr = nullptr, *lo_i = nullptr, *lo_sj = nullptr, *lo_si = nullptr;
+  int32_t *fl_ptr = nullptr, *fl_rows = nullptr, *bl_ptr = nullptr, *bl_rows = nullptr;
+  double *dc = nullptr, *rc = nullptr;
+};
+
+struct IluArgs {
+  int N, W, nlf, nlb, itmax;
+  const int32_t *ncf, *cn, *lo_ptr, *lo_i, *lo_sj, *lo_si, *fl_ptr, *fl_rows, *bl_ptr, *bl_rows;
+  const double *ac, *anb, *bc;
+  double *x, *dc, *rc, *part;
+  const double *ires;
+  double rrf;
+  int32_t *iters;
+  double *diag;
+};
+
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_ilu(IluArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  const int N = a.N;
+  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+  const int32_t *__restrict__ cn = a.cn;
+  const double *__restrict__ anb = a.anb;
+  // ILUFactorization: dc = 1/(ac - sum a_ji dc_i a_ij); element N-2 (the
+  // reference's NumberOfElements-1) updates none of its later neighbours
+  for (int L = 0; L < a.nlf; L++) {
+    for (long q = a.fl_ptr[L] + tid0; q < a.fl_ptr[L + 1]; q += nth) {
+      const int j = a.fl_rows[q];
+      double d = a.ac[j];
+      for (int e = a.lo_ptr[j]; e < a.lo_ptr[j + 1]; e++) {
+        const int i = a.lo_i[e];
+        if (i == N - 2) continue;
+        d = d - anb[(long)a.lo_sj[e] * N + j] * a.dc[i] * anb[(long)a.lo_si[e] * N + i];
+      }
+      a.dc[j] = 1.0 / d;
+    }
+    grid.sync();
+  }
+  double ires = *a.ires, fres = ires;
+  int iter = 0, buf = 0;
+  while (fres > a.rrf * ires && iter < a.itmax) {
+    // residual (ILUMethod.for:20-40)
+    for (long i = tid0; i < N; i += nth) {
+      double res = -a.ac[i] * a.x[i] + a.bc[i];
+      for (int j = 0; j < a.ncf[i]; j++) {
+        const int k = cn[(long)j * N + i];
+        if (k >= 0) res = res - anb[(long)j * N + i] * a.x[k];
+      }
+      a.rc[i] = res;
+    }
+    grid.sync();
+    // forward substitution (:44-100): row j takes dc_i rc_i of each earlier neighbour
+    for (int L = 0; L < a.nlf; L++) {
+      for (long q = a.fl_ptr[L] + tid0; q < a.fl_ptr[L + 1]; q += nth) {
+        const int j = a.fl_rows[q];
+        double r = a.rc[j];
+        for (int e = a.lo_ptr[j]; e < a.lo_ptr[j + 1]; e++) {
+          const int i = a.lo_i[e];
+          const double product1 = a.dc[i] * a.rc[i];
+          r = r - anb[(long)a.lo_sj[e] * N + j] * product1;
+        }
+        a.rc[j] = r;
+      }
+      grid.sync();
+    }
+    // backward substitution (:104-150): later neighbours in slot order, then dphi += dc rc
+    for (int L = 0; L < a.nlb; L++) {
+      for (long q = a.bl_ptr[L] + tid0; q < a.bl_ptr[L + 1]; q += nth) {
+        const int i = a.bl_rows[q];
+        double r = a.rc[i];
+        if (i < N - 1)
+          for (int j2 = 0; j2 < a.ncf[i]; j2++) {
+            const int j = cn[(long)j2 * N + i];
+            if (j > i) r = r - anb[(long)j2 * N + i] * a.rc[j];
+          }
+        const double product1 = a.dc[i] * r;
+        a.rc[i] = product1;
+        a.x[i] = a.x[i] + product1;
+      }
+      grid.sync();
+    }
+    // CheckConvergence
+    double l0 = 0., dum;
+    for (long i = tid0; i < N; i += 2 * nth) {
+      const long i2 = i + nth;
+      const bool h2 = i2 < N;
+      double q1 = a.bc[i] - a.ac[i] * a.x[i], q2 = h2 ? a.bc[i2] - a.ac[i2] * a.x[i2] : 0.;
+      ell_acc2<6, true>(q1, q2, N, a.W, cn, anb, i, i2, h2, [&](int k) { return a.x[k]; });
+      l0 += fabs(q1);
+      if (h2) l0 += fabs(q2);
+    }
+    grid_sum2(grid, a.part, buf, l0, 0., fres, dum); buf ^= 1;
+    iter++;
+  }
+  if (tid0 == 0) { *a.iters = iter; a.diag[0] = fres; a.diag[1] = ires; }
+}
+
+static int ilu_build(fs_ctx *ctx) {
+  if (ctx->ilu) return FS_OK;
+  const int N = ctx->N, W = ctx->W;
+  const std::vector<int32_t> &ncf = ctx->h_ncf, &cn = ctx->h_cn;
+  std::vector<std::vector<std::array<int32_t, 3>>> lo(N);
+  for (int i = 0; i < N; i++)
+    for (int si = 0; si < ncf[i]; si++) {
+      const int j = cn[(size_t)si * N + i];
+      if (j > i && j < N) {
+        int sj = -1;
+        for (int q = 0; q < ncf[j]; q++) if (cn[(size_t)q * N + j] == i) { sj = q; break; }
+        if (sj < 0) { ctx->err = "ilu: a neighbour does not list the cell back"; return FS_E_MESH; }
+        lo[j].push_back({i, sj, si});   // visited in (i, si) order already
+      }
+    }
+  std::vector<int32_t> lo_ptr(N + 1, 0), lo_i, lo_sj, lo_si, lf(N, 0), lb(N, 0);
+  int nlf = 0, nlb = 0;
+  for (int j = 0; j < N; j++) {
+    lo_ptr[j + 1] = lo_ptr[j] + (int)lo[j].size();
+    int L = 0;
+    for (auto &e : lo[j]) { lo_i.push_back(e[0]); lo_sj.push_back(e[1]); lo_si.push_back(e[2]); L = std::max(L, lf[e[0]] + 1); }
+    lf[j] = L; nlf = std::max(nlf, L + 1);
+  }
+  for (int i = N - 1; i >= 0; i--) {
+    int L = 0;
+    for (int q = 0; q < ncf[i]; q++) { const int j = cn[(size_t)q * N + i]; if (j > i) L = std::max(L, lb[j] + 1); }
+    lb[i] = L; nlb = std::max(nlb, L + 1);
+  }
+  auto by_level = [&](const std::vector<int32_t> &lev, int nl, std::vector<int32_t> &ptr, std::vector<int32_t> &rows) {
+    ptr.assign(nl + 1, 0);
+    for (int r = 0; r < N; r++) ptr[lev[r] + 1]++;
+    for (int L = 0; L < nl; L++) ptr[L + 1] += ptr[L];
+    std::vector<int32_t> pos(ptr.begin(), ptr.end() - 1);
+    rows.assign(N, 0);
+    for (int r = 0; r < N; r++) rows[pos[lev[r]]++] = r;
+  };
+  std::vector<int32_t> fl_ptr, fl_rows, bl_ptr, bl_rows;
+  by_level(lf, nlf, fl_ptr, fl_rows);
+  by_level(lb, nlb, bl_ptr, bl_rows);
+  fs_ilu *I = new fs_ilu();
+  ctx->ilu = I;
+  I->nlf = nlf; I->nlb = nlb;
+  auto up = [&](int32_t **d, const std::vector<int32_t> &h) -> int {
+    FS_CK(cudaMalloc((void **)d, std::max<size_t>(h.size(), 1) * sizeof(int32_t)));
+    if (!h.empty()) FS_CK(cudaMemcpy(*d, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    return FS_OK;
+  };
+  int rc;
+  if ((rc = up(&I->lo_ptr, lo_ptr)) || (rc = up(&I->lo_i, lo_i)) || (rc = up(&I->lo_sj, lo_sj)) ||
+      (rc = up(&I->lo_si, lo_si)) || (rc = up(&I->fl_ptr, fl_ptr)) || (rc = up(&I->fl_rows, fl_rows)) ||
+      (rc = up(&I->bl_ptr, bl_ptr)) || (rc = up(&I->bl_rows, bl_rows)))
+    return rc;
+  FS_CK(cudaMalloc(&I->dc, sizeof(double) * N));
+  FS_CK(cudaMalloc(&I->rc, sizeof(double) * N));
+  (void)W;
+  return FS_OK;
+}
+
+void fs_ilu_free(fs_ctx *ctx) {
+  fs_ilu *I = ctx->ilu;
+  if (!I) return;
+  void *p[] = {I->lo_ptr, I->lo_i, I->lo_sj, I->lo_si, I->fl_ptr, I->fl_rows, I->bl_ptr, I->bl_rows, I->dc, I->rc};
+  for (void *x : p) if (x) cudaFree(x);
+  delete I;
+  ctx->ilu = nullptr;
 }
 
 static SolveArgs solve_args(fs_ctx *ctx, int nf, double rrf, int itmax) {
@@ -681,6 +865,24 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
     k_from_colour<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->dphiP, ctx->dphi);
     FS_LAUNCH_CHECK();
+  } else if (solver == FS_SOLVER_ILU) {
+    if ((rc = ilu_build(ctx))) return rc;
+    if ((rc = coop_grid_size(ctx))) return rc;
+    fs_ilu *I = ctx->ilu;
+    IluArgs g{};
+    g.N = N; g.W = ctx->W; g.nlf = I->nlf; g.nlb = I->nlb; g.itmax = itmax;
+    g.ncf = ctx->ncf; g.cn = ctx->cn; g.lo_ptr = I->lo_ptr; g.lo_i = I->lo_i; g.lo_sj = I->lo_sj; g.lo_si = I->lo_si;
+    g.fl_ptr = I->fl_ptr; g.fl_rows = I->fl_rows; g.bl_ptr = I->bl_ptr; g.bl_rows = I->bl_rows;
+    g.ac = ctx->ac; g.anb = ctx->anb; g.bc = ctx->bc; g.x = ctx->dphi; g.dc = I->dc; g.rc = I->rc; g.part = ctx->red;
+    g.ires = a.ires; g.rrf = rrf; g.iters = a.iters; g.diag = a.diag;
+    int G = ctx->coop_grid;
+    long need = (N + FS_COOP_BLOCK - 1) / FS_COOP_BLOCK;
+    if (need < G) G = (int)(need < 1 ? 1 : need);
+    void *args[] = {&g};
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
+    FS_CK(fs_coop_launch((const void *)k_ilu, G, FS_COOP_BLOCK, args, ctx->st));
+    FS_LAUNCH_CHECK();
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
   } else if (solver == FS_SOLVER_BICGS) {
     a.itmax = ctx->cfg.krylov_maxit;
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
@@ -758,9 +960,12 @@ int fs_solver_stats_collect(fs_ctx *ctx) {
 //   - nothing in the array has to start at zero: the kernel writes every work
 //     entry (r0, r, p first, then v, s, t, then the partial sums) before it
 //     reads it in the same call, so the previous call's contents are ignored;
-//   - the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make that
-//     first call before any stream capture that should contain the solve.
+//   - the first call on a device does the set-up: with that device current
+//     it looks up the array's device address with cudaGetSymbolAddress and
+//     caches it, keyed on the CUDA context current at the call.  A call under
+//     another context of the same device (a driver-API context, or the
+//     primary context re-created after cudaDeviceReset) repeats the set-up.
+//     Make the first call on a device before any stream capture begins.
 // ======================================================================
 #define FS_NOALLOC_VECS 6
 #define FS_NOALLOC_PARTS (6 * FS_RED_BLOCKS)
@@ -770,9 +975,26 @@ static __device__ __align__(256) double g_noalloc_scratch[FS_NOALLOC_VECS * (siz
 
 #include <mutex>
 namespace {
-struct NoallocDev { double *base = nullptr; int grid = 0; };
+struct NoallocDev { double *base = nullptr; int grid = 0; void *cuctx = nullptr; };
 std::mutex g_noalloc_mu;
 NoallocDev g_noalloc_dev[64];
+
+// the CUDA context current on this thread (cuCtxGetCurrent through the
+// runtime's driver entry point, so the library needs no link to libcuda)
+int noalloc_current_context(void **cuctx) {
+  typedef int (*CtxGetCurrent)(void **);
+  static CtxGetCurrent fn = nullptr;
+  if (!fn) {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !f)
+      return FS_E_CUDA;
+    fn = (CtxGetCurrent)f;
+  }
+  *cuctx = nullptr;
+  return fn(cuctx) == 0 ? FS_OK : FS_E_CUDA;   // null when no context is current yet
+}
 }  // namespace
 
 extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, const int32_t *cn,
@@ -782,13 +1004,18 @@ extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, con
   if (n > FS_NOALLOC_MAX_ROWS) return FS_E_TOO_LARGE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FS_E_CUDA;
+  void *cuctx = nullptr;
   NoallocDev d;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_dev[dev].base) {
-      // once per device, with that device current: the symbol's device address
+    if (noalloc_current_context(&cuctx) != FS_OK) return FS_E_CUDA;
+    if (!cuctx || !g_noalloc_dev[dev].base || g_noalloc_dev[dev].cuctx != cuctx) {
+      // once per device and context, with that device current: the symbol's
+      // device address (the lookup also makes the primary context current
+      // when no context was)
       double *ptr = nullptr;
       if (cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return FS_E_CUDA;
+      if (noalloc_current_context(&cuctx) != FS_OK || !cuctx) return FS_E_CUDA;
       int per_sm = 0, per_sm2 = 0, sms = 0;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_bicgstab, FS_COOP_BLOCK, 0) != cudaSuccess ||
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, (const void *)k_sor_colour, FS_COOP_BLOCK, 0) != cudaSuccess ||
@@ -800,6 +1027,7 @@ extern "C" int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, con
       if (g > FS_RED_BLOCKS) g = FS_RED_BLOCKS;
       g_noalloc_dev[dev].base = ptr;
       g_noalloc_dev[dev].grid = g;
+      g_noalloc_dev[dev].cuctx = cuctx;
     }
     d = g_noalloc_dev[dev];
   }

@@ -166,6 +166,7 @@ int fs_advance_time(fs_ctx *ctx, double dt_next) {
   ctx->time = ctx->time + ctx->dt;
   ctx->ndt++;
   ctx->nIter = 0;
+  ctx->div_ref = 0.;   // the divergence check restarts with the time step
   return FS_OK;
 }
 

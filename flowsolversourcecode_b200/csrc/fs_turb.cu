@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_TURB_MINB) k_turb_assemble(TurbAr
           fcf = fcl;
           tf = fcl * ps + ffl * a.bphi[b] + fvl;
         }
-        if (fs_is_inlet(t) || t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP || t == FS_BC_OUTLET_MASS) {
+        if (fs_is_inlet(t) || t == FS_BC_OUTLET_FD || fs_is_sp_outlet(t) || t == FS_BC_OUTLET_MASS) {
           double cc = fmax(bm, 0.), cn_ = -fmax(-bm, 0.);
           fcf = fcf + cc;
           tf = tf + (cc * ps + cn_ * a.bphi[b]);
@@ -331,7 +331,7 @@ __global__ void k_turb_bound(int N, int B, const int32_t *bown, const int32_t *b
   if (t < N) phi[t] = fmax(phi[t], TINY);
   if (t < B) {
     int ty = btype[t];
-    if (ty == FS_BC_OUTLET_FD || ty == FS_BC_OUTLET_SP || ty == FS_BC_OUTLET_MASS || ty == FS_BC_SYMMETRY)
+    if (ty == FS_BC_OUTLET_FD || fs_is_sp_outlet(ty) || ty == FS_BC_OUTLET_MASS || ty == FS_BC_SYMMETRY)
       bphi[t] = fmax(phi[bown[t]], TINY);
     else bphi[t] = fmax(bphi[t], 0.);
   }
@@ -596,7 +596,7 @@ int fs_turb_effects(fs_ctx *ctx) {
 int fs_flow_in_out(fs_ctx *ctx) {
   const fs_case &c = ctx->cfg;
   int nfd = 0, other = 0;
-  for (int s = 0; s < ctx->NS; s++) { nfd += c.patch_type[s] == FS_BC_OUTLET_FD; other += c.patch_type[s] == FS_BC_OUTLET_SP || c.patch_type[s] == FS_BC_OUTLET_MASS; }
+  for (int s = 0; s < ctx->NS; s++) { nfd += c.patch_type[s] == FS_BC_OUTLET_FD; other += fs_is_sp_outlet(c.patch_type[s]) || c.patch_type[s] == FS_BC_OUTLET_MASS; }
   if (!nfd || other) return FS_OK;   // FlowOut / AdjustFlow act only when every outlet is fully developed
   FlowArgs a{};
   a.B = ctx->B; a.NS = ctx->NS; a.rho = c.rho;

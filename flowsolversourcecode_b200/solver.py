@@ -261,6 +261,20 @@ class Solver:
         return {"sizes": sizes[:k].tolist(), "widths": widths[:k].tolist(), "prec_coarsest": lc.value,
                 "direct": bool(direct.value)}
 
+    def mg_coarse_matrix(self, level: int) -> dict:
+        """AssembleAgglomeratedLHS of the last assembled system: the matrix of
+        multigrid level `level` >= 1 (ac, n_nbr, nbr and anb slot-major)."""
+        info = self.mg_info()
+        sizes = np.zeros(16, np.int32)
+        nl = C.c_int()
+        self._chk(self.lib.fs_mg_levels(self.ctx, C.byref(nl), L.iptr(sizes), 16), "mg_levels")
+        n, w = int(sizes[level]), int(info["widths"][level])
+        out = {"ac": np.zeros(n), "n_nbr": np.zeros(n, np.int32), "nbr": np.zeros(n * w, np.int32),
+               "anb": np.zeros(n * w)}
+        self._chk(self.lib.fs_mg_coarse_matrix(self.ctx, level, L.dptr(out["ac"]), L.iptr(out["n_nbr"]),
+                                               L.iptr(out["nbr"]), L.dptr(out["anb"]), n, w), "mg_coarse_matrix")
+        return out
+
     def set_launch_shape(self, ctas_per_sm: int):
         """Cooperative CTAs per SM of the persistent solver kernels (0: default)."""
         self._chk(self.lib.fs_set_launch_shape(self.ctx, ctas_per_sm), "fs_set_launch_shape")

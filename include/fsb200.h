@@ -36,11 +36,17 @@ extern "C" {
 #define FS_E_CUDA        -2   /* CUDA runtime error */
 #define FS_E_NOMEM       -3   /* device allocation failed */
 #define FS_E_NAN         -4   /* NaN/Inf detected in a residual */
-#define FS_E_DIVERGED    -5   /* residual grew by > 1e6 */
+#define FS_E_DIVERGED    -5   /* stop metric grew by > FS_DIVERGENCE_FACTOR */
 #define FS_E_TIMEOUT     -6   /* bounded device wait gave up */
 #define FS_E_MESH        -7   /* inconsistent mesh */
 #define FS_E_UNSUPPORTED -8   /* option not implemented */
 #define FS_E_TOO_LARGE   -9   /* problem larger than a fixed-size scratch allows */
+
+/* An outer iteration whose stop metric exceeds FS_DIVERGENCE_FACTOR times
+ * the largest stop metric of the context's earlier outer iterations (of the
+ * current time step, for unsteady runs) returns FS_E_DIVERGED.  The
+ * reference has no such check (it prints and continues). */
+#define FS_DIVERGENCE_FACTOR 1e6
 
 /* ------------------------------------------------------- variable ids (NF)
  * GetNFfromVariable (AlgebraicSolvers/AssignNFvaluesToVariables.for:4):
@@ -91,8 +97,12 @@ enum fs_bc {
                             * direction (xVeldirection...), patch_mass_flow the inflow */
   FS_BC_INLET_SP    = 7,   /* 'inlet','specifiedstaticpressure': patch_pressure, and
                             * patch_vel the velocity direction */
-  FS_BC_OUTLET_MASS = 8    /* 'outlet','specifiedmassflowrate': patch_mass_flow leaves the
+  FS_BC_OUTLET_MASS = 8,   /* 'outlet','specifiedmassflowrate': patch_mass_flow leaves the
                             * domain, along the owner cell's velocity */
+  FS_BC_OUTLET_ASP  = 9    /* 'outlet','specifiedaveragestaticpressure': treated as a static-pressure
+                            * outlet, except that after each pressure correction the face pressure
+                            * is the owner's, shifted so that its area average is patch_pressure
+                            * (CorrectPressure.for:169-205) */
 };
 
 /* ---------------------------------------------------------- scheme enums */
@@ -111,7 +121,9 @@ enum fs_solver {
   FS_SOLVER_AMG = 2,       /* LMultigrid=.true., MGType='geometricelement' */
   FS_SOLVER_AMG_BICGS = 3, /* FP64 BiCGSTAB right-preconditioned by one AMG V-cycle (no reference row) */
   FS_SOLVER_AMG32_BICGS = 4,/* same with an FP32 AMG hierarchy (iterative refinement, no reference row) */
-  FS_SOLVER_GMRES = 5      /* 'gmres': GMRES_RESTARTED_OMP_RETURNR restated (matrixSolverOMP.f90:48) */
+  FS_SOLVER_GMRES = 5,     /* 'gmres': GMRES_RESTARTED_OMP_RETURNR restated (matrixSolverOMP.f90:48) */
+  FS_SOLVER_ILU = 6        /* 'ilu': D-ILU factorisation once, then ILU sweeps until rrF or itmax
+                            * (FactorizeUsingILU.for:4, ILUMethod.for:4, SolveAlegbraicEquations.for:122-133) */
 };
 enum fs_algorithm { FS_SIMPLE = 0, FS_SIMPLEC = 1 };
 
@@ -377,6 +389,12 @@ int fs_mg_parents(fs_ctx *ctx, int level, int32_t *parents, size_t n);
  * the bench roofline): ELL width of each level and the coarsest level the
  * AMG preconditioner cycles to (inverted densely when *direct is 1). */
 int fs_mg_info(fs_ctx *ctx, int32_t *widths, int max_levels, int32_t *prec_coarsest, int32_t *direct);
+/* AssembleAgglomeratedLHS (AssembleElementBasedAgglomoratedLHS.for:45-150) of
+ * the last assembled system, read back for level `level` >= 1: ac [n],
+ * n_nbr [n], nbr and anb [w*n slot-major, nbr -1 past n_nbr[i]], with n and
+ * w the level's size and ELL width (fs_mg_levels, fs_mg_info). */
+int fs_mg_coarse_matrix(fs_ctx *ctx, int level, double *ac, int32_t *n_nbr, int32_t *nbr, double *anb,
+                        size_t n, size_t w);
 
 /* ----------------------------------------------------- learned p' initial guess
  * No reference counterpart: the reference starts every p' solve from zero.
@@ -469,8 +487,10 @@ int fs_sync(fs_ctx *ctx);
  * otherwise).  The solve is queued on `stream` (a cudaStream_t, NULL for the
  * default stream) and the call returns without waiting.  Every call on a
  * device shares that array: calls that overlap on the GPU race on it.  The
- * first call on a device looks the array's address up (cudaGetSymbolAddress)
- * and should come before any stream capture that is meant to contain it. */
+ * first call on a device does a one-time set-up: it looks the array's device
+ * address up with cudaGetSymbolAddress and keeps it for the CUDA context
+ * current at the call (a call under another context of the device repeats
+ * it); make that first call before any stream capture begins. */
 #define FS_NOALLOC_MAX_ROWS 262144
 int fs_bicgstab_noalloc(int32_t n, int32_t w, const int32_t *ncf, const int32_t *cn,
                         const double *ac, const double *anb, const double *bc, double *x,

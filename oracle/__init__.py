@@ -67,8 +67,20 @@ def load():
         lib.om_mg_level_size.argtypes = [C.c_void_p, C.c_int]
         lib.om_mg_parents.restype = C.POINTER(C.c_int)
         lib.om_mg_parents.argtypes = [C.c_void_p, C.c_int]
+        lib.om_set_threads.restype = C.c_int
+        lib.om_set_threads.argtypes = [C.c_int]
+        lib.om_mg_width.restype = C.c_int
+        lib.om_mg_width.argtypes = [C.c_void_p, C.c_int]
+        lib.om_mg_coarse_matrix.restype = C.c_int
+        lib.om_mg_coarse_matrix.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = lib
     return _lib
+
+
+def set_threads(n: int) -> int:
+    """Threads of the AxOMP loop (the reference's OpenMP region); n <= 0 keeps
+    the current count.  Returns the count in effect."""
+    return load().om_set_threads(int(n))
 
 
 class Oracle:
@@ -186,6 +198,16 @@ class Oracle:
         n = self.lib.om_mg_level_size(self.h, level)
         p = self.lib.om_mg_parents(self.h, level)
         return np.ctypeslib.as_array(p, shape=(n,)).copy()
+
+    def mg_coarse_matrix(self, level: int) -> dict:
+        """AssembleAgglomeratedLHS of the current system: the matrix of `level`."""
+        n, w = self.lib.om_mg_level_size(self.h, level), self.lib.om_mg_width(self.h, level)
+        out = {"ac": np.zeros(n), "n_nbr": np.zeros(n, np.int32), "nbr": np.zeros(n * w, np.int32),
+               "anb": np.zeros(n * w)}
+        rc = self.lib.om_mg_coarse_matrix(self.h, level, *[out[k].ctypes.data for k in ("ac", "n_nbr", "nbr", "anb")])
+        if rc != 0:
+            raise ValueError(f"no coarse level {level}")
+        return out
 
     def close(self):
         if self.h:

@@ -20,6 +20,7 @@
  */
 #include "oracle.h"
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdio.h>
@@ -33,7 +34,11 @@
  * AssembleConvection.for:260-300, AssemblePressureCorrectionFluxes.for:545-575) */
 #define OM_INLET(t) ((t) == FS_BC_INLET_VEL || (t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP)
 /* static pressure specified: Rhie-Chow boundary flux, p'_b = 0 (AssembleMdotUsingRhieChow.for:1441-1598, 2105-2283) */
-#define OM_PRESSURE(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_INLET_SP)
+#define OM_PRESSURE(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_INLET_SP || (t) == FS_BC_OUTLET_ASP)
+/* 'specifiedstaticpressure' and 'specifiedaveragestaticpressure' outlets share
+ * every loop body but CorrectPressure's (AssembleMdotUsingRhieChow.for:1441-1812,
+ * AssemblePressureCorrectionFluxes.for:244-400, CorrectMdotandVelocity.for:264-320, ...) */
+#define OM_SP_OUTLET(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_OUTLET_ASP)
 /* Dirichlet momentum diffusion and plain upwind convection at the face
  * (AssembleIsotropicDiffusion.for:254-300, 507-525; AssembleConvection.for:260-330, 505-520) */
 #define OM_GIVEN_FLOW(t) (OM_INLET(t) || (t) == FS_BC_OUTLET_MASS)
@@ -99,6 +104,8 @@ struct om {
   /* BICGSTAB_OMP persistent storage (SparseMatricesVariables) */
   int csr_built; long *csr_ptr; int *csr_j; int *csr_slot; double *csr_val;
   double *kx, *kr, *kb;
+  /* ILU (Variables2 dc, rc) */
+  double *ilu_dc, *ilu_rc;
   /* multigrid */
   int mg_nlev; int mg_built; void *mgt;
   /* unsteady (Variables1 ...Old and ...OldOld, Transient1 dt, dtOld, dtOldOld; time, ndt) */
@@ -426,7 +433,7 @@ void om_gradient(om *m, int var, int method, int niter, const double *phi, const
   /* RelaxGradient: all LrelaxGradient* are .false. (User0.F90:164-179) -> return */
   /* CorrectGradientAtOulet for velocities (CorrectGradients.for:188-238) */
   if (var == FS_VAR_U || var == FS_VAR_V || var == FS_VAR_W) {
-    for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_FD || m->btype[b] == FS_BC_OUTLET_SP) {
+    for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_OUTLET_FD || OM_SP_OUTLET(m->btype[b])) {
       int k = m->bf_own[b], s = m->bf_set[b];
       tproj(m->bnx[b], m->bny[b], nz_ii(m, s), gx[k], gy[k], gz[k], &bgx[b], &bgy[b], &bgz[b], 0);
     }
@@ -685,7 +692,7 @@ void om_assemble_momentum(om *m, int comp)
     if (OM_GIVEN_FLOW(t)) {
       double fcl = fmax(m->bmdot[b], 0.), ffl = -fmax(-m->bmdot[b], 0.);
       m->fcf[i4] += fcl; m->fff[i4] += ffl; m->ftf[i4] += fcl * fi[i1] + ffl * bfi[b];
-    } else if (t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_SP) {   /* :421-448 the same for both */
+    } else if (t == FS_BC_OUTLET_FD || OM_SP_OUTLET(t)) {   /* :421-476 the same for all three */
       const double *bgx = bfg, *bgy = bfg + B, *bgz = bfg + 2 * (long)B;
       double fcl = fmax(m->bmdot[b], 0.), ffl = -fmax(-m->bmdot[b], 0.);
       double fvl = m->bmdot[b] * (bgx[b] * m->bdx[b] + bgy[b] * m->bdy[b] + bgz[b] * m->bdz[b]);
@@ -768,7 +775,7 @@ static void om_flow_in_out(om *m)
   int nfd = 0, other = 0;
   for (int s = 0; s < NS; s++) {
     if (c->patch_type[s] == FS_BC_OUTLET_FD) nfd++;
-    if (c->patch_type[s] == FS_BC_OUTLET_SP || c->patch_type[s] == FS_BC_OUTLET_MASS) other++;
+    if (OM_SP_OUTLET(c->patch_type[s]) || c->patch_type[s] == FS_BC_OUTLET_MASS) other++;
   }
   /* FlowOut/AdjustFlow return at once unless every outlet is fully developed */
   if (nfd == 0 || other) return;
@@ -862,7 +869,7 @@ static void om_assemble_mdot(om *m)
   for (int b = 0; b < B; b++) if (OM_PRESSURE(m->btype[b])) {
     int i1 = m->bf_own[b];
     double rhof = c->rho, sx = m->bsx[b], sy = m->bsy[b], sz = m->bsz[b];
-    if (m->btype[b] == FS_BC_OUTLET_SP) {
+    if (OM_SP_OUTLET(m->btype[b])) {
       m->bu[b] = m->u[i1] + (m->bug[b] * m->bdx[b] + m->bug[B + b] * m->bdy[b] + m->bug[2L * B + b] * m->bdz[b]);
       m->bv[b] = m->v[i1] + (m->bvg[b] * m->bdx[b] + m->bvg[B + b] * m->bdy[b] + m->bvg[2L * B + b] * m->bdz[b]);
       m->bw[b] = m->w[i1] + (m->bwg[b] * m->bdx[b] + m->bwg[B + b] * m->bdy[b] + m->bwg[2L * B + b] * m->bdz[b]);
@@ -986,6 +993,21 @@ void om_correct_continuity(om *m)
       m->bp[b] = m->p[i1] + m->bpg[b] * m->bdx[b] + m->bpg[B + b] * m->bdy[b] + m->bpg[2 * (long)B + b] * m->bdz[b];
     else if (t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS || t == FS_BC_OUTLET_FD || t == FS_BC_OUTLET_MASS)   /* :120-138, 220-226; static pressures stay */
       m->bp[b] = m->bp[b] + c->urf_pressure * (m->bpc[b] - rpc);
+    else if (t == FS_BC_OUTLET_ASP)   /* :169-176 */
+      m->bp[b] = m->p[i1];
+  }
+  /* 'specifiedaveragestaticpressure': the face pressures shifted so that their
+   * area average is AverageOutletPressure (:178-203) */
+  for (int s = 0; s < m->NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_ASP) {
+    double avg = 0., area = 0.;
+    for (int j = 0; j < m->bset_n[s]; j++) {
+      int b = m->bset_start[s] + j;
+      avg = avg + m->bfa[b] * m->bp[b];
+      area = area + m->bfa[b];
+    }
+    avg = avg / (area + OM_TINY);
+    avg = c->patch_pressure[s] - avg;
+    for (int j = 0; j < m->bset_n[s]; j++) { int b = m->bset_start[s] + j; m->bp[b] = m->bp[b] + avg; }
   }
   /* CalculateResidualsContinuity (CalculateContinuityResiduals.for:130-235) */
   double *mi = dz_(N);
@@ -1079,6 +1101,82 @@ static void sor_sweep(om *m)   /* SolveEquationsUsingSOR (SORMethod.for:20-60) *
     }
 }
 
+/* the first slot of row j whose neighbour is i (the reference's search loops,
+ * FactorizeUsingILU.for:47-51, ILUMethod.for:86-92); -1 when there is none */
+static int slot_of(const om *m, int j, int i)
+{
+  const int N = m->N;
+  for (int q = 0; q < m->ncf[j]; q++) if (m->cn[(long)q * N + j] == i) return q;
+  return -1;
+}
+
+/* ILUFactorization (FactorizeUsingILU.for:4-75): the diagonal of the D-ILU
+ * factorisation, dc = 1/(ac - sum over earlier neighbours), in element order.
+ * Quirk kept: element NumberOfElements-1 (1-based; 0-based N-2) does not
+ * update its later neighbours (:36). */
+static void ilu_factor(om *m)
+{
+  const int N = m->N;
+  if (!m->ilu_dc) { m->ilu_dc = dz_(N); m->ilu_rc = dz_(N); }
+  double *dc = m->ilu_dc;
+  for (int i = 0; i < N; i++) dc[i] = m->ac[i];
+  for (int i1 = 0; i1 < N; i1++) {
+    dc[i1] = 1.0 / dc[i1];
+    m->ilu_rc[i1] = m->bc[i1];
+    if (i1 == N - 2) continue;
+    for (int j2 = 0; j2 < m->ncf[i1]; j2++) {
+      const int j4 = m->cn[(long)j2 * N + i1];
+      if (j4 > i1 && j4 < N) {
+        const int i2 = slot_of(m, j4, i1);
+        if (i2 >= 0) dc[j4] = dc[j4] - m->anb[(long)i2 * N + j4] * dc[i1] * m->anb[(long)j2 * N + i1];
+        else fprintf(stderr, "the index for i in j is not found\n");
+      }
+    }
+  }
+}
+
+/* SolveEquationsUsingILU (ILUMethod.for:4-170): residual, forward
+ * substitution through the earlier neighbours, backward substitution through
+ * the later ones, dphi += D r */
+static void ilu_sweep(om *m)
+{
+  const int N = m->N;
+  double *dc = m->ilu_dc, *rc = m->ilu_rc, *dphi = m->dphi;
+  for (int i = 0; i < N; i++) {
+    double res = -m->ac[i] * dphi[i] + m->bc[i];
+    for (int j = 0; j < m->ncf[i]; j++) {
+      const int k = m->cn[(long)j * N + i];
+      if (k >= 0) res = res - m->anb[(long)j * N + i] * dphi[k];
+    }
+    rc[i] = res;
+  }
+  for (int i1 = 0; i1 < N; i1++) {
+    const double product1 = dc[i1] * rc[i1];
+    for (int j2 = 0; j2 < m->ncf[i1]; j2++) {
+      const int j1 = m->cn[(long)j2 * N + i1];
+      if (j1 >= 0 && j1 > i1 && j1 < N) {
+        const int i2 = slot_of(m, j1, i1);
+        if (i2 >= 0) {
+          const double product2 = m->anb[(long)i2 * N + j1] * product1;
+          rc[j1] = rc[j1] - product2;
+        } else {
+          fprintf(stderr, "ILU Solver Error The index for i in element j is not found\n");
+        }
+      }
+    }
+  }
+  for (int i1 = N - 1; i1 >= 0; i1--) {
+    if (i1 < N - 1)
+      for (int j2 = 0; j2 < m->ncf[i1]; j2++) {
+        const int j = m->cn[(long)j2 * N + i1];
+        if (j > i1) rc[i1] = rc[i1] - m->anb[(long)j2 * N + i1] * rc[j];
+      }
+    const double product1 = dc[i1] * rc[i1];
+    rc[i1] = product1;
+    dphi[i1] = dphi[i1] + product1;
+  }
+}
+
 /* SolveAlgebraicSystemInParallel CSR (matrixSolverOMP.f90:462-584) + AxOMP (:390-423) */
 static void csr_build(om *m)
 {
@@ -1110,13 +1208,49 @@ static void csr_build(om *m)
   }
 }
 
-static void axomp(const om *m, const double *x, double *y)
+/* AxOMP (matrixSolverOMP.f90:390-423): the one loop of the reference that
+ * runs on several threads (its OpenMP loop over rows, statically split; here
+ * POSIX threads over equal row ranges).  Every row is summed as in the
+ * sequential loop, so the result does not depend on the thread count.  The
+ * dot products of BICGSTAB_OMP sit in orphaned WORKSHARE constructs outside
+ * any parallel region, which one thread executes: they stay sequential. */
+static int g_axomp_threads = 1;
+typedef struct { const om *m; const double *x; double *y; int i0, i1; } ax_job;
+
+static void ax_rows(const om *m, const double *x, double *y, int i0, int i1)
 {
-  for (int i = 0; i < m->N; i++) {
+  for (int i = i0; i < i1; i++) {
     double t = 0.0;
     for (long q = m->csr_ptr[i]; q < m->csr_ptr[i + 1]; q++) t = t + m->csr_val[q] * x[m->csr_j[q]];
     y[i] = t;
   }
+}
+
+static void *ax_thread(void *p)
+{
+  ax_job *j = (ax_job *)p;
+  ax_rows(j->m, j->x, j->y, j->i0, j->i1);
+  return NULL;
+}
+
+static void axomp(const om *m, const double *x, double *y)
+{
+  int T = g_axomp_threads;
+  if (T <= 1 || m->N < 65536) { ax_rows(m, x, y, 0, m->N); return; }
+  if (T > 256) T = 256;
+  pthread_t th[256];
+  ax_job jb[256];
+  int started = 0;
+  for (int t = 0; t < T; t++) {
+    jb[t].m = m; jb[t].x = x; jb[t].y = y;
+    jb[t].i0 = (int)((long)m->N * t / T); jb[t].i1 = (int)((long)m->N * (t + 1) / T);
+    if (t == 0) continue;
+    if (pthread_create(&th[t], NULL, ax_thread, &jb[t]) != 0) { ax_rows(m, x, y, jb[t].i0, jb[t].i1); jb[t].i0 = -1; }
+    else started++;
+  }
+  ax_rows(m, x, y, jb[0].i0, jb[0].i1);
+  for (int t = 1; t < T; t++) if (jb[t].i0 >= 0) pthread_join(th[t], NULL);
+  (void)started;
 }
 
 static double dot(const double *a, const double *b, int n)
@@ -1288,6 +1422,9 @@ void om_solve_equation(om *m, int nf, double *fi, double rrf, int itmax, int sol
   int iter = 0;
   if (solver == FS_SOLVER_SOR) {
     while (FRes > rrf * IRes && iter < itmax) { sor_sweep(m); FRes = check_convergence(m); iter++; }
+  } else if (solver == FS_SOLVER_ILU) {   /* SolveAlegbraicEquations.for:122-133 */
+    ilu_factor(m);
+    while (FRes > rrf * IRes && iter < itmax) { ilu_sweep(m); FRes = check_convergence(m); iter++; }
   } else if (solver == FS_SOLVER_BICGS) {
     iter = om_bicgstab(m, m->cfg.krylov_maxit, m->cfg.krylov_tol);
   } else if (solver == FS_SOLVER_AMG) {
@@ -1356,6 +1493,14 @@ void om_initialize_mdot(om *m)
 }
 
 void om_set_iter(om *m, int nIter) { m->nIter = nIter; }
+
+/* threads of the AxOMP loop (OMP_NUM_THREADS of the reference build; 1 by
+ * default); returns the count in effect */
+int om_set_threads(int n)
+{
+  if (n > 0) g_axomp_threads = n;
+  return g_axomp_threads;
+}
 void om_residuals(om *m, double out[20])
 {
   for (int q = 0; q < 5; q++) { out[q] = m->rabs[q]; out[5 + q] = m->rmax[q]; out[10 + q] = m->rrms[q]; out[15 + q] = m->rscl[q]; }
@@ -1483,7 +1628,7 @@ void *om_array(om *m, const char *name, long *len, int *is_int)
     {"ncf", m->ncf, N, 1}, {"cf", m->cf, N*W, 1}, {"cn", m->cn, N*W, 1},
     {"own_slot", m->own_slot, F, 1}, {"nbr_slot", m->nbr_slot, F, 1},
     {"if_own", m->if_own, F, 1}, {"if_nbr", m->if_nbr, F, 1}, {"bf_own", m->bf_own, B, 1},
-    {"btype", m->btype, B, 1}, {"kx", m->kx, m->kx ? N : 0, 0},
+    {"btype", m->btype, B, 1}, {"kx", m->kx, m->kx ? N : 0, 0}, {"ilu_dc", m->ilu_dc, m->ilu_dc ? N : 0, 0},
     {"tke", m->tke, N, 0}, {"ted", m->ted, N, 0}, {"mut", m->mut, N, 0},
     {"btke", m->btke, B, 0}, {"bted", m->bted, B, 0}, {"bmut", m->bmut, B, 0},
     {"tkeg", m->tkeg, 3*N, 0}, {"tedg", m->tedg, 3*N, 0}, {"prod", m->prod, N, 0},

@@ -65,6 +65,11 @@ void   om_calc_residuals(om *m, int nf, const double *fi);
 int    om_mg_setup(om *m);                     /* returns number of levels */
 int    om_mg_level_size(om *m, int level);
 const int *om_mg_parents(om *m, int level);    /* level l cell -> level l+1 parent (0-based) */
+int    om_mg_width(om *m, int level);          /* ELL width of a level */
+int    om_set_threads(int n);                  /* AxOMP threads (n <= 0: keep); returns the count */
+/* AssembleAgglomeratedLHS of the current system up to `level` >= 1, copied out:
+ * ac [n], n_nbr [n], nbr and anb [w*n slot-major] of that level */
+int    om_mg_coarse_matrix(om *m, int level, double *ac, int *n_nbr, int *nbr, double *anb);
 
 #ifdef __cplusplus
 }

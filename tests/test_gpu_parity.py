@@ -211,6 +211,31 @@ def test_sor_solution():
     assert _rel(x_g, fi) <= 1e-9
 
 
+def test_ilu_sweeps_bit_identical():
+    """'ilu' (FactorizeUsingILU.for, ILUMethod.for): the level-scheduled GPU
+    factorisation and sweeps apply every term in the element-order loops'
+    order, so a fixed number of sweeps gives the restatement's dphi bit for
+    bit (rrF 0: no early stop, whose sum|r| test sums in another order)."""
+    mesh, case = cs.cavity(12, nz=10, jitter=0.2, seed=3)
+    s, o = _pair(mesh, case)
+    for _ in range(2):
+        o.simple_iteration()
+    o.set_iter(3)
+    for assemble in (lambda: o.assemble_momentum(0), o.assemble_continuity):
+        assemble()
+        ac, anb, bc = o.get("ac"), o.get("anb"), o.get("bc")
+        x_g, it = s.solve_system(ac, anb, bc, rrf=0.0, itmax=7, solver="ilu")
+        fi = np.zeros(o.N)
+        o.lib.om_solve_equation(o.h, 1, fi.ctypes.data, 0.0, 7, 6)
+        assert it == 7
+        assert np.array_equal(x_g, fi)
+    # to a tolerance: the converged solution
+    x_g, it = s.solve_system(ac, anb, bc, rrf=1e-12, itmax=5000, solver="ilu")
+    fi = np.zeros(o.N)
+    o.lib.om_solve_equation(o.h, 1, fi.ctypes.data, 1e-12, 5000, 6)
+    assert _rel(x_g, fi) <= 1e-9
+
+
 def test_outer_iterations_bicgs():
     # non-zero initial velocities so no momentum system has a zero right-hand side
     mesh, case = cs.cavity(10, nz=8, jitter=0.2, seed=1, conv_scheme="sou", niter_start_hr=1,

@@ -2,9 +2,11 @@
 CorrectMdotandVelocity.for:165-175, InitializaMdot.for:55, CalculateFlowIn.for:37-48)
 and 'specifiedstaticpressure' inlets (AssembleMdotUsingRhieChow.for:2105-2283,
 AssemblePressureCorrectionFluxes.for:585-657, CorrectMdotandVelocity.for:180-205),
-and 'specifiedmassflowrate' outlets (AssembleMdotUsingRhieChow.for:1999-2031,
-CorrectMdotandVelocity.for:354-364):
-the restatement's invariants on the step case (CPU) and the GPU path against it."""
+'specifiedmassflowrate' outlets (AssembleMdotUsingRhieChow.for:1999-2031,
+CorrectMdotandVelocity.for:354-364) and 'specifiedaveragestaticpressure'
+outlets (CorrectPressure.for:169-203; elsewhere the static-pressure outlet's
+loops): the restatement's invariants on the step case (CPU) and the GPU path
+against it."""
 
 import numpy as np
 import pytest
@@ -274,4 +276,69 @@ def test_mass_inlet_phases_match_oracle():
                 scale = vel if k in ("u", "v", "w") else bvel if k in ("bu", "bv", "bw") else np.linalg.norm(ref[k])
                 err = np.linalg.norm(g.get(k) - ref[k]) / max(scale, 1e-300)
                 assert err <= 1e-9, (it, name, k, err)
+    g.close()
+
+
+# ------------------------------------------------ 'specifiedaveragestaticpressure' outlets
+def _avg_outlet(case, p_avg=0.0):
+    """The step's outlet at a given area-averaged static pressure
+    (CorrectPressure.for:169-203); the face pressures follow the owners'."""
+    case.patches["xmax"] = ("average_pressure_outlet", p_avg)
+
+
+def _outlet(mesh):
+    s = mesh.patch("xmax")
+    b0 = int(mesh.patch_start[s]) - mesh.n_internal
+    return slice(b0, b0 + int(mesh.patch_size[s]))
+
+
+def test_oracle_average_pressure_outlet_step():
+    """Converged laminar step: the outlet's face pressures vary across the
+    patch, their area average is the one specified, and the outflow
+    balances the inflow."""
+    import oracle
+    m, c = cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, **_tight())
+    _avg_outlet(c, 0.02)
+    o = oracle.Oracle(m, c)
+    for k, v in cs.bfs_initial_state(m, c, seed=0, perturbation=0.0).items():
+        o.set(k, v)
+    o.initialize_mdot()
+    for it in range(4000):
+        if o.simple_iteration() < 1e-8:
+            break
+    assert it < 3999
+    sl = _outlet(m)
+    bp, area = o.get("bp")[sl], o.get("bfa")[sl]
+    assert abs((area * bp).sum() / area.sum() - 0.02) <= 1e-12
+    assert bp.max() - bp.min() > 1e-6 * abs(bp).max()
+    out = o.get("bmdot")[sl].sum()
+    inflow = o.get("bmdot")[_inlet(m)].sum()
+    assert abs(out + inflow) <= 1e-8 * abs(inflow)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("turbulence", [False, True])
+def test_average_pressure_outlet_step_matches_oracle(turbulence):
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, re_h=100.0 if not turbulence else 5000.0, turbulence=turbulence, **_tight())
+    _avg_outlet(c, 0.02)
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
+    for obj in (o, g):
+        for k, v in cs.bfs_initial_state(m, c, seed=0).items():
+            obj.set(k, v)
+        obj.initialize_mdot()
+    for it in range(6):
+        so = o.simple_iteration()
+        rg = g.simple_iteration()
+        assert abs(rg["source"] - so) <= 1e-6 * abs(so) + 1e-14, (it, rg["source"], so)
+    keys = ("u", "v", "w", "p", "bmdot", "bu", "bp") + (("tke", "ted", "mut", "btke") if turbulence else ())
+    for k in keys:
+        x, ref = g.get(k), o.get(k)
+        err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+        assert err <= 1e-9, (k, err)
+    sl = _outlet(m)
+    bp, area = g.get("bp")[sl], o.get("bfa")[sl]
+    assert abs((area * bp).sum() / area.sum() - 0.02) <= 1e-12
     g.close()

@@ -156,6 +156,35 @@ def test_solvers_match_direct(oracle_lib):
     assert 0 < steps
     assert np.linalg.norm(A @ x - b) <= 2e-9 * np.linalg.norm(b)
     assert np.abs(x - x_direct).max() <= 1e-7 * np.abs(x_direct).max()
+    # 'ilu': D-ILU factorisation, then ILU sweeps to the tolerance
+    fi = np.zeros(o.N)
+    lib.om_solve_equation(o.h, 1, fi.ctypes.data, 1e-13, 5000, 6)
+    assert np.abs(fi - x_direct).max() <= 1e-9 * np.abs(x_direct).max()
+
+
+def test_ilu_factorisation_restated(oracle_lib):
+    """FactorizeUsingILU.for: dc_j = 1/(ac_j - sum_i a_ji dc_i a_ij) over the
+    earlier neighbours i in element order, except that element N-1 (1-based)
+    updates none of its later neighbours; restated here in numpy on a
+    jittered mesh and compared bit for bit."""
+    mesh, case = cs.cavity(6, nz=5, jitter=0.2, seed=4, solver_mom="ilu", rrf_mom=0.1, itmax_mom=2)
+    o = _oracle(mesh, case)
+    o.set_iter(1)
+    o.momentum(0)
+    N, W = o.N, o.W
+    ac, anb, cn = o.get("ac"), o.get("anb").reshape(W, N), o.get("cn").reshape(W, N)
+    ncf = o.get("ncf")
+    dc = ac.copy()
+    for i in range(N):
+        dc[i] = 1.0 / dc[i]
+        if i == N - 2:
+            continue
+        for j2 in range(ncf[i]):
+            j = cn[j2, i]
+            if j > i:
+                i2 = next(q for q in range(ncf[j]) if cn[q, j] == i)
+                dc[j] = dc[j] - anb[i2, j] * dc[i] * anb[j2, i]
+    assert np.array_equal(o.get("ilu_dc"), dc)
 
 
 def test_connectivity_slot_order(oracle_lib):

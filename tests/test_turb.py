@@ -217,6 +217,30 @@ def test_kepsilon_step_matches_oracle(wall_function):
 
 
 @pytest.mark.gpu
+def test_kepsilon_step_ilu_matches_oracle():
+    """k and epsilon by 'ilu', the reference's default ASSolverTKE/TED, with
+    the case's sweep limits run in full (rrF 0: a sum|r| test that lands on
+    its threshold cannot change a sweep count between the two sides)."""
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, **_tight(solver_turb="ilu", rrf_tke=0.0, rrf_ted=0.0))
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
+    _setup(o, m, c)
+    _setup(g, m, c)
+    for it in range(6):
+        so = o.simple_iteration()
+        rg = g.simple_iteration()
+        assert abs(rg["source"] - so) <= 1e-6 * abs(so) + 1e-14, (it, rg["source"], so)
+    for k in ("u", "v", "w", "p", "tke", "ted", "mut"):
+        x, ref = g.get(k), o.get(k)
+        err = np.linalg.norm(x - ref) / max(np.linalg.norm(ref), 1e-300)
+        assert err <= 1e-9, (k, err)
+    assert g.residuals["turb_lin_iters"][0] >= 1
+    g.close()
+
+
+@pytest.mark.gpu
 def test_kepsilon_step_outlet_balance_and_bounds():
     from flowsolversourcecode_b200.solver import Solver
     m, c = cs.bfs(48, 12, 8, solver_cont="amg_bicgs", krylov_tol=1e-8, krylov_maxit=200)
