@@ -27,14 +27,14 @@ VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
 VAR_TKE, VAR_TED, VAR_RHOK = 8, 9, 10
 # boundary types
 (BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD, BC_OUTLET_SP, BC_INLET_MASS, BC_INLET_SP,
- BC_OUTLET_MASS, BC_OUTLET_ASP) = range(10)
+ BC_OUTLET_MASS, BC_OUTLET_ASP, BC_OUTLET_RES, BC_INLET_STAG) = range(12)
 TRANSIENT = {"euler": 0, "cranknicolson1": 1, "cranknicolson2": 2, "adamsmoulton": 3}
 # gradient interpolation
 GI_AVERAGE, GI_UPWIND, GI_DOWNWIND, GI_AVERAGECORRECTED = 0, 1, 2, 3
 HR_NONE, HR_TVD = 0, 1
 TVD = {n: i for i, n in enumerate(["upwind", "downwind", "fromm", "sou", "cd", "quick", "superbee", "minmod",
                                     "osher", "vanleer", "muscl", "smart", "hquick", "umist", "charm"])}
-SOLVER = {"sor": 0, "bicgs": 1, "amg": 2, "amg_bicgs": 3, "amg32_bicgs": 4, "gmres": 5, "ilu": 6}
+SOLVER = {"sor": 0, "bicgs": 1, "amg": 2, "amg_bicgs": 3, "amg32_bicgs": 4, "gmres": 5, "ilu": 6, "amg32gs_bicgs": 7}
 SIMPLE, SIMPLEC = 0, 1
 
 FIELDS = ["u", "v", "w", "p", "pc", "mdot", "bu", "bv", "bw", "bp", "bpc", "bmdot", "ac", "bc", "anb",
@@ -77,6 +77,7 @@ class FsCase(C.Structure):
         ("patch_pressure", C.c_double * FS_MAX_PATCHES),
         ("unsteady", C.c_int), ("transient_scheme", C.c_int), ("dt", C.c_double),
         ("patch_mass_flow", C.c_double * FS_MAX_PATCHES),
+        ("patch_resistance", C.c_double * FS_MAX_PATCHES),
     ]
 
 

@@ -74,7 +74,9 @@ class Case:
     # "mass_inlet" ('specifiedmassflowrate') takes (type, (direction x,y,z), mass flow into the domain),
     # "pressure_inlet" ('specifiedstaticpressure' inlet) takes (type, (direction x,y,z), static pressure),
     # "mass_outlet" ('specifiedmassflowrate' outlet) takes (type, mass flow out of the domain),
-    # "average_pressure_outlet" ('specifiedaveragestaticpressure') takes (type, average static pressure)
+    # "average_pressure_outlet" ('specifiedaveragestaticpressure') takes (type, average static pressure),
+    # "resistance_outlet" ('specifiedresistance') takes (type, resistance, initial static pressure),
+    # "stagnation_inlet" ('specifiedstagnationpressure') takes (type, (direction x,y,z), stagnation pressure)
     patches: dict = field(default_factory=dict)
     # 'fullydeveloped' outlets: patch name -> MassFlowFraction (default 1)
     mass_flow_fraction: dict = field(default_factory=dict)
@@ -131,7 +133,8 @@ class Case:
         bct = {"wall": L.BC_WALL_NOSLIP, "slip": L.BC_WALL_SLIP, "symmetry": L.BC_SYMMETRY,
                "inlet": L.BC_INLET_VEL, "outlet": L.BC_OUTLET_FD, "pressure_outlet": L.BC_OUTLET_SP,
                "mass_inlet": L.BC_INLET_MASS, "pressure_inlet": L.BC_INLET_SP, "mass_outlet": L.BC_OUTLET_MASS,
-               "average_pressure_outlet": L.BC_OUTLET_ASP}
+               "average_pressure_outlet": L.BC_OUTLET_ASP, "resistance_outlet": L.BC_OUTLET_RES,
+               "stagnation_inlet": L.BC_INLET_STAG}
         for s, name in enumerate(mesh.patch_names):
             spec = self.patches.get(name, ("wall", (0.0, 0.0, 0.0)))
             t, vel = spec[0], spec[1]
@@ -140,7 +143,11 @@ class Case:
                 c.patch_pressure[s] = float(vel)
             elif t == "mass_outlet":     # (type, mass flow)
                 c.patch_mass_flow[s] = float(vel)
-            elif t in ("mass_inlet", "pressure_inlet"):   # (type, direction, mass flow | static pressure)
+            elif t == "resistance_outlet":   # (type, resistance, initial static pressure)
+                c.patch_resistance[s] = float(vel)
+                c.patch_pressure[s] = float(spec[2])
+            elif t in ("mass_inlet", "pressure_inlet", "stagnation_inlet"):
+                # (type, direction, mass flow | static pressure | stagnation pressure)
                 for q in range(3):
                     c.patch_vel[s][q] = float(vel[q])
                 if t == "mass_inlet":

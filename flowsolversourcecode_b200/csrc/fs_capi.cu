@@ -153,7 +153,8 @@ static void free_all(fs_ctx *c) {
                   c->kx, c->kr, c->kr0, c->kp, c->kv, c->ks, c->kt, c->kz, c->ky, c->sysx,
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
                   c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP,
-                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm, c->d_bset, c->flow, c->bdir};
+                  c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm, c->d_bset, c->flow, c->bdir,
+                  c->bpcoefc, c->bgd, c->bp0, c->d_patch};
   for (void *p : ptrs) if (p) cudaFree(p);
 }
 
@@ -177,7 +178,11 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (auto &e : ctx->tev) cudaEventCreate(&e);
   for (auto &pr : ctx->sev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
   for (auto &pr : ctx->kev) { cudaEventCreate(&pr[0]); cudaEventCreate(&pr[1]); }
-  for (int s = 0; s < ctx->cfg.n_patches; s++) ctx->has_sp |= fs_is_pressure(ctx->cfg.patch_type[s]);
+  for (int s = 0; s < ctx->cfg.n_patches; s++) {
+    ctx->has_sp |= fs_is_pressure(ctx->cfg.patch_type[s]);
+    ctx->has_res |= ctx->cfg.patch_type[s] == FS_BC_OUTLET_RES;
+    ctx->has_stag |= ctx->cfg.patch_type[s] == FS_BC_INLET_STAG;
+  }
   // SetReferencePressure (ReferenceAndSetPressureRoutines.for:4-50): a pressure-specified patch fixes the level
   if (ctx->cfg.set_reference_pressure < 0) ctx->cfg.set_reference_pressure = ctx->has_sp ? 1 : 0;
   if ((rc = fs_geometry_build(ctx, mesh))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
@@ -199,7 +204,9 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   for (auto p : cell3) if ((rc = alloc0(ctx, p, 3 * N))) return fail(rc);
   if ((rc = alloc0(ctx, &ctx->gtmp, 12 * N))) return fail(rc);
   if ((rc = alloc0(ctx, &ctx->anb, W * N))) return fail(rc);
-  if ((rc = alloc0(ctx, &ctx->mdot, F)) || (rc = alloc0(ctx, &ctx->pcoef, F)) || (rc = alloc0(ctx, &ctx->bpcoef, B)))
+  if ((rc = alloc0(ctx, &ctx->mdot, F)) || (rc = alloc0(ctx, &ctx->pcoef, F)) || (rc = alloc0(ctx, &ctx->bpcoef, B)) ||
+      (rc = alloc0(ctx, &ctx->bpcoefc, B)) || (rc = alloc0(ctx, &ctx->bgd, B)) || (rc = alloc0(ctx, &ctx->bp0, B)) ||
+      (rc = alloc0(ctx, &ctx->d_patch, 2 * FS_MAX_PATCHES)))
     return fail(rc);
   double **bnd[] = {&ctx->bu, &ctx->bv, &ctx->bw, &ctx->bp, &ctx->bpc, &ctx->bmdot};
   for (auto p : bnd) if ((rc = alloc0(ctx, p, B))) return fail(rc);
@@ -236,7 +243,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   std::vector<double> hm(B, 0.);
   bool has_mass = false;
   for (int s = 0; s < ctx->cfg.n_patches; s++)
-    has_mass |= ctx->cfg.patch_type[s] == FS_BC_INLET_MASS || ctx->cfg.patch_type[s] == FS_BC_INLET_SP ||
+    has_mass |= ctx->cfg.patch_type[s] == FS_BC_INLET_MASS || fs_is_p_inlet(ctx->cfg.patch_type[s]) ||
                 ctx->cfg.patch_type[s] == FS_BC_OUTLET_MASS;
   if (has_mass && B) {
     std::vector<double> hfa(B), hsf(3 * B), hd(3 * B, 0.);
@@ -247,7 +254,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
     for (int s = 0; s < ctx->cfg.n_patches; s++) {
       const int b0 = ctx->h_bset_start[s], nb = ctx->h_bset_n[s];
       const double *d = ctx->cfg.patch_vel[s], rho = ctx->cfg.rho;
-      if (ctx->cfg.patch_type[s] == FS_BC_INLET_SP)   // direction only
+      if (fs_is_p_inlet(ctx->cfg.patch_type[s]))   // direction only
         for (int j = 0; j < nb; j++) for (int q = 0; q < 3; q++) hd[3 * (size_t)(b0 + j) + q] = d[q];
       if (ctx->cfg.patch_type[s] == FS_BC_OUTLET_MASS) {   // outflow: Bmdot > 0; velocity from the first mdot assembly
         double area = 0.;
@@ -271,6 +278,10 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   }
   if (B) {
     cudaMemcpyAsync(ctx->bp, hp.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
+    cudaMemcpyAsync(ctx->bp0, hp.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
+    // ArteryResistance per patch ('specifiedresistance'); the patch sums of geoDiff follow
+    cudaMemcpyAsync(ctx->d_patch, ctx->cfg.patch_resistance, sizeof(double) * FS_MAX_PATCHES, cudaMemcpyHostToDevice,
+                    ctx->st);
     cudaMemcpyAsync(ctx->bu, hb.data(), sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
     cudaMemcpyAsync(ctx->bv, hb.data() + B, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);
     cudaMemcpyAsync(ctx->bw, hb.data() + 2 * B, sizeof(double) * B, cudaMemcpyHostToDevice, ctx->st);

@@ -23,16 +23,27 @@
 // p' and k-epsilon treatment (AssembleIsotropicDiffusion.for:254-300,
 // AssembleConvection.for:260-300, AssemblePressureCorrectionFluxes.for:545-575)
 __host__ __device__ inline bool fs_is_inlet(int t) {
-  return t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS || t == FS_BC_INLET_SP;
+  return t == FS_BC_INLET_VEL || t == FS_BC_INLET_MASS || t == FS_BC_INLET_SP || t == FS_BC_INLET_STAG;
 }
+// static- and stagnation-pressure inlets: the same loop bodies everywhere but
+// in the boundary pressure and the p' coefficients (incompressible)
+__host__ __device__ inline bool fs_is_p_inlet(int t) { return t == FS_BC_INLET_SP || t == FS_BC_INLET_STAG; }
 // static pressure specified: Rhie-Chow boundary flux and p'_b = 0
 // (AssembleMdotUsingRhieChow.for:1441-1598, 2105-2283)
 __host__ __device__ inline bool fs_is_pressure(int t) {
+  return t == FS_BC_OUTLET_SP || t == FS_BC_INLET_SP || t == FS_BC_OUTLET_ASP || t == FS_BC_OUTLET_RES ||
+         t == FS_BC_INLET_STAG;
+}
+// static-pressure, average-static-pressure and resistance outlets: one
+// treatment in every routine but the p' coefficients, the p' boundary values
+// and CorrectPressure (the other loops of the three types are the same text)
+__host__ __device__ inline bool fs_is_sp_outlet(int t) {
+  return t == FS_BC_OUTLET_SP || t == FS_BC_OUTLET_ASP || t == FS_BC_OUTLET_RES;
+}
+// p'_b = 0 (UpdatePressureCorrectionAtBoundaries.for:85-90, 126-143)
+__host__ __device__ inline bool fs_pc_dirichlet(int t) {
   return t == FS_BC_OUTLET_SP || t == FS_BC_INLET_SP || t == FS_BC_OUTLET_ASP;
 }
-// static-pressure and average-static-pressure outlets: one treatment in every
-// routine but CorrectPressure (the loops of the two types are the same text)
-__host__ __device__ inline bool fs_is_sp_outlet(int t) { return t == FS_BC_OUTLET_SP || t == FS_BC_OUTLET_ASP; }
 // the velocity follows from Bmdot along a given direction (AssembleMdotUsingRhieChow.for:2089-2099)
 __device__ __forceinline__ void fs_directed_velocity(const double *bdir, const double *bsf, double rho, int B, int b,
                                                      double bm, double *bu, double *bv, double *bw) {
@@ -105,7 +116,12 @@ struct fs_ctx {
   double *ac = nullptr, *anb = nullptr, *bc = nullptr, *dphi = nullptr;
   double *ac_int = nullptr, *bc_int = nullptr, *effdiv = nullptr;  // bc_int: 3N
   double *pcoef = nullptr;                                         // F: p' face coefficient
-  double *bpcoef = nullptr;                                        // B: p' coefficient of pressure outlets
+  double *bpcoef = nullptr;                                        // B: p' coefficient of pressure outlets (FluxFf)
+  double *bpcoefc = nullptr;                                       // B: its diagonal part FluxCf (resistance, stagnation)
+  double *bgd = nullptr;                                           // B: geoDiff of 'specifiedresistance' faces
+  double *bp0 = nullptr;                                           // B: patch_pressure per face (stagnation p0)
+  double *d_patch = nullptr;                                       // 2*FS_MAX_PATCHES: resistance R, then sum geoDiff
+  bool has_res = false, has_stag = false;                          // resistance outlets, stagnation inlets
   bool has_sp = false;                                             // a 'specifiedstaticpressure' outlet exists
   double *bdir = nullptr;                                          // 3B: direction of 'specifiedmassflowrate' inlets
   // krylov work (device)
@@ -163,9 +179,10 @@ struct fs_ctx {
 
 // residual block layout on the device (double resblk[RB_SIZE]): four norms of
 // NF 1..9 (u, v, w, p', mass, -, -, k, epsilon), the overall imbalance and its
-// cell, then two scratch slots
+// cell, the last linear solve's final residual and |b|, and the inlet mass
+// flow of the last continuity residual (the module's mdotIn)
 enum { RB_ABS = 0, RB_MAX = 9, RB_RMS = 18, RB_SCL = 27, RB_OVERALL = 36, RB_IMAX = 37,
-       RB_DIAG = 38, RB_MDOTIN = 39, RB_SIZE = 40 };
+       RB_DIAG = 38, RB_MDOTIN = 40, RB_SIZE = 41 };
 
 #define FS_CK(call)                                                          \
   do {                                                                       \

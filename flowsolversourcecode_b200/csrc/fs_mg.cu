@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
 #endif
 #define FS_PC_SPIN_LIMIT (1L << 20)   // polls of a team barrier before it reports a timeout
 #ifndef FS_PC_FUSE_DOWN
-#define FS_PC_FUSE_DOWN 2     // restrictions from levels below this one form the residual on the fly
+#define FS_PC_FUSE_DOWN 0     // restrictions from levels below this one form the residual on the fly
 #endif
 
 template <class R>
@@ -690,7 +690,18 @@ struct PCycle {
       for (long P = scc.tid0(); P < C.n; P += scc.nth()) {
         R s = 0.;
         const int c0 = C.rptr[P], c1 = C.rptr[P + 1];
-        for (int c = c0; c < c1; c++) s = s + L.r[C.rlist[c]];
+        // children's residuals eight at a time: their list entries, then their
+        // values, all in flight before the (ascending) sum
+        for (int c = c0; c < c1; c += 8) {
+          int f[8];
+          R v[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) f[u] = c + u < c1 ? C.rlist[c + u] : -1;
+#pragma unroll
+          for (int u = 0; u < 8; u++) v[u] = f[u] >= 0 ? L.r[f[u]] : (R)0.;
+#pragma unroll
+          for (int u = 0; u < 8; u++) if (f[u] >= 0) s = s + v[u];
+        }
         C.b[P] = s;
         if (first_sweep) C.x[P] = om(l + 1) * s / C.ac[P];
       }
@@ -785,6 +796,81 @@ struct PCycle {
       scatter_children(Cc, xf, i, af * (R)t, lane, 32);
     }
   }
+  // ------------------------------------------------------------ Gauss-Seidel V-cycle
+  // One multicolour Gauss-Seidel pass over level l in place: the colours in
+  // order (forward) or reversed (backward); rows of one colour read only
+  // rows of other colours, so each colour is one phase of independent rows.
+  __device__ void gs_colours(int l, const double *__restrict__ in, R *__restrict__ x, bool backward) {
+    const LevelDev<R> L = lev[l];
+    Scope sc = pc_scope(L);
+    for (int cc = 0; cc < L.ncolors; cc++) {
+      const int c = backward ? L.ncolors - 1 - cc : cc;
+      enter(sc);
+      if (!sc.active()) continue;
+      const int r0 = L.color_ptr[c], r1 = L.color_ptr[c + 1];
+      for (long q = r0 + sc.tid0(); q < r1; q += sc.nth()) {
+        const int i = L.color_rows[q];
+        const R t = ell_acc<6, false>((R)0., L.n, L.w, L.nbr, L.anb, i, [&](int k) { return x[k]; });
+        const R bi = l == 0 ? (R)in[i] : L.b[i];
+        x[i] = (bi - t) / L.ac[i];
+      }
+    }
+  }
+  // The V-cycle with symmetric multicolour Gauss-Seidel smoothing: on every
+  // level a forward pass from zero before the restriction and, after the
+  // correction x += alpha x_c[parent], a backward pass; the coarsest level by
+  // the dense inverse.  out = M^-1 in; callers have made `in` visible.
+  __device__ void run_gs(const double *__restrict__ in, double *__restrict__ out) {
+    Scope g;
+    g.grid = true;
+    const LevelDev<R> L0 = lev[0];
+    for (long i = g.tid0(); i < L0.n; i += g.nth()) L0.x[i] = (R)0.;
+    last.grid = true;
+    last.team = false;
+    gs_colours(0, in, L0.x, false);
+    for (int l = 0; l < lc; l++) {
+      const LevelDev<R> L = lev[l], C = lev[l + 1];
+      residual(l, in, L.x, L.r);
+      Scope scc = pc_scope(C);
+      enter(scc);
+      if (scc.active())
+        for (long P = scc.tid0(); P < C.n; P += scc.nth()) {
+          R s = 0.;
+          for (int c = C.rptr[P]; c < C.rptr[P + 1]; c++) s = s + L.r[C.rlist[c]];
+          C.b[P] = s;
+          C.x[P] = (R)0.;
+        }
+      if (l + 1 < lc) gs_colours(l + 1, in, C.x, false);
+    }
+    {
+      Scope c0;
+      c0.grid = false;
+      enter(c0);
+      if (blockIdx.x == 0) {
+        const LevelDev<R> Cc = lev[lc];
+        const int n = Cc.n, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        for (int i = threadIdx.x >> 5; i < n; i += nw) {
+          double t = 0.;
+          for (int j = lane; j < n; j += 32) t += sinv[(long)i * n + j] * (double)Cc.b[j];
+          t = wsum(t);
+          if (lane == 0) Cc.x[i] = (R)t;
+        }
+      }
+    }
+    for (int l = lc - 1; l >= 0; l--) {
+      const LevelDev<R> L = lev[l];
+      const R *__restrict__ xc = lev[l + 1].x;
+      Scope sl = pc_scope(L);
+      enter(sl);
+      if (sl.active())
+        for (long i = sl.tid0(); i < L.n; i += sl.nth()) L.x[i] = L.x[i] + al(l) * xc[L.parent[i]];
+      gs_colours(l, in, L.x, true);
+    }
+    enter(g);
+    for (long i = g.tid0(); i < L0.n; i += g.nth()) out[i] = (double)L0.x[i];
+    enter(g);
+  }
+
   __device__ void run_fused(const double *__restrict__ in, double *__restrict__ out) {
     Scope g;
     g.grid = true;
@@ -833,22 +919,24 @@ __device__ __forceinline__ void row_ax2(const A &a, long i, long i2, bool h2, co
 
 // apply the preconditioner: out (FP64) = M^-1 in (FP64), via the R-precision
 // V-cycle; `fused`: the caller has set x_0 = omega0 in / ac_0 (run_fused)
-template <class R, bool FUSED>
+// MODE: 0 the V-cycle of run(), 1 run_fused(), 2 run_gs()
+template <class R, int MODE>
 __device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, double *out, unsigned &gen) {
   Scope all;
   all.grid = true;
   PCycle<R> C{S, a.lev, a.lc, a.direct != 0, a.sinv, a.pre, a.post, 20, (R)FS_MG_OMEGA, (R)FS_MG_ALPHA, all,
                (R)FS_MG_OMEGA0, (R)FS_MG_ALPHA0, a.teambar, a.status, gen, a.team_extra, false};
-  if (FUSED) C.run_fused(in, out);
+  if (MODE == 1) C.run_fused(in, out);
+  else if (MODE == 2) C.run_gs(in, out);
   else C.run(in, out);
   gen = C.gen;
 }
 
-// right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle;
-// FUSED: the fused V-cycle (one pre- and one post-sweep, dense coarsest
-// level), whose first sweep from zero, x_0 = omega0 in / ac_0, rides on the
-// loops that form p and s
-template <class R, bool FUSED>
+// right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle:
+// MODE 0 run(), 2 run_gs() (multicolour Gauss-Seidel smoothing), 1 the fused
+// V-cycle (one pre- and one post-sweep, dense coarsest level), whose first
+// sweep from zero, x_0 = omega0 in / ac_0, rides on the loops that form p and s
+template <class R, int MODE>
 __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(AmgKArgs<R> a) {
   Sync S(a.part);
   unsigned gen = 0;   // team-barrier generation (the counters are zeroed before the launch)
@@ -860,17 +948,34 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   // with c not finite or zero falls back to the zero start (same decision in
   // every CTA: the sums are grid-deterministic).  Whether guesses pay is decided
   // on iteration counts by the host policy (fs_nn.cu).
+  // A pure-Neumann system (every row sums to zero: the closed-cavity p'
+  // system) is singular.  Its right-hand side is taken with its mean removed,
+  // the part a solution can match; otherwise, once the outer iterations have
+  // converged the mean (rounding in the mass fluxes) is no longer small
+  // against |b|, the tolerance cannot be met and the iterates drift.  The
+  // constant null vector is left to the caller (pressure reference cell).
+  double nonsing = 0., bsum = 0.;
+  for (long i = t0; i < N; i += nt) {
+    double rs = a.ac[i];
+    for (int j = 0; j < a.W; j++)
+      if (a.cn[(long)j * N + i] >= 0) rs += a.anb[(long)j * N + i];
+    nonsing += fabs(rs) > 1e-9 * fabs(a.ac[i]) ? 1. : 0.;
+    bsum += a.bc[i];
+  }
+  double n_nonsing, b_total;
+  S.sum2(nonsing, bsum, n_nonsing, b_total);
+  const double bmean = n_nonsing == 0. ? b_total / N : 0.;
   double l0 = 0., l1 = 0., l2 = 0.;
   for (long i = t0; i < N; i += 2 * nt) {
     const long i2 = i + nt;
     const bool h2 = i2 < N;
     double q1 = 0., q2 = 0.;
     if (a.x0) row_ax2(a, i, i2, h2, a.x0, q1, q2);
-    const double b1 = a.bc[i];
+    const double b1 = a.bc[i] - bmean;
     a.r[i] = q1;
     l0 += q1 * b1; l1 += q1 * q1; l2 += b1 * b1;
     if (h2) {
-      const double b2 = a.bc[i2];
+      const double b2 = a.bc[i2] - bmean;
       a.r[i2] = q2;
       l0 += q2 * b2; l1 += q2 * q2; l2 += b2 * b2;
     }
@@ -884,7 +989,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   l0 = 0.;
   for (long i = t0; i < N; i += nt) {
     const double xi = a.x0 ? c * a.x0[i] : 0.;
-    const double ri = a.bc[i] - c * a.r[i];
+    const double ri = (a.bc[i] - bmean) - c * a.r[i];
     a.x[i] = xi; a.r[i] = ri; a.r0[i] = ri; a.p[i] = 0.; a.v[i] = 0.;
     l0 += ri * ri;
   }
@@ -910,10 +1015,10 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     for (long i = t0; i < N; i += nt) {
       const double pi = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
       a.p[i] = pi;
-      if (FUSED) x0v[i] = om0 * (R)pi / ac0[i];
+      if (MODE == 1) x0v[i] = om0 * (R)pi / ac0[i];
     }
     S.all();
-    apply_prec<R, FUSED>(S, a, a.p, a.y, gen);                      // y = M^-1 p
+    apply_prec<R, MODE>(S, a, a.p, a.y, gen);                       // y = M^-1 p
     l0 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
       const long i2 = i + nt;
@@ -932,7 +1037,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
       const double si = a.r[i] - alpha * a.v[i];
       a.s[i] = si;
       l0 += si * si;
-      if (FUSED) x0v[i] = om0 * (R)si / ac0[i];
+      if (MODE == 1) x0v[i] = om0 * (R)si / ac0[i];
     }
     double ss;
     S.sum2(l0, 0., ss, dum);
@@ -941,7 +1046,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
       resn = sqrt(ss);
       break;
     }
-    apply_prec<R, FUSED>(S, a, a.s, a.z, gen);                      // z = M^-1 s
+    apply_prec<R, MODE>(S, a, a.s, a.z, gen);                       // z = M^-1 s
     l0 = 0.; l1 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
       const long i2 = i + nt;
@@ -1349,12 +1454,13 @@ int fs_mg_build(fs_ctx *ctx) {
   // cooperative grid: smallest co-resident count of the three kernels, <= 4 CTAs/SM
   int a = 0, b = 0, c = 0;
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, (void *)k_mg_solve, FS_COOP_BLOCK, 0));
-  int b2 = 0, c2 = 0;
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double, false>, FS_COOP_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float, false>, FS_COOP_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, (void *)k_amg_bicgstab<double, true>, FS_COOP_BLOCK, 0));
-  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c2, (void *)k_amg_bicgstab<float, true>, FS_COOP_BLOCK, 0));
-  int per = std::min(std::min(a, std::min(b, c)), std::min(b2, c2));
+  int b2 = 0, c2 = 0, c3 = 0;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double, 0>, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float, 0>, FS_COOP_BLOCK, 0));
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, (void *)k_amg_bicgstab<double, 1>, FS_COOP_BLOCK, 0));
+  c2 = c;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c3, (void *)k_amg_bicgstab<float, 2>, FS_COOP_BLOCK, 0));
+  int per = std::min(std::min(a, std::min(b, c)), std::min(std::min(b2, c2), c3));
   if (per < 1) { ctx->err = "multigrid kernels do not fit on an SM"; return FS_E_CUDA; }
   M->per_sm = per;   // occupancy limit; the grid follows the launch shape at each solve
   return FS_OK;
@@ -1409,7 +1515,12 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
   int rc = fs_mg_build(ctx);
   if (rc) return rc;
   fs_mg_dev *M = ctx->mg;
-  const bool f32 = solver == FS_SOLVER_AMG32_BICGS;
+  const bool gs = solver == FS_SOLVER_AMG32GS_BICGS;
+  const bool f32 = solver == FS_SOLVER_AMG32_BICGS || gs;
+  if (gs && !(M->direct && M->lc > 0)) {
+    ctx->err = "the Gauss-Seidel V-cycle needs a coarsest level small enough for the dense inverse";
+    return FS_E_UNSUPPORTED;
+  }
   const int G = std::min(ctx->num_sms * fs_coop_per_sm(ctx, M->per_sm), FS_RED_BLOCKS);
   if (solver == FS_SOLVER_AMG) {
     if ((rc = mg_coarse_matrices(ctx, M->nlev - 1, false))) return rc;
@@ -1456,7 +1567,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.lev = M->lev64;
     void *args[] = {&a};
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
-    FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<double, true> : (const void *)k_amg_bicgstab<double, false>,
+    FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<double, 1> : (const void *)k_amg_bicgstab<double, 0>,
                          G, FS_COOP_BLOCK, args, ctx->st));
   } else {
     AmgKArgs<float> a{};
@@ -1464,8 +1575,10 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.lev = M->lev32;
     void *args[] = {&a};
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
-    FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<float, true> : (const void *)k_amg_bicgstab<float, false>,
-                         G, FS_COOP_BLOCK, args, ctx->st));
+    // the FP32 cycle runs the unfused V-cycle: measured at 128^3, its fused
+    // form was 1.5 % slower (the FP64 cycle gains 5 % from fusion)
+    const void *k = gs ? (const void *)k_amg_bicgstab<float, 2> : (const void *)k_amg_bicgstab<float, 0>;
+    FS_CK(fs_coop_launch(k, G, FS_COOP_BLOCK, args, ctx->st));
   }
   FS_LAUNCH_CHECK();
   FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));

@@ -423,6 +423,9 @@ struct ContArgs {
   const double *rhok, *drk;   // k-epsilon: 2/3 rho k and its gradient (3N), nullptr when laminar
   // pressure outlets
   double *bpcoef, *bu_w, *bv_w, *bw_w;
+  double *bpcoefc, *bgd, *bp_w;   // FluxCf of the p' diagonal, geoDiff of resistance faces, p_b (stagnation)
+  const double *bp0, *patch;      // p0 per face; per patch: resistance R [0,32), sum of geoDiff [32,64)
+  const int32_t *bset;            // patch of each boundary face
   const double *bdir;   // 3B direction of 'specifiedmassflowrate' inlets (nullptr: none)
   const double *bug, *bvg, *bwg, *bdv, *bpg, *bp, *brhok, *bdrk;
   double *ac, *anb, *bc;
@@ -547,7 +550,8 @@ __global__ void k_bmdot_sp(ContArgs a) {
   const int N = a.N, B = a.B;
   const long N2 = 2L * N, B2 = 2L * B;
   const int i1 = a.bown[b];
-  const bool inlet = a.btype[b] == FS_BC_INLET_SP;   // :2105-2283, the same flux; velocity from Bmdot
+  // static- and stagnation-pressure inlets (:2105-2460): the same flux; velocity from Bmdot
+  const bool inlet = fs_is_p_inlet(a.btype[b]);
   const double rhof = a.rho, sx = a.bsf[b], sy = a.bsf[B + b], sz = a.bsf[B2 + b];
   const double dx = a.bdv[b], dy = a.bdv[B + b], dz = a.bdv[B2 + b];
   if (!inlet) {
@@ -576,7 +580,50 @@ __global__ void k_bmdot_sp(ContArgs a) {
   a.bmdot[b] = fcl * a.p[i1] + ffl * a.bp[b] + fvl;
   if (inlet) fs_directed_velocity(a.bdir, a.bsf, rhof, B, b, a.bmdot[b], a.bu_w, a.bv_w, a.bw_w);
   double t2x, t2y, t2z;
-  a.bpcoef[b] = rhof * geo_diff(a.msd, a.du2[i1], a.dv2[i1], a.dw2[i1], sx, sy, sz, ex, ey, ez, cf, t2x, t2y, t2z);
+  const double gd2 = geo_diff(a.msd, a.du2[i1], a.dv2[i1], a.dw2[i1], sx, sy, sz, ex, ey, ez, cf, t2x, t2y, t2z);
+  a.bpcoef[b] = rhof * gd2;
+  if (a.btype[b] == FS_BC_OUTLET_RES) a.bgd[b] = gd2;   // geoDiffB (AssemblePressureCorrectionFluxes.for:474)
+}
+
+// sum of geoDiff over each 'specifiedresistance' patch (geoDiffSum,
+// AssemblePressureCorrectionFluxes.for:400-476), one CTA per patch
+struct ResPatches { int n; int s[FS_MAX_PATCHES], start[FS_MAX_PATCHES], cnt[FS_MAX_PATCHES]; };
+__global__ void __launch_bounds__(1024) k_res_sum(ResPatches rp, const double *__restrict__ bgd, double *patch) {
+  __shared__ double sh[32];
+  const int q = blockIdx.x;
+  const int b0 = rp.start[q], n = rp.cnt[q];
+  double t = 0.;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) t = t + bgd[b0 + j];
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) patch[FS_MAX_PATCHES + rp.s[q]] = t;
+}
+
+// UpdateBoundaryForTotalConditions (TotalConditionsBoundary.for:25-45) and the
+// boundary FluxCf of the p' system (AssemblePressureCorrectionFluxes.for:
+// 244-313 static, 322-400 average, 476-500 resistance, 585-720 inlets):
+// FluxFf stays rho geoDiff; FluxCf is rho geoDiff (1 + (S - geoDiff) R) /
+// (1 + R S) on a resistance outlet, Bmdot FluxFf / (Bmdot - FluxFf rho |U_b|^2)
+// on a stagnation-pressure inlet after p_b = max(p0 - rho |U_b|^2 / 2, 0)
+__global__ void k_pc_bcoef(ContArgs a) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.B) return;
+  const int t = a.btype[b];
+  if (!fs_is_pressure(t)) return;
+  const double ff = a.bpcoef[b];
+  double fc = ff;
+  if (t == FS_BC_INLET_STAG) {
+    const double u = a.bu_w[b], v = a.bv_w[b], w = a.bw_w[b];
+    const double vel2 = u * u + v * v + w * w;
+    a.bp_w[b] = fmax(a.bp0[b] - 0.5 * a.rho * vel2, 0.);
+    const double bm = a.bmdot[b];
+    fc = bm * ff / (bm - ff * a.rho * vel2);
+  } else if (t == FS_BC_OUTLET_RES) {
+    const int s = a.bset[b];
+    const double R = a.patch[s], S = a.patch[FS_MAX_PATCHES + s], g = a.bgd[b];
+    fc = a.rho * g;
+    fc = fc * (1. + (S - g) * R) / (1. + R * S);
+  }
+  a.bpcoefc[b] = fc;
 }
 
 // p' system (AssemblePressureCorrectionFluxes.for + global assembly): ac = sum coef,
@@ -596,7 +643,7 @@ __global__ void __launch_bounds__(FS_BLOCK) k_pc_assemble(ContArgs a) {
         if (s & 1) { ac = ac - fff; a.anb[(long)j * N + i] = 0. - c; bc = bc + md; }
         else { ac = ac + c; a.anb[(long)j * N + i] = 0. + fff; bc = bc - md; }
       } else {
-        ac = ac + (fs_is_pressure(a.btype[f - F]) ? a.bpcoef[f - F] : 0.);
+        ac = ac + (fs_is_pressure(a.btype[f - F]) ? a.bpcoefc[f - F] : 0.);
         bc = bc - a.bmdot[f - F];
       }
     };
@@ -621,10 +668,43 @@ struct CorrArgs {
   const double *bdir, *bsf; double rho;             // inlets with a given velocity direction
 };
 
-// UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for)
+// UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for):
+// 0 at static pressures (:85-90, 126-143), the owner's elsewhere; on a
+// stagnation-pressure inlet -rho |U_b|^2 FluxFf p'_C / (Bmdot - FluxFf rho |U_b|^2)
+// (:97-112); resistance outlets are set by k_res_pc
 __global__ void k_bpc(CorrArgs a) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < a.B) a.bpc[b] = fs_is_pressure(a.btype[b]) ? 0. : a.pc[a.bown[b]];   // :85-90, 126-130
+  if (b >= a.B) return;
+  const int t = a.btype[b];
+  if (t == FS_BC_OUTLET_RES) return;
+  if (t == FS_BC_INLET_STAG) {
+    const double gd = a.bpcoef[b];
+    const double u = a.bu[b], v = a.bv[b], w = a.bw[b];
+    const double vel2 = u * u + v * v + w * w;
+    a.bpc[b] = -a.rho * vel2 * gd * a.pc[a.bown[b]] / (a.bmdot[b] - gd * a.rho * vel2);
+    return;
+  }
+  a.bpc[b] = fs_pc_dirichlet(t) ? 0. : a.pc[a.bown[b]];
+}
+// 'specifiedresistance' outlets (UpdatePressureCorrectionAtBoundaries.for:144-175):
+// p'_b = R sum(geoDiff p'_C) / (1 + R sum geoDiff) on every face of the patch
+struct ResPatchesC { int n; int s[FS_MAX_PATCHES], start[FS_MAX_PATCHES], cnt[FS_MAX_PATCHES]; };
+__global__ void __launch_bounds__(1024) k_res_pc(ResPatchesC rp, const double *__restrict__ bgd,
+                                                 const int32_t *__restrict__ bown, const double *__restrict__ pc,
+                                                 const double *__restrict__ patch, double *bpc) {
+  __shared__ double sh[32];
+  __shared__ double val;
+  const int q = blockIdx.x;
+  const int b0 = rp.start[q], n = rp.cnt[q], s = rp.s[q];
+  double t = 0.;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) t = t + bgd[b0 + j] * pc[bown[b0 + j]];
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) {
+    const double R = patch[s], S = patch[FS_MAX_PATCHES + s];
+    val = R * t / (1. + R * S);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < n; j += blockDim.x) bpc[b0 + j] = val;
 }
 // CorrectPressure (CorrectPressure.for:21-42)
 __global__ void k_corr_p(CorrArgs a) {
@@ -663,7 +743,7 @@ __global__ void k_bcorr(CorrArgs a) {
     // again from Bmdot); the static pressure stays (CorrectPressure.for:146-150, 162-166)
     const int N = a.N;
     a.bmdot[b] = a.bmdot[b] - a.bpcoef[b] * (a.bpc[b] - a.pc[i1]);
-    if (t == FS_BC_INLET_SP) {
+    if (fs_is_p_inlet(t)) {
       fs_directed_velocity(a.bdir, a.bsf, a.rho, B, b, a.bmdot[b], a.bu, a.bv, a.bw);
     } else {
       a.bu[b] = a.bu[b] - a.du2[i1] * a.pcg[i1];
@@ -671,6 +751,11 @@ __global__ void k_bcorr(CorrArgs a) {
       a.bw[b] = a.bw[b] - a.dw2[i1] * a.pcg[2L * N + i1];
     }
     if (t == FS_BC_OUTLET_ASP) a.bp[b] = a.p[i1];   // CorrectPressure.for:169-176; k_avg_pressure shifts it
+    if (t == FS_BC_OUTLET_RES || t == FS_BC_INLET_STAG) {   // CorrectPressure.for:152-160, 206-214
+      double rpc = (a.ref_cell >= 0) ? a.pc[a.ref_cell] : 0.;
+      if (a.set_ref) rpc = 0.;
+      a.bp[b] = a.bp[b] + a.urfp * (a.bpc[b] - rpc);
+    }
   } else if (t == FS_BC_WALL_SLIP || t == FS_BC_WALL_NOSLIP || t == FS_BC_SYMMETRY) {
     a.bp[b] = a.p[i1] + a.bpg[b] * a.bdv[b] + a.bpg[B + b] * a.bdv[B + b] + a.bpg[B2 + b] * a.bdv[B2 + b];
   } else {
@@ -937,6 +1022,8 @@ static ContArgs cont_args(fs_ctx *ctx) {
   fs_turb_rhok_ptrs(ctx, &a.rhok, &a.drk);
   fs_turb_brhok_ptrs(ctx, &a.brhok, &a.bdrk);
   a.bpcoef = ctx->bpcoef; a.bu_w = ctx->bu; a.bv_w = ctx->bv; a.bw_w = ctx->bw; a.bdir = ctx->bdir;
+  a.bpcoefc = ctx->bpcoefc; a.bgd = ctx->bgd; a.bp_w = ctx->bp; a.bp0 = ctx->bp0; a.patch = ctx->d_patch;
+  a.bset = ctx->d_bset;
   a.bug = ctx->bug; a.bvg = ctx->bvg; a.bwg = ctx->bwg; a.bdv = ctx->bdv; a.bpg = ctx->bpg; a.bp = ctx->bp;
   a.ac = ctx->ac; a.anb = ctx->anb; a.bc = ctx->bc; a.red = ctx->red; a.nblk = fs_grid(ctx->N);
   return a;
@@ -969,6 +1056,16 @@ int fs_continuity_assemble(fs_ctx *ctx) {
   rc = fs_assemble_mdot(ctx, ctx->p);
   if (rc) return rc;
   ContArgs a = cont_args(ctx);
+  if (ctx->has_res) {
+    ResPatches rp{};
+    for (int s = 0; s < ctx->NS; s++)
+      if (ctx->cfg.patch_type[s] == FS_BC_OUTLET_RES) {
+        rp.s[rp.n] = s; rp.start[rp.n] = ctx->h_bset_start[s]; rp.cnt[rp.n] = ctx->h_bset_n[s]; rp.n++;
+      }
+    k_res_sum<<<rp.n, 1024, 0, ctx->st>>>(rp, ctx->bgd, ctx->d_patch);
+    FS_LAUNCH_CHECK();
+  }
+  if (B && ctx->has_sp) { k_pc_bcoef<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
   k_pc_assemble<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();
   k_residual_final<<<1, 1024, 0, ctx->st>>>(ctx->red, a.nblk, N, 3, ctx->resblk);
@@ -998,6 +1095,15 @@ int fs_continuity_correct(fs_ctx *ctx) {
   const fs_case &c = ctx->cfg;
   CorrArgs a = corr_args(ctx);
   if (B) { k_bpc<<<fs_grid(B), FS_BLOCK, 0, ctx->st>>>(a); FS_LAUNCH_CHECK(); }
+  if (ctx->has_res) {
+    ResPatchesC rp{};
+    for (int s = 0; s < ctx->NS; s++)
+      if (c.patch_type[s] == FS_BC_OUTLET_RES) {
+        rp.s[rp.n] = s; rp.start[rp.n] = ctx->h_bset_start[s]; rp.cnt[rp.n] = ctx->h_bset_n[s]; rp.n++;
+      }
+    k_res_pc<<<rp.n, 1024, 0, ctx->st>>>(rp, ctx->bgd, ctx->bown, ctx->pc, ctx->d_patch, ctx->bpc);
+    FS_LAUNCH_CHECK();
+  }
   k_corr_p<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();
   int var = FS_VAR_PC, meth = c.method_grad_cont, nit = c.niter_grad_cont;

@@ -907,7 +907,8 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     FS_CK(fs_coop_launch((const void *)k_gmres, G, FS_COOP_BLOCK, args, ctx->st));
     FS_LAUNCH_CHECK();
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
-  } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS) {
+  } else if (solver == FS_SOLVER_AMG || solver == FS_SOLVER_AMG_BICGS || solver == FS_SOLVER_AMG32_BICGS ||
+             solver == FS_SOLVER_AMG32GS_BICGS) {
     rc = fs_mg_solve(ctx, nf, rrf, solver);
   } else {
     ctx->err = "unknown solver";

@@ -360,6 +360,10 @@ struct FlowArgs {
   const int32_t *bown;
   const double *bsf, *u, *v, *w;
   double *bu, *bv, *bw, *bmdot, *flow;
+  // FlowIn returns at once when an inlet is a static- or stagnation-pressure
+  // one (CalculateFlowIn.for:19-31): mdotIn is then the inlet flow the last
+  // continuity residual summed (every inlet face), or 0 before the first
+  const double *mdot_in_prev;   // nullptr: FlowIn sums velocity and mass-flow inlets
 };
 
 // FlowIn (CalculateFlowIn.for:4-40), FlowOut (CalculateFlowOut.for:4-55),
@@ -373,10 +377,12 @@ __global__ void __launch_bounds__(1024) k_flow_in_out(FlowArgs a) {
   __shared__ double bcast;
   const int B = a.B;
   double s = 0.;
-  for (int q = 0; q < a.NS; q++)
-    if (a.ptype[q] == FS_BC_INLET_VEL || a.ptype[q] == FS_BC_INLET_MASS)   // CalculateFlowIn.for:37-48
-      for (int j = threadIdx.x; j < a.pn[q]; j += blockDim.x) s = s + a.bmdot[a.pstart[q] + j];
+  if (!a.mdot_in_prev)
+    for (int q = 0; q < a.NS; q++)
+      if (a.ptype[q] == FS_BC_INLET_VEL || a.ptype[q] == FS_BC_INLET_MASS)   // CalculateFlowIn.for:37-48
+        for (int j = threadIdx.x; j < a.pn[q]; j += blockDim.x) s = s + a.bmdot[a.pstart[q] + j];
   s = block_sum(s, sh);
+  if (a.mdot_in_prev) s = *a.mdot_in_prev;
   if (threadIdx.x == 0) { a.flow[0] = s; bcast = s; }
   __syncthreads();
   const double mdot_in = bcast;
@@ -607,6 +613,8 @@ int fs_flow_in_out(fs_ctx *ctx) {
     a.frac[s] = c.mass_flow_fraction[s] / (tff + TINY);
   }
   a.bown = ctx->bown; a.bsf = ctx->bsf; a.u = ctx->u; a.v = ctx->v; a.w = ctx->w;
+  for (int s = 0; s < ctx->NS; s++)
+    if (fs_is_p_inlet(c.patch_type[s])) a.mdot_in_prev = ctx->resblk + RB_MDOTIN;
   a.bu = ctx->bu; a.bv = ctx->bv; a.bw = ctx->bw; a.bmdot = ctx->bmdot; a.flow = ctx->flow;
   k_flow_in_out<<<1, 1024, 0, ctx->st>>>(a);
   FS_LAUNCH_CHECK();

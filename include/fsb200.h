@@ -99,10 +99,20 @@ enum fs_bc {
                             * patch_vel the velocity direction */
   FS_BC_OUTLET_MASS = 8,   /* 'outlet','specifiedmassflowrate': patch_mass_flow leaves the
                             * domain, along the owner cell's velocity */
-  FS_BC_OUTLET_ASP  = 9    /* 'outlet','specifiedaveragestaticpressure': treated as a static-pressure
+  FS_BC_OUTLET_ASP  = 9,   /* 'outlet','specifiedaveragestaticpressure': treated as a static-pressure
                             * outlet, except that after each pressure correction the face pressure
                             * is the owner's, shifted so that its area average is patch_pressure
                             * (CorrectPressure.for:169-205) */
+  FS_BC_OUTLET_RES  = 10,  /* 'outlet','specifiedresistance': the static-pressure outlet's flux and
+                            * velocity; p'_b = R sum(gd p'_C)/(1 + R sum gd) over the patch, the p'
+                            * diagonal coupled through it (AssemblePressureCorrectionFluxes.for:400-500,
+                            * UpdatePressureCorrectionAtBoundaries.for:144-175) and p_b += urfP p'_b;
+                            * R = patch_resistance (ArteryResistance), patch_pressure the initial p_b */
+  FS_BC_INLET_STAG  = 11   /* 'inlet','specifiedstagnationpressure': the static-pressure inlet's flux
+                            * and velocity (patch_vel the direction); after AssembleMdot
+                            * p_b = max(p0 - rho |U_b|^2 / 2, 0) (TotalConditionsBoundary.for:25-45),
+                            * the p' coefficients of AssemblePressureCorrectionFluxes.for:663-720 and
+                            * UpdatePressureCorrectionAtBoundaries.for:97-112; patch_pressure = p0 */
 };
 
 /* ---------------------------------------------------------- scheme enums */
@@ -122,8 +132,10 @@ enum fs_solver {
   FS_SOLVER_AMG_BICGS = 3, /* FP64 BiCGSTAB right-preconditioned by one AMG V-cycle (no reference row) */
   FS_SOLVER_AMG32_BICGS = 4,/* same with an FP32 AMG hierarchy (iterative refinement, no reference row) */
   FS_SOLVER_GMRES = 5,     /* 'gmres': GMRES_RESTARTED_OMP_RETURNR restated (matrixSolverOMP.f90:48) */
-  FS_SOLVER_ILU = 6        /* 'ilu': D-ILU factorisation once, then ILU sweeps until rrF or itmax
+  FS_SOLVER_ILU = 6,       /* 'ilu': D-ILU factorisation once, then ILU sweeps until rrF or itmax
                             * (FactorizeUsingILU.for:4, ILUMethod.for:4, SolveAlegbraicEquations.for:122-133) */
+  FS_SOLVER_AMG32GS_BICGS = 7 /* FP64 BiCGSTAB preconditioned by an FP32 V-cycle with symmetric multicolour
+                            * Gauss-Seidel smoothing (no reference row) */
 };
 enum fs_algorithm { FS_SIMPLE = 0, FS_SIMPLEC = 1 };
 
@@ -207,6 +219,8 @@ typedef struct fs_case {
    * the initial Bmdot (the reference leaves the face values to
    * DescribeProblem: set FS_F_BMDOT to override) */
   double patch_mass_flow[FS_MAX_PATCHES];
+  /* 'specifiedresistance' outlets: ArteryResistance per patch */
+  double patch_resistance[FS_MAX_PATCHES];
 } fs_case;
 
 /* TransientScheme values (AssembleTheTransientTerm.for:52,124,199,290). */

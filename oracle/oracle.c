@@ -32,18 +32,22 @@
 /* 'specifiedvelocity' and 'specifiedmassflowrate' inlets take the same
  * momentum, p' and k-epsilon treatment (AssembleIsotropicDiffusion.for:254-300,
  * AssembleConvection.for:260-300, AssemblePressureCorrectionFluxes.for:545-575) */
-#define OM_INLET(t) ((t) == FS_BC_INLET_VEL || (t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP)
+#define OM_INLET(t) ((t) == FS_BC_INLET_VEL || (t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP || (t) == FS_BC_INLET_STAG)
+/* static- and stagnation-pressure inlets: the same loop bodies (incompressible)
+ * but for the boundary pressure and the p' coefficients */
+#define OM_P_INLET(t) ((t) == FS_BC_INLET_SP || (t) == FS_BC_INLET_STAG)
 /* static pressure specified: Rhie-Chow boundary flux, p'_b = 0 (AssembleMdotUsingRhieChow.for:1441-1598, 2105-2283) */
-#define OM_PRESSURE(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_INLET_SP || (t) == FS_BC_OUTLET_ASP)
+#define OM_PRESSURE(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_INLET_SP || (t) == FS_BC_OUTLET_ASP || \
+                        (t) == FS_BC_OUTLET_RES || (t) == FS_BC_INLET_STAG)
 /* 'specifiedstaticpressure' and 'specifiedaveragestaticpressure' outlets share
  * every loop body but CorrectPressure's (AssembleMdotUsingRhieChow.for:1441-1812,
  * AssemblePressureCorrectionFluxes.for:244-400, CorrectMdotandVelocity.for:264-320, ...) */
-#define OM_SP_OUTLET(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_OUTLET_ASP)
+#define OM_SP_OUTLET(t) ((t) == FS_BC_OUTLET_SP || (t) == FS_BC_OUTLET_ASP || (t) == FS_BC_OUTLET_RES)
 /* Dirichlet momentum diffusion and plain upwind convection at the face
  * (AssembleIsotropicDiffusion.for:254-300, 507-525; AssembleConvection.for:260-330, 505-520) */
 #define OM_GIVEN_FLOW(t) (OM_INLET(t) || (t) == FS_BC_OUTLET_MASS)
 /* the direction of the inlet velocity is given (xVeldirection...) */
-#define OM_DIRECTED(t) ((t) == FS_BC_INLET_MASS || (t) == FS_BC_INLET_SP)
+#define OM_DIRECTED(t) ((t) == FS_BC_INLET_MASS || OM_P_INLET(t))
 
 struct om {
   fs_case cfg;
@@ -104,6 +108,9 @@ struct om {
   /* BICGSTAB_OMP persistent storage (SparseMatricesVariables) */
   int csr_built; long *csr_ptr; int *csr_j; int *csr_slot; double *csr_val;
   double *kx, *kr, *kb;
+  /* 'specifiedstagnationpressure' p0 per boundary face (BStagnationPressure);
+   * 'specifiedresistance' geoDiffB per face and geoDiffSum per patch (ArteryResistance1) */
+  double *bp0, *bgd, gdsum[FS_MAX_PATCHES];
   /* ILU (Variables2 dc, rc) */
   double *ilu_dc, *ilu_rc;
   /* multigrid */
@@ -779,10 +786,17 @@ static void om_flow_in_out(om *m)
   }
   /* FlowOut/AdjustFlow return at once unless every outlet is fully developed */
   if (nfd == 0 || other) return;
-  m->mdot_in = 0.;
-  for (int s = 0; s < NS; s++)   /* velocity and mass-flow inlets (CalculateFlowIn.for:37-48) */
-    if (c->patch_type[s] == FS_BC_INLET_VEL || c->patch_type[s] == FS_BC_INLET_MASS)
-    for (int j = 0; j < m->bset_n[s]; j++) m->mdot_in = m->mdot_in + m->bmdot[m->bset_start[s] + j];
+  /* FlowIn returns at once when an inlet is a static- or stagnation-pressure
+   * one (CalculateFlowIn.for:19-31): mdotIn keeps the value the last
+   * CalculateResidualsContinuity left (every inlet face, :195-203) */
+  int p_inlet = 0;
+  for (int s = 0; s < NS; s++) p_inlet |= OM_P_INLET(c->patch_type[s]);
+  if (!p_inlet) {
+    m->mdot_in = 0.;
+    for (int s = 0; s < NS; s++)   /* velocity and mass-flow inlets (CalculateFlowIn.for:37-48) */
+      if (c->patch_type[s] == FS_BC_INLET_VEL || c->patch_type[s] == FS_BC_INLET_MASS)
+        for (int j = 0; j < m->bset_n[s]; j++) m->mdot_in = m->mdot_in + m->bmdot[m->bset_start[s] + j];
+  }
   for (int s = 0; s < NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_FD) {
     m->mdot1[s] = 0.;
     for (int j = 0; j < m->bset_n[s]; j++) {
@@ -891,7 +905,7 @@ static void om_assemble_mdot(om *m)
       fvl = fvl + (1. - c->urf_momentum) * (m->bmdot[b] - ms);
     }
     m->bmdot[b] = fcl * m->p[i1] + ffl * m->bp[b] + fvl;
-    if (m->btype[b] == FS_BC_INLET_SP) om_directed_velocity(m, b);   /* :2277-2282 */
+    if (OM_P_INLET(m->btype[b])) om_directed_velocity(m, b);   /* :2277-2282, 2455-2460 */
   }
   /* inlet specified velocity Bmdot (AssembleMdotUsingRhieChow.for:2054-2075) */
   for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_VEL)
@@ -922,6 +936,11 @@ void om_assemble_continuity(om *m)
   memset(m->pc, 0, sizeof(double) * N);          /* InitializePressureCorrection */
   om_flow_in_out(m);                             /* FlowIn, FlowOut, AdjustFlow */
   om_assemble_mdot(m);
+  /* UpdateBoundaryForTotalConditions (TotalConditionsBoundary.for:25-45), incompressible */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_STAG) {
+    const double vel2 = m->bu[b] * m->bu[b] + m->bv[b] * m->bv[b] + m->bw[b] * m->bw[b];
+    m->bp[b] = fmax(m->bp0[b] - 0.5 * c->rho * vel2, 0.);
+  }
   /* AssemblePressureCorrection (AssemblePressureCorrectionFluxes.for:85-164) */
   for (int k = 0; k < F; k++) {
     double du = avgf(m, k, m->du2), dv = avgf(m, k, m->dv2), dw = avgf(m, k, m->dw2);
@@ -936,6 +955,26 @@ void om_assemble_continuity(om *m)
     double gd = geo_diff(c->method_decompose_s, m->du2[i1], m->dv2[i1], m->dw2[i1], m->bsx[b], m->bsy[b], m->bsz[b],
                          m->bex[b], m->bey[b], m->bez[b], m->bd[b], 0, 0, 0);
     m->fcf[F + b] = c->rho * gd; m->fff[F + b] = c->rho * gd;
+    m->bgd[b] = gd;
+  }
+  /* 'specifiedresistance' outlets (:400-500): geoDiffSum per patch, FluxCf
+   * rho geoDiff (1 + (geoDiffSum - geoDiff) R) / (1 + R geoDiffSum) */
+  for (int s = 0; s < m->NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_RES) {
+    m->gdsum[s] = 0.;
+    for (int j = 0; j < m->bset_n[s]; j++) m->gdsum[s] = m->gdsum[s] + m->bgd[m->bset_start[s] + j];
+    const double R = c->patch_resistance[s];
+    for (int j = 0; j < m->bset_n[s]; j++) {
+      const int b = m->bset_start[s] + j;
+      double fcl = c->rho * m->bgd[b];
+      fcl = fcl * (1 + (m->gdsum[s] - m->bgd[b]) * R) / (1. + R * m->gdsum[s]);
+      m->fcf[F + b] = fcl;
+    }
+  }
+  /* 'specifiedstagnationpressure' inlets (:663-720): FluxCf Bmdot FluxFf / (Bmdot - FluxFf rho |U_b|^2) */
+  for (int b = 0; b < B; b++) if (m->btype[b] == FS_BC_INLET_STAG) {
+    const double vel2 = m->bu[b] * m->bu[b] + m->bv[b] * m->bv[b] + m->bw[b] * m->bw[b];
+    const double ff = m->fff[F + b];
+    m->fcf[F + b] = m->bmdot[b] * ff / (m->bmdot[b] - ff * c->rho * vel2);
   }
   /* specified-velocity inlet: FluxCf=FluxFf=0 (AssemblePressureCorrectionFluxes.for:545-563) */
   global_assembly(m);
@@ -951,8 +990,27 @@ void om_correct_continuity(om *m)
   int N = m->N, F = m->F, B = m->B;
   const fs_case *c = &m->cfg;
   /* UpdateBoundaryPressureCorrection (UpdatePressureCorrectionAtBoundaries.for) */
-  for (int b = 0; b < B; b++)
-    m->bpc[b] = OM_PRESSURE(m->btype[b]) ? 0. : m->pc[m->bf_own[b]];   /* :85-90, 126-130 */
+  for (int b = 0; b < B; b++) {
+    const int t = m->btype[b];
+    if (t == FS_BC_INLET_STAG) {   /* :97-112, geoDiff = FluxFf */
+      const double gd = m->fff[F + b];
+      const double vel2 = m->bu[b] * m->bu[b] + m->bv[b] * m->bv[b] + m->bw[b] * m->bw[b];
+      m->bpc[b] = -c->rho * vel2 * gd * m->pc[m->bf_own[b]] / (m->bmdot[b] - gd * c->rho * vel2);
+    } else if (t != FS_BC_OUTLET_RES) {
+      m->bpc[b] = (t == FS_BC_OUTLET_SP || t == FS_BC_INLET_SP || t == FS_BC_OUTLET_ASP) ? 0. : m->pc[m->bf_own[b]];   /* :85-90, 126-143 */
+    }
+  }
+  /* 'specifiedresistance' (:144-175): R sum(geoDiffB p'_C) / (1 + R geoDiffSum) on the patch */
+  for (int s = 0; s < m->NS; s++) if (c->patch_type[s] == FS_BC_OUTLET_RES) {
+    double pcr = 0.;
+    for (int j = 0; j < m->bset_n[s]; j++) {
+      const int b = m->bset_start[s] + j;
+      pcr = pcr + m->bgd[b] * m->pc[m->bf_own[b]];
+    }
+    const double R = c->patch_resistance[s];
+    pcr = R * pcr / (1. + R * m->gdsum[s]);
+    for (int j = 0; j < m->bset_n[s]; j++) m->bpc[m->bset_start[s] + j] = pcr;
+  }
   /* CorrectPressure (CorrectPressure.for:4-42) */
   double rpc = (c->ref_pressure_cell >= 0) ? m->pc[c->ref_pressure_cell] : 0.;
   if (c->set_reference_pressure == 1) rpc = 0.;
@@ -973,7 +1031,7 @@ void om_correct_continuity(om *m)
     int i1 = m->bf_own[b];
     double gd = m->fff[F + b];
     m->bmdot[b] = m->bmdot[b] - gd * (m->bpc[b] - m->pc[i1]);
-    if (m->btype[b] == FS_BC_INLET_SP) { om_directed_velocity(m, b); continue; }
+    if (OM_P_INLET(m->btype[b])) { om_directed_velocity(m, b); continue; }
     m->bu[b] = m->bu[b] - m->du2[i1] * m->pcg[i1];
     m->bv[b] = m->bv[b] - m->dv2[i1] * m->pcg[N + i1];
     m->bw[b] = m->bw[b] - m->dw2[i1] * m->pcg[2L * N + i1];
@@ -995,6 +1053,8 @@ void om_correct_continuity(om *m)
       m->bp[b] = m->bp[b] + c->urf_pressure * (m->bpc[b] - rpc);
     else if (t == FS_BC_OUTLET_ASP)   /* :169-176 */
       m->bp[b] = m->p[i1];
+    else if (t == FS_BC_OUTLET_RES || t == FS_BC_INLET_STAG)   /* :152-160, 206-214 */
+      m->bp[b] = m->bp[b] + c->urf_pressure * (m->bpc[b] - rpc);
   }
   /* 'specifiedaveragestaticpressure': the face pressures shifted so that their
    * area average is AverageOutletPressure (:178-203) */
@@ -1028,6 +1088,7 @@ void om_correct_continuity(om *m)
   m->overall_imbalance = ov; m->imax_imbalance = imx;
   double min_ = 0.;
   for (int b = 0; b < B; b++) if (OM_INLET(m->btype[b])) min_ += m->bmdot[b];   /* every 'inlet' face (:195-203) */
+  m->mdot_in = min_;                                                                /* the module's mdotIn */
   m->rscl[4] = (min_ == 0.) ? 0. : m->rmax[4] / fabs(min_);
   free(mi);
   /* UpdateSymmetry (SymmetryAndAxisBoundary.for:4-33), UpdateSlipWallBoundary */
@@ -1541,7 +1602,10 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
    * (ReferenceAndSetPressureRoutines.for:4-50): a pressure-specified patch
    * fixes the level, no reference cell */
   int has_sp = 0;
-  for (int b = 0; b < B; b++) if (OM_PRESSURE(m->btype[b])) { m->bp[b] = cfg->patch_pressure[m->bf_set[b]]; has_sp = 1; }
+  m->bp0 = dz_(B); m->bgd = dz_(B);
+  for (int b = 0; b < B; b++) if (OM_PRESSURE(m->btype[b])) {
+    m->bp[b] = cfg->patch_pressure[m->bf_set[b]]; m->bp0[b] = m->bp[b]; has_sp = 1;
+  }
   if (m->cfg.set_reference_pressure < 0) m->cfg.set_reference_pressure = has_sp;
   m->ug = dz_(3L*N); m->vg = dz_(3L*N); m->wg = dz_(3L*N); m->pg = dz_(3L*N); m->pcg = dz_(3L*N);
   m->bug = dz_(3L*B); m->bvg = dz_(3L*B); m->bwg = dz_(3L*B); m->bpg = dz_(3L*B); m->bpcg = dz_(3L*B);
@@ -1564,7 +1628,7 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
   om_wall_distance(m);
   /* 'specifiedmassflowrate' inlets: direction per face, Bmdot = -mdot |S_f| / sum |S| in face order */
   m->bdir = dz_(3L * B);
-  for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_INLET_SP)
+  for (int s = 0; s < m->NS; s++) if (OM_P_INLET(cfg->patch_type[s]))
     for (int j = 0; j < m->bset_n[s]; j++)
       for (int q = 0; q < 3; q++) m->bdir[3L * (m->bset_start[s] + j) + q] = cfg->patch_vel[s][q];
   for (int s = 0; s < m->NS; s++) if (cfg->patch_type[s] == FS_BC_OUTLET_MASS) {   /* outflow: Bmdot > 0 */

@@ -325,7 +325,8 @@ def _scipy_solution(o):
     return A, spla.spsolve(A.tocsc(), o.get("bc"))
 
 
-@pytest.mark.parametrize("solver,tol", [("amg", 1e-6), ("amg_bicgs", 1e-8), ("amg32_bicgs", 1e-8)])
+@pytest.mark.parametrize("solver,tol", [("amg", 1e-6), ("amg_bicgs", 1e-8), ("amg32_bicgs", 1e-8),
+                                        ("amg32gs_bicgs", 1e-8)])
 def test_multigrid_solvers_momentum_system(solver, tol):
     mesh, case = cs.cavity(16, nz=14, jitter=0.2, seed=3, krylov_tol=1e-10, krylov_maxit=200,
                            mg_max_cycles=200)
@@ -340,7 +341,7 @@ def test_multigrid_solvers_momentum_system(solver, tol):
     assert _rel(x, x_direct) <= tol, (solver, it, _rel(x, x_direct))
 
 
-@pytest.mark.parametrize("solver", ["amg_bicgs", "amg32_bicgs", "amg"])
+@pytest.mark.parametrize("solver", ["amg_bicgs", "amg32_bicgs", "amg32gs_bicgs", "amg"])
 def test_multigrid_pressure_correction_residual(solver):
     # the closed-cavity p' system is singular: check the residual, and the
     # solution up to the constant null vector
