@@ -54,7 +54,7 @@ __device__ __forceinline__ void fs_directed_velocity(const double *bdir, const d
 
 #define FS_BLOCK 256
 #ifndef FS_COOP_BLOCK
-#define FS_COOP_BLOCK 256            // threads per CTA of the persistent cooperative solvers
+#define FS_COOP_BLOCK 1024           // most threads per CTA of the persistent cooperative solvers
 #endif
 #define FS_RED_BLOCKS 1184           // 148 SMs x 8: partial-sum slots of the grid reductions
 
@@ -267,7 +267,8 @@ int fs_mg_free(fs_ctx *ctx);
 void fs_ilu_free(fs_ctx *ctx);
 int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);
 int fs_solver_stats_collect(fs_ctx *ctx);
-int fs_coop_per_sm(fs_ctx *ctx, int occupancy);         // CTAs per SM for a cooperative launch
+int fs_coop_per_sm(fs_ctx *ctx, int occupancy);         // CTAs per SM for a cooperative launch (1)
+int fs_coop_block(const fs_ctx *ctx);                   // threads per CTA of a cooperative launch
 int fs_nn_before_pc(fs_ctx *ctx, const double **x0);   // features (+ guess) before the p' solve
 int fs_nn_after_pc(fs_ctx *ctx);                        // snapshot capture, previous p'
 void fs_nn_free(fs_ctx *ctx);

@@ -47,7 +47,7 @@ namespace cg = cooperative_groups;
 #endif
 // CTAs per SM the preconditioned Krylov kernel is compiled for (register cap)
 #ifndef FS_AMG_MINB
-#define FS_AMG_MINB 4
+#define FS_AMG_MINB 1
 #endif
 #ifndef FS_MG_ALPHA
 #define FS_MG_ALPHA 1.8
@@ -374,6 +374,9 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
 #define FS_PC_TEAM_MAX 4096   // levels up to this many rows run on the CTA team
 #endif
 #define FS_PC_SPIN_LIMIT (1L << 20)   // polls of a team barrier before it reports a timeout
+#ifndef FS_PC_GS_LEVELS
+#define FS_PC_GS_LEVELS 1     // amg32gs_bicgs: Gauss-Seidel on the levels below this one, Jacobi above
+#endif
 #ifndef FS_PC_FUSE_DOWN
 #define FS_PC_FUSE_DOWN 0     // restrictions from levels below this one form the residual on the fly
 #endif
@@ -816,10 +819,12 @@ struct PCycle {
       }
     }
   }
-  // The V-cycle with symmetric multicolour Gauss-Seidel smoothing: on every
-  // level a forward pass from zero before the restriction and, after the
-  // correction x += alpha x_c[parent], a backward pass; the coarsest level by
-  // the dense inverse.  out = M^-1 in; callers have made `in` visible.
+  // The V-cycle with symmetric multicolour Gauss-Seidel smoothing on the
+  // levels below FS_PC_GS_LEVELS (a forward pass from zero before the
+  // restriction and, after the correction x += alpha x_c[parent], a backward
+  // pass) and the damped Jacobi sweeps of run() on the others; the coarsest
+  // level by the dense inverse.  Results stay in each level's x.  out =
+  // M^-1 in; callers have made `in` visible.
   __device__ void run_gs(const double *__restrict__ in, double *__restrict__ out) {
     Scope g;
     g.grid = true;
@@ -833,14 +838,16 @@ struct PCycle {
       residual(l, in, L.x, L.r);
       Scope scc = pc_scope(C);
       enter(scc);
+      const bool gsc = l + 1 < FS_PC_GS_LEVELS;
+      const R omc = (gsc || l + 1 == lc) ? (R)0. : om(l + 1);   // Jacobi: the first sweep from zero
       if (scc.active())
         for (long P = scc.tid0(); P < C.n; P += scc.nth()) {
           R s = 0.;
           for (int c = C.rptr[P]; c < C.rptr[P + 1]; c++) s = s + L.r[C.rlist[c]];
           C.b[P] = s;
-          C.x[P] = (R)0.;
+          C.x[P] = omc * s / C.ac[P];
         }
-      if (l + 1 < lc) gs_colours(l + 1, in, C.x, false);
+      if (l + 1 < lc && gsc) gs_colours(l + 1, in, C.x, false);
     }
     {
       Scope c0;
@@ -864,7 +871,13 @@ struct PCycle {
       enter(sl);
       if (sl.active())
         for (long i = sl.tid0(); i < L.n; i += sl.nth()) L.x[i] = L.x[i] + al(l) * xc[L.parent[i]];
-      gs_colours(l, in, L.x, true);
+      if (l < FS_PC_GS_LEVELS) {
+        gs_colours(l, in, L.x, true);
+      } else {   // one damped Jacobi sweep in place: residual into t, then the update
+        residual(l, in, L.x, L.t);
+        enter(sl);
+        if (sl.active()) for (long i = sl.tid0(); i < L.n; i += sl.nth()) L.x[i] = L.x[i] + om(l) * L.t[i] / L.ac[i];
+      }
     }
     enter(g);
     for (long i = g.tid0(); i < L0.n; i += g.nth()) out[i] = (double)L0.x[i];
@@ -1530,7 +1543,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.rrf = rrf; a.ires = ctx->resblk + RB_ABS + (nf - 1); a.part = M->red; a.iters = ctx->d_iters + (nf - 1);
     void *args[] = {&a};
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
-    FS_CK(fs_coop_launch((const void *)k_mg_solve, G, FS_COOP_BLOCK, args, ctx->st));
+    FS_CK(fs_coop_launch((const void *)k_mg_solve, G, fs_coop_block(ctx), args, ctx->st));
     FS_LAUNCH_CHECK();
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
     return FS_OK;
@@ -1568,7 +1581,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     void *args[] = {&a};
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<double, 1> : (const void *)k_amg_bicgstab<double, 0>,
-                         G, FS_COOP_BLOCK, args, ctx->st));
+                         G, fs_coop_block(ctx), args, ctx->st));
   } else {
     AmgKArgs<float> a{};
     fill(a);
@@ -1578,7 +1591,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     // the FP32 cycle runs the unfused V-cycle: measured at 128^3, its fused
     // form was 1.5 % slower (the FP64 cycle gains 5 % from fusion)
     const void *k = gs ? (const void *)k_amg_bicgstab<float, 2> : (const void *)k_amg_bicgstab<float, 0>;
-    FS_CK(fs_coop_launch(k, G, FS_COOP_BLOCK, args, ctx->st));
+    FS_CK(fs_coop_launch(k, G, fs_coop_block(ctx), args, ctx->st));
   }
   FS_LAUNCH_CHECK();
   FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));

@@ -101,8 +101,9 @@ class Ensemble:
         self.shapes = [0] * len(self.solvers)
 
     def autotune(self, shapes=(1, 2, 3, 4), iters: int = 2) -> list[int]:
-        """Pick each case's cooperative CTAs per SM by timing `iters` SIMPLE
-        iterations per candidate (after one untimed iteration at that shape)."""
+        """Pick each case's cooperative launch shape (256 x shape threads on
+        every SM) by timing `iters` SIMPLE iterations per candidate (after one
+        untimed iteration at that shape)."""
         best = []
         for s in self.solvers:
             t = {}

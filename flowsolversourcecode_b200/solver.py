@@ -275,9 +275,10 @@ class Solver:
                                                L.iptr(out["nbr"]), L.dptr(out["anb"]), n, w), "mg_coarse_matrix")
         return out
 
-    def set_launch_shape(self, ctas_per_sm: int):
-        """Cooperative CTAs per SM of the persistent solver kernels (0: default)."""
-        self._chk(self.lib.fs_set_launch_shape(self.ctx, ctas_per_sm), "fs_set_launch_shape")
+    def set_launch_shape(self, shape: int):
+        """Threads per SM of the persistent cooperative solver kernels in units
+        of 256 (1..4; 0: the default 1024), one CTA per SM."""
+        self._chk(self.lib.fs_set_launch_shape(self.ctx, shape), "fs_set_launch_shape")
 
     # ------------------------------------------------------------ learned p' guess
     def nn_create(self, snapshot_capacity: int = 0, seed: int = 0):

@@ -446,8 +446,9 @@ int fs_nn_policy(fs_ctx *ctx, double *avg_guessed, double *avg_zero, int32_t *pa
 
 /* ----------------------------------------------------- ensemble and launch shape
  * No reference counterparts.
- * fs_set_launch_shape: cooperative CTAs per SM of the persistent solver
- *   kernels (1..8; 0 = occupancy limit capped at 4); the project's autotuner
+ * fs_set_launch_shape: threads per SM of the persistent cooperative solver
+ *   kernels, in units of 256 (1..4; 0 = 1024): every cooperative launch puts
+ *   one CTA of 256 * shape threads on each SM; the project's autotuner
  *   (flowsolversourcecode_b200/ensemble.py) picks it per case by timing.
  * fs_ensemble_run: `iters` SIMPLE iterations of each of n independent cases
  *   (contexts on one GPU) captured into one CUDA graph, cases in sequence so
@@ -457,7 +458,7 @@ int fs_nn_policy(fs_ctx *ctx, double *avg_guessed, double *avg_zero, int32_t *pa
  *   (optional, same shape) the p' iterations, ms_out the device time.  One
  *   ordinary iteration per case runs first (hierarchies, colourings, grids);
  *   the learned guess is not used inside the graph. */
-int fs_set_launch_shape(fs_ctx *ctx, int ctas_per_sm);
+int fs_set_launch_shape(fs_ctx *ctx, int shape);
 /* Test of the bounded device waits (no reference counterpart): with extra > 0
  * the AMG preconditioner's team barriers wait for `extra` more CTAs than take
  * part, so their bounded polls run out (well under a second); the iteration

@@ -487,9 +487,12 @@ def test_oracle_flow_in_keeps_last_inflow_with_pressure_inlet():
 
 @pytest.mark.gpu
 def test_pressure_inlet_fully_developed_outlet_matches_oracle():
+    """The degenerate combination above on the GPU.  The stop metric is the
+    RMS norm (NstopType 3): v is rounding noise of 1e-16 on both sides, so its
+    normalised residual (noise over noise) would decide a NstopType-4 metric."""
     import oracle
     from flowsolversourcecode_b200.solver import Solver
-    m, c = cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, **_tight())
+    m, c = cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, nstop_type=3, **_tight())
     c.patches["inlet"] = ("pressure_inlet", (1.0, 0.0, 0.0), 0.05)
     o = oracle.Oracle(m, c)
     g = Solver(m, c)
