@@ -23,11 +23,14 @@ FS_E_TOO_LARGE = -9
 FS_NOALLOC_MAX_ROWS = 262144
 FS_NN_NPARAM = 33665
 # variable ids (GetNFfromVariable)
-VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_P = 1, 2, 3, 4, 5, 6
-VAR_TKE, VAR_TED, VAR_RHOK = 8, 9, 10
+VAR_U, VAR_V, VAR_W, VAR_PC, VAR_MASS, VAR_TEMP = 1, 2, 3, 4, 5, 6
+VAR_TKE, VAR_TED, VAR_RHOK, VAR_P = 8, 9, 10, 20
 # boundary types
 (BC_WALL_NOSLIP, BC_WALL_SLIP, BC_SYMMETRY, BC_INLET_VEL, BC_OUTLET_FD, BC_OUTLET_SP, BC_INLET_MASS, BC_INLET_SP,
  BC_OUTLET_MASS, BC_OUTLET_ASP, BC_OUTLET_RES, BC_INLET_STAG) = range(12)
+# thermal boundary types (fs_tbc)
+TBC = {"default": 0, "dirichlet": 1, "vonneumann": 2, "robin": 3, "statictemperature": 4,
+       "stagnationtemperature": 5, "fullydevelopedenergy": 6, "symmetry": 7}
 TRANSIENT = {"euler": 0, "cranknicolson1": 1, "cranknicolson2": 2, "adamsmoulton": 3}
 # gradient interpolation
 GI_AVERAGE, GI_UPWIND, GI_DOWNWIND, GI_AVERAGECORRECTED = 0, 1, 2, 3
@@ -41,7 +44,7 @@ FIELDS = ["u", "v", "w", "p", "pc", "mdot", "bu", "bv", "bw", "bp", "bpc", "bmdo
           "du1", "dv1", "dw1", "du2", "dv2", "dw2", "ugrad", "vgrad", "wgrad", "pgrad", "pcgrad",
           "volume", "xc", "gfactor", "sf", "gdiff", "ft", "bsf", "dphi",
           "tke", "ted", "mut", "btke", "bted", "bmut", "kx", "utau", "yplus",
-          "old", "oldold", "bold"]
+          "old", "oldold", "bold", "temp", "btemp", "tgrad"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
 
@@ -78,6 +81,16 @@ class FsCase(C.Structure):
         ("unsteady", C.c_int), ("transient_scheme", C.c_int), ("dt", C.c_double),
         ("patch_mass_flow", C.c_double * FS_MAX_PATCHES),
         ("patch_resistance", C.c_double * FS_MAX_PATCHES),
+        ("energy", C.c_int), ("cp", C.c_double), ("conductivity", C.c_double), ("temp_init", C.c_double),
+        ("solver_energy", C.c_int), ("rrf_energy", C.c_double), ("itmax_energy", C.c_int),
+        ("relax_energy", C.c_int), ("urf_energy", C.c_double), ("conv_scheme_energy", C.c_int),
+        ("bleed_energy", C.c_double), ("method_grad_energy", C.c_int), ("niter_grad_energy", C.c_int),
+        ("grad_interp_energy", C.c_int), ("gamma_interp_energy", C.c_int),
+        ("energy_sc", C.c_double), ("energy_sb", C.c_double),
+        ("limit_temperature", C.c_int), ("temp_min", C.c_double), ("temp_max", C.c_double),
+        ("sigma_t", C.c_double), ("energy_wall_function", C.c_int),
+        ("patch_thermal", C.c_int * FS_MAX_PATCHES), ("patch_temperature", C.c_double * FS_MAX_PATCHES),
+        ("patch_heat_flux", C.c_double * FS_MAX_PATCHES), ("patch_h_inf", C.c_double * FS_MAX_PATCHES),
     ]
 
 
@@ -107,6 +120,8 @@ class FsResiduals(C.Structure):
         ("source", C.c_double),
         ("turb_abs", C.c_double * 2), ("turb_max", C.c_double * 2), ("turb_rms", C.c_double * 2),
         ("turb_scaled", C.c_double * 2), ("turb_lin_iters", C.c_int * 2),
+        ("temp_abs", C.c_double), ("temp_max", C.c_double), ("temp_rms", C.c_double), ("temp_scaled", C.c_double),
+        ("temp_lin_iters", C.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -114,7 +129,9 @@ class FsResiduals(C.Structure):
                 "overall_imbalance": self.overall_imbalance, "imax_imbalance": self.imax_imbalance,
                 "lin_iters": list(self.lin_iters), "source": self.source,
                 "turb_abs": list(self.turb_abs), "turb_max": list(self.turb_max), "turb_rms": list(self.turb_rms),
-                "turb_scaled": list(self.turb_scaled), "turb_lin_iters": list(self.turb_lin_iters)}
+                "turb_scaled": list(self.turb_scaled), "turb_lin_iters": list(self.turb_lin_iters),
+                "temp_abs": self.temp_abs, "temp_max": self.temp_max, "temp_rms": self.temp_rms,
+                "temp_scaled": self.temp_scaled, "temp_lin_iters": self.temp_lin_iters}
 
 
 # every entry point of include/fsb200.h with its argument types
@@ -128,6 +145,7 @@ PROTOTYPES = {
     "fs_last_error": (C.c_char_p, [_V]),
     "fs_solve_momentum": (C.c_int, [_V, C.c_int]),
     "fs_solve_continuity": (C.c_int, [_V]),
+    "fs_solve_energy": (C.c_int, [_V]),
     "fs_simple_iteration": (C.c_int, [_V, C.POINTER(FsResiduals)]),
     "fs_simple_iteration_host": (C.c_int, [_V, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, C.POINTER(FsResiduals)]),
     "fs_assemble_momentum": (C.c_int, [_V, C.c_int]),

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfsb200.so")
-SOURCES = ["fs_geometry.cu", "fs_simple.cu", "fs_turb.cu", "fs_time.cu", "fs_neutral.cu", "fs_solvers.cu", "fs_mg.cu", "fs_nn.cu", "fs_capi.cu"]
+SOURCES = ["fs_geometry.cu", "fs_simple.cu", "fs_turb.cu", "fs_energy.cu", "fs_time.cu", "fs_neutral.cu", "fs_solvers.cu", "fs_mg.cu", "fs_nn.cu", "fs_capi.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC,-O2",

@@ -101,6 +101,34 @@ class Case:
     unsteady: bool = False
     transient_scheme: str = "euler"        # 'euler', 'cranknicolson1', 'cranknicolson2', 'adamsmoulton'
     dt: float = 1.0e-2
+    # temperature equation (LSolveEnergy, EnergyEquation='temperature'); defaults
+    # of ProblemDescriptionRoutine.for:101-525 and User0.F90:83
+    energy: bool = False
+    cp: float = 1.0                        # SpecificHeat
+    conductivity: float = 0.01             # Conductivity
+    temp_init: float = 0.0                 # initial temperature
+    solver_energy: str = "sor"             # ASSolverEnergy
+    rrf_energy: float = 0.01               # rrfEnergy
+    itmax_energy: int = 30                 # ASIterEnergy
+    relax_energy: bool = True              # LRelaxEnergy
+    urf_energy: float = 0.7                # urfEnergy
+    conv_scheme_energy: str = "minmod"     # ConvectionSchemeEnergy
+    bleed_energy: float = 0.0              # BleedEnergy
+    method_grad_energy: int = 2            # MethodCalcGradientEnergy
+    niter_grad_energy: int = 2             # nIterGradientEnergy
+    grad_interp_energy: str = "average"    # GradientInterpolationSchemeEnergy
+    gamma_interp_energy: str = "harmonic"  # InterpolationSchemeGamaEnergy
+    energy_sc: float = 0.0                 # ScEnergy (uniform)
+    energy_sb: float = 0.0                 # SbEnergy (uniform)
+    limit_temperature: bool = False        # LimitTemperature
+    temp_min: float = 0.0                  # tempmin
+    temp_max: float = 1.0e30               # tempmax
+    sigma_t: float = 0.0                   # SigT (0: the k-epsilon default 0.9)
+    energy_wall_function: str = "standard" # EnergyWallFunctionType
+    # patch name -> (thermal type, value[, h_inf]): "dirichlet" (T_wall), "vonneumann"
+    # (heat flux), "robin" (T_inf, h_inf), "statictemperature" (T), "stagnationtemperature"
+    # (T0), "fullydevelopedenergy", "symmetry"; unnamed patches take the flow type's default
+    thermal: dict = field(default_factory=dict)
 
     def struct(self, mesh: PolyMesh) -> L.FsCase:
         c = L.FsCase()
@@ -169,6 +197,26 @@ class Case:
         c.conv_scheme_tke, c.conv_scheme_ted = L.TVD[self.conv_scheme_tke], L.TVD[self.conv_scheme_ted]
         c.wall_function = {"standard": 0, "scalable": 1, "automatic": 2}[self.wall_function]
         c.unsteady, c.transient_scheme, c.dt = int(self.unsteady), L.TRANSIENT[self.transient_scheme], float(self.dt)
+        c.energy, c.cp, c.conductivity, c.temp_init = int(self.energy), self.cp, self.conductivity, self.temp_init
+        c.solver_energy, c.rrf_energy, c.itmax_energy = L.SOLVER[self.solver_energy], self.rrf_energy, self.itmax_energy
+        c.relax_energy, c.urf_energy = int(self.relax_energy), self.urf_energy
+        c.conv_scheme_energy, c.bleed_energy = L.TVD[self.conv_scheme_energy], self.bleed_energy
+        c.method_grad_energy, c.niter_grad_energy = self.method_grad_energy, self.niter_grad_energy
+        c.grad_interp_energy = gi[self.grad_interp_energy]
+        c.gamma_interp_energy = {"average": 0, "upwind": 1, "downwind": 2, "harmonic": 3}[self.gamma_interp_energy]
+        c.energy_sc, c.energy_sb = self.energy_sc, self.energy_sb
+        c.limit_temperature, c.temp_min, c.temp_max = int(self.limit_temperature), self.temp_min, self.temp_max
+        c.sigma_t = self.sigma_t
+        c.energy_wall_function = {"standard": 0, "scalable": 1, "automatic": 2}[self.energy_wall_function]
+        for s, name in enumerate(mesh.patch_names):
+            spec = self.thermal.get(name, ("default",))
+            c.patch_thermal[s] = L.TBC[spec[0]]
+            if spec[0] == "vonneumann":
+                c.patch_heat_flux[s] = float(spec[1])
+            elif spec[0] == "robin":
+                c.patch_temperature[s], c.patch_h_inf[s] = float(spec[1]), float(spec[2])
+            elif len(spec) > 1:
+                c.patch_temperature[s] = float(spec[1])
         return c
 
 

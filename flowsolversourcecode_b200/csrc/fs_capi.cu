@@ -128,9 +128,11 @@ static double *field_ptr(fs_ctx *c, int f, size_t *n) {
   case FS_F_TKE: case FS_F_TED: case FS_F_MUT: case FS_F_BTKE: case FS_F_BTED: case FS_F_BMUT:
   case FS_F_UTAU: case FS_F_YPLUS:
     return fs_turb_field(c, f, n);
-  case FS_F_OLD: *n = c->old ? 6 * N : 0; return c->old;
-  case FS_F_OLDOLD: *n = c->oldold ? 6 * N : 0; return c->oldold;
-  case FS_F_BOLD: *n = c->bold ? 6 * B : 0; return c->bold;
+  case FS_F_OLD: *n = c->old ? FS_NLEVELS * N : 0; return c->old;
+  case FS_F_OLDOLD: *n = c->oldold ? FS_NLEVELS * N : 0; return c->oldold;
+  case FS_F_BOLD: *n = c->bold ? FS_NLEVELS * B : 0; return c->bold;
+  case FS_F_T: case FS_F_BT: case FS_F_TGRAD:
+    return fs_energy_field(c, f, n);
   }
   *n = 0;
   return nullptr;
@@ -170,7 +172,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   ctx->cfg = *cfg;
   ctx->dev = device;
   int rc = FS_OK;
-  auto fail = [&](int r) { fs_transient_free(ctx); fs_turb_free(ctx); free_all(ctx); if (ctx->st) cudaStreamDestroy(ctx->st); delete ctx; return r; };
+  auto fail = [&](int r) { fs_transient_free(ctx); fs_energy_free(ctx); fs_turb_free(ctx); free_all(ctx); if (ctx->st) cudaStreamDestroy(ctx->st); delete ctx; return r; };
   if (cudaSetDevice(device) != cudaSuccess) return fail(FS_E_CUDA);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(FS_E_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -225,6 +227,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   if (cudaMalloc(&ctx->d_bset, sizeof(int32_t) * (B ? B : 1)) != cudaSuccess) return fail(FS_E_NOMEM);
   if (B) cudaMemcpyAsync(ctx->d_bset, ctx->h_bset.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice, ctx->st);
   if ((rc = fs_turb_create(ctx))) return fail(rc);
+  if ((rc = fs_energy_create(ctx))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
   // boundary values from the patches (setBoundaryConditions): wall / inlet velocities
   std::vector<double> hb(3 * B, 0.);
   for (size_t b = 0; b < B; b++) {
@@ -303,6 +306,7 @@ int fs_destroy(fs_ctx *ctx) {
   fs_ilu_free(ctx);
   fs_nn_free(ctx);
   fs_turb_free(ctx);
+  fs_energy_free(ctx);
   fs_transient_free(ctx);
   free_all(ctx);
   for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
@@ -345,6 +349,13 @@ static int pc_solve(fs_ctx *ctx) {
   return fs_nn_after_pc(ctx);
 }
 
+int fs_solve_energy(fs_ctx *ctx) {
+  if (!ctx) return FS_E_ARG;
+  if (!ctx->energy) { ctx->err = "fs_solve_energy: the case does not solve the temperature equation"; return FS_E_ARG; }
+  cudaSetDevice(ctx->dev);
+  return fs_energy_solve(ctx);
+}
+
 int fs_solve_continuity(fs_ctx *ctx) {
   if (!ctx) return FS_E_ARG;
   int rc = fs_continuity_assemble(ctx);
@@ -384,6 +395,7 @@ static double stop_metric(const fs_case &c, const double *rb) {
   s = fmax(s, fmax(fabs(rb[o]), fmax(fabs(rb[o + 1]), fabs(rb[o + 2]))));
   s = fmax(s, fabs(rb[o + 4]));
   if (c.turbulence) { s = fmax(s, fabs(rb[o + FS_VAR_TKE - 1])); s = fmax(s, fabs(rb[o + FS_VAR_TED - 1])); }
+  if (c.energy) s = fmax(s, fabs(rb[o + FS_VAR_TEMP - 1]));
   return s;
 }
 
@@ -412,6 +424,11 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
     r.turb_abs[q] = rb[RB_ABS + e]; r.turb_max[q] = rb[RB_MAX + e]; r.turb_rms[q] = rb[RB_RMS + e];
     r.turb_scaled[q] = rb[RB_SCL + e]; r.turb_lin_iters[q] = it[e];
   }
+  {
+    const int e = FS_VAR_TEMP - 1;
+    r.temp_abs = rb[RB_ABS + e]; r.temp_max = rb[RB_MAX + e]; r.temp_rms = rb[RB_RMS + e];
+    r.temp_scaled = rb[RB_SCL + e]; r.temp_lin_iters = it[e];
+  }
   if (ctx->nn) fs_nn_note_iters(ctx, it[FS_VAR_PC - 1]);
   r.overall_imbalance = rb[RB_OVERALL];
   r.imax_imbalance = (int)rb[RB_IMAX];
@@ -422,6 +439,7 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   if (ctx->cfg.turbulence)
     for (int q = 0; q < 2; q++)
       if (!std::isfinite(r.turb_abs[q])) { ctx->err = "NaN/Inf residual"; return FS_E_NAN; }
+  if (ctx->cfg.energy && !std::isfinite(r.temp_abs)) { ctx->err = "NaN/Inf residual"; return FS_E_NAN; }
   // divergence: the stop metric grew past FS_DIVERGENCE_FACTOR times the largest
   // one of the earlier outer iterations of the run (or of the time step)
   if (std::isfinite(r.source) && r.source > 0.) {
@@ -460,8 +478,9 @@ static int iteration_body(fs_ctx *ctx) {
   if (rc) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[3], ctx->st));
   if ((rc = fs_continuity_correct(ctx))) return rc;
-  // CalculateEffectsOfTurbulence (MainProgram.for:275-277)
+  // CalculateEffectsOfTurbulence (MainProgram.for:275-277), SolveEnergy (:281)
   if ((rc = fs_turb_effects(ctx))) return rc;
+  if ((rc = fs_energy_solve(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[4], ctx->st));
   return FS_OK;
 }
@@ -511,6 +530,14 @@ int fs_gradient(fs_ctx *ctx, int var, int method, int n_iter) {
   case FS_VAR_W: phi = ctx->w; bphi = ctx->bw; g = ctx->wg; bg = ctx->bwg; break;
   case FS_VAR_P: phi = ctx->p; bphi = ctx->bp; g = ctx->pg; bg = ctx->bpg; break;
   case FS_VAR_PC: phi = ctx->pc; bphi = ctx->bpc; g = ctx->pcg; bg = ctx->bpcg; break;
+  case FS_VAR_TEMP: {
+    size_t n;
+    phi = fs_energy_field(ctx, FS_F_T, &n); bphi = fs_energy_field(ctx, FS_F_BT, &n);
+    g = fs_energy_field(ctx, FS_F_TGRAD, &n);
+    bg = fs_energy_bgrad(ctx);
+    if (!phi) { ctx->err = "fs_gradient: the case does not solve the temperature equation"; return FS_E_ARG; }
+    break;
+  }
   default: return FS_E_ARG;
   }
   return fs_gradient_dev(ctx, 1, &var, &phi, &bphi, &g, &bg, &method, &n_iter);
@@ -519,7 +546,9 @@ int fs_gradient(fs_ctx *ctx, int var, int method, int n_iter) {
 int fs_gradient_host(fs_ctx *ctx, int var, int method, int n_iter, const double *phi, const double *bphi,
                      double *grad, double *bgrad) {
   if (!ctx || !phi || !bphi || !grad || !bgrad) return FS_E_ARG;
-  if (var < FS_VAR_U || var > FS_VAR_P || var == FS_VAR_MASS) return FS_E_ARG;
+  if (var != FS_VAR_U && var != FS_VAR_V && var != FS_VAR_W && var != FS_VAR_PC && var != FS_VAR_P &&
+      var != FS_VAR_TEMP)
+    return FS_E_ARG;
   cudaSetDevice(ctx->dev);
   const size_t N = ctx->N, B = ctx->B;
   // stage through the (otherwise unused during this call) Krylov vectors
@@ -560,8 +589,11 @@ static int residual_of_system(fs_ctx *ctx, int nf, const double *fi) {
 }
 
 int fs_solve_equation(fs_ctx *ctx, int var, double rrf, int itmax, int solver) {
-  if (!ctx || var < FS_VAR_U || var > FS_VAR_PC) return FS_E_ARG;
-  double *fi = var == FS_VAR_U ? ctx->u : var == FS_VAR_V ? ctx->v : var == FS_VAR_W ? ctx->w : ctx->pc;
+  if (!ctx || ((var < FS_VAR_U || var > FS_VAR_PC) && var != FS_VAR_TEMP)) return FS_E_ARG;
+  size_t n;
+  double *fi = var == FS_VAR_U ? ctx->u : var == FS_VAR_V ? ctx->v : var == FS_VAR_W ? ctx->w :
+               var == FS_VAR_TEMP ? fs_energy_field(ctx, FS_F_T, &n) : ctx->pc;
+  if (!fi) { ctx->err = "fs_solve_equation: the case does not solve the temperature equation"; return FS_E_ARG; }
   int rc = residual_of_system(ctx, var, fi);
   if (rc) return rc;
   return fs_linear_solve(ctx, var, fi, rrf, itmax, solver);

@@ -155,9 +155,11 @@ __device__ __forceinline__ double tvd_psi(int s, double rf) {
   return 0.;
 }
 
-// HRSchemesCorrections (AssembleHRSchemeCorrection.for:36-134), TVD framework, cpf=1
+// HRSchemesCorrections (AssembleHRSchemeCorrection.for:36-134), TVD framework; cpf is 1
+// but for the temperature equation's face specific heat (:121-124)
 __device__ __forceinline__ double hr_flux(int scheme, double bleed, double md, double phio, double phin,
-                                          const double go[3], const double gn[3], double dx, double dy, double dz) {
+                                          const double go[3], const double gn[3], double dx, double dy, double dz,
+                                          double cpf = 1.) {
   double phic, phid, gx, gy, gz;
   if (md > 0.) { phic = phio; phid = phin; gx = go[0]; gy = go[1]; gz = go[2]; }
   else { phic = phin; phid = phio; gx = gn[0]; gy = gn[1]; gz = gn[2]; dx = -dx; dy = -dy; dz = -dz; }
@@ -167,22 +169,24 @@ __device__ __forceinline__ double hr_flux(int scheme, double bleed, double md, d
   double psi = tvd_psi(scheme, rf);
   double phiHR = phic + 0.5 * psi * diff;
   phiHR = (1. - bleed) * phiHR + bleed * phic;
-  return md * (phiHR - phic) * 1.;
+  return md * (phiHR - phic) * cpf;
 }
 
 // AssembleTransientTerm (AssembleTheTransientTerm.for:52-330) for time-level
-// block lvl (0..2 velocity, 4 k, 5 epsilon) of cell i: adds to the cell's
-// FluxCE and FluxTE sums in the reference's order.
+// block lvl (0..2 velocity, 4 k, 5 epsilon, 6 temperature) of cell i: adds to
+// the cell's FluxCE and FluxTE sums in the reference's order.  cp is the
+// temperature equation's SpecificHeat (Density*SpecificHeat*Volume), 1 otherwise
+// (multiplying by 1 leaves the other equations' products unchanged).
 __device__ __forceinline__ void transient_term(const FsTransient &t, int lvl, long N, long i, double V, double phi,
-                                               double &fce, double &fte) {
+                                               double &fce, double &fte, double cp = 1.) {
   const double po = t.old[lvl * N + i];
   if (!t.three) {
-    const double fcl = t.rho * V / t.d, fcol = -(t.rho * V / t.d);
+    const double fcl = t.rho * cp * V / t.d, fcol = -(t.rho * cp * V / t.d);
     fce = fce + fcl;
     fte = fte + fcl * phi + fcol * po;
   } else {
     const double poo = t.oldold[lvl * N + i];
-    const double fcl = t.f1 * t.rho * V, fcol = t.s2 * (t.f2 * t.rho * V), fcool = t.f3 * t.rho * V;
+    const double fcl = t.f1 * t.rho * cp * V, fcol = t.s2 * (t.f2 * t.rho * cp * V), fcool = t.f3 * t.rho * cp * V;
     fce = fce + fcl;
     fte = fte + fcl * phi + fcol * po + fcool * poo;
   }

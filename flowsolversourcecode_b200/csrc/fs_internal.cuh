@@ -63,10 +63,12 @@ enum { RED_SUM0 = 0, RED_SUM1, RED_SUM2, RED_MAX0, RED_MAX1, RED_NQ };
 
 struct fs_mg_dev;  // multigrid hierarchy (fs_mg.cu)
 struct fs_turb;    // k-epsilon state (fs_turb.cu)
+struct fs_energy;  // temperature equation state (fs_energy.cu)
 struct fs_nn;      // learned p' initial guess (fs_nn.cu)
 struct fs_ilu;     // D-ILU level schedule (fs_solvers.cu)
 
 #define FS_NEQ 9        // equations with residual slots: NF 1..9
+#define FS_NLEVELS 7    // unsteady time levels: u v w p k epsilon T
 #define FS_NITERS 16     // int32 iteration-count slots (NF - 1 indexed)
 
 struct fs_ctx {
@@ -140,13 +142,14 @@ struct fs_ctx {
   // [0] mdotIn, [1 + s] mdot1(s), [1 + FS_MAX_PATCHES + s] mdotOut(s)
   int32_t *d_bset = nullptr;
   double *flow = nullptr;
-  // unsteady runs: u v w p k epsilon at time levels n-1, n-2 (6N each), their
-  // boundary values at n-1 (6B), p at the last X-momentum gradient ('cranknicolson1')
+  // unsteady runs: u v w p k epsilon T at time levels n-1, n-2 (FS_NLEVELS N each),
+  // their boundary values at n-1 (FS_NLEVELS B), p at the last X-momentum gradient ('cranknicolson1')
   double *old = nullptr, *oldold = nullptr, *bold = nullptr, *p_mx = nullptr;
   double dt = 0., dto = 0., dtoo = 0., time = 0.;
   int ndt = 0, tscheme = 0;      // tscheme: the TransientScheme in effect
   // k-epsilon (nullptr: laminar)
   fs_turb *turb = nullptr;
+  fs_energy *energy = nullptr;
   // multigrid
   fs_mg_dev *mg = nullptr;
   // level schedule and factor of the 'ilu' solver (built on first use)
@@ -245,7 +248,7 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
 struct FsTransient {
   int on, three;
   double rho, d, f1, f2, f3, s2;
-  const double *old, *oldold;    // 6N blocks: u v w p k epsilon
+  const double *old, *oldold;    // FS_NLEVELS blocks of N: u v w p k epsilon T
 };
 FsTransient fs_transient_args(const fs_ctx *ctx);
 double fs_drhodt(const fs_ctx *ctx);                   // d rho/dt of the continuity residual
@@ -261,6 +264,13 @@ void fs_turb_brhok_ptrs(fs_ctx *ctx, const double **brhok, const double **bdrk);
 int fs_turb_wall_functions(fs_ctx *ctx);
 int fs_turb_rhok_gradient(fs_ctx *ctx);
 int fs_turb_effects(fs_ctx *ctx);
+double *fs_turb_wall_distance(fs_ctx *ctx);            // WallDistance (N), nullptr when laminar
+// temperature equation (fs_energy.cu)
+int fs_energy_create(fs_ctx *ctx);
+void fs_energy_free(fs_ctx *ctx);
+double *fs_energy_field(fs_ctx *ctx, int field, size_t *n);
+double *fs_energy_bgrad(fs_ctx *ctx);                   // BTempGrad (3B)
+int fs_energy_solve(fs_ctx *ctx);
 int fs_flow_in_out(fs_ctx *ctx);
 int fs_mg_build(fs_ctx *ctx);
 int fs_mg_free(fs_ctx *ctx);

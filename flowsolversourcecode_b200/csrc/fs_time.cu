@@ -4,9 +4,9 @@
 // (MainProgram.for:184-245: CrankNicolson, updateVariablesInTime, dt
 // bookkeeping).  Density, DensityOld and DensityOldOld are the constant rho.
 //
-// Layout: old / oldold hold u, v, w, p, k, epsilon in blocks of N (time
+// Layout: old / oldold hold u, v, w, p, k, epsilon, T in blocks of N (time
 // levels n-1 and n-2); bold the boundary values at n-1 in blocks of B.  The
-// k and epsilon blocks stay zero in laminar runs.
+// k and epsilon blocks stay zero in laminar runs, the T block in isothermal ones.
 #include "fs_internal.cuh"
 
 namespace {
@@ -31,7 +31,8 @@ void time_factors(int scheme, double dt, double dto, double dtoo, double f[3]) {
   }
 }
 
-// the six solved fields (cell values, or boundary values with bnd)
+// the solved fields of the time levels (cell values, or boundary values with
+// bnd); nullptr for k, epsilon or T when their equation is not solved
 double *level_field(fs_ctx *ctx, int q, bool bnd) {
   size_t n = 0;
   switch (q) {
@@ -40,7 +41,8 @@ double *level_field(fs_ctx *ctx, int q, bool bnd) {
   case 2: return bnd ? ctx->bw : ctx->w;
   case 3: return bnd ? ctx->bp : ctx->p;
   case 4: return fs_turb_field(ctx, bnd ? FS_F_BTKE : FS_F_TKE, &n);
-  default: return fs_turb_field(ctx, bnd ? FS_F_BTED : FS_F_TED, &n);
+  case 5: return fs_turb_field(ctx, bnd ? FS_F_BTED : FS_F_TED, &n);
+  default: return fs_energy_field(ctx, bnd ? FS_F_BT : FS_F_T, &n);
   }
 }
 
@@ -98,21 +100,21 @@ int fs_transient_create(fs_ctx *ctx) {
     return FS_E_ARG;
   }
   const size_t N = ctx->N, B = ctx->B;
-  if (cudaMalloc(&ctx->old, sizeof(double) * 6 * N) != cudaSuccess ||
-      cudaMalloc(&ctx->oldold, sizeof(double) * 6 * N) != cudaSuccess ||
-      cudaMalloc(&ctx->bold, sizeof(double) * 6 * (B ? B : 1)) != cudaSuccess)
+  if (cudaMalloc(&ctx->old, sizeof(double) * FS_NLEVELS * N) != cudaSuccess ||
+      cudaMalloc(&ctx->oldold, sizeof(double) * FS_NLEVELS * N) != cudaSuccess ||
+      cudaMalloc(&ctx->bold, sizeof(double) * FS_NLEVELS * (B ? B : 1)) != cudaSuccess)
     return FS_E_NOMEM;
   if (c.transient_scheme == FS_TRANSIENT_CRANKNICOLSON1 && cudaMalloc(&ctx->p_mx, sizeof(double) * N) != cudaSuccess)
     return FS_E_NOMEM;
-  FS_CK(cudaMemsetAsync(ctx->old, 0, sizeof(double) * 6 * N, ctx->st));
-  FS_CK(cudaMemsetAsync(ctx->bold, 0, sizeof(double) * 6 * (B ? B : 1), ctx->st));
+  FS_CK(cudaMemsetAsync(ctx->old, 0, sizeof(double) * FS_NLEVELS * N, ctx->st));
+  FS_CK(cudaMemsetAsync(ctx->bold, 0, sizeof(double) * FS_NLEVELS * (B ? B : 1), ctx->st));
   if (ctx->p_mx) FS_CK(cudaMemsetAsync(ctx->p_mx, 0, sizeof(double) * N, ctx->st));
-  for (int q = 0; q < 6; q++) {
+  for (int q = 0; q < FS_NLEVELS; q++) {
     const double *x = level_field(ctx, q, false), *bx = level_field(ctx, q, true);
     if (x) FS_CK(cudaMemcpyAsync(ctx->old + q * N, x, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->st));
     if (bx && B) FS_CK(cudaMemcpyAsync(ctx->bold + q * B, bx, sizeof(double) * B, cudaMemcpyDeviceToDevice, ctx->st));
   }
-  FS_CK(cudaMemcpyAsync(ctx->oldold, ctx->old, sizeof(double) * 6 * N, cudaMemcpyDeviceToDevice, ctx->st));
+  FS_CK(cudaMemcpyAsync(ctx->oldold, ctx->old, sizeof(double) * FS_NLEVELS * N, cudaMemcpyDeviceToDevice, ctx->st));
   ctx->dt = ctx->dto = ctx->dtoo = c.dt;
   ctx->time = 0.;
   ctx->ndt = 0;
@@ -134,12 +136,12 @@ int fs_advance_time(fs_ctx *ctx, double dt_next) {
   if (!c.unsteady || !ctx->old) { ctx->err = "fs_advance_time: the case is not unsteady"; return FS_E_ARG; }
   if (!(dt_next > 0.)) { ctx->err = "fs_advance_time: dt_next must be > 0"; return FS_E_ARG; }
   const long N = ctx->N, B = ctx->B;
-  const int nq = ctx->turb ? 6 : 4;
   if (c.transient_scheme == FS_TRANSIENT_CRANKNICOLSON1 && ctx->ndt != 0) {
     // CrankNicolson (CrankNicolsonRoutine.for:51-80,150): extrapolate, then AssembleMdot,
     // whose PressGradf is still the one the last X-momentum solve interpolated
     ctx->tscheme = FS_TRANSIENT_CRANKNICOLSON1;
-    for (int q = 0; q < nq; q++) {
+    for (int q = 0; q < FS_NLEVELS; q++) {
+      if (!level_field(ctx, q, false)) continue;   // an equation the case does not solve
       k_cn_extrapolate<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(level_field(ctx, q, false), ctx->old + q * N, N);
       FS_LAUNCH_CHECK();
       if (B) {
@@ -152,8 +154,9 @@ int fs_advance_time(fs_ctx *ctx, double dt_next) {
   }
   ctx->tscheme = scheme_in_effect(c.transient_scheme, ctx->ndt);
   // updateVariablesInTime (AdvanceVariablesInTime.for:98-160)
-  FS_CK(cudaMemcpyAsync(ctx->oldold, ctx->old, sizeof(double) * 6 * N, cudaMemcpyDeviceToDevice, ctx->st));
-  for (int q = 0; q < nq; q++) {
+  FS_CK(cudaMemcpyAsync(ctx->oldold, ctx->old, sizeof(double) * FS_NLEVELS * N, cudaMemcpyDeviceToDevice, ctx->st));
+  for (int q = 0; q < FS_NLEVELS; q++) {
+    if (!level_field(ctx, q, false)) continue;
     FS_CK(cudaMemcpyAsync(ctx->old + q * N, level_field(ctx, q, false), sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->st));
     if (B)
       FS_CK(cudaMemcpyAsync(ctx->bold + q * B, level_field(ctx, q, true), sizeof(double) * B, cudaMemcpyDeviceToDevice, ctx->st));

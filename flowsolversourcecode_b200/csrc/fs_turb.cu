@@ -500,6 +500,8 @@ double *fs_turb_field(fs_ctx *ctx, int field, size_t *n) {
   return nullptr;
 }
 
+double *fs_turb_wall_distance(fs_ctx *ctx) { return ctx->turb ? ctx->turb->wdist : nullptr; }
+
 // pointers the momentum kernels read: mu_t (N), BeDiffCoefficient (B), grad(2/3 rho k) (3N)
 void fs_turb_momentum_ptrs(fs_ctx *ctx, const double **mut, const double **bedif, const double **drk) {
   fs_turb *T = ctx->turb;

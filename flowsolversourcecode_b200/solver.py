@@ -24,7 +24,8 @@ from . import _lib as L
 from .case import Case
 from .mesh import PolyMesh
 
-VARIABLE = {"velx": L.VAR_U, "vely": L.VAR_V, "velz": L.VAR_W, "pressc": L.VAR_PC, "press": L.VAR_P}
+VARIABLE = {"velx": L.VAR_U, "vely": L.VAR_V, "velz": L.VAR_W, "pressc": L.VAR_PC, "press": L.VAR_P,
+            "temp": L.VAR_TEMP}
 
 
 class Solver:
@@ -71,6 +72,12 @@ class Solver:
 
     def SolveContinuity(self):
         self._chk(self.lib.fs_solve_continuity(self.ctx), "SolveContinuity")
+
+    def SolveEnergy(self):
+        """SolveEnergy, 'temperature' (SelectEnergyEquationToSolve.for:4)."""
+        self._chk(self.lib.fs_solve_energy(self.ctx), "SolveEnergy")
+
+    energy = SolveEnergy
 
     def assemble_momentum(self, comp: int):
         self._chk(self.lib.fs_assemble_momentum(self.ctx, comp), "assemble_momentum")
@@ -188,7 +195,7 @@ class Solver:
         sizes = {"mdot": F, "gfactor": F, "gdiff": F, "sf": 3 * F, "ft": 3 * F, "anb": W * N,
                  "bu": B, "bv": B, "bw": B, "bp": B, "bpc": B, "bmdot": B, "bsf": 3 * B, "xc": 3 * N,
                  "btke": B, "bted": B, "bmut": B, "utau": B, "yplus": B,
-                 "old": 6 * N, "oldold": 6 * N, "bold": 6 * B}
+                 "old": 7 * N, "oldold": 7 * N, "bold": 7 * B, "btemp": B}
         if name.endswith("grad"):
             return 3 * N
         return sizes.get(name, N)
@@ -205,6 +212,7 @@ class Solver:
     # fields that carry information from one outer iteration to the next
     RESTART_FIELDS = ("u", "v", "w", "p", "mdot", "bu", "bv", "bw", "bp", "bmdot", "kx")
     RESTART_TURB = ("tke", "ted", "mut", "btke", "bted", "bmut", "utau", "yplus")
+    RESTART_ENERGY = ("temp", "btemp")
     # unsteady runs: the old time levels (ReadSolutionToContinue.for:59-108)
     RESTART_UNSTEADY = ("old", "oldold", "bold")
 
@@ -216,6 +224,7 @@ class Solver:
         to a .npz file.  Gradients, D, u* and the matrices are rebuilt by the
         next iteration before they are read, so they are not stored."""
         names = self.RESTART_FIELDS + (self.RESTART_TURB if self.case.turbulence else ())
+        names += self.RESTART_ENERGY if self.case.energy else ()
         names += self.RESTART_UNSTEADY if self.case.unsteady else ()
         data = {k: self.get(k) for k in names}
         data["nIter"] = np.array([self.nIter], np.int64)

@@ -56,10 +56,13 @@ extern "C" {
 #define FS_VAR_W      3
 #define FS_VAR_PC     4
 #define FS_VAR_MASS   5
-#define FS_VAR_P      6   /* 'press' (pressure itself, gradient calls only) */
+#define FS_VAR_TEMP   6   /* 'temp' (AssignNFvaluesToVariables.for:45), the temperature equation */
 #define FS_VAR_TKE    8   /* 'tke' (AssignNFvaluesToVariables.for:55) */
 #define FS_VAR_TED    9   /* 'ted' (AssignNFvaluesToVariables.for:60) */
 #define FS_VAR_RHOK  10   /* 'rhok' = 2/3 rho k (gradient calls only, AssembleMinusTwoThirdsRhoK.for) */
+#define FS_VAR_P     20   /* 'press' (pressure itself, gradient calls only; the reference's
+                           * 'press' shares NF 5 with the continuity residual, so it takes
+                           * an id of its own here) */
 
 /* ------------------------------------------------------ field ids (get/set) */
 enum fs_field {
@@ -78,8 +81,10 @@ enum fs_field {
   FS_F_BTKE, FS_F_BTED, FS_F_BMUT,                   /* B */
   FS_F_KX,                                           /* N: BICGSTAB_OMP's persistent solution vector */
   FS_F_UTAU, FS_F_YPLUS,                             /* B: wall-function state (uTau, yplus) */
-  FS_F_OLD, FS_F_OLDOLD,                             /* 6N: u v w p k epsilon at time levels n-1, n-2 (unsteady) */
-  FS_F_BOLD,                                         /* 6B: their boundary values at n-1 */
+  FS_F_OLD, FS_F_OLDOLD,                             /* 7N: u v w p k epsilon T at time levels n-1, n-2 (unsteady) */
+  FS_F_BOLD,                                         /* 7B: their boundary values at n-1 */
+  FS_F_T, FS_F_BT,                                   /* N, B: temperature (energy equation) */
+  FS_F_TGRAD,                                        /* 3N: its gradient */
   FS_F_COUNT
 };
 
@@ -113,6 +118,24 @@ enum fs_bc {
                             * p_b = max(p0 - rho |U_b|^2 / 2, 0) (TotalConditionsBoundary.for:25-45),
                             * the p' coefficients of AssemblePressureCorrectionFluxes.for:663-720 and
                             * UpdatePressureCorrectionAtBoundaries.for:97-112; patch_pressure = p0 */
+};
+
+/* ------------------------------------------------ thermal boundary types
+ * The temperature equation's boundary sets (BoundaryConditions1: IWallDirichlet,
+ * IWallVonNeumann, IWallRobin, IinletSpecifiedStaticTemperature,
+ * IinletSpecifiedStagnationTemperature, IoutletFullyDevelopedEnergy, Isymmetry),
+ * one per patch.  FS_TBC_DEFAULT takes the flow type's counterpart: walls von
+ * Neumann with patch_heat_flux (adiabatic at 0), inlets static temperature,
+ * outlets fully developed, symmetry planes symmetry. */
+enum fs_tbc {
+  FS_TBC_DEFAULT = 0,
+  FS_TBC_WALL_DIRICHLET = 1,   /* wall temperature patch_temperature */
+  FS_TBC_WALL_NEUMANN = 2,     /* heat flux patch_heat_flux into the domain per unit area */
+  FS_TBC_WALL_ROBIN = 3,       /* HinfinityRobin = patch_h_inf, TinfinityRobin = patch_temperature */
+  FS_TBC_INLET_STATIC = 4,     /* 'specifiedstatictemperature': patch_temperature */
+  FS_TBC_INLET_STAGNATION = 5, /* 'specifiedstagnationtemperature': T = patch_temperature - |U_b|^2/(2 cp) */
+  FS_TBC_OUTLET_FD = 6,        /* 'fullydevelopedenergy': T_b = T_owner */
+  FS_TBC_SYMMETRY = 7          /* T_b = T_owner, no flux */
 };
 
 /* ---------------------------------------------------------- scheme enums */
@@ -221,6 +244,35 @@ typedef struct fs_case {
   double patch_mass_flow[FS_MAX_PATCHES];
   /* 'specifiedresistance' outlets: ArteryResistance per patch */
   double patch_resistance[FS_MAX_PATCHES];
+  /* temperature equation (LSolveEnergy, EnergyEquation='temperature';
+   * Energy/SolveTemperatureEquation.for:4-291), solved after the turbulence
+   * equations of each outer iteration (MainProgram.for:281): constant rho, cp
+   * and conductivity, isotropic diffusion.  0 = isothermal. */
+  int    energy;
+  double cp;                     /* SpecificHeat */
+  double conductivity;           /* Conductivity */
+  double temp_init;              /* initial temperature of the cells and of the faces no boundary type sets */
+  int    solver_energy;          /* ASSolverEnergy */
+  double rrf_energy;             /* rrfEnergy */
+  int    itmax_energy;           /* ASIterEnergy */
+  int    relax_energy;           /* LRelaxEnergy */
+  double urf_energy;             /* urfEnergy */
+  int    conv_scheme_energy;     /* ConvectionSchemeEnergy (fs_tvd, HRFrameworkEnergy 'tvd') */
+  double bleed_energy;           /* BleedEnergy */
+  int    method_grad_energy;     /* MethodCalcGradientEnergy (1 or 2) */
+  int    niter_grad_energy;      /* nIterGradientEnergy */
+  int    grad_interp_energy;     /* GradientInterpolationSchemeEnergy (fs_gradinterp) */
+  int    gamma_interp_energy;    /* InterpolationSchemeGamaEnergy: 0 'average', 1 'upwind',
+                                  * 2 'downwind', 3 'harmonic' (InterpolateFromElementToFace.for:17-60) */
+  double energy_sc, energy_sb;   /* ScEnergy, SbEnergy, uniform: the source Sb + Sc T per unit volume */
+  int    limit_temperature;      /* LimitTemperature */
+  double temp_min, temp_max;     /* tempmin, tempmax */
+  double sigma_t;                /* SigT, the turbulent Prandtl number of k-epsilon runs */
+  int    energy_wall_function;   /* EnergyWallFunctionType of k-epsilon runs: 0 'standard', 1 'scalable', 2 'automatic' */
+  int    patch_thermal[FS_MAX_PATCHES];      /* fs_tbc */
+  double patch_temperature[FS_MAX_PATCHES];  /* wall, inlet static or stagnation temperature; TinfinityRobin */
+  double patch_heat_flux[FS_MAX_PATCHES];    /* HeatFlux of von Neumann walls */
+  double patch_h_inf[FS_MAX_PATCHES];        /* HinfinityRobin */
 } fs_case;
 
 /* TransientScheme values (AssembleTheTransientTerm.for:52,124,199,290). */
@@ -283,6 +335,9 @@ typedef struct fs_residuals {
   /* k and epsilon equations (NF 8, 9), filled when the case is turbulent */
   double turb_abs[2], turb_max[2], turb_rms[2], turb_scaled[2];
   int    turb_lin_iters[2];
+  /* temperature equation (NF 6), filled when the case solves it */
+  double temp_abs, temp_max, temp_rms, temp_scaled;
+  int    temp_lin_iters;
 } fs_residuals;
 
 typedef struct fs_ctx fs_ctx;
@@ -305,8 +360,12 @@ const char *fs_last_error(const fs_ctx *ctx);
 int fs_solve_momentum(fs_ctx *ctx, int comp);
 /* SolveContinuity (ContinuityEquation/SolveContinuityEquation.for:4). */
 int fs_solve_continuity(fs_ctx *ctx);
+/* SolveEnergy, EnergyEquation='temperature' (Energy/SelectEnergyEquationToSolve.for:4,
+ * SolveTemperatureEquation.for:4): one temperature solve on the current
+ * velocities and mass fluxes.  FS_E_ARG when the case has energy = 0. */
+int fs_solve_energy(fs_ctx *ctx);
 /* One outer iteration of MainProgram.for:257-325 (momentum x,y,z,
- * continuity, PrintConvergenceHistory's stop metric). */
+ * continuity, k-epsilon, temperature, PrintConvergenceHistory's stop metric). */
 int fs_simple_iteration(fs_ctx *ctx, fs_residuals *res);
 /* Same, but the state arrays live on the HOST: they are copied in, the
  * iteration runs, and they are copied back (the Fortran-owned layout of a

@@ -54,6 +54,8 @@ def load():
         lib.om_gmres.argtypes = [C.c_void_p]
         lib.om_calc_residuals.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         lib.om_residuals_turb.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.om_residuals_temp.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        lib.om_energy.argtypes = [C.c_void_p]
         lib.om_initialize_mdot.argtypes = [C.c_void_p]
         lib.om_turb_production.argtypes = [C.c_void_p]
         lib.om_neu_connectivity_literal.restype = C.c_int
@@ -147,6 +149,17 @@ class Oracle:
         self.lib.om_residuals_turb(self.h, a)
         a = list(a)
         return {"abs": a[0:2], "max": a[2:4], "rms": a[4:6], "scaled": a[6:8]}
+
+    def energy(self):
+        """SolveEnergy ('temperature') on the current velocities and mdot."""
+        self.lib.om_energy(self.h)
+
+    def residuals_temp(self) -> dict:
+        """Residual norms of the temperature equation (NF 6)."""
+        a = (C.c_double * 4)()
+        self.lib.om_residuals_temp(self.h, a)
+        a = list(a)
+        return {"abs": a[0], "max": a[1], "rms": a[2], "scaled": a[3]}
 
     def turb_production(self) -> np.ndarray:
         """k-epsilon production from the current gradients, k, epsilon, mu_t."""

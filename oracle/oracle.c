@@ -115,12 +115,16 @@ struct om {
   double *ilu_dc, *ilu_rc;
   /* multigrid */
   int mg_nlev; int mg_built; void *mgt;
+  /* temperature (Variables1 Temperature, BTemperature, TempGrad*; BStagnationTemperature;
+   * the thermal boundary set of each face) */
+  double *tmp, *btmp, *tmpg, *btmpg, *tmpgf, *bt0; int *tbc;
   /* unsteady (Variables1 ...Old and ...OldOld, Transient1 dt, dtOld, dtOldOld; time, ndt) */
   double *old, *oldold, *bold;
   double dt, dto, dtoo, time;
   int ndt, tscheme;                         /* tscheme: the TransientScheme in effect */
 };
 
+#define OM_NLEVELS 7                  /* time levels: u v w p k epsilon T */
 static double *dz_(long n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
 static void om_momentum_wall_functions(om *m);   /* oracle_turb.inc */
 static int *iz_(long n) { return (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int)); }
@@ -1503,6 +1507,7 @@ void om_solve_equation(om *m, int nf, double *fi, double rrf, int itmax, int sol
 /*  k-epsilon (Turbulence/)                                               */
 /* ===================================================================== */
 #include "oracle_turb.inc"
+#include "oracle_energy.inc"
 
 /* ===================================================================== */
 /*  Stop metric (PrintConvergenceToFileAndScreen.for:613-700)             */
@@ -1515,6 +1520,7 @@ static double stop_metric(om *m)
   s = fmax(s, fmax(fabs(r[0]), fmax(fabs(r[1]), fabs(r[2]))));
   s = fmax(s, fabs(r[4]));
   if (m->cfg.turbulence) { s = fmax(s, fabs(r[7])); s = fmax(s, fabs(r[8])); }
+  if (m->cfg.energy) s = fmax(s, fabs(r[FS_VAR_TEMP - 1]));
   return s;
 }
 
@@ -1524,12 +1530,22 @@ double om_simple_iteration(om *m)
   om_momentum(m, 0); om_momentum(m, 1); om_momentum(m, 2);
   om_continuity(m);
   if (m->cfg.turbulence) om_effects_of_turbulence(m);
+  if (m->cfg.energy) om_solve_temperature(m);   /* SolveEnergy (MainProgram.for:281) */
   return stop_metric(m);
 }
 
 /* CalculateStrainRateTensor + CalculateTurbulenceProduction on the current
  * velocity gradients, k, epsilon and mu_t (into "prod"), for the unit tests */
 void om_turb_production(om *m) { om_strain_rate(m); om_production(m); }
+
+/* SolveEnergy alone, on the current mdot and velocities */
+void om_energy(om *m) { om_solve_temperature(m); }
+
+void om_residuals_temp(om *m, double out[4])
+{
+  int q = FS_VAR_TEMP - 1;
+  out[0] = m->rabs[q]; out[1] = m->rmax[q]; out[2] = m->rrms[q]; out[3] = m->rscl[q];
+}
 
 void om_residuals_turb(om *m, double out[8])
 {
@@ -1649,6 +1665,7 @@ om *om_create(const fs_mesh_in *mi, const fs_case *cfg)
     }
   }
   om_initialize_mdot(m);
+  om_energy_init(m);
   om_transient_init(m);
   return m;
 }
@@ -1700,7 +1717,8 @@ void *om_array(om *m, const char *name, long *len, int *is_int)
     {"wdist", m->wdist, N, 0}, {"itau", m->itau, N, 1},
     {"utau", m->utau, B, 0}, {"yplus", m->yplus, B, 0}, {"uplus", m->uplus, B, 0},
     {"dupdyp", m->dupdyp, B, 0}, {"wallvisc", m->wallvisc, B, 0}, {"bprod", m->bprod, B, 0},
-    {"old", m->old, 6*N, 0}, {"oldold", m->oldold, 6*N, 0}, {"bold", m->bold, 6*B, 0},
+    {"old", m->old, OM_NLEVELS*N, 0}, {"oldold", m->oldold, OM_NLEVELS*N, 0}, {"bold", m->bold, OM_NLEVELS*B, 0},
+    {"temp", m->tmp, N, 0}, {"btemp", m->btmp, B, 0}, {"tempg", m->tmpg, 3*N, 0}, {"btempg", m->btmpg, 3*B, 0},
   };
   for (unsigned q = 0; q < sizeof(t) / sizeof(t[0]); q++)
     if (strcmp(t[q].n, name) == 0) { *len = t[q].len; *is_int = t[q].isint; return t[q].p; }

@@ -39,6 +39,8 @@ double om_simple_iteration(om *m);             /* one outer iteration, returns s
 void   om_set_iter(om *m, int nIter);          /* MultiGrid2 nIter */
 void   om_residuals(om *m, double out[20]);    /* ResorAbs/Max/RMS/Scaled x5 */
 int    om_lin_iters(om *m, int nf);            /* linear iterations last solve of NF */
+void   om_energy(om *m);                      /* SolveEnergy ('temperature') on the current flow */
+void   om_residuals_temp(om *m, double out[4]);/* abs/max/rms/scaled of the temperature (NF 6) */
 void   om_residuals_turb(om *m, double out[8]);/* abs/max/rms/scaled of k, epsilon (NF 8, 9) */
 void   om_initialize_mdot(om *m);              /* CalculateInitialmdot from the current fields */
 int    om_neu_connectivity_literal(const fs_neu_in *in, int *n_internal, int *n_faces, int *face_ptr,
