@@ -77,3 +77,56 @@ def test_ensemble_shards_over_ranks():
     assert out[1][0] == total == float(sum(s.cells for s in specs))
     assert sorted(q for p in parts for q in p) == list(range(64))
     assert not set(parts[0]) & set(parts[1])
+
+
+def _solve_shard(specs, idx, iters=4):
+    """Outer iterations of the cases `idx` on the CPU restatement (the stand-in
+    for a GPU rank's work here): per case the final stop metric and u."""
+    import numpy as np
+    import oracle
+    from flowsolversourcecode_b200 import ensemble as E
+    out = {}
+    for q, (mesh, case) in zip(idx, E.build_cases([specs[q] for q in idx], workers=1, solver_cont="bicgs",
+                                                     batched_momentum=False)):
+        o = oracle.Oracle(mesh, case)
+        src = [o.simple_iteration() for _ in range(iters)]
+        out[q] = (src[-1], float(np.abs(o.get("u")).sum()))
+    return out
+
+
+def _solve_worker(rank, world, port, out):
+    # each rank solves its shard of a small ensemble end to end; the results and
+    # the per-rank time meet only in the final gather and max-reduce
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import time
+    import bench
+    from flowsolversourcecode_b200 import ensemble as E
+    specs = E.make_specs(6, seed=3, edges=(4, 7))
+    mine = E.shard([s.cells for s in specs], world)[rank]
+    t0 = time.perf_counter()
+    res = _solve_shard(specs, mine)
+    ms = bench.reduce_max((time.perf_counter() - t0) * 1e3, dist, "cpu")
+    got = [None] * world
+    dist.all_gather_object(got, res)
+    out[rank] = (ms, got)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_ensemble_solves_match_single_process(oracle_lib):
+    from flowsolversourcecode_b200 import ensemble as E
+    world = 2
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_solve_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn", join=True)
+    specs = E.make_specs(6, seed=3, edges=(4, 7))
+    ref = _solve_shard(specs, list(range(len(specs))))
+    assert out[0][0] == out[1][0] > 0.0                       # the job time is the max over ranks
+    merged = {}
+    for part in out[0][1]:
+        assert not set(part) & set(merged)                   # every case on exactly one rank
+        merged.update(part)
+    assert sorted(merged) == list(range(len(specs)))
+    for q in ref:
+        assert merged[q] == ref[q], q                        # same iterates, bit for bit
