@@ -78,7 +78,8 @@ def test_gradient(distorted, var, method):
     rng = np.random.default_rng(1)
     phi = rng.standard_normal(s.N)
     bphi = rng.standard_normal(s.B)
-    vid = {"velx": 1, "pressc": 4, "press": 6}[var]
+    from flowsolversourcecode_b200 import _lib as L
+    vid = {"velx": L.VAR_U, "pressc": L.VAR_PC, "press": L.VAR_P}[var]
     g, bg = s.gradient_host(var, method, 2, phi, bphi)
     go, bgo = o.gradient(vid, method, 2, phi, bphi)
     _close("grad", g, go)
