@@ -37,7 +37,7 @@ GI_AVERAGE, GI_UPWIND, GI_DOWNWIND, GI_AVERAGECORRECTED = 0, 1, 2, 3
 HR_NONE, HR_TVD = 0, 1
 TVD = {n: i for i, n in enumerate(["upwind", "downwind", "fromm", "sou", "cd", "quick", "superbee", "minmod",
                                     "osher", "vanleer", "muscl", "smart", "hquick", "umist", "charm"])}
-SOLVER = {"sor": 0, "bicgs": 1, "amg": 2, "amg_bicgs": 3, "amg32_bicgs": 4, "gmres": 5, "ilu": 6, "amg32gs_bicgs": 7}
+SOLVER = {"sor": 0, "bicgs": 1, "amg": 2, "amg_bicgs": 3, "amg32_bicgs": 4, "gmres": 5, "ilu": 6, "amg32gs_bicgs": 7, "pbcg": 8}
 SIMPLE, SIMPLEC = 0, 1
 
 FIELDS = ["u", "v", "w", "p", "pc", "mdot", "bu", "bv", "bw", "bp", "bpc", "bmdot", "ac", "bc", "anb",

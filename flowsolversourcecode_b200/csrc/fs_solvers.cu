@@ -600,6 +600,8 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_gmres(GmresAr
 
 struct IluArgs;
 __global__ void k_ilu(IluArgs a);
+struct PbcgArgs;
+__global__ void k_pbcg(PbcgArgs a);
 
 static int coop_grid_size(fs_ctx *ctx) {
   if (ctx->coop_grid > 0) return FS_OK;
@@ -611,7 +613,9 @@ static int coop_grid_size(fs_ctx *ctx) {
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, (void *)k_sor3_colour, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, (void *)k_gmres, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_ilu, FS_COOP_BLOCK, 0));
-  int per_sm = std::min(std::min(std::min(a, d), std::min(b, c)), e);
+  int f = 0;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, (void *)k_pbcg, FS_COOP_BLOCK, 0));
+  int per_sm = std::min(std::min(std::min(a, d), std::min(b, c)), std::min(e, f));
   if (per_sm < 1) { ctx->err = "cooperative kernel does not fit on an SM"; return FS_E_CUDA; }
   ctx->coop_grid = ctx->num_sms * fs_coop_per_sm(ctx, per_sm);
   return FS_OK;
@@ -670,7 +674,30 @@ struct fs_ilu {
   int32_t *lo_ptr = nullptr, *lo_i = nullptr, *lo_sj = nullptr, *lo_si = nullptr;
   int32_t *fl_ptr = nullptr, *fl_rows = nullptr, *bl_ptr = nullptr, *bl_rows = nullptr;
   double *dc = nullptr, *rc = nullptr;
+  // 'pbcg': the transpose lists, every (row i, slot si) whose neighbour is j, sorted by (i, si)
+  int32_t *tr_ptr = nullptr, *tr_i = nullptr, *tr_si = nullptr;
 };
+
+// ILUFactorization: dc = 1/(ac - sum a_ji dc_i a_ij) level by level; element
+// N-2 (the reference's NumberOfElements-1) updates none of its later neighbours
+__device__ void ilu_factor_levels(cg::grid_group &grid, int N, int nlf, const int32_t *fl_ptr, const int32_t *fl_rows,
+                                  const int32_t *lo_ptr, const int32_t *lo_i, const int32_t *lo_sj,
+                                  const int32_t *lo_si, const double *ac, const double *__restrict__ anb, double *dc,
+                                  long tid0, long nth) {
+  for (int L = 0; L < nlf; L++) {
+    for (long q = fl_ptr[L] + tid0; q < fl_ptr[L + 1]; q += nth) {
+      const int j = fl_rows[q];
+      double d = ac[j];
+      for (int e = lo_ptr[j]; e < lo_ptr[j + 1]; e++) {
+        const int i = lo_i[e];
+        if (i == N - 2) continue;
+        d = d - anb[(long)lo_sj[e] * N + j] * dc[i] * anb[(long)lo_si[e] * N + i];
+      }
+      dc[j] = 1.0 / d;
+    }
+    grid.sync();
+  }
+}
 
 struct IluArgs {
   int N, W, nlf, nlb, itmax;
@@ -689,21 +716,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_ilu(IluArgs a
   const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
   const int32_t *__restrict__ cn = a.cn;
   const double *__restrict__ anb = a.anb;
-  // ILUFactorization: dc = 1/(ac - sum a_ji dc_i a_ij); element N-2 (the
-  // reference's NumberOfElements-1) updates none of its later neighbours
-  for (int L = 0; L < a.nlf; L++) {
-    for (long q = a.fl_ptr[L] + tid0; q < a.fl_ptr[L + 1]; q += nth) {
-      const int j = a.fl_rows[q];
-      double d = a.ac[j];
-      for (int e = a.lo_ptr[j]; e < a.lo_ptr[j + 1]; e++) {
-        const int i = a.lo_i[e];
-        if (i == N - 2) continue;
-        d = d - anb[(long)a.lo_sj[e] * N + j] * a.dc[i] * anb[(long)a.lo_si[e] * N + i];
-      }
-      a.dc[j] = 1.0 / d;
-    }
-    grid.sync();
-  }
+  ilu_factor_levels(grid, N, a.nlf, a.fl_ptr, a.fl_rows, a.lo_ptr, a.lo_i, a.lo_sj, a.lo_si, a.ac, anb, a.dc, tid0, nth);
   double ires = *a.ires, fres = ires;
   int iter = 0, buf = 0;
   while (fres > a.rrf * ires && iter < a.itmax) {
@@ -761,6 +774,134 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_ilu(IluArgs a
     iter++;
   }
   if (tid0 == 0) { *a.iters = iter; a.diag[0] = fres; a.diag[1] = ires; }
+}
+
+// 'pbcg' (SolveAlegbraicEquations.for:138-152): sprsin, ILUFactorization, then
+// SolveEquationsUsingPBCG (PBCGMethod.for:96-180) and CheckConvergence until
+// sum|r| <= rrF*IResiduals or itmax.  Numerical Recipes' biconjugate gradient
+// in its minimum-residual form (rr = A r), both systems preconditioned by the
+// D-ILU diagonal; A x sums each row's diagonal then its slots in order
+// (dsprsax), A^T x each column's diagonal then the rows that reference it in
+// element order (dsprstx, through the transpose lists).  bkden carries from
+// one iteration to the next.  Per iteration: p, pp update | A p, A^T pp and
+// the denominator | x, r, rr update | residual sum and the next numerator.
+struct PbcgArgs {
+  int N, W, nlf, itmax;
+  const int32_t *ncf, *cn, *lo_ptr, *lo_i, *lo_sj, *lo_si, *fl_ptr, *fl_rows, *tr_ptr, *tr_i, *tr_si;
+  const double *ac, *anb, *bc;
+  double *x, *dc, *r, *rr, *p, *pp, *z, *zz, *part;
+  const double *ires;
+  double rrf;
+  int32_t *iters;
+  double *diag;
+};
+
+__device__ __forceinline__ double pbcg_ax(const PbcgArgs &a, long i, const double *x) {
+  double t = a.ac[i] * x[i];
+  return ell_acc<8, false>(t, a.N, a.W, a.cn, a.anb, i, [&](int k) { return x[k]; });
+}
+
+__device__ __forceinline__ double pbcg_atx(const PbcgArgs &a, long j, const double *x) {
+  double t = a.ac[j] * x[j];
+  for (int e = a.tr_ptr[j]; e < a.tr_ptr[j + 1]; e++) {
+    const int i = a.tr_i[e];
+    t = t + a.anb[(long)a.tr_si[e] * a.N + i] * x[i];
+  }
+  return t;
+}
+
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_pbcg(PbcgArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  const int N = a.N;
+  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+  ilu_factor_levels(grid, N, a.nlf, a.fl_ptr, a.fl_rows, a.lo_ptr, a.lo_i, a.lo_sj, a.lo_si, a.ac, a.anb, a.dc,
+                    tid0, nth);
+  // iter 0: r = bc - A x, then the minimum-residual shadow rr = A r
+  for (long i = tid0; i < N; i += nth) {
+    const double ri = a.bc[i] - pbcg_ax(a, i, a.x);
+    a.r[i] = ri;
+  }
+  grid.sync();
+  double l0 = 0., l1 = 0., dum;
+  for (long i = tid0; i < N; i += nth) {
+    const double rri = pbcg_ax(a, i, a.r);
+    a.rr[i] = rri;
+    const double zi = a.r[i] * a.dc[i], zzi = rri * a.dc[i];
+    a.z[i] = zi; a.zz[i] = zzi;
+    l0 += zi * rri;
+  }
+  int buf = 0;
+  double bknum, bkden = 0.;
+  grid_sum2(grid, a.part, buf, l0, 0., bknum, dum); buf ^= 1;
+  const double ires = *a.ires;
+  double fres = ires;
+  int iter = 0;
+  while (fres > a.rrf * ires && iter < a.itmax) {
+    const double bk = bknum / (bkden + 1.e-10);
+    for (long i = tid0; i < N; i += nth) {
+      if (iter == 0) { a.p[i] = a.z[i]; a.pp[i] = a.zz[i]; }
+      else { a.p[i] = bk * a.p[i] + a.z[i]; a.pp[i] = bk * a.pp[i] + a.zz[i]; }
+    }
+    bkden = bknum;
+    grid.sync();
+    l0 = 0.;
+    for (long i = tid0; i < N; i += nth) {
+      const double zi = pbcg_ax(a, i, a.p), zzi = pbcg_atx(a, i, a.pp);
+      a.z[i] = zi; a.zz[i] = zzi;
+      l0 += zi * a.pp[i];
+    }
+    double akden;
+    grid_sum2(grid, a.part, buf, l0, 0., akden, dum); buf ^= 1;
+    const double ak = bknum / (akden + 1.e-10);
+    for (long i = tid0; i < N; i += nth) {
+      a.x[i] = a.x[i] + ak * a.p[i];
+      a.r[i] = a.r[i] - ak * a.z[i];
+      a.rr[i] = a.rr[i] - ak * a.zz[i];
+    }
+    grid.sync();
+    // CheckConvergence, and the next call's z = dc r, zz = dc rr, bknum = z.rr
+    l0 = 0.; l1 = 0.;
+    for (long i = tid0; i < N; i += nth) {
+      double q = a.bc[i] - a.ac[i] * a.x[i];
+      q = ell_acc<8, true>(q, N, a.W, a.cn, a.anb, i, [&](int k) { return a.x[k]; });
+      l0 += fabs(q);
+      const double zi = a.r[i] * a.dc[i], zzi = a.rr[i] * a.dc[i];
+      a.z[i] = zi; a.zz[i] = zzi;
+      l1 += zi * a.rr[i];
+    }
+    grid_sum2(grid, a.part, buf, l0, l1, fres, bknum); buf ^= 1;
+    iter++;
+  }
+  if (tid0 == 0) { *a.iters = iter; a.diag[0] = fres; a.diag[1] = ires; }
+}
+
+// the transpose lists of 'pbcg', built once per context after the ILU levels
+static int pbcg_build(fs_ctx *ctx) {
+  fs_ilu *I = ctx->ilu;
+  if (I->tr_ptr) return FS_OK;
+  const int N = ctx->N;
+  const std::vector<int32_t> &ncf = ctx->h_ncf, &cn = ctx->h_cn;
+  std::vector<int32_t> ptr(N + 1, 0);
+  for (int i = 0; i < N; i++)
+    for (int si = 0; si < ncf[i]; si++) {
+      const int j = cn[(size_t)si * N + i];
+      if (j >= 0 && j != i) ptr[j + 1]++;
+    }
+  for (int j = 0; j < N; j++) ptr[j + 1] += ptr[j];
+  std::vector<int32_t> ti(ptr[N]), ts(ptr[N]), pos(ptr.begin(), ptr.end() - 1);
+  for (int i = 0; i < N; i++)   // rows in element order, slots in order: (i, si) sorted per column
+    for (int si = 0; si < ncf[i]; si++) {
+      const int j = cn[(size_t)si * N + i];
+      if (j >= 0 && j != i) { ti[pos[j]] = i; ts[pos[j]] = si; pos[j]++; }
+    }
+  auto up = [&](int32_t **d, const std::vector<int32_t> &h) -> int {
+    FS_CK(cudaMalloc((void **)d, std::max<size_t>(h.size(), 1) * sizeof(int32_t)));
+    if (!h.empty()) FS_CK(cudaMemcpy(*d, h.data(), h.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    return FS_OK;
+  };
+  int rc;
+  if ((rc = up(&I->tr_ptr, ptr)) || (rc = up(&I->tr_i, ti)) || (rc = up(&I->tr_si, ts))) return rc;
+  return FS_OK;
 }
 
 static int ilu_build(fs_ctx *ctx) {
@@ -824,7 +965,8 @@ static int ilu_build(fs_ctx *ctx) {
 void fs_ilu_free(fs_ctx *ctx) {
   fs_ilu *I = ctx->ilu;
   if (!I) return;
-  void *p[] = {I->lo_ptr, I->lo_i, I->lo_sj, I->lo_si, I->fl_ptr, I->fl_rows, I->bl_ptr, I->bl_rows, I->dc, I->rc};
+  void *p[] = {I->lo_ptr, I->lo_i, I->lo_sj, I->lo_si, I->fl_ptr, I->fl_rows, I->bl_ptr, I->bl_rows, I->dc, I->rc,
+               I->tr_ptr, I->tr_i, I->tr_si};
   for (void *x : p) if (x) cudaFree(x);
   delete I;
   ctx->ilu = nullptr;
@@ -889,6 +1031,25 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     void *args[] = {&g};
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     FS_CK(fs_coop_launch((const void *)k_ilu, G, fs_coop_block(ctx), args, ctx->st));
+    FS_LAUNCH_CHECK();
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
+  } else if (solver == FS_SOLVER_PBCG) {
+    if ((rc = ilu_build(ctx)) || (rc = pbcg_build(ctx))) return rc;
+    if ((rc = coop_grid_size(ctx))) return rc;
+    fs_ilu *I = ctx->ilu;
+    PbcgArgs g{};
+    g.N = N; g.W = ctx->W; g.nlf = I->nlf; g.itmax = itmax;
+    g.ncf = ctx->ncf; g.cn = ctx->cn; g.lo_ptr = I->lo_ptr; g.lo_i = I->lo_i; g.lo_sj = I->lo_sj; g.lo_si = I->lo_si;
+    g.fl_ptr = I->fl_ptr; g.fl_rows = I->fl_rows; g.tr_ptr = I->tr_ptr; g.tr_i = I->tr_i; g.tr_si = I->tr_si;
+    g.ac = ctx->ac; g.anb = ctx->anb; g.bc = ctx->bc; g.x = ctx->dphi; g.dc = I->dc;
+    g.r = ctx->kr; g.rr = ctx->kr0; g.p = ctx->kp; g.pp = ctx->kv; g.z = ctx->ks; g.zz = ctx->kt; g.part = ctx->red;
+    g.ires = a.ires; g.rrf = rrf; g.iters = a.iters; g.diag = a.diag;
+    int G = ctx->coop_grid;
+    long need = (N + fs_coop_block(ctx) - 1) / fs_coop_block(ctx);
+    if (need < G) G = (int)(need < 1 ? 1 : need);
+    void *args[] = {&g};
+    FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
+    FS_CK(fs_coop_launch((const void *)k_pbcg, G, fs_coop_block(ctx), args, ctx->st));
     FS_LAUNCH_CHECK();
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
   } else if (solver == FS_SOLVER_BICGS) {

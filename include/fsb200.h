@@ -157,8 +157,11 @@ enum fs_solver {
   FS_SOLVER_GMRES = 5,     /* 'gmres': GMRES_RESTARTED_OMP_RETURNR restated (matrixSolverOMP.f90:48) */
   FS_SOLVER_ILU = 6,       /* 'ilu': D-ILU factorisation once, then ILU sweeps until rrF or itmax
                             * (FactorizeUsingILU.for:4, ILUMethod.for:4, SolveAlegbraicEquations.for:122-133) */
-  FS_SOLVER_AMG32GS_BICGS = 7 /* FP64 BiCGSTAB preconditioned by an FP32 V-cycle with symmetric multicolour
+  FS_SOLVER_AMG32GS_BICGS = 7,/* FP64 BiCGSTAB preconditioned by an FP32 V-cycle with symmetric multicolour
                             * Gauss-Seidel smoothing (no reference row) */
+  FS_SOLVER_PBCG = 8       /* 'pbcg': biconjugate gradient, minimum-residual form, preconditioned by the
+                            * D-ILU diagonal, one iteration per CheckConvergence until rrF or itmax
+                            * (PBCGMethod.for:96-180, SolveAlegbraicEquations.for:138-152) */
 };
 enum fs_algorithm { FS_SIMPLE = 0, FS_SIMPLEC = 1 };
 

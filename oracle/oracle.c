@@ -1242,6 +1242,74 @@ static void ilu_sweep(om *m)
   }
 }
 
+/* PBCG (PBCGMethod.for): Numerical Recipes' biconjugate gradient in its
+ * minimum-residual form (rr = A r at the start), both systems preconditioned
+ * by the D-ILU diagonal dc (asolve, :196-212).  A is sprsin's copy of the
+ * system (:290-333): the diagonal ac, then every neighbour slot of each row
+ * in slot order (thresh 0 keeps zero coefficients).  dsprsax (A x) sums a
+ * row as the diagonal term, then the off-diagonal terms in slot order;
+ * dsprstx (A^T x) starts from the diagonal terms and adds every row's
+ * off-diagonal terms to their columns, rows in element order.  bkden is a
+ * local of SolveEquationsUsingPBCG without SAVE: it is kept from one call
+ * (iteration) to the next here, the only reading under which the recurrence
+ * is defined. */
+struct om_pbcg { double *p, *pp, *r, *rr, *z, *zz, bkden; };
+
+static void pbcg_atimes(const om *m, int trn, const double *b, double *x)
+{
+  const int N = m->N;
+  if (!trn) {
+    for (int i = 0; i < N; i++) {
+      double t = m->ac[i] * b[i];
+      for (int j = 0; j < m->ncf[i]; j++) {
+        const int k = m->cn[(long)j * N + i];
+        if (k >= 0 && k != i) t = t + m->anb[(long)j * N + i] * b[k];
+      }
+      x[i] = t;
+    }
+  } else {
+    for (int i = 0; i < N; i++) x[i] = m->ac[i] * b[i];
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < m->ncf[i]; j++) {
+        const int k = m->cn[(long)j * N + i];
+        if (k >= 0 && k != i) x[k] = x[k] + m->anb[(long)j * N + i] * b[i];
+      }
+  }
+}
+
+/* SolveEquationsUsingPBCG (PBCGMethod.for:96-180), one call = one iteration */
+static void pbcg_step(om *m, struct om_pbcg *w, int iter)
+{
+  const int N = m->N;
+  const double *dc = m->ilu_dc;
+  if (iter == 0) {
+    pbcg_atimes(m, 0, m->dphi, w->r);
+    for (int j = 0; j < N; j++) { w->r[j] = m->bc[j] - w->r[j]; w->rr[j] = w->r[j]; }
+    pbcg_atimes(m, 0, w->r, w->rr);          /* the minimum-residual variant */
+  }
+  for (int i = 0; i < N; i++) w->z[i] = w->r[i] * dc[i];
+  for (int i = 0; i < N; i++) w->zz[i] = w->rr[i] * dc[i];
+  double bknum = 0.;
+  for (int j = 0; j < N; j++) bknum = bknum + w->z[j] * w->rr[j];
+  if (iter == 0) {
+    for (int j = 0; j < N; j++) { w->p[j] = w->z[j]; w->pp[j] = w->zz[j]; }
+  } else {
+    const double bk = bknum / (w->bkden + 1.e-10);
+    for (int j = 0; j < N; j++) { w->p[j] = bk * w->p[j] + w->z[j]; w->pp[j] = bk * w->pp[j] + w->zz[j]; }
+  }
+  w->bkden = bknum;
+  pbcg_atimes(m, 0, w->p, w->z);
+  double akden = 0.;
+  for (int j = 0; j < N; j++) akden = akden + w->z[j] * w->pp[j];
+  const double ak = bknum / (akden + 1.e-10);
+  pbcg_atimes(m, 1, w->pp, w->zz);
+  for (int j = 0; j < N; j++) {
+    m->dphi[j] = m->dphi[j] + ak * w->p[j];
+    w->r[j] = w->r[j] - ak * w->z[j];
+    w->rr[j] = w->rr[j] - ak * w->zz[j];
+  }
+}
+
 /* SolveAlgebraicSystemInParallel CSR (matrixSolverOMP.f90:462-584) + AxOMP (:390-423) */
 static void csr_build(om *m)
 {
@@ -1490,6 +1558,12 @@ void om_solve_equation(om *m, int nf, double *fi, double rrf, int itmax, int sol
   } else if (solver == FS_SOLVER_ILU) {   /* SolveAlegbraicEquations.for:122-133 */
     ilu_factor(m);
     while (FRes > rrf * IRes && iter < itmax) { ilu_sweep(m); FRes = check_convergence(m); iter++; }
+  } else if (solver == FS_SOLVER_PBCG) {  /* SolveAlegbraicEquations.for:138-152 */
+    struct om_pbcg w;
+    w.p = dz_(N); w.pp = dz_(N); w.r = dz_(N); w.rr = dz_(N); w.z = dz_(N); w.zz = dz_(N); w.bkden = 0.;
+    ilu_factor(m);
+    while (FRes > rrf * IRes && iter < itmax) { pbcg_step(m, &w, iter); FRes = check_convergence(m); iter++; }
+    free(w.p); free(w.pp); free(w.r); free(w.rr); free(w.z); free(w.zz);
   } else if (solver == FS_SOLVER_BICGS) {
     iter = om_bicgstab(m, m->cfg.krylov_maxit, m->cfg.krylov_tol);
   } else if (solver == FS_SOLVER_AMG) {

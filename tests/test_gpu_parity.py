@@ -237,6 +237,31 @@ def test_ilu_sweeps_bit_identical():
     assert _rel(x_g, fi) <= 1e-9
 
 
+def test_pbcg_matches_restatement():
+    """'pbcg' (PBCGMethod.for): the same factorisation (bit for bit) and the
+    same recurrence; only the order of the two dot products per iteration
+    differs, so a fixed number of iterations agrees to rounding, and the
+    iterations to rrF agree on the momentum and p' systems."""
+    mesh, case = cs.cavity(12, nz=10, jitter=0.2, seed=3)
+    s, o = _pair(mesh, case)
+    for _ in range(2):
+        o.simple_iteration()
+    o.set_iter(3)
+    for assemble in (lambda: o.assemble_momentum(0), o.assemble_continuity):
+        assemble()
+        ac, anb, bc = o.get("ac"), o.get("anb"), o.get("bc")
+        x_g, it = s.solve_system(ac, anb, bc, rrf=0.0, itmax=6, solver="pbcg")
+        fi = np.zeros(o.N)
+        o.lib.om_solve_equation(o.h, 1, fi.ctypes.data, 0.0, 6, 8)
+        assert it == 6
+        assert _rel(x_g, fi) <= 1e-10
+        x_g, it = s.solve_system(ac, anb, bc, rrf=0.05, itmax=200, solver="pbcg")
+        fi = np.zeros(o.N)
+        o.lib.om_solve_equation(o.h, 1, fi.ctypes.data, 0.05, 200, 8)
+        assert it == o.lin_iters(1)
+        assert _rel(x_g, fi) <= 1e-9
+
+
 def test_outer_iterations_bicgs():
     # non-zero initial velocities so no momentum system has a zero right-hand side
     mesh, case = cs.cavity(10, nz=8, jitter=0.2, seed=1, conv_scheme="sou", niter_start_hr=1,
