@@ -23,6 +23,8 @@ Forms (same case, same initial state):
   python bench.py --ensemble 64 [--gpus N]     the batched-ensemble configuration
   python bench.py --case distorted             the same cavity on the jittered mesh
   python bench.py --case bfs                   the k-epsilon backward-facing step (512x96x48)
+  python bench.py --learned [--case bfs] [--n N]   train the learned p' guess on snapshots, then the
+                                               case with and without it (cavity: the mixed form at 1e-3)
 
 b200 arm: `value` is device-timed (CUDA events on the solver's stream) with
 the state resident in HBM; `e2e` runs the fp64 steps through the C ABI
@@ -474,23 +476,42 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
     ens.close()
 
 
-def run_bfs_learned(args, local: int, n_re: int = 8, per_re: int = 50, epochs: int = 20) -> None:
-    """The learned p' guess on the step: snapshots from plain FP64 runs at
-    `n_re` Reynolds numbers Re_H ~ U[2000, 8000] (splitmix64 seed 1), `per_re`
-    snapshots each (the p' solves of the first per_re+1 SIMPLE iterations
-    from the initial state), the network trained on each run's snapshots in
-    turn (parameters carried over); then Re_H = 5000 from the initial state
-    with and without the guess, `--steps` iterations each after `--warmup`.
-    The guess only changes the p' starting vector: the solve still runs to
-    the same tolerance."""
+def learned_workload(n: int, kind: str, re: float, form: str):
+    """The case of the learned-guess leg: the step at Re_H = re (FP64 form), or
+    the n^3 cavity (SOU from iteration 1) at Re = re in `form`."""
+    from flowsolversourcecode_b200 import case as cs
+    if kind == "bfs":
+        return workload(n, "fp64", "bfs", re_h=re)
+    mesh, case = cs.cavity(n, re=re, conv_scheme="sou", niter_start_hr=1, **FORMS[form])
+    return mesh, case, None
+
+
+def run_learned(args, local: int, n_re: int = 8, per_re: int = 50, epochs: int = 20) -> None:
+    """The learned p' guess.  Step (`--case bfs`): snapshots from plain FP64
+    runs at `n_re` Reynolds numbers Re_H ~ U[2000, 8000] (splitmix64 seed 1),
+    evaluated at Re_H = 5000.  Cavity (`--case cubic`): snapshots from runs of
+    the mixed form with the p' solve to 1e-3 at Re log-uniform on [300, 3000]
+    (seed 1), evaluated at Re = 1000 in the same form -- the mixed + learned
+    form.  `per_re` snapshots per run (the p' solves of the first per_re+1
+    SIMPLE iterations from the initial state); the network is trained on each
+    run's snapshots in turn (parameters carried over); the evaluation case runs
+    from the initial state with and without the guess, `--steps` iterations
+    each after `--warmup`.  The guess only changes the p' starting vector: the
+    solve still runs to the same tolerance."""
     import numpy as np
     from flowsolversourcecode_b200.mesh import uniform01
     from flowsolversourcecode_b200.solver import Solver
-    res = [2000.0 + 6000.0 * float(x) for x in uniform01(1, n_re)]
+    kind = args.case
+    if kind == "bfs":
+        res, re_eval, form = [2000.0 + 6000.0 * float(x) for x in uniform01(1, n_re)], 5000.0, "fp64"
+    else:
+        n_re = 4
+        res = [float(np.exp(np.log(300.0) + float(x) * (np.log(3000.0) - np.log(300.0)))) for x in uniform01(1, n_re)]
+        re_eval, form = 1000.0, "mixed_rrf"
     theta, train = None, []
     t0 = time.time()
     for q, re in enumerate(res):
-        mesh, case, init = workload(args.n, "fp64", "bfs", re_h=re)
+        mesh, case, init = learned_workload(args.n, kind, re, form)
         s = start(Solver(mesh, case, device=local), init)
         s.nn_create(snapshot_capacity=per_re, seed=5)
         if theta is not None:
@@ -500,12 +521,12 @@ def run_bfs_learned(args, local: int, n_re: int = 8, per_re: int = 50, epochs: i
             s.simple_iteration()
         first, last = s.nn_train(epochs=epochs, lr=2e-3, seed=q)
         theta = s.nn_params()
-        train.append({"re_h": round(re, 1), "snapshots": s.nn_snapshots(), "loss_first": first, "loss_last": last})
+        train.append({"re": round(re, 1), "snapshots": s.nn_snapshots(), "loss_first": first, "loss_last": last})
         s.close()
     t_train = time.time() - t0
     legs = {}
     for name, use in (("plain", False), ("learned", True)):
-        mesh, case, init = workload(args.n, "fp64", "bfs")
+        mesh, case, init = learned_workload(args.n, kind, re_eval, form)
         s = start(Solver(mesh, case, device=local), init)
         if use:
             s.nn_create(0, seed=5)
@@ -536,8 +557,11 @@ def run_bfs_learned(args, local: int, n_re: int = 8, per_re: int = 50, epochs: i
         "metric": "SIMPLE iters/s", "value": legs["learned"]["value"], "unit": "iter/s", "n_gpus": 1,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": legs["learned"]["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.n, "bfs") + ", learned p' initial guess",
-                   "training": {"re_h": [t["re_h"] for t in train], "snapshots_total": sum(t["snapshots"] for t in train),
+        "config": {"workload": (workload_name(args.n, kind) if kind == "bfs" else
+                                f"cavity3d_{args.n} lid-driven cavity, Re={re_eval:g}, SOU, the mixed form with the "
+                                f"p' solve to 1e-3") + ", learned p' initial guess",
+                   "form": form,
+                   "training": {"re": [t["re"] for t in train], "snapshots_total": sum(t["snapshots"] for t in train),
                                 "epochs_per_run": epochs, "runs": train, "seconds": round(t_train, 1)}},
         "plain": legs["plain"], "learned": legs["learned"],
         "learned_vs_plain_time": legs["learned"]["ms_per_step"] / legs["plain"]["ms_per_step"],
@@ -556,7 +580,8 @@ def main():
     ap.add_argument("--case", default="cubic", choices=["cubic", "distorted", "bfs"])
     ap.add_argument("--ttr", type=int, default=6000, help="max iterations of the time-to-1e-6 legs (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--learned", action="store_true", help="with --case bfs: train and measure the learned p' guess")
+    ap.add_argument("--learned", action="store_true",
+                    help="train and measure the learned p' guess (--case bfs: FP64 step; cubic: the mixed form at 1e-3)")
     ap.add_argument("--ensemble", type=int, default=0, help="run the batched-ensemble configuration with this many cases")
     args = ap.parse_args()
 
@@ -594,9 +619,9 @@ def main():
             dist.barrier()
 
     if args.learned:
-        if args.case != "bfs" or world > 1:
-            raise SystemExit("--learned runs with --case bfs on one GPU")
-        run_bfs_learned(args, local)
+        if args.case == "distorted" or world > 1:
+            raise SystemExit("--learned runs with --case bfs or cubic on one GPU")
+        run_learned(args, local)
         return
 
     warm = max(args.warmup, 3)

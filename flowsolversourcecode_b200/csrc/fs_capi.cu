@@ -410,7 +410,7 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
   if (status) {
     // a bounded device wait gave up: the iteration's results are not valid
     FS_CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int32_t), ctx->st));
-    ctx->err = "a bounded device wait (multigrid team barrier) timed out";
+    ctx->err = "a bounded device wait (multigrid team barrier or tensor-core completion) timed out";
     return FS_E_TIMEOUT;
   }
   fs_solver_stats_collect(ctx);

@@ -335,54 +335,187 @@ __device__ void stage_hm(int N, int W, const int32_t *__restrict__ cn, const flo
   for (int c = 0; c < 32; c++) arow[NN_H + q * 32 + c] = __float2bfloat16(acc[c]);
 }
 
-// ---------------------------------------------------------------- layer forward
-// Hout = Hin + relu([Hin, m] W + b); mask (training) = z > 0.  One 128-row tile per CTA.
+// ---------------------------------------------------------------- layer forward (tcgen05)
+// Hout = Hin + relu([Hin, m] W + b); mask (training) = z > 0.  One 128-row tile
+// per CTA on the 5th-generation tensor cores: the [h, m] tile (128 x 128) and
+// W^T (64 x 128) sit in shared memory in the K-major, no-swizzle canonical
+// layout of the UMMA descriptors (8-row x 16-byte core matrices: a K chunk of 8
+// every 128 bytes, an 8-row group every 2048 bytes), one thread issues the eight
+// K=16 steps of tcgen05.mma (M=128, N=64, BF16 x BF16 -> FP32) into a 64-column
+// TMEM accumulator, tcgen05.commit arrives on an mbarrier, and every warp reads
+// its 32 lanes x 32 columns back with tcgen05.ld for the epilogue.  The wait on
+// the mbarrier is bounded: on a timeout the CTA records it in *status, skips the
+// epilogue and still frees its TMEM.
+#define NN_TC_COLS 64            // TMEM columns of the accumulator (power of 2, >= 32)
+#define NN_TC_SPIN (1L << 22)    // polls of the MMA-completion mbarrier before giving up
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// byte offset of element (row, k) of a K-major canonical tile with 16 K chunks per row group
+__device__ __forceinline__ int canon_off(int row, int k) { return (row >> 3) * 2048 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2; }
+
+// UMMA shared-memory descriptor: K-major, SWIZZLE_NONE, LBO = 128 B (next K chunk),
+// SBO = 2048 B (next 8-row group), version 1
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(2048 >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+
+// instruction descriptor: D FP32, A and B BF16, both K-major, N = 64, M = 128
+constexpr uint32_t NN_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NN_H >> 3) << 17) |
+                              ((uint32_t)(NN_TM >> 4) << 24);
+
+__device__ __forceinline__ void pack8_store(unsigned char *dst, const float *v) {
+  uint4 u;
+  u.x = pack2(__float2bfloat16(v[0]), __float2bfloat16(v[1]));
+  u.y = pack2(__float2bfloat16(v[2]), __float2bfloat16(v[3]));
+  u.z = pack2(__float2bfloat16(v[4]), __float2bfloat16(v[5]));
+  u.w = pack2(__float2bfloat16(v[6]), __float2bfloat16(v[7]));
+  *(uint4 *)dst = u;
+}
+
+// stage the [h, m] tile (rows i0..i0+127) as bf16 in the canonical layout: m = sum_j w_ij h_j
+__device__ void stage_hm_canon(int N, int W, const int32_t *__restrict__ cn, const float *__restrict__ wgt,
+                               const float *__restrict__ H, long i0, unsigned char *A) {
+  const int rr = threadIdx.x >> 1, q = threadIdx.x & 1;
+  const long i = i0 + rr;
+  float hv[32], acc[32];
+#pragma unroll
+  for (int c = 0; c < 32; c++) { hv[c] = 0.f; acc[c] = 0.f; }
+  if (i < N) {
+    const float4 *hs = (const float4 *)(H + i * NN_H + q * 32);
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      float4 v = hs[c];
+      hv[4 * c] = v.x; hv[4 * c + 1] = v.y; hv[4 * c + 2] = v.z; hv[4 * c + 3] = v.w;
+    }
+    for (int j = 0; j < W; j++) {
+      int k = cn[(long)j * N + i];
+      if (k < 0) continue;
+      float w = wgt[(long)j * N + i];
+      const float4 *hk = (const float4 *)(H + (long)k * NN_H + q * 32);
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        float4 v = hk[c];
+        acc[4 * c] += w * v.x; acc[4 * c + 1] += w * v.y; acc[4 * c + 2] += w * v.z; acc[4 * c + 3] += w * v.w;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    pack8_store(A + canon_off(rr, q * 32 + 8 * c), hv + 8 * c);
+    pack8_store(A + canon_off(rr, NN_H + q * 32 + 8 * c), acc + 8 * c);
+  }
+}
+
 __global__ void __launch_bounds__(NN_THREADS) k_nn_layer_fwd(int N, int W, const int32_t *__restrict__ cn,
                                                              const float *__restrict__ wgt, const float *Hin,
                                                              const bf16 *__restrict__ wt, const float *__restrict__ bias,
-                                                             float *Hout, uint8_t *mask) {
+                                                             float *Hout, uint8_t *mask, int32_t *status) {
   extern __shared__ __align__(16) unsigned char smem[];
-  bf16 *A = (bf16 *)smem;                       // 128 x NN_APAD
-  bf16 *WT = A + NN_TM * NN_APAD;               // 64 x NN_WPAD
+  // tiles on a 128-byte boundary (the launch adds 128 bytes of slack)
+  unsigned char *A = smem + ((128u - (smem_u32(smem) & 127u)) & 127u);   // 128 x 128 bf16, canonical (32 KB)
+  unsigned char *WT = A + NN_TM * NN_K * 2;                              // 64 x 128 bf16, canonical (16 KB)
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long i0 = (long)blockIdx.x * NN_TM;
-  for (int q = threadIdx.x; q < NN_H * NN_K; q += blockDim.x) {
-    int n = q / NN_K, k = q - n * NN_K;
-    WT[n * NN_WPAD + k] = wt[q];
+  if (warp == 0) {   // TMEM accumulator: one warp allocates, the address lands in tbase
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tbase)),
+                 "r"(NN_TC_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  stage_hm(N, W, cn, wgt, Hin, i0, A);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int c = threadIdx.x; c < NN_H * (NN_K / 8); c += blockDim.x) {   // W^T, 16-byte chunks
+    const int n = c / (NN_K / 8), kc = c - n * (NN_K / 8);
+    *(uint4 *)(WT + (n >> 3) * 2048 + kc * 128 + (n & 7) * 16) = *(const uint4 *)(wt + n * NN_K + kc * 8);
+  }
+  stage_hm_canon(N, W, cn, wgt, Hin, i0, A);
+  // the tensor cores read shared memory through the async proxy
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  const int r0 = warp * 16;
-  float acc[8][4];
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tbase;
+  if (threadIdx.x == 0) {
+    const uint32_t a0 = smem_u32(A), b0 = smem_u32(WT);
 #pragma unroll
-  for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+    for (int kk = 0; kk < NN_K / 16; kk++) {
+      const uint64_t da = umma_desc(a0 + kk * 256), db = umma_desc(b0 + kk * 256);
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "setp.ne.b32 p, %4, 0;\n\t"
+          "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
+          "}\n" ::"r"(tmem),
+          "l"(da), "l"(db), "r"(NN_IDESC), "r"(kk) : "memory");
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar))
+                 : "memory");
+  }
+  // bounded wait for the accumulator (phase 0 of the mbarrier)
+  uint32_t done = 0;
+  for (long spin = 0; spin < NN_TC_SPIN && !done; spin++) {
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t"
+        "}\n"
+        : "=r"(done)
+        : "r"(smem_u32(&mbar)), "r"(0)
+        : "memory");
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!done) {
+    if (lane == 0) atomicExch(status, 1);
+  } else {
+    // warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows), columns 32 (w / 4) .. +31
+    const int rowq = warp & 3, colh = warp >> 2;
+    uint32_t v[32];
+    const uint32_t ta = tmem + ((uint32_t)(32 * rowq) << 16) + (uint32_t)(32 * colh);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(ta)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    const long i = i0 + 32 * rowq + lane;
+    if (i < N) {
+      const int c0 = 32 * colh;
+      const float4 *hin = (const float4 *)(Hin + i * NN_H + c0);
+      float4 *hout = (float4 *)(Hout + i * NN_H + c0);
+      uint32_t mb[8];
 #pragma unroll
-  for (int kk = 0; kk < NN_K / 16; kk++) {
-    const int k0 = kk * 16;
-    uint32_t a0 = ld2(A + (r0 + g) * NN_APAD + k0 + 2 * t);
-    uint32_t a1 = ld2(A + (r0 + g + 8) * NN_APAD + k0 + 2 * t);
-    uint32_t a2 = ld2(A + (r0 + g) * NN_APAD + k0 + 2 * t + 8);
-    uint32_t a3 = ld2(A + (r0 + g + 8) * NN_APAD + k0 + 2 * t + 8);
+      for (int c = 0; c < 8; c++) {
+        const float4 h = hin[c];
+        float z[4], o[4];
+        const float hh[4] = {h.x, h.y, h.z, h.w};
 #pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      const int n0 = nt * 8;
-      uint32_t b0 = ld2(WT + (n0 + g) * NN_WPAD + k0 + 2 * t);
-      uint32_t b1 = ld2(WT + (n0 + g) * NN_WPAD + k0 + 2 * t + 8);
-      mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
+        for (int e = 0; e < 4; e++) {
+          z[e] = __uint_as_float(v[4 * c + e]) + bias[c0 + 4 * c + e];
+          o[e] = hh[e] + (z[e] > 0.f ? z[e] : 0.f);
+        }
+        hout[c] = make_float4(o[0], o[1], o[2], o[3]);
+        mb[c] = (uint32_t)(z[0] > 0.f) | ((uint32_t)(z[1] > 0.f) << 8) | ((uint32_t)(z[2] > 0.f) << 16) |
+                ((uint32_t)(z[3] > 0.f) << 24);
+      }
+      if (mask) {
+        uint4 *m4 = (uint4 *)(mask + i * NN_H + c0);
+        m4[0] = make_uint4(mb[0], mb[1], mb[2], mb[3]);
+        m4[1] = make_uint4(mb[4], mb[5], mb[6], mb[7]);
+      }
     }
   }
-#pragma unroll
-  for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const int row = r0 + g + (e >= 2 ? 8 : 0), col = nt * 8 + 2 * t + (e & 1);
-      const long i = i0 + row;
-      if (i >= N) continue;
-      float z = acc[nt][e] + bias[col];
-      float rz = z > 0.f ? z : 0.f;
-      Hout[i * NN_H + col] = Hin[i * NN_H + col] + rz;
-      if (mask) mask[i * NN_H + col] = z > 0.f;
-    }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NN_TC_COLS) : "memory");
 }
 
 // ---------------------------------------------------------------- layer backward (a)
@@ -548,7 +681,7 @@ __global__ void k_nn_guess(int N, const float *y, const double *sumy, const doub
 }  // namespace
 
 // ================================================================ host
-static const size_t NN_SMEM_FWD = sizeof(bf16) * (NN_TM * NN_APAD + NN_H * NN_WPAD);
+static const size_t NN_SMEM_FWD = sizeof(bf16) * (NN_TM * NN_K + NN_H * NN_K) + 128;   // canonical tiles + alignment slack
 static const size_t NN_SMEM_BWD = sizeof(bf16) * (NN_TM * NN_APAD + NN_TM * NN_DPAD + NN_K * NN_DPAD);
 static const int NN_PSTRIDE = NN_K * NN_H + NN_H;
 
@@ -595,7 +728,7 @@ static int nn_forward(fs_ctx *ctx, const float *X, const float *wgt, bool train)
     k_nn_layer_fwd<<<tiles, NN_THREADS, NN_SMEM_FWD, ctx->st>>>(N, W, ctx->cn, wgt, hin,
                                                                  nn->wt + (size_t)l * NN_K * NN_H,
                                                                  nn->theta + NN_OFF_L(l) + NN_K * NN_H, hout,
-                                                                 train ? nn->mask[l + 1] : nullptr);
+                                                                 train ? nn->mask[l + 1] : nullptr, ctx->d_status);
     FS_LAUNCH_CHECK();
   }
   const float *hl = train ? nn->H[NN_L] : nn->H[NN_L & 1];
