@@ -29,11 +29,13 @@ Forms (same case, same initial state):
 b200 arm: `value` is device-timed (CUDA events on the solver's stream) with
 the state resident in HBM; `e2e` runs the fp64 steps through the C ABI
 fs_simple_iteration_host with the state in pinned host buffers, copies inside
-the timed region.  On one GPU the time to residual 1e-6 of the fp64 form,
-the fp64 form with the p' solve to 1e-3 (fp64_rrf), and both mixed forms
-follows, from the initial state, with each form's converged fields against
-the fp64 form's (at 128^3 about 3,300 outer iterations per form; `--ttr 0`
-skips it, `--ttr MAXIT` caps the iterations).  N>1
+the timed region.  On one GPU the time to residual 1e-6 follows, from the
+initial state, for the fp64 form, fp64 with the p' solves started from the
+least-squares combination of the 4 previous p' solutions (fp64_guess), fp64
+with the p' solve to 1e-3 (fp64_rrf), the mixed form at 1e-3 (mixed_rrf) and
+the same with the initial guess (mixed_rrf_guess), with each form's converged
+fields against the fp64 form's (at 128^3 about 3,300 outer iterations per
+form; `--ttr 0` skips it, `--ttr MAXIT` caps the iterations).  N>1
 (torchrun) runs one independent replica per GPU (the single-mesh path does not
 shard) and reports the aggregate over ranks with the max-over-ranks time.
 reference arm: the CPU restatement of the reference's loop with the
@@ -71,6 +73,13 @@ FORMS = {
     # (the distorted-mesh configuration names this smoother)
     "mixed_gs": dict(solver_mom="sor", solver_cont="amg32gs_bicgs", krylov_tol=1e-8, krylov_maxit=200,
                      batched_momentum=True),
+    # the mixed form at 1e-3 whose p' solves start from the least-squares
+    # combination of the 4 previous p' solutions (the learned network's guess
+    # joins that basis when it is trained and on)
+    "mixed_rrf_guess": dict(solver_mom="sor", solver_cont="amg32_bicgs", krylov_tol=1e-3, krylov_maxit=200,
+                            batched_momentum=True, pc_history=4),
+    # the plain FP64 form with the same initial guess (p' still to 1e-8)
+    "fp64_guess": dict(solver_mom="sor", solver_cont="amg_bicgs", krylov_tol=1e-8, krylov_maxit=200, pc_history=4),
 }
 REFERENCE_SOLVERS = dict(solver_mom="sor", solver_cont="bicgs", krylov_tol=1e-8, krylov_maxit=300)
 
@@ -696,15 +705,27 @@ def main():
         # converged fields of each against the fp64 form's, and the times
         # against both fp64 legs (same p' tolerance 1e-8, and 1e-3)
         _, case_f, _ = workload(args.n, "fp64_rrf", kind)
+        _, case_g, _ = workload(args.n, "mixed_rrf_guess", kind)
+        _, case_fg, _ = workload(args.n, "fp64_guess", kind)
         ttr, tf = {}, {}
-        for name, c in (("fp64", case), ("fp64_rrf", case_f), ("mixed", case_m), ("mixed_rrf", case_r)):
+        legs = (("fp64", case), ("fp64_guess", case_fg), ("fp64_rrf", case_f), ("mixed_rrf", case_r),
+                ("mixed_rrf_guess", case_g))
+        for name, c in legs:
             ttr[name], tf[name] = time_to_residual(Solver, mesh, c, local, args.ttr, init=init, keys=fkeys)
-        for name in ("fp64_rrf", "mixed", "mixed_rrf"):
+        for name, _ in legs[1:]:
             ttr[name]["time_vs_fp64"] = ttr[name]["seconds"] / ttr["fp64"]["seconds"]
             ttr[name]["field_rel_l2_vs_fp64"] = {
                 k: float(np.linalg.norm(tf[name][k] - tf["fp64"][k]) / max(np.linalg.norm(tf["fp64"][k]), 1e-300))
                 for k in fkeys}
-        ttr["mixed_rrf"]["time_vs_fp64_rrf"] = ttr["mixed_rrf"]["seconds"] / ttr["fp64_rrf"]["seconds"]
+        for name in ("mixed_rrf", "mixed_rrf_guess"):
+            ttr[name]["time_vs_fp64_rrf"] = ttr[name]["seconds"] / ttr["fp64_rrf"]["seconds"]
+        ttr["mixed_rrf_guess"]["time_vs_fp64_guess"] = ttr["mixed_rrf_guess"]["seconds"] / ttr["fp64_guess"]["seconds"]
+        ttr["forms"] = {"fp64": "the plain path (p' from zero to 1e-8)",
+                        "fp64_guess": "fp64 with the p' solves started from the least-squares combination of the "
+                                      "4 previous p' solutions",
+                        "fp64_rrf": "fp64 with the p' solves to 1e-3 (the reference's default rrFContinuity)",
+                        "mixed_rrf": "FP32 V-cycle + multi-RHS momentum, p' to 1e-3",
+                        "mixed_rrf_guess": "mixed_rrf with the least-squares initial guess of fp64_guess"}
         ttr["tolerance"] = "stop metric (NstopType 4, normalised residual) below 1e-6 from the initial state"
 
     if rank == 0:

@@ -91,6 +91,7 @@ class FsCase(C.Structure):
         ("sigma_t", C.c_double), ("energy_wall_function", C.c_int),
         ("patch_thermal", C.c_int * FS_MAX_PATCHES), ("patch_temperature", C.c_double * FS_MAX_PATCHES),
         ("patch_heat_flux", C.c_double * FS_MAX_PATCHES), ("patch_h_inf", C.c_double * FS_MAX_PATCHES),
+        ("pc_history", C.c_int),
     ]
 
 
@@ -146,6 +147,7 @@ PROTOTYPES = {
     "fs_solve_momentum": (C.c_int, [_V, C.c_int]),
     "fs_solve_continuity": (C.c_int, [_V]),
     "fs_solve_energy": (C.c_int, [_V]),
+    "fs_set_pc_history": (C.c_int, [_V, C.c_int]),
     "fs_simple_iteration": (C.c_int, [_V, C.POINTER(FsResiduals)]),
     "fs_simple_iteration_host": (C.c_int, [_V, _D, _D, _D, _D, _D, _D, _D, _D, _D, _D, C.POINTER(FsResiduals)]),
     "fs_assemble_momentum": (C.c_int, [_V, C.c_int]),

@@ -129,6 +129,9 @@ class Case:
     # (heat flux), "robin" (T_inf, h_inf), "statictemperature" (T), "stagnationtemperature"
     # (T0), "fullydevelopedenergy", "symmetry"; unnamed patches take the flow type's default
     thermal: dict = field(default_factory=dict)
+    # p' initial guess: least-squares combination of this many previous p'
+    # solutions (AMG-BiCGSTAB solvers; no reference counterpart, 0 = zero start)
+    pc_history: int = 0
 
     def struct(self, mesh: PolyMesh) -> L.FsCase:
         c = L.FsCase()
@@ -208,6 +211,7 @@ class Case:
         c.limit_temperature, c.temp_min, c.temp_max = int(self.limit_temperature), self.temp_min, self.temp_max
         c.sigma_t = self.sigma_t
         c.energy_wall_function = {"standard": 0, "scalable": 1, "automatic": 2}[self.energy_wall_function]
+        c.pc_history = int(self.pc_history)
         for s, name in enumerate(mesh.patch_names):
             spec = self.thermal.get(name, ("default",))
             c.patch_thermal[s] = L.TBC[spec[0]]

@@ -156,7 +156,7 @@ static void free_all(fs_ctx *c) {
                   c->red, c->redi, c->resblk, c->d_iters, c->d_status,
                   c->cposP, c->cnP, c->ncfP, c->acP, c->bcP, c->anbP, c->dphiP,
                   c->ac3, c->bc3, c->ac3P, c->bc3P, c->x3P, c->gm, c->d_bset, c->flow, c->bdir,
-                  c->bpcoefc, c->bgd, c->bp0, c->d_patch};
+                  c->bpcoefc, c->bgd, c->bp0, c->d_patch, c->hist};
   for (void *p : ptrs) if (p) cudaFree(p);
 }
 
@@ -228,6 +228,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   if (B) cudaMemcpyAsync(ctx->d_bset, ctx->h_bset.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice, ctx->st);
   if ((rc = fs_turb_create(ctx))) return fail(rc);
   if ((rc = fs_energy_create(ctx))) { std::string e = ctx->err; fprintf(stderr, "fs_create: %s\n", e.c_str()); return fail(rc); }
+  if ((rc = fs_set_pc_history(ctx, ctx->cfg.pc_history))) { ctx->err = "pc_history must be 0..7"; return fail(rc); }
   // boundary values from the patches (setBoundaryConditions): wall / inlet velocities
   std::vector<double> hb(3 * B, 0.);
   for (size_t b = 0; b < B; b++) {
@@ -338,15 +339,42 @@ int fs_solve_momentum(fs_ctx *ctx, int comp) {
 }
 
 // the p' solve, with the learned initial guess when one is enabled
+// the p' solve with its initial-guess basis: the previous p' solutions kept
+// by fs_set_pc_history (newest first) and the network's guess
 static int pc_solve(fs_ctx *ctx) {
   const double *x0 = nullptr;
   int rc = fs_nn_before_pc(ctx, &x0);
   if (rc) return rc;
-  ctx->pc_guess = x0;
+  const size_t N = ctx->N;
+  ctx->pc_nguess = 0;
+  for (int q = 0; q < ctx->hist_cnt && ctx->pc_nguess < FS_GUESS_MAX - 1; q++) {
+    const int h = (ctx->hist_next - 1 - q + ctx->hist_cap) % ctx->hist_cap;
+    ctx->pc_guess[ctx->pc_nguess++] = ctx->hist + (size_t)h * N;
+  }
+  ctx->pc_nn = x0 != nullptr;
+  if (x0) ctx->pc_guess[ctx->pc_nguess++] = x0;
   rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
-  ctx->pc_guess = nullptr;
+  ctx->pc_nguess = 0;
+  ctx->pc_nn = false;
   if (rc) return rc;
+  if (ctx->hist_cap > 0) {
+    FS_CK(cudaMemcpyAsync(ctx->hist + (size_t)ctx->hist_next * N, ctx->dphi, sizeof(double) * N,
+                          cudaMemcpyDeviceToDevice, ctx->st));
+    ctx->hist_next = (ctx->hist_next + 1) % ctx->hist_cap;
+    ctx->hist_cnt = std::min(ctx->hist_cnt + 1, ctx->hist_cap);
+  }
   return fs_nn_after_pc(ctx);
+}
+
+int fs_set_pc_history(fs_ctx *ctx, int m) {
+  if (!ctx || m < 0 || m > FS_GUESS_MAX - 1) return FS_E_ARG;
+  cudaSetDevice(ctx->dev);
+  if (ctx->hist) { FS_CK(cudaStreamSynchronize(ctx->st)); cudaFree(ctx->hist); ctx->hist = nullptr; }
+  ctx->hist_cap = ctx->hist_cnt = ctx->hist_next = 0;
+  if (m == 0) return FS_OK;
+  FS_CK(cudaMalloc(&ctx->hist, sizeof(double) * (size_t)m * ctx->N));
+  ctx->hist_cap = m;
+  return FS_OK;
 }
 
 int fs_solve_energy(fs_ctx *ctx) {

@@ -69,6 +69,7 @@ struct fs_ilu;     // D-ILU level schedule (fs_solvers.cu)
 
 #define FS_NEQ 9        // equations with residual slots: NF 1..9
 #define FS_NLEVELS 7    // unsteady time levels: u v w p k epsilon T
+#define FS_GUESS_MAX 8  // vectors of the p' initial-guess fit (history + the network's guess)
 #define FS_NITERS 16     // int32 iteration-count slots (NF - 1 indexed)
 
 struct fs_ctx {
@@ -156,7 +157,14 @@ struct fs_ctx {
   fs_ilu *ilu = nullptr;
   // learned initial guess of the p' solve (nullptr: zero guess)
   fs_nn *nn = nullptr;
-  const double *pc_guess = nullptr;   // set around the p' solve only
+  // initial-guess basis of the p' solve (set around it only): previous p'
+  // solutions, then the network's guess
+  const double *pc_guess[FS_GUESS_MAX] = {};
+  int pc_nguess = 0;
+  bool pc_nn = false;   // the last basis vector is the network's guess
+  // previous p' solutions kept for the guess (fs_set_pc_history): ring of hist_cap vectors of N
+  double *hist = nullptr;
+  int hist_cap = 0, hist_cnt = 0, hist_next = 0;
 
   // timing
   cudaEvent_t tev[2] = {};                 // fs_timer_start / fs_timer_stop

@@ -40,6 +40,7 @@ namespace cg = cooperative_groups;
 #define FS_MG_SMALL 2048
 #define FS_MG_DIRECT 160   // largest coarsest level inverted densely (n^2 doubles in shared memory)
 #define FS_MG_MAXLEV 16
+#define FS_SUMK (FS_GUESS_MAX * (FS_GUESS_MAX + 1) / 2 + FS_GUESS_MAX + 1)   // sums of the guess fit
 // preconditioner V-cycle: Jacobi weight and coarse-correction factor
 // (over-correction compensates the energy of piecewise-constant prolongation)
 #ifndef FS_MG_OMEGA
@@ -141,6 +142,22 @@ struct Sync {
     for (int q = threadIdx.x; q < G; q += blockDim.x) { s0 += part[(2 * buf) * G + q]; s1 += part[(2 * buf + 1) * G + q]; }
     o0 = bsum(s0); o1 = bsum(s1);
     buf = (buf + 1) % 3;
+  }
+  // grid-deterministic sums of K <= FS_SUMK values, in the partial slots after
+  // the three buffers of sum2 (every CTA gets the same results)
+  __device__ void sumK(const double *in, double *out, int K) {
+    const int G = gridDim.x;
+    double *pk = part + 6L * G;
+    for (int k = 0; k < K; k++) {
+      const double b = bsum(in[k]);
+      if (threadIdx.x == 0) pk[(long)k * G + blockIdx.x] = b;
+    }
+    grid.sync();
+    for (int k = 0; k < K; k++) {
+      double t = 0.;
+      for (int q = threadIdx.x; q < G; q += blockDim.x) t += pk[(long)k * G + q];
+      out[k] = bsum(t);
+    }
   }
 };
 
@@ -913,7 +930,9 @@ struct AmgKArgs {
   double *part;
   int32_t *iters;
   double *diag;
-  const double *x0;   // initial guess (nullptr: zero)
+  const double *xs[FS_GUESS_MAX];   // initial-guess basis: previous p' solutions, the network's guess
+  int nx;             // vectors in xs (0: zero start)
+  int32_t *fit;       // [0]: k_guess_fit found a guess (device)
   int32_t *nncnt;     // [fallbacks, uses] of the initial guess, or nullptr
   unsigned *teambar;  // team barrier words of the V-cycle (zeroed before the launch)
   int32_t *status;    // [0] team-barrier timeout flag
@@ -945,6 +964,112 @@ __device__ void apply_prec(Sync &S, const AmgKArgs<R> &a, const double *in, doub
   gen = C.gen;
 }
 
+// mean of the right-hand side of a pure-Neumann system (every row sums to
+// zero), else 0; the same grid-deterministic sums in every kernel that calls it
+template <class R>
+__device__ double rhs_mean(Sync &S, const AmgKArgs<R> &a) {
+  const int N = a.N;
+  const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long)gridDim.x * blockDim.x;
+  double nonsing = 0., bsum = 0.;
+  for (long i = t0; i < N; i += nt) {
+    double rs = a.ac[i];
+    for (int j = 0; j < a.W; j++)
+      if (a.cn[(long)j * N + i] >= 0) rs += a.anb[(long)j * N + i];
+    nonsing += fabs(rs) > 1e-9 * fabs(a.ac[i]) ? 1. : 0.;
+    bsum += a.bc[i];
+  }
+  double n_nonsing, b_total;
+  S.sum2(nonsing, bsum, n_nonsing, b_total);
+  return n_nonsing == 0. ? b_total / N : 0.;
+}
+
+// The initial guess of k_amg_bicgstab, one cooperative launch before it: the
+// combination x = sum_j c_j x_j of the basis vectors (previous p' solutions,
+// the network's guess) that minimises |b - A x|, least squares over their
+// span, so |b - A x| <= |b|.  The normal equations (Gram matrix of the A x_j)
+// are solved by every CTA alike from grid-deterministic sums, by a Cholesky
+// factorisation with a relative diagonal shift.  x goes to a.x and fit[0] = 1;
+// a failed factorisation leaves fit[0] = 0 (the solve starts from zero).
+template <class R>
+__global__ void __launch_bounds__(FS_COOP_BLOCK, 1) k_guess_fit(AmgKArgs<R> a) {
+  Sync S(a.part);
+  const int N = a.N, nx = a.nx;
+  const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long)gridDim.x * blockDim.x;
+  const double bmean = rhs_mean(S, a);
+  double c[FS_GUESS_MAX];
+  for (int j = 0; j < FS_GUESS_MAX; j++) c[j] = 0.;
+  bool fell_back = false;
+  {
+    // Gram matrix G_jk = (A x_j).(A x_k) (upper triangle), g_j = (A x_j).b, |b|^2
+    double acc[FS_SUMK];
+    const int ng = nx * (nx + 1) / 2;
+    for (int k = 0; k < ng + nx + 1; k++) acc[k] = 0.;
+    for (long i = t0; i < N; i += nt) {
+      double y[FS_GUESS_MAX];
+      for (int j = 0; j < nx; j++) {
+        const double *xj = a.xs[j];
+        double t = 0.;
+        t = t + a.ac[i] * xj[i];
+        y[j] = ell_acc<8, false>(t, a.N, a.W, a.cn, a.anb, i, [&](int k) { return xj[k]; });
+      }
+      const double b1 = a.bc[i] - bmean;
+      int q = 0;
+      for (int j = 0; j < nx; j++)
+        for (int k = j; k < nx; k++) acc[q++] += y[j] * y[k];
+      for (int j = 0; j < nx; j++) acc[ng + j] += y[j] * b1;
+      acc[ng + nx] += b1 * b1;
+    }
+    double tot[FS_SUMK];
+    S.sumK(acc, tot, ng + nx + 1);
+    // Cholesky of G + 1e-12 max(diag) I, then the two triangular solves (row-major L)
+    double L[FS_GUESS_MAX * FS_GUESS_MAX];
+    double dmax = 0.;
+    {
+      int q = 0;
+      for (int j = 0; j < nx; j++)
+        for (int k = j; k < nx; k++) { L[k * FS_GUESS_MAX + j] = tot[q]; if (k == j) dmax = fmax(dmax, tot[q]); q++; }
+    }
+    bool ok = dmax > 0. && isfinite(dmax);
+    for (int j = 0; j < nx && ok; j++) {
+      double d = L[j * FS_GUESS_MAX + j] + 1e-12 * dmax;
+      for (int k = 0; k < j; k++) d -= L[j * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
+      if (!(d > 1e-14 * dmax)) { ok = false; break; }
+      d = sqrt(d);
+      L[j * FS_GUESS_MAX + j] = d;
+      for (int r = j + 1; r < nx; r++) {
+        double v = L[r * FS_GUESS_MAX + j];
+        for (int k = 0; k < j; k++) v -= L[r * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
+        L[r * FS_GUESS_MAX + j] = v / d;
+      }
+    }
+    if (ok) {
+      double z[FS_GUESS_MAX];
+      for (int j = 0; j < nx; j++) {
+        double v = tot[ng + j];
+        for (int k = 0; k < j; k++) v -= L[j * FS_GUESS_MAX + k] * z[k];
+        z[j] = v / L[j * FS_GUESS_MAX + j];
+      }
+      for (int j = nx - 1; j >= 0; j--) {
+        double v = z[j];
+        for (int k = j + 1; k < nx; k++) v -= L[k * FS_GUESS_MAX + j] * c[k];
+        c[j] = v / L[j * FS_GUESS_MAX + j];
+      }
+      for (int j = 0; j < nx; j++) if (!isfinite(c[j])) ok = false;
+    }
+    if (!ok) for (int j = 0; j < nx; j++) c[j] = 0.;
+    fell_back = !ok;
+    for (long i = t0; i < N; i += nt) {
+      double xi = 0.;
+      for (int j = 0; j < nx; j++) xi += c[j] * a.xs[j][i];
+      a.x[i] = xi;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.fit[0] = fell_back ? 0 : 1;
+    if (a.nncnt) { a.nncnt[1] += 1; if (fell_back) a.nncnt[0] += 1; }
+  }
+}
+
 // right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle:
 // MODE 0 run(), 2 run_gs() (multicolour Gauss-Seidel smoothing), 1 the fused
 // V-cycle (one pre- and one post-sweep, dense coarsest level), whose first
@@ -956,59 +1081,34 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   const int N = a.N;
   Scope g; g.grid = true;
   const long t0 = g.tid0(), nt = g.nth();
-  // start from the initial guess scaled by the c that minimises |b - c A x0|
-  // (c = (A x0 . b) / (A x0 . A x0), so |r0| <= |b|), or from zero.  A guess
-  // with c not finite or zero falls back to the zero start (same decision in
-  // every CTA: the sums are grid-deterministic).  Whether guesses pay is decided
-  // on iteration counts by the host policy (fs_nn.cu).
+  // start from the initial guess k_guess_fit left in x (the least-squares
+  // combination of the basis vectors; fit[0] = 0 when it fell back), or from zero.
   // A pure-Neumann system (every row sums to zero: the closed-cavity p'
   // system) is singular.  Its right-hand side is taken with its mean removed,
   // the part a solution can match; otherwise, once the outer iterations have
   // converged the mean (rounding in the mass fluxes) is no longer small
   // against |b|, the tolerance cannot be met and the iterates drift.  The
   // constant null vector is left to the caller (pressure reference cell).
-  double nonsing = 0., bsum = 0.;
+  const double bmean = rhs_mean(S, a);
+  const bool has_x = a.nx > 0 && a.fit[0] != 0;
+  double l0 = 0., l1 = 0.;
   for (long i = t0; i < N; i += nt) {
-    double rs = a.ac[i];
-    for (int j = 0; j < a.W; j++)
-      if (a.cn[(long)j * N + i] >= 0) rs += a.anb[(long)j * N + i];
-    nonsing += fabs(rs) > 1e-9 * fabs(a.ac[i]) ? 1. : 0.;
-    bsum += a.bc[i];
-  }
-  double n_nonsing, b_total;
-  S.sum2(nonsing, bsum, n_nonsing, b_total);
-  const double bmean = n_nonsing == 0. ? b_total / N : 0.;
-  double l0 = 0., l1 = 0., l2 = 0.;
-  for (long i = t0; i < N; i += 2 * nt) {
-    const long i2 = i + nt;
-    const bool h2 = i2 < N;
-    double q1 = 0., q2 = 0.;
-    if (a.x0) row_ax2(a, i, i2, h2, a.x0, q1, q2);
     const double b1 = a.bc[i] - bmean;
-    a.r[i] = q1;
-    l0 += q1 * b1; l1 += q1 * q1; l2 += b1 * b1;
-    if (h2) {
-      const double b2 = a.bc[i2] - bmean;
-      a.r[i2] = q2;
-      l0 += q2 * b2; l1 += q2 * q2; l2 += b2 * b2;
+    double ri = b1;
+    if (has_x) {
+      double t = 0.;
+      t = t + a.ac[i] * a.x[i];
+      t = ell_acc<8, false>(t, a.N, a.W, a.cn, a.anb, i, [&](int k) { return a.x[k]; });
+      ri = ri - t;
+    } else {
+      a.x[i] = 0.;
     }
-  }
-  double qb, qq, bb, dum;
-  S.sum2(l0, l1, qb, qq);
-  S.sum2(l2, 0., bb, dum);
-  double c = (a.x0 && qq > 0.) ? qb / qq : 0.;
-  if (!isfinite(c)) c = 0.;
-  const bool fell_back = a.x0 && c == 0.;
-  l0 = 0.;
-  for (long i = t0; i < N; i += nt) {
-    const double xi = a.x0 ? c * a.x0[i] : 0.;
-    const double ri = (a.bc[i] - bmean) - c * a.r[i];
-    a.x[i] = xi; a.r[i] = ri; a.r0[i] = ri; a.p[i] = 0.; a.v[i] = 0.;
+    a.r[i] = ri; a.r0[i] = ri; a.p[i] = 0.; a.v[i] = 0.;
     l0 += ri * ri;
+    l1 += b1 * b1;
   }
-  double rr;
-  S.sum2(l0, 0., rr, dum);
-  if (a.nncnt && a.x0 && blockIdx.x == 0 && threadIdx.x == 0) { a.nncnt[1] += 1; if (fell_back) a.nncnt[0] += 1; }
+  double rr, bb, dum;
+  S.sum2(l0, l1, rr, bb);
   double normb = sqrt(bb), rho = 1., alpha = 1., omega = 1.;
   int k = 0;
   double resn = sqrt(rr);
@@ -1450,7 +1550,7 @@ int fs_mg_build(fs_ctx *ctx) {
   FS_CK(cudaMemcpy(M->lev64, L64.data(), sizeof(LevelDev<double>) * M->nlev, cudaMemcpyHostToDevice));
   FS_CK(cudaMalloc(&M->lev32, sizeof(LevelDev<float>) * M->nlev));
   FS_CK(cudaMemcpy(M->lev32, L32.data(), sizeof(LevelDev<float>) * M->nlev, cudaMemcpyHostToDevice));
-  FS_CK(cudaMalloc(&M->red, sizeof(double) * 6 * FS_RED_BLOCKS));
+  FS_CK(cudaMalloc(&M->red, sizeof(double) * (6 + FS_SUMK) * FS_RED_BLOCKS));
   // preconditioner: stop at the first level small enough for the dense inverse
   M->lc = M->nlev - 1;
   for (int q = 0; q < M->nlev; q++)
@@ -1566,8 +1666,11 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     a.pre = std::max(1, ctx->cfg.mg_pre); a.post = std::max(1, ctx->cfg.mg_pre);
     a.maxit = ctx->cfg.krylov_maxit; a.tol = ctx->cfg.krylov_tol; a.part = M->red;
     a.iters = ctx->d_iters + (nf - 1); a.diag = ctx->resblk + RB_DIAG;
-    a.x0 = nf == FS_VAR_PC ? ctx->pc_guess : nullptr;
-    a.nncnt = fs_nn_counters(ctx);
+    a.nx = 0;
+    if (nf == FS_VAR_PC)
+      for (int j = 0; j < ctx->pc_nguess && j < FS_GUESS_MAX; j++) a.xs[a.nx++] = ctx->pc_guess[j];
+    a.fit = ctx->d_status + 6;
+    a.nncnt = ctx->pc_nn ? fs_nn_counters(ctx) : nullptr;   // the network's guess is in the basis
     a.teambar = (unsigned *)(ctx->d_status + 4);
     a.status = ctx->d_status;
     a.team_extra = ctx->test_wait_extra;
@@ -1579,6 +1682,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     fill(a);
     a.lev = M->lev64;
     void *args[] = {&a};
+    if (a.nx > 0) FS_CK(fs_coop_launch((const void *)k_guess_fit<double>, G, fs_coop_block(ctx), args, ctx->st));
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<double, 1> : (const void *)k_amg_bicgstab<double, 0>,
                          G, fs_coop_block(ctx), args, ctx->st));
@@ -1587,6 +1691,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     fill(a);
     a.lev = M->lev32;
     void *args[] = {&a};
+    if (a.nx > 0) FS_CK(fs_coop_launch((const void *)k_guess_fit<float>, G, fs_coop_block(ctx), args, ctx->st));
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     // the FP32 cycle runs the unfused V-cycle: measured at 128^3, its fused
     // form was 1.5 % slower (the FP64 cycle gains 5 % from fusion)

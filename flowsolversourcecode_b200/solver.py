@@ -289,6 +289,11 @@ class Solver:
         of 256 (1..4; 0: the default 1024), one CTA per SM."""
         self._chk(self.lib.fs_set_launch_shape(self.ctx, shape), "fs_set_launch_shape")
 
+    def set_pc_history(self, m: int):
+        """Start each AMG-BiCGSTAB p' solve from the least-squares combination of
+        the m (0..7) previous p' solutions (and the learned guess when on)."""
+        self._chk(self.lib.fs_set_pc_history(self.ctx, int(m)), "fs_set_pc_history")
+
     # ------------------------------------------------------------ learned p' guess
     def nn_create(self, snapshot_capacity: int = 0, seed: int = 0):
         """Network for the learned p' initial guess, with room for

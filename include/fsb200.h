@@ -276,6 +276,9 @@ typedef struct fs_case {
   double patch_temperature[FS_MAX_PATCHES];  /* wall, inlet static or stagnation temperature; TinfinityRobin */
   double patch_heat_flux[FS_MAX_PATCHES];    /* HeatFlux of von Neumann walls */
   double patch_h_inf[FS_MAX_PATCHES];        /* HinfinityRobin */
+  /* p' initial guess from the pc_history (0..7) previous p' solutions
+   * (fs_set_pc_history; no reference counterpart); 0 = zero start */
+  int    pc_history;
 } fs_case;
 
 /* TransientScheme values (AssembleTheTransientTerm.for:52,124,199,290). */
@@ -363,6 +366,13 @@ const char *fs_last_error(const fs_ctx *ctx);
 int fs_solve_momentum(fs_ctx *ctx, int comp);
 /* SolveContinuity (ContinuityEquation/SolveContinuityEquation.for:4). */
 int fs_solve_continuity(fs_ctx *ctx);
+/* p' initial guess from the m (0..7) previous p' solutions (no reference
+ * counterpart: the reference starts p' from zero).  The AMG-BiCGSTAB solvers
+ * start from the combination of those solutions (and of the learned guess,
+ * when it is on) that minimises |b - A x0| -- least squares over their span,
+ * so the starting residual never exceeds |b| -- and iterate to the same
+ * tolerance.  m = 0 (the default) starts from zero; other solvers ignore it. */
+int fs_set_pc_history(fs_ctx *ctx, int m);
 /* SolveEnergy, EnergyEquation='temperature' (Energy/SelectEnergyEquationToSolve.for:4,
  * SolveTemperatureEquation.for:4): one temperature solve on the current
  * velocities and mass fluxes.  FS_E_ARG when the case has energy = 0. */

@@ -239,3 +239,26 @@ def test_ensemble_member_converges_to_oracle():
             err = _field_err(ens.solvers[q], o, k)
             assert err <= 1e-8, (q, k, err)
     ens.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,cap", [("fp64", 0.85), ("mixed_rrf", 0.7)])
+def test_pc_history_guess(form, cap):
+    """The p' solves started from the least-squares combination of the 4
+    previous p' solutions take fewer iterations and leave the outer iterates
+    where the zero start leaves them (to the p' tolerance)."""
+    import bench
+    from flowsolversourcecode_b200.solver import Solver
+    out = {}
+    for m in (0, 4):
+        mesh, case, _ = bench.workload(24, form)
+        case.pc_history = m
+        s = Solver(mesh, case)
+        its = sum(s.simple_iteration()["lin_iters"][3] for _ in range(60))
+        out[m] = (its, {k: s.get(k) for k in ("u", "v", "w", "p")})
+        s.close()
+    assert out[4][0] <= cap * out[0][0], (out[0][0], out[4][0])
+    tol = 1e-9 if form == "fp64" else 1e-4
+    for k in ("u", "v", "w", "p"):
+        a, b = out[4][1][k], out[0][1][k]
+        assert np.linalg.norm(a - b) <= tol * np.linalg.norm(b), k
