@@ -435,16 +435,19 @@ def time_to_residual(Solver, mesh, case, local: int, maxit: int, tol: float = 1e
 def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
     """64 independent cavities of uneven size (edges U{32..96}, lid U[0.5, 2],
     Re log-uniform 100..2000, seed 0): FP64 outer iterations, FP32 AMG
-    preconditioner, multi-RHS momentum, launch shape autotuned per case, every
-    `--steps` iterations of all of a GPU's cases one CUDA graph.  Cases shard
-    over ranks by size (longest processing time first); no collective on the
-    data path.  Metric: cell-iterations per second, whole job."""
+    preconditioner, p' to `--ensemble-tol` (default 1e-3, the reference's
+    rrFContinuity; the time-to-residual legs show the outer iterations and
+    converged fields unchanged by it) from the least-squares combination of the
+    4 previous p' solutions, multi-RHS momentum, launch shape autotuned per
+    case, every `--steps` iterations of all of a GPU's cases one CUDA graph.
+    Cases shard over ranks by size (longest processing time first); no
+    collective on the data path.  Metric: cell-iterations per second, whole job."""
     import numpy as np
     from flowsolversourcecode_b200 import ensemble as E
     specs = E.make_specs(args.ensemble, seed=0)
     mine = E.shard([s.cells for s in specs], world)[rank]
     t0 = time.time()
-    cases = E.build_cases([specs[q] for q in mine])
+    cases = E.build_cases([specs[q] for q in mine], krylov_tol=args.ensemble_tol)
     ens = E.Ensemble(cases, device=local)
     del cases
     t_setup = time.time() - t0
@@ -474,7 +477,9 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
                        "cases": len(specs), "cells_total": sum(s.cells for s in specs), "cases_rank0": len(mine),
                        "cells_rank0": cells, "graph": f"{args.steps} iterations of all rank cases per CUDA graph, "
                                                       f"{launches} launches",
-                       "solvers": "momentum multi-RHS SOR; p' FP64 BiCGSTAB + FP32 AMG V-cycle to 1e-8",
+                       "solvers": f"momentum multi-RHS SOR; p' FP64 BiCGSTAB + FP32 AMG V-cycle to "
+                                  f"{args.ensemble_tol:g}, started from the least-squares combination of the 4 "
+                                  f"previous p' solutions",
                        "launch_shapes_rank0": {str(k): shapes.count(k) for k in sorted(set(shapes))},
                        "setup_s_rank0": round(t_setup, 1),
                        "source_rank0": {"min": float(np.min(out["source"][:, -1])),
@@ -592,6 +597,8 @@ def main():
     ap.add_argument("--learned", action="store_true",
                     help="train and measure the learned p' guess (--case bfs: FP64 step; cubic: the mixed form at 1e-3)")
     ap.add_argument("--ensemble", type=int, default=0, help="run the batched-ensemble configuration with this many cases")
+    ap.add_argument("--ensemble-tol", type=float, default=1e-3,
+                    help="p' tolerance of the ensemble cases (1e-3: the reference's default rrFContinuity)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

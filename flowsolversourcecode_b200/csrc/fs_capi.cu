@@ -340,17 +340,18 @@ int fs_solve_momentum(fs_ctx *ctx, int comp) {
 
 // the p' solve, with the learned initial guess when one is enabled
 // the p' solve with its initial-guess basis: the previous p' solutions kept
-// by fs_set_pc_history (newest first) and the network's guess
+// by fs_set_pc_history (slot 0 the newest) and the network's guess.  The
+// slots shift by device copies after each solve, so the pointers stay fixed and
+// the solve can be captured into a graph (the network's guess, which needs host
+// bookkeeping, is left out there).
 static int pc_solve(fs_ctx *ctx) {
   const double *x0 = nullptr;
-  int rc = fs_nn_before_pc(ctx, &x0);
-  if (rc) return rc;
+  int rc;
+  if (!ctx->graph_mode && (rc = fs_nn_before_pc(ctx, &x0))) return rc;
   const size_t N = ctx->N;
   ctx->pc_nguess = 0;
-  for (int q = 0; q < ctx->hist_cnt && ctx->pc_nguess < FS_GUESS_MAX - 1; q++) {
-    const int h = (ctx->hist_next - 1 - q + ctx->hist_cap) % ctx->hist_cap;
-    ctx->pc_guess[ctx->pc_nguess++] = ctx->hist + (size_t)h * N;
-  }
+  for (int q = 0; q < ctx->hist_cnt && ctx->pc_nguess < FS_GUESS_MAX - 1; q++)
+    ctx->pc_guess[ctx->pc_nguess++] = ctx->hist + (size_t)q * N;
   ctx->pc_nn = x0 != nullptr;
   if (x0) ctx->pc_guess[ctx->pc_nguess++] = x0;
   rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
@@ -358,19 +359,20 @@ static int pc_solve(fs_ctx *ctx) {
   ctx->pc_nn = false;
   if (rc) return rc;
   if (ctx->hist_cap > 0) {
-    FS_CK(cudaMemcpyAsync(ctx->hist + (size_t)ctx->hist_next * N, ctx->dphi, sizeof(double) * N,
-                          cudaMemcpyDeviceToDevice, ctx->st));
-    ctx->hist_next = (ctx->hist_next + 1) % ctx->hist_cap;
+    for (int q = std::min(ctx->hist_cnt, ctx->hist_cap - 1); q >= 1; q--)
+      FS_CK(cudaMemcpyAsync(ctx->hist + (size_t)q * N, ctx->hist + (size_t)(q - 1) * N, sizeof(double) * N,
+                            cudaMemcpyDeviceToDevice, ctx->st));
+    FS_CK(cudaMemcpyAsync(ctx->hist, ctx->dphi, sizeof(double) * N, cudaMemcpyDeviceToDevice, ctx->st));
     ctx->hist_cnt = std::min(ctx->hist_cnt + 1, ctx->hist_cap);
   }
-  return fs_nn_after_pc(ctx);
+  return ctx->graph_mode ? FS_OK : fs_nn_after_pc(ctx);
 }
 
 int fs_set_pc_history(fs_ctx *ctx, int m) {
   if (!ctx || m < 0 || m > FS_GUESS_MAX - 1) return FS_E_ARG;
   cudaSetDevice(ctx->dev);
   if (ctx->hist) { FS_CK(cudaStreamSynchronize(ctx->st)); cudaFree(ctx->hist); ctx->hist = nullptr; }
-  ctx->hist_cap = ctx->hist_cnt = ctx->hist_next = 0;
+  ctx->hist_cap = ctx->hist_cnt = 0;
   if (m == 0) return FS_OK;
   FS_CK(cudaMalloc(&ctx->hist, sizeof(double) * (size_t)m * ctx->N));
   ctx->hist_cap = m;
@@ -498,12 +500,7 @@ static int iteration_body(fs_ctx *ctx) {
   FS_TIMING(cudaEventRecord(ctx->ev[1], ctx->st));
   if ((rc = fs_continuity_assemble(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[2], ctx->st));
-  // the learned guess needs host-side bookkeeping per solve: not in captured graphs
-  if (ctx->graph_mode)
-    rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
-  else
-    rc = pc_solve(ctx);
-  if (rc) return rc;
+  if ((rc = pc_solve(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[3], ctx->st));
   if ((rc = fs_continuity_correct(ctx))) return rc;
   // CalculateEffectsOfTurbulence (MainProgram.for:275-277), SolveEnergy (:281)
@@ -743,7 +740,8 @@ int fs_sync(fs_ctx *ctx) {
 // pinned host memory by copies inside the graph.  source_out[q*T + t] is the
 // stop metric of case q after its t-th run iteration (T = iters*launches),
 // pc_iters_out (optional) the p' iterations, ms_out the device time of the
-// launches.  The learned guess is not used inside the graph.
+// launches.  The p' history guess runs inside the graph; the learned network's
+// guess (host bookkeeping per solve) does not.
 int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
                     float *ms_out) {
   if (!cs || n < 1 || iters < 1 || launches < 1 || !source_out) return FS_E_ARG;
@@ -752,15 +750,16 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
     if (!cs[q] || cs[q]->dev != c0->dev) return FS_E_ARG;
   cudaSetDevice(c0->dev);
   fs_ctx *ctx = c0;  // FS_CK reports into the first context
-  // one ordinary iteration per case builds hierarchies, colourings and grids
+  // ordinary iterations per case build hierarchies, colourings and grids
   // (nothing may allocate during capture); the HR start must already be passed
+  // and the p' history full (the captured solves take a fixed basis)
   for (int q = 0; q < n; q++) {
     fs_ctx *c = cs[q];
     do {
       fs_residuals r;
       int rc = fs_simple_iteration(c, &r);
       if (rc) { if (c != ctx) ctx->err = c->err; return rc; }
-    } while (c->nIter < c->cfg.niter_start_hr);
+    } while (c->nIter < c->cfg.niter_start_hr || c->hist_cnt < c->hist_cap);
   }
   const size_t slot = RB_SIZE + FS_NITERS / 2;  // residual block, then the int32 iteration counts
   double *h = nullptr;

@@ -162,9 +162,10 @@ struct fs_ctx {
   const double *pc_guess[FS_GUESS_MAX] = {};
   int pc_nguess = 0;
   bool pc_nn = false;   // the last basis vector is the network's guess
-  // previous p' solutions kept for the guess (fs_set_pc_history): ring of hist_cap vectors of N
+  // previous p' solutions kept for the guess (fs_set_pc_history): hist_cap
+  // slots of N, slot 0 the newest, hist_cnt filled
   double *hist = nullptr;
-  int hist_cap = 0, hist_cnt = 0, hist_next = 0;
+  int hist_cap = 0, hist_cnt = 0;
 
   // timing
   cudaEvent_t tev[2] = {};                 // fs_timer_start / fs_timer_stop

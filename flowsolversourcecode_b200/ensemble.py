@@ -66,9 +66,11 @@ def shard(sizes, world: int) -> list[list[int]]:
 
 def build_case(spec: CaseSpec, **kw):
     """Mesh and Case of one ensemble member: the 3-D cavity with SOU deferred
-    correction from iteration 1, the FP32 AMG preconditioner and the multi-RHS
-    momentum solve unless overridden."""
+    correction from iteration 1, the FP32 AMG preconditioner, p' solves started
+    from the least-squares combination of the 4 previous p' solutions, and the
+    multi-RHS momentum solve unless overridden."""
     kw.setdefault("solver_cont", "amg32_bicgs")
+    kw.setdefault("pc_history", 4)
     kw.setdefault("krylov_tol", 1e-8)
     kw.setdefault("krylov_maxit", 200)
     kw.setdefault("batched_momentum", True)

@@ -39,7 +39,9 @@ def test_graph_run_matches_ordinary_iterations():
     ens.close()
     for q, (m, c) in enumerate(cases):
         s = Solver(m, c)
-        ref = [s.simple_iteration()["source"] for _ in range(7)][1:]   # the run starts after one ordinary iteration
+        # the run starts after ordinary iterations that pass the HR start and fill the p' history
+        warm = max(1, c.niter_start_hr, c.pc_history)
+        ref = [s.simple_iteration()["source"] for _ in range(warm + 6)][warm:]
         s.close()
         assert np.allclose(out["source"][q], ref, rtol=1e-12, atol=0), (q, out["source"][q], ref)
     assert out["ms"] > 0 and out["cell_iters_per_s"] > 0
