@@ -91,7 +91,7 @@ class FsCase(C.Structure):
         ("sigma_t", C.c_double), ("energy_wall_function", C.c_int),
         ("patch_thermal", C.c_int * FS_MAX_PATCHES), ("patch_temperature", C.c_double * FS_MAX_PATCHES),
         ("patch_heat_flux", C.c_double * FS_MAX_PATCHES), ("patch_h_inf", C.c_double * FS_MAX_PATCHES),
-        ("pc_history", C.c_int),
+        ("pc_history", C.c_int), ("pc_refresh", C.c_int),
     ]
 
 

@@ -132,6 +132,8 @@ class Case:
     # p' initial guess: least-squares combination of this many previous p'
     # solutions (AMG-BiCGSTAB solvers; no reference counterpart, 0 = zero start)
     pc_history: int = 0
+    # rebuild the AMG preconditioner's coarse levels every this many p' solves (1: every solve)
+    pc_refresh: int = 1
 
     def struct(self, mesh: PolyMesh) -> L.FsCase:
         c = L.FsCase()
@@ -212,6 +214,7 @@ class Case:
         c.sigma_t = self.sigma_t
         c.energy_wall_function = {"standard": 0, "scalable": 1, "automatic": 2}[self.energy_wall_function]
         c.pc_history = int(self.pc_history)
+        c.pc_refresh = int(self.pc_refresh)
         for s, name in enumerate(mesh.patch_names):
             spec = self.thermal.get(name, ("default",))
             c.patch_thermal[s] = L.TBC[spec[0]]

@@ -98,6 +98,10 @@ struct fs_mg_dev {
   LevelDev<float> *lev32 = nullptr;
   double *red = nullptr;                // partial sums
   int per_sm = 0;                       // co-resident CTAs per SM of the multigrid kernels
+  // preconditioner reuse (pc_refresh): the system and precision the coarse
+  // levels and the dense inverse were last built for, and the solves since
+  int built_nf = 0, age = 0;
+  bool built_f32 = false;
 };
 
 namespace {
@@ -1637,6 +1641,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
   const int G = std::min(ctx->num_sms * fs_coop_per_sm(ctx, M->per_sm), FS_RED_BLOCKS);
   if (solver == FS_SOLVER_AMG) {
     if ((rc = mg_coarse_matrices(ctx, M->nlev - 1, false))) return rc;
+    M->built_nf = 0;
     MgSolveArgs a{};
     a.lev = M->lev64; a.nlev = M->nlev; a.type = ctx->cfg.mg_cycle; a.pre = ctx->cfg.mg_pre; a.post = ctx->cfg.mg_post;
     a.maxcycles = ctx->cfg.mg_max_cycles; a.b0 = ctx->bc; a.x0 = ctx->dphi; a.r0 = M->r[0];
@@ -1648,10 +1653,28 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][1], ctx->st)));
     return FS_OK;
   }
-  if ((rc = mg_coarse_matrices(ctx, M->lc, f32))) return rc;
+  // coarse levels and the dense coarsest inverse: rebuilt every pc_refresh solves
+  // of the same system (1: every solve); in between the V-cycle keeps them and
+  // only level 0 (the current system) is new -- a fixed preconditioner within
+  // each solve, which still runs to its tolerance
+  const int refresh = std::max(1, ctx->cfg.pc_refresh);
+  const bool reuse = M->built_nf == nf && M->built_f32 == f32 && M->age + 1 < refresh;
+  if (reuse) {
+    M->age++;
+    if (f32) {   // level 0 in FP32 from the current system
+      const long n = M->n[0], nw = (long)M->w[0] * M->n[0];
+      k_to_f32<<<fs_grid(n), FS_BLOCK, 0, ctx->st>>>(n, M->ac[0], M->acf[0]);
+      FS_LAUNCH_CHECK();
+      k_to_f32<<<fs_grid(nw), FS_BLOCK, 0, ctx->st>>>(nw, M->anb[0], M->anbf[0]);
+      FS_LAUNCH_CHECK();
+    }
+  } else {
+    if ((rc = mg_coarse_matrices(ctx, M->lc, f32))) return rc;
+    M->built_nf = nf; M->built_f32 = f32; M->age = 0;
+  }
   // team-barrier counters of the V-cycle start at zero for every launch
   FS_CK(cudaMemsetAsync(ctx->d_status + 4, 0, sizeof(int32_t) * 2, ctx->st));
-  if (M->direct) {
+  if (M->direct && !reuse) {
     const int n = M->n[M->lc];
     k_mg_dense_inverse<<<1, 1024, sizeof(double) * ((size_t)n * n + 5 * (size_t)n), ctx->st>>>(
         n, M->nnb[M->lc], M->nbr[M->lc], M->ac[M->lc], M->anb[M->lc], M->sinv);

@@ -279,6 +279,11 @@ typedef struct fs_case {
   /* p' initial guess from the pc_history (0..7) previous p' solutions
    * (fs_set_pc_history; no reference counterpart); 0 = zero start */
   int    pc_history;
+  /* AMG-BiCGSTAB preconditioner reuse: the coarse matrices and the dense
+   * coarsest inverse are rebuilt every pc_refresh solves of the same system
+   * and kept in between (level 0 is always the current system); 0 or 1 =
+   * every solve.  No reference counterpart. */
+  int    pc_refresh;
 } fs_case;
 
 /* TransientScheme values (AssembleTheTransientTerm.for:52,124,199,290). */
