@@ -75,9 +75,10 @@ FORMS = {
                      batched_momentum=True),
     # the mixed form at 1e-3 whose p' solves start from the least-squares
     # combination of the 4 previous p' solutions (the learned network's guess
-    # joins that basis when it is trained and on)
+    # joins that basis when it is trained and on); the preconditioner's coarse
+    # levels are rebuilt every 4th p' solve
     "mixed_rrf_guess": dict(solver_mom="sor", solver_cont="amg32_bicgs", krylov_tol=1e-3, krylov_maxit=200,
-                            batched_momentum=True, pc_history=4),
+                            batched_momentum=True, pc_history=4, pc_refresh=4),
     # the plain FP64 form with the same initial guess (p' still to 1e-8)
     "fp64_guess": dict(solver_mom="sor", solver_cont="amg_bicgs", krylov_tol=1e-8, krylov_maxit=200, pc_history=4),
 }
@@ -732,7 +733,8 @@ def main():
                                       "4 previous p' solutions",
                         "fp64_rrf": "fp64 with the p' solves to 1e-3 (the reference's default rrFContinuity)",
                         "mixed_rrf": "FP32 V-cycle + multi-RHS momentum, p' to 1e-3",
-                        "mixed_rrf_guess": "mixed_rrf with the least-squares initial guess of fp64_guess"}
+                        "mixed_rrf_guess": "mixed_rrf with the least-squares initial guess of fp64_guess, "
+                                           "coarse preconditioner levels rebuilt every 4th p' solve"}
         ttr["tolerance"] = "stop metric (NstopType 4, normalised residual) below 1e-6 from the initial state"
 
     if rank == 0:

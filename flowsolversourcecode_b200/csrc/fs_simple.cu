@@ -89,12 +89,41 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_GG0_MINB) k_gg0(GradJob J, int N,
   }
 }
 
+// Shared-memory staging of the correction pass (FS_GG_STAGE > 0, off by
+// default): a CTA first copies phi and the previous gradient of the cells
+// [first - FS_GG_STAGE, last + FS_GG_STAGE] with coalesced loads, and the
+// face loop takes a neighbour inside that window from shared memory (on a
+// structured ordering the +-1 and +-nx neighbours), the others from global
+// memory.  The values are the same either way.  Measured at 128^3 with a
+// window of +-128 cells: the assembly phases took 3.73 ms per iteration
+// against 3.42 ms unstaged -- the neighbours it serves are L1/L2 hits
+// already, and the window load, the barrier and the extra spills cost more.
+#ifndef FS_GG_STAGE
+#define FS_GG_STAGE 0
+#endif
+constexpr int GG_WIN = FS_BLOCK + 2 * FS_GG_STAGE;   // staged cells per CTA
+
 // correction pass of StandardGreenGaussFaceCorrection1 (:98-172)
 template <int NF>
 __global__ void __launch_bounds__(FS_BLOCK, FS_GG_MINB) k_gg_corr(GradJob J, int N, int F, int B,
     const int32_t *__restrict__ ncf, const int32_t *__restrict__ slot, const int32_t *__restrict__ cn,
     const double *__restrict__ gf, const double *__restrict__ sf, const double *__restrict__ dfp,
     const double *__restrict__ bsf, const double *__restrict__ vol) {
+#if FS_GG_STAGE > 0
+  extern __shared__ double stg[];   // [q][phi, gx, gy, gz][GG_WIN]
+  const long w0 = (long)blockIdx.x * blockDim.x - FS_GG_STAGE;
+#pragma unroll
+  for (int q = 0; q < NF; q++)
+    for (int t = threadIdx.x; t < GG_WIN; t += blockDim.x) {
+      const long c = w0 + t;
+      const bool in = c >= 0 && c < N;
+      stg[(4 * q + 0) * GG_WIN + t] = in ? J.phi[q][c] : 0.;
+      stg[(4 * q + 1) * GG_WIN + t] = in ? J.in[q][c] : 0.;
+      stg[(4 * q + 2) * GG_WIN + t] = in ? J.in[q][N + c] : 0.;
+      stg[(4 * q + 3) * GG_WIN + t] = in ? J.in[q][2L * N + c] : 0.;
+    }
+  __syncthreads();
+#endif
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   int nc = ncf[i];
@@ -114,10 +143,24 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_GG_MINB) k_gg_corr(GradJob J, int
       double sx = sf[f], sy = sf[F + f], sz = sf[2L * F + f];
       double dx = dfp[f], dy = dfp[F + f], dz = dfp[2L * F + f];
       bool nb = s & 1;
+#if FS_GG_STAGE > 0
+      const long lk = k - w0;
+      const bool sm = (unsigned long)lk < (unsigned long)GG_WIN;
+#endif
 #pragma unroll
       for (int q = 0; q < NF; q++) {
         const double *__restrict__ gi = J.in[q];
+#if FS_GG_STAGE > 0
+        double pk, gkx, gky, gkz;
+        if (sm) {
+          pk = stg[(4 * q + 0) * GG_WIN + lk]; gkx = stg[(4 * q + 1) * GG_WIN + lk];
+          gky = stg[(4 * q + 2) * GG_WIN + lk]; gkz = stg[(4 * q + 3) * GG_WIN + lk];
+        } else {
+          pk = J.phi[q][k]; gkx = gi[k]; gky = gi[N + k]; gkz = gi[2L * N + k];
+        }
+#else
         double pk = J.phi[q][k], gkx = gi[k], gky = gi[N + k], gkz = gi[2L * N + k];
+#endif
         double po = nb ? pk : ps[q], pn = nb ? ps[q] : pk;
         double gox = nb ? gkx : gsx[q], gnx = nb ? gsx[q] : gkx;
         double goy = nb ? gky : gsy[q], gny = nb ? gsy[q] : gky;
@@ -891,10 +934,23 @@ __global__ void k_sum_inlet(InletRanges r, const double *bmdot, double *out) {
 // ======================================================================
 // host drivers
 // ======================================================================
+// dynamic shared memory of a k_gg_corr<nf> launch (the staged window)
+static size_t gg_smem(int nf) { return FS_GG_STAGE > 0 ? sizeof(double) * 4 * nf * GG_WIN : 0; }
+
 int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const *phi,
                     const double *const *bphi, double *const *g, double *const *bg,
                     const int *method, const int *niter) {
   const int N = ctx->N, F = ctx->F, B = ctx->B;
+  if (FS_GG_STAGE > 0) {   // windows above 48 KB: a per-function attribute, shared by every context
+    static bool attr = false;
+    if (!attr) {
+      const void *fns[4] = {(const void *)k_gg_corr<1>, (const void *)k_gg_corr<2>, (const void *)k_gg_corr<3>,
+                            (const void *)k_gg_corr<4>};
+      for (int q = 0; q < 4; q++)
+        FS_CK(cudaFuncSetAttribute(fns[q], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gg_smem(q + 1)));
+      attr = true;
+    }
+  }
   int passes[4], maxp = 0;
   for (int q = 0; q < nfld; q++) {
     passes[q] = 1 + (method[q] == 2 ? niter[q] : 0);
@@ -921,8 +977,8 @@ int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const 
       k_gg0<NFV><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf, ctx->sf,  \
                                                        ctx->bsf, ctx->vol);                                         \
     else                                                                                                            \
-      k_gg_corr<NFV><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn, ctx->gf,       \
-                                                           ctx->sf, ctx->dfp, ctx->bsf, ctx->vol);                  \
+      k_gg_corr<NFV><<<fs_grid(N), FS_BLOCK, gg_smem(NFV), ctx->st>>>(J, N, F, B, ctx->ncf, ctx->slot, ctx->cn,     \
+                                                                     ctx->gf, ctx->sf, ctx->dfp, ctx->bsf, ctx->vol); \
   } while (0)
     switch (n) {
     case 1: FS_GG_LAUNCH(1); break;
