@@ -505,9 +505,11 @@ def run_learned(args, local: int, n_re: int = 8, per_re: int = 50, epochs: int =
     """The learned p' guess.  Step (`--case bfs`): snapshots from plain FP64
     runs at `n_re` Reynolds numbers Re_H ~ U[2000, 8000] (splitmix64 seed 1),
     evaluated at Re_H = 5000.  Cavity (`--case cubic`): snapshots from runs of
-    the mixed form with the p' solve to 1e-3 at Re log-uniform on [300, 3000]
-    (seed 1), evaluated at Re = 1000 in the same form -- the mixed + learned
-    form.  `per_re` snapshots per run (the p' solves of the first per_re+1
+    the mixed form with the p' solve to 1e-3 and the history guess at Re
+    log-uniform on [300, 3000] (seed 1), evaluated at Re = 1000 in the same
+    form, whose p' initial guess is the least-squares combination of the 4
+    previous p' solutions: the learned leg adds the network's guess to that
+    basis, so the comparison shows what the network adds on top of it.  `per_re` snapshots per run (the p' solves of the first per_re+1
     SIMPLE iterations from the initial state); the network is trained on each
     run's snapshots in turn (parameters carried over); the evaluation case runs
     from the initial state with and without the guess, `--steps` iterations
@@ -522,7 +524,7 @@ def run_learned(args, local: int, n_re: int = 8, per_re: int = 50, epochs: int =
     else:
         n_re = 4
         res = [float(np.exp(np.log(300.0) + float(x) * (np.log(3000.0) - np.log(300.0)))) for x in uniform01(1, n_re)]
-        re_eval, form = 1000.0, "mixed_rrf"
+        re_eval, form = 1000.0, "mixed_rrf_guess"
     theta, train = None, []
     t0 = time.time()
     for q, re in enumerate(res):
@@ -574,7 +576,7 @@ def run_learned(args, local: int, n_re: int = 8, per_re: int = 50, epochs: int =
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": (workload_name(args.n, kind) if kind == "bfs" else
                                 f"cavity3d_{args.n} lid-driven cavity, Re={re_eval:g}, SOU, the mixed form with the "
-                                f"p' solve to 1e-3") + ", learned p' initial guess",
+                                f"p' solve to 1e-3 and the history guess") + ", learned p' initial guess",
                    "form": form,
                    "training": {"re": [t["re"] for t in train], "snapshots_total": sum(t["snapshots"] for t in train),
                                 "epochs_per_run": epochs, "runs": train, "seconds": round(t_train, 1)}},
