@@ -133,8 +133,8 @@ __device__ double bsum(double v) {
 struct Sync {
   cg::grid_group grid;
   double *part;
-  int buf;
-  __device__ Sync(double *p) : grid(cg::this_grid()), part(p), buf(0) {}
+  int buf, buf3;
+  __device__ Sync(double *p) : grid(cg::this_grid()), part(p), buf(0), buf3(0) {}
   __device__ void all() { grid.sync(); }
   // grid-deterministic sum of two values (every CTA gets the same result)
   __device__ void sum2(double a0, double a1, double &o0, double &o1) {
@@ -162,6 +162,19 @@ struct Sync {
       for (int q = threadIdx.x; q < G; q += blockDim.x) t += pk[(long)k * G + q];
       out[k] = bsum(t);
     }
+  }
+  // grid-deterministic sums of three values, in three rotating buffers of
+  // their own after the sumK slots
+  __device__ void sum3(double a0, double a1, double a2, double &o0, double &o1, double &o2) {
+    const int G = gridDim.x;
+    double *pb = part + (6L + FS_SUMK + 3L * buf3) * G;
+    const double b0 = bsum(a0), b1 = bsum(a1), b2 = bsum(a2);
+    if (threadIdx.x == 0) { pb[blockIdx.x] = b0; pb[G + blockIdx.x] = b1; pb[2 * G + blockIdx.x] = b2; }
+    grid.sync();
+    double s0 = 0., s1 = 0., s2 = 0.;
+    for (int q = threadIdx.x; q < G; q += blockDim.x) { s0 += pb[q]; s1 += pb[G + q]; s2 += pb[2 * G + q]; }
+    o0 = bsum(s0); o1 = bsum(s1); o2 = bsum(s2);
+    buf3 = (buf3 + 1) % 3;
   }
 };
 
@@ -655,10 +668,13 @@ struct PCycle {
   //     FS_PC_FUSE_DOWN levels; a warp takes a chunk of coarse rows, a lane
   //     two children, and each coarse row sums its children's residuals in
   //     ascending order through shuffles;
-  //   up: the sweep of a row of level l >= 1 scatters its new value, times
+  //   up: the sweep of a row of level l >= 2 scatters its new value, times
   //     alpha, to the row's children on level l-1 (the prolongation: every
   //     finer row has one parent, so no two writes meet), and the coarsest
-  //     level's dense solve does the same; level 0's sweep writes `out`.
+  //     level's dense solve does the same; level 1's sweep keeps its values
+  //     and level 0 gathers them through parent (prolong0); level 0's sweep
+  //     writes `out`.  (The restriction fused with the residual measured
+  //     slower than the two phases on every level, so FS_PC_FUSE_DOWN is 0.)
   // The caller has set x_0 = omega0 in / ac_0 and passed a grid barrier.
   __device__ void restrict_fused(int l, const double *__restrict__ in) {
     const LevelDev<R> L = lev[l], C = lev[l + 1];
@@ -783,6 +799,9 @@ struct PCycle {
         if (l == 0) {
           out[i] = (double)xn;
           if (h2) out[i2] = (double)xm;
+        } else if (gather_into(l)) {
+          L.r[i] = xn;
+          if (h2) L.r[i2] = xm;
         } else {
           scatter_children(L, xf, i, af * xn, 0, 1);
           if (h2) scatter_children(L, xf, i2, af * xm, 0, 1);
@@ -798,9 +817,27 @@ struct PCycle {
       if (act) {
         R xi = L.x[i], bi = L.b[i];
         R xn = xi + om(l) * (bi - L.ac[i] * xi - t) / L.ac[i];
-        scatter_children(L, xf, i, af * xn, q, G);
+        if (!gather_into(l)) scatter_children(L, xf, i, af * xn, q, G);
+        else if (q == 0) L.r[i] = xn;
       }
     });
+  }
+  // level 1's post-sweep leaves its result in its r, and level 0 gathers the
+  // correction through parent in a phase of its own (x_0 += alpha x_1[parent],
+  // the same sum the scatter forms): a coalesced pass over the fine rows
+  // instead of one read-modify-write per fine row in agglomerate order.  At
+  // 128^3 the extra grid barrier costs less than the scattered writes: the
+  // FP64 p' solve 2 % faster, and the FP32 one, which ran the unfused cycle
+  // before, 10 %.
+  __device__ __forceinline__ bool gather_into(int l) const { return l == 1 && lc >= 2; }
+  __device__ void prolong0() {
+    const LevelDev<R> L = lev[0];
+    const R *__restrict__ xc = lev[1].r;
+    Scope g;
+    g.grid = true;
+    enter(g);
+    const R a0 = al(0);
+    for (long i = g.tid0(); i < L.n; i += g.nth()) L.x[i] = L.x[i] + a0 * xc[L.parent[i]];
   }
   // the dense coarsest solve (CTA 0, warps on rows), scattered into level lc-1
   __device__ void coarsest_scatter() {
@@ -916,7 +953,10 @@ struct PCycle {
       else restrict_plain(l, in);
     }
     coarsest_scatter();
-    for (int l = lc - 1; l >= 0; l--) smooth_scatter(l, in, out);
+    for (int l = lc - 1; l >= 0; l--) {
+      if (l == 0 && gather_into(1)) prolong0();
+      smooth_scatter(l, in, out);
+    }
     enter(g);
   }
 };
@@ -1077,7 +1117,18 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, 1) k_guess_fit(AmgKArgs<R> a) {
 // right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle:
 // MODE 0 run(), 2 run_gs() (multicolour Gauss-Seidel smoothing), 1 the fused
 // V-cycle (one pre- and one post-sweep, dense coarsest level), whose first
-// sweep from zero, x_0 = omega0 in / ac_0, rides on the loops that form p and s
+// sweep from zero, x_0 = omega0 in / ac_0, rides on the loops that form p and s.
+// Four grid synchronisations per iteration besides the V-cycles': the sums
+// after v = A y and after s, the sums after t = A z, and the barrier after one
+// pass that updates x and r and forms the next p.  That pass needs beta
+// before |r|^2 and r0.r of the new r are summed; both come from the t-pass
+// sums instead: r0.r_new = r0.s - omega r0.t, and |s - omega t|^2 = |s|^2 -
+// omega t.s (omega = t.s / t.t), with |s|^2 summed fresh from s, so the
+// estimate's rounding is relative to |s|^2 of this iteration.  Only an
+// iteration whose estimate says it has converged (or the last one) sums |r|^2
+// and r0.r of the stored r instead, so the exit is always decided on a
+// residual summed from its vector, and a solve that has not really converged
+// continues with p formed in a separate pass.
 template <class R, int MODE>
 __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(AmgKArgs<R> a) {
   Sync S(a.part);
@@ -1085,6 +1136,9 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   const int N = a.N;
   Scope g; g.grid = true;
   const long t0 = g.tid0(), nt = g.nth();
+  R *__restrict__ x0v = a.lev[0].x;
+  const R *__restrict__ ac0 = a.lev[0].ac;
+  const R om0 = (R)FS_MG_OMEGA0;
   // start from the initial guess k_guess_fit left in x (the least-squares
   // combination of the basis vectors; fit[0] = 0 when it fell back), or from zero.
   // A pure-Neumann system (every row sums to zero: the closed-cavity p'
@@ -1095,7 +1149,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
   // constant null vector is left to the caller (pressure reference cell).
   const double bmean = rhs_mean(S, a);
   const bool has_x = a.nx > 0 && a.fit[0] != 0;
-  double l0 = 0., l1 = 0.;
+  double l0 = 0., l1 = 0., l2 = 0.;
   for (long i = t0; i < N; i += nt) {
     const double b1 = a.bc[i] - bmean;
     double ri = b1;
@@ -1107,34 +1161,39 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     } else {
       a.x[i] = 0.;
     }
-    a.r[i] = ri; a.r0[i] = ri; a.p[i] = 0.; a.v[i] = 0.;
+    // the first p is r (beta's factors are 1 and p = v = 0 before it)
+    a.r[i] = ri; a.r0[i] = ri; a.p[i] = ri; a.v[i] = 0.;
+    if (MODE == 1) x0v[i] = om0 * (R)ri / ac0[i];
     l0 += ri * ri;
     l1 += b1 * b1;
   }
   double rr, bb, dum;
   S.sum2(l0, l1, rr, bb);
-  double normb = sqrt(bb), rho = 1., alpha = 1., omega = 1.;
+  double normb = sqrt(bb), alpha = 1., omega = 1.;
   int k = 0;
   double resn = sqrt(rr);
-  R *__restrict__ x0v = a.lev[0].x;
-  const R *__restrict__ ac0 = a.lev[0].ac;
-  const R om0 = (R)FS_MG_OMEGA0;
-  // r0 . r of the next iteration, formed with the residual update (r = r0 at first)
-  double rho_next = rr;
+  // rho = r0 . r of the iteration; rho_next that of the next one, summed from
+  // the stored r when p still has to be formed (p_ready false)
+  double rho = rr, rho_next = rr;
+  bool p_ready = true;
+  if (!(rr != 0.) || !isfinite(rr)) p_ready = false;   // the loop's breakdown test takes it
   while (k < a.maxit && resn > a.tol * normb && normb > 0.) {
     k++;
-    const double rho1 = rho_next;
-    // breakdown (r0 . r vanished: r at round-off): keep x.  Every CTA holds the
-    // same sums, so every CTA takes the same branch.
-    if (!(rho1 != 0.) || !isfinite(rho1)) break;
-    double beta = (rho1 / rho) * (alpha / omega);
-    rho = rho1;
-    for (long i = t0; i < N; i += nt) {
-      const double pi = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
-      a.p[i] = pi;
-      if (MODE == 1) x0v[i] = om0 * (R)pi / ac0[i];
+    if (!p_ready) {
+      const double rho1 = rho_next;
+      // breakdown (r0 . r vanished: r at round-off): keep x.  Every CTA holds
+      // the same sums, so every CTA takes the same branch.
+      if (!(rho1 != 0.) || !isfinite(rho1)) break;
+      const double beta = (rho1 / rho) * (alpha / omega);
+      rho = rho1;
+      for (long i = t0; i < N; i += nt) {
+        const double pi = a.r[i] + beta * (a.p[i] - omega * a.v[i]);
+        a.p[i] = pi;
+        if (MODE == 1) x0v[i] = om0 * (R)pi / ac0[i];
+      }
+      S.all();
     }
-    S.all();
+    p_ready = false;
     apply_prec<R, MODE>(S, a, a.p, a.y, gen);                       // y = M^-1 p
     l0 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
@@ -1149,32 +1208,33 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
     S.sum2(l0, 0., rv, dum);
     if (!(rv != 0.) || !isfinite(rho / rv)) break;
     alpha = rho / rv;
-    l0 = 0.;
+    l0 = 0.; l1 = 0.;
     for (long i = t0; i < N; i += nt) {
       const double si = a.r[i] - alpha * a.v[i];
       a.s[i] = si;
       l0 += si * si;
+      l1 += a.r0[i] * si;
       if (MODE == 1) x0v[i] = om0 * (R)si / ac0[i];
     }
-    double ss;
-    S.sum2(l0, 0., ss, dum);
+    double ss, r0s;
+    S.sum2(l0, l1, ss, r0s);
     if (sqrt(ss) <= a.tol * normb) {
       for (long i = t0; i < N; i += nt) a.x[i] = a.x[i] + alpha * a.y[i];
       resn = sqrt(ss);
       break;
     }
     apply_prec<R, MODE>(S, a, a.s, a.z, gen);                       // z = M^-1 s
-    l0 = 0.; l1 = 0.;
+    l0 = 0.; l1 = 0.; l2 = 0.;
     for (long i = t0; i < N; i += 2 * nt) {
       const long i2 = i + nt;
       const bool h2 = i2 < N;
       double t1, t2;
       row_ax2(a, i, i2, h2, a.z, t1, t2);
-      a.t[i] = t1; l0 += t1 * a.s[i]; l1 += t1 * t1;
-      if (h2) { a.t[i2] = t2; l0 += t2 * a.s[i2]; l1 += t2 * t2; }
+      a.t[i] = t1; l0 += t1 * a.s[i]; l1 += t1 * t1; l2 += a.r0[i] * t1;
+      if (h2) { a.t[i2] = t2; l0 += t2 * a.s[i2]; l1 += t2 * t2; l2 += a.r0[i2] * t2; }
     }
-    double ts, tt;
-    S.sum2(l0, l1, ts, tt);
+    double ts, tt, r0t;
+    S.sum3(l0, l1, l2, ts, tt, r0t);
     if (!(tt > 0.) || !(ts != 0.) || !isfinite(ts / tt)) {
       // t = A z vanished or is orthogonal to s: take the half step and stop
       for (long i = t0; i < N; i += nt) a.x[i] = a.x[i] + alpha * a.y[i];
@@ -1182,17 +1242,36 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB) k_amg_bicgstab(Amg
       break;
     }
     omega = ts / tt;
-    l0 = 0.; l1 = 0.;
-    for (long i = t0; i < N; i += nt) {
-      a.x[i] = a.x[i] + alpha * a.y[i] + omega * a.z[i];
-      double ri = a.s[i] - omega * a.t[i];
-      a.r[i] = ri;
-      l0 += ri * ri;
-      l1 += a.r0[i] * ri;
+    const double rn_est = fmax(ss - omega * ts, 0.);
+    const double rho_est = r0s - omega * r0t;
+    if (k < a.maxit && sqrt(rn_est) > a.tol * normb && rho_est != 0. && isfinite(rho_est)) {
+      // x and r of this iteration and p of the next in one pass
+      const double beta = (rho_est / rho) * (alpha / omega);
+      rho = rho_est;
+      for (long i = t0; i < N; i += nt) {
+        a.x[i] = a.x[i] + alpha * a.y[i] + omega * a.z[i];
+        const double ri = a.s[i] - omega * a.t[i];
+        a.r[i] = ri;
+        const double pi = ri + beta * (a.p[i] - omega * a.v[i]);
+        a.p[i] = pi;
+        if (MODE == 1) x0v[i] = om0 * (R)pi / ac0[i];
+      }
+      S.all();
+      resn = sqrt(rn_est);
+      p_ready = true;
+    } else {
+      l0 = 0.; l1 = 0.;
+      for (long i = t0; i < N; i += nt) {
+        a.x[i] = a.x[i] + alpha * a.y[i] + omega * a.z[i];
+        const double ri = a.s[i] - omega * a.t[i];
+        a.r[i] = ri;
+        l0 += ri * ri;
+        l1 += a.r0[i] * ri;
+      }
+      double rn;
+      S.sum2(l0, l1, rn, rho_next);
+      resn = sqrt(rn);
     }
-    double rn;
-    S.sum2(l0, l1, rn, rho_next);
-    resn = sqrt(rn);
   }
   S.all();
   for (long i = t0; i < N; i += nt) a.dphi[i] = a.x[i];
@@ -1554,7 +1633,7 @@ int fs_mg_build(fs_ctx *ctx) {
   FS_CK(cudaMemcpy(M->lev64, L64.data(), sizeof(LevelDev<double>) * M->nlev, cudaMemcpyHostToDevice));
   FS_CK(cudaMalloc(&M->lev32, sizeof(LevelDev<float>) * M->nlev));
   FS_CK(cudaMemcpy(M->lev32, L32.data(), sizeof(LevelDev<float>) * M->nlev, cudaMemcpyHostToDevice));
-  FS_CK(cudaMalloc(&M->red, sizeof(double) * (6 + FS_SUMK) * FS_RED_BLOCKS));
+  FS_CK(cudaMalloc(&M->red, sizeof(double) * (6 + FS_SUMK + 9) * FS_RED_BLOCKS));
   // preconditioner: stop at the first level small enough for the dense inverse
   M->lc = M->nlev - 1;
   for (int q = 0; q < M->nlev; q++)
@@ -1575,7 +1654,7 @@ int fs_mg_build(fs_ctx *ctx) {
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (void *)k_amg_bicgstab<double, 0>, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, (void *)k_amg_bicgstab<float, 0>, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, (void *)k_amg_bicgstab<double, 1>, FS_COOP_BLOCK, 0));
-  c2 = c;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c2, (void *)k_amg_bicgstab<float, 1>, FS_COOP_BLOCK, 0));
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c3, (void *)k_amg_bicgstab<float, 2>, FS_COOP_BLOCK, 0));
   int per = std::min(std::min(a, std::min(b, c)), std::min(std::min(b2, c2), c3));
   if (per < 1) { ctx->err = "multigrid kernels do not fit on an SM"; return FS_E_CUDA; }
@@ -1716,9 +1795,8 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     void *args[] = {&a};
     if (a.nx > 0) FS_CK(fs_coop_launch((const void *)k_guess_fit<float>, G, fs_coop_block(ctx), args, ctx->st));
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
-    // the FP32 cycle runs the unfused V-cycle: measured at 128^3, its fused
-    // form was 1.5 % slower (the FP64 cycle gains 5 % from fusion)
-    const void *k = gs ? (const void *)k_amg_bicgstab<float, 2> : (const void *)k_amg_bicgstab<float, 0>;
+    const void *k = gs ? (const void *)k_amg_bicgstab<float, 2>
+                    : fused ? (const void *)k_amg_bicgstab<float, 1> : (const void *)k_amg_bicgstab<float, 0>;
     FS_CK(fs_coop_launch(k, G, fs_coop_block(ctx), args, ctx->st));
   }
   FS_LAUNCH_CHECK();
