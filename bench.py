@@ -440,7 +440,10 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
     rrFContinuity; the time-to-residual legs show the outer iterations and
     converged fields unchanged by it) from the least-squares combination of the
     4 previous p' solutions, multi-RHS momentum, launch shape autotuned per
-    case, every `--steps` iterations of all of a GPU's cases one CUDA graph.
+    case, every `--steps` iterations of all of a GPU's cases one CUDA graph,
+    timed in two forms -- cases in sequence, and the p' solves of all cases in
+    one cooperative launch with a CTA group per case -- and the faster one
+    reported (both rates in `config`).
     Cases shard over ranks by size (longest processing time first); no
     collective on the data path.  Metric: cell-iterations per second, whole job."""
     import numpy as np
@@ -453,13 +456,19 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
     del cases
     t_setup = time.time() - t0
     shapes = ens.autotune(shapes=(1, 2, 3, 4), iters=1)
-    warm = ens.run(iters=args.steps, launches=1)           # graph capture + one untimed launch
-    if dist is not None:
-        dist.barrier()
     launches = max(1, args.warmup)
-    with Clocks(local) as clk:
-        out = ens.run(iters=args.steps, launches=launches)
-    ms = reduce_max(out["ms"], dist, f"cuda:{local}")
+    # both graph forms, each after one untimed launch of its own graph: cases in
+    # sequence, and the p' solves of all cases in one launch (a CTA group each)
+    timed = {}
+    for batched in (False, True):
+        ens.run(iters=args.steps, launches=1, batched=batched)
+        if dist is not None:
+            dist.barrier()
+        with Clocks(local) as clk:
+            out = ens.run(iters=args.steps, launches=launches, batched=batched)
+        timed[batched] = (reduce_max(out["ms"], dist, f"cuda:{local}"), out, clk.summary())
+    best = min(timed, key=lambda b: timed[b][0])
+    ms, out, clocks = timed[best]
     cells = sum(ens.cells)
     total_cells = cells
     if dist is not None:
@@ -482,10 +491,15 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
                                   f"{args.ensemble_tol:g}, started from the least-squares combination of the 4 "
                                   f"previous p' solutions",
                        "launch_shapes_rank0": {str(k): shapes.count(k) for k in sorted(set(shapes))},
+                       "pc_launch": "one cooperative launch for the p' solves of all cases, a CTA group each"
+                                    if best else "the cases' p' solves one after another",
+                       "cell_iter_per_s_by_form": {
+                           "sequential": total_cells * T / (timed[False][0] * 1e-3),
+                           "batched_pc": total_cells * T / (timed[True][0] * 1e-3)},
                        "setup_s_rank0": round(t_setup, 1),
                        "source_rank0": {"min": float(np.min(out["source"][:, -1])),
                                         "max": float(np.max(out["source"][:, -1]))}},
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     ens.close()

@@ -338,13 +338,13 @@ int fs_solve_momentum(fs_ctx *ctx, int comp) {
   return fs_linear_solve(ctx, comp + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom);
 }
 
-// the p' solve, with the learned initial guess when one is enabled
 // the p' solve with its initial-guess basis: the previous p' solutions kept
 // by fs_set_pc_history (slot 0 the newest) and the network's guess.  The
 // slots shift by device copies after each solve, so the pointers stay fixed and
 // the solve can be captured into a graph (the network's guess, which needs host
-// bookkeeping, is left out there).
-static int pc_solve(fs_ctx *ctx) {
+// bookkeeping, is left out there).  With pc_defer the Krylov launch itself is
+// left to fs_pc_batch_launch between pc_solve_pre and pc_solve_post.
+static int pc_solve_pre(fs_ctx *ctx) {
   const double *x0 = nullptr;
   int rc;
   if (!ctx->graph_mode && (rc = fs_nn_before_pc(ctx, &x0))) return rc;
@@ -357,7 +357,13 @@ static int pc_solve(fs_ctx *ctx) {
   rc = fs_linear_solve(ctx, FS_VAR_PC, ctx->pc, ctx->cfg.rrf_cont, ctx->cfg.itmax_cont, ctx->cfg.solver_cont);
   ctx->pc_nguess = 0;
   ctx->pc_nn = false;
-  if (rc) return rc;
+  return rc;
+}
+
+static int pc_solve_post(fs_ctx *ctx) {
+  int rc;
+  if (ctx->pc_defer && (rc = fs_linear_solve_finish(ctx, FS_VAR_PC, ctx->pc))) return rc;
+  const size_t N = ctx->N;
   if (ctx->hist_cap > 0) {
     for (int q = std::min(ctx->hist_cnt, ctx->hist_cap - 1); q >= 1; q--)
       FS_CK(cudaMemcpyAsync(ctx->hist + (size_t)q * N, ctx->hist + (size_t)(q - 1) * N, sizeof(double) * N,
@@ -366,6 +372,12 @@ static int pc_solve(fs_ctx *ctx) {
     ctx->hist_cnt = std::min(ctx->hist_cnt + 1, ctx->hist_cap);
   }
   return ctx->graph_mode ? FS_OK : fs_nn_after_pc(ctx);
+}
+
+static int pc_solve(fs_ctx *ctx) {
+  int rc = pc_solve_pre(ctx);
+  if (rc) return rc;
+  return pc_solve_post(ctx);
 }
 
 int fs_set_pc_history(fs_ctx *ctx, int m) {
@@ -483,7 +495,8 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
 }
 
 // one SIMPLE outer iteration enqueued on the context stream (MainProgram.for:257-325)
-static int iteration_body(fs_ctx *ctx) {
+// one SIMPLE iteration in two parts around the p' Krylov launch (MainProgram.for:257-348)
+static int iteration_pre(fs_ctx *ctx) {
   int rc;
   FS_TIMING(cudaEventRecord(ctx->ev[0], ctx->st));
   if (ctx->cfg.batched_momentum && ctx->cfg.solver_mom == FS_SOLVER_SOR) {
@@ -500,7 +513,12 @@ static int iteration_body(fs_ctx *ctx) {
   FS_TIMING(cudaEventRecord(ctx->ev[1], ctx->st));
   if ((rc = fs_continuity_assemble(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[2], ctx->st));
-  if ((rc = pc_solve(ctx))) return rc;
+  return pc_solve_pre(ctx);
+}
+
+static int iteration_post(fs_ctx *ctx) {
+  int rc;
+  if ((rc = pc_solve_post(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[3], ctx->st));
   if ((rc = fs_continuity_correct(ctx))) return rc;
   // CalculateEffectsOfTurbulence (MainProgram.for:275-277), SolveEnergy (:281)
@@ -508,6 +526,12 @@ static int iteration_body(fs_ctx *ctx) {
   if ((rc = fs_energy_solve(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[4], ctx->st));
   return FS_OK;
+}
+
+static int iteration_body(fs_ctx *ctx) {
+  int rc = iteration_pre(ctx);
+  if (rc) return rc;
+  return iteration_post(ctx);
 }
 
 static int iteration_enqueue(fs_ctx *ctx) {
@@ -736,14 +760,18 @@ int fs_sync(fs_ctx *ctx) {
 // iterations of every case captured into ONE CUDA graph -- the cases in
 // sequence, so their cooperative solver kernels never run concurrently -- and
 // the graph launched `launches` times, one host synchronisation per launch.
+// Batched: each iteration runs every case up to its p' solve, then all the p'
+// solves in one cooperative launch (k_amg_bicgstab_batch: CTA groups sized by
+// rows x p' iterations, each solving its case behind its own bounded barrier),
+// then the rest of every case's iteration.
 // Residual blocks and linear iteration counts of every captured iteration go to
 // pinned host memory by copies inside the graph.  source_out[q*T + t] is the
 // stop metric of case q after its t-th run iteration (T = iters*launches),
 // pc_iters_out (optional) the p' iterations, ms_out the device time of the
 // launches.  The p' history guess runs inside the graph; the learned network's
 // guess (host bookkeeping per solve) does not.
-int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
-                    float *ms_out) {
+static int ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
+                        float *ms_out, bool batched) {
   if (!cs || n < 1 || iters < 1 || launches < 1 || !source_out) return FS_E_ARG;
   fs_ctx *c0 = cs[0];
   for (int q = 0; q < n; q++)
@@ -753,13 +781,22 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
   // ordinary iterations per case build hierarchies, colourings and grids
   // (nothing may allocate during capture); the HR start must already be passed
   // and the p' history full (the captured solves take a fixed basis)
+  std::vector<double> weight(n, 1.);
   for (int q = 0; q < n; q++) {
     fs_ctx *c = cs[q];
+    fs_residuals r;
     do {
-      fs_residuals r;
       int rc = fs_simple_iteration(c, &r);
       if (rc) { if (c != ctx) ctx->err = c->err; return rc; }
     } while (c->nIter < c->cfg.niter_start_hr || c->hist_cnt < c->hist_cap);
+    // the batched p' launch gives each case CTAs in proportion to its rows
+    // times its last p' iterations
+    weight[q] = (double)c->N * std::max(1, r.lin_iters[FS_VAR_PC - 1]);
+  }
+  fs_pc_batch *PB = nullptr;
+  if (batched) {
+    int rc = fs_pc_batch_create(cs, n, weight.data(), &PB);
+    if (rc) return rc;
   }
   const size_t slot = RB_SIZE + FS_NITERS / 2;  // residual block, then the int32 iteration counts
   double *h = nullptr;
@@ -771,6 +808,7 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
   std::vector<int> nit0(n);
   int rc = FS_OK;
   auto cleanup = [&]() {
+    fs_pc_batch_free(PB);
     if (x) cudaGraphExecDestroy(x);
     if (g) cudaGraphDestroy(g);
     if (ej) cudaEventDestroy(ej);
@@ -794,22 +832,41 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
   (void)cudaGetLastError();  // no stale error may be reported by a launch check inside the capture
   if ((e = cudaStreamBeginCapture(S, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return fail("capture", e);
   const char *what = nullptr;
-  for (int t = 0; t < iters && rc == FS_OK && !what; t++)
+  // one part of case q's iteration on its stream, joined to S before and after
+  auto on_case = [&](fs_ctx *c, auto &&part) -> bool {
+    if ((e = cudaEventRecord(ej, S)) != cudaSuccess) { what = "join record"; return false; }
+    if ((e = cudaStreamWaitEvent(c->st, ej, 0)) != cudaSuccess) { what = "join wait"; return false; }
+    c->graph_mode = true;
+    c->pc_defer = batched;
+    rc = part(c);
+    c->graph_mode = false;
+    c->pc_defer = false;
+    if (rc != FS_OK) { if (c != ctx) ctx->err = c->err; return false; }
+    if ((e = cudaEventRecord(ej, c->st)) != cudaSuccess) { what = "rejoin record"; return false; }
+    if ((e = cudaStreamWaitEvent(S, ej, 0)) != cudaSuccess) { what = "rejoin wait"; return false; }
+    return true;
+  };
+  for (int t = 0; t < iters && rc == FS_OK && !what; t++) {
+    if (batched) {
+      // every case up to its p' solve, all p' solves in one launch, then the rest
+      bool ok = true;
+      for (int q = 0; q < n && ok; q++)
+        ok = on_case(cs[q], [](fs_ctx *c) { c->nIter++; return iteration_pre(c); });
+      if (!ok) break;
+      if ((rc = fs_pc_batch_launch(PB, cs, n, S)) != FS_OK) break;
+    }
     for (int q = 0; q < n && rc == FS_OK && !what; q++) {
       fs_ctx *c = cs[q];
-      if ((e = cudaEventRecord(ej, S)) != cudaSuccess) { what = "join record"; break; }
-      if ((e = cudaStreamWaitEvent(c->st, ej, 0)) != cudaSuccess) { what = "join wait"; break; }
-      c->graph_mode = true;
-      rc = iteration_enqueue(c);
-      c->graph_mode = false;
-      if (rc != FS_OK) { if (c != ctx) ctx->err = c->err; break; }
+      const bool ok = batched ? on_case(c, [](fs_ctx *cc) { return iteration_post(cc); })
+                              : on_case(c, [](fs_ctx *cc) { return iteration_enqueue(cc); });
+      if (!ok) break;
+      // the residual block and iteration counts of this iteration, on S after the case's work
       double *d = h + ((size_t)q * iters + t) * slot;
-      if ((e = cudaMemcpyAsync(d, c->resblk, sizeof(double) * RB_SIZE, cudaMemcpyDeviceToHost, c->st)) != cudaSuccess ||
-          (e = cudaMemcpyAsync(d + RB_SIZE, c->d_iters, sizeof(int32_t) * FS_NITERS, cudaMemcpyDeviceToHost, c->st)) !=
+      if ((e = cudaMemcpyAsync(d, c->resblk, sizeof(double) * RB_SIZE, cudaMemcpyDeviceToHost, S)) != cudaSuccess ||
+          (e = cudaMemcpyAsync(d + RB_SIZE, c->d_iters, sizeof(int32_t) * FS_NITERS, cudaMemcpyDeviceToHost, S)) !=
               cudaSuccess) { what = "residual copy"; break; }
-      if ((e = cudaEventRecord(ej, c->st)) != cudaSuccess) { what = "rejoin record"; break; }
-      if ((e = cudaStreamWaitEvent(S, ej, 0)) != cudaSuccess) { what = "rejoin wait"; break; }
     }
+  }
   cudaError_t ec = cudaStreamEndCapture(S, &g);
   for (int q = 0; q < n; q++) cs[q]->nIter = nit0[q];
   if (what) return fail(what, e);
@@ -837,6 +894,16 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
   for (int q = 0; q < n; q++) cs[q]->nIter = nit0[q] + T;
   cleanup();
   return FS_OK;
+}
+
+int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
+                    float *ms_out) {
+  return ensemble_run(cs, n, iters, launches, source_out, pc_iters_out, ms_out, false);
+}
+
+int fs_ensemble_run_batched(fs_ctx **cs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
+                            float *ms_out) {
+  return ensemble_run(cs, n, iters, launches, source_out, pc_iters_out, ms_out, true);
 }
 
 }  // extern "C"

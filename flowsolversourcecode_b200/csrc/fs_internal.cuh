@@ -180,6 +180,7 @@ struct fs_ctx {
   int coop_grid = 0;            // blocks of a cooperative solver launch
   int coop_per_sm = 0;          // launch shape: cooperative CTAs per SM (0: up to 4; fs_set_launch_shape)
   bool graph_mode = false;      // enqueueing for stream capture: no host syncs, no timing events
+  bool pc_defer = false;        // the AMG-BiCGSTAB solve prepares its launch and leaves it to fs_pc_batch_launch
   int test_wait_extra = 0;      // fs_test_wait_timeout: extra arrivals the team barrier waits for
 };
 
@@ -288,6 +289,17 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver);
 int fs_solver_stats_collect(fs_ctx *ctx);
 int fs_coop_per_sm(fs_ctx *ctx, int occupancy);         // CTAs per SM for a cooperative launch (1)
 int fs_coop_block(const fs_ctx *ctx);                   // threads per CTA of a cooperative launch
+// batched AMG-BiCGSTAB p' solves of several contexts in one cooperative launch
+// (ensembles): fs_pc_batch_form reports whether a context's p' solver can take
+// part and in which kernel form; fs_pc_batch_create splits the co-resident
+// CTAs among the contexts by weight; fs_pc_batch_launch launches the solves
+// the contexts prepared with pc_defer set
+struct fs_pc_batch;
+int fs_linear_solve_finish(fs_ctx *ctx, int nf, double *fi);
+int fs_pc_batch_form(fs_ctx *ctx, int *form);
+int fs_pc_batch_create(fs_ctx **cs, int n, const double *weight, fs_pc_batch **out);
+int fs_pc_batch_launch(fs_pc_batch *B, fs_ctx **cs, int n, cudaStream_t st);
+void fs_pc_batch_free(fs_pc_batch *B);
 int fs_nn_before_pc(fs_ctx *ctx, const double **x0);   // features (+ guess) before the p' solve
 int fs_nn_after_pc(fs_ctx *ctx);                        // snapshot capture, previous p'
 void fs_nn_free(fs_ctx *ctx);

@@ -1084,7 +1084,17 @@ int fs_linear_solve(fs_ctx *ctx, int nf, double *fi, double rrf, int itmax, int 
     return FS_E_ARG;
   }
   if (rc) return rc;
+  if (ctx->pc_defer && nf == FS_VAR_PC) return FS_OK;   // fs_linear_solve_finish after the batched launch
   FS_TIMING(FS_CK(cudaEventRecord(ctx->sev[nf - 1][1], ctx->st)); ctx->s_pending[nf - 1] = true);
+  k_axpy_field<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, fi, ctx->dphi);
+  FS_LAUNCH_CHECK();
+  return FS_OK;
+}
+
+// the end of a solve whose Krylov launch was deferred (pc_defer): fi += dphi
+int fs_linear_solve_finish(fs_ctx *ctx, int nf, double *fi) {
+  (void)nf;
+  const int N = ctx->N;
   k_axpy_field<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, fi, ctx->dphi);
   FS_LAUNCH_CHECK();
   return FS_OK;

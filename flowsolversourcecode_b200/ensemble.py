@@ -8,7 +8,9 @@ counterpart: the reference solves one case per process).
 
 Every case keeps its own context (mesh, fields, matrices, multigrid hierarchy);
 `fs_ensemble_run` captures `iters` SIMPLE iterations of all cases into one CUDA
-graph and launches it `launches` times.  Across GPUs the cases shard by size
+graph and launches it `launches` times; `fs_ensemble_run_batched` (run(...,
+batched=True)) does the same with the p' solves of all cases in one cooperative
+launch, a group of CTAs per case.  Across GPUs the cases shard by size
 (`shard`, longest processing time first) with no collective on the data path.
 """
 from __future__ import annotations
@@ -122,15 +124,20 @@ class Ensemble:
         self.shapes = best
         return best
 
-    def run(self, iters: int, launches: int = 1) -> dict:
+    def run(self, iters: int, launches: int = 1, batched: bool = False) -> dict:
+        """`iters` SIMPLE iterations of every case per graph launch.  batched:
+        the p' solves of all cases run as one cooperative launch with a CTA
+        group per case (`fs_ensemble_run_batched`); otherwise the cases run
+        one after another (`fs_ensemble_run`)."""
         n = len(self.solvers)
         T = iters * launches
         arr = (C.c_void_p * n)(*[s.ctx.value for s in self.solvers])
         src = np.zeros(n * T)
         pci = np.zeros(n * T, np.int32)
         ms = C.c_float()
-        rc = self.lib.fs_ensemble_run(arr, n, iters, launches, L.dptr(src), L.iptr(pci), C.byref(ms))
-        L.check(rc, self.solvers[0].ctx, "fs_ensemble_run")
+        fn = "fs_ensemble_run_batched" if batched else "fs_ensemble_run"
+        rc = getattr(self.lib, fn)(arr, n, iters, launches, L.dptr(src), L.iptr(pci), C.byref(ms))
+        L.check(rc, self.solvers[0].ctx, fn)
         return {"source": src.reshape(n, T), "pc_iters": pci.reshape(n, T), "ms": ms.value,
                 "cell_iters_per_s": sum(self.cells) * T / (ms.value * 1e-3)}
 

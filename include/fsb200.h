@@ -544,6 +544,16 @@ int fs_set_launch_shape(fs_ctx *ctx, int shape);
 int fs_test_wait_timeout(fs_ctx *ctx, int extra);
 int fs_ensemble_run(fs_ctx **ctxs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
                     float *ms_out);
+/* fs_ensemble_run_batched: the same, except that inside each iteration every
+ * case runs up to its p' solve, then the p' solves of all cases run as ONE
+ * cooperative launch in which each case has its own group of CTAs (sized in
+ * proportion to its cells times its p' iterations in the warm-up) and its own
+ * bounded barriers, and then every case finishes its iteration.  All cases
+ * must use the same AMG-BiCGSTAB p' solver form (FS_E_UNSUPPORTED otherwise).
+ * The Krylov reductions of a case then run over its group rather than the whole
+ * grid, so results differ from fs_ensemble_run's within the p' tolerance. */
+int fs_ensemble_run_batched(fs_ctx **ctxs, int n, int iters, int launches, double *source_out,
+                            int32_t *pc_iters_out, float *ms_out);
 
 /* Timing of the last outer iteration's phases in milliseconds (CUDA events):
  * [0] momentum assembly, [1] momentum solves, [2] continuity assembly,

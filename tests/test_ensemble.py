@@ -56,3 +56,33 @@ def test_autotune_picks_a_shape():
     out = ens.run(iters=2, launches=1)
     assert np.all(np.isfinite(out["source"]))
     ens.close()
+
+
+@pytest.mark.gpu
+def test_batched_run_matches_sequential_within_tolerance():
+    """The p' solves of all cases in one launch, a CTA group per case: the
+    Krylov sums run over the group instead of the whole grid, so the results
+    match the sequential graph run within the p' tolerance, not bit for bit."""
+    specs = [E.CaseSpec(10, 1.0, 400.0), E.CaseSpec(12, 0.7, 150.0), E.CaseSpec(16, 1.6, 900.0)]
+    outs = []
+    for batched in (False, True):
+        ens = E.Ensemble([E.build_case(s, krylov_tol=1e-10) for s in specs])
+        outs.append(ens.run(iters=3, launches=2, batched=batched))
+        ens.close()
+    seq, bat = outs
+    assert np.all(np.isfinite(bat["source"]))
+    assert np.allclose(bat["source"], seq["source"], rtol=1e-6, atol=0), (bat["source"], seq["source"])
+    assert np.all(np.abs(bat["pc_iters"] - seq["pc_iters"]) <= 2), (bat["pc_iters"], seq["pc_iters"])
+    assert bat["ms"] > 0
+
+
+@pytest.mark.gpu
+def test_batched_run_rejects_mixed_solvers():
+    from flowsolversourcecode_b200._lib import FsError
+    a = E.build_case(E.CaseSpec(10, 1.0, 400.0))
+    m, c = E.build_case(E.CaseSpec(12, 1.0, 400.0))
+    c.solver_cont = "bicgs"
+    ens = E.Ensemble([a, (m, c)])
+    with pytest.raises(FsError):
+        ens.run(iters=1, launches=1, batched=True)
+    ens.close()
