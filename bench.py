@@ -441,9 +441,10 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
     converged fields unchanged by it) from the least-squares combination of the
     4 previous p' solutions, multi-RHS momentum, launch shape autotuned per
     case, every `--steps` iterations of all of a GPU's cases one CUDA graph,
-    timed in two forms -- cases in sequence, and the p' solves of all cases in
-    one cooperative launch with a CTA group per case -- and the faster one
-    reported (both rates in `config`).
+    timed in two forms -- cases in sequence, and the cases concurrently (the
+    momentum solves of all cases in one cooperative launch and their p' solves
+    in another, a CTA group per case, the remaining kernels as concurrent graph
+    branches) -- and the faster one reported (both rates in `config`).
     Cases shard over ranks by size (longest processing time first); no
     collective on the data path.  Metric: cell-iterations per second, whole job."""
     import numpy as np
@@ -491,8 +492,9 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
                                   f"{args.ensemble_tol:g}, started from the least-squares combination of the 4 "
                                   f"previous p' solutions",
                        "launch_shapes_rank0": {str(k): shapes.count(k) for k in sorted(set(shapes))},
-                       "pc_launch": "one cooperative launch for the p' solves of all cases, a CTA group each"
-                                    if best else "the cases' p' solves one after another",
+                       "pc_launch": "the momentum solves of all cases in one cooperative launch and their p' "
+                                    "solves in another, a CTA group per case; the other kernels of the cases as "
+                                    "concurrent graph branches" if best else "the cases one after another",
                        "cell_iter_per_s_by_form": {
                            "sequential": total_cells * T / (timed[False][0] * 1e-3),
                            "batched_pc": total_cells * T / (timed[True][0] * 1e-3)},

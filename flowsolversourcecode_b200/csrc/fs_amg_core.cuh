@@ -735,6 +735,93 @@ __device__ double rhs_mean(Sync &S, const AmgKArgs<R> &a) {
   return n_nonsing == 0. ? b_total / N : 0.;
 }
 
+// The initial guess of k_amg_bicgstab, one cooperative launch before it: the
+// combination x = sum_j c_j x_j of the basis vectors (previous p' solutions,
+// the network's guess) that minimises |b - A x|, least squares over their
+// span, so |b - A x| <= |b|.  The normal equations (Gram matrix of the A x_j)
+// are solved by every CTA alike from grid-deterministic sums, by a Cholesky
+// factorisation with a relative diagonal shift.  x goes to a.x and fit[0] = 1;
+// a failed factorisation leaves fit[0] = 0 (the solve starts from zero).
+template <class R>
+__device__ __forceinline__ void guess_fit_body(const AmgKArgs<R> a) {
+  Sync S(a.part);
+  const int N = a.N, nx = a.nx;
+  const long t0 = (long)cta_id() * blockDim.x + threadIdx.x, nt = (long)cta_count() * blockDim.x;
+  const double bmean = rhs_mean(S, a);
+  double c[FS_GUESS_MAX];
+  for (int j = 0; j < FS_GUESS_MAX; j++) c[j] = 0.;
+  bool fell_back = false;
+  {
+    // Gram matrix G_jk = (A x_j).(A x_k) (upper triangle), g_j = (A x_j).b, |b|^2
+    double acc[FS_SUMK];
+    const int ng = nx * (nx + 1) / 2;
+    for (int k = 0; k < ng + nx + 1; k++) acc[k] = 0.;
+    for (long i = t0; i < N; i += nt) {
+      double y[FS_GUESS_MAX];
+      for (int j = 0; j < nx; j++) {
+        const double *xj = a.xs[j];
+        double t = 0.;
+        t = t + a.ac[i] * xj[i];
+        y[j] = ell_acc<8, false>(t, a.N, a.W, a.cn, a.anb, i, [&](int k) { return xj[k]; });
+      }
+      const double b1 = a.bc[i] - bmean;
+      int q = 0;
+      for (int j = 0; j < nx; j++)
+        for (int k = j; k < nx; k++) acc[q++] += y[j] * y[k];
+      for (int j = 0; j < nx; j++) acc[ng + j] += y[j] * b1;
+      acc[ng + nx] += b1 * b1;
+    }
+    double tot[FS_SUMK];
+    S.sumK(acc, tot, ng + nx + 1);
+    // Cholesky of G + 1e-12 max(diag) I, then the two triangular solves (row-major L)
+    double L[FS_GUESS_MAX * FS_GUESS_MAX];
+    double dmax = 0.;
+    {
+      int q = 0;
+      for (int j = 0; j < nx; j++)
+        for (int k = j; k < nx; k++) { L[k * FS_GUESS_MAX + j] = tot[q]; if (k == j) dmax = fmax(dmax, tot[q]); q++; }
+    }
+    bool ok = dmax > 0. && isfinite(dmax);
+    for (int j = 0; j < nx && ok; j++) {
+      double d = L[j * FS_GUESS_MAX + j] + 1e-12 * dmax;
+      for (int k = 0; k < j; k++) d -= L[j * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
+      if (!(d > 1e-14 * dmax)) { ok = false; break; }
+      d = sqrt(d);
+      L[j * FS_GUESS_MAX + j] = d;
+      for (int r = j + 1; r < nx; r++) {
+        double v = L[r * FS_GUESS_MAX + j];
+        for (int k = 0; k < j; k++) v -= L[r * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
+        L[r * FS_GUESS_MAX + j] = v / d;
+      }
+    }
+    if (ok) {
+      double z[FS_GUESS_MAX];
+      for (int j = 0; j < nx; j++) {
+        double v = tot[ng + j];
+        for (int k = 0; k < j; k++) v -= L[j * FS_GUESS_MAX + k] * z[k];
+        z[j] = v / L[j * FS_GUESS_MAX + j];
+      }
+      for (int j = nx - 1; j >= 0; j--) {
+        double v = z[j];
+        for (int k = j + 1; k < nx; k++) v -= L[k * FS_GUESS_MAX + j] * c[k];
+        c[j] = v / L[j * FS_GUESS_MAX + j];
+      }
+      for (int j = 0; j < nx; j++) if (!isfinite(c[j])) ok = false;
+    }
+    if (!ok) for (int j = 0; j < nx; j++) c[j] = 0.;
+    fell_back = !ok;
+    for (long i = t0; i < N; i += nt) {
+      double xi = 0.;
+      for (int j = 0; j < nx; j++) xi += c[j] * a.xs[j][i];
+      a.x[i] = xi;
+    }
+  }
+  if (cta_id() == 0 && threadIdx.x == 0) {
+    a.fit[0] = fell_back ? 0 : 1;
+    if (a.nncnt) { a.nncnt[1] += 1; if (fell_back) a.nncnt[0] += 1; }
+  }
+}
+
 // right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle:
 // MODE 0 run(), 2 run_gs() (multicolour Gauss-Seidel smoothing), 1 the fused
 // V-cycle (one pre- and one post-sweep, dense coarsest level), whose first

@@ -496,7 +496,9 @@ static int read_residuals(fs_ctx *ctx, fs_residuals *res) {
 
 // one SIMPLE outer iteration enqueued on the context stream (MainProgram.for:257-325)
 // one SIMPLE iteration in two parts around the p' Krylov launch (MainProgram.for:257-348)
-static int iteration_pre(fs_ctx *ctx) {
+// the momentum part (with mom_defer the multi-RHS SOR launch is left to
+// fs_mom_batch_launch), then the part up to the p' Krylov launch
+static int iteration_mom(fs_ctx *ctx) {
   int rc;
   FS_TIMING(cudaEventRecord(ctx->ev[0], ctx->st));
   if (ctx->cfg.batched_momentum && ctx->cfg.solver_mom == FS_SOLVER_SOR) {
@@ -510,10 +512,22 @@ static int iteration_pre(fs_ctx *ctx) {
       if ((rc = fs_linear_solve(ctx, c + 1, fi, ctx->cfg.rrf_mom, ctx->cfg.itmax_mom, ctx->cfg.solver_mom))) return rc;
     }
   }
+  return FS_OK;
+}
+
+static int iteration_mid(fs_ctx *ctx) {
+  int rc;
+  if (ctx->mom_defer && (rc = fs_momentum_batched_finish(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[1], ctx->st));
   if ((rc = fs_continuity_assemble(ctx))) return rc;
   FS_TIMING(cudaEventRecord(ctx->ev[2], ctx->st));
   return pc_solve_pre(ctx);
+}
+
+static int iteration_pre(fs_ctx *ctx) {
+  int rc = iteration_mom(ctx);
+  if (rc) return rc;
+  return iteration_mid(ctx);
 }
 
 static int iteration_post(fs_ctx *ctx) {
@@ -793,10 +807,25 @@ static int ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *sou
     // times its last p' iterations
     weight[q] = (double)c->N * std::max(1, r.lin_iters[FS_VAR_PC - 1]);
   }
+  // batched: the multi-RHS momentum solves also go into one launch when every
+  // case uses them; the parts of an iteration that have no cooperative kernel
+  // then run as concurrent branches, one per case (cases with k-epsilon or the
+  // temperature equation solve those with cooperative kernels, so their last
+  // part stays in sequence)
+  bool mom_b = batched, fork_post = batched;
+  std::vector<double> mom_w(n);
+  for (int q = 0; q < n; q++) {
+    mom_b = mom_b && cs[q]->cfg.batched_momentum && cs[q]->cfg.solver_mom == FS_SOLVER_SOR;
+    fork_post = fork_post && !cs[q]->turb && !cs[q]->energy;
+    mom_w[q] = (double)cs[q]->N;
+  }
   fs_pc_batch *PB = nullptr;
+  fs_mom_batch *MB = nullptr;
+  std::vector<cudaEvent_t> ev(n, nullptr);
   if (batched) {
     int rc = fs_pc_batch_create(cs, n, weight.data(), &PB);
     if (rc) return rc;
+    if (mom_b && (rc = fs_mom_batch_create(cs, n, mom_w.data(), &MB))) { fs_pc_batch_free(PB); return rc; }
   }
   const size_t slot = RB_SIZE + FS_NITERS / 2;  // residual block, then the int32 iteration counts
   double *h = nullptr;
@@ -809,6 +838,8 @@ static int ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *sou
   int rc = FS_OK;
   auto cleanup = [&]() {
     fs_pc_batch_free(PB);
+    fs_mom_batch_free(MB);
+    for (auto &v : ev) if (v) cudaEventDestroy(v);
     if (x) cudaGraphExecDestroy(x);
     if (g) cudaGraphDestroy(g);
     if (ej) cudaEventDestroy(ej);
@@ -826,6 +857,9 @@ static int ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *sou
   if ((e = cudaStreamCreateWithFlags(&S, cudaStreamNonBlocking)) != cudaSuccess) return fail("stream", e);
   if ((e = cudaEventCreateWithFlags(&ej, cudaEventDisableTiming)) != cudaSuccess) return fail("event", e);
   if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) return fail("event", e);
+  if (batched)
+    for (int q = 0; q < n; q++)
+      if ((e = cudaEventCreateWithFlags(&ev[q], cudaEventDisableTiming)) != cudaSuccess) return fail("event", e);
   for (int q = 0; q < n; q++) nit0[q] = cs[q]->nIter;
   for (int q = 0; q < n; q++)
     if ((e = cudaStreamSynchronize(cs[q]->st)) != cudaSuccess) return fail("before capture", e);
@@ -846,19 +880,50 @@ static int ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *sou
     if ((e = cudaStreamWaitEvent(S, ej, 0)) != cudaSuccess) { what = "rejoin wait"; return false; }
     return true;
   };
+  // one part of every case's iteration as concurrent branches off S (no
+  // cooperative kernel may be in such a part), joined back into S
+  auto on_all = [&](auto &&part) -> bool {
+    if ((e = cudaEventRecord(ej, S)) != cudaSuccess) { what = "fork record"; return false; }
+    for (int q = 0; q < n; q++) {
+      fs_ctx *c = cs[q];
+      if ((e = cudaStreamWaitEvent(c->st, ej, 0)) != cudaSuccess) { what = "fork wait"; return false; }
+      c->graph_mode = true;
+      c->pc_defer = true;
+      c->mom_defer = mom_b;
+      rc = part(c);
+      c->graph_mode = false;
+      c->pc_defer = false;
+      c->mom_defer = false;
+      if (rc != FS_OK) { if (c != ctx) ctx->err = c->err; return false; }
+      if ((e = cudaEventRecord(ev[q], c->st)) != cudaSuccess) { what = "join record"; return false; }
+    }
+    for (int q = 0; q < n; q++)
+      if ((e = cudaStreamWaitEvent(S, ev[q], 0)) != cudaSuccess) { what = "join wait"; return false; }
+    return true;
+  };
   for (int t = 0; t < iters && rc == FS_OK && !what; t++) {
     if (batched) {
-      // every case up to its p' solve, all p' solves in one launch, then the rest
+      // every case up to its p' solve (the momentum solves in one launch when
+      // mom_b), all p' solves in one launch, then the rest
       bool ok = true;
-      for (int q = 0; q < n && ok; q++)
-        ok = on_case(cs[q], [](fs_ctx *c) { c->nIter++; return iteration_pre(c); });
+      if (mom_b) {
+        ok = on_all([](fs_ctx *c) { c->nIter++; return iteration_mom(c); });
+        if (!ok) break;
+        if ((rc = fs_mom_batch_launch(MB, cs, n, S)) != FS_OK) break;
+        ok = on_all([](fs_ctx *c) { return iteration_mid(c); });
+      } else {
+        for (int q = 0; q < n && ok; q++)
+          ok = on_case(cs[q], [](fs_ctx *c) { c->nIter++; return iteration_pre(c); });
+      }
       if (!ok) break;
       if ((rc = fs_pc_batch_launch(PB, cs, n, S)) != FS_OK) break;
+      if (fork_post && !on_all([](fs_ctx *c) { return iteration_post(c); })) break;
     }
     for (int q = 0; q < n && rc == FS_OK && !what; q++) {
       fs_ctx *c = cs[q];
-      const bool ok = batched ? on_case(c, [](fs_ctx *cc) { return iteration_post(cc); })
-                              : on_case(c, [](fs_ctx *cc) { return iteration_enqueue(cc); });
+      bool ok = true;
+      if (!batched) ok = on_case(c, [](fs_ctx *cc) { return iteration_enqueue(cc); });
+      else if (!fork_post) ok = on_case(c, [](fs_ctx *cc) { return iteration_post(cc); });
       if (!ok) break;
       // the residual block and iteration counts of this iteration, on S after the case's work
       double *d = h + ((size_t)q * iters + t) * slot;

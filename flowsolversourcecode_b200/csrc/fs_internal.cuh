@@ -181,6 +181,9 @@ struct fs_ctx {
   int coop_per_sm = 0;          // launch shape: cooperative CTAs per SM (0: up to 4; fs_set_launch_shape)
   bool graph_mode = false;      // enqueueing for stream capture: no host syncs, no timing events
   bool pc_defer = false;        // the AMG-BiCGSTAB solve prepares its launch and leaves it to fs_pc_batch_launch
+  bool mom_defer = false;       // the multi-RHS momentum solve prepares its launch for fs_mom_batch_launch
+  bool mom_pending = false;
+  alignas(8) unsigned char mom_pend[160];   // the prepared launch's arguments (Sor3Args)
   int test_wait_extra = 0;      // fs_test_wait_timeout: extra arrivals the team barrier waits for
 };
 
@@ -296,6 +299,17 @@ int fs_coop_block(const fs_ctx *ctx);                   // threads per CTA of a 
 // the contexts prepared with pc_defer set
 struct fs_pc_batch;
 int fs_linear_solve_finish(fs_ctx *ctx, int nf, double *fi);
+// the multi-RHS momentum solves of several contexts in one cooperative launch
+// (ensembles), as the p' solves above; fs_momentum_batched_finish moves a
+// deferred solve's result back to cell order
+struct fs_mom_batch;
+int fs_momentum_batched_finish(fs_ctx *ctx);
+int fs_mom_batch_create(fs_ctx **cs, int n, const double *weight, fs_mom_batch **out);
+int fs_mom_batch_launch(fs_mom_batch *B, fs_ctx **cs, int n, cudaStream_t st);
+void fs_mom_batch_free(fs_mom_batch *B);
+// CTA offsets of n groups sharing `cap` co-resident CTAs in proportion to
+// weight (at least one each; largest remainders, so the split is reproducible)
+std::vector<int32_t> fs_cta_split(int cap, const double *weight, int n);
 int fs_pc_batch_form(fs_ctx *ctx, int *form);
 int fs_pc_batch_create(fs_ctx **cs, int n, const double *weight, fs_pc_batch **out);
 int fs_pc_batch_launch(fs_pc_batch *B, fs_ctx **cs, int n, cudaStream_t st);

@@ -375,91 +375,11 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.iters = ncycle - 1;
 }
 
-// The initial guess of k_amg_bicgstab, one cooperative launch before it: the
-// combination x = sum_j c_j x_j of the basis vectors (previous p' solutions,
-// the network's guess) that minimises |b - A x|, least squares over their
-// span, so |b - A x| <= |b|.  The normal equations (Gram matrix of the A x_j)
-// are solved by every CTA alike from grid-deterministic sums, by a Cholesky
-// factorisation with a relative diagonal shift.  x goes to a.x and fit[0] = 1;
-// a failed factorisation leaves fit[0] = 0 (the solve starts from zero).
+// the initial guess of k_amg_bicgstab on the whole cooperative grid
+// (guess_fit_body in fs_amg_core.cuh)
 template <class R>
 __global__ void __launch_bounds__(FS_COOP_BLOCK, 1) k_guess_fit(AmgKArgs<R> a) {
-  Sync S(a.part);
-  const int N = a.N, nx = a.nx;
-  const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long)gridDim.x * blockDim.x;
-  const double bmean = rhs_mean(S, a);
-  double c[FS_GUESS_MAX];
-  for (int j = 0; j < FS_GUESS_MAX; j++) c[j] = 0.;
-  bool fell_back = false;
-  {
-    // Gram matrix G_jk = (A x_j).(A x_k) (upper triangle), g_j = (A x_j).b, |b|^2
-    double acc[FS_SUMK];
-    const int ng = nx * (nx + 1) / 2;
-    for (int k = 0; k < ng + nx + 1; k++) acc[k] = 0.;
-    for (long i = t0; i < N; i += nt) {
-      double y[FS_GUESS_MAX];
-      for (int j = 0; j < nx; j++) {
-        const double *xj = a.xs[j];
-        double t = 0.;
-        t = t + a.ac[i] * xj[i];
-        y[j] = ell_acc<8, false>(t, a.N, a.W, a.cn, a.anb, i, [&](int k) { return xj[k]; });
-      }
-      const double b1 = a.bc[i] - bmean;
-      int q = 0;
-      for (int j = 0; j < nx; j++)
-        for (int k = j; k < nx; k++) acc[q++] += y[j] * y[k];
-      for (int j = 0; j < nx; j++) acc[ng + j] += y[j] * b1;
-      acc[ng + nx] += b1 * b1;
-    }
-    double tot[FS_SUMK];
-    S.sumK(acc, tot, ng + nx + 1);
-    // Cholesky of G + 1e-12 max(diag) I, then the two triangular solves (row-major L)
-    double L[FS_GUESS_MAX * FS_GUESS_MAX];
-    double dmax = 0.;
-    {
-      int q = 0;
-      for (int j = 0; j < nx; j++)
-        for (int k = j; k < nx; k++) { L[k * FS_GUESS_MAX + j] = tot[q]; if (k == j) dmax = fmax(dmax, tot[q]); q++; }
-    }
-    bool ok = dmax > 0. && isfinite(dmax);
-    for (int j = 0; j < nx && ok; j++) {
-      double d = L[j * FS_GUESS_MAX + j] + 1e-12 * dmax;
-      for (int k = 0; k < j; k++) d -= L[j * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
-      if (!(d > 1e-14 * dmax)) { ok = false; break; }
-      d = sqrt(d);
-      L[j * FS_GUESS_MAX + j] = d;
-      for (int r = j + 1; r < nx; r++) {
-        double v = L[r * FS_GUESS_MAX + j];
-        for (int k = 0; k < j; k++) v -= L[r * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
-        L[r * FS_GUESS_MAX + j] = v / d;
-      }
-    }
-    if (ok) {
-      double z[FS_GUESS_MAX];
-      for (int j = 0; j < nx; j++) {
-        double v = tot[ng + j];
-        for (int k = 0; k < j; k++) v -= L[j * FS_GUESS_MAX + k] * z[k];
-        z[j] = v / L[j * FS_GUESS_MAX + j];
-      }
-      for (int j = nx - 1; j >= 0; j--) {
-        double v = z[j];
-        for (int k = j + 1; k < nx; k++) v -= L[k * FS_GUESS_MAX + j] * c[k];
-        c[j] = v / L[j * FS_GUESS_MAX + j];
-      }
-      for (int j = 0; j < nx; j++) if (!isfinite(c[j])) ok = false;
-    }
-    if (!ok) for (int j = 0; j < nx; j++) c[j] = 0.;
-    fell_back = !ok;
-    for (long i = t0; i < N; i += nt) {
-      double xi = 0.;
-      for (int j = 0; j < nx; j++) xi += c[j] * a.xs[j][i];
-      a.x[i] = xi;
-    }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.fit[0] = fell_back ? 0 : 1;
-    if (a.nncnt) { a.nncnt[1] += 1; if (fell_back) a.nncnt[0] += 1; }
-  }
+  g1::guess_fit_body<R>(a);
 }
 
 // right-preconditioned BiCGSTAB with the V-cycle on the whole cooperative grid
@@ -491,6 +411,27 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB)
   __syncthreads();
   const AmgKArgs<R> a = as[G.q];
   gb::amg_bicgstab_body<R, MODE>(a);
+}
+
+// the initial guesses of the batched solves, in the same CTA groups (a group
+// whose system has no basis vectors does nothing)
+template <class R>
+__global__ void __launch_bounds__(FS_COOP_BLOCK, 1)
+    k_guess_fit_batch(const AmgKArgs<R> *__restrict__ as, const int32_t *__restrict__ start, int n, unsigned *gbar) {
+  gb::GroupState &G = gb::gstate();
+  if (threadIdx.x == 0) {
+    int q = 0;
+    while (q + 1 < n && (int)blockIdx.x >= start[q + 1]) q++;
+    G.q = q;
+    G.cta = (int)blockIdx.x - start[q];
+    G.ncta = start[q + 1] - start[q];
+    G.gen = 0;
+    G.bar = gbar + 2 * q;
+    G.status = as[q].status;
+  }
+  __syncthreads();
+  const AmgKArgs<R> a = as[G.q];
+  if (a.nx > 0) gb::guess_fit_body<R>(a);
 }
 
 // coarse matrix of level lc from level lc-1 (AssembleElementBasedAgglomoratedLHS.for:45-150)
@@ -998,23 +939,16 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     int form = -1;
     if ((rc = fs_pc_batch_form(ctx, &form))) return rc;
     if (form < 0) { ctx->err = "this p' solver cannot join a batched launch"; return FS_E_UNSUPPORTED; }
-    M->pend_form = form;
+    M->pend_form = form;   // the initial-guess fit runs in the batched launch too
     if (!f32) {
       M->pend64 = AmgKArgs<double>{};
       fill(M->pend64);
       M->pend64.lev = M->lev64;
-      void *args[] = {&M->pend64};
-      if (M->pend64.nx > 0)
-        FS_CK(fs_coop_launch((const void *)k_guess_fit<double>, G, fs_coop_block(ctx), args, ctx->st));
     } else {
       M->pend32 = AmgKArgs<float>{};
       fill(M->pend32);
       M->pend32.lev = M->lev32;
-      void *args[] = {&M->pend32};
-      if (M->pend32.nx > 0)
-        FS_CK(fs_coop_launch((const void *)k_guess_fit<float>, G, fs_coop_block(ctx), args, ctx->st));
     }
-    FS_LAUNCH_CHECK();
     return FS_OK;
   }
   if (!f32) {
@@ -1150,8 +1084,7 @@ void fs_pc_batch_free(fs_pc_batch *B) {
 }
 
 // CTAs of one co-resident launch (1024 threads each, one per SM) split among
-// the n contexts in proportion to weight[q] (at least one each), by largest
-// remainders so the split is the same on every run
+// the n contexts in proportion to weight[q] (fs_cta_split)
 int fs_pc_batch_create(fs_ctx **cs, int n, const double *weight, fs_pc_batch **out) {
   if (!cs || n < 1 || !weight || !out) return FS_E_ARG;
   *out = nullptr;
@@ -1168,28 +1101,11 @@ int fs_pc_batch_create(fs_ctx **cs, int n, const double *weight, fs_pc_batch **o
   FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel(form), FS_COOP_BLOCK, 0));
   const int cap = std::min(ctx->num_sms * std::max(occ, 0), FS_RED_BLOCKS);
   if (cap < n) { ctx->err = "more contexts than co-resident CTAs for a batched p' launch"; return FS_E_UNSUPPORTED; }
-  double wsum = 0.;
-  for (int q = 0; q < n; q++) wsum += std::max(weight[q], 0.);
-  std::vector<int> cnt(n, 1);
-  int left = cap - n;
-  if (wsum > 0.) {
-    std::vector<double> rem(n);
-    int given = 0;
-    for (int q = 0; q < n; q++) {
-      const double share = left * std::max(weight[q], 0.) / wsum;
-      const int k = (int)share;
-      cnt[q] += k; given += k; rem[q] = share - k;
-    }
-    std::vector<int> order(n);
-    for (int q = 0; q < n; q++) order[q] = q;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rem[a] > rem[b]; });
-    for (int j = 0; j < left - given && j < n; j++) cnt[order[j]]++;
-  }
+  const std::vector<int32_t> split = fs_cta_split(cap, weight, n);
   fs_pc_batch *B = new fs_pc_batch;
   B->n = n; B->form = form;
   B->argsz = form <= 1 ? sizeof(AmgKArgs<double>) : sizeof(AmgKArgs<float>);
-  B->start.assign(n + 1, 0);
-  for (int q = 0; q < n; q++) B->start[q + 1] = B->start[q] + cnt[q];
+  B->start = split;
   B->ncta = B->start[n];
   cudaError_t e;
   if ((e = cudaHostAlloc(&B->h_args, B->argsz * n, cudaHostAllocDefault)) != cudaSuccess ||
@@ -1210,6 +1126,7 @@ int fs_pc_batch_create(fs_ctx **cs, int n, const double *weight, fs_pc_batch **o
 int fs_pc_batch_launch(fs_pc_batch *B, fs_ctx **cs, int n, cudaStream_t st) {
   if (!B || !cs || n != B->n) return FS_E_ARG;
   fs_ctx *ctx = cs[0];
+  bool nx_any = false;
   for (int q = 0; q < n; q++) {
     fs_mg_dev *M = cs[q]->mg;
     if (!M || M->pend_form != B->form) { ctx->err = "batched p' launch: a context prepared no matching solve"; return FS_E_ARG; }
@@ -1217,18 +1134,26 @@ int fs_pc_batch_launch(fs_pc_batch *B, fs_ctx **cs, int n, cudaStream_t st) {
     if (B->form <= 1) {
       AmgKArgs<double> a = M->pend64;
       a.teambar = B->d_words + 2 * q;
+      nx_any |= a.nx > 0;
       memcpy(dst, &a, sizeof(a));
     } else {
       AmgKArgs<float> a = M->pend32;
       a.teambar = B->d_words + 2 * q;
+      nx_any |= a.nx > 0;
       memcpy(dst, &a, sizeof(a));
     }
     M->pend_form = -1;
   }
   FS_CK(cudaMemcpyAsync(B->d_args, B->h_args, B->argsz * n, cudaMemcpyHostToDevice, st));
-  FS_CK(cudaMemsetAsync(B->d_words, 0, sizeof(unsigned) * 4 * n, st));
   unsigned *gw = B->d_words + 2 * n;
   void *args[] = {&B->d_args, &B->d_start, &B->n, &gw};
+  if (nx_any) {   // the initial guesses, same groups; the barrier words start from zero for each launch
+    FS_CK(cudaMemsetAsync(B->d_words, 0, sizeof(unsigned) * 4 * n, st));
+    FS_CK(fs_coop_launch(B->form <= 1 ? (const void *)k_guess_fit_batch<double> : (const void *)k_guess_fit_batch<float>,
+                         B->ncta, FS_COOP_BLOCK, args, st));
+    FS_LAUNCH_CHECK();
+  }
+  FS_CK(cudaMemsetAsync(B->d_words, 0, sizeof(unsigned) * 4 * n, st));
   FS_CK(fs_coop_launch(batch_kernel(B->form), B->ncta, FS_COOP_BLOCK, args, st));
   FS_LAUNCH_CHECK();
   return FS_OK;

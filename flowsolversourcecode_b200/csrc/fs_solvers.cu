@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 #include <algorithm>
 #include <array>
+#include <cstring>
 
 namespace cg = cooperative_groups;
 
@@ -326,10 +327,66 @@ __device__ __forceinline__ void sub3x2(long N, int W, const int32_t *__restrict_
   }
 }
 
-__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor3_colour(Sor3Args a) {
-  cg::grid_group grid = cg::this_grid();
+// the CTAs a multi-RHS SOR solve runs on: the whole cooperative grid, or one
+// group of a batched launch (CTAs [c0, c0 + n) with a bounded barrier of their
+// own in global memory: bar[0] arrivals, bar[1] generation, zero at launch; a
+// timeout sets status[0] and later barriers stop waiting)
+struct GridCtas {
+  cg::grid_group g;
+  __device__ GridCtas() : g(cg::this_grid()) {}
+  __device__ __forceinline__ int cta() const { return (int)blockIdx.x; }
+  __device__ __forceinline__ int ncta() const { return (int)gridDim.x; }
+  __device__ __forceinline__ void sync() { g.sync(); }
+};
+#define FS_GROUP_SPIN_LIMIT (1L << 20)
+struct GroupCtas {
+  int c, n;
+  unsigned *bar;
+  int32_t *status;
+  unsigned gen;
+  __device__ __forceinline__ int cta() const { return c; }
+  __device__ __forceinline__ int ncta() const { return n; }
+  __device__ void sync() {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (atomicAdd(&bar[0], 1u) == (unsigned)n - 1) {
+        atomicExch(&bar[0], 0u);
+        __threadfence();
+        atomicAdd(&bar[1], 1u);
+      } else {
+        const volatile unsigned *vg = bar + 1;
+        const volatile int32_t *vs = status;
+        long spins = 0;
+        while (*vg == gen && *vs == 0) {
+          if (++spins > FS_GROUP_SPIN_LIMIT) { atomicExch(status, 1); break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    gen++;
+    __syncthreads();
+  }
+};
+
+// grid_sum2 over the CTAs of C
+template <class CT>
+__device__ void ctas_sum2(CT &C, double *part, int buf, double a0, double a1, double &o0, double &o1) {
+  const int G = C.ncta();
+  double b0 = block_sum_all(a0), b1 = block_sum_all(a1);
+  if (threadIdx.x == 0) { part[(2 * buf) * G + C.cta()] = b0; part[(2 * buf + 1) * G + C.cta()] = b1; }
+  C.sync();
+  double s0 = 0., s1 = 0.;
+  for (int q = threadIdx.x; q < G; q += blockDim.x) { s0 += part[(2 * buf) * G + q]; s1 += part[(2 * buf + 1) * G + q]; }
+  o0 = block_sum_all(s0);
+  o1 = block_sum_all(s1);
+}
+
+template <class CT>
+__device__ __forceinline__ void sor3_body(const Sor3Args &a, CT &C) {
   const int N = a.N;
-  const long tid0 = (long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long)gridDim.x * blockDim.x;
+  const long tid0 = (long)C.cta() * blockDim.x + threadIdx.x, nth = (long)C.ncta() * blockDim.x;
   const int32_t *__restrict__ cn = a.cn;
   const double *__restrict__ anb = a.anb;
   double ires[3], fres[3];
@@ -361,7 +418,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor3_colour(S
             if (act[c] && h2) a.x3[c * (long)N + i2] = m[c] / a.ac3[c * (long)N + i2];
           }
         }
-        grid.sync();
+        C.sync();
       }
     }
     double s0 = 0., s1 = 0., s2 = 0.;
@@ -379,13 +436,37 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor3_colour(S
       if (h2) { s0 += fabs(m[0]); s1 += fabs(m[1]); s2 += fabs(m[2]); }
     }
     double o0, o1, o2, d;
-    grid_sum2(grid, a.part, buf, s0, s1, o0, o1);
-    grid_sum2(grid, a.part, buf + 1, s2, 0., o2, d);
+    ctas_sum2(C, a.part, buf, s0, s1, o0, o1);
+    ctas_sum2(C, a.part, buf + 1, s2, 0., o2, d);
     buf = buf == 0 ? 2 : 0;
     double o[3] = {o0, o1, o2};
     for (int c = 0; c < 3; c++) if (act[c]) { fres[c] = o[c]; iters[c]++; }
   }
   if (tid0 == 0) for (int c = 0; c < 3; c++) a.iters3[c] = iters[c];
+}
+
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor3_colour(Sor3Args a) {
+  GridCtas C;
+  sor3_body(a, C);
+}
+
+// the multi-RHS SOR solves of n systems in one cooperative launch: CTAs
+// [start[q], start[q+1]) solve system q (an ensemble's momentum solves); a
+// system's barrier timeout is recorded in status[q][0]
+__global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB)
+    k_sor3_colour_batch(const Sor3Args *__restrict__ as, const int32_t *__restrict__ start, int n, unsigned *gbar,
+                        int32_t *const *__restrict__ status) {
+  __shared__ int sq;
+  if (threadIdx.x == 0) {
+    int q = 0;
+    while (q + 1 < n && (int)blockIdx.x >= start[q + 1]) q++;
+    sq = q;
+  }
+  __syncthreads();
+  const int q = sq;
+  GroupCtas C{(int)blockIdx.x - start[q], start[q + 1] - start[q], gbar + 2 * q, status[q], 0u};
+  const Sor3Args a = as[q];
+  sor3_body(a, C);
 }
 
 __global__ void k_to_colour3(int N, const int32_t *__restrict__ rows, const int32_t *__restrict__ ncfP,
@@ -1249,6 +1330,12 @@ int fs_momentum_batched_solve(fs_ctx *ctx) {
   a.ac3 = ctx->ac3P; a.anb = ctx->anbP; a.bc3 = ctx->bc3P; a.x3 = ctx->x3P; a.part = ctx->red;
   a.ires3 = ctx->resblk + RB_ABS; a.rrf = ctx->cfg.rrf_mom; a.itmax = ctx->cfg.itmax_mom; a.ncolors = ctx->ncolors;
   a.iters3 = ctx->d_iters;
+  if (ctx->mom_defer) {   // launched with other contexts' by fs_mom_batch_launch, then fs_momentum_batched_finish
+    static_assert(sizeof(Sor3Args) <= sizeof(ctx->mom_pend), "mom_pend too small");
+    memcpy(ctx->mom_pend, &a, sizeof(a));
+    ctx->mom_pending = true;
+    return FS_OK;
+  }
   int G = ctx->coop_grid;
   long need = (N + fs_coop_block(ctx) - 1) / fs_coop_block(ctx);
   if (need < G) G = (int)(need < 1 ? 1 : need);
@@ -1257,8 +1344,105 @@ int fs_momentum_batched_solve(fs_ctx *ctx) {
   FS_CK(fs_coop_launch((const void *)k_sor3_colour, G, fs_coop_block(ctx), args, ctx->st));
   FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[0][1], ctx->st)));
   FS_LAUNCH_CHECK();
+  return fs_momentum_batched_finish(ctx);
+}
+
+int fs_momentum_batched_finish(fs_ctx *ctx) {
+  const int N = ctx->N;
   k_from_colour3<<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(N, ctx->cposP, ctx->x3P, ctx->u, ctx->v, ctx->w);
   FS_LAUNCH_CHECK();
   FS_TIMING(FS_CK(cudaEventRecord(ctx->sev[0][1], ctx->st)); ctx->s_pending[0] = true);
+  return FS_OK;
+}
+
+std::vector<int32_t> fs_cta_split(int cap, const double *weight, int n) {
+  double wsum = 0.;
+  for (int q = 0; q < n; q++) wsum += std::max(weight[q], 0.);
+  std::vector<int> cnt(n, 1);
+  const int left = cap - n;
+  if (wsum > 0. && left > 0) {
+    std::vector<double> rem(n);
+    int given = 0;
+    for (int q = 0; q < n; q++) {
+      const double share = left * std::max(weight[q], 0.) / wsum;
+      const int k = (int)share;
+      cnt[q] += k; given += k; rem[q] = share - k;
+    }
+    std::vector<int> order(n);
+    for (int q = 0; q < n; q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return rem[x] > rem[y]; });
+    for (int j = 0; j < left - given && j < n; j++) cnt[order[j]]++;
+  }
+  std::vector<int32_t> start(n + 1, 0);
+  for (int q = 0; q < n; q++) start[q + 1] = start[q] + cnt[q];
+  return start;
+}
+
+struct fs_mom_batch {
+  int n = 0, ncta = 0;
+  Sor3Args *h_args = nullptr;   // pinned, copied to d_args by each launch
+  Sor3Args *d_args = nullptr;
+  int32_t *d_start = nullptr;
+  unsigned *d_words = nullptr;  // 2n group-barrier words (zero at each launch)
+  int32_t **d_status = nullptr;
+};
+
+void fs_mom_batch_free(fs_mom_batch *B) {
+  if (!B) return;
+  if (B->h_args) cudaFreeHost(B->h_args);
+  if (B->d_args) cudaFree(B->d_args);
+  if (B->d_start) cudaFree(B->d_start);
+  if (B->d_words) cudaFree(B->d_words);
+  if (B->d_status) cudaFree(B->d_status);
+  delete B;
+}
+
+int fs_mom_batch_create(fs_ctx **cs, int n, const double *weight, fs_mom_batch **out) {
+  if (!cs || n < 1 || !weight || !out) return FS_E_ARG;
+  *out = nullptr;
+  fs_ctx *ctx = cs[0];
+  for (int q = 0; q < n; q++)
+    if (!cs[q]->cfg.batched_momentum || cs[q]->cfg.solver_mom != FS_SOLVER_SOR) {
+      ctx->err = "a batched momentum launch needs the multi-RHS SOR solve in every context";
+      return FS_E_UNSUPPORTED;
+    }
+  int occ = 0;
+  FS_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)k_sor3_colour_batch, FS_COOP_BLOCK, 0));
+  const int cap = std::min(ctx->num_sms * std::max(occ, 0), FS_RED_BLOCKS);
+  if (cap < n) { ctx->err = "more contexts than co-resident CTAs for a batched momentum launch"; return FS_E_UNSUPPORTED; }
+  const std::vector<int32_t> start = fs_cta_split(cap, weight, n);
+  std::vector<int32_t *> st(n);
+  for (int q = 0; q < n; q++) st[q] = cs[q]->d_status;
+  fs_mom_batch *B = new fs_mom_batch;
+  B->n = n; B->ncta = start[n];
+  cudaError_t e;
+  if ((e = cudaHostAlloc((void **)&B->h_args, sizeof(Sor3Args) * n, cudaHostAllocDefault)) != cudaSuccess ||
+      (e = cudaMalloc(&B->d_args, sizeof(Sor3Args) * n)) != cudaSuccess ||
+      (e = cudaMalloc(&B->d_start, sizeof(int32_t) * (n + 1))) != cudaSuccess ||
+      (e = cudaMalloc(&B->d_words, sizeof(unsigned) * 2 * n)) != cudaSuccess ||
+      (e = cudaMalloc(&B->d_status, sizeof(int32_t *) * n)) != cudaSuccess ||
+      (e = cudaMemcpy(B->d_start, start.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(B->d_status, st.data(), sizeof(int32_t *) * n, cudaMemcpyHostToDevice)) != cudaSuccess) {
+    ctx->err = std::string("batched momentum set-up: ") + cudaGetErrorString(e);
+    fs_mom_batch_free(B);
+    return FS_E_CUDA;
+  }
+  *out = B;
+  return FS_OK;
+}
+
+int fs_mom_batch_launch(fs_mom_batch *B, fs_ctx **cs, int n, cudaStream_t st) {
+  if (!B || !cs || n != B->n) return FS_E_ARG;
+  fs_ctx *ctx = cs[0];
+  for (int q = 0; q < n; q++) {
+    if (!cs[q]->mom_pending) { ctx->err = "batched momentum launch: a context prepared no solve"; return FS_E_ARG; }
+    memcpy(&B->h_args[q], cs[q]->mom_pend, sizeof(Sor3Args));
+    cs[q]->mom_pending = false;
+  }
+  FS_CK(cudaMemcpyAsync(B->d_args, B->h_args, sizeof(Sor3Args) * n, cudaMemcpyHostToDevice, st));
+  FS_CK(cudaMemsetAsync(B->d_words, 0, sizeof(unsigned) * 2 * n, st));
+  void *args[] = {&B->d_args, &B->d_start, &B->n, &B->d_words, &B->d_status};
+  FS_CK(fs_coop_launch((const void *)k_sor3_colour_batch, B->ncta, FS_COOP_BLOCK, args, st));
+  FS_LAUNCH_CHECK();
   return FS_OK;
 }

@@ -544,14 +544,18 @@ int fs_set_launch_shape(fs_ctx *ctx, int shape);
 int fs_test_wait_timeout(fs_ctx *ctx, int extra);
 int fs_ensemble_run(fs_ctx **ctxs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
                     float *ms_out);
-/* fs_ensemble_run_batched: the same, except that inside each iteration every
- * case runs up to its p' solve, then the p' solves of all cases run as ONE
- * cooperative launch in which each case has its own group of CTAs (sized in
- * proportion to its cells times its p' iterations in the warm-up) and its own
- * bounded barriers, and then every case finishes its iteration.  All cases
- * must use the same AMG-BiCGSTAB p' solver form (FS_E_UNSUPPORTED otherwise).
- * The Krylov reductions of a case then run over its group rather than the whole
- * grid, so results differ from fs_ensemble_run's within the p' tolerance. */
+/* fs_ensemble_run_batched: the same with the cases concurrent.  Inside each
+ * iteration the p' solves of all cases (initial-guess fit, then the Krylov
+ * solve) run as ONE cooperative launch in which each case has its own group of
+ * CTAs (sized in proportion to its cells times its p' iterations in the
+ * warm-up) and its own bounded barriers; when every case uses the multi-RHS
+ * momentum SOR, the momentum solves are one such launch too (groups by cells),
+ * and the cases' other kernels run as concurrent graph branches between the
+ * launches (the part after the p' solve stays in sequence for cases with
+ * k-epsilon or the temperature equation).  All cases must use the same
+ * AMG-BiCGSTAB p' solver form (FS_E_UNSUPPORTED otherwise).  A case's sums then
+ * run over its group rather than the whole grid, so results differ from
+ * fs_ensemble_run's within the linear solvers' tolerances. */
 int fs_ensemble_run_batched(fs_ctx **ctxs, int n, int iters, int launches, double *source_out,
                             int32_t *pc_iters_out, float *ms_out);
 
