@@ -13,15 +13,17 @@
 //   y          = h w_out + b_out ;  guess = (y - mean y) * rms(previous p')
 //
 // The layer products [h, m] (N x 128) x W_l (128 x 64) and their backward
-// products (dW = A^T dz, dA = dz W^T) run on the tensor cores as BF16 operands
-// with FP32 accumulation (mma.sync m16n8k16); activations, the gather, the
-// small input/output layers and the optimiser are FP32.  The products are
-// skinny (K = 128, N = 64) and the layer kernels move ~0.5 KB per row, so they
-// are bounded by HBM, not by the tensor pipe.
+// products (dW = A^T dz, dA = dz W^T) run on the 5th-generation tensor cores
+// (tcgen05.mma, BF16 operands staged in shared memory in the UMMA canonical
+// layout, FP32 accumulators in TMEM); activations, the gather, the small
+// input/output layers and the optimiser are FP32.  The products are skinny
+// (K = 128, N = 64) and the layer kernels move ~0.5 KB per row, so they are
+// bounded by the neighbour gather, not by the tensor pipe.
 //
-// The p' solver scales the guess by the c minimising |b - c A x0| and iterates to
-// its usual tolerance; a host policy (fs_nn_before_pc) keeps the guess only
-// while it reduces iterations against zero-start probes.
+// The p' solver takes the guess into the basis of its least-squares initial
+// guess (k_guess_fit) and iterates to its usual tolerance; a host policy
+// (fs_nn_before_pc) keeps the guess only while it reduces iterations against
+// zero-start probes.
 //
 // Training: supervised on snapshots the plain solver captures (features,
 // edge weights, converged p' normalised by rms(previous p')), loss
@@ -39,9 +41,6 @@
 #define NN_L 4
 #define NN_TM 128           // rows per tile of the layer kernels
 #define NN_THREADS 256
-#define NN_APAD (NN_K + 8)  // smem row pitch of the [h, m] tile (bf16)
-#define NN_WPAD (NN_K + 8)  // smem row pitch of W^T (64 x 128)
-#define NN_DPAD (NN_H + 8)  // smem row pitch of dz and W (rows of 64)
 #define NN_RED 296          // CTAs of the reduction-style kernels
 
 #define NN_OFF_WIN 0
@@ -283,56 +282,8 @@ __global__ void __launch_bounds__(NN_THREADS) k_nn_in_bwd(int N, const float *X,
 }
 
 // ---------------------------------------------------------------- tensor-core helpers
-__device__ __forceinline__ uint32_t ld2(const bf16 *p) { return *(const uint32_t *)p; }
 __device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
   return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
-}
-// D = A(16x16, row) * B(16x8, col) + C, BF16 operands, FP32 accumulators
-__device__ __forceinline__ void mma16816(float *d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                         uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-// stage the [h, m] tile (rows i0..i0+127) into smem as bf16: m = sum_j w_ij h_j
-__device__ void stage_hm(int N, int W, const int32_t *__restrict__ cn, const float *__restrict__ wgt,
-                         const float *__restrict__ H, long i0, bf16 *A) {
-  const int rr = threadIdx.x >> 1, q = threadIdx.x & 1;
-  const long i = i0 + rr;
-  bf16 *arow = A + rr * NN_APAD;
-  float acc[32];
-#pragma unroll
-  for (int c = 0; c < 32; c++) acc[c] = 0.f;
-  if (i < N) {
-    const float4 *hs = (const float4 *)(H + i * NN_H + q * 32);
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      float4 v = hs[c];
-      arow[q * 32 + 4 * c] = __float2bfloat16(v.x);
-      arow[q * 32 + 4 * c + 1] = __float2bfloat16(v.y);
-      arow[q * 32 + 4 * c + 2] = __float2bfloat16(v.z);
-      arow[q * 32 + 4 * c + 3] = __float2bfloat16(v.w);
-    }
-    for (int j = 0; j < W; j++) {
-      int k = cn[(long)j * N + i];
-      if (k < 0) continue;
-      float w = wgt[(long)j * N + i];
-      const float4 *hk = (const float4 *)(H + (long)k * NN_H + q * 32);
-#pragma unroll
-      for (int c = 0; c < 8; c++) {
-        float4 v = hk[c];
-        acc[4 * c] += w * v.x; acc[4 * c + 1] += w * v.y; acc[4 * c + 2] += w * v.z; acc[4 * c + 3] += w * v.w;
-      }
-    }
-  } else {
-#pragma unroll
-    for (int c = 0; c < 32; c++) arow[q * 32 + c] = __float2bfloat16(0.f);
-  }
-#pragma unroll
-  for (int c = 0; c < 32; c++) arow[NN_H + q * 32 + c] = __float2bfloat16(acc[c]);
 }
 
 // ---------------------------------------------------------------- layer forward (tcgen05)
@@ -518,111 +469,209 @@ __global__ void __launch_bounds__(NN_THREADS) k_nn_layer_fwd(int N, int W, const
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NN_TC_COLS) : "memory");
 }
 
-// ---------------------------------------------------------------- layer backward (a)
-// dz = dHout * mask ; partial dW += [h, m]^T dz, db += sum dz ;
-// dHin = dHout + (dz W^T)[:, :64] ; DM = (dz W^T)[:, 64:].  Persistent over tiles.
-__global__ void __launch_bounds__(NN_THREADS) k_nn_layer_bwd(int N, int W, const int32_t *__restrict__ cn,
-                                                             const float *__restrict__ wgt, const float *Hin,
-                                                             const uint8_t *__restrict__ mask, const float *dHout,
-                                                             const bf16 *__restrict__ wr, float *dHin, float *DM,
-                                                             float *part, int pstride) {
+// ---------------------------------------------------------------- layer backward (tcgen05)
+// The same backward on the 5th-generation tensor cores, persistent over tiles:
+//   dW (128 x 64) += [h, m]^T dz: UMMA M = 128 features, N = 64, K = the tile's
+//     128 rows; operands [h, m]^T and dz^T staged K-major (rows contiguous),
+//     accumulated in TMEM columns 128..191 across all of the CTA's tiles;
+//   dA (128 x 128) = dz W^T: UMMA M = 128 rows, N = 128 features, K = 64;
+//     operands dz and W staged K-major (outputs contiguous), TMEM columns 0..127,
+//     read back per tile: dHin = dHout + dA[:, :64], DM = dA[:, 64:].
+// One thread issues the twelve K=16 steps of a tile and commits them to an
+// mbarrier (one phase per tile); the waits are bounded as in the forward.
+__device__ __forceinline__ int canon64_off(int row, int k) { return (row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2; }
+__device__ __forceinline__ uint64_t umma_desc64(uint32_t saddr) {   // K-major, 8 K chunks per row group
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+constexpr uint32_t NN_IDESC_DA = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NN_K >> 3) << 17) |
+                                 ((uint32_t)(NN_TM >> 4) << 24);   // M = 128, N = 128
+#define NN_TC_BWD_COLS 256   // dA in columns 0..127, dW in 128..191
+
+__device__ __forceinline__ void tmem_ld32(uint32_t ta, uint32_t *v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(ta)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, int acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
+      "}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+}
+
+__global__ void __launch_bounds__(NN_THREADS) k_nn_layer_bwd_tc(int N, int W, const int32_t *__restrict__ cn,
+                                                                const float *__restrict__ wgt, const float *Hin,
+                                                                const uint8_t *__restrict__ mask, const float *dHout,
+                                                                const bf16 *__restrict__ wr, float *dHin, float *DM,
+                                                                float *part, int pstride, int32_t *status) {
   extern __shared__ __align__(16) unsigned char smem[];
-  bf16 *A = (bf16 *)smem;                       // 128 x NN_APAD   ([h, m])
-  bf16 *DZ = A + NN_TM * NN_APAD;               // 128 x NN_DPAD   (dz)
-  bf16 *WR = DZ + NN_TM * NN_DPAD;              // 128 x NN_DPAD   (W, rows = input features)
+  unsigned char *AT = smem + ((128u - (smem_u32(smem) & 127u)) & 127u);   // [h, m]^T: 128 features x 128 rows (32 KB)
+  unsigned char *DZT = AT + NN_K * NN_TM * 2;                             // dz^T: 64 outputs x 128 rows (16 KB)
+  unsigned char *DZ = DZT + NN_H * NN_TM * 2;                             // dz: 128 rows x 64 outputs (16 KB)
+  unsigned char *WC = DZ + NN_TM * NN_H * 2;                              // W: 128 features x 64 outputs (16 KB)
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tbase;
   __shared__ float shb[4][NN_H];
-  for (int q = threadIdx.x; q < NN_K * NN_H; q += blockDim.x) {
-    int n = q / NN_H, k = q - n * NN_H;
-    WR[n * NN_DPAD + k] = wr[q];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tbase)),
+                 "r"(NN_TC_BWD_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int q = threadIdx.x; q < NN_K * NN_H; q += blockDim.x) {   // W, rows = input features
+    const int f = q / NN_H, o = q - f * NN_H;
+    *(bf16 *)(WC + canon64_off(f, o)) = wr[q];
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tbase;
   const int c = threadIdx.x & (NN_H - 1), rg = threadIdx.x >> 6;
-  float accW[8][4];
-#pragma unroll
-  for (int nt = 0; nt < 8; nt++) accW[nt][0] = accW[nt][1] = accW[nt][2] = accW[nt][3] = 0.f;
   float db = 0.f;
+  bool ok = true;
+  int it = 0;
   const long ntiles = ((long)N + NN_TM - 1) / NN_TM;
-  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, it++) {
     const long i0 = tile * NN_TM;
-    __syncthreads();
-    stage_hm(N, W, cn, wgt, Hin, i0, A);
+    // [h, m]^T: each thread forms half of one row's 128 features, stored transposed
+    {
+      const int rr = threadIdx.x >> 1, qh = threadIdx.x & 1;
+      const long i = i0 + rr;
+      float hv[32], acc[32];
+#pragma unroll
+      for (int e = 0; e < 32; e++) { hv[e] = 0.f; acc[e] = 0.f; }
+      if (i < N) {
+        const float4 *hs = (const float4 *)(Hin + i * NN_H + qh * 32);
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+          const float4 v = hs[e];
+          hv[4 * e] = v.x; hv[4 * e + 1] = v.y; hv[4 * e + 2] = v.z; hv[4 * e + 3] = v.w;
+        }
+        for (int j = 0; j < W; j++) {
+          const int k = cn[(long)j * N + i];
+          if (k < 0) continue;
+          const float w = wgt[(long)j * N + i];
+          const float4 *hk = (const float4 *)(Hin + (long)k * NN_H + qh * 32);
+#pragma unroll
+          for (int e = 0; e < 8; e++) {
+            const float4 v = hk[e];
+            acc[4 * e] += w * v.x; acc[4 * e + 1] += w * v.y; acc[4 * e + 2] += w * v.z; acc[4 * e + 3] += w * v.w;
+          }
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 32; e++) {
+        *(bf16 *)(AT + canon_off(qh * 32 + e, rr)) = __float2bfloat16(hv[e]);
+        *(bf16 *)(AT + canon_off(NN_H + qh * 32 + e, rr)) = __float2bfloat16(acc[e]);
+      }
+    }
+    // dz = dHout * mask, as dz (rows x outputs) and dz^T
     for (int rr = rg; rr < NN_TM; rr += 4) {
       const long i = i0 + rr;
       float dz = 0.f;
       if (i < N && mask[i * NN_H + c]) dz = dHout[i * NN_H + c];
       db += dz;
-      DZ[rr * NN_DPAD + c] = __float2bfloat16(dz);
+      const bf16 b = __float2bfloat16(dz);
+      *(bf16 *)(DZ + canon64_off(rr, c)) = b;
+      *(bf16 *)(DZT + canon_off(c, rr)) = b;
     }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    // dW (features f0..f0+15 of warp) += A^T dz over the 128 rows of the tile
-    {
-      const int f0 = warp * 16;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (threadIdx.x == 0) {
+      const uint32_t at = smem_u32(AT), dzt = smem_u32(DZT), dz = smem_u32(DZ), wc = smem_u32(WC);
 #pragma unroll
-      for (int kk = 0; kk < NN_TM / 16; kk++) {
-        const int k0 = kk * 16;
-        uint32_t a0 = pack2(A[(k0 + 2 * t) * NN_APAD + f0 + g], A[(k0 + 2 * t + 1) * NN_APAD + f0 + g]);
-        uint32_t a1 = pack2(A[(k0 + 2 * t) * NN_APAD + f0 + g + 8], A[(k0 + 2 * t + 1) * NN_APAD + f0 + g + 8]);
-        uint32_t a2 = pack2(A[(k0 + 2 * t + 8) * NN_APAD + f0 + g], A[(k0 + 2 * t + 9) * NN_APAD + f0 + g]);
-        uint32_t a3 = pack2(A[(k0 + 2 * t + 8) * NN_APAD + f0 + g + 8], A[(k0 + 2 * t + 9) * NN_APAD + f0 + g + 8]);
+      for (int kk = 0; kk < NN_TM / 16; kk++)
+        umma_f16(tmem + 128, umma_desc(at + kk * 256), umma_desc(dzt + kk * 256), NN_IDESC, (it > 0 || kk > 0) ? 1 : 0);
 #pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-          const int n0 = nt * 8;
-          uint32_t b0 = pack2(DZ[(k0 + 2 * t) * NN_DPAD + n0 + g], DZ[(k0 + 2 * t + 1) * NN_DPAD + n0 + g]);
-          uint32_t b1 = pack2(DZ[(k0 + 2 * t + 8) * NN_DPAD + n0 + g], DZ[(k0 + 2 * t + 9) * NN_DPAD + n0 + g]);
-          mma16816(accW[nt], a0, a1, a2, a3, b0, b1);
+      for (int kk = 0; kk < NN_H / 16; kk++)
+        umma_f16(tmem, umma_desc64(dz + kk * 256), umma_desc64(wc + kk * 256), NN_IDESC_DA, kk > 0 ? 1 : 0);
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mbar))
+                   : "memory");
+    }
+    uint32_t done = 0;
+    for (long spin = 0; spin < NN_TC_SPIN && !done; spin++) {
+      asm volatile(
+          "{\n\t.reg .pred P1;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+          "selp.b32 %0, 1, 0, P1;\n\t"
+          "}\n"
+          : "=r"(done)
+          : "r"(smem_u32(&mbar)), "r"((uint32_t)(it & 1))
+          : "memory");
+    }
+    // one verdict for the whole CTA, so every thread takes the same path
+    // through the remaining block barriers
+    done = __syncthreads_and(done);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!done) {
+      if (threadIdx.x == 0) atomicExch(status, 1);
+      ok = false;
+    } else {
+      // warp w: TMEM lanes 32 (w % 4) .. +31 (rows of the tile), columns 64 (w / 4) .. +63 of dA
+      const int rowq = warp & 3, half = warp >> 2;
+      const long i = i0 + 32 * rowq + lane;
+#pragma unroll
+      for (int part32 = 0; part32 < 2; part32++) {
+        uint32_t v[32];
+        const int col0 = 64 * half + 32 * part32;
+        tmem_ld32(tmem + ((uint32_t)(32 * rowq) << 16) + (uint32_t)col0, v);
+        if (i < N) {
+          if (half == 0) {
+            const float4 *dh = (const float4 *)(dHout + i * NN_H + col0);
+            float4 *out = (float4 *)(dHin + i * NN_H + col0);
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+              const float4 d = dh[e];
+              out[e] = make_float4(d.x + __uint_as_float(v[4 * e]), d.y + __uint_as_float(v[4 * e + 1]),
+                                   d.z + __uint_as_float(v[4 * e + 2]), d.w + __uint_as_float(v[4 * e + 3]));
+            }
+          } else {
+            float4 *out = (float4 *)(DM + i * NN_H + (col0 - NN_H));
+#pragma unroll
+            for (int e = 0; e < 8; e++)
+              out[e] = make_float4(__uint_as_float(v[4 * e]), __uint_as_float(v[4 * e + 1]),
+                                   __uint_as_float(v[4 * e + 2]), __uint_as_float(v[4 * e + 3]));
+          }
         }
       }
     }
-    // dA = dz W^T for the warp's 16 rows, in two halves of 64 columns
-    const int r0 = warp * 16;
-#pragma unroll
-    for (int half = 0; half < 2; half++) {
-      float acc[8][4];
-#pragma unroll
-      for (int nt = 0; nt < 8; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-#pragma unroll
-      for (int kk = 0; kk < NN_H / 16; kk++) {
-        const int k0 = kk * 16;
-        uint32_t a0 = ld2(DZ + (r0 + g) * NN_DPAD + k0 + 2 * t);
-        uint32_t a1 = ld2(DZ + (r0 + g + 8) * NN_DPAD + k0 + 2 * t);
-        uint32_t a2 = ld2(DZ + (r0 + g) * NN_DPAD + k0 + 2 * t + 8);
-        uint32_t a3 = ld2(DZ + (r0 + g + 8) * NN_DPAD + k0 + 2 * t + 8);
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-          const int n0 = half * NN_H + nt * 8;
-          uint32_t b0 = ld2(WR + (n0 + g) * NN_DPAD + k0 + 2 * t);
-          uint32_t b1 = ld2(WR + (n0 + g) * NN_DPAD + k0 + 2 * t + 8);
-          mma16816(acc[nt], a0, a1, a2, a3, b0, b1);
-        }
-      }
-#pragma unroll
-      for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const int row = r0 + g + (e >= 2 ? 8 : 0), col = nt * 8 + 2 * t + (e & 1);
-          const long i = i0 + row;
-          if (i >= N) continue;
-          if (half == 0) dHin[i * NN_H + col] = dHout[i * NN_H + col] + acc[nt][e];
-          else DM[i * NN_H + col] = acc[nt][e];
-        }
-    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
-  // partials: dW (128 x 64) then db (64)
+  // partials: dW (128 features x 64) from TMEM, then db (64)
   float *pp = part + (long)blockIdx.x * pstride;
-  {
-    const int f0 = warp * 16;
+  if (ok) {
+    const int rowq = warp & 3, half = warp >> 2;
+    uint32_t v[32];
+    tmem_ld32(tmem + ((uint32_t)(32 * rowq) << 16) + (uint32_t)(128 + 32 * half), v);
+    const int f = 32 * rowq + lane;
 #pragma unroll
-    for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int f = f0 + g + (e >= 2 ? 8 : 0), col = nt * 8 + 2 * t + (e & 1);
-        pp[f * NN_H + col] = accW[nt][e];
-      }
+    for (int e = 0; e < 32; e++) pp[f * NN_H + 32 * half + e] = it > 0 ? __uint_as_float(v[e]) : 0.f;
   }
-  __syncthreads();
   shb[rg][c] = db;
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (rg == 0) pp[NN_K * NN_H + c] = shb[0][c] + shb[1][c] + shb[2][c] + shb[3][c];
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NN_TC_BWD_COLS) : "memory");
 }
 
 // layer backward (b): dHin[j] += sum_s w_js DM[cn(j,s)] (the aggregation is symmetric)
@@ -682,7 +731,7 @@ __global__ void k_nn_guess(int N, const float *y, const double *sumy, const doub
 
 // ================================================================ host
 static const size_t NN_SMEM_FWD = sizeof(bf16) * (NN_TM * NN_K + NN_H * NN_K) + 128;   // canonical tiles + alignment slack
-static const size_t NN_SMEM_BWD = sizeof(bf16) * (NN_TM * NN_APAD + NN_TM * NN_DPAD + NN_K * NN_DPAD);
+static const size_t NN_SMEM_BWD = sizeof(bf16) * (NN_K * NN_TM + 2 * NN_H * NN_TM + NN_K * NN_H) + 128;   // canonical tiles + slack
 static const int NN_PSTRIDE = NN_K * NN_H + NN_H;
 
 static int nn_sum_rows(fs_ctx *ctx, fs_nn *nn, SumArgs s, double *out, int mode) {
@@ -757,9 +806,9 @@ static int nn_backward(fs_ctx *ctx, const float *X, const float *wgt, const floa
   const int G = std::min(tiles, NN_RED);
   float *dcur = nn->dH, *dnext = nn->dH2;
   for (int l = NN_L - 1; l >= 0; l--) {
-    k_nn_layer_bwd<<<G, NN_THREADS, NN_SMEM_BWD, ctx->st>>>(N, W, ctx->cn, wgt, nn->H[l], nn->mask[l + 1], dcur,
-                                                            nn->wr + (size_t)l * NN_K * NN_H, dnext, nn->DM,
-                                                            nn->part, NN_PSTRIDE);
+    k_nn_layer_bwd_tc<<<G, NN_THREADS, NN_SMEM_BWD, ctx->st>>>(N, W, ctx->cn, wgt, nn->H[l], nn->mask[l + 1], dcur,
+                                                               nn->wr + (size_t)l * NN_K * NN_H, dnext, nn->DM,
+                                                               nn->part, NN_PSTRIDE, ctx->d_status);
     FS_LAUNCH_CHECK();
     k_nn_reduce<<<fs_grid(NN_PSTRIDE), FS_BLOCK, 0, ctx->st>>>(nn->part, G, NN_PSTRIDE, NN_PSTRIDE,
                                                                nn->grad + NN_OFF_L(l));
@@ -960,7 +1009,7 @@ extern "C" int fs_nn_create(fs_ctx *ctx, int snapshot_capacity, uint64_t seed) {
   FS_CK(cudaMemcpy(nn->theta, th.data(), sizeof(float) * NN_NP, cudaMemcpyHostToDevice));
   FS_CK(cudaFuncSetAttribute((const void *)k_nn_layer_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)NN_SMEM_FWD));
-  FS_CK(cudaFuncSetAttribute((const void *)k_nn_layer_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  FS_CK(cudaFuncSetAttribute((const void *)k_nn_layer_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)NN_SMEM_BWD));
   if ((rc = nn_pack(ctx))) return rc;
   FS_CK(cudaStreamSynchronize(ctx->st));

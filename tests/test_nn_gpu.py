@@ -16,8 +16,11 @@ def _solver(n=12, **kw):
     return Solver(mesh, case)
 
 
-def test_kernels_match_oracle():
-    s = _solver(12)
+@pytest.mark.parametrize("n", [12, 40])
+def test_kernels_match_oracle(n):
+    # 12^3: one 128-row tile per CTA of the persistent backward; 40^3 (500
+    # tiles over 296 CTAs): CTAs that accumulate dW over two tiles in TMEM
+    s = _solver(n)
     s.nn_create(0, seed=3)
     con = s.connectivity()
     W, N, F = s.W, s.N, s.F
