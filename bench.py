@@ -457,6 +457,7 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
     del cases
     t_setup = time.time() - t0
     shapes = ens.autotune(shapes=(1, 2, 3, 4), iters=1)
+    split = ens.autotune_split(exponents=(0.75, 1.0, 1.25), iters=2)
     launches = max(1, args.warmup)
     # both graph forms, each after one untimed launch of its own graph: cases in
     # sequence, and the p' solves of all cases in one launch (a CTA group each)
@@ -492,6 +493,8 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
                                   f"{args.ensemble_tol:g}, started from the least-squares combination of the 4 "
                                   f"previous p' solutions",
                        "launch_shapes_rank0": {str(k): shapes.count(k) for k in sorted(set(shapes))},
+                       "cta_split_exponent_rank0": split,
+                       "cta_split_ms_rank0": {str(k): round(v, 2) for k, v in ens.split_ms.items()},
                        "pc_launch": "the momentum solves of all cases in one cooperative launch and their p' "
                                     "solves in another, a CTA group per case; the other kernels of the cases as "
                                     "concurrent graph branches" if best else "the cases one after another",

@@ -185,6 +185,7 @@ PROTOTYPES = {
     "fs_test_wait_timeout": (C.c_int, [_V, C.c_int]),
     "fs_ensemble_run": (C.c_int, [C.POINTER(_V), C.c_int, C.c_int, C.c_int, _D, _I, C.POINTER(C.c_float)]),
     "fs_ensemble_run_batched": (C.c_int, [C.POINTER(_V), C.c_int, C.c_int, C.c_int, _D, _I, C.POINTER(C.c_float)]),
+    "fs_ensemble_split": (C.c_int, [_V, C.c_double]),
     "fs_phase_times": (C.c_int, [_V, C.POINTER(C.c_float)]),
     "fs_timer_start": (C.c_int, [_V]),
     "fs_timer_stop": (C.c_int, [_V, C.POINTER(C.c_float)]),

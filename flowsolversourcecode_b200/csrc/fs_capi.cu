@@ -805,7 +805,7 @@ static int ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *sou
     } while (c->nIter < c->cfg.niter_start_hr || c->hist_cnt < c->hist_cap);
     // the batched p' launch gives each case CTAs in proportion to its rows
     // times its last p' iterations
-    weight[q] = (double)c->N * std::max(1, r.lin_iters[FS_VAR_PC - 1]);
+    weight[q] = std::pow((double)c->N, ctx->ens_split) * std::max(1, r.lin_iters[FS_VAR_PC - 1]);
   }
   // batched: the multi-RHS momentum solves also go into one launch when every
   // case uses them; the parts of an iteration that have no cooperative kernel
@@ -817,7 +817,7 @@ static int ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *sou
   for (int q = 0; q < n; q++) {
     mom_b = mom_b && cs[q]->cfg.batched_momentum && cs[q]->cfg.solver_mom == FS_SOLVER_SOR;
     fork_post = fork_post && !cs[q]->turb && !cs[q]->energy;
-    mom_w[q] = (double)cs[q]->N;
+    mom_w[q] = std::pow((double)cs[q]->N, ctx->ens_split);
   }
   fs_pc_batch *PB = nullptr;
   fs_mom_batch *MB = nullptr;
@@ -969,6 +969,12 @@ int fs_ensemble_run(fs_ctx **cs, int n, int iters, int launches, double *source_
 int fs_ensemble_run_batched(fs_ctx **cs, int n, int iters, int launches, double *source_out, int32_t *pc_iters_out,
                             float *ms_out) {
   return ensemble_run(cs, n, iters, launches, source_out, pc_iters_out, ms_out, true);
+}
+
+int fs_ensemble_split(fs_ctx *ctx, double exponent) {
+  if (!ctx || !(exponent >= 0.) || exponent > 2.) return FS_E_ARG;
+  ctx->ens_split = exponent;
+  return FS_OK;
 }
 
 }  // extern "C"

@@ -182,6 +182,7 @@ struct fs_ctx {
   bool graph_mode = false;      // enqueueing for stream capture: no host syncs, no timing events
   bool pc_defer = false;        // the AMG-BiCGSTAB solve prepares its launch and leaves it to fs_pc_batch_launch
   bool mom_defer = false;       // the multi-RHS momentum solve prepares its launch for fs_mom_batch_launch
+  double ens_split = 1.;        // batched ensembles: CTA groups in proportion to cells^ens_split (x p' iterations)
   bool mom_pending = false;
   alignas(8) unsigned char mom_pend[160];   // the prepared launch's arguments (Sor3Args)
   int test_wait_extra = 0;      // fs_test_wait_timeout: extra arrivals the team barrier waits for

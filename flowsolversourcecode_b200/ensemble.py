@@ -103,6 +103,8 @@ class Ensemble:
         self.lib = self.solvers[0].lib
         self.cells = [s.N for s in self.solvers]
         self.shapes = [0] * len(self.solvers)
+        self.split = 1.0
+        self.split_ms = {}
 
     def autotune(self, shapes=(1, 2, 3, 4), iters: int = 2) -> list[int]:
         """Pick each case's cooperative launch shape (256 x shape threads on
@@ -122,6 +124,22 @@ class Ensemble:
             s.set_launch_shape(k)
             best.append(k)
         self.shapes = best
+        return best
+
+    def autotune_split(self, exponents=(0.5, 0.75, 1.0, 1.25), iters: int = 2) -> float:
+        """Pick the exponent of the CTA split of the batched form (groups in
+        proportion to cells^e) by timing one launch of an `iters`-iteration
+        graph per candidate; the fastest is kept."""
+        t = {}
+        for e in exponents:
+            L.check(self.lib.fs_ensemble_split(self.solvers[0].ctx, float(e)), self.solvers[0].ctx,
+                    "fs_ensemble_split")
+            t[e] = self.run(iters=iters, launches=1, batched=True)["ms"]
+        best = min(t, key=lambda e: (t[e], -e))
+        L.check(self.lib.fs_ensemble_split(self.solvers[0].ctx, float(best)), self.solvers[0].ctx,
+                "fs_ensemble_split")
+        self.split = best
+        self.split_ms = t
         return best
 
     def run(self, iters: int, launches: int = 1, batched: bool = False) -> dict:

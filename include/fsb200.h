@@ -558,6 +558,13 @@ int fs_ensemble_run(fs_ctx **ctxs, int n, int iters, int launches, double *sourc
  * fs_ensemble_run's within the linear solvers' tolerances. */
 int fs_ensemble_run_batched(fs_ctx **ctxs, int n, int iters, int launches, double *source_out,
                             int32_t *pc_iters_out, float *ms_out);
+/* fs_ensemble_split: the CTA groups of fs_ensemble_run_batched calls whose
+ * first context is ctx are sized in proportion to cells^exponent (momentum) and
+ * cells^exponent x warm-up p' iterations (p'); exponent in [0, 2], 1 by default.
+ * Below 1 small cases get more CTAs than their share of cells, which pays when
+ * their latency-bound phases, not bandwidth, set a group's time.  The project's
+ * autotuner (ensemble.py) picks it by timing.  No reference counterpart. */
+int fs_ensemble_split(fs_ctx *ctx, double exponent);
 
 /* Timing of the last outer iteration's phases in milliseconds (CUDA events):
  * [0] momentum assembly, [1] momentum solves, [2] continuity assembly,

@@ -86,3 +86,20 @@ def test_batched_run_rejects_mixed_solvers():
     with pytest.raises(FsError):
         ens.run(iters=1, launches=1, batched=True)
     ens.close()
+
+
+@pytest.mark.gpu
+def test_split_autotune_picks_a_candidate():
+    specs = [E.CaseSpec(10, 1.0, 400.0), E.CaseSpec(16, 1.0, 300.0)]
+    ens = E.Ensemble([E.build_case(s) for s in specs])
+    e = ens.autotune_split(exponents=(0.5, 1.0), iters=1)
+    assert e in (0.5, 1.0) and set(ens.split_ms) == {0.5, 1.0}
+    out = ens.run(iters=2, launches=1, batched=True)
+    assert np.all(np.isfinite(out["source"]))
+    ens.close()
+
+
+def test_split_exponent_rejects_out_of_range():
+    from flowsolversourcecode_b200 import _lib as L
+    lib = L.load()
+    assert lib.fs_ensemble_split(None, 1.0) == L.FS_E_ARG
