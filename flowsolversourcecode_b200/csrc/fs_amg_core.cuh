@@ -76,20 +76,37 @@ struct Sync {
     buf = (buf + 1) % 3;
   }
   // grid-deterministic sums of K <= FS_SUMK values, in the partial slots after
-  // the three buffers of sum2 (every CTA gets the same results)
-  __device__ void sumK(const double *in, double *out, int K) {
-    const int G = cta_count();
+  // the three buffers of sum2 (every CTA gets the same results), with one
+  // block barrier before and one after the grid barrier: warp sums into shared
+  // memory, thread k adds the warps' and then the CTAs' partials of value k in
+  // a fixed order
+  template <int K>
+  __device__ void sumKt(const double (&in)[K], double (&out)[K]) {
+    __shared__ double sh[K][33];
+    const int G = cta_count(), lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     double *pk = part + 6L * G;
+#pragma unroll
     for (int k = 0; k < K; k++) {
-      const double b = bsum(in[k]);
-      if (threadIdx.x == 0) pk[(long)k * G + cta_id()] = b;
+      const double v = wsum(in[k]);
+      if (lane == 0) sh[k][wid] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < K) {
+      const int k = threadIdx.x;
+      double t = 0.;
+      for (int w = 0; w < nw; w++) t += sh[k][w];
+      pk[(long)k * G + cta_id()] = t;
     }
     gbar();
-    for (int k = 0; k < K; k++) {
+    if ((int)threadIdx.x < K) {
+      const int k = threadIdx.x;
       double t = 0.;
-      for (int q = threadIdx.x; q < G; q += blockDim.x) t += pk[(long)k * G + q];
-      out[k] = bsum(t);
+      for (int q = 0; q < G; q++) t += pk[(long)k * G + q];
+      sh[k][32] = t;
     }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) out[k] = sh[k][32];
   }
   // grid-deterministic sums of three values, in three rotating buffers of
   // their own after the sumK slots
@@ -742,85 +759,114 @@ __device__ double rhs_mean(Sync &S, const AmgKArgs<R> &a) {
 // are solved by every CTA alike from grid-deterministic sums, by a Cholesky
 // factorisation with a relative diagonal shift.  x goes to a.x and fit[0] = 1;
 // a failed factorisation leaves fit[0] = 0 (the solve starts from zero).
-template <class R>
+template <class R, int NX>
 __device__ __forceinline__ void guess_fit_body(const AmgKArgs<R> a) {
+  constexpr int NG = NX * (NX + 1) / 2, K = NG + NX + 1;
   Sync S(a.part);
-  const int N = a.N, nx = a.nx;
-  const long t0 = (long)cta_id() * blockDim.x + threadIdx.x, nt = (long)cta_count() * blockDim.x;
   const double bmean = rhs_mean(S, a);
-  double c[FS_GUESS_MAX];
-  for (int j = 0; j < FS_GUESS_MAX; j++) c[j] = 0.;
-  bool fell_back = false;
+  double c[NX];
+  bool fell_back;
+  const int N = a.N, W = a.W;
+  const long t0 = (long)cta_id() * blockDim.x + threadIdx.x, nt = (long)cta_count() * blockDim.x;
+  const double *xs[NX];
+#pragma unroll
+  for (int j = 0; j < NX; j++) xs[j] = a.xs[j];
+  // Gram matrix G_jk = (A x_j).(A x_k) (upper triangle), g_j = (A x_j).b, |b|^2;
+  // each row of A is read once for all basis vectors, its slots in order
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) acc[k] = 0.;
+  for (long i = t0; i < N; i += nt) {
+    double y[NX];
+    const double aci = a.ac[i];
+#pragma unroll
+    for (int j = 0; j < NX; j++) { double t = 0.; t = t + aci * xs[j][i]; y[j] = t; }
+    for (int w0 = 0; w0 < W; w0 += 4) {
+      int kk[4];
+      double av[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const bool in = w0 + u < W;
+        kk[u] = in ? a.cn[(long)(w0 + u) * N + i] : -1;
+        av[u] = in ? a.anb[(long)(w0 + u) * N + i] : 0.;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (kk[u] >= 0)
+#pragma unroll
+          for (int j = 0; j < NX; j++) y[j] = y[j] + av[u] * xs[j][kk[u]];
+    }
+    const double b1 = a.bc[i] - bmean;
+    int q = 0;
+#pragma unroll
+    for (int j = 0; j < NX; j++)
+#pragma unroll
+      for (int k = j; k < NX; k++) acc[q++] += y[j] * y[k];
+#pragma unroll
+    for (int j = 0; j < NX; j++) acc[NG + j] += y[j] * b1;
+    acc[NG + NX] += b1 * b1;
+  }
+  double tot[K];
+  S.sumKt<K>(acc, tot);
+  // Cholesky of G + 1e-12 max(diag) I, then the two triangular solves (row-major L)
+  double L[NX][NX];
+  double dmax = 0.;
   {
-    // Gram matrix G_jk = (A x_j).(A x_k) (upper triangle), g_j = (A x_j).b, |b|^2
-    double acc[FS_SUMK];
-    const int ng = nx * (nx + 1) / 2;
-    for (int k = 0; k < ng + nx + 1; k++) acc[k] = 0.;
-    for (long i = t0; i < N; i += nt) {
-      double y[FS_GUESS_MAX];
-      for (int j = 0; j < nx; j++) {
-        const double *xj = a.xs[j];
-        double t = 0.;
-        t = t + a.ac[i] * xj[i];
-        y[j] = ell_acc<8, false>(t, a.N, a.W, a.cn, a.anb, i, [&](int k) { return xj[k]; });
-      }
-      const double b1 = a.bc[i] - bmean;
-      int q = 0;
-      for (int j = 0; j < nx; j++)
-        for (int k = j; k < nx; k++) acc[q++] += y[j] * y[k];
-      for (int j = 0; j < nx; j++) acc[ng + j] += y[j] * b1;
-      acc[ng + nx] += b1 * b1;
+    int q = 0;
+#pragma unroll
+    for (int j = 0; j < NX; j++)
+#pragma unroll
+      for (int k = j; k < NX; k++) { L[k][j] = tot[q]; if (k == j) dmax = fmax(dmax, tot[q]); q++; }
+  }
+  bool ok = dmax > 0. && isfinite(dmax);
+#pragma unroll
+  for (int j = 0; j < NX; j++) {
+    if (!ok) break;
+    double d = L[j][j] + 1e-12 * dmax;
+    for (int k = 0; k < j; k++) d -= L[j][k] * L[j][k];
+    if (!(d > 1e-14 * dmax)) { ok = false; break; }
+    d = sqrt(d);
+    L[j][j] = d;
+#pragma unroll
+    for (int r = j + 1; r < NX; r++) {
+      double v = L[r][j];
+      for (int k = 0; k < j; k++) v -= L[r][k] * L[j][k];
+      L[r][j] = v / d;
     }
-    double tot[FS_SUMK];
-    S.sumK(acc, tot, ng + nx + 1);
-    // Cholesky of G + 1e-12 max(diag) I, then the two triangular solves (row-major L)
-    double L[FS_GUESS_MAX * FS_GUESS_MAX];
-    double dmax = 0.;
-    {
-      int q = 0;
-      for (int j = 0; j < nx; j++)
-        for (int k = j; k < nx; k++) { L[k * FS_GUESS_MAX + j] = tot[q]; if (k == j) dmax = fmax(dmax, tot[q]); q++; }
+  }
+  if (ok) {
+    double z[NX];
+#pragma unroll
+    for (int j = 0; j < NX; j++) {
+      double v = tot[NG + j];
+      for (int k = 0; k < j; k++) v -= L[j][k] * z[k];
+      z[j] = v / L[j][j];
     }
-    bool ok = dmax > 0. && isfinite(dmax);
-    for (int j = 0; j < nx && ok; j++) {
-      double d = L[j * FS_GUESS_MAX + j] + 1e-12 * dmax;
-      for (int k = 0; k < j; k++) d -= L[j * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
-      if (!(d > 1e-14 * dmax)) { ok = false; break; }
-      d = sqrt(d);
-      L[j * FS_GUESS_MAX + j] = d;
-      for (int r = j + 1; r < nx; r++) {
-        double v = L[r * FS_GUESS_MAX + j];
-        for (int k = 0; k < j; k++) v -= L[r * FS_GUESS_MAX + k] * L[j * FS_GUESS_MAX + k];
-        L[r * FS_GUESS_MAX + j] = v / d;
-      }
+#pragma unroll
+    for (int j = NX - 1; j >= 0; j--) {
+      double v = z[j];
+      for (int k = j + 1; k < NX; k++) v -= L[k][j] * c[k];
+      c[j] = v / L[j][j];
     }
-    if (ok) {
-      double z[FS_GUESS_MAX];
-      for (int j = 0; j < nx; j++) {
-        double v = tot[ng + j];
-        for (int k = 0; k < j; k++) v -= L[j * FS_GUESS_MAX + k] * z[k];
-        z[j] = v / L[j * FS_GUESS_MAX + j];
-      }
-      for (int j = nx - 1; j >= 0; j--) {
-        double v = z[j];
-        for (int k = j + 1; k < nx; k++) v -= L[k * FS_GUESS_MAX + j] * c[k];
-        c[j] = v / L[j * FS_GUESS_MAX + j];
-      }
-      for (int j = 0; j < nx; j++) if (!isfinite(c[j])) ok = false;
-    }
-    if (!ok) for (int j = 0; j < nx; j++) c[j] = 0.;
-    fell_back = !ok;
-    for (long i = t0; i < N; i += nt) {
-      double xi = 0.;
-      for (int j = 0; j < nx; j++) xi += c[j] * a.xs[j][i];
-      a.x[i] = xi;
-    }
+#pragma unroll
+    for (int j = 0; j < NX; j++) if (!isfinite(c[j])) ok = false;
+  }
+  if (!ok)
+#pragma unroll
+    for (int j = 0; j < NX; j++) c[j] = 0.;
+  fell_back = !ok;
+  for (long i = t0; i < N; i += nt) {
+    double xi = 0.;
+#pragma unroll
+    for (int j = 0; j < NX; j++) xi += c[j] * xs[j][i];
+    a.x[i] = xi;
   }
   if (cta_id() == 0 && threadIdx.x == 0) {
     a.fit[0] = fell_back ? 0 : 1;
     if (a.nncnt) { a.nncnt[1] += 1; if (fell_back) a.nncnt[0] += 1; }
   }
 }
+
 
 // right-preconditioned BiCGSTAB (van der Vorst 1992) with a multigrid V-cycle:
 // MODE 0 run(), 2 run_gs() (multicolour Gauss-Seidel smoothing), 1 the fused

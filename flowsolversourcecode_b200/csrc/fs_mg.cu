@@ -377,9 +377,9 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK) k_mg_solve(MgSolveArgs a) {
 
 // the initial guess of k_amg_bicgstab on the whole cooperative grid
 // (guess_fit_body in fs_amg_core.cuh)
-template <class R>
+template <class R, int NX>
 __global__ void __launch_bounds__(FS_COOP_BLOCK, 1) k_guess_fit(AmgKArgs<R> a) {
-  g1::guess_fit_body<R>(a);
+  g1::guess_fit_body<R, NX>(a);
 }
 
 // right-preconditioned BiCGSTAB with the V-cycle on the whole cooperative grid
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_AMG_MINB)
 
 // the initial guesses of the batched solves, in the same CTA groups (a group
 // whose system has no basis vectors does nothing)
-template <class R>
+template <class R, int NX>
 __global__ void __launch_bounds__(FS_COOP_BLOCK, 1)
     k_guess_fit_batch(const AmgKArgs<R> *__restrict__ as, const int32_t *__restrict__ start, int n, unsigned *gbar) {
   gb::GroupState &G = gb::gstate();
@@ -431,7 +431,38 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, 1)
   }
   __syncthreads();
   const AmgKArgs<R> a = as[G.q];
-  if (a.nx > 0) gb::guess_fit_body<R>(a);
+  if (a.nx == NX) gb::guess_fit_body<R, NX>(a);   // groups of other basis sizes take another launch
+}
+
+// the fit kernels by basis size (1 .. FS_GUESS_MAX): each instance keeps its
+// sums in registers
+template <class R>
+static const void *guess_fit_kernel(int nx) {
+  switch (nx) {
+    case 1: return (const void *)k_guess_fit<R, 1>;
+    case 2: return (const void *)k_guess_fit<R, 2>;
+    case 3: return (const void *)k_guess_fit<R, 3>;
+    case 4: return (const void *)k_guess_fit<R, 4>;
+    case 5: return (const void *)k_guess_fit<R, 5>;
+    case 6: return (const void *)k_guess_fit<R, 6>;
+    case 7: return (const void *)k_guess_fit<R, 7>;
+    case 8: return (const void *)k_guess_fit<R, 8>;
+  }
+  return nullptr;
+}
+template <class R>
+static const void *guess_fit_batch_kernel(int nx) {
+  switch (nx) {
+    case 1: return (const void *)k_guess_fit_batch<R, 1>;
+    case 2: return (const void *)k_guess_fit_batch<R, 2>;
+    case 3: return (const void *)k_guess_fit_batch<R, 3>;
+    case 4: return (const void *)k_guess_fit_batch<R, 4>;
+    case 5: return (const void *)k_guess_fit_batch<R, 5>;
+    case 6: return (const void *)k_guess_fit_batch<R, 6>;
+    case 7: return (const void *)k_guess_fit_batch<R, 7>;
+    case 8: return (const void *)k_guess_fit_batch<R, 8>;
+  }
+  return nullptr;
 }
 
 // coarse matrix of level lc from level lc-1 (AssembleElementBasedAgglomoratedLHS.for:45-150)
@@ -956,7 +987,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     fill(a);
     a.lev = M->lev64;
     void *args[] = {&a};
-    if (a.nx > 0) FS_CK(fs_coop_launch((const void *)k_guess_fit<double>, G, fs_coop_block(ctx), args, ctx->st));
+    if (a.nx > 0) FS_CK(fs_coop_launch(guess_fit_kernel<double>(a.nx), G, fs_coop_block(ctx), args, ctx->st));
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     FS_CK(fs_coop_launch(fused ? (const void *)k_amg_bicgstab<double, 1> : (const void *)k_amg_bicgstab<double, 0>,
                          G, fs_coop_block(ctx), args, ctx->st));
@@ -965,7 +996,7 @@ int fs_mg_solve(fs_ctx *ctx, int nf, double rrf, int solver) {
     fill(a);
     a.lev = M->lev32;
     void *args[] = {&a};
-    if (a.nx > 0) FS_CK(fs_coop_launch((const void *)k_guess_fit<float>, G, fs_coop_block(ctx), args, ctx->st));
+    if (a.nx > 0) FS_CK(fs_coop_launch(guess_fit_kernel<float>(a.nx), G, fs_coop_block(ctx), args, ctx->st));
     FS_TIMING(FS_CK(cudaEventRecord(ctx->kev[nf - 1][0], ctx->st)));
     const void *k = gs ? (const void *)k_amg_bicgstab<float, 2>
                     : fused ? (const void *)k_amg_bicgstab<float, 1> : (const void *)k_amg_bicgstab<float, 0>;
@@ -1126,7 +1157,7 @@ int fs_pc_batch_create(fs_ctx **cs, int n, const double *weight, fs_pc_batch **o
 int fs_pc_batch_launch(fs_pc_batch *B, fs_ctx **cs, int n, cudaStream_t st) {
   if (!B || !cs || n != B->n) return FS_E_ARG;
   fs_ctx *ctx = cs[0];
-  bool nx_any = false;
+  unsigned nx_mask = 0;
   for (int q = 0; q < n; q++) {
     fs_mg_dev *M = cs[q]->mg;
     if (!M || M->pend_form != B->form) { ctx->err = "batched p' launch: a context prepared no matching solve"; return FS_E_ARG; }
@@ -1134,12 +1165,12 @@ int fs_pc_batch_launch(fs_pc_batch *B, fs_ctx **cs, int n, cudaStream_t st) {
     if (B->form <= 1) {
       AmgKArgs<double> a = M->pend64;
       a.teambar = B->d_words + 2 * q;
-      nx_any |= a.nx > 0;
+      if (a.nx > 0 && a.nx <= FS_GUESS_MAX) nx_mask |= 1u << a.nx;
       memcpy(dst, &a, sizeof(a));
     } else {
       AmgKArgs<float> a = M->pend32;
       a.teambar = B->d_words + 2 * q;
-      nx_any |= a.nx > 0;
+      if (a.nx > 0 && a.nx <= FS_GUESS_MAX) nx_mask |= 1u << a.nx;
       memcpy(dst, &a, sizeof(a));
     }
     M->pend_form = -1;
@@ -1147,9 +1178,13 @@ int fs_pc_batch_launch(fs_pc_batch *B, fs_ctx **cs, int n, cudaStream_t st) {
   FS_CK(cudaMemcpyAsync(B->d_args, B->h_args, B->argsz * n, cudaMemcpyHostToDevice, st));
   unsigned *gw = B->d_words + 2 * n;
   void *args[] = {&B->d_args, &B->d_start, &B->n, &gw};
-  if (nx_any) {   // the initial guesses, same groups; the barrier words start from zero for each launch
+  // the initial guesses, same groups: one launch per basis size present (a
+  // group sits out the launches of other sizes); the barrier words start from
+  // zero for each launch
+  for (int nx = 1; nx <= FS_GUESS_MAX; nx++) {
+    if (!(nx_mask & (1u << nx))) continue;
     FS_CK(cudaMemsetAsync(B->d_words, 0, sizeof(unsigned) * 4 * n, st));
-    FS_CK(fs_coop_launch(B->form <= 1 ? (const void *)k_guess_fit_batch<double> : (const void *)k_guess_fit_batch<float>,
+    FS_CK(fs_coop_launch(B->form <= 1 ? guess_fit_batch_kernel<double>(nx) : guess_fit_batch_kernel<float>(nx),
                          B->ncta, FS_COOP_BLOCK, args, st));
     FS_LAUNCH_CHECK();
   }
