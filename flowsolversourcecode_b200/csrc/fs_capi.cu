@@ -215,7 +215,7 @@ int fs_create(const fs_mesh_in *mesh, const fs_case *cfg, int device, fs_ctx **o
   double **bnd3[] = {&ctx->bug, &ctx->bvg, &ctx->bwg, &ctx->bpg, &ctx->bpcg};
   for (auto p : bnd3) if ((rc = alloc0(ctx, p, 3 * B))) return fail(rc);
   size_t nblk = (size_t)fs_grid((long)N);
-  size_t nred = 8 * (nblk > FS_RED_BLOCKS ? nblk : FS_RED_BLOCKS);
+  size_t nred = 16 * (nblk > FS_RED_BLOCKS ? nblk : FS_RED_BLOCKS);   // three components' partials (k_mom_finish3)
   if ((rc = alloc0(ctx, &ctx->red, nred))) return fail(rc);
   if (cudaMalloc(&ctx->redi, sizeof(int64_t) * (nblk > FS_RED_BLOCKS ? nblk : FS_RED_BLOCKS)) != cudaSuccess) return fail(FS_E_NOMEM);
   if ((rc = alloc0(ctx, &ctx->resblk, RB_SIZE))) return fail(rc);
@@ -502,8 +502,7 @@ static int iteration_mom(fs_ctx *ctx) {
   int rc;
   FS_TIMING(cudaEventRecord(ctx->ev[0], ctx->st));
   if (ctx->cfg.batched_momentum && ctx->cfg.solver_mom == FS_SOLVER_SOR) {
-    for (int c = 0; c < 3; c++)
-      if ((rc = fs_momentum_assemble_to(ctx, c, ctx->ac3 + (size_t)c * ctx->N, ctx->bc3 + (size_t)c * ctx->N))) return rc;
+    if ((rc = fs_momentum_assemble3(ctx))) return rc;
     if ((rc = fs_momentum_batched_solve(ctx))) return rc;
   } else {
     for (int c = 0; c < 3; c++) {

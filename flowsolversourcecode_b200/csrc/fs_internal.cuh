@@ -250,6 +250,7 @@ int fs_gradient_dev(fs_ctx *ctx, int nfld, const int *vars, const double *const 
                     const int *method, const int *niter);
 int fs_momentum_assemble(fs_ctx *ctx, int comp);
 int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac, double *bc);
+int fs_momentum_assemble3(fs_ctx *ctx);   // u, v, w into ac3/bc3 (multi-RHS form)
 int fs_momentum_batched_solve(fs_ctx *ctx);
 int fs_continuity_assemble(fs_ctx *ctx);
 int fs_continuity_correct(fs_ctx *ctx);

@@ -353,11 +353,9 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_MOM_MINB) k_mom_interior(MomArgs 
 // TURB: boundary faces diffuse with BeDiffCoefficient (wall functions on no-slip
 // walls) and FluxTE takes MinusTwoThirdsRhoK (AssembleMinusTwoThirdsRhoK.for:96-110).
 template <bool TURB>
-__global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a, int comp) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = i < a.N;
-  double r = 0., acphi = -1.;
-  if (live) {
+__device__ __forceinline__ void mom_finish_cell(const MomArgs &a, int comp, int i, double *ac_o, double *bc_o,
+                                                double *d1_o, double *d2_o, double *star_o, double &r, double &acphi) {
+  {
     const int N = a.N, F = a.F, B = a.B;
     const long N2 = 2L * N, B2 = 2L * B;
     const double mu = a.mu;
@@ -445,11 +443,41 @@ __global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a
       for (int j = 0; j < nc; j++) sa = sa + a.anb[(long)j * N + i];
       d2 = V / sa;
     }
-    a.ac[i] = ac; a.bc[i] = bc; a.d1[i] = d1; a.d2[i] = d2; a.star[i] = phi;
+    ac_o[i] = ac; bc_o[i] = bc; d1_o[i] = d1; d2_o[i] = d2; star_o[i] = phi;
     r = fabs(bc);
     acphi = fabs(ac * phi);
   }
+}
+
+template <bool TURB>
+__global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish(MomArgs a, int comp) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double r = 0., acphi = -1.;
+  if (i < a.N) mom_finish_cell<TURB>(a, comp, i, a.ac, a.bc, a.d1, a.d2, a.star, r, acphi);
   residual_partials(r, acphi, a.red, a.nblk);
+}
+
+// the three components in one launch (the multi-RHS form assembles u, v, w
+// from the same fields): a thread finishes its cell for u, v, then w, so the
+// cell's slots, coefficients and volume come from cache after the first; the
+// residual partials of component c go to red + RED_NQ c nblk
+struct MomOut3 {
+  double *ac[3], *bc[3], *d1[3], *d2[3], *star[3];
+};
+template <bool TURB>
+__global__ void __launch_bounds__(FS_BLOCK, FS_FACE_MINB) k_mom_finish3(MomArgs a, MomOut3 o) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll 1
+  for (int comp = 0; comp < 3; comp++) {
+    double r = 0., acphi = -1.;
+    double *ac_o = comp == 0 ? o.ac[0] : comp == 1 ? o.ac[1] : o.ac[2];
+    double *bc_o = comp == 0 ? o.bc[0] : comp == 1 ? o.bc[1] : o.bc[2];
+    double *d1_o = comp == 0 ? o.d1[0] : comp == 1 ? o.d1[1] : o.d1[2];
+    double *d2_o = comp == 0 ? o.d2[0] : comp == 1 ? o.d2[1] : o.d2[2];
+    double *st_o = comp == 0 ? o.star[0] : comp == 1 ? o.star[1] : o.star[2];
+    if (i < a.N) mom_finish_cell<TURB>(a, comp, i, ac_o, bc_o, d1_o, d2_o, st_o, r, acphi);
+    residual_partials(r, acphi, a.red + (long)RED_NQ * comp * a.nblk, a.nblk);
+  }
 }
 
 // ------------------------------------------------------------ continuity
@@ -1023,11 +1051,46 @@ static MomArgs mom_args(fs_ctx *ctx) {
 // SolveMomentumX/Y/Z up to (not including) SolveEquation
 int fs_momentum_assemble(fs_ctx *ctx, int comp) { return fs_momentum_assemble_to(ctx, comp, ctx->ac, ctx->bc); }
 
+static int mom_prologue(fs_ctx *ctx);
+
+// u, v and w into ac3/bc3 (the multi-RHS form): the same kernels as three
+// fs_momentum_assemble_to calls, with the three finishing launches as one
+// (k_mom_finish3) when no k-epsilon wall treatment runs between them
+int fs_momentum_assemble3(fs_ctx *ctx) {
+  const int N = ctx->N;
+  if (ctx->turb) {
+    for (int c = 0; c < 3; c++) {
+      int rc = fs_momentum_assemble_to(ctx, c, ctx->ac3 + (size_t)c * N, ctx->bc3 + (size_t)c * N);
+      if (rc) return rc;
+    }
+    return FS_OK;
+  }
+  int rc = mom_prologue(ctx);
+  if (rc) return rc;
+  MomArgs a = mom_args(ctx);
+  MomOut3 o;
+  double *d1[3] = {ctx->du1, ctx->dv1, ctx->dw1}, *d2[3] = {ctx->du2, ctx->dv2, ctx->dw2};
+  double *st[3] = {ctx->us, ctx->vs, ctx->ws};
+  for (int c = 0; c < 3; c++) {
+    o.ac[c] = ctx->ac3 + (size_t)c * N; o.bc[c] = ctx->bc3 + (size_t)c * N;
+    o.d1[c] = d1[c]; o.d2[c] = d2[c]; o.star[c] = st[c];
+  }
+  k_mom_finish3<false><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a, o);
+  FS_LAUNCH_CHECK();
+  for (int c = 0; c < 3; c++) {
+    k_residual_final<<<1, 1024, 0, ctx->st>>>(ctx->red + (size_t)RED_NQ * c * a.nblk, a.nblk, N, c, ctx->resblk);
+    FS_LAUNCH_CHECK();
+  }
+  return FS_OK;
+}
+
 // the same, writing the component's ac/bc to the given arrays
-int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac_out, double *bc_out) {
+// gradients of u, v, w, p and the fused interior-face assembly of the three
+// components (the part of the X-momentum call that the Y and Z calls reuse)
+static int mom_prologue(fs_ctx *ctx) {
   const fs_case &c = ctx->cfg;
   const int N = ctx->N;
-  if (comp == 0) {
+  {
     int vars[4] = {FS_VAR_U, FS_VAR_V, FS_VAR_W, FS_VAR_P};
     const double *phi[4] = {ctx->u, ctx->v, ctx->w, ctx->p};
     const double *bphi[4] = {ctx->bu, ctx->bv, ctx->bw, ctx->bp};
@@ -1045,6 +1108,16 @@ int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac_out, double *bc_ou
     if (ctx->turb) k_mom_interior<true><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
     else k_mom_interior<false><<<fs_grid(N), FS_BLOCK, 0, ctx->st>>>(a);
     FS_LAUNCH_CHECK();
+  }
+  return FS_OK;
+}
+
+int fs_momentum_assemble_to(fs_ctx *ctx, int comp, double *ac_out, double *bc_out) {
+  const fs_case &c = ctx->cfg;
+  const int N = ctx->N;
+  if (comp == 0) {
+    int rc = mom_prologue(ctx);
+    if (rc) return rc;
   }
   if (ctx->turb && !c.inviscid) {
     int rc = fs_turb_wall_functions(ctx);

@@ -408,6 +408,33 @@ def test_batched_momentum_same_fixed_point():
         assert np.linalg.norm(x - y) <= 1e-8 * np.linalg.norm(x), k
 
 
+def test_three_component_finish_matches_per_component_assembly():
+    # the multi-RHS form finishes u, v, w in one launch; from the same fields
+    # the D values it leaves equal, bit for bit, those of the three separate
+    # X/Y/Z assemblies
+    from flowsolversourcecode_b200.solver import Solver
+    mesh, case = cs.cavity(10, nz=8, jitter=0.2, seed=1, re=400.0, conv_scheme="sou", niter_start_hr=1,
+                           batched_momentum=True)
+    a, b = Solver(mesh, case), Solver(mesh, case)
+    rng = np.random.default_rng(3)
+    for k in ("u", "v", "w", "p"):
+        x = 0.05 * rng.standard_normal(a.N)
+        a.set(k, x)
+        b.set(k, x)
+    a.set_iteration(1)
+    ref = {}
+    for c, names in enumerate((("du1", "du2"), ("dv1", "dv2"), ("dw1", "dw2"))):
+        a.assemble_momentum(c)
+        for k in names:
+            ref[k] = a.get(k)
+    b.set_iteration(0)
+    b.simple_iteration()
+    for k, x in ref.items():
+        assert np.array_equal(b.get(k), x), k
+    a.close()
+    b.close()
+
+
 def test_bounded_wait_runs_out_and_reports_timeout():
     # Failure detection without a GPU fault: the AMG preconditioner's team
     # barriers are made to wait for one CTA more than takes part, so their
