@@ -421,19 +421,27 @@ __device__ __forceinline__ void sor3_body(const Sor3Args &a, CT &C) {
         C.sync();
       }
     }
+    // |residual| sums of the active components.  The rows of the colour just
+    // solved satisfy their equations up to rounding (each was solved from
+    // neighbours of other colours, unchanged since), so only the other
+    // colours' rows are summed: half the pass on a two-colour mesh
     double s0 = 0., s1 = 0., s2 = 0.;
-    for (long i = tid0; i < N; i += 2 * nth) {
-      const long i2 = i + nth;
-      const bool h2 = i2 < N;
-      double l[3], m[3] = {0., 0., 0.};
+    const long lr0 = a.color_ptr[last], lr1 = a.color_ptr[last + 1];
+    for (int part = 0; part < 2; part++) {
+      const long q0 = part == 0 ? 0 : lr1, q1 = part == 0 ? lr0 : N;
+      for (long i = q0 + tid0; i < q1; i += 2 * nth) {
+        const long i2 = i + nth;
+        const bool h2 = i2 < q1;
+        double l[3], m[3] = {0., 0., 0.};
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        l[c] = a.bc3[c * (long)N + i] - a.ac3[c * (long)N + i] * a.x3[c * (long)N + i];
-        if (h2) m[c] = a.bc3[c * (long)N + i2] - a.ac3[c * (long)N + i2] * a.x3[c * (long)N + i2];
+        for (int c = 0; c < 3; c++) {
+          l[c] = a.bc3[c * (long)N + i] - a.ac3[c * (long)N + i] * a.x3[c * (long)N + i];
+          if (h2) m[c] = a.bc3[c * (long)N + i2] - a.ac3[c * (long)N + i2] * a.x3[c * (long)N + i2];
+        }
+        sub3x2(N, a.W, cn, anb, i, i2, h2, a.x3, l, m);
+        s0 += fabs(l[0]); s1 += fabs(l[1]); s2 += fabs(l[2]);
+        if (h2) { s0 += fabs(m[0]); s1 += fabs(m[1]); s2 += fabs(m[2]); }
       }
-      sub3x2(N, a.W, cn, anb, i, i2, h2, a.x3, l, m);
-      s0 += fabs(l[0]); s1 += fabs(l[1]); s2 += fabs(l[2]);
-      if (h2) { s0 += fabs(m[0]); s1 += fabs(m[1]); s2 += fabs(m[2]); }
     }
     double o0, o1, o2, d;
     ctas_sum2(C, a.part, buf, s0, s1, o0, o1);
