@@ -252,14 +252,21 @@ __global__ void __launch_bounds__(FS_COOP_BLOCK, FS_KRYLOV_MINB) k_sor_colour(So
         grid.sync();
       }
     }
+    // sum of |residual|: the rows of the colour just solved satisfy their
+    // equations up to rounding (solved from neighbours of other colours,
+    // unchanged since), so only the other colours' rows are summed
     double l0 = 0., dum;
-    for (long i = tid0; i < N; i += 2 * nth) {
-      const long i2 = i + nth;
-      const bool h2 = i2 < N;
-      double q1 = a.bc[i] - a.ac[i] * a.x[i], q2 = h2 ? a.bc[i2] - a.ac[i2] * a.x[i2] : 0.;
-      ell_acc2<6, true>(q1, q2, N, a.W, cn, anb, i, i2, h2, [&](int k) { return a.x[k]; });
-      l0 += fabs(q1);
-      if (h2) l0 += fabs(q2);
+    const long lr0 = a.color_ptr[last], lr1 = a.color_ptr[last + 1];
+    for (int part = 0; part < 2; part++) {
+      const long q0 = part == 0 ? 0 : lr1, qe = part == 0 ? lr0 : N;
+      for (long i = q0 + tid0; i < qe; i += 2 * nth) {
+        const long i2 = i + nth;
+        const bool h2 = i2 < qe;
+        double q1 = a.bc[i] - a.ac[i] * a.x[i], q2 = h2 ? a.bc[i2] - a.ac[i2] * a.x[i2] : 0.;
+        ell_acc2<6, true>(q1, q2, N, a.W, cn, anb, i, i2, h2, [&](int k) { return a.x[k]; });
+        l0 += fabs(q1);
+        if (h2) l0 += fabs(q2);
+      }
     }
     grid_sum2(grid, a.part, buf, l0, 0., fres, dum); buf ^= 1;
     iter++;
