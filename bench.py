@@ -457,7 +457,7 @@ def run_ensemble(args, world: int, rank: int, local: int, dist) -> None:
     del cases
     t_setup = time.time() - t0
     shapes = ens.autotune(shapes=(1, 2, 3, 4), iters=1)
-    split = ens.autotune_split(exponents=(0.75, 1.0, 1.25), iters=2)
+    split = ens.autotune_split(exponents=(0.75, 1.0, 1.25, 1.5), iters=2)
     launches = max(1, args.warmup)
     # both graph forms, each after one untimed launch of its own graph: cases in
     # sequence, and the p' solves of all cases in one launch (a CTA group each)

@@ -126,7 +126,7 @@ class Ensemble:
         self.shapes = best
         return best
 
-    def autotune_split(self, exponents=(0.5, 0.75, 1.0, 1.25), iters: int = 2) -> float:
+    def autotune_split(self, exponents=(0.75, 1.0, 1.25, 1.5), iters: int = 2) -> float:
         """Pick the exponent of the CTA split of the batched form (groups in
         proportion to cells^e) by timing one launch of an `iters`-iteration
         graph per candidate; the fastest is kept."""
