@@ -156,6 +156,7 @@ PROTOTYPES = {
     "fs_set_iteration": (C.c_int, [_V, C.c_int]),
     "fs_initialize_mdot": (C.c_int, [_V]),
     "fs_advance_time": (C.c_int, [_V, C.c_double]),
+    "fs_adaptive_time_step": (C.c_int, [_V, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "fs_neu_connectivity": (C.c_int, [C.POINTER(FsNeuIn)] + [C.POINTER(C.c_int32)] * 8),
     "fs_get_time": (C.c_int, [_V, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "fs_set_time": (C.c_int, [_V, C.POINTER(C.c_double), C.c_int32]),

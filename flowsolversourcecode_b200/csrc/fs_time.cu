@@ -189,3 +189,138 @@ int fs_set_time(fs_ctx *ctx, const double t[4], int32_t n_steps) {
   ctx->tscheme = scheme_in_effect(ctx->cfg.transient_scheme, n_steps > 0 ? n_steps - 1 : 0);
   return FS_OK;
 }
+
+// ------------------------------------------------ adaptive time step
+// AdaptiveTimeStep of a laminar, isothermal case (CalculateAdaptiveTimeStep.for:4-200
+// and the 'velx' branch of CalculateAdaptiveTimeStepValue, :203-1758).  The
+// reference scatters over faces into TimeStep(cell); here one thread per cell
+// gathers its slots (faces in increasing index) in the reference's loop order:
+// interior diffusion, the boundary lists in the order the reference visits
+// them, interior convection, boundary convection.  Each block writes the max
+// of TimeStep / (rho V) over its cells; one CTA reduces the partials.
+namespace {
+
+struct DtArgs {
+  int N, F, B, inviscid, nblk;
+  const int32_t *ncf, *slot, *btype;
+  const double *gf, *gdiff, *bfa, *bnf, *bdv, *bgdiff, *mdot, *bmdot, *vol;
+  double rho, mu;
+  double *part, *out;
+};
+
+__device__ __forceinline__ double block_max(double v, double *sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  return sh[0];
+}
+
+__global__ void __launch_bounds__(FS_BLOCK) k_adaptive_dt(DtArgs a) {
+  __shared__ double sh[FS_BLOCK];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double val = -1.;
+  if (i < a.N) {
+    const int N = a.N, F = a.F, B = a.B, nc = a.ncf[i];
+    const double mu = a.mu;
+    double ts = 0.;
+    if (!a.inviscid) {
+      for (int j = 0; j < nc; j++) {   // :329-346
+        const int f = a.slot[(long)j * N + i] >> 1;
+        if (f < F) {
+          const double g = a.gf[f];
+          const double gamf = g * mu + (1. - g) * mu;
+          ts = ts + gamf * a.gdiff[f];
+        }
+      }
+      // the boundary lists of :384-589, in that order
+      const int order[7] = {FS_BC_WALL_NOSLIP, FS_BC_INLET_VEL, FS_BC_INLET_MASS, FS_BC_INLET_SP,
+                            FS_BC_INLET_STAG, FS_BC_OUTLET_MASS, FS_BC_SYMMETRY};
+      for (int l = 0; l < 7; l++)
+        for (int j = 0; j < nc; j++) {
+          const int f = a.slot[(long)j * N + i] >> 1;
+          if (f < F) continue;
+          const int b = f - F;
+          if (a.btype[b] != order[l]) continue;
+          if (order[l] == FS_BC_WALL_NOSLIP || order[l] == FS_BC_SYMMETRY) {
+            const double nx = a.bnf[b], ny = a.bnf[B + b], nz = a.bnf[2L * B + b];
+            const double dN = a.bdv[b] * nx + a.bdv[B + b] * ny + a.bdv[2L * B + b] * nz;
+            const double area = a.bfa[b];
+            double fl;
+            if (order[l] == FS_BC_WALL_NOSLIP) {
+              fl = mu * area * (1. - nx * nx) / dN;
+              fl = fmax(fl, mu * area * (1. - ny * ny) / dN);
+              fl = fmax(fl, mu * area * (1. - nz * nz) / dN);
+            } else {
+              fl = 2. * mu * area * (nx * nx) / dN;
+              fl = fmax(fl, 2. * mu * area * (ny * ny) / dN);
+              fl = fmax(fl, 2. * mu * area * (nz * nz) / dN);
+            }
+            ts = ts + fl;
+          } else {
+            ts = ts + mu * a.bgdiff[b];
+          }
+        }
+    }
+    // convection (:1685-1708); the neighbour side subtracts, as the reference writes it
+    for (int j = 0; j < nc; j++) {
+      const int s = a.slot[(long)j * N + i], f = s >> 1;
+      if (f < F) ts = (s & 1) ? ts - fmax(-a.mdot[f], 0.) : ts + fmax(a.mdot[f], 0.);
+    }
+    for (int j = 0; j < nc; j++) {
+      const int f = a.slot[(long)j * N + i] >> 1;
+      if (f >= F) ts = ts + fmax(a.bmdot[f - F], 0.);
+    }
+    val = ts / (a.rho * a.vol[i]);
+  }
+  const double m = block_max(val, sh);
+  if (threadIdx.x == 0) a.part[blockIdx.x] = m;
+}
+
+__global__ void __launch_bounds__(1024) k_adaptive_dt_final(DtArgs a) {
+  __shared__ double sh[1024];
+  double m = -1.;
+  for (int b = threadIdx.x; b < a.nblk; b += blockDim.x) m = fmax(m, a.part[b]);
+  m = block_max(m, sh);
+  if (threadIdx.x == 0) *a.out = m;
+}
+
+}  // namespace
+
+int fs_adaptive_time_step(fs_ctx *ctx, double courant, double min_factor, double max_factor, double *dt_next) {
+  if (!ctx || !dt_next) return FS_E_ARG;
+  const fs_case &c = ctx->cfg;
+  if (!c.unsteady || !ctx->old) { ctx->err = "fs_adaptive_time_step: the case is not unsteady"; return FS_E_ARG; }
+  if (c.turbulence || c.energy) {
+    ctx->err = "fs_adaptive_time_step: laminar isothermal cases only (the k, epsilon and temperature limits are not built)";
+    return FS_E_ARG;
+  }
+  if (!(courant > 0.) || !(min_factor > 0.) || !(max_factor >= min_factor)) {
+    ctx->err = "fs_adaptive_time_step: courant and min_factor must be > 0 and max_factor >= min_factor";
+    return FS_E_ARG;
+  }
+  cudaSetDevice(ctx->dev);
+  DtArgs a{};
+  a.N = (int)ctx->N; a.F = (int)ctx->F; a.B = (int)ctx->B; a.inviscid = c.inviscid;
+  a.nblk = fs_grid(ctx->N);
+  a.ncf = ctx->ncf; a.slot = ctx->slot; a.btype = ctx->btype;
+  a.gf = ctx->gf; a.gdiff = ctx->gdiff; a.bfa = ctx->bfa; a.bnf = ctx->bnf; a.bdv = ctx->bdv;
+  a.bgdiff = ctx->bgdiff; a.mdot = ctx->mdot; a.bmdot = ctx->bmdot; a.vol = ctx->vol;
+  a.rho = c.rho; a.mu = c.mu;
+  a.part = ctx->red + (long)RED_MAX1 * a.nblk;   // ctx->red holds 16 x nblk doubles
+  a.out = ctx->red + (long)RED_NQ * a.nblk;
+  k_adaptive_dt<<<a.nblk, FS_BLOCK, 0, ctx->st>>>(a);
+  FS_LAUNCH_CHECK();
+  k_adaptive_dt_final<<<1, 1024, 0, ctx->st>>>(a);
+  FS_LAUNCH_CHECK();
+  double mx = 0.;
+  FS_CK(cudaMemcpyAsync(&mx, a.out, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  FS_CK(cudaStreamSynchronize(ctx->st));
+  // dtlocal = GlobalCourantNumber / max, then the change-factor clamp (:192-193)
+  double dtl = courant / mx;
+  dtl = fmax(dtl, min_factor * ctx->dt);
+  *dt_next = fmin(dtl, max_factor * ctx->dt);
+  return FS_OK;
+}

@@ -101,6 +101,17 @@ class Solver:
         self._chk(self.lib.fs_advance_time(self.ctx, float(dt_next)), "advance_time")
         self.nIter = 0
 
+    def adaptive_time_step(self, courant: float = 2.0, min_factor: float = 0.5, max_factor: float = 5.0) -> float:
+        """AdaptiveTimeStep (CalculateAdaptiveTimeStep.for:4-200) of a laminar,
+        isothermal case: the next dt from the current mass fluxes, clamped to
+        [min_factor dt, max_factor dt]; defaults are the reference's
+        GlobalCourantNumber, minimumdtChangeFactor and maximumdtChangeFactor
+        (ProblemDescriptionRoutine.for:544-546).  Pass it to advance_time."""
+        dt = C.c_double(0.)
+        self._chk(self.lib.fs_adaptive_time_step(self.ctx, float(courant), float(min_factor),
+                                                 float(max_factor), C.byref(dt)), "adaptive_time_step")
+        return dt.value
+
     def time_state(self) -> dict:
         t = (C.c_double * 4)()
         n = C.c_int32(0)

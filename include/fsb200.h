@@ -433,6 +433,20 @@ int fs_neu_connectivity(const fs_neu_in *in, int32_t *n_internal, int32_t *n_fac
  * dtOld = dt, dt = dt_next, time += dt and the outer-iteration counter
  * restarts (do nIter=1,IterMax).  Requires cfg.unsteady. */
 int fs_advance_time(fs_ctx *ctx, double dt_next);
+/* AdaptiveTimeStep (CalculateAdaptiveTimeStep.for:4-200; called from the time
+ * loop when LadaptiveTimeStep, MainProgram.for:235-241) for a laminar,
+ * isothermal unsteady case: the 'velx' limit of CalculateAdaptiveTimeStepValue
+ * (:203-1758) from the current mass fluxes -- per cell the diffusion sum
+ * gamf gDiff of its faces with the boundary terms of no-slip walls, inlets,
+ * mass-flow outlets and symmetry, plus the convection max(mdot, 0) terms --
+ * dtlocal = courant / max over cells of that sum / (rho V), and
+ * *dt_next = min(max(dtlocal, min_factor dt), max_factor dt) with dt the
+ * current time step.  The reference's defaults are GlobalCourantNumber 2,
+ * minimumdtChangeFactor 0.5, maximumdtChangeFactor 5
+ * (ProblemDescriptionRoutine.for:544-546).  Pass *dt_next to
+ * fs_advance_time.  FS_E_ARG for steady, turbulent or energy cases (their
+ * k, epsilon and temperature limits are not built).  Synchronises ctx's stream. */
+int fs_adaptive_time_step(fs_ctx *ctx, double courant, double min_factor, double max_factor, double *dt_next);
 /* Time state: t[0] time, t[1] dt, t[2] dtOld, t[3] dtOldOld, and ndt (the
  * number of time steps taken).  fs_set_time restores it for a restart
  * (readSolution, ReadSolutionToContinue.for:59-108, restores the old time

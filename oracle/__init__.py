@@ -61,6 +61,8 @@ def load():
         lib.om_neu_connectivity_literal.restype = C.c_int
         lib.om_neu_connectivity_literal.argtypes = [C.c_void_p] + [C.POINTER(C.c_int32)] * 8
         lib.om_advance_time.argtypes = [C.c_void_p, C.c_double]
+        lib.om_adaptive_dt.restype = C.c_double
+        lib.om_adaptive_dt.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
         lib.om_get_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         lib.om_set_time.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
         lib.om_mg_setup.restype = C.c_int
@@ -174,6 +176,11 @@ class Oracle:
         """Time-step prologue of the unsteady loop (MainProgram.for:184-245)."""
         self.lib.om_advance_time(self.h, float(dt_next))
         self.nIter = 0
+
+    def adaptive_time_step(self, courant: float = 2.0, min_factor: float = 0.5, max_factor: float = 5.0) -> float:
+        """AdaptiveTimeStep of a laminar, isothermal case (CalculateAdaptiveTimeStep.for:4-200):
+        the next dt from the current mass fluxes, clamped to [min_factor dt, max_factor dt]."""
+        return self.lib.om_adaptive_dt(self.h, float(courant), float(min_factor), float(max_factor))
 
     def get_time(self) -> dict:
         t = (C.c_double * 4)()

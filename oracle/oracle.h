@@ -47,6 +47,7 @@ int    om_neu_connectivity_literal(const fs_neu_in *in, int *n_internal, int *n_
                                    int *face_nodes, int *owner, int *neighbour, int *cell_face_ptr,
                                    int *cell_faces);   /* GlobalConnectivity, O(N^2) as written */
 void   om_advance_time(om *m, double dt_next);  /* time-step prologue (MainProgram.for:184-245) */
+double om_adaptive_dt(om *m, double courant, double min_factor, double max_factor);  /* AdaptiveTimeStep, laminar */
 void   om_get_time(om *m, double t[4], int *ndt);        /* time, dt, dtOld, dtOldOld; ndt */
 void   om_set_time(om *m, const double t[4], int ndt);
 void   om_turb_production(om *m);              /* strain rate + k-epsilon production (into "prod") */

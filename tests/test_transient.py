@@ -257,3 +257,84 @@ def test_unsteady_restart_continues_bitwise(tmp_path):
     for k in STATE + ("old", "oldold"):
         assert np.array_equal(runs[0][k], runs[1][k]), k
     assert runs[0]["t"] == runs[1]["t"]
+
+
+# ------------------------------------------------- adaptive time step
+def test_oracle_adaptive_time_step_at_rest():
+    """AdaptiveTimeStep on a uniform n^3 cavity at rest (mdot = 0): a corner
+    cell has three interior faces (mu h each) and three no-slip wall faces
+    (mu h^2 / (h/2) each), the largest diffusion sum, 9 mu h; so dtlocal =
+    Courant rho h^2 / (9 mu), then the change-factor clamp."""
+    import oracle
+    n = 6
+    m, c = cs.cavity(n, jitter=0.0, unsteady=True, transient_scheme="euler", dt=0.05)
+    o = oracle.Oracle(m, c)
+    h = 1.0 / n
+    want = 2.0 * c.rho * h * h / (9.0 * c.mu)
+    got = o.adaptive_time_step(2.0, 1e-6, 1e6)
+    assert abs(got - want) <= 1e-13 * want
+    # clamps against the current dt (0.05): [0.5 dt, 5 dt]
+    assert o.adaptive_time_step(2.0, 0.5, 5.0) == pytest.approx(min(max(want, 0.025), 0.25), rel=1e-13)
+    assert o.adaptive_time_step(1e-9, 0.5, 5.0) == 0.025
+    assert o.adaptive_time_step(1e9, 0.5, 5.0) == 0.25
+
+
+def _adaptive_case(which):
+    kw = dict(unsteady=True, transient_scheme="euler", dt=0.05, solver_mom="bicgs", solver_cont="bicgs",
+              krylov_tol=1e-13, krylov_maxit=400)
+    if which == "cavity3d":
+        return cs.cavity(8, nz=6, jitter=0.2, seed=0, **kw)
+    if which == "cavity2d":   # z patches are symmetry planes
+        return cs.cavity(10, nz=1, jitter=0.2, seed=1, **kw)
+    return cs.bfs(24, 9, 6, re_h=100.0, turbulence=False, **kw)   # velocity inlet, fully developed outlet
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["cavity3d", "cavity2d", "step"])
+def test_adaptive_time_step_matches_oracle(which):
+    """fs_adaptive_time_step against the restatement on the same state (the
+    oracle's mass fluxes copied into the device context): the unclamped
+    dtlocal and the clamped dt agree to 1e-13 relative, over two time steps
+    of no-slip walls, symmetry planes and a velocity inlet with outflow."""
+    import oracle
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = _adaptive_case(which)
+    o = oracle.Oracle(m, c)
+    g = Solver(m, c)
+    if which == "step":
+        for k, v in cs.bfs_initial_state(m, c, seed=0).items():
+            o.set(k, v)
+            g.set(k, v)
+        o.initialize_mdot()
+        g.initialize_mdot()
+    else:
+        _seed(o, o.N, 3)
+        _seed(g, o.N, 3)
+    for step in range(2):
+        o.simple_iteration()
+        g.simple_iteration()
+        for k in ("mdot", "bmdot"):
+            g.set(k, o.get(k))
+        free_o = o.adaptive_time_step(2.0, 1e-9, 1e9)
+        free_g = g.adaptive_time_step(2.0, 1e-9, 1e9)
+        assert free_o > 0.0
+        assert abs(free_g - free_o) <= 1e-13 * free_o, (step, free_g, free_o)
+        dt_o = o.adaptive_time_step()
+        dt_g = g.adaptive_time_step()
+        assert abs(dt_g - dt_o) <= 1e-13 * dt_o, (step, dt_g, dt_o)
+        o.advance_time(dt_o)
+        g.advance_time(dt_o)
+    assert g.time_state()["dt"] == o.get_time()["dt"]
+    g.close()
+
+
+@pytest.mark.gpu
+def test_adaptive_time_step_rejects_unbuilt_forms():
+    """Turbulent (and energy) cases have k, epsilon and temperature limits
+    the device path does not build: the call fails with FS_E_ARG."""
+    from flowsolversourcecode_b200.solver import Solver
+    m, c = cs.bfs(24, 9, 6, turbulence=True, unsteady=True, transient_scheme="euler", dt=0.05)
+    g = Solver(m, c)
+    with pytest.raises(Exception):
+        g.adaptive_time_step()
+    g.close()
